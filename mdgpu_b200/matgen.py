@@ -1,0 +1,146 @@
+"""Seeded synthetic SPD test matrices with the shapes of the benchmark workloads.
+
+All generators return the LOWER triangle (diagonal included) in compressed
+sparse column form ``(n, Ap, Ai, Ax)`` with int32 indices, row indices sorted
+ascending inside each column -- the layout the reference's ``cs`` struct holds
+after ``cs_compress`` of a column-sorted triplet file (cs.cpp:251).
+
+``write_triplets`` writes the reference's input format: a headerless text file
+of 1-based ``i j x`` lines (cs.cpp:4-27), lower triangle only, one entry per
+line in column-major order, values printed with 17 significant digits so the
+reference parses exactly the doubles generated here.
+
+Grid numbering is lexicographic, node (x, y, z) -> x + nx*(y + ny*z).  Edge
+conductances are drawn from ``numpy.random.default_rng(seed)`` (PCG64) in a
+fixed order: all x-edges, then y-edges, then z-edges, each block in node
+order of the edge's lower endpoint.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _edges_grid(dims):
+    """Return (lo, hi, axis) arrays of the 2*d-point stencil edges of a grid."""
+    dims = tuple(int(d) for d in dims)
+    idx = np.arange(int(np.prod(dims)), dtype=np.int64).reshape(dims[::-1])  # [z][y][x]
+    los, his = [], []
+    nd = len(dims)
+    for ax in range(nd):
+        # axis 0 is x which is the last axis of idx
+        a = nd - 1 - ax
+        sl_lo = [slice(None)] * nd
+        sl_hi = [slice(None)] * nd
+        sl_lo[a] = slice(0, dims[ax] - 1)
+        sl_hi[a] = slice(1, dims[ax])
+        lo = idx[tuple(sl_lo)].ravel()
+        hi = idx[tuple(sl_hi)].ravel()
+        order = np.argsort(lo, kind="stable")
+        los.append(lo[order])
+        his.append(hi[order])
+    return los, his
+
+
+def _assemble_lower(n, rows, cols, vals):
+    """Sum duplicate (row, col) lower-triangle entries and build sorted CSC."""
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    vals = np.asarray(vals, dtype=np.float64)
+    assert np.all(rows >= cols)
+    key = cols * n + rows
+    order = np.argsort(key, kind="stable")
+    key = key[order]
+    vals = vals[order]
+    uniq, start = np.unique(key, return_index=True)
+    sums = np.add.reduceat(vals, start) if len(vals) else vals
+    c = (uniq // n).astype(np.int64)
+    r = (uniq % n).astype(np.int32)
+    Ap = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(Ap, c + 1, 1)
+    Ap = np.cumsum(Ap).astype(np.int32)
+    return n, Ap, r.astype(np.int32), sums.astype(np.float64)
+
+
+def laplacian_grid(dims, *, seed=None, sigma=1.0, shift=0.0, const=None):
+    """Variable- or constant-coefficient 2D/3D grid Laplacian, lower CSC.
+
+    ``const=(diag, off)`` gives the constant stencil (e.g. ``(4, -1)`` for the
+    2D 5-point Dirichlet Laplacian).  Otherwise each edge has conductance
+    c ~ lognormal(0, sigma) drawn from ``default_rng(seed)``; off-diagonals
+    are -c and the diagonal is the sum of incident conductances + ``shift``.
+    """
+    dims = tuple(int(d) for d in dims)
+    n = int(np.prod(dims))
+    los, his = _edges_grid(dims)
+    lo = np.concatenate(los)
+    hi = np.concatenate(his)
+    if const is not None:
+        d, off = const
+        cond = np.full(lo.shape, -float(off))
+        diag = np.full(n, float(d))
+    else:
+        rng = np.random.default_rng(seed)
+        cond = np.concatenate([rng.lognormal(0.0, sigma, size=len(l)) for l in los])
+        diag = np.full(n, float(shift))
+        np.add.at(diag, lo, cond)
+        np.add.at(diag, hi, cond)
+    rows = np.concatenate([np.arange(n), hi])
+    cols = np.concatenate([np.arange(n), lo])
+    vals = np.concatenate([diag, -cond])
+    return _assemble_lower(n, rows, cols, vals)
+
+
+def laplacian_2d_5pt(side=100):
+    """2D 5-point Dirichlet Laplacian: diagonal 4, off-diagonals -1."""
+    return laplacian_grid((side, side), const=(4.0, -1.0))
+
+
+def laplacian_3d_varcoef(side=64, seed=0, sigma=1.0, shift=1e-3):
+    """3D 7-point Laplacian with lognormal(0, sigma) edge conductances."""
+    return laplacian_grid((side, side, side), seed=seed, sigma=sigma, shift=shift)
+
+
+def random_spd(n, density=0.05, seed=0):
+    """Random sparse SPD matrix (diagonally dominant), lower CSC."""
+    rng = np.random.default_rng(seed)
+    m = max(1, int(density * n * (n - 1) / 2))
+    r = rng.integers(0, n, size=m)
+    c = rng.integers(0, n, size=m)
+    keep = r != c
+    r, c = r[keep], c[keep]
+    lo = np.minimum(r, c)
+    hi = np.maximum(r, c)
+    v = -rng.uniform(0.1, 1.0, size=len(lo))
+    diag = np.full(n, 1.0)
+    np.add.at(diag, lo, -v)
+    np.add.at(diag, hi, -v)
+    rows = np.concatenate([np.arange(n), hi])
+    cols = np.concatenate([np.arange(n), lo])
+    vals = np.concatenate([diag, v])
+    return _assemble_lower(n, rows, cols, vals)
+
+
+def rhs_uniform(n, seed=0, nrhs=1):
+    """Right-hand sides with entries i.i.d. U(-1, 1), column-major (n, nrhs)."""
+    rng = np.random.default_rng(seed)
+    b = rng.uniform(-1.0, 1.0, size=(nrhs, n)).T
+    return np.ascontiguousarray(b if nrhs > 1 else b[:, 0])
+
+
+def lower_to_full_scipy(n, Ap, Ai, Ax):
+    """Full symmetric scipy CSC matrix from the lower CSC triple."""
+    import scipy.sparse as sp
+
+    L = sp.csc_matrix((Ax, Ai, Ap), shape=(n, n))
+    return (L + sp.tril(L, -1).T).tocsc()
+
+
+def write_triplets(path, n, Ap, Ai, Ax):
+    """Write the reference's headerless 1-based ``i j x`` triplet file."""
+    cols = np.repeat(np.arange(n, dtype=np.int64), np.diff(Ap))
+    with open(path, "w") as f:
+        lines = [
+            "%d %d %.17g\n" % (int(i) + 1, int(j) + 1, float(x))
+            for i, j, x in zip(Ai, cols, Ax)
+        ]
+        f.writelines(lines)

@@ -1,0 +1,187 @@
+"""ctypes front-end of the oracle (liboracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module; the product never does.  ``run`` mirrors
+the reference driver (mdgpu.cu:1745-1972) on a lower-triangular CSC matrix and
+returns every intermediate the parity tests compare.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_HARNESS = os.path.join(HERE, "_ref", "mdgpu_ref_harness")
+
+MODES = {"nodal": 0, "sn": 1, "rn": 2}
+
+_lib = None
+
+
+def build():
+    """Compile the restatement with gcc (oracle/Makefile)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+            os.path.join(HERE, "mdgpu_oracle.c")
+        ):
+            build()
+        L = C.CDLL(LIB_PATH)
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        L.orc_analyze.argtypes = [C.c_int, i32p, i32p, f64p, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(C.c_void_p)]
+        L.orc_analyze.restype = C.c_int
+        L.orc_plan_free.argtypes = [C.c_void_p]
+        for f in ("orc_plan_n", "orc_plan_nsuper", "orc_plan_nchild_total", "orc_plan_nnz_low"):
+            getattr(L, f).argtypes = [C.c_void_p]
+            getattr(L, f).restype = C.c_int
+        L.orc_plan_lnz.argtypes = [C.c_void_p]
+        L.orc_plan_lnz.restype = C.c_longlong
+        L.orc_plan_copy.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        L.orc_factor.argtypes = [C.c_void_p, C.c_int, i32p, f64p, C.POINTER(C.c_double),
+                                 C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_factor.restype = C.c_int
+        L.orc_solve.argtypes = [C.c_void_p, i32p, f64p, f64p, f64p]
+        L.orc_residual.argtypes = [C.c_int, i32p, i32p, f64p, f64p, f64p]
+        L.orc_residual.restype = C.c_double
+        L.orc_amd.argtypes = [C.c_int, i32p, i32p, i32p]
+        L.orc_etree.argtypes = [C.c_int, i32p, i32p, i32p]
+        L.orc_post.argtypes = [C.c_int, i32p, i32p]
+        L.orc_counts.argtypes = [C.c_int, i32p, i32p, i32p, i32p, i32p]
+        L.orc_front_factor.argtypes = [C.c_int, C.c_int, C.c_int, f64p]
+        _lib = L
+    return _lib
+
+
+class Plan:
+    """Owns an orc_plan*; fields are copied out as numpy arrays."""
+
+    def __init__(self, n, Ap, Ai, Ax, amd=True, mode="sn", rn_zeros=0):
+        L = lib()
+        self._p = C.c_void_p()
+        rc = L.orc_analyze(int(n), np.ascontiguousarray(Ap, np.int32),
+                           np.ascontiguousarray(Ai, np.int32),
+                           np.ascontiguousarray(Ax, np.float64), int(bool(amd)), MODES[mode],
+                           int(rn_zeros), C.byref(self._p))
+        if rc != 0:
+            raise ValueError("oracle analyze failed (%d)" % rc)
+        self.n = L.orc_plan_n(self._p)
+        self.nsuper = L.orc_plan_nsuper(self._p)
+        self.lnz = L.orc_plan_lnz(self._p)
+        nk = L.orc_plan_nchild_total(self._p)
+        nnz = L.orc_plan_nnz_low(self._p)
+        n, ns = self.n, self.nsuper
+        sizes = {"perm": n, "parent": n, "post": n, "count0": n, "count": n, "rn_perm": n,
+                 "sn_nodo": ns, "sn_cols": ns, "sn_childptr": ns + 1, "sn_child": nk,
+                 "Lp": n + 1, "Ap": n + 1, "Ai": nnz}
+        self.has_perm = bool(amd) or mode == "rn"
+        for k, sz in sizes.items():
+            if k == "perm" and not self.has_perm:
+                setattr(self, k, None)
+                continue
+            if k == "rn_perm" and mode != "rn":
+                setattr(self, k, None)
+                continue
+            a = np.zeros(max(sz, 1), np.int32)
+            L.orc_plan_copy(self._p, k.encode(), a.ctypes.data)
+            setattr(self, k, a[:sz])
+        self.Ax = np.zeros(max(nnz, 1), np.float64)
+        L.orc_plan_copy(self._p, b"Ax", self.Ax.ctypes.data)
+        self.Ax = self.Ax[:nnz]
+
+    def factor(self, block_size=0, maps=False):
+        L = lib()
+        Li = np.zeros(max(self.lnz, 1), np.int32)
+        Lx = np.zeros(max(self.lnz, 1), np.float64)
+        flops = C.c_double()
+        rows_ptr = rows = relmap = None
+        args = [None, None, None]
+        if maps:
+            rows_ptr = np.zeros(self.nsuper + 1, np.int32)
+            tot = int(sum(self.count[self.sn_nodo]))
+            rows = np.zeros(max(tot, 1), np.int32)
+            relmap = np.zeros(max(tot, 1), np.int32)
+            args = [rows_ptr.ctypes.data, rows.ctypes.data, relmap.ctypes.data]
+        rc = L.orc_factor(self._p, int(block_size), Li, Lx, C.byref(flops), *args)
+        out = {"Li": Li[: self.lnz], "Lx": Lx[: self.lnz], "flops": flops.value, "status": rc}
+        if maps:
+            out.update(rows_ptr=rows_ptr, rows=rows[: rows_ptr[-1]], relmap=relmap[: rows_ptr[-1]])
+        return out
+
+    def solve(self, Li, Lx, b):
+        x = np.zeros(self.n, np.float64)
+        lib().orc_solve(self._p, np.ascontiguousarray(Li, np.int32),
+                        np.ascontiguousarray(Lx, np.float64),
+                        np.ascontiguousarray(b, np.float64), x)
+        return x
+
+    def __del__(self):
+        try:
+            if self._p:
+                lib().orc_plan_free(self._p)
+        except Exception:
+            pass
+
+
+def residual(n, Ap, Ai, Ax, x, b):
+    return lib().orc_residual(int(n), np.ascontiguousarray(Ap, np.int32),
+                              np.ascontiguousarray(Ai, np.int32),
+                              np.ascontiguousarray(Ax, np.float64),
+                              np.ascontiguousarray(x, np.float64),
+                              np.ascontiguousarray(b, np.float64))
+
+
+def front_factor(F, cols, block_size=0):
+    """Dense partial Cholesky of one column-major square front (in place copy)."""
+    F = np.array(F, dtype=np.float64, order="F")
+    n = F.shape[0]
+    buf = np.ascontiguousarray(F.T).ravel()  # column-major flattening
+    lib().orc_front_factor(n, int(cols), int(block_size), buf)
+    return buf.reshape(n, n).T
+
+
+def run_reference(matrix_file, outdir, amd=True, mode="sn", rn_zeros=0, block=0, bfile=None,
+                  factor=True, timeout=None):
+    """Run the compiled reference (oracle/_ref) and load its outputs."""
+    args = [REF_HARNESS]
+    if amd:
+        args.append("-amd")
+    if mode == "sn":
+        args.append("-sn")
+    elif mode == "rn":
+        args += ["-rn", str(rn_zeros)]
+    if block:
+        args += ["-b", str(block)]
+    if not factor:
+        args.append("-nofactor")
+    if bfile:
+        args += ["-bfile", bfile]
+    args += [matrix_file, outdir]
+    os.makedirs(outdir, exist_ok=True)
+    subprocess.run(args, check=True, capture_output=True, timeout=timeout)
+    return load_dir(outdir)
+
+
+def load_dir(d):
+    import json
+
+    out = {}
+    for f in os.listdir(d):
+        p = os.path.join(d, f)
+        if f.endswith(".i32"):
+            out[f[:-4]] = np.fromfile(p, dtype=np.int32)
+        elif f.endswith(".f64"):
+            out[f[:-4]] = np.fromfile(p, dtype=np.float64)
+        elif f == "meta.json":
+            with open(p) as fh:
+                out["meta"] = json.load(fh)
+    return out
