@@ -1,0 +1,138 @@
+/*
+ * mdgpu_b200 -- C ABI of the B200 multifrontal sparse Cholesky.
+ *
+ * Plain pointers and sizes only.  Index arrays are 32-bit `int` like the
+ * reference's CSparse `cs` struct (cs.h:20-29); values are `double` (the
+ * reference's FLOTANTE in its FP64 build, types.h:13-22).  The input matrix is
+ * the LOWER triangle, diagonal included, in compressed-column form with sorted
+ * row indices -- what the reference holds after cs_load + cs_compress
+ * (mdgpu.cu:1724-1729).
+ *
+ * Every function returns an mdgpu_status (0 = success).  There is no global
+ * state: one handle per sparsity pattern; calls on different handles may run
+ * concurrently from different host threads.  A handle must not be used by two
+ * host threads at once.
+ */
+#ifndef MDGPU_B200_H
+#define MDGPU_B200_H
+
+#if defined(__GNUC__)
+#define MDGPU_API __attribute__((visibility("default")))
+#else
+#define MDGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mdgpu_handle_s *mdgpu_handle;
+
+enum mdgpu_status {
+    MDGPU_OK = 0,
+    MDGPU_ERR_INVALID = -1,   /* bad argument or pattern */
+    MDGPU_ERR_NOT_SPD = -2,   /* non-positive pivot; see mdgpu_not_spd_column */
+    MDGPU_ERR_OOM = -3,       /* device or host allocation failed */
+    MDGPU_ERR_CUDA = -4,      /* CUDA runtime error (message: mdgpu_last_error) */
+    MDGPU_ERR_NOT_TREE = -5,  /* elimination tree is a forest (etree.cpp:27-31) */
+    MDGPU_ERR_STATE = -6,     /* e.g. solve before factor */
+    MDGPU_ERR_NO_DEVICE = -7  /* no CUDA device: the numeric phase never runs on the CPU */
+};
+
+enum mdgpu_ordering { MDGPU_ORDER_NATURAL = 0, MDGPU_ORDER_AMD = 1 };
+enum mdgpu_tree { MDGPU_TREE_NODAL = 0, MDGPU_TREE_SUPER = 1, MDGPU_TREE_RELAXED = 2 };
+enum mdgpu_precision {
+    MDGPU_FP64 = 0, /* plain FP64 factor: the drop-in mode */
+    MDGPU_FP32 = 1  /* FP32 factor; Schur updates of large fronts on TF32 tensor cores */
+};
+
+/*
+ * Symbolic analysis.  Replaces the reference driver's symbolic sequence
+ * (mdgpu.cu:1745-1875): cs_transpose + cs_amd + cs_pinv + cs_symperm +
+ * make_sym, cs_etree, cs_post, cs_counts, GetETree, then GetSuperETree
+ * (tree = SUPER, flag -sn) or GetRelaxedETree (tree = RELAXED, flag -rn z),
+ * and the spL->p column pointers.  Bit-identical to the reference.  Also
+ * uploads the numeric plan (front row sets, extend-add maps, schedules) to
+ * the current CUDA device when one is present.
+ */
+MDGPU_API int mdgpu_analyze(int n, const int *Ap, const int *Ai, int ordering, int tree, int relax_zeros,
+                  mdgpu_handle *out);
+
+/*
+ * Analysis from an already permuted lower triangle and a given assembly tree,
+ * the inputs of the reference's Factor(cs *A, cs *spL, ETree **listaNodos,
+ * int cantNodos) (mdgpu.cu:1394): supernode s eliminates columns
+ * first_col[s] .. first_col[s]+ncols[s]-1, its children are
+ * child[child_ptr[s] .. child_ptr[s+1]-1], supernodes in postorder (root
+ * last), and count[] are the L column counts that define spL->p.
+ */
+MDGPU_API int mdgpu_analyze_tree(int n, const int *Ap, const int *Ai, int nsuper, const int *first_col,
+                       const int *ncols, const int *child_ptr, const int *child, const int *count,
+                       mdgpu_handle *out);
+
+MDGPU_API void mdgpu_destroy(mdgpu_handle h);
+
+/* Scalars: "n", "nsuper", "lnz", "nlevels", "nnz", "max_front", "flops"
+ * (the reference's own count, mdgpu.cu:1354-1359), "lstore_bytes",
+ * "ustore_bytes", "rows_total", "nchild", "large_fronts". */
+MDGPU_API int mdgpu_info(mdgpu_handle h, const char *key, long long *value);
+
+/* Copy a symbolic array out: "perm" (n, new->old; identity if natural),
+ * "parent", "post", "count0" (n; cs_etree / cs_post / cs_counts), "count"
+ * (n; counts defining L, after GetRelaxedETree's padding), "relax_perm",
+ * "sn_first", "sn_ncols" (nsuper), "child_ptr" (nsuper+1), "child",
+ * "Lp" (n+1, as long long), "rows_ptr" (nsuper+1), "rows" (front row sets),
+ * "relmap" (per front row: its position in the parent's front, -1 for pivot
+ * rows and the root), "level" (nsuper). */
+MDGPU_API int mdgpu_get_array(mdgpu_handle h, const char *name, void *dst);
+
+/*
+ * Numeric factorization on the GPU.  Replaces Factor (mdgpu.cu:1394-1608)
+ * with FactorAux_GPU_2 / FactorAux_CPU_3 (mdgpu.cu:903,1298) and ExtendAdd
+ * (mdgpu.cu:802).  Ax: the values of the caller's lower triangle in the
+ * caller's (original) ordering, host memory; _device: device memory.
+ * stream: a cudaStream_t or NULL (the handle's own stream).  Returns
+ * MDGPU_ERR_NOT_SPD if a pivot was not positive.
+ */
+MDGPU_API int mdgpu_factor(mdgpu_handle h, const double *Ax, int precision, void *stream);
+MDGPU_API int mdgpu_factor_device(mdgpu_handle h, const double *dAx, int precision, void *stream);
+MDGPU_API int mdgpu_not_spd_column(mdgpu_handle h); /* first failing column (permuted), -1 if none */
+
+/*
+ * x = A^-1 b with the last factor: the reference's cs_pvec + cs_lsolve +
+ * cs_ltsolve + cs_ipvec sequence (mdgpu.cu:1952-1961, cs.cpp:1086-1146) as
+ * supernodal GPU sweeps.  B, X: n x nrhs column-major (leading dims ldb,
+ * ldx), original ordering; host memory, or device memory for _device.
+ */
+MDGPU_API int mdgpu_solve(mdgpu_handle h, const double *B, int ldb, double *X, int ldx, int nrhs,
+                void *stream);
+MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, double *dX, int ldx, int nrhs,
+                       void *stream);
+
+/*
+ * Solve with FP64 iterative refinement on the GPU: r = b - A x with the
+ * caller's FP64 values (the reference's residual, mdgpu.cu:1963-1972), then
+ * x += A_factor^-1 r until the backward error ||r||inf / (||A||inf ||x||inf +
+ * ||b||inf) <= tol or maxit corrections.  berr[nrhs] (optional) receives the
+ * final backward errors, *iters (optional) the number of corrections.
+ */
+MDGPU_API int mdgpu_refine(mdgpu_handle h, const double *B, int ldb, double *X, int ldx, int nrhs,
+                 double tol, int maxit, double *berr, int *iters, void *stream);
+MDGPU_API int mdgpu_refine_device(mdgpu_handle h, const double *dB, int ldb, double *dX, int ldx, int nrhs,
+                        double tol, int maxit, double *berr, int *iters, void *stream);
+
+/*
+ * Copy L out as compressed columns, the spL contract of the reference
+ * (mdgpu.cu:1346-1352, 1859-1875): Lp[n+1] (long long), Li[lnz] row indices
+ * ascending with the diagonal first, Lx[lnz] values (FP64; an FP32 factor is
+ * widened).  Any of the three may be NULL.
+ */
+MDGPU_API int mdgpu_get_L(mdgpu_handle h, long long *Lp, int *Li, double *Lx);
+
+MDGPU_API const char *mdgpu_status_string(int status);
+MDGPU_API const char *mdgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,223 @@
+"""mdgpu_b200: B200-native multifrontal sparse Cholesky (Python front-end).
+
+A thin ctypes layer over the C ABI in ``include/mdgpu_b200.h`` (library
+``mdgpu_b200/libmdgpu_b200.so``).  The numeric phase runs only on the GPU:
+when the library or a CUDA device is missing the calls raise instead of
+falling back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdgpu_b200.so")
+
+FP64, FP32 = 0, 1
+ORDER_NATURAL, ORDER_AMD = 0, 1
+TREE_NODAL, TREE_SUPER, TREE_RELAXED = 0, 1, 2
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out of memory",
+          -4: "CUDA error", -5: "elimination tree is a forest", -6: "invalid call order",
+          -7: "no CUDA device"}
+
+# every entry point declared in include/mdgpu_b200.h
+EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
+           "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
+           "mdgpu_solve", "mdgpu_solve_device", "mdgpu_refine", "mdgpu_refine_device",
+           "mdgpu_get_L", "mdgpu_status_string", "mdgpu_last_error")
+
+
+class MdgpuError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("%s (%d)%s" % (STATUS.get(status, "error"), status,
+                                        (": " + msg) if msg else ""))
+
+
+class NotSPDError(MdgpuError):
+    def __init__(self, status, msg, column):
+        super().__init__(status, msg)
+        self.column = column
+
+
+_lib = None
+
+
+def lib():
+    """Load the C-ABI library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libmdgpu_b200.so not built: run `make -C mdgpu_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.c_void_p, C.c_void_p
+        L.mdgpu_analyze.argtypes = [C.c_int, ip, ip, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+        L.mdgpu_analyze_tree.argtypes = [C.c_int, ip, ip, C.c_int, ip, ip, ip, ip, ip,
+                                         C.POINTER(vp)]
+        L.mdgpu_destroy.argtypes = [vp]
+        L.mdgpu_destroy.restype = None
+        L.mdgpu_info.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
+        L.mdgpu_get_array.argtypes = [vp, C.c_char_p, vp]
+        L.mdgpu_factor.argtypes = [vp, dp, C.c_int, vp]
+        L.mdgpu_factor_device.argtypes = [vp, dp, C.c_int, vp]
+        L.mdgpu_not_spd_column.argtypes = [vp]
+        L.mdgpu_solve.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, vp]
+        L.mdgpu_solve_device.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, vp]
+        L.mdgpu_refine.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                   dp, vp, vp]
+        L.mdgpu_refine_device.argtypes = L.mdgpu_refine.argtypes
+        L.mdgpu_get_L.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_status_string.argtypes = [C.c_int]
+        L.mdgpu_status_string.restype = C.c_char_p
+        L.mdgpu_last_error.restype = C.c_char_p
+        for name in EXPORTS:
+            f = getattr(L, name)
+            if f.restype is C.c_int and name not in ("mdgpu_not_spd_column",):
+                pass
+        _lib = L
+    return _lib
+
+
+def _check(rc, h=None):
+    if rc == 0:
+        return
+    msg = lib().mdgpu_last_error().decode()
+    if rc == -2 and h is not None:
+        raise NotSPDError(rc, msg, lib().mdgpu_not_spd_column(h))
+    raise MdgpuError(rc, msg)
+
+
+def _ptr(a):
+    return a.ctypes.data
+
+
+def _tensor_ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Solver:
+    """One sparsity pattern: symbolic analysis at construction, then any
+    number of GPU factorizations and solves.
+
+    ``Ap, Ai`` describe the lower triangle (diagonal included) in compressed
+    columns with sorted rows, int32 -- the reference's ``cs`` layout.
+    """
+
+    def __init__(self, n, Ap, Ai, ordering=ORDER_AMD, tree=TREE_SUPER, relax_zeros=0):
+        L = lib()
+        self.n = int(n)
+        self.Ap = np.ascontiguousarray(Ap, dtype=np.int32)
+        self.Ai = np.ascontiguousarray(Ai, dtype=np.int32)
+        self._h = C.c_void_p()
+        _check(L.mdgpu_analyze(self.n, _ptr(self.Ap), _ptr(self.Ai), int(ordering), int(tree),
+                               int(relax_zeros), C.byref(self._h)))
+
+    @classmethod
+    def from_tree(cls, n, Ap, Ai, first_col, ncols, child_ptr, child, count):
+        self = cls.__new__(cls)
+        L = lib()
+        self.n = int(n)
+        self.Ap = np.ascontiguousarray(Ap, dtype=np.int32)
+        self.Ai = np.ascontiguousarray(Ai, dtype=np.int32)
+        arrs = [np.ascontiguousarray(a, dtype=np.int32)
+                for a in (first_col, ncols, child_ptr, child, count)]
+        self._keep = arrs
+        self._h = C.c_void_p()
+        _check(L.mdgpu_analyze_tree(self.n, _ptr(self.Ap), _ptr(self.Ai), len(arrs[0]),
+                                    *[_ptr(a) for a in arrs], C.byref(self._h)))
+        return self
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mdgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self, key):
+        v = C.c_longlong()
+        _check(lib().mdgpu_info(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def array(self, name):
+        n, ns = self.n, self.info("nsuper")
+        sizes = {"perm": n, "parent": n, "post": n, "count0": n, "count": n, "relax_perm": n,
+                 "sn_first": ns, "sn_ncols": ns, "child_ptr": ns + 1,
+                 "child": self.info("nchild"), "rows_ptr": ns + 1,
+                 "rows": self.info("rows_total"), "relmap": self.info("rows_total"),
+                 "level": ns}
+        if name == "Lp":
+            a = np.zeros(n + 1, np.int64)
+        else:
+            a = np.zeros(max(sizes[name], 1), np.int32)
+        _check(lib().mdgpu_get_array(self._h, name.encode(), _ptr(a)))
+        return a if name == "Lp" else a[: sizes[name]]
+
+    # ---- numeric -----------------------------------------------------
+    def factor(self, Ax, precision=FP64, stream=None):
+        """Ax: numpy float64 (host) or a CUDA torch tensor (device)."""
+        if hasattr(Ax, "data_ptr"):
+            _check(lib().mdgpu_factor_device(self._h, _tensor_ptr(Ax), int(precision), stream),
+                   self._h)
+        else:
+            Ax = np.ascontiguousarray(Ax, dtype=np.float64)
+            _check(lib().mdgpu_factor(self._h, _ptr(Ax), int(precision), stream), self._h)
+
+    def solve(self, B, stream=None):
+        """B: (n,) or (n, k) float64 numpy array, or CUDA torch tensors.
+        Device tensors must be column-major contiguous (use B.T.contiguous().T)."""
+        if hasattr(B, "data_ptr"):
+            import torch
+
+            nrhs = 1 if B.dim() == 1 else B.shape[1]
+            X = torch.empty_like(B)
+            ld = self.n if B.dim() == 1 else B.stride(1)
+            _check(lib().mdgpu_solve_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X), ld,
+                                            nrhs, stream))
+            return X
+        B = np.asarray(B, dtype=np.float64)
+        one = B.ndim == 1
+        Bf = np.asfortranarray(B.reshape(self.n, -1))
+        X = np.zeros_like(Bf, order="F")
+        _check(lib().mdgpu_solve(self._h, _ptr(Bf), self.n, _ptr(X), self.n, Bf.shape[1],
+                                 stream))
+        return X[:, 0] if one else X
+
+    def refine(self, B, tol=1e-14, maxit=10, stream=None):
+        """Solve with FP64 iterative refinement; returns (x, berr, iters)."""
+        B = np.asarray(B, dtype=np.float64)
+        one = B.ndim == 1
+        Bf = np.asfortranarray(B.reshape(self.n, -1))
+        X = np.zeros_like(Bf, order="F")
+        berr = np.zeros(Bf.shape[1])
+        it = C.c_int()
+        _check(lib().mdgpu_refine(self._h, _ptr(Bf), self.n, _ptr(X), self.n, Bf.shape[1],
+                                  float(tol), int(maxit), _ptr(berr), C.byref(it), stream))
+        return (X[:, 0] if one else X), berr, it.value
+
+    def refine_device(self, B, X, tol=1e-14, maxit=10, stream=None):
+        nrhs = 1 if B.dim() == 1 else B.shape[1]
+        ld = self.n if B.dim() == 1 else B.stride(1)
+        berr = np.zeros(nrhs)
+        it = C.c_int()
+        _check(lib().mdgpu_refine_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X), ld, nrhs,
+                                         float(tol), int(maxit), _ptr(berr), C.byref(it),
+                                         stream))
+        return berr, it.value
+
+    def get_L(self, values=True):
+        """L as (Lp int64, Li int32, Lx float64) -- the reference's spL."""
+        lnz = self.info("lnz")
+        Lp = np.zeros(self.n + 1, np.int64)
+        Li = np.zeros(max(lnz, 1), np.int32)
+        Lx = np.zeros(max(lnz, 1), np.float64) if values else None
+        _check(lib().mdgpu_get_L(self._h, _ptr(Lp), _ptr(Li),
+                                 _ptr(Lx) if values else None))
+        return Lp, Li[:lnz], (Lx[:lnz] if values else None)

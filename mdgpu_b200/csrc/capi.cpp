@@ -1,0 +1,635 @@
+// C ABI implementation (include/mdgpu_b200.h): symbolic on the host, plan
+// resident on the device, numeric factor / solve / refinement on the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ir.hpp"
+#include "kernels.hpp"
+#include "mdgpu_b200.h"
+#include "plan.hpp"
+#include "symbolic.hpp"
+
+using namespace mdgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
+};
+
+void ck(cudaError_t e, const char* where) {
+    if (e != cudaSuccess)
+        throw CudaError(e, (std::string(where) + ": " + cudaGetErrorString(e)).c_str());
+}
+
+template <typename T>
+T* dalloc(size_t count) {
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+T* upload(const std::vector<T>& v) {
+    T* d = dalloc<T>(v.size());
+    if (!v.empty()) ck(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return d;
+}
+
+int device_available() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0;
+}
+
+}  // namespace
+
+struct mdgpu_handle_s {
+    Symbolic sym;
+    Plan plan;
+    TileSchedule fsched;
+    SolveScheduleHost ssched;
+    DevPlan D;
+    std::vector<int> level;
+    SymCsr csr;
+    std::vector<int> h_csr_rowptr, h_csr_col, h_csr_src;
+    bool on_device = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> owned;  // device allocations of the plan
+    int* d_perm = nullptr;
+    int* d_status = nullptr;
+    unsigned long long* d_norms = nullptr;  // [0] = ||A||, then 3 per rhs
+    double* d_Ax = nullptr;
+    double* dL64 = nullptr;
+    double* dU64 = nullptr;
+    float* dL32 = nullptr;
+    float* dU32 = nullptr;
+    double *d_xp = nullptr, *d_fv = nullptr, *d_B = nullptr, *d_X = nullptr, *d_R = nullptr,
+           *d_D = nullptr;
+    int nrhs_cap = 0;
+    int factored = -1;  // precision of the current factor, -1 none
+    int not_spd = -1;
+
+    template <typename T>
+    T* keep(T* p) {
+        owned.push_back(p);
+        return p;
+    }
+    ~mdgpu_handle_s() {
+        if (!on_device) return;
+        cudaSetDevice(device);
+        for (void* p : owned) cudaFree(p);
+        for (void* p : {(void*)d_Ax, (void*)dL64, (void*)dU64, (void*)dL32, (void*)dU32,
+                        (void*)d_xp, (void*)d_fv, (void*)d_B, (void*)d_X, (void*)d_R, (void*)d_D})
+            if (p) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+constexpr int kLargeThreshold = 160;  // rows above which a front is tiled
+
+void build_csr(mdgpu_handle_s* h, int n, const int* Ap, const int* Ai) {
+    // full symmetric CSR of the caller's lower triangle, rows in original order
+    std::vector<int> cnt(n, 0);
+    for (int j = 0; j < n; ++j)
+        for (int p = Ap[j]; p < Ap[j + 1]; ++p) {
+            int i = Ai[p];
+            cnt[i]++;
+            if (i != j) cnt[j]++;
+        }
+    h->h_csr_rowptr.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) h->h_csr_rowptr[i + 1] = h->h_csr_rowptr[i] + cnt[i];
+    int64_t nnz = h->h_csr_rowptr[n];
+    h->h_csr_col.resize(nnz);
+    h->h_csr_src.resize(nnz);
+    std::vector<int> next(h->h_csr_rowptr.begin(), h->h_csr_rowptr.end() - 1);
+    for (int j = 0; j < n; ++j)
+        for (int p = Ap[j]; p < Ap[j + 1]; ++p) {
+            int i = Ai[p];
+            int q = next[i]++;
+            h->h_csr_col[q] = j;
+            h->h_csr_src[q] = p;
+            if (i != j) {
+                q = next[j]++;
+                h->h_csr_col[q] = i;
+                h->h_csr_src[q] = p;
+            }
+        }
+    h->csr.n = n;
+    h->csr.nnz = nnz;
+}
+
+void finish_plan(mdgpu_handle_s* h) {
+    build_plan(h->sym, h->sym.lower.nnz(), kLargeThreshold, h->plan);
+    build_factor_schedule(h->plan, kTile, kAssembleCols, h->fsched);
+    build_solve_schedule(h->plan, kTile, h->ssched);
+    h->level = front_levels(h->plan);
+}
+
+void upload_plan(mdgpu_handle_s* h) {
+    if (!device_available()) return;
+    ck(cudaGetDevice(&h->device), "cudaGetDevice");
+    h->on_device = true;
+    ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    const Plan& P = h->plan;
+    DevPlan& D = h->D;
+    D.n = P.n;
+    D.nsuper = P.nsuper;
+    D.nlevels = P.nlevels;
+    D.fronts = h->keep(upload(P.fronts));
+    D.child = h->keep(upload(P.child));
+    D.rows = h->keep(upload(P.rows));
+    D.relmap = h->keep(upload(P.relmap));
+    D.a_src = h->keep(upload(P.a_src));
+    D.a_pos = h->keep(upload(P.a_pos));
+    D.a_colptr = h->keep(upload(P.a_colptr));
+    D.a_colptr_off = h->keep(upload(P.a_colptr_off));
+    D.small_list = h->keep(upload(P.small_list));
+    D.large_list = h->keep(upload(P.large_list));
+    D.h_small_ptr = P.small_ptr;
+    D.h_large_ptr = P.large_ptr;
+    std::vector<int64_t> fvo(P.nsuper);
+    int64_t acc = 0;
+    for (int s = 0; s < P.nsuper; ++s) {
+        fvo[s] = acc;
+        acc += P.fronts[s].m;
+    }
+    D.fv_total = acc;
+    D.fv_off = h->keep(upload(fvo));
+    D.sched64.items = h->keep(upload(h->fsched.store.items));
+    D.sched64.before = h->keep(upload(h->fsched.store.ctas_before));
+    D.sched64.h_level_beg = h->fsched.level_beg;
+    D.sched64.h_trsm = h->fsched.trsm;
+    D.sched64.h_update = h->fsched.update;
+    D.h_assemble = h->fsched.assemble;
+    D.solve.items = h->keep(upload(h->ssched.store.items));
+    D.solve.before = h->keep(upload(h->ssched.store.ctas_before));
+    D.solve.fwd_beg = h->ssched.fwd_beg;
+    D.solve.bwd_beg = h->ssched.bwd_beg;
+    D.solve.fwd = h->ssched.fwd;
+    D.solve.bwd = h->ssched.bwd;
+    D.solve.gather = h->ssched.gather;
+    if (!P.perm.empty()) h->d_perm = h->keep(upload(P.perm));
+    h->d_status = h->keep(dalloc<int>(1));
+    h->d_Ax = dalloc<double>(std::max<int64_t>(P.nnz_user, 1));
+    h->csr.rowptr = h->keep(upload(h->h_csr_rowptr));
+    h->csr.col = h->keep(upload(h->h_csr_col));
+    h->csr.src = h->keep(upload(h->h_csr_src));
+}
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        return fail(MDGPU_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(MDGPU_ERR_OOM, "allocation failed");
+    } catch (const std::exception& e) {
+        return fail(MDGPU_ERR_INVALID, e.what());
+    }
+}
+
+cudaStream_t pick_stream(mdgpu_handle_s* h, void* s) {
+    return s ? static_cast<cudaStream_t>(s) : h->stream;
+}
+
+void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
+    const Plan& P = h->plan;
+    if (precision == MDGPU_FP64) {
+        if (!h->dL64) h->dL64 = dalloc<double>(P.lstore);
+        if (!h->dU64) h->dU64 = dalloc<double>(P.ustore);
+    } else {
+        if (!h->dL32) h->dL32 = dalloc<float>(P.lstore);
+        if (!h->dU32) h->dU32 = dalloc<float>(P.ustore);
+    }
+}
+
+void ensure_solve_storage(mdgpu_handle_s* h, int nrhs) {
+    if (nrhs <= h->nrhs_cap) return;
+    for (double** p : {&h->d_xp, &h->d_fv, &h->d_B, &h->d_X, &h->d_R, &h->d_D})
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    if (h->d_norms) {
+        cudaFree(h->d_norms);
+        h->d_norms = nullptr;
+    }
+    int64_t n = h->plan.n;
+    int chunk = std::min(nrhs, 64);
+    h->d_xp = dalloc<double>(n * nrhs);
+    h->d_fv = dalloc<double>(h->D.fv_total * chunk);
+    h->d_B = dalloc<double>(n * nrhs);
+    h->d_X = dalloc<double>(n * nrhs);
+    h->d_R = dalloc<double>(n * nrhs);
+    h->d_D = dalloc<double>(n * nrhs);
+    h->d_norms = dalloc<unsigned long long>(1 + 3 * nrhs);
+    h->nrhs_cap = nrhs;
+}
+
+int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
+    if (precision != MDGPU_FP64 && precision != MDGPU_FP32)
+        return fail(MDGPU_ERR_INVALID, "unknown precision");
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    ensure_factor_storage(h, precision);
+    if (dAx != h->d_Ax)
+        ck(cudaMemcpyAsync(h->d_Ax, dAx, h->plan.nnz_user * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st),
+           "copy values");
+    const int big = INT_MAX;
+    ck(cudaMemcpyAsync(h->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, st), "status");
+    if (precision == MDGPU_FP64)
+        factor_levels<double>(h->D, h->dL64, h->dU64, h->d_Ax, h->d_status, st);
+    else
+        factor_levels<float>(h->D, h->dL32, h->dU32, h->d_Ax, h->d_status, st);
+    ck(cudaGetLastError(), "factor launch");
+    int col = big;
+    ck(cudaMemcpyAsync(&col, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    ck(cudaStreamSynchronize(st), "factor");
+    h->factored = precision;
+    h->not_spd = (col == big) ? -1 : col;
+    if (h->not_spd >= 0) {
+        h->factored = -1;
+        return fail(MDGPU_ERR_NOT_SPD,
+                    "non-positive pivot at permuted column " + std::to_string(h->not_spd));
+    }
+    return MDGPU_OK;
+}
+
+// dB, dX device, original ordering; chunks of at most 64 right-hand sides
+void do_solve(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
+              cudaStream_t st) {
+    const int n = h->plan.n;
+    for (int q0 = 0; q0 < nrhs; q0 += 64) {
+        int nq = std::min(64, nrhs - q0);
+        permute_gather(h->d_perm, dB + (int64_t)q0 * ldb, h->d_xp, n, nq, ldb, st);
+        if (h->factored == MDGPU_FP64)
+            solve_levels<double, double>(h->D, h->dL64, h->d_xp, h->d_fv, nq, st);
+        else
+            solve_levels<float, double>(h->D, h->dL32, h->d_xp, h->d_fv, nq, st);
+        permute_scatter(h->d_perm, h->d_xp, dX + (int64_t)q0 * ldx, n, nq, ldx, st);
+    }
+    ck(cudaGetLastError(), "solve launch");
+}
+
+int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
+              double tol, int maxit, double* berr, int* iters, cudaStream_t st) {
+    const int n = h->plan.n;
+    ensure_solve_storage(h, nrhs);
+    launch_anorm(h->csr, h->d_Ax, h->d_norms, st);
+    do_solve(h, dB, ldb, dX, ldx, nrhs, st);
+    std::vector<unsigned long long> raw(1 + 3 * nrhs);
+    std::vector<double> be(nrhs, 0.0);
+    int it = 0;
+    for (;; ++it) {
+        launch_residual(h->csr, h->d_Ax, dX, ldx, dB, ldb, h->d_R, n, nrhs, st);
+        launch_absmax3(n, nrhs, h->d_R, n, dX, ldx, dB, ldb, h->d_norms + 1, st);
+        ck(cudaMemcpyAsync(raw.data(), h->d_norms, raw.size() * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st),
+           "norms");
+        ck(cudaStreamSynchronize(st), "refine");
+        double anorm;
+        std::memcpy(&anorm, &raw[0], sizeof(double));
+        bool done = true;
+        for (int q = 0; q < nrhs; ++q) {
+            double nr, nx, nb;
+            std::memcpy(&nr, &raw[1 + 3 * q], sizeof(double));
+            std::memcpy(&nx, &raw[2 + 3 * q], sizeof(double));
+            std::memcpy(&nb, &raw[3 + 3 * q], sizeof(double));
+            double den = anorm * nx + nb;
+            be[q] = den > 0 ? nr / den : 0.0;
+            if (!(be[q] <= tol)) done = false;
+        }
+        if (done || it >= maxit) break;
+        do_solve(h, h->d_R, n, h->d_D, n, nrhs, st);
+        for (int q = 0; q < nrhs; ++q)
+            launch_axpy(n, h->d_D + (int64_t)q * n, dX + (int64_t)q * ldx, st);
+    }
+    if (berr) std::copy(be.begin(), be.end(), berr);
+    if (iters) *iters = it;
+    return MDGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdgpu_analyze(int n, const int* Ap, const int* Ai, int ordering, int tree, int relax_zeros,
+                  mdgpu_handle* out) {
+    if (!out || n <= 0 || !Ap || !Ai) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (tree < 0 || tree > 2 || ordering < 0 || ordering > 1)
+        return fail(MDGPU_ERR_INVALID, "bad ordering or tree kind");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        for (int j = 0; j < n; ++j) {
+            if (Ap[j + 1] < Ap[j]) return fail(MDGPU_ERR_INVALID, "column pointers decrease");
+            for (int p = Ap[j]; p < Ap[j + 1]; ++p)
+                if (Ai[p] < j || Ai[p] >= n)
+                    return fail(MDGPU_ERR_INVALID, "entry outside the lower triangle");
+        }
+        auto* h = new mdgpu_handle_s();
+        int rc = analyze(n, Ap, Ai, nullptr, ordering == MDGPU_ORDER_AMD, (TreeKind)tree,
+                         relax_zeros, h->sym);
+        if (rc != 0) {
+            delete h;
+            return fail(MDGPU_ERR_NOT_TREE, "the elimination tree is a forest");
+        }
+        try {
+            finish_plan(h);
+            build_csr(h, n, Ap, Ai);
+            upload_plan(h);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_analyze_tree(int n, const int* Ap, const int* Ai, int nsuper, const int* first_col,
+                       const int* ncols, const int* child_ptr, const int* child, const int* count,
+                       mdgpu_handle* out) {
+    if (!out || n <= 0 || !Ap || !Ai || nsuper <= 0 || !first_col || !ncols || !child_ptr ||
+        !count)
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        auto* h = new mdgpu_handle_s();
+        Symbolic& S = h->sym;
+        S.n = n;
+        S.lower.nrows = S.lower.ncols = n;
+        S.lower.colptr.assign(Ap, Ap + n + 1);
+        S.lower.rowidx.assign(Ai, Ai + Ap[n]);
+        S.lower_src.resize(Ap[n]);
+        for (int p = 0; p < Ap[n]; ++p) S.lower_src[p] = p;
+        S.count.assign(count, count + n);
+        S.count0 = S.count;
+        S.tree.first_col.assign(first_col, first_col + nsuper);
+        S.tree.ncols.assign(ncols, ncols + nsuper);
+        S.tree.child_ptr.assign(child_ptr, child_ptr + nsuper + 1);
+        S.tree.child.assign(child, child + child_ptr[nsuper]);
+        S.Lp.assign(n + 1, 0);
+        for (int j = 0; j < n; ++j) S.Lp[j + 1] = S.Lp[j] + S.count[j];
+        try {
+            finish_plan(h);
+            build_csr(h, n, Ap, Ai);
+            upload_plan(h);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return MDGPU_OK;
+    });
+}
+
+void mdgpu_destroy(mdgpu_handle h) { delete h; }
+
+int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
+    if (!h || !key || !value) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    const Plan& P = h->plan;
+    std::string k(key);
+    if (k == "n") *value = P.n;
+    else if (k == "nsuper") *value = P.nsuper;
+    else if (k == "lnz") *value = P.lnz;
+    else if (k == "nlevels") *value = P.nlevels;
+    else if (k == "nnz") *value = P.nnz_user;
+    else if (k == "max_front") *value = P.max_m;
+    else if (k == "flops") *value = (long long)P.flops;
+    else if (k == "lstore_bytes") *value = P.lstore * 8;
+    else if (k == "ustore_bytes") *value = P.ustore * 8;
+    else if (k == "rows_total") *value = (long long)P.rows.size();
+    else if (k == "nchild") *value = (long long)P.child.size();
+    else if (k == "large_fronts") *value = (long long)P.large_list.size();
+    else if (k == "on_device") *value = h->on_device;
+    else return fail(MDGPU_ERR_INVALID, "unknown key " + k);
+    return MDGPU_OK;
+}
+
+int mdgpu_get_array(mdgpu_handle h, const char* name, void* dst) {
+    if (!h || !name || !dst) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    const Plan& P = h->plan;
+    const Symbolic& S = h->sym;
+    std::string k(name);
+    auto put = [&](const std::vector<int>& v) {
+        if (!v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int));
+        return MDGPU_OK;
+    };
+    if (k == "perm") {
+        if (P.perm.empty()) {
+            int* d = static_cast<int*>(dst);
+            for (int i = 0; i < P.n; ++i) d[i] = i;
+            return MDGPU_OK;
+        }
+        return put(P.perm);
+    }
+    if (k == "parent") return put(S.parent);
+    if (k == "post") return put(S.post);
+    if (k == "count0") return put(S.count0);
+    if (k == "count") return put(S.count);
+    if (k == "relax_perm") return put(S.relax_perm);
+    if (k == "sn_first") return put(S.tree.first_col);
+    if (k == "sn_ncols") return put(S.tree.ncols);
+    if (k == "child_ptr") return put(S.tree.child_ptr);
+    if (k == "child") return put(S.tree.child);
+    if (k == "level") return put(h->level);
+    if (k == "rows") return put(P.rows);
+    if (k == "relmap") return put(P.relmap);
+    if (k == "rows_ptr") {
+        int* d = static_cast<int*>(dst);
+        for (int s = 0; s < P.nsuper; ++s) d[s] = P.fronts[s].rows_off;
+        d[P.nsuper] = (int)P.rows.size();
+        return MDGPU_OK;
+    }
+    if (k == "Lp") {
+        std::memcpy(dst, P.Lp.data(), P.Lp.size() * sizeof(int64_t));
+        return MDGPU_OK;
+    }
+    return fail(MDGPU_ERR_INVALID, "unknown array " + k);
+}
+
+int mdgpu_factor_device(mdgpu_handle h, const double* dAx, int precision, void* stream) {
+    if (!h || !dAx) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    return guarded([&] { return do_factor(h, dAx, precision, pick_stream(h, stream)); });
+}
+
+int mdgpu_factor(mdgpu_handle h, const double* Ax, int precision, void* stream) {
+    if (!h || !Ax) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ck(cudaMemcpyAsync(h->d_Ax, Ax, h->plan.nnz_user * sizeof(double),
+                           cudaMemcpyHostToDevice, st),
+           "upload values");
+        return do_factor(h, h->d_Ax, precision, st);
+    });
+}
+
+int mdgpu_not_spd_column(mdgpu_handle h) { return h ? h->not_spd : -1; }
+
+int mdgpu_solve_device(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
+                       void* stream) {
+    if (!h || !dB || !dX || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n)
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ensure_solve_storage(h, nrhs);
+        do_solve(h, dB, ldb, dX, ldx, nrhs, st);
+        ck(cudaStreamSynchronize(st), "solve");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_solve(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, int nrhs,
+                void* stream) {
+    if (!h || !B || !X || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n)
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ensure_solve_storage(h, nrhs);
+        const int n = h->plan.n;
+        ck(cudaMemcpy2DAsync(h->d_B, n * sizeof(double), B, ldb * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st),
+           "upload rhs");
+        do_solve(h, h->d_B, n, h->d_X, n, nrhs, st);
+        ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
+           "download solution");
+        ck(cudaStreamSynchronize(st), "solve");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_refine_device(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
+                        double tol, int maxit, double* berr, int* iters, void* stream) {
+    if (!h || !dB || !dX || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n || maxit < 0)
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        return do_refine(h, dB, ldb, dX, ldx, nrhs, tol, maxit, berr, iters, st);
+    });
+}
+
+int mdgpu_refine(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, int nrhs,
+                 double tol, int maxit, double* berr, int* iters, void* stream) {
+    if (!h || !B || !X || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n || maxit < 0)
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ensure_solve_storage(h, nrhs);
+        const int n = h->plan.n;
+        ck(cudaMemcpy2DAsync(h->d_B, n * sizeof(double), B, ldb * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st),
+           "upload rhs");
+        int rc = do_refine(h, h->d_B, n, h->d_X, n, nrhs, tol, maxit, berr, iters, st);
+        ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
+           "download solution");
+        ck(cudaStreamSynchronize(st), "refine");
+        return rc;
+    });
+}
+
+int mdgpu_get_L(mdgpu_handle h, long long* Lp, int* Li, double* Lx) {
+    if (!h) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    const Plan& P = h->plan;
+    if (Lp) std::memcpy(Lp, P.Lp.data(), P.Lp.size() * sizeof(int64_t));
+    if (Li) {
+        for (int s = 0; s < P.nsuper; ++s) {
+            const FrontDesc& f = P.fronts[s];
+            const int* r = P.rows.data() + f.rows_off;
+            for (int j = 0; j < f.c; ++j) {
+                int64_t p0 = P.Lp[f.first_col + j];
+                for (int i = j; i < f.m; ++i) Li[p0 + i - j] = r[i];
+            }
+        }
+    }
+    if (!Lx) return MDGPU_OK;
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        std::vector<double> L64;
+        std::vector<float> L32;
+        if (h->factored == MDGPU_FP64) {
+            L64.resize(P.lstore);
+            ck(cudaMemcpy(L64.data(), h->dL64, P.lstore * sizeof(double), cudaMemcpyDeviceToHost),
+               "download L");
+        } else {
+            L32.resize(P.lstore);
+            ck(cudaMemcpy(L32.data(), h->dL32, P.lstore * sizeof(float), cudaMemcpyDeviceToHost),
+               "download L");
+        }
+        for (int s = 0; s < P.nsuper; ++s) {
+            const FrontDesc& f = P.fronts[s];
+            for (int j = 0; j < f.c; ++j) {
+                int64_t p0 = P.Lp[f.first_col + j];
+                int64_t base = f.loff + (int64_t)j * f.ldl;
+                for (int i = j; i < f.m; ++i)
+                    Lx[p0 + i - j] = h->factored == MDGPU_FP64 ? L64[base + i] : (double)L32[base + i];
+            }
+        }
+        return MDGPU_OK;
+    });
+}
+
+const char* mdgpu_status_string(int status) {
+    switch (status) {
+        case MDGPU_OK: return "ok";
+        case MDGPU_ERR_INVALID: return "invalid argument";
+        case MDGPU_ERR_NOT_SPD: return "matrix is not positive definite";
+        case MDGPU_ERR_OOM: return "out of memory";
+        case MDGPU_ERR_CUDA: return "CUDA error";
+        case MDGPU_ERR_NOT_TREE: return "elimination tree is a forest";
+        case MDGPU_ERR_STATE: return "invalid call order";
+        case MDGPU_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* mdgpu_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+// Numeric plan construction (see plan.hpp).
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+namespace mdgpu {
+
+const int Plan::small_limit[kSmallBuckets] = {16, 32, 64, 96, 128, 160};
+
+int small_front_limit(int scalar_bytes) { return scalar_bytes == 8 ? 160 : 160; }
+
+static int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+static int round8(int x) { return (x + 7) & ~7; }
+
+int front_tiles(int m, int c, int T) { return (c + T - 1) / T + (m - c + T - 1) / T; }
+
+void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& P) {
+    P = Plan();
+    const AssemblyTree& t = S.tree;
+    int n = S.n, ns = t.size();
+    P.n = n;
+    P.nsuper = ns;
+    P.nnz_user = nnz_user;
+    P.perm = S.perm;
+    if (!P.perm.empty()) {
+        P.iperm.resize(n);
+        for (int k = 0; k < n; ++k) P.iperm[P.perm[k]] = k;
+    }
+    P.Lp = S.Lp;
+    P.lnz = S.Lp[n];
+    for (int j = 0; j < n; ++j) P.flops += (double)S.count[j] * S.count[j] + 1.0;
+
+    std::vector<int> col2sn(n);
+    for (int s = 0; s < ns; ++s)
+        for (int j = 0; j < t.ncols[s]; ++j) col2sn[t.first_col[s] + j] = s;
+    std::vector<int> parent(ns, -1);
+    for (int s = 0; s < ns; ++s)
+        for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h) parent[t.child[h]] = s;
+
+    // Front row sets, bottom-up in visiting order: the pivot rows, then the
+    // sorted union of A's rows below the supernode and the children's update
+    // rows.  This is the row set the reference builds with MatrizGetFk_3 and
+    // VectorMerge (mdgpu.cu:180-291,1456,1489-1508,1566).
+    const SparseCol& A = S.lower;
+    std::vector<int64_t> rows_off(ns + 1, 0);
+    std::vector<std::vector<int>> rows(ns);
+    std::vector<int> scratch;
+    for (int s = 0; s < ns; ++s) {
+        int k = t.first_col[s], c = t.ncols[s];
+        scratch.clear();
+        for (int j = k; j < k + c; ++j)
+            for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
+                if (A.rowidx[p] >= k + c) scratch.push_back(A.rowidx[p]);
+        for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h) {
+            int ch = t.child[h];
+            const auto& rc = rows[ch];
+            for (size_t i = t.ncols[ch]; i < rc.size(); ++i) {
+                if (rc[i] < k) throw std::runtime_error("child update row below its parent");
+                if (rc[i] >= k + c) scratch.push_back(rc[i]);
+            }
+        }
+        std::sort(scratch.begin(), scratch.end());
+        scratch.erase(std::unique(scratch.begin(), scratch.end()), scratch.end());
+        auto& r = rows[s];
+        r.resize(c + scratch.size());
+        for (int i = 0; i < c; ++i) r[i] = k + i;
+        std::copy(scratch.begin(), scratch.end(), r.begin() + c);
+        int m = (int)r.size();
+        if (m != S.count[k])
+            throw std::runtime_error("front " + std::to_string(s) + " has " + std::to_string(m) +
+                                     " rows but column count " + std::to_string(S.count[k]));
+        rows_off[s + 1] = rows_off[s] + m;
+    }
+    if (rows_off[ns] > INT32_MAX) throw std::runtime_error("row arrays exceed 2^31 entries");
+    P.rows.resize(rows_off[ns]);
+    P.relmap.assign(rows_off[ns], -1);
+    for (int s = 0; s < ns; ++s)
+        std::copy(rows[s].begin(), rows[s].end(), P.rows.begin() + rows_off[s]);
+    // relative maps: position of each update row of s inside its parent's rows
+    for (int s = 0; s < ns; ++s) {
+        int p = parent[s];
+        if (p < 0) continue;
+        const auto& rs = rows[s];
+        const auto& rp = rows[p];
+        size_t q = 0;
+        for (size_t i = t.ncols[s]; i < rs.size(); ++i) {
+            while (q < rp.size() && rp[q] < rs[i]) ++q;
+            if (q == rp.size() || rp[q] != rs[i]) throw std::runtime_error("row not in parent");
+            P.relmap[rows_off[s] + i] = (int)q;
+        }
+    }
+
+    // storage offsets and descriptors
+    P.fronts.resize(ns);
+    int64_t lo = 0, uo = 0;
+    for (int s = 0; s < ns; ++s) {
+        FrontDesc& f = P.fronts[s];
+        f.m = (int)rows[s].size();
+        f.c = t.ncols[s];
+        f.ldl = round8(f.m);
+        int u = f.m - f.c;
+        f.ldu = round8(u);
+        f.loff = lo;
+        lo = align_up(lo + (int64_t)f.ldl * f.c, 32);
+        if (parent[s] >= 0 && u > 0) {
+            f.uoff = uo;
+            uo = align_up(uo + (int64_t)f.ldu * u, 32);
+        } else {
+            f.uoff = -1;
+        }
+        f.rows_off = (int)rows_off[s];
+        f.first_col = t.first_col[s];
+        f.child_beg = t.child_ptr[s];
+        f.child_end = t.child_ptr[s + 1];
+        f.a_beg = A.colptr[f.first_col];
+        f.a_end = A.colptr[f.first_col + f.c];
+        f.parent = parent[s];
+        f.pad_ = 0;
+        P.max_m = std::max(P.max_m, f.m);
+        P.max_u = std::max(P.max_u, u);
+    }
+    P.lstore = std::max<int64_t>(lo, 32);
+    P.ustore = std::max<int64_t>(uo, 32);
+    P.child = t.child;
+
+    // A entries: the lower triangle's entries of the supernode's columns are
+    // contiguous (columns are consecutive).  A repeated (row, col) keeps the
+    // last occurrence, as the reference's front assembly overwrites
+    // (mdgpu.cu:274-282).
+    int nnz = A.nnz();
+    P.a_src.resize(nnz);
+    P.a_pos.resize(nnz);
+    std::vector<int> last_at;  // per local position of the current front
+    for (int s = 0; s < ns; ++s) {
+        const FrontDesc& f = P.fronts[s];
+        const int* r = P.rows.data() + f.rows_off;
+        for (int jj = 0; jj < f.c; ++jj) {
+            int j = f.first_col + jj;
+            for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p) {
+                int row = A.rowidx[p];
+                int pos = (int)(std::lower_bound(r, r + f.m, row) - r);
+                if (pos >= f.m || r[pos] != row) throw std::runtime_error("A entry outside front");
+                if (f.m >= 65536) throw std::runtime_error("front too large for packed A map");
+                P.a_src[p] = S.lower_src[p];
+                P.a_pos[p] = pos | (jj << 16);
+            }
+        }
+        // duplicates: keep the last in storage order
+        bool dup = false;
+        for (int jj = 0; jj < f.c && !dup; ++jj) {
+            int j = f.first_col + jj;
+            for (int p = A.colptr[j] + 1; p < A.colptr[j + 1]; ++p)
+                if (A.rowidx[p] <= A.rowidx[p - 1]) dup = true;
+        }
+        if (dup) {
+            for (int jj = 0; jj < f.c; ++jj) {
+                int j = f.first_col + jj;
+                for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
+                    for (int q = p + 1; q < A.colptr[j + 1]; ++q)
+                        if (A.rowidx[q] == A.rowidx[p]) {
+                            P.a_src[p] = -1;
+                            break;
+                        }
+            }
+        }
+    }
+
+    // levels
+    std::vector<int> level(ns, 0);
+    for (int s = 0; s < ns; ++s)
+        for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h)
+            level[s] = std::max(level[s], level[t.child[h]] + 1);
+    P.nlevels = ns ? *std::max_element(level.begin(), level.end()) + 1 : 0;
+    int L = P.nlevels;
+    std::vector<std::vector<int>> small(L * kSmallBuckets), large(L);
+    for (int s = 0; s < ns; ++s) {
+        int m = P.fronts[s].m;
+        if (m > large_threshold) {
+            large[level[s]].push_back(s);
+            continue;
+        }
+        int b = 0;
+        while (b < kSmallBuckets - 1 && m > Plan::small_limit[b]) ++b;
+        small[level[s] * kSmallBuckets + b].push_back(s);
+    }
+    P.small_ptr.assign(L * kSmallBuckets + 1, 0);
+    for (int i = 0; i < L * kSmallBuckets; ++i) {
+        P.small_ptr[i + 1] = P.small_ptr[i] + (int)small[i].size();
+        P.small_list.insert(P.small_list.end(), small[i].begin(), small[i].end());
+    }
+    P.large_ptr.assign(L + 1, 0);
+    P.a_colptr_off.assign(ns, -1);
+    for (int l = 0; l < L; ++l) {
+        P.large_ptr[l + 1] = P.large_ptr[l] + (int)large[l].size();
+        P.large_list.insert(P.large_list.end(), large[l].begin(), large[l].end());
+        for (int s : large[l]) {
+            const FrontDesc& f = P.fronts[s];
+            P.a_colptr_off[s] = (int)P.a_colptr.size();
+            for (int jj = 0; jj <= f.c; ++jj)
+                P.a_colptr.push_back(A.colptr[f.first_col + jj] - f.a_beg);
+        }
+    }
+    if (P.a_colptr.empty()) P.a_colptr.push_back(0);
+}
+
+WorkList ListStore::add(const std::vector<std::pair<int, int>>& it, int step) {
+    WorkList w;
+    w.off = (int64_t)items.size();
+    w.nitems = (int)it.size();
+    w.step = step;
+    int acc = 0;
+    for (auto& [s, cnt] : it) {
+        items.push_back(s);
+        ctas_before.push_back(acc);
+        acc += cnt;
+    }
+    items.push_back(-1);
+    ctas_before.push_back(acc);
+    w.nctas = acc;
+    return w;
+}
+
+void build_factor_schedule(const Plan& P, int T, int assemble_cols, TileSchedule& S) {
+    S = TileSchedule();
+    S.T = T;
+    S.level_beg.assign(P.nlevels + 1, 0);
+    for (int l = 0; l < P.nlevels; ++l) {
+        S.level_beg[l] = (int)S.trsm.size();
+        std::vector<std::pair<int, int>> as;
+        int maxsteps = 0;
+        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+            const FrontDesc& f = P.fronts[P.large_list[q]];
+            maxsteps = std::max(maxsteps, (f.c + T - 1) / T);
+            as.push_back({P.large_list[q], (f.m + assemble_cols - 1) / assemble_cols});
+        }
+        S.assemble.push_back(S.store.add(as, 0));
+        for (int k = 0; k < maxsteps; ++k) {
+            std::vector<std::pair<int, int>> tr, up;
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                int s = P.large_list[q];
+                const FrontDesc& f = P.fronts[s];
+                int nt1 = (f.c + T - 1) / T;
+                if (k >= nt1) continue;
+                int rem = front_tiles(f.m, f.c, T) - k - 1;
+                if (rem > 0) {
+                    tr.push_back({s, rem});
+                    up.push_back({s, rem * (rem + 1) / 2});
+                }
+            }
+            S.trsm.push_back(S.store.add(tr, k));
+            S.update.push_back(S.store.add(up, k));
+        }
+    }
+    S.level_beg[P.nlevels] = (int)S.trsm.size();
+}
+
+void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
+    S = SolveScheduleHost();
+    S.T = T;
+    S.fwd_beg.assign(P.nlevels + 1, 0);
+    S.bwd_beg.assign(P.nlevels + 1, 0);
+    for (int l = 0; l < P.nlevels; ++l) {
+        int maxsteps = 0;
+        std::vector<std::pair<int, int>> ga;
+        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+            const FrontDesc& f = P.fronts[P.large_list[q]];
+            int nt1 = (f.c + T - 1) / T;
+            maxsteps = std::max(maxsteps, nt1);
+            ga.push_back({P.large_list[q], nt1});
+        }
+        S.gather.push_back(S.store.add(ga, 0));
+        S.fwd_beg[l] = (int)S.fwd.size();
+        for (int k = 0; k < maxsteps; ++k) {
+            std::vector<std::pair<int, int>> it;
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                const FrontDesc& f = P.fronts[P.large_list[q]];
+                if (k < (f.c + T - 1) / T) it.push_back({P.large_list[q], front_tiles(f.m, f.c, T) - k});
+            }
+            S.fwd.push_back(S.store.add(it, k));
+        }
+        S.bwd_beg[l] = (int)S.bwd.size();
+        for (int k = maxsteps - 1; k >= 0; --k) {
+            std::vector<std::pair<int, int>> it;
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                const FrontDesc& f = P.fronts[P.large_list[q]];
+                if (k < (f.c + T - 1) / T) it.push_back({P.large_list[q], k + 1});
+            }
+            S.bwd.push_back(S.store.add(it, k));
+        }
+    }
+    S.fwd_beg[P.nlevels] = (int)S.fwd.size();
+    S.bwd_beg[P.nlevels] = (int)S.bwd.size();
+}
+
+std::vector<int> front_levels(const Plan& P) {
+    std::vector<int> level(P.nsuper, 0);
+    for (int s = 0; s < P.nsuper; ++s)
+        for (int h = P.fronts[s].child_beg; h < P.fronts[s].child_end; ++h)
+            level[s] = std::max(level[s], level[P.child[h]] + 1);
+    return level;
+}
+
+}  // namespace mdgpu

@@ -1,0 +1,122 @@
+// Numeric plan: everything the GPU factor and solve need, computed once per
+// sparsity pattern on the host and uploaded once.
+//
+// Layout in HBM (element offsets, all 256-byte aligned):
+//   L store   one column-major m_s x c_s panel per supernode s, leading
+//             dimension ldl_s = m_s rounded up to 8.  The panel holds the
+//             supernode's columns of L (rows = the front's row set); it is the
+//             factor's final storage and the input of the solves.
+//   U store   one column-major u_s x u_s update matrix per non-root supernode
+//             (u_s = m_s - c_s, leading dimension ldu_s = u_s rounded up to 8),
+//             lower triangle only; written when s is factored, read when its
+//             parent is assembled.
+// Front s is the m_s x m_s matrix [L panel | U]; its rows are the sorted
+// global (permuted) column indices rows_s, the first c_s of which are
+// first_col_s .. first_col_s + c_s - 1.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.hpp"
+
+namespace mdgpu {
+
+// Per-supernode record mirrored on the device.
+struct FrontDesc {
+    int64_t loff;    // L store offset of the panel
+    int64_t uoff;    // U store offset of the update matrix (-1 for the root)
+    int m, c;        // front rows, pivot columns
+    int ldl, ldu;    // leading dimensions
+    int rows_off;    // offset of rows_s / relmap_s in the row arrays
+    int first_col;   // global (permuted) index of the first pivot column
+    int child_beg, child_end;  // range in the child list
+    int a_beg, a_end;          // range in the A-entry lists
+    int parent;                // parent supernode (-1 for the root)
+    int pad_;
+};
+
+// A tiled work list for one (level, step) launch of a multi-CTA kernel over
+// the large fronts: CTA b belongs to item[k] where ctas_before[k] <= b <
+// ctas_before[k+1].
+struct WorkList {
+    int64_t off;   // offset into the shared work-list arrays
+    int nitems;
+    int nctas;
+    int step;
+};
+
+constexpr int kSmallBuckets = 6;
+
+struct Plan {
+    int n = 0;
+    int nsuper = 0;
+    int64_t nnz_user = 0;       // entries of the caller's lower triangle
+    std::vector<int> perm;      // new -> old (empty: natural)
+    std::vector<int> iperm;     // old -> new
+    std::vector<FrontDesc> fronts;
+    std::vector<int> child;     // children lists
+    std::vector<int> rows;      // front row sets, concatenated
+    std::vector<int> relmap;    // per row r >= c_s of front s: position in the parent's front
+    std::vector<int> a_src;     // per A entry: index in the caller's value array
+    std::vector<int> a_pos;     // per A entry: local (row | col << 16) inside the front
+    std::vector<int> a_colptr;  // per large front: c+1 offsets into its A entries
+    std::vector<int> a_colptr_off;  // per supernode: offset into a_colptr (-1 if small)
+    std::vector<int64_t> Lp;    // CSC column pointers of L (reference spL->p)
+    int64_t lstore = 0, ustore = 0;  // element counts
+    int64_t lnz = 0;
+    double flops = 0;           // sum over columns of count^2 (the reference's count)
+    int max_m = 0, max_u = 0;
+
+    // level schedule: supernodes grouped by tree height (leaves = level 0)
+    int nlevels = 0;
+    // small fronts of each level, bucketed by m (bucket limits small_limit[])
+    std::vector<int> small_ptr;     // nlevels * kSmallBuckets + 1
+    std::vector<int> small_list;
+    // large fronts of each level
+    std::vector<int> large_ptr;     // nlevels + 1
+    std::vector<int> large_list;
+
+    static const int small_limit[kSmallBuckets];
+};
+
+// Largest m handled by the fused one-CTA-per-front kernel for a scalar size.
+int small_front_limit(int scalar_bytes);
+
+// Build the plan from a completed symbolic analysis.  `large_threshold` is
+// the row count above which a front takes the tiled multi-CTA path.
+void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& P);
+
+// Work-list storage: every list is a run of (front id, CTAs before it)
+// pairs closed by a sentinel carrying the list's CTA total.
+struct ListStore {
+    std::vector<int> items;
+    std::vector<int> ctas_before;
+    WorkList add(const std::vector<std::pair<int, int>>& fronts_ctas, int step);
+};
+
+// Work lists of the tiled factor kernels, for tile size T.
+struct TileSchedule {
+    int T = 64;
+    ListStore store;
+    std::vector<int> level_beg;          // per level: range of (trsm, update) pairs
+    std::vector<WorkList> trsm, update;  // one pair per (level, step)
+    std::vector<WorkList> assemble;      // per level: CTA per (front, column block)
+};
+
+// Work lists of the tiled solve kernels.
+struct SolveScheduleHost {
+    int T = 64;
+    ListStore store;
+    std::vector<int> fwd_beg, bwd_beg;   // per level: range in fwd / bwd
+    std::vector<WorkList> fwd, bwd;      // one per (level, step)
+    std::vector<WorkList> gather;        // per level
+};
+
+int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling
+void build_factor_schedule(const Plan& P, int T, int assemble_cols, TileSchedule& S);
+void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S);
+// per supernode: tree level (leaves 0)
+std::vector<int> front_levels(const Plan& P);
+
+}  // namespace mdgpu
