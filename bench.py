@@ -1,0 +1,367 @@
+"""Benchmark: numeric factor + refined solve of the 64^3 variable-coefficient
+3D Laplacian on B200.
+
+One step = the hot path over one system: numeric FP32 factorization (Schur
+updates of large fronts on the tensor cores) + solve of one right-hand side
+with FP64 iterative refinement to backward error <= 1e-14.  The plain FP64
+factor + solve of the same system is timed beside it (``fp64`` block).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--side 64] [--impl reference]
+
+value   = reference flop count (sum over L columns of count^2, the count the
+          reference prints, mdgpu.cu:1354-1359) / device time per step, inputs
+          resident in HBM; GFLOP/s, whole job (N replicas for --gpus N).
+e2e     = the same metric through the public C ABI with host buffers
+          (mdgpu_factor + mdgpu_refine: values and right-hand side copied in,
+          solution copied out, every step).
+Multi-GPU: a single system does not shard -- N independent replicas, one per
+GPU (weak scaling), barrier + max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "factor+solve time & GFLOP/s, FP32+IR vs FP64 on B200 at backward error <=1e-14"
+UNIT = "GFLOP/s"
+REF_SIDE = 28  # CPU sample of the reference arm (the full 64^3 takes ~12 min on one core)
+CPU_BASELINE_SIDE = 32
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--side", type=int, default=64)
+    ap.add_argument("--impl", default="mdgpu_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(side):
+    from mdgpu_b200 import matgen as mg
+
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(side, seed=0, sigma=1.0, shift=1e-3)
+    b = mg.rhs_uniform(n, seed=0)
+    return n, Ap, Ai, Ax, b
+
+
+def config(side, extra=None):
+    c = {"workload": "3D 7-point Laplacian %d^3 (n=%d), lognormal(0,1) edge conductances, "
+                     "shift 1e-3, AMD + supernodes (-amd -sn), 1 RHS U(-1,1)" % (side, side ** 3),
+         "matrix": "laplacian_3d_varcoef(side=%d, seed=0)" % side,
+         "factor": "FP32 (TF32 tensor-core Schur on large fronts) + FP64 iterative refinement",
+         "tolerance": 1e-14,
+         "l2": "flushed between steps (256 MiB write); working set (L + update matrices) >> L2"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref, compiled from the reference sources)
+# ---------------------------------------------------------------------------
+
+def reference_cpu_sample(side, timeout=600):
+    """Run the reference's own CPU Factor + cs_lsolve/cs_ltsolve on one core."""
+    from mdgpu_b200 import matgen as mg
+    from oracle import oracle as O
+
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(side, seed=0)
+    b = mg.rhs_uniform(n, seed=0)
+    with tempfile.TemporaryDirectory() as d:
+        mf = os.path.join(d, "A.txt")
+        bf = os.path.join(d, "b.f64")
+        mg.write_triplets(mf, n, Ap, Ai, Ax)
+        b.tofile(bf)
+        if os.path.exists(O.REF_HARNESS):
+            cmd = ["taskset", "-c", "0", O.REF_HARNESS, "-amd", "-sn", "-bfile", bf, mf,
+                   os.path.join(d, "out")]
+            os.makedirs(os.path.join(d, "out"))
+            try:
+                subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
+            except FileNotFoundError:
+                subprocess.run(cmd[3:], check=True, capture_output=True, timeout=timeout)
+            meta = O.load_dir(os.path.join(d, "out"))["meta"]
+            t = meta["t_factor"] + meta["t_solve"]
+            return {"value": meta["flops"] / t / 1e9, "unit": UNIT, "cores": 1,
+                    "kind": "reference", "seconds": t, "resid": meta["resid_rel"],
+                    "sample": "reference Factor + cs_lsolve + cs_ltsolve (oracle/_ref, FP64, "
+                              "-amd -sn, 1 core) on the %d^3 grid of the same generator "
+                              "(n=%d, %.3g flop)" % (side, n, meta["flops"])}
+        # restated port (same arithmetic, bit-identical results)
+        P = O.Plan(n, Ap, Ai, Ax, amd=True, mode="sn")
+        t0 = time.perf_counter()
+        F = P.factor()
+        P.solve(F["Li"], F["Lx"], b)
+        t = time.perf_counter() - t0
+        return {"value": F["flops"] / t / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+                "seconds": t,
+                "sample": "oracle port of the reference CPU path on the %d^3 grid" % side}
+
+
+def cpu_info():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        reference_cpu_sample(12)
+    vals, secs = [], []
+    base = None
+    for _ in range(args.steps):
+        base = reference_cpu_sample(REF_SIDE)
+        vals.append(base["value"])
+        secs.append(base["seconds"])
+    v = statistics.median(vals)
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(REF_SIDE, {"cpu": cpu_info(), "nproc": os.cpu_count(),
+                                        "note": "single-threaded reference (no threading in "
+                                                "its CPU path); 64^3 would take ~12 min/step"}),
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                                          "--query-gpu=" + q, "--format=csv,noheader,nounits"],
+                                         capture_output=True, text=True, timeout=5).stdout
+                    self.rows.append([x.strip() for x in out.strip().split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=loop, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if len(r) >= 6 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 6 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 6:
+                for k, nm in enumerate(names):
+                    if r[2 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def run_gpu_arm(args):
+    import torch
+
+    import mdgpu_b200 as M
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    side = args.side
+    n, Ap, Ai, Ax, b = workload(side)
+    t0 = time.perf_counter()
+    S = M.Solver(n, Ap, Ai)
+    t_analyze = time.perf_counter() - t0
+    flops = float(S.info("flops"))
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    dAx = torch.from_numpy(Ax).cuda()
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty_like(db)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step_fp32():
+        S.factor(dAx, M.FP32, stream=sptr)
+        return S.refine_device(db, dx, tol=1e-14, maxit=30, stream=sptr)
+
+    def step_fp64():
+        S.factor(dAx, M.FP64, stream=sptr)
+        return S.refine_device(db, dx, tol=1e-14, maxit=0, stream=sptr)
+
+    def timed(fn, steps, warmup, profile=False):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        times, extra = [], None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            extra = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+        return times, extra
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    t32, (berr32, it32) = timed(step_fp32, args.steps, args.warmup)
+    clocks = sampler.stop()
+    t64, (berr64, _) = timed(step_fp64, max(1, min(args.steps, 3)), 1)
+    ms32 = allmax(statistics.mean(t32))
+    ms64 = allmax(statistics.mean(t64))
+
+    # kernel-level evidence for the roofline: the dominant kernel class, timed
+    # with CUDA events around each of its launches during one extra step
+    prof = S.profile_step(lambda: step_fp32())
+
+    # end to end through the public API with host buffers
+    Axh = np.ascontiguousarray(Ax)
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.factor(Axh, M.FP32)
+        x, be, _ = S.refine(b, tol=1e-14, maxit=30)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_ms = allmax(1e3 * statistics.mean(e2e_t))
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks, peak_src = measured_peaks()
+    value = world * flops / (ms32 * 1e-3) / 1e9
+    dom = prof["dominant"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor (tf32 tensor-core Schur) + f64 refinement",
+        "data": "synthetic",
+        "config": config(side, {"n": n, "nnz_lower": int(Ap[-1]), "nsuper": S.info("nsuper"),
+                                "lnz": S.info("lnz"), "flops_per_step": flops,
+                                "parallelism": "replicas x%d (a single system does not shard)"
+                                               % world,
+                                "analyze_s": t_analyze}),
+        "backward_error": float(berr32[0]), "ir_iterations": int(it32),
+        "fp64": {"ms_per_step": ms64, "value": world * flops / (ms64 * 1e-3) / 1e9,
+                 "backward_error": float(berr64[0]),
+                 "speedup_fp32_ir_over_fp64": ms64 / ms32},
+        "e2e": {"value": world * flops / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+                "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(Ax.nbytes + b.nbytes),
+                "d2h_bytes_per_step": int(b.nbytes)},
+        "gpu_launches": prof["launches_per_step"],
+        "clocks": clocks,
+        "roofline": None,
+        "kernels": prof["classes"],
+    }
+    if dom is not None:
+        c = prof["classes"][dom]
+        if c["bound"] == "tensor":
+            peak = peaks["bf16_tflops"] / 2.0  # TF32 dense rate is half the bf16 rate
+            achieved = c["flops"] / c["launches"] / (c["ms"] / c["launches"] * 1e-3) / 1e12
+            unit = "TFLOP/s"
+            note = "TF32 peak = measured dense bf16 / 2 (%s)" % peak_src
+        else:
+            peak = peaks["hbm_gbs"]
+            achieved = c["bytes"] / c["launches"] / (c["ms"] / c["launches"] * 1e-3) / 1e9
+            unit = "GB/s"
+            note = "%s HBM copy bandwidth" % peak_src
+        line["roofline"] = {"kernel": dom, "bound": c["bound"], "achieved": achieved,
+                            "peak": peak, "unit": unit, "frac": achieved / peak,
+                            "traffic": c.get("traffic"), "peak_source": note,
+                            "launches": c["launches"], "ms_total": c["ms"]}
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = reference_cpu_sample(CPU_BASELINE_SIDE)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

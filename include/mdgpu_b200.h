@@ -129,6 +129,21 @@ MDGPU_API int mdgpu_refine_device(mdgpu_handle h, const double *dB, int ldb, dou
  */
 MDGPU_API int mdgpu_get_L(mdgpu_handle h, long long *Lp, int *Li, double *Lx);
 
+/*
+ * Diagnostics (no counterpart in the reference, whose only instrumentation is
+ * its tic/toc phase timers, mdgpu.cu:31-57,1901-1930).  mdgpu_profile(h, 1)
+ * brackets every kernel launch of the numeric phase with CUDA events, grouped
+ * by kernel class; mdgpu_profile(h, 0) (or a second enable) stops recording
+ * and folds the recorded events into per-class totals read back with
+ * mdgpu_profile_read: device milliseconds, launches, and the algorithmic flops
+ * / bytes of those launches.  Classes: 0 small-front factor, 1 large-front
+ * assembly, 2 first diagonal tile, 3 panel TRSM, 4 Schur tile update, 5 small-
+ * front solve sweeps, 6 large-front solve steps, 7 other.
+ */
+MDGPU_API int mdgpu_profile(mdgpu_handle h, int enable);
+MDGPU_API int mdgpu_profile_read(mdgpu_handle h, int cls, double *ms, long long *launches,
+                                 double *flops, double *bytes);
+
 MDGPU_API const char *mdgpu_status_string(int status);
 MDGPU_API const char *mdgpu_last_error(void);
 

@@ -27,7 +27,16 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
 EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
            "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_refine", "mdgpu_refine_device",
-           "mdgpu_get_L", "mdgpu_status_string", "mdgpu_last_error")
+           "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
+           "mdgpu_last_error")
+
+KERNEL_CLASSES = ("small_front", "assemble", "potrf", "trsm", "schur_update", "solve_small",
+                  "solve_large", "other")
+# the bound that limits each class (tensor/FP pipes for the dense updates,
+# HBM for the assembly-dominated small fronts)
+KERNEL_BOUND = {"small_front": "hbm", "assemble": "hbm", "potrf": "latency", "trsm": "latency",
+                "schur_update": "tensor", "solve_small": "hbm", "solve_large": "hbm",
+                "other": "hbm"}
 
 
 class MdgpuError(RuntimeError):
@@ -70,6 +79,8 @@ def lib():
                                    dp, vp, vp]
         L.mdgpu_refine_device.argtypes = L.mdgpu_refine.argtypes
         L.mdgpu_get_L.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_profile.argtypes = [vp, C.c_int]
+        L.mdgpu_profile_read.argtypes = [vp, C.c_int, vp, vp, vp, vp]
         L.mdgpu_status_string.argtypes = [C.c_int]
         L.mdgpu_status_string.restype = C.c_char_p
         L.mdgpu_last_error.restype = C.c_char_p
@@ -211,6 +222,25 @@ class Solver:
                                          float(tol), int(maxit), _ptr(berr), C.byref(it),
                                          stream))
         return berr, it.value
+
+    def profile_step(self, fn):
+        """Run fn() once with per-launch event timing on; return per-class
+        totals and the dominant class (most device time)."""
+        _check(lib().mdgpu_profile(self._h, 1))
+        fn()
+        _check(lib().mdgpu_profile(self._h, 0))
+        classes = {}
+        total_launches = 0
+        for k, name in enumerate(KERNEL_CLASSES):
+            ms, n, fl, by = C.c_double(), C.c_longlong(), C.c_double(), C.c_double()
+            _check(lib().mdgpu_profile_read(self._h, k, C.byref(ms), C.byref(n), C.byref(fl),
+                                            C.byref(by)))
+            if n.value:
+                classes[name] = {"ms": ms.value, "launches": n.value, "flops": fl.value,
+                                 "bytes": by.value, "bound": KERNEL_BOUND[name]}
+                total_launches += n.value
+        dom = max(classes, key=lambda k: classes[k]["ms"]) if classes else None
+        return {"classes": classes, "dominant": dom, "launches_per_step": total_launches}
 
     def get_L(self, values=True):
         """L as (Lp int64, Li int32, Lx float64) -- the reference's spL."""

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <map>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -67,6 +68,8 @@ struct mdgpu_handle_s {
     Plan plan;
     TileSchedule fsched;
     SolveScheduleHost ssched;
+    PanelSchedule pschedh;
+    bool use_tensor_cores = true;
     DevPlan D;
     std::vector<int> level;
     SymCsr csr;
@@ -83,22 +86,40 @@ struct mdgpu_handle_s {
     double* dU64 = nullptr;
     float* dL32 = nullptr;
     float* dU32 = nullptr;
+    double* dD64 = nullptr;  // inverted diagonal tiles of the large fronts
+    float* dD32 = nullptr;
     double *d_xp = nullptr, *d_fv = nullptr, *d_B = nullptr, *d_X = nullptr, *d_R = nullptr,
            *d_D = nullptr;
     int nrhs_cap = 0;
+    // CUDA graphs of the numeric launch sequences (captured once, replayed)
+    bool use_graphs = true;
+    cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
+    std::map<int, cudaGraphExec_t> sgraph;  // key: precision * 1024 + rhs count
     int factored = -1;  // precision of the current factor, -1 none
+    int status_init[2] = {0, 0};
     int not_spd = -1;
+    Profiler prof;
+    std::vector<double> prof_ms, prof_flops, prof_bytes;
+    std::vector<long long> prof_n;
 
     template <typename T>
     T* keep(T* p) {
         owned.push_back(p);
         return p;
     }
+    void drop_solve_graphs() {
+        for (auto& kv : sgraph) cudaGraphExecDestroy(kv.second);
+        sgraph.clear();
+    }
     ~mdgpu_handle_s() {
         if (!on_device) return;
         cudaSetDevice(device);
+        for (auto g : fgraph)
+            if (g) cudaGraphExecDestroy(g);
+        drop_solve_graphs();
         for (void* p : owned) cudaFree(p);
         for (void* p : {(void*)d_Ax, (void*)dL64, (void*)dU64, (void*)dL32, (void*)dU32,
+                        (void*)dD64, (void*)dD32,
                         (void*)d_xp, (void*)d_fv, (void*)d_B, (void*)d_X, (void*)d_R, (void*)d_D})
             if (p) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
@@ -142,13 +163,40 @@ void build_csr(mdgpu_handle_s* h, int n, const int* Ap, const int* Ai) {
 
 void finish_plan(mdgpu_handle_s* h) {
     build_plan(h->sym, h->sym.lower.nnz(), kLargeThreshold, h->plan);
+    build_large_tables(h->plan, kTile, kAssembleCols);
     build_factor_schedule(h->plan, kTile, kAssembleCols, h->fsched);
     build_solve_schedule(h->plan, kTile, h->ssched);
+    build_panel_schedule(h->plan, kTile, kPanel, kAssembleCols, h->pschedh);
     h->level = front_levels(h->plan);
+}
+
+void init_kernels_once() {
+    static bool done = false;
+    if (done) return;
+    init_factor_kernels();
+    init_solve_kernels();
+    init_schur_tc();
+    init_schur_f64();
+    done = true;
+}
+
+// Capture fn(stream) on the handle's own stream into an executable graph.
+template <typename F>
+cudaGraphExec_t capture(mdgpu_handle_s* h, F&& fn) {
+    cudaGraph_t g = nullptr;
+    ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    fn(h->stream);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    ck(e, "end capture");
+    cudaGraphExec_t ex = nullptr;
+    ck(cudaGraphInstantiate(&ex, g, 0), "instantiate graph");
+    cudaGraphDestroy(g);
+    return ex;
 }
 
 void upload_plan(mdgpu_handle_s* h) {
     if (!device_available()) return;
+    init_kernels_once();
     ck(cudaGetDevice(&h->device), "cudaGetDevice");
     h->on_device = true;
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
@@ -157,6 +205,9 @@ void upload_plan(mdgpu_handle_s* h) {
     D.n = P.n;
     D.nsuper = P.nsuper;
     D.nlevels = P.nlevels;
+    D.max_u = std::max(P.max_u, 1);
+    if ((size_t)D.max_u * sizeof(int) > 227 * 1024)
+        throw std::runtime_error("update matrix order exceeds the assembly kernel's shared memory");
     D.fronts = h->keep(upload(P.fronts));
     D.child = h->keep(upload(P.child));
     D.rows = h->keep(upload(P.rows));
@@ -177,12 +228,20 @@ void upload_plan(mdgpu_handle_s* h) {
     }
     D.fv_total = acc;
     D.fv_off = h->keep(upload(fvo));
+    D.dinv_off = h->keep(upload(P.dinv_off));
+    D.asm_off = h->keep(upload(P.asm_off));
+    D.asm_range = h->keep(upload(P.asm_range));
+    D.dinv_total = P.dinv_total;
     D.sched64.items = h->keep(upload(h->fsched.store.items));
     D.sched64.before = h->keep(upload(h->fsched.store.ctas_before));
     D.sched64.h_level_beg = h->fsched.level_beg;
     D.sched64.h_trsm = h->fsched.trsm;
     D.sched64.h_update = h->fsched.update;
     D.h_assemble = h->fsched.assemble;
+    D.psched.items = h->keep(upload(h->pschedh.store.items));
+    D.psched.before = h->keep(upload(h->pschedh.store.ctas_before));
+    D.psched.h_op_beg = h->pschedh.op_beg;
+    D.psched.h_ops = h->pschedh.ops;
     D.solve.items = h->keep(upload(h->ssched.store.items));
     D.solve.before = h->keep(upload(h->ssched.store.ctas_before));
     D.solve.fwd_beg = h->ssched.fwd_beg;
@@ -190,8 +249,52 @@ void upload_plan(mdgpu_handle_s* h) {
     D.solve.fwd = h->ssched.fwd;
     D.solve.bwd = h->ssched.bwd;
     D.solve.gather = h->ssched.gather;
+    // algorithmic work per launch, for the profiler's roofline figures
+    {
+        const TileSchedule& TS = h->fsched;
+        D.h_update_flops.assign(TS.update.size(), 0.0);
+        for (size_t q = 0; q < TS.update.size(); ++q) {
+            const WorkList& w = TS.update[q];
+            int k = w.step;
+            double fl = 0;
+            for (int it = 0; it < w.nitems; ++it) {
+                const FrontDesc& f = P.fronts[TS.store.items[w.off + it]];
+                int NT = front_tiles(f.m, f.c, kTile);
+                double K = std::min(kTile, f.c - k * kTile);
+                auto sz = [&](int t) {
+                    int nt1 = (f.c + kTile - 1) / kTile;
+                    if (t < nt1) return std::min(kTile, f.c - t * kTile);
+                    int s0 = f.c + (t - nt1) * kTile;
+                    return std::min(kTile, f.m - s0);
+                };
+                for (int i = k + 1; i < NT; ++i) {
+                    double ri = sz(i);
+                    fl += K * ri * (ri + 1);  // diagonal tile, lower part
+                    for (int j = k + 1; j < i; ++j) fl += 2.0 * K * ri * sz(j);
+                }
+            }
+            D.h_update_flops[q] = fl;
+        }
+        D.h_small_bytes.assign(P.small_ptr.size(), 0.0);
+        for (size_t b = 0; b + 1 < P.small_ptr.size(); ++b) {
+            double by = 0;
+            for (int q = P.small_ptr[b]; q < P.small_ptr[b + 1]; ++q) {
+                const FrontDesc& f = P.fronts[P.small_list[q]];
+                double u = f.m - f.c;
+                by += (f.a_end - f.a_beg) * 16.0 + 8.0 * f.m * f.c;
+                if (f.uoff >= 0) by += 8.0 * u * (u + 1) / 2;
+                for (int hh = f.child_beg; hh < f.child_end; ++hh) {
+                    const FrontDesc& g = P.fronts[P.child[hh]];
+                    double uc = g.m - g.c;
+                    by += 8.0 * uc * (uc + 1) / 2 + 4.0 * uc;
+                }
+            }
+            D.h_small_bytes[b] = by;
+        }
+    }
+    D.prof = &h->prof;
     if (!P.perm.empty()) h->d_perm = h->keep(upload(P.perm));
-    h->d_status = h->keep(dalloc<int>(1));
+    h->d_status = h->keep(dalloc<int>(2));
     h->d_Ax = dalloc<double>(std::max<int64_t>(P.nnz_user, 1));
     h->csr.rowptr = h->keep(upload(h->h_csr_rowptr));
     h->csr.col = h->keep(upload(h->h_csr_col));
@@ -225,14 +328,28 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
     if (precision == MDGPU_FP64) {
         if (!h->dL64) h->dL64 = dalloc<double>(P.lstore);
         if (!h->dU64) h->dU64 = dalloc<double>(P.ustore);
+        if (!h->dD64) h->dD64 = dalloc<double>(P.dinv_total);
     } else {
-        if (!h->dL32) h->dL32 = dalloc<float>(P.lstore);
+        if (!h->dL32) {
+            h->dL32 = dalloc<float>(P.lstore);
+            // TMA descriptors of every large front's FP32 panel (tensor-core path)
+            if (h->use_tensor_cores && !P.large_list.empty()) {
+                std::vector<CUtensorMap> maps;
+                std::vector<int> idx;
+                if (build_panel_maps(P, h->dL32, maps, idx) == 0) {
+                    h->D.tmaps = h->keep(upload(maps));
+                    h->D.tmap_idx = h->keep(upload(idx));
+                }
+            }
+        }
         if (!h->dU32) h->dU32 = dalloc<float>(P.ustore);
+        if (!h->dD32) h->dD32 = dalloc<float>(P.dinv_total);
     }
 }
 
 void ensure_solve_storage(mdgpu_handle_s* h, int nrhs) {
     if (nrhs <= h->nrhs_cap) return;
+    h->drop_solve_graphs();  // they reference the buffers replaced below
     for (double** p : {&h->d_xp, &h->d_fv, &h->d_B, &h->d_X, &h->d_R, &h->d_D})
         if (*p) {
             cudaFree(*p);
@@ -264,15 +381,33 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
                            cudaMemcpyDeviceToDevice, st),
            "copy values");
     const int big = INT_MAX;
-    ck(cudaMemcpyAsync(h->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, st), "status");
-    if (precision == MDGPU_FP64)
-        factor_levels<double>(h->D, h->dL64, h->dU64, h->d_Ax, h->d_status, st);
-    else
-        factor_levels<float>(h->D, h->dL32, h->dU32, h->d_Ax, h->d_status, st);
+    h->status_init[0] = big;
+    h->status_init[1] = 0;
+    ck(cudaMemcpyAsync(h->d_status, h->status_init, 2 * sizeof(int), cudaMemcpyHostToDevice, st),
+       "status");
+    auto run = [h, precision](cudaStream_t s) {
+        if (precision == MDGPU_FP64)
+            factor_levels<double>(h->D, h->dL64, h->dU64, h->dD64, h->d_Ax, h->d_status, s);
+        else
+            factor_levels<float>(h->D, h->dL32, h->dU32, h->dD32, h->d_Ax, h->d_status, s);
+    };
+    if (h->use_graphs && !h->prof.on) {
+        cudaGraphExec_t& g = h->fgraph[precision];
+        if (!g) g = capture(h, run);
+        ck(cudaGraphLaunch(g, st), "factor graph");
+    } else {
+        run(st);
+    }
     ck(cudaGetLastError(), "factor launch");
-    int col = big;
-    ck(cudaMemcpyAsync(&col, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    int stat[2] = {big, 0};
+    ck(cudaMemcpyAsync(stat, h->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "status");
     ck(cudaStreamSynchronize(st), "factor");
+    int col = stat[0];
+    if (stat[1] != 0) {
+        h->factored = -1;
+        return fail(MDGPU_ERR_CUDA, "tensor-core Schur update: pipeline wait timed out (code " +
+                                        std::to_string(stat[1]) + ")");
+    }
     h->factored = precision;
     h->not_spd = (col == big) ? -1 : col;
     if (h->not_spd >= 0) {
@@ -290,10 +425,20 @@ void do_solve(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
     for (int q0 = 0; q0 < nrhs; q0 += 64) {
         int nq = std::min(64, nrhs - q0);
         permute_gather(h->d_perm, dB + (int64_t)q0 * ldb, h->d_xp, n, nq, ldb, st);
-        if (h->factored == MDGPU_FP64)
-            solve_levels<double, double>(h->D, h->dL64, h->d_xp, h->d_fv, nq, st);
-        else
-            solve_levels<float, double>(h->D, h->dL32, h->d_xp, h->d_fv, nq, st);
+        const int prec = h->factored;
+        auto run = [h, prec, nq](cudaStream_t s) {
+            if (prec == MDGPU_FP64)
+                solve_levels<double, double>(h->D, h->dL64, h->dD64, h->d_xp, h->d_fv, nq, s);
+            else
+                solve_levels<float, double>(h->D, h->dL32, h->dD32, h->d_xp, h->d_fv, nq, s);
+        };
+        if (h->use_graphs && !h->prof.on) {
+            cudaGraphExec_t& g = h->sgraph[prec * 1024 + nq];
+            if (!g) g = capture(h, run);
+            ck(cudaGraphLaunch(g, st), "solve graph");
+        } else {
+            run(st);
+        }
         permute_scatter(h->d_perm, h->d_xp, dX + (int64_t)q0 * ldx, n, nq, ldx, st);
     }
     ck(cudaGetLastError(), "solve launch");
@@ -614,6 +759,44 @@ int mdgpu_get_L(mdgpu_handle h, long long* Lp, int* Li, double* Lx) {
         }
         return MDGPU_OK;
     });
+}
+
+int mdgpu_profile(mdgpu_handle h, int enable) {
+    if (!h) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    return guarded([&] {
+        Profiler& P = h->prof;
+        if (!P.recs.empty()) {
+            ck(cudaDeviceSynchronize(), "profile sync");
+            h->prof_ms.assign(KC_COUNT, 0.0);
+            h->prof_flops.assign(KC_COUNT, 0.0);
+            h->prof_bytes.assign(KC_COUNT, 0.0);
+            h->prof_n.assign(KC_COUNT, 0);
+            for (auto& r : P.recs) {
+                float ms = 0;
+                ck(cudaEventElapsedTime(&ms, r.a, r.b), "event time");
+                h->prof_ms[r.cls] += ms;
+                h->prof_flops[r.cls] += r.flops;
+                h->prof_bytes[r.cls] += r.bytes;
+                h->prof_n[r.cls] += 1;
+            }
+        }
+        P.recs.clear();
+        P.used = 0;
+        P.on = enable != 0;
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_profile_read(mdgpu_handle h, int cls, double* ms, long long* launches, double* flops,
+                       double* bytes) {
+    if (!h || cls < 0 || cls >= KC_COUNT) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    bool have = (int)h->prof_ms.size() == KC_COUNT;
+    if (ms) *ms = have ? h->prof_ms[cls] : 0.0;
+    if (launches) *launches = have ? h->prof_n[cls] : 0;
+    if (flops) *flops = have ? h->prof_flops[cls] : 0.0;
+    if (bytes) *bytes = have ? h->prof_bytes[cls] : 0.0;
+    return MDGPU_OK;
 }
 
 const char* mdgpu_status_string(int status) {

@@ -9,8 +9,10 @@
 // storage, batched over all large fronts of one tree level:
 //   k_big_assemble   CTA per (front, 32-column block): zero, scatter A, pull the
 //                    children's update columns that land in the block
-//   k_tile_potrf     CTA per front: Cholesky of the first diagonal tile
-//   k_tile_trsm      CTA per (front, row tile below the panel): X = A L^-T
+//   k_tile_potrf     CTA per front: Cholesky of the first diagonal tile, and its
+//                    inverse (kept: it turns every TRSM and every solve step
+//                    with this tile into a small matrix product)
+//   k_tile_trsm      CTA per (front, row tile below the panel): X = A inv(L)'
 //   k_tile_update    CTA per (front, lower tile right of the panel):
 //                    C -= A B'; the CTA holding the next diagonal tile also
 //                    factors it, so the next step's TRSM can start at once.
@@ -112,14 +114,17 @@ __global__ void __launch_bounds__(256)
                    const int* __restrict__ child, const int* __restrict__ relmap,
                    const int* __restrict__ a_src, const int* __restrict__ a_pos,
                    const int* __restrict__ a_colptr, const int* __restrict__ a_colptr_off,
+                   const int* __restrict__ asm_off, const int* __restrict__ asm_range,
                    const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us) {
-    __shared__ int range[2];
+    extern __shared__ int rel_sh[];  // a child's relative map from its first column in range
     const int it = find_item(before, nitems, blockIdx.x);
     const int s = items[it];
     const int blk = blockIdx.x - before[it];
     const FrontDesc f = fronts[s];
     const int j0 = blk * CB, j1 = min(j0 + CB, f.m);
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int nch = f.child_end - f.child_beg;
+    const int* ranges = asm_range + asm_off[s] + blk * nch * 2;
 
     for (int jj = j0; jj < j1; ++jj) {
         if (jj < f.c) {
@@ -143,33 +148,34 @@ __global__ void __launch_bounds__(256)
         }
     }
     __syncthreads();
-    for (int h = f.child_beg; h < f.child_end; ++h) {
-        const FrontDesc g = fronts[child[h]];
+    // children one after another (deterministic sums); each child's update
+    // columns that land in [j0, j1) were located on the host.  The child's
+    // relative map goes to shared memory and every thread keeps four
+    // independent loads in flight before its read-modify-writes.
+    for (int h = 0; h < nch; ++h) {
+        const int jlo = ranges[2 * h], jhi = ranges[2 * h + 1];
+        if (jlo == jhi) continue;
+        const FrontDesc g = fronts[child[f.child_beg + h]];
         const int uc = g.m - g.c;
         const int* rm = relmap + g.rows_off + g.c;
-        if (tid == 0) {
-            int lo = 0, hi = uc;  // first update column mapping to >= j0
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (rm[mid] < j0) lo = mid + 1; else hi = mid;
-            }
-            int a = lo;
-            hi = uc;
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (rm[mid] < j1) lo = mid + 1; else hi = mid;
-            }
-            range[0] = a;
-            range[1] = lo;
-        }
+        for (int q = jlo + tid; q < uc; q += nt) rel_sh[q - jlo] = rm[q];
         __syncthreads();
-        const int jlo = range[0], jhi = range[1];
         const T* U = Us + g.uoff;
         for (int jc = jlo; jc < jhi; ++jc) {
-            const int pc = rm[jc];
-            for (int ic = jc + tid; ic < uc; ic += nt) {
-                T v = U[ic + (int64_t)jc * g.ldu];
-                *front_elem(Ls, Us, f, rm[ic], pc) += v;
+            const int pc = rel_sh[jc - jlo];
+            const T* ucol = U + (int64_t)jc * g.ldu;
+            for (int ic0 = jc + tid; ic0 < uc; ic0 += 4 * nt) {
+                T v[4];
+                int pr[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int ic = ic0 + u * nt;
+                    pr[u] = ic < uc ? rel_sh[ic - jlo] : -1;
+                    v[u] = ic < uc ? ucol[ic] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (pr[u] >= 0) *front_elem(Ls, Us, f, pr[u], pc) += v[u];
             }
         }
         __syncthreads();
@@ -201,12 +207,36 @@ __device__ void tile_potrf_smem(T* S, int LDS, int n, int* status, int col0) {
     }
 }
 
+// In-place inverse of an n x n lower-triangular tile in shared memory (ld =
+// LDS), columns right to left: column j of inv(L) is -inv(L_jj) times the
+// already inverted trailing block applied to L's column j.  tmp: n entries.
+template <typename T>
+__device__ void tile_trtri_smem(T* S, int LDS, int n, T* tmp) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int j = n - 1; j >= 0; --j) {
+        for (int i = j + 1 + tid; i < n; i += nt) tmp[i] = S[i + j * LDS];
+        __syncthreads();
+        const T djj = T(1) / S[j + j * LDS];
+        for (int i = j + 1 + tid; i < n; i += nt) {
+            T acc = T(0);
+            for (int l = j + 1; l <= i; ++l) acc += S[i + l * LDS] * tmp[l];
+            S[i + j * LDS] = -djj * acc;
+        }
+        __syncthreads();
+        if (tid == 0) S[j + j * LDS] = djj;
+        __syncthreads();
+    }
+}
+
+// Factor diagonal tile k of front f in place and store its inverse (TB x TB,
+// column-major, upper part zero) at Dk.
 template <typename T, int TB>
-__device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* S, int* status) {
+__device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, int* status) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
     T* base = Ls + f.loff + tk.start + (int64_t)tk.start * f.ldl;
+    T* tmp = S + TB * (TB + 1);
     for (int idx = tid; idx < n * n; idx += nt) {
         int j = idx / n, i = idx - j * n;
         S[i + j * (TB + 1)] = (i >= j) ? base[i + (int64_t)j * f.ldl] : T(0);
@@ -217,91 +247,33 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* S, int* sta
         int j = idx / n, i = idx - j * n;
         if (i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * (TB + 1)];
     }
+    __syncthreads();
+    tile_trtri_smem(S, TB + 1, n, tmp);
+    for (int idx = tid; idx < TB * TB; idx += nt) {
+        int j = idx / TB, i = idx - j * TB;
+        Dk[idx] = (i >= j && i < n && j < n) ? S[i + j * (TB + 1)] : T(0);
+    }
 }
 
 template <typename T, int TB>
 __global__ void __launch_bounds__(256)
     k_tile_potrf(const FrontDesc* __restrict__ fronts, const int* __restrict__ list, int k,
-                 T* __restrict__ Ls, int* __restrict__ status) {
-    __shared__ T S[TB * (TB + 1)];
-    const FrontDesc f = fronts[list[blockIdx.x]];
+                 const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
+                 int* __restrict__ status) {
+    __shared__ T S[TB * (TB + 1) + TB];
+    const int s = list[blockIdx.x];
+    const FrontDesc f = fronts[s];
     if (k >= tiles_l(f.c, TB)) return;
-    potrf_diag_tile<T, TB>(f, k, Ls, S, status);
+    potrf_diag_tile<T, TB>(f, k, Ls, Dinv + dinv_off[s] + (int64_t)k * TB * TB, S, status);
 }
 
+// C (TB x TB, tile (i, j) of front f) -= A B' with A = rows of tile i and
+// B = rows of tile j, both over the K columns of panel tile k; 256 threads,
+// 4 x 4 outputs each.  As/Bs: K x TB staging in shared memory.
 template <typename T, int TB>
-__global__ void __launch_bounds__(TB)
-    k_tile_trsm(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-                const int* __restrict__ before, int nitems, int k, T* __restrict__ Ls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Lkk = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1)
-    T* X = Lkk + TB * (TB + 1);               // TB x (TB + 1), row-major rows
-    T* dinv = X + TB * (TB + 1);              // TB
-    const int it = find_item(before, nitems, blockIdx.x);
-    const FrontDesc f = fronts[items[it]];
-    const int i = k + 1 + (blockIdx.x - before[it]);
-    const TileRange tk = tile_range(k, f.m, f.c, TB);
-    const TileRange ti = tile_range(i, f.m, f.c, TB);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int nk = tk.size, ni = ti.size;
-    const T* lkk = Ls + f.loff + tk.start + (int64_t)tk.start * f.ldl;
-    T* aik = Ls + f.loff + ti.start + (int64_t)tk.start * f.ldl;
-    for (int idx = tid; idx < nk * nk; idx += nt) {
-        int j = idx / nk, r = idx - j * nk;
-        Lkk[r + j * (TB + 1)] = lkk[r + (int64_t)j * f.ldl];
-    }
-    for (int idx = tid; idx < ni * nk; idx += nt) {
-        int j = idx / ni, r = idx - j * ni;
-        X[r * (TB + 1) + j] = aik[r + (int64_t)j * f.ldl];  // row-major: row r contiguous
-    }
-    __syncthreads();
-    for (int j = tid; j < nk; j += nt) dinv[j] = T(1) / Lkk[j + j * (TB + 1)];
-    __syncthreads();
-    // X L' = A, one row per thread: x_j = (a_j - sum_{l<j} x_l L_jl) / L_jj
-    for (int r = tid; r < ni; r += nt) {
-        T* x = X + r * (TB + 1);
-        for (int j = 0; j < nk; ++j) {
-            T acc = x[j];
-            for (int l = 0; l < j; ++l) acc -= x[l] * Lkk[j + l * (TB + 1)];
-            x[j] = acc * dinv[j];
-        }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < ni * nk; idx += nt) {
-        int j = idx / ni, r = idx - j * ni;
-        aik[r + (int64_t)j * f.ldl] = X[r * (TB + 1) + j];
-    }
-}
-
-template <typename T, int TB>
-__global__ void __launch_bounds__(256)
-    k_tile_update(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-                  const int* __restrict__ before, int nitems, int k, T* __restrict__ Ls,
-                  T* __restrict__ Us, int* __restrict__ status) {
-    static_assert(TB == 64, "4x4 register tile over 256 threads assumes TB = 64");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* As = reinterpret_cast<T*>(smem_raw);  // [K][TB]
-    T* Bs = As + TB * TB;                    // [K][TB]
-    const int it = find_item(before, nitems, blockIdx.x);
-    const FrontDesc f = fronts[items[it]];
-    int ii, jj;
-    lower_index(blockIdx.x - before[it], ii, jj);
-    const int i = k + 1 + ii, j = k + 1 + jj;
-    const TileRange tk = tile_range(k, f.m, f.c, TB);
-    const TileRange ti = tile_range(i, f.m, f.c, TB);
-    const TileRange tj = tile_range(j, f.m, f.c, TB);
+__device__ void tile_gemm_nt_acc(const T* As, const T* Bs, int K, T (&acc)[4][4]) {
     const int tid = threadIdx.x;
-    const int K = tk.size;
-    const T* pa = Ls + f.loff + ti.start + (int64_t)tk.start * f.ldl;
-    const T* pb = Ls + f.loff + tj.start + (int64_t)tk.start * f.ldl;
-    for (int idx = tid; idx < TB * K; idx += 256) {
-        int q = idx / TB, r = idx - q * TB;
-        As[q * TB + r] = r < ti.size ? pa[r + (int64_t)q * f.ldl] : T(0);
-        Bs[q * TB + r] = r < tj.size ? pb[r + (int64_t)q * f.ldl] : T(0);
-    }
-    __syncthreads();
     const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
-    T acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -317,6 +289,98 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
     }
+}
+
+// X = A_ik inv(L_kk)' in place, CTA per row tile below the panel tile.
+template <typename T, int TB>
+__global__ void __launch_bounds__(256)
+    k_tile_trsm(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+                const int* __restrict__ before, int nitems, int k,
+                const int64_t* __restrict__ dinv_off, T* __restrict__ Ls,
+                const T* __restrict__ Dinv) {
+    static_assert(TB == 64, "4x4 register tile over 256 threads assumes TB = 64");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* As = reinterpret_cast<T*>(smem_raw);  // [K][TB]
+    T* Bs = As + TB * TB;                    // [K][TB]: inv(L_kk)' columns
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it];
+    const FrontDesc f = fronts[s];
+    const int i = k + 1 + (blockIdx.x - before[it]);
+    const TileRange tk = tile_range(k, f.m, f.c, TB);
+    const TileRange ti = tile_range(i, f.m, f.c, TB);
+    const int tid = threadIdx.x;
+    const int K = tk.size;
+    T* aik = Ls + f.loff + ti.start + (int64_t)tk.start * f.ldl;
+    const T* Dk = Dinv + dinv_off[s] + (int64_t)k * TB * TB;  // inv(L_kk), col-major TB
+    for (int idx = tid; idx < TB * K; idx += 256) {
+        int q = idx / TB, r = idx - q * TB;
+        As[q * TB + r] = r < ti.size ? aik[r + (int64_t)q * f.ldl] : T(0);
+        Bs[q * TB + r] = Dk[r + q * TB];  // Bs[q][j] = inv(L)[j][q]
+    }
+    __syncthreads();
+    T acc[4][4];
+    tile_gemm_nt_acc<T, TB>(As, Bs, K, acc);
+    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        int cc = c0 + b;
+        if (cc >= K) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            int rr = r0 + a;
+            if (rr < ti.size) aik[rr + (int64_t)cc * f.ldl] = acc[a][b];
+        }
+    }
+}
+
+// jcap < 0: every lower tile right of panel tile k (the FP64 schedule).
+// jcap >= 0: only tile columns k < j <= jcap (the rest of a 256-column panel;
+// the trailing part then gets one tensor-core update per panel).
+template <typename T, int TB>
+__global__ void __launch_bounds__(256)
+    k_tile_update(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+                  const int* __restrict__ before, int nitems, int k, int jcap,
+                  const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Us,
+                  T* __restrict__ Dinv, int* __restrict__ status) {
+    static_assert(TB == 64, "4x4 register tile over 256 threads assumes TB = 64");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* As = reinterpret_cast<T*>(smem_raw);  // [K][TB]
+    T* Bs = As + TB * TB;                    // [K][TB]
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it];
+    const FrontDesc f = fronts[s];
+    int i, j;
+    if (jcap < 0) {
+        int ii, jj;
+        lower_index(blockIdx.x - before[it], ii, jj);
+        i = k + 1 + ii;
+        j = k + 1 + jj;
+    } else {  // column-major over the panel's remaining tile columns
+        const int NT = tiles_l(f.c, TB) + (f.m - f.c + TB - 1) / TB;
+        int l = blockIdx.x - before[it];
+        j = k + 1;
+        while (l >= NT - j) {
+            l -= NT - j;
+            ++j;
+        }
+        i = j + l;
+    }
+    const TileRange tk = tile_range(k, f.m, f.c, TB);
+    const TileRange ti = tile_range(i, f.m, f.c, TB);
+    const TileRange tj = tile_range(j, f.m, f.c, TB);
+    const int tid = threadIdx.x;
+    const int K = tk.size;
+    const T* pa = Ls + f.loff + ti.start + (int64_t)tk.start * f.ldl;
+    const T* pb = Ls + f.loff + tj.start + (int64_t)tk.start * f.ldl;
+    for (int idx = tid; idx < TB * K; idx += 256) {
+        int q = idx / TB, r = idx - q * TB;
+        As[q * TB + r] = r < ti.size ? pa[r + (int64_t)q * f.ldl] : T(0);
+        Bs[q * TB + r] = r < tj.size ? pb[r + (int64_t)q * f.ldl] : T(0);
+    }
+    __syncthreads();
+    T acc[4][4];
+    tile_gemm_nt_acc<T, TB>(As, Bs, K, acc);
+    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
         int cc = c0 + b;
@@ -332,9 +396,9 @@ __global__ void __launch_bounds__(256)
         }
     }
     // the next diagonal tile is final now: factor it for the next step
-    if (i == k + 1 && j == k + 1 && i < tiles_l(f.c, TB)) {
+    if (i == k + 1 && j == k + 1 && i < tiles_l(f.c, TB) && (jcap < 0 || i <= jcap)) {
         __syncthreads();
-        potrf_diag_tile<T, TB>(f, i, Ls, As, status);
+        potrf_diag_tile<T, TB>(f, i, Ls, Dinv + dinv_off[s] + (int64_t)i * TB * TB, As, status);
     }
 }
 
@@ -343,13 +407,8 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 
 template <typename T>
-static size_t trsm_smem() {
-    return (size_t)(2 * 64 * 65 + 64) * sizeof(T);
-}
-
-template <typename T>
-void launch_small_fronts(const DevPlan& D, int level, const T* /*tag*/, T* Ls, T* Us,
-                         const double* Ax, int* status, cudaStream_t st) {
+void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax,
+                         int* status, cudaStream_t st) {
     for (int b = 0; b < kSmallBuckets; ++b) {
         int beg = D.h_small_ptr[level * kSmallBuckets + b];
         int end = D.h_small_ptr[level * kSmallBuckets + b + 1];
@@ -358,6 +417,8 @@ void launch_small_fronts(const DevPlan& D, int level, const T* /*tag*/, T* Ls, T
         int LD = MB + 1;
         size_t smem = (size_t)MB * LD * sizeof(T) + (size_t)MB * sizeof(int);
         int threads = MB <= 16 ? 64 : (MB <= 32 ? 128 : 256);
+        ProfScope ps(D.prof, KC_SMALL_FRONT, st, 0,
+                     D.h_small_bytes[level * kSmallBuckets + b] * sizeof(T) / 8.0);
         k_small_front<T><<<end - beg, threads, smem, st>>>(D.fronts, D.small_list + beg, D.child,
                                                           D.relmap, D.a_src, D.a_pos, Ax, Ls, Us,
                                                           LD, status);
@@ -365,51 +426,132 @@ void launch_small_fronts(const DevPlan& D, int level, const T* /*tag*/, T* Ls, T
 }
 
 template <typename T>
-void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax, int* status,
-                        cudaStream_t st) {
+void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, const double* Ax,
+                        int* status, cudaStream_t st) {
     const int lb = D.h_large_ptr[level], le = D.h_large_ptr[level + 1];
     if (le == lb) return;
     const DevSchedule& S = D.sched64;
     const WorkList& asl = D.h_assemble[level];
-    k_big_assemble<T><<<asl.nctas, 256, 0, st>>>(D.fronts, S.items + asl.off, S.before + asl.off,
-                                                 asl.nitems, kAssembleCols, D.child, D.relmap,
-                                                 D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off, Ax,
-                                                 Ls, Us);
-    k_tile_potrf<T, 64><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, 0, Ls, status);
+    {
+        ProfScope ps(D.prof, KC_ASSEMBLE, st);
+        k_big_assemble<T><<<asl.nctas, 256, D.max_u * sizeof(int), st>>>(
+            D.fronts, S.items + asl.off, S.before + asl.off, asl.nitems, kAssembleCols, D.child,
+            D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off, D.asm_off, D.asm_range, Ax,
+            Ls, Us);
+    }
+    {
+        ProfScope ps(D.prof, KC_POTRF, st);
+        k_tile_potrf<T, kTile><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, 0,
+                                                        D.dinv_off, Ls, Dinv, status);
+    }
+    const size_t gsm = 2 * kTile * kTile * sizeof(T);
     for (int q = S.h_level_beg[level]; q < S.h_level_beg[level + 1]; ++q) {
         const WorkList& tr = S.h_trsm[q];
         const WorkList& up = S.h_update[q];
-        if (tr.nctas > 0)
-            k_tile_trsm<T, 64><<<tr.nctas, 64, trsm_smem<T>(), st>>>(D.fronts, S.items + tr.off,
-                                                        S.before + tr.off, tr.nitems, tr.step, Ls);
-        if (up.nctas > 0)
-            k_tile_update<T, 64><<<up.nctas, 256, 2 * 64 * 64 * sizeof(T), st>>>(
-                D.fronts, S.items + up.off, S.before + up.off, up.nitems, up.step, Ls, Us, status);
+        if (tr.nctas > 0) {
+            ProfScope ps(D.prof, KC_TRSM, st);
+            k_tile_trsm<T, kTile><<<tr.nctas, 256, gsm, st>>>(
+                D.fronts, S.items + tr.off, S.before + tr.off, tr.nitems, tr.step, D.dinv_off, Ls,
+                Dinv);
+        }
+        if (up.nctas > 0) {
+            ProfScope ps(D.prof, KC_SCHUR, st, D.h_update_flops[q]);
+            k_tile_update<T, kTile><<<up.nctas, 256, gsm, st>>>(
+                D.fronts, S.items + up.off, S.before + up.off, up.nitems, up.step, -1, D.dinv_off,
+                Ls, Us, Dinv, status);
+        }
+    }
+}
+
+// Large fronts in 256-column panels: inside a panel the 64-wide tile steps
+// (TRSM, in-panel updates, fused diagonal POTRF); after it one wide Schur
+// update of the whole trailing part -- tcgen05 tensor cores (TF32) for FP32,
+// the register-tiled FP64 kernel for FP64.  status[1] receives the
+// tensor-core kernel's error code (pipeline wait timeout).
+template <typename T>
+static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv,
+                                      const double* Ax, int* status, cudaStream_t st) {
+    const DevSchedule& S = D.psched;
+    const size_t gsm = 2 * kTile * kTile * sizeof(T);
+    for (int q = S.h_op_beg[level]; q < S.h_op_beg[level + 1]; ++q) {
+        const PanelOp& op = S.h_ops[q];
+        const WorkList& w = op.w;
+        if (w.nctas == 0) continue;
+        switch (op.kind) {
+            case OP_ASSEMBLE: {
+                ProfScope ps(D.prof, KC_ASSEMBLE, st);
+                k_big_assemble<T><<<w.nctas, 256, D.max_u * sizeof(int), st>>>(
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols, D.child,
+                    D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off, D.asm_off, D.asm_range,
+                    Ax, Ls, Us);
+                break;
+            }
+            case OP_POTRF: {
+                ProfScope ps(D.prof, KC_POTRF, st);
+                k_tile_potrf<T, kTile><<<w.nitems, 256, 0, st>>>(
+                    D.fronts, S.items + w.off, op.arg, D.dinv_off, Ls, Dinv, status);
+                break;
+            }
+            case OP_TRSM: {
+                ProfScope ps(D.prof, KC_TRSM, st);
+                k_tile_trsm<T, kTile><<<w.nctas, 256, gsm, st>>>(
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, D.dinv_off, Ls,
+                    Dinv);
+                break;
+            }
+            case OP_UPDATE_PANEL: {
+                ProfScope ps(D.prof, KC_TRSM, st);
+                k_tile_update<T, kTile><<<w.nctas, 256, gsm, st>>>(
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, op.arg2,
+                    D.dinv_off, Ls, Us, Dinv, status);
+                break;
+            }
+            case OP_SCHUR_TC: {
+                ProfScope ps(D.prof, KC_SCHUR, st, op.flops);
+                if constexpr (sizeof(T) == 4)
+                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, st);
+                else
+                    launch_schur_f64(D, w, op.arg, kPanel, Ls, Us, st);
+                break;
+            }
+        }
     }
 }
 
 template <typename T>
-void factor_levels(const DevPlan& D, T* Ls, T* Us, const double* Ax, int* status,
+static void set_factor_attributes() {
+    cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    cudaFuncSetAttribute(k_tile_update<T, kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * kTile * kTile * sizeof(T));
+    cudaFuncSetAttribute(k_tile_trsm<T, kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * kTile * kTile * sizeof(T));
+    cudaFuncSetAttribute(k_big_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+}
+
+void init_factor_kernels() {
+    set_factor_attributes<double>();
+    set_factor_attributes<float>();
+}
+
+template <typename T>
+void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
                    cudaStream_t st) {
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             227 * 1024);
-        cudaFuncSetAttribute(k_tile_update<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             2 * 64 * 64 * sizeof(T));
-        cudaFuncSetAttribute(k_tile_trsm<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             trsm_smem<T>());
-        attr_done = true;
-    }
     for (int l = 0; l < D.nlevels; ++l) {
-        launch_small_fronts<T>(D, l, nullptr, Ls, Us, Ax, status, st);
-        launch_large_level<T>(D, l, Ls, Us, Ax, status, st);
+        launch_small_fronts<T>(D, l, Ls, Us, Ax, status, st);
+        // FP32 needs the TMA descriptors of the tensor-core path; without them
+        // (descriptor encoding unavailable) it keeps the 64-wide tile schedule
+        if (sizeof(T) == 8 || D.tmaps)
+            launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, st);
+        else
+            launch_large_level<T>(D, l, Ls, Us, Dinv, Ax, status, st);
     }
 }
 
-template void factor_levels<double>(const DevPlan&, double*, double*, const double*, int*,
-                                    cudaStream_t);
-template void factor_levels<float>(const DevPlan&, float*, float*, const double*, int*,
+template void factor_levels<double>(const DevPlan&, double*, double*, double*, const double*,
+                                    int*, cudaStream_t);
+template void factor_levels<float>(const DevPlan&, float*, float*, float*, const double*, int*,
                                    cudaStream_t);
 
 }  // namespace mdgpu

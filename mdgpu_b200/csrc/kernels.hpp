@@ -1,6 +1,7 @@
 // Host-side view of the device-resident plan and the kernel launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -10,7 +11,70 @@
 namespace mdgpu {
 
 constexpr int kAssembleCols = 32;  // columns per CTA in the large-front assembly
+
+// Kernel classes timed by the profiler.
+enum KernelClass {
+    KC_SMALL_FRONT = 0,  // fused small-front factor
+    KC_ASSEMBLE,         // large-front assembly
+    KC_POTRF,            // first diagonal tile of large fronts
+    KC_TRSM,             // panel triangular solves
+    KC_SCHUR,            // Schur-complement tile updates (dominant flops)
+    KC_SOLVE_SMALL,      // small-front forward/backward sweeps
+    KC_SOLVE_LARGE,      // large-front forward/backward steps
+    KC_OTHER,            // permutations, residual, norms
+    KC_COUNT
+};
+
+// Optional per-launch CUDA-event timing, grouped by kernel class; off by
+// default (no events recorded).  Algorithmic flops / bytes per launch are
+// accumulated alongside for roofline figures.
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int cls;
+        cudaEvent_t a, b;
+        double flops, bytes;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    cudaEvent_t take() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    ~Profiler() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+// RAII helper: records a begin/end event pair around the launches in scope.
+struct ProfScope {
+    Profiler* p;
+    int cls;
+    double flops, bytes;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    ProfScope(Profiler* p_, int cls_, cudaStream_t st_, double fl = 0, double by = 0)
+        : p(p_), cls(cls_), flops(fl), bytes(by), st(st_) {
+        if (p && p->on) {
+            a = p->take();
+            cudaEventRecord(a, st);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            cudaEvent_t b = p->take();
+            cudaEventRecord(b, st);
+            p->recs.push_back({cls, a, b, flops, bytes});
+        }
+    }
+};
 constexpr int kTile = 64;          // tile of the large-front factor and solve kernels
+constexpr int kPanel = 256;        // FP32 path: pivot columns per tensor-core Schur update
 
 // A work-list schedule resident on the device (items/before arrays) with the
 // host copy of the per-launch descriptors.
@@ -19,6 +83,9 @@ struct DevSchedule {
     int* before = nullptr;
     std::vector<int> h_level_beg;
     std::vector<WorkList> h_trsm, h_update;
+    // panel schedule (FP32): per level a run of operations
+    std::vector<int> h_op_beg;
+    std::vector<PanelOp> h_ops;
 };
 
 struct SolveSchedule {
@@ -33,6 +100,7 @@ struct SolveSchedule {
 
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
+    int max_u = 0;  // largest update-matrix order (child relative maps in shared memory)
     FrontDesc* fronts = nullptr;
     int* child = nullptr;
     int* rows = nullptr;
@@ -44,22 +112,49 @@ struct DevPlan {
     int* small_list = nullptr;
     int* large_list = nullptr;
     int64_t* fv_off = nullptr;  // per supernode: offset of its front vector (m entries)
+    int64_t* dinv_off = nullptr;  // per supernode: inverted diagonal tiles (large fronts)
+    int* asm_off = nullptr;       // per supernode: child column ranges (large fronts)
+    int* asm_range = nullptr;
+    int64_t dinv_total = 0;
+    // FP32 path: per large front a TMA descriptor of its L panel, and the
+    // panel-wise schedule whose Schur updates run on the tensor cores
+    CUtensorMap* tmaps = nullptr;
+    int* tmap_idx = nullptr;
+    DevSchedule psched;
     std::vector<int> h_small_ptr, h_large_ptr;
     std::vector<WorkList> h_assemble;  // per level, offsets into sched64 arrays
     DevSchedule sched64;
     SolveSchedule solve;
     int64_t fv_total = 0;  // sum of m over supernodes
+    std::vector<double> h_update_flops;  // per update work list (algorithmic)
+    std::vector<double> h_small_bytes;   // per (level, bucket) small-front launch
+    Profiler* prof = nullptr;
 };
 
+// one-time kernel attribute setup (dynamic shared memory limits); must run
+// before any launch sequence is captured into a CUDA graph
+void init_factor_kernels();
+void init_solve_kernels();
+void init_schur_tc();
+void init_schur_f64();
+
 template <typename T>
-void factor_levels(const DevPlan& D, T* Ls, T* Us, const double* Ax, int* status,
+void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
                    cudaStream_t st);
 
 // Solves with the factor L (scalar TL) on vectors of type TV.  xp holds the
 // permuted right-hand sides on entry (n x nrhs, ld n) and the permuted
 // solution on exit; fv is scratch of fv_total * nrhs entries.
 template <typename TL, typename TV>
-void solve_levels(const DevPlan& D, const TL* Ls, TV* xp, TV* fv, int nrhs, cudaStream_t st);
+void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
+                  cudaStream_t st);
+
+int build_panel_maps(const Plan& P, const float* Ls, std::vector<CUtensorMap>& maps,
+                     std::vector<int>& idx);
+void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
+                     float* Us, int* err, cudaStream_t st);
+void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,
+                      double* Us, cudaStream_t st);
 
 // gather / scatter with the fill-reducing permutation (perm: new -> old)
 void permute_gather(const int* perm, const double* b, double* xp, int n, int nrhs, int ldb,

@@ -206,6 +206,34 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
     if (P.a_colptr.empty()) P.a_colptr.push_back(0);
 }
 
+void build_large_tables(Plan& P, int T, int CB) {
+    P.dinv_off.assign(P.nsuper, -1);
+    P.asm_off.assign(P.nsuper, -1);
+    P.asm_range.clear();
+    int64_t d = 0;
+    for (int s : P.large_list) {
+        const FrontDesc& f = P.fronts[s];
+        P.dinv_off[s] = d;
+        d += (int64_t)((f.c + T - 1) / T) * T * T;
+        int nblk = (f.m + CB - 1) / CB;
+        P.asm_off[s] = (int)P.asm_range.size();
+        for (int b = 0; b < nblk; ++b) {
+            int j0 = b * CB, j1 = std::min(j0 + CB, f.m);
+            for (int h = f.child_beg; h < f.child_end; ++h) {
+                const FrontDesc& g = P.fronts[P.child[h]];
+                const int* rm = P.relmap.data() + g.rows_off + g.c;
+                int uc = g.m - g.c;
+                int lo = (int)(std::lower_bound(rm, rm + uc, j0) - rm);
+                int hi = (int)(std::lower_bound(rm, rm + uc, j1) - rm);
+                P.asm_range.push_back(lo);
+                P.asm_range.push_back(hi);
+            }
+        }
+    }
+    P.dinv_total = std::max<int64_t>(d, 32);
+    if (P.asm_range.empty()) P.asm_range.push_back(0);
+}
+
 WorkList ListStore::add(const std::vector<std::pair<int, int>>& it, int step) {
     WorkList w;
     w.off = (int64_t)items.size();
@@ -293,6 +321,78 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     }
     S.fwd_beg[P.nlevels] = (int)S.fwd.size();
     S.bwd_beg[P.nlevels] = (int)S.bwd.size();
+}
+
+void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S) {
+    S = PanelSchedule();
+    const int TPP = PW / T;  // tiles per panel
+    S.op_beg.assign(P.nlevels + 1, 0);
+    auto tsize = [&](const FrontDesc& f, int t) {
+        int nt1 = (f.c + T - 1) / T;
+        if (t < nt1) return std::min(T, f.c - t * T);
+        return std::min(T, f.m - (f.c + (t - nt1) * T));
+    };
+    for (int l = 0; l < P.nlevels; ++l) {
+        S.op_beg[l] = (int)S.ops.size();
+        std::vector<int> fr(P.large_list.begin() + P.large_ptr[l],
+                            P.large_list.begin() + P.large_ptr[l + 1]);
+        if (fr.empty()) continue;
+        std::vector<std::pair<int, int>> as, po;
+        int maxpanels = 0;
+        for (int s : fr) {
+            const FrontDesc& f = P.fronts[s];
+            as.push_back({s, (f.m + CB - 1) / CB});
+            po.push_back({s, 1});
+            maxpanels = std::max(maxpanels, (f.c + PW - 1) / PW);
+        }
+        S.ops.push_back({OP_ASSEMBLE, 0, 0, S.store.add(as, 0), 0});
+        S.ops.push_back({OP_POTRF, 0, 0, S.store.add(po, 0), 0});
+        for (int p = 0; p < maxpanels; ++p) {
+            for (int k = p * TPP; k < (p + 1) * TPP; ++k) {
+                std::vector<std::pair<int, int>> tr, up;
+                double upfl = 0;
+                for (int s : fr) {
+                    const FrontDesc& f = P.fronts[s];
+                    int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                    if (k >= nt1) continue;
+                    if (NT - k - 1 > 0) tr.push_back({s, NT - k - 1});
+                    int jl = std::min((p + 1) * TPP - 1, nt1 - 1);
+                    int cnt = 0;
+                    for (int j = k + 1; j <= jl; ++j) {
+                        cnt += NT - j;
+                        double K = tsize(f, k), rj = tsize(f, j);
+                        upfl += K * rj * (rj + 1);
+                        for (int i = j + 1; i < NT; ++i) upfl += 2.0 * K * tsize(f, i) * rj;
+                    }
+                    if (cnt > 0) up.push_back({s, cnt});
+                }
+                if (!tr.empty()) S.ops.push_back({OP_TRSM, k, 0, S.store.add(tr, k), 0});
+                if (!up.empty())
+                    S.ops.push_back({OP_UPDATE_PANEL, k, (p + 1) * TPP - 1, S.store.add(up, k), upfl});
+            }
+            std::vector<std::pair<int, int>> big, nextp;
+            double fl = 0;
+            for (int s : fr) {
+                const FrontDesc& f = P.fronts[s];
+                int k0 = p * PW;
+                if (k0 >= f.c) continue;
+                int K = std::min(PW, f.c - k0);
+                int cbeg = std::min(k0 + PW, f.c);
+                if (cbeg < f.m) {
+                    int NB = (f.m + 127) / 128, J0 = cbeg / 128;
+                    int nb = NB - J0;
+                    big.push_back({s, nb * (nb + 1) / 2});
+                    double tr = f.m - cbeg;
+                    fl += (double)K * tr * (tr + 1);  // lower trailing part, 2 flops per FMA
+                }
+                if ((p + 1) * PW < f.c) nextp.push_back({s, 1});
+            }
+            if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), fl});
+            if (!nextp.empty())
+                S.ops.push_back({OP_POTRF, (p + 1) * TPP, 0, S.store.add(nextp, 0), 0});
+        }
+    }
+    S.op_beg[P.nlevels] = (int)S.ops.size();
 }
 
 std::vector<int> front_levels(const Plan& P) {

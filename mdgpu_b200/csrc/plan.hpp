@@ -62,6 +62,13 @@ struct Plan {
     std::vector<int> a_pos;     // per A entry: local (row | col << 16) inside the front
     std::vector<int> a_colptr;  // per large front: c+1 offsets into its A entries
     std::vector<int> a_colptr_off;  // per supernode: offset into a_colptr (-1 if small)
+    // large fronts: inverted diagonal tiles (T x T each, one per pivot tile)
+    std::vector<int64_t> dinv_off;  // per supernode (-1 if small)
+    int64_t dinv_total = 0;         // elements
+    // large fronts: per 32-column block of the front and per child, the
+    // child's update columns [lo, hi) that land in the block
+    std::vector<int> asm_off;       // per supernode (-1 if small)
+    std::vector<int> asm_range;
     std::vector<int64_t> Lp;    // CSC column pointers of L (reference spL->p)
     int64_t lstore = 0, ustore = 0;  // element counts
     int64_t lnz = 0;
@@ -86,6 +93,8 @@ int small_front_limit(int scalar_bytes);
 // Build the plan from a completed symbolic analysis.  `large_threshold` is
 // the row count above which a front takes the tiled multi-CTA path.
 void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& P);
+// Fill dinv_off / asm_off / asm_range for tile size T and assembly width CB.
+void build_large_tables(Plan& P, int T, int CB);
 
 // Work-list storage: every list is a run of (front id, CTAs before it)
 // pairs closed by a sentinel carrying the list's CTA total.
@@ -103,6 +112,22 @@ struct TileSchedule {
     std::vector<WorkList> trsm, update;  // one pair per (level, step)
     std::vector<WorkList> assemble;      // per level: CTA per (front, column block)
 };
+
+// FP32 panel schedule: per level, operations in launch order.
+enum PanelOpKind { OP_ASSEMBLE = 0, OP_POTRF, OP_TRSM, OP_UPDATE_PANEL, OP_SCHUR_TC };
+struct PanelOp {
+    int kind;
+    int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_TC)
+    int arg2;     // UPDATE_PANEL: last tile index of the panel
+    WorkList w;
+    double flops;  // algorithmic flops of SCHUR_TC / UPDATE_PANEL launches
+};
+struct PanelSchedule {
+    ListStore store;
+    std::vector<int> op_beg;  // per level
+    std::vector<PanelOp> ops;
+};
+void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S);
 
 // Work lists of the tiled solve kernels.
 struct SolveScheduleHost {

@@ -9,8 +9,9 @@
 // solution entries of its update rows (ancestors) directly.
 //
 // Small fronts: one CTA per front.  Large fronts: tiled, one launch per
-// 64-row block of the diagonal block, many CTAs per launch; every CTA solves
-// the small triangle redundantly so no launch needs a second phase.
+// 64-row block of the diagonal block, many CTAs per launch; every CTA applies
+// the block's inverse (stored by the factorization) redundantly -- a 64 x 64
+// product, no serial substitution -- so no launch needs a second phase.
 #include "device_common.cuh"
 #include "kernels.hpp"
 
@@ -161,93 +162,39 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Solve the nk x nk (nk <= 64) lower triangle held in shared memory against
-// y (nk x nrhs).  Few right-hand sides: warp 0 alone, rows in lanes, no block
-// barriers inside; many: the whole block, two barriers per column.
+// y = inv(L_kk) f or x = inv(L_kk)' t for one pivot tile, with the inverse
+// stored by the factorization (Dk: T x T column-major, zero above the
+// diagonal); in and out are nk x nrhs in shared memory.
 template <typename TV>
-__device__ void tri_lower_solve(const TV* Lkk, int LDK, TV* y, int nk, int nrhs) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (nrhs <= 8) {
-        if (tid < 32) {
-            const int r0 = tid, r1 = tid + 32;
-            for (int q = 0; q < nrhs; ++q) {
-                TV* yq = y + q * nk;
-                TV v0 = r0 < nk ? yq[r0] : TV(0), v1 = r1 < nk ? yq[r1] : TV(0);
-                for (int j = 0; j < nk; ++j) {
-                    TV yj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-                    yj *= TV(1) / Lkk[j + j * LDK];
-                    if (r0 == j) v0 = yj;
-                    if (r1 == j) v1 = yj;
-                    if (r0 > j && r0 < nk) v0 -= Lkk[r0 + j * LDK] * yj;
-                    if (r1 > j && r1 < nk) v1 -= Lkk[r1 + j * LDK] * yj;
-                }
-                if (r0 < nk) yq[r0] = v0;
-                if (r1 < nk) yq[r1] = v1;
-            }
+__device__ void apply_tile_inverse(const TV* Dk, const TV* in, TV* out, int nk, int nrhs,
+                                   bool transpose) {
+    constexpr int T = kTile;
+    for (int idx = threadIdx.x; idx < nk * nrhs; idx += blockDim.x) {
+        int q = idx / nk, r = idx - q * nk;
+        const TV* v = in + q * nk;
+        TV acc = TV(0);
+        if (!transpose) {
+            for (int l = 0; l <= r; ++l) acc += Dk[r + l * T] * v[l];
+        } else {
+            for (int l = r; l < nk; ++l) acc += Dk[l + r * T] * v[l];
         }
-        __syncthreads();
-        return;
+        out[idx] = acc;
     }
-    for (int j = 0; j < nk; ++j) {
-        const TV inv = TV(1) / Lkk[j + j * LDK];
-        for (int q = tid; q < nrhs; q += nt) y[j + q * nk] *= inv;
-        __syncthreads();
-        const int rows = nk - j - 1;
-        for (int idx = tid; idx < rows * nrhs; idx += nt) {
-            int q = idx / rows, r = j + 1 + (idx - q * rows);
-            y[r + q * nk] -= Lkk[r + j * LDK] * y[j + q * nk];
-        }
-        __syncthreads();
-    }
-}
-
-// x = Lkk^-T t in shared memory (t overwritten); same two regimes.
-template <typename TV>
-__device__ void tri_upper_solve(const TV* Lkk, int LDK, TV* t, int nk, int nrhs) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (nrhs <= 8) {
-        if (tid < 32) {
-            const int r0 = tid, r1 = tid + 32;
-            for (int q = 0; q < nrhs; ++q) {
-                TV* tq = t + q * nk;
-                TV v0 = r0 < nk ? tq[r0] : TV(0), v1 = r1 < nk ? tq[r1] : TV(0);
-                for (int j = nk - 1; j >= 0; --j) {
-                    TV xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-                    xj *= TV(1) / Lkk[j + j * LDK];
-                    if (r0 == j) v0 = xj;
-                    if (r1 == j) v1 = xj;
-                    if (r0 < j) v0 -= Lkk[j + r0 * LDK] * xj;
-                    if (r1 < j) v1 -= Lkk[j + r1 * LDK] * xj;
-                }
-                if (r0 < nk) tq[r0] = v0;
-                if (r1 < nk) tq[r1] = v1;
-            }
-        }
-        __syncthreads();
-        return;
-    }
-    for (int j = nk - 1; j >= 0; --j) {
-        const TV inv = TV(1) / Lkk[j + j * LDK];
-        for (int q = tid; q < nrhs; q += nt) t[j + q * nk] *= inv;
-        __syncthreads();
-        for (int idx = tid; idx < j * nrhs; idx += nt) {
-            int q = idx / j, l = idx - q * j;
-            t[l + q * nk] -= Lkk[j + l * LDK] * t[j + q * nk];
-        }
-        __syncthreads();
-    }
+    __syncthreads();
 }
 
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(256)
     k_fwd_step(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int kb,
-               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
-               TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs) {
+               const int64_t* __restrict__ fv_off, const int64_t* __restrict__ dinv_off,
+               const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
+               TV* __restrict__ fv, int n, int nrhs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int T = kTile, LDK = kTile + 1;
-    TV* Lkk = reinterpret_cast<TV*>(smem_raw);  // T x LDK
-    TV* y = Lkk + T * LDK;                      // nk x nrhs
+    constexpr int T = kTile;
+    TV* Dk = reinterpret_cast<TV*>(smem_raw);  // T x T
+    TV* fk = Dk + T * T;                       // nk x nrhs
+    TV* y = fk + T * nrhs;                     // nk x nrhs
     const int it = find_item(before, nitems, blockIdx.x);
     const int s = items[it];
     const FrontDesc F = fronts[s];
@@ -257,16 +204,14 @@ __global__ void __launch_bounds__(256)
     const int tid = threadIdx.x, nt = blockDim.x;
     const TL* L = Ls + F.loff;
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < nk * nk; idx += nt) {
-        int j = idx / nk, r = idx - j * nk;
-        Lkk[r + j * LDK] = (TV)L[tk.start + r + (int64_t)(tk.start + j) * F.ldl];
-    }
+    const TL* dk = Dinv + dinv_off[s] + (int64_t)kb * T * T;
+    for (int idx = tid; idx < T * T; idx += nt) Dk[idx] = (TV)dk[idx];
     for (int idx = tid; idx < nk * nrhs; idx += nt) {
         int q = idx / nk, r = idx - q * nk;
-        y[idx] = f[tk.start + r + (int64_t)q * F.m];
+        fk[idx] = f[tk.start + r + (int64_t)q * F.m];
     }
     __syncthreads();
-    tri_lower_solve(Lkk, LDK, y, nk, nrhs);
+    apply_tile_inverse(Dk, fk, y, nk, nrhs, false);
     if (i == kb) {
         for (int idx = tid; idx < nk * nrhs; idx += nt) {
             int q = idx / nk, r = idx - q * nk;
@@ -274,13 +219,31 @@ __global__ void __launch_bounds__(256)
         }
         return;
     }
+    // f[tile i] -= L(tile i, tile kb) y: warp w takes columns w, w+8, ...; lanes
+    // take rows lane, lane+32 (coalesced, 16 independent loads per thread);
+    // the eight partial sums per row meet in shared memory
     const TileRange ti = tile_range(i, F.m, F.c, T);
-    for (int idx = tid; idx < ti.size * nrhs; idx += nt) {
-        int q = idx / ti.size, r = idx - q * ti.size;
-        const TL* row = L + ti.start + r + (int64_t)tk.start * F.ldl;
-        TV acc = TV(0);
-        for (int j = 0; j < nk; ++j) acc += (TV)row[(int64_t)j * F.ldl] * y[j + q * nk];
-        f[ti.start + r + (int64_t)q * F.m] -= acc;
+    TV* part = y + T * nrhs;  // 8 x T, one right-hand side at a time
+    const int lane = tid & 31, warp = tid >> 5;
+    const TL* blk = L + ti.start + (int64_t)tk.start * F.ldl;
+    for (int q = 0; q < nrhs; ++q) {
+        TV a0 = TV(0), a1 = TV(0);
+        for (int j = warp; j < nk; j += 8) {
+            const TV yj = y[j + q * nk];
+            const TL* col = blk + (int64_t)j * F.ldl;
+            if (lane < ti.size) a0 += (TV)col[lane] * yj;
+            if (lane + 32 < ti.size) a1 += (TV)col[lane + 32] * yj;
+        }
+        part[warp * T + lane] = a0;
+        part[warp * T + lane + 32] = a1;
+        __syncthreads();
+        for (int r = tid; r < ti.size; r += nt) {
+            TV acc = TV(0);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) acc += part[w * T + r];
+            f[ti.start + r + (int64_t)q * F.m] -= acc;
+        }
+        __syncthreads();
     }
 }
 
@@ -319,12 +282,14 @@ template <typename TL, typename TV>
 __global__ void __launch_bounds__(256)
     k_bwd_step(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int kb,
-               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
-               TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs) {
+               const int64_t* __restrict__ fv_off, const int64_t* __restrict__ dinv_off,
+               const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
+               TV* __restrict__ fv, int n, int nrhs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int T = kTile, LDK = kTile + 1;
-    TV* Lkk = reinterpret_cast<TV*>(smem_raw);
-    TV* x = Lkk + T * LDK;
+    constexpr int T = kTile;
+    TV* Dk = reinterpret_cast<TV*>(smem_raw);  // T x T
+    TV* tk_ = Dk + T * T;                      // nk x nrhs
+    TV* x = tk_ + T * nrhs;                    // nk x nrhs
     const int it = find_item(before, nitems, blockIdx.x);
     const int s = items[it];
     const FrontDesc F = fronts[s];
@@ -335,16 +300,14 @@ __global__ void __launch_bounds__(256)
     const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const TL* L = Ls + F.loff;
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < nk * nk; idx += nt) {
-        int j = idx / nk, r = idx - j * nk;
-        Lkk[r + j * LDK] = (TV)L[tk.start + r + (int64_t)(tk.start + j) * F.ldl];
-    }
+    const TL* dk = Dinv + dinv_off[s] + (int64_t)kb * T * T;
+    for (int idx = tid; idx < T * T; idx += nt) Dk[idx] = (TV)dk[idx];
     for (int idx = tid; idx < nk * nrhs; idx += nt) {
         int q = idx / nk, r = idx - q * nk;
-        x[idx] = f[tk.start + r + (int64_t)q * F.m];
+        tk_[idx] = f[tk.start + r + (int64_t)q * F.m];
     }
     __syncthreads();
-    tri_upper_solve(Lkk, LDK, x, nk, nrhs);
+    apply_tile_inverse(Dk, tk_, x, nk, nrhs, true);
     if (jb == kb) {
         for (int idx = tid; idx < nk * nrhs; idx += nt) {
             int q = idx / nk, r = idx - q * nk;
@@ -408,44 +371,54 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 // ---------------------------------------------------------------------------
 
 template <typename TL, typename TV>
-void solve_levels(const DevPlan& D, const TL* Ls, TV* xp, TV* fv, int nrhs, cudaStream_t st) {
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(k_fwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
-        cudaFuncSetAttribute(k_bwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
-        cudaFuncSetAttribute(k_fwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
-        cudaFuncSetAttribute(k_bwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
-        attr_done = true;
-    }
+static void set_solve_attributes() {
+    cudaFuncSetAttribute(k_fwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(k_bwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(k_fwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    cudaFuncSetAttribute(k_bwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+}
+
+void init_solve_kernels() {
+    set_solve_attributes<double, double>();
+    set_solve_attributes<float, double>();
+}
+
+template <typename TL, typename TV>
+void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
+                  cudaStream_t st) {
     const int n = D.n;
     const int msmall = Plan::small_limit[kSmallBuckets - 1];
-    const size_t step_smem = (size_t)(kTile * (kTile + 1) + kTile * nrhs) * sizeof(TV);
+    const size_t step_smem = (size_t)(kTile * kTile + 2 * kTile * nrhs + 8 * kTile) * sizeof(TV);
     const SolveSchedule& S = D.solve;
     for (int l = 0; l < D.nlevels; ++l) {
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
-        if (end > beg)
+        if (end > beg) {
+            ProfScope ps(D.prof, KC_SOLVE_SMALL, st);
             k_fwd_small<TL, TV><<<end - beg, 128, (size_t)msmall * nrhs * sizeof(TV), st>>>(
                 D.fronts, D.small_list + beg, D.child, D.relmap, D.fv_off, Ls, xp, fv, n, nrhs);
+        }
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st);
             k_fwd_assemble<TV><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, D.child,
                                                         D.relmap, D.fv_off, xp, fv, n, nrhs);
             for (int q = S.fwd_beg[l]; q < S.fwd_beg[l + 1]; ++q) {
                 const WorkList& w = S.fwd[q];
                 if (w.nctas == 0) continue;
                 k_fwd_step<TL, TV><<<w.nctas, 256, step_smem, st>>>(
-                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off, Ls,
-                    xp, fv, n, nrhs);
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off,
+                    D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
             }
         }
     }
     for (int l = D.nlevels - 1; l >= 0; --l) {
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st);
             const WorkList& g = S.gather[l];
             if (g.nctas > 0)
                 k_bwd_gather<TL, TV><<<g.nctas, 256, 0, st>>>(D.fronts, S.items + g.off,
@@ -455,23 +428,24 @@ void solve_levels(const DevPlan& D, const TL* Ls, TV* xp, TV* fv, int nrhs, cuda
                 const WorkList& w = S.bwd[q];
                 if (w.nctas == 0) continue;
                 k_bwd_step<TL, TV><<<w.nctas, 256, step_smem, st>>>(
-                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off, Ls,
-                    xp, fv, n, nrhs);
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off,
+                    D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
             }
         }
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
             int umax = msmall;
             size_t smem = (size_t)(umax + msmall) * nrhs * sizeof(TV);
+            ProfScope ps(D.prof, KC_SOLVE_SMALL, st);
             k_bwd_small<TL, TV><<<end - beg, 128, smem, st>>>(D.fronts, D.small_list + beg,
                                                               D.rows, Ls, xp, n, nrhs, umax);
         }
     }
 }
 
-template void solve_levels<double, double>(const DevPlan&, const double*, double*, double*, int,
-                                           cudaStream_t);
-template void solve_levels<float, double>(const DevPlan&, const float*, double*, double*, int,
-                                          cudaStream_t);
+template void solve_levels<double, double>(const DevPlan&, const double*, const double*, double*,
+                                           double*, int, cudaStream_t);
+template void solve_levels<float, double>(const DevPlan&, const float*, const float*, double*,
+                                          double*, int, cudaStream_t);
 
 }  // namespace mdgpu
