@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--side", type=int, default=64)
     ap.add_argument("--impl", default="mdgpu_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling helpers: run only one arm of the step (for ncu launch lists)
+    ap.add_argument("--only", choices=["fp32", "fp64"], default=None)
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -276,6 +279,15 @@ def run_gpu_arm(args):
         barrier()
         return times, extra
 
+    if args.only:
+        fn = step_fp32 if args.only == "fp32" else step_fp64
+        t, _ = timed(fn, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "ms_per_step": statistics.mean(t)}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     sampler = ClockSampler(local)
     sampler.start()
     t32, (berr32, it32) = timed(step_fp32, args.steps, args.warmup)
@@ -291,7 +303,7 @@ def run_gpu_arm(args):
     # end to end through the public API with host buffers
     Axh = np.ascontiguousarray(Ax)
     e2e_t = []
-    for k in range(args.warmup + args.steps):
+    for k in range(0 if args.no_e2e else args.warmup + args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -300,7 +312,7 @@ def run_gpu_arm(args):
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e_t.append(time.perf_counter() - t0)
-    e2e_ms = allmax(1e3 * statistics.mean(e2e_t))
+    e2e_ms = allmax(1e3 * statistics.mean(e2e_t)) if e2e_t else float("nan")
 
     if rank != 0:
         if dist is not None:

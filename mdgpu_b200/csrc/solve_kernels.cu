@@ -253,27 +253,50 @@ __global__ void __launch_bounds__(256)
                  const int* __restrict__ before, int nitems, const int* __restrict__ rows,
                  const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
                  const TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs) {
-    // t[cols of tile jb] = y - L21' x_below, written into the front vector
-    constexpr int T = kTile;
+    // t[cols of tile jb] = y - L21' x_below, written into the front vector.
+    // x_below (the already final solution at the front's update rows) is
+    // gathered into shared memory a chunk of rows at a time, so the L21
+    // column reads stream without waiting on the row-index indirection.
+    constexpr int T = kTile, CH = 2048;
+    __shared__ TV xs[CH];
     const int it = find_item(before, nitems, blockIdx.x);
     const int s = items[it];
     const FrontDesc F = fronts[s];
     const int jb = blockIdx.x - before[it];
     const TileRange tj = tile_range(jb, F.m, F.c, T);
     const int c = F.c, u = F.m - c;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const TL* L = Ls + F.loff;
     const int* rw = rows + F.rows_off + c;
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int l = warp; l < tj.size; l += nw) {
-        const int j = tj.start + l;
-        const TL* col = L + c + (int64_t)j * F.ldl;
-        for (int q = 0; q < nrhs; ++q) {
-            TV acc = TV(0);
-            for (int r = lane; r < u; r += 32) acc += (TV)col[r] * xp[rw[r] + (int64_t)q * n];
+    for (int q = 0; q < nrhs; ++q) {
+        TV acc[T / 8];  // this warp's columns: warp, warp + 8, ...
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) f[j + (int64_t)q * F.m] = xp[F.first_col + j + (int64_t)q * n] - acc;
+        for (int a = 0; a < T / 8; ++a) acc[a] = TV(0);
+        for (int r0 = 0; r0 < u; r0 += CH) {
+            const int nr = min(CH, u - r0);
+            for (int r = tid; r < nr; r += blockDim.x) xs[r] = xp[rw[r0 + r] + (int64_t)q * n];
+            __syncthreads();
+#pragma unroll
+            for (int a = 0; a < T / 8; ++a) {
+                const int l = warp + 8 * a;
+                if (l >= tj.size) break;
+                const TL* col = L + c + r0 + (int64_t)(tj.start + l) * F.ldl;
+                TV sum = TV(0);
+                for (int r = lane; r < nr; r += 32) sum += (TV)col[r] * xs[r];
+                acc[a] += sum;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int a = 0; a < T / 8; ++a) {
+            const int l = warp + 8 * a;
+            if (l >= tj.size) break;
+            TV v = acc[a];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int j = tj.start + l;
+            if (lane == 0) f[j + (int64_t)q * F.m] = xp[F.first_col + j + (int64_t)q * n] - v;
         }
     }
 }
