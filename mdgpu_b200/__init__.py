@@ -181,18 +181,35 @@ class Solver:
             Ax = np.ascontiguousarray(Ax, dtype=np.float64)
             _check(lib().mdgpu_factor(self._h, _ptr(Ax), int(precision), stream), self._h)
 
+    def _device_layout(self, T):
+        """(nrhs, leading dimension) of a column-major float64 CUDA tensor of
+        shape (n,) or (n, k); raises on any other layout."""
+        import torch
+
+        if T.dtype != torch.float64 or not T.is_cuda:
+            raise ValueError("device vectors must be float64 CUDA tensors")
+        if T.dim() == 1:
+            if T.shape[0] != self.n or (self.n > 1 and T.stride(0) != 1):
+                raise ValueError("device vector must be contiguous of length n")
+            return 1, self.n
+        if T.dim() != 2 or T.shape[0] != self.n:
+            raise ValueError("device right-hand sides must have shape (n, k)")
+        if self.n > 1 and T.stride(0) != 1:
+            raise ValueError("device right-hand sides must be column-major (B.T.contiguous().T)")
+        # a single column's stride is arbitrary in torch (size-1 dimension)
+        return T.shape[1], (self.n if T.shape[1] == 1 else T.stride(1))
+
     def solve(self, B, stream=None):
         """B: (n,) or (n, k) float64 numpy array, or CUDA torch tensors.
         Device tensors must be column-major contiguous (use B.T.contiguous().T)."""
         if hasattr(B, "data_ptr"):
             import torch
 
-            nrhs = 1 if B.dim() == 1 else B.shape[1]
-            X = torch.empty_like(B)
-            ld = self.n if B.dim() == 1 else B.stride(1)
-            _check(lib().mdgpu_solve_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X), ld,
-                                            nrhs, stream))
-            return X
+            nrhs, ld = self._device_layout(B)
+            X = torch.empty((nrhs, self.n), dtype=B.dtype, device=B.device).t()
+            _check(lib().mdgpu_solve_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X),
+                                            self.n, nrhs, stream))
+            return X[:, 0] if B.dim() == 1 else X
         B = np.asarray(B, dtype=np.float64)
         one = B.ndim == 1
         Bf = np.asfortranarray(B.reshape(self.n, -1))
@@ -214,11 +231,13 @@ class Solver:
         return (X[:, 0] if one else X), berr, it.value
 
     def refine_device(self, B, X, tol=1e-14, maxit=10, stream=None):
-        nrhs = 1 if B.dim() == 1 else B.shape[1]
-        ld = self.n if B.dim() == 1 else B.stride(1)
+        nrhs, ldb = self._device_layout(B)
+        nx, ldx = self._device_layout(X)
+        if nx != nrhs:
+            raise ValueError("B and X hold different numbers of right-hand sides")
         berr = np.zeros(nrhs)
         it = C.c_int()
-        _check(lib().mdgpu_refine_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X), ld, nrhs,
+        _check(lib().mdgpu_refine_device(self._h, _tensor_ptr(B), ldb, _tensor_ptr(X), ldx, nrhs,
                                          float(tol), int(maxit), _ptr(berr), C.byref(it),
                                          stream))
         return berr, it.value

@@ -482,6 +482,19 @@ int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
     return MDGPU_OK;
 }
 
+// Argument check shared by the solve entry points; names the offending argument.
+int check_solve_args(mdgpu_handle_s* h, const void* B, int ldb, const void* X, int ldx,
+                     int nrhs) {
+    if (!h) return fail(MDGPU_ERR_INVALID, "null handle");
+    if (!B || !X) return fail(MDGPU_ERR_INVALID, "null right-hand side or solution pointer");
+    if (nrhs <= 0) return fail(MDGPU_ERR_INVALID, "nrhs must be positive, got " + std::to_string(nrhs));
+    if (ldb < h->plan.n || ldx < h->plan.n)
+        return fail(MDGPU_ERR_INVALID, "leading dimensions (" + std::to_string(ldb) + ", " +
+                                           std::to_string(ldx) + ") below n = " +
+                                           std::to_string(h->plan.n));
+    return MDGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -644,8 +657,7 @@ int mdgpu_not_spd_column(mdgpu_handle h) { return h ? h->not_spd : -1; }
 
 int mdgpu_solve_device(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
                        void* stream) {
-    if (!h || !dB || !dX || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n)
-        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (int rc = check_solve_args(h, dB, ldb, dX, ldx, nrhs)) return rc;
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
     if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
     return guarded([&] {
@@ -660,8 +672,7 @@ int mdgpu_solve_device(mdgpu_handle h, const double* dB, int ldb, double* dX, in
 
 int mdgpu_solve(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, int nrhs,
                 void* stream) {
-    if (!h || !B || !X || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n)
-        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (int rc = check_solve_args(h, B, ldb, X, ldx, nrhs)) return rc;
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
     if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
     return guarded([&] {
@@ -683,8 +694,8 @@ int mdgpu_solve(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, in
 
 int mdgpu_refine_device(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
                         double tol, int maxit, double* berr, int* iters, void* stream) {
-    if (!h || !dB || !dX || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n || maxit < 0)
-        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (int rc = check_solve_args(h, dB, ldb, dX, ldx, nrhs)) return rc;
+    if (maxit < 0) return fail(MDGPU_ERR_INVALID, "maxit must be >= 0");
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
     if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
     return guarded([&] {
@@ -696,8 +707,8 @@ int mdgpu_refine_device(mdgpu_handle h, const double* dB, int ldb, double* dX, i
 
 int mdgpu_refine(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, int nrhs,
                  double tol, int maxit, double* berr, int* iters, void* stream) {
-    if (!h || !B || !X || nrhs <= 0 || ldb < h->plan.n || ldx < h->plan.n || maxit < 0)
-        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (int rc = check_solve_args(h, B, ldb, X, ldx, nrhs)) return rc;
+    if (maxit < 0) return fail(MDGPU_ERR_INVALID, "maxit must be >= 0");
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
     if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
     return guarded([&] {

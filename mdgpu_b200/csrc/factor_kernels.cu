@@ -228,30 +228,142 @@ __device__ void tile_trtri_smem(T* S, int LDS, int n, T* tmp) {
     }
 }
 
+// Cholesky of a 32 x 32 SPD block held one column per lane in registers
+// (lane j owns column j; rows i >= j are meaningful), in place.  Pivots are
+// broadcast by shuffles: no barriers.  A non-positive pivot is recorded at
+// global column col0 + k.
+template <typename T>
+__device__ __forceinline__ void warp_chol32(T (&a)[32], int lane, int* status, int col0) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        const T piv = __shfl_sync(0xffffffffu, a[k], k);
+        if (lane == 0 && !(piv > T(0))) flag_pivot(status, col0 + k);
+        const T d = sqrt(piv);
+        const T inv = T(1) / d;
+        if (lane == k) {
+            a[k] = d;
+#pragma unroll
+            for (int i = k + 1; i < 32; ++i) a[i] *= inv;
+        }
+        T ljk = T(0);
+#pragma unroll
+        for (int i = k + 1; i < 32; ++i) {
+            const T v = __shfl_sync(0xffffffffu, a[i], k);  // L(i, k)
+            if (lane == i) ljk = v;
+            if (lane > k && i >= lane) a[i] -= v * ljk;
+        }
+    }
+}
+
+// Column `lane` of inv(L) for a 32 x 32 lower-triangular L in shared memory
+// (element (i, l) at L[i + l * ld]), by forward substitution; written to X.
+template <typename T>
+__device__ __forceinline__ void warp_trinv32(const T* L, int ld, T* X, int ldx, int lane) {
+    T x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        T acc = (i == lane) ? T(1) : T(0);
+#pragma unroll
+        for (int l = 0; l < i; ++l)
+            if (l >= lane) acc -= L[i + l * ld] * x[l];
+        x[i] = (i >= lane) ? acc / L[i + i * ld] : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) X[i + lane * ldx] = x[i];
+}
+
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
-// column-major, upper part zero) at Dk.
+// column-major, zero above the diagonal) at Dk.  2 x 2 blocks of 32:
+//   L11 = chol(A11)             warp 0, registers          X11 = inv(L11)
+//   L21 = A21 X11'              all threads
+//   A22 -= L21 L21'             all threads
+//   L22 = chol(A22)             warp 0, registers          X22 = inv(L22)
+//   X21 = -X22 (L21 X11)        all threads
+// A partial tile (n < 64) is padded with the identity.  S, W: 64 x 65 each.
 template <typename T, int TB>
-__device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, int* status) {
-    const int tid = threadIdx.x, nt = blockDim.x;
+__device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
+                                int* status) {
+    static_assert(TB == 64, "2 x 2 blocks of 32");
+    constexpr int LD = TB + 1;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
+    const int col0 = f.first_col + tk.start;
     T* base = Ls + f.loff + tk.start + (int64_t)tk.start * f.ldl;
-    T* tmp = S + TB * (TB + 1);
-    for (int idx = tid; idx < n * n; idx += nt) {
-        int j = idx / n, i = idx - j * n;
-        S[i + j * (TB + 1)] = (i >= j) ? base[i + (int64_t)j * f.ldl] : T(0);
-    }
-    __syncthreads();
-    tile_potrf_smem(S, TB + 1, n, status, f.first_col + tk.start);
-    for (int idx = tid; idx < n * n; idx += nt) {
-        int j = idx / n, i = idx - j * n;
-        if (i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * (TB + 1)];
-    }
-    __syncthreads();
-    tile_trtri_smem(S, TB + 1, n, tmp);
     for (int idx = tid; idx < TB * TB; idx += nt) {
         int j = idx / TB, i = idx - j * TB;
-        Dk[idx] = (i >= j && i < n && j < n) ? S[i + j * (TB + 1)] : T(0);
+        T v = (i == j) ? T(1) : T(0);
+        if (i < n && j < n && i >= j) v = base[i + (int64_t)j * f.ldl];
+        S[i + j * LD] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {  // L11, X11
+        T a[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) a[i] = S[i + lane * LD];
+        warp_chol32(a, lane, status, col0);
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i >= lane) S[i + lane * LD] = a[i];
+        __syncwarp();
+        warp_trinv32(S, LD, W, LD, lane);
+    }
+    __syncthreads();
+    // L21 = A21 X11' into W rows 32..63, columns 0..31
+    for (int idx = tid; idx < 32 * 32; idx += nt) {
+        int c = idx >> 5, r = idx & 31;
+        T acc = T(0);
+#pragma unroll 8
+        for (int l = 0; l <= c; ++l) acc += S[(32 + r) + l * LD] * W[c + l * LD];
+        W[(32 + r) + c * LD] = acc;
+    }
+    __syncthreads();
+    // A22 -= L21 L21' (lower), and L21 into its final place in S
+    for (int idx = tid; idx < 32 * 32; idx += nt) {
+        int c = idx >> 5, r = idx & 31;
+        S[(32 + r) + c * LD] = W[(32 + r) + c * LD];
+        if (r >= c) {
+            T acc = T(0);
+#pragma unroll 8
+            for (int l = 0; l < 32; ++l) acc += W[(32 + r) + l * LD] * W[(32 + c) + l * LD];
+            S[(32 + r) + (32 + c) * LD] -= acc;
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {  // L22, X22
+        T a[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) a[i] = S[(32 + i) + (32 + lane) * LD];
+        warp_chol32(a, lane, status, col0 + 32);
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i >= lane) S[(32 + i) + (32 + lane) * LD] = a[i];
+        __syncwarp();
+        warp_trinv32(S + 32 + 32 * LD, LD, W + 32 + 32 * LD, LD, lane);
+    }
+    __syncthreads();
+    // T1 = L21 X11 into W rows 0..31, columns 32..63
+    for (int idx = tid; idx < 32 * 32; idx += nt) {
+        int c = idx >> 5, r = idx & 31;
+        T acc = T(0);
+#pragma unroll 8
+        for (int l = c; l < 32; ++l) acc += S[(32 + r) + l * LD] * W[l + c * LD];
+        W[r + (32 + c) * LD] = acc;
+    }
+    __syncthreads();
+    // X21 = -X22 T1 into W rows 32..63, columns 0..31
+    for (int idx = tid; idx < 32 * 32; idx += nt) {
+        int c = idx >> 5, r = idx & 31;
+        T acc = T(0);
+#pragma unroll 8
+        for (int l = 0; l <= r; ++l) acc += W[(32 + r) + (32 + l) * LD] * W[l + (32 + c) * LD];
+        W[(32 + r) + c * LD] = -acc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < TB * TB; idx += nt) {
+        int j = idx / TB, i = idx - j * TB;
+        if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * LD];
+        Dk[idx] = (i >= j && i < n && j < n) ? W[i + j * LD] : T(0);
     }
 }
 
@@ -260,11 +372,13 @@ __global__ void __launch_bounds__(256)
     k_tile_potrf(const FrontDesc* __restrict__ fronts, const int* __restrict__ list, int k,
                  const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
                  int* __restrict__ status) {
-    __shared__ T S[TB * (TB + 1) + TB];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* S = reinterpret_cast<T*>(smem_raw);
+    T* W = S + TB * (TB + 1);
     const int s = list[blockIdx.x];
     const FrontDesc f = fronts[s];
     if (k >= tiles_l(f.c, TB)) return;
-    potrf_diag_tile<T, TB>(f, k, Ls, Dinv + dinv_off[s] + (int64_t)k * TB * TB, S, status);
+    potrf_diag_tile<T, TB>(f, k, Ls, Dinv + dinv_off[s] + (int64_t)k * TB * TB, S, W, status);
 }
 
 // C (TB x TB, tile (i, j) of front f) -= A B' with A = rows of tile i and
@@ -398,13 +512,21 @@ __global__ void __launch_bounds__(256)
     // the next diagonal tile is final now: factor it for the next step
     if (i == k + 1 && j == k + 1 && i < tiles_l(f.c, TB) && (jcap < 0 || i <= jcap)) {
         __syncthreads();
-        potrf_diag_tile<T, TB>(f, i, Ls, Dinv + dinv_off[s] + (int64_t)i * TB * TB, As, status);
+        potrf_diag_tile<T, TB>(f, i, Ls, Dinv + dinv_off[s] + (int64_t)i * TB * TB, As,
+                               As + TB * (TB + 1), status);
     }
 }
 
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+
+// shared memory of the tile kernels: two 64 x 65 buffers (operands of the
+// tile products, or S and W of the diagonal-tile factorization)
+template <typename T>
+static size_t diag_smem() {
+    return (size_t)2 * kTile * (kTile + 1) * sizeof(T);
+}
 
 template <typename T>
 void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax,
@@ -441,10 +563,11 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
     }
     {
         ProfScope ps(D.prof, KC_POTRF, st);
-        k_tile_potrf<T, kTile><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, 0,
-                                                        D.dinv_off, Ls, Dinv, status);
+        k_tile_potrf<T, kTile><<<le - lb, 256, diag_smem<T>(), st>>>(D.fronts, D.large_list + lb,
+                                                                     0, D.dinv_off, Ls, Dinv,
+                                                                     status);
     }
-    const size_t gsm = 2 * kTile * kTile * sizeof(T);
+    const size_t gsm = diag_smem<T>();
     for (int q = S.h_level_beg[level]; q < S.h_level_beg[level + 1]; ++q) {
         const WorkList& tr = S.h_trsm[q];
         const WorkList& up = S.h_update[q];
@@ -472,7 +595,7 @@ template <typename T>
 static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv,
                                       const double* Ax, int* status, cudaStream_t st) {
     const DevSchedule& S = D.psched;
-    const size_t gsm = 2 * kTile * kTile * sizeof(T);
+    const size_t gsm = diag_smem<T>();
     for (int q = S.h_op_beg[level]; q < S.h_op_beg[level + 1]; ++q) {
         const PanelOp& op = S.h_ops[q];
         const WorkList& w = op.w;
@@ -488,7 +611,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
             }
             case OP_POTRF: {
                 ProfScope ps(D.prof, KC_POTRF, st);
-                k_tile_potrf<T, kTile><<<w.nitems, 256, 0, st>>>(
+                k_tile_potrf<T, kTile><<<w.nitems, 256, diag_smem<T>(), st>>>(
                     D.fronts, S.items + w.off, op.arg, D.dinv_off, Ls, Dinv, status);
                 break;
             }
@@ -523,9 +646,11 @@ static void set_factor_attributes() {
     cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          227 * 1024);
     cudaFuncSetAttribute(k_tile_update<T, kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         2 * kTile * kTile * sizeof(T));
+                         (int)diag_smem<T>());
     cudaFuncSetAttribute(k_tile_trsm<T, kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         2 * kTile * kTile * sizeof(T));
+                         (int)diag_smem<T>());
+    cudaFuncSetAttribute(k_tile_potrf<T, kTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)diag_smem<T>());
     cudaFuncSetAttribute(k_big_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          227 * 1024);
 }

@@ -15,7 +15,9 @@
 // 3-stage ring of shared-memory buffers.
 //
 // Roles: thread 0 issues the TMA loads and the MMAs (one thread, the MMA
-// instruction is single-issued per CTA); all 128 threads then read the
+// instruction is single-issued per CTA); all 128 threads split each landed
+// stage into TF32 high and low parts (3xTF32: hi*hi + hi*lo + lo*hi, close to
+// FP32 accuracy, which keeps iterative refinement short), then read the
 // accumulator out of TMEM (warp w owns TMEM lanes 32w..32w+31 = tile rows)
 // and subtract it from C in place -- coalesced along the column.
 //
@@ -39,7 +41,9 @@ namespace tc {
 constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3;
 constexpr int BOX = 32;                                   // TMA box: 32 rows x 32 columns (fp32)
 constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes
-constexpr int STAGE_BYTES = STAGE_A + STAGE_B;
+constexpr int STAGE_TMA = STAGE_A + STAGE_B;              // bytes the TMA writes per stage
+// per stage: A_hi, B_hi (TMA destination, split in place), A_lo, B_lo
+constexpr int STAGE_BYTES = 2 * STAGE_TMA;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack
 constexpr uint32_t TMEM_COLS = 128;
 constexpr long long WAIT_LIMIT = 1ll << 22;               // polls (with backoff) before giving up
@@ -199,57 +203,90 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
 
-    if (tid == 0) {
-        auto load_chunk = [&](int c) {
-            const int st = c % STAGES;
-            unsigned char* a = smem + st * STAGE_BYTES;
-            unsigned char* b = a + STAGE_A;
-            tc::mbar_expect_tx(&full_bar[st], STAGE_BYTES);
-            const int col = k0 + c * BK;
+    // Thread 0 issues TMA loads and MMAs.  Every thread takes part in the
+    // split of each landed stage: x = hi + lo with hi the exact TF32 value
+    // (low 13 mantissa bits cleared, written back in place) and lo = x - hi
+    // (exact in FP32).  The three products hi*hi + hi*lo + lo*hi then give
+    // close to FP32 accuracy on the TF32 tensor pipe ("3xTF32").
+    auto load_chunk = [&](int c) {
+        const int st = c % STAGES;
+        unsigned char* a = smem + st * STAGE_BYTES;
+        unsigned char* b = a + STAGE_A;
+        tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
+        const int col = k0 + c * BK;
 #pragma unroll
-            for (int q = 0; q < BM / BOX; ++q) {
-                tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st], I * BM + q * BOX, col);
-                tc::tma_load_2d(b + q * BOX * BK * 4, map, &full_bar[st], J * BN + q * BOX, col);
-            }
-        };
-        int issued = 0, committed = 0;
-        bool ok = true;
+        for (int q = 0; q < BM / BOX; ++q) {
+            tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st], I * BM + q * BOX, col);
+            tc::tma_load_2d(b + q * BOX * BK * 4, map, &full_bar[st], J * BN + q * BOX, col);
+        }
+    };
+    int issued = 0, committed = 0;
+    bool ok = true;
+    if (tid == 0)
         for (; issued < nk && issued < STAGES; ++issued) load_chunk(issued);
-        for (int c = 0; c < nk && ok; ++c) {
-            const int st = c % STAGES;
-            if (!tc::mbar_wait(&full_bar[st], (c / STAGES) & 1)) {
-                ok = false;
-                break;
+    for (int c = 0; c < nk; ++c) {
+        const int st = c % STAGES;
+        if (!tc::mbar_wait(&full_bar[st], (c / STAGES) & 1)) ok = false;
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+        // split the landed stage (same swizzled positions in the lo buffers)
+        {
+            float4* hi = reinterpret_cast<float4*>(smem + st * STAGE_BYTES);
+            float4* lo = reinterpret_cast<float4*>(smem + st * STAGE_BYTES + STAGE_TMA);
+#pragma unroll 4
+            for (int v = tid; v < STAGE_TMA / 16; v += 128) {
+                float4 x = hi[v], h, l;
+                h.x = __uint_as_float(__float_as_uint(x.x) & 0xffffe000u);
+                h.y = __uint_as_float(__float_as_uint(x.y) & 0xffffe000u);
+                h.z = __uint_as_float(__float_as_uint(x.z) & 0xffffe000u);
+                h.w = __uint_as_float(__float_as_uint(x.w) & 0xffffe000u);
+                l.x = x.x - h.x;
+                l.y = x.y - h.y;
+                l.z = x.z - h.z;
+                l.w = x.w - h.w;
+                hi[v] = h;
+                lo[v] = l;
             }
+        }
+        // make the generic-proxy stores visible to the tensor core's reads
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = tc::smem_u32(smem + st * STAGE_BYTES);
-            const uint32_t b0 = a0 + STAGE_A;
+            const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
+            const uint32_t bh = ah + STAGE_A;
+            const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
 #pragma unroll
-            for (int t = 0; t < BK / 8; ++t)
-                tc::mma_tf32(tmem, tc::make_desc(a0 + t * 1024), tc::make_desc(b0 + t * 1024),
+            for (int t = 0; t < BK / 8; ++t) {
+                const uint32_t o = t * 1024;
+                tc::mma_tf32(tmem, tc::make_desc(al + o), tc::make_desc(bh + o),
                              (c > 0 || t > 0) ? 1u : 0u);
+                tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
+                tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
+            }
             tc::mma_commit(&empty_bar[st]);
             committed = c + 1;
             // refill the stage of the previous chunk once its MMAs are done
             if (c >= 1 && issued < nk) {
                 const int pc = c - 1, pst = pc % STAGES;
-                if (!tc::mbar_wait(&empty_bar[pst], (pc / STAGES) & 1)) {
+                if (!tc::mbar_wait(&empty_bar[pst], (pc / STAGES) & 1))
                     ok = false;
-                    break;
-                }
-                load_chunk(issued++);
+                else
+                    load_chunk(issued++);
             }
         }
+    }
+    if (tid == 0) {
         if (ok) {
             tc::mma_commit(&done_bar);
         } else {
             atomicExch(err, 1);
             abort_sh = 1;
-            // drain: wait (bounded) for the loads and MMAs already issued
+            // drain: wait (bounded) for the loads already issued
             for (int c = 0; c < issued; ++c) tc::mbar_wait(&full_bar[c % STAGES], (c / STAGES) & 1);
-            if (committed > 0) {
-                tc::mma_commit(&done_bar);
-            }
+            if (committed > 0) tc::mma_commit(&done_bar);
         }
     }
     __syncthreads();
