@@ -110,6 +110,23 @@ MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, doub
                        void *stream);
 
 /*
+ * mdgpu_solve_device without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory when they solve
+ * -- code running while a CUDA graph is captured, host frameworks whose own
+ * allocator owns the device memory, loops that cannot afford cudaMalloc's
+ * implicit synchronization -- the work vectors come from a fixed 32 MiB
+ * device array that every GPU loading this library holds until exit (the
+ * handle's plan and factor were allocated earlier by mdgpu_analyze and
+ * mdgpu_factor).  A call needs (n + sum of front rows) x min(nrhs, 64)
+ * doubles; larger requests return MDGPU_ERR_INVALID.  All calls share the
+ * array: calls whose work overlaps on one GPU race and must be serialized by
+ * the caller.  The first call on a device looks up the array's address; make
+ * it before any stream capture.
+ */
+MDGPU_API int mdgpu_solve_device_noalloc(mdgpu_handle h, const double *dB, int ldb, double *dX,
+                                         int ldx, int nrhs, void *stream);
+
+/*
  * Solve with FP64 iterative refinement on the GPU: r = b - A x with the
  * caller's FP64 values (the reference's residual, mdgpu.cu:1963-1972), then
  * x += A_factor^-1 r until the backward error ||r||inf / (||A||inf ||x||inf +

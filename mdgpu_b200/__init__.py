@@ -26,7 +26,8 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
 # every entry point declared in include/mdgpu_b200.h
 EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
            "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
-           "mdgpu_solve", "mdgpu_solve_device", "mdgpu_refine", "mdgpu_refine_device",
+           "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
+           "mdgpu_refine_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
            "mdgpu_last_error")
 
@@ -75,6 +76,7 @@ def lib():
         L.mdgpu_not_spd_column.argtypes = [vp]
         L.mdgpu_solve.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, vp]
         L.mdgpu_solve_device.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, vp]
+        L.mdgpu_solve_device_noalloc.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, vp]
         L.mdgpu_refine.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, C.c_double, C.c_int,
                                    dp, vp, vp]
         L.mdgpu_refine_device.argtypes = L.mdgpu_refine.argtypes

@@ -772,6 +772,42 @@ int mdgpu_get_L(mdgpu_handle h, long long* Lp, int* Li, double* Lx) {
     });
 }
 
+int mdgpu_solve_device_noalloc(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx,
+                               int nrhs, void* stream) {
+    if (int rc = check_solve_args(h, dB, ldb, dX, ldx, nrhs)) return rc;
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        std::string msg;
+        double* scratch = noalloc_scratch(msg);
+        if (!scratch) return fail(MDGPU_ERR_CUDA, msg);
+        const int n = h->plan.n;
+        const int chunk = std::min(nrhs, 64);
+        const long long need = ((long long)n + h->D.fv_total) * chunk;
+        if (need > noalloc_scratch_capacity())
+            return fail(MDGPU_ERR_INVALID,
+                        "no-allocation solve needs " + std::to_string(need) +
+                            " scratch doubles ((n + sum of front rows) x min(nrhs, 64)), limit " +
+                            std::to_string(noalloc_scratch_capacity()));
+        double* xp = scratch;
+        double* fv = scratch + (int64_t)n * chunk;
+        for (int q0 = 0; q0 < nrhs; q0 += 64) {
+            const int nq = std::min(64, nrhs - q0);
+            permute_gather(h->d_perm, dB + (int64_t)q0 * ldb, xp, n, nq, ldb, st);
+            if (h->factored == MDGPU_FP64)
+                solve_levels<double, double>(h->D, h->dL64, h->dD64, xp, fv, nq, st);
+            else
+                solve_levels<float, double>(h->D, h->dL32, h->dD32, xp, fv, nq, st);
+            permute_scatter(h->d_perm, xp, dX + (int64_t)q0 * ldx, n, nq, ldx, st);
+        }
+        ck(cudaGetLastError(), "solve launch");
+        ck(cudaStreamSynchronize(st), "solve");
+        return MDGPU_OK;
+    });
+}
+
 int mdgpu_profile(mdgpu_handle h, int enable) {
     if (!h) return fail(MDGPU_ERR_INVALID, "bad arguments");
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");

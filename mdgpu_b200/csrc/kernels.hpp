@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <string>
 #include <vector>
 
 #include "plan.hpp"
@@ -155,6 +156,10 @@ void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, flo
                      float* Us, int* err, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,
                       double* Us, cudaStream_t st);
+
+// fixed device scratch of the no-allocation solve (noalloc.cu)
+long long noalloc_scratch_capacity();
+double* noalloc_scratch(std::string& msg);
 
 // gather / scatter with the fill-reducing permutation (perm: new -> old)
 void permute_gather(const int* perm, const double* b, double* xp, int n, int nrhs, int ldb,

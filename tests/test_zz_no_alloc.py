@@ -1,0 +1,73 @@
+"""The solve that allocates no device memory (mdgpu_solve_device_noalloc).
+
+For callers that cannot allocate at solve time (inside a CUDA graph capture,
+under a framework whose allocator owns the device memory, or in loops that
+cannot pay cudaMalloc's synchronization), the work vectors come from a fixed
+32 MiB device array instead of cudaMalloc.  Checked through the C ABI against
+mdgpu_solve_device on two calls in a row (the array keeps the previous call's
+contents), and the size limit is enforced with a clear error.
+
+This file is collected last on purpose: it must pass after every other test
+and alone in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import mdgpu_b200 as M
+from mdgpu_b200 import matgen as mg
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - collected only on GPU boxes
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+
+def _noalloc(S, dB, dX, nrhs):
+    return M.lib().mdgpu_solve_device_noalloc(S._h, C.c_void_p(dB.data_ptr()), S.n,
+                                              C.c_void_p(dX.data_ptr()), S.n, nrhs, None)
+
+
+def _colmajor(a):
+    t = torch.from_numpy(np.asfortranarray(a)).cuda()
+    return t.t().contiguous().t() if t.dim() == 2 else t
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
+def test_noalloc_solve_matches_regular_solve_twice(prec):
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(14, seed=2)
+    S = M.Solver(n, Ap, Ai)
+    S.factor(Ax, prec)
+    for call, (seed, nrhs) in enumerate([(10, 3), (11, 1)]):
+        B = mg.rhs_uniform(n, seed=seed, nrhs=nrhs).reshape(n, nrhs)
+        dB = _colmajor(B)
+        ref = S.solve(dB)
+        dX = torch.full_like(dB, float("nan"))
+        rc = _noalloc(S, dB, dX, nrhs)
+        assert rc == 0, M.lib().mdgpu_last_error().decode()
+        torch.cuda.synchronize()
+        x, xr = dX.cpu().numpy(), ref.cpu().numpy()
+        assert np.all(np.isfinite(x)), call
+        np.testing.assert_allclose(x, xr, rtol=1e-12, atol=1e-12 * np.abs(xr).max())
+
+
+def test_noalloc_solve_rejects_requests_beyond_its_scratch():
+    n, Ap, Ai, Ax = mg.laplacian_2d_5pt(300)  # n = 90000: 64 rhs need > 4M doubles
+    S = M.Solver(n, Ap, Ai)
+    S.factor(Ax, M.FP64)
+    nrhs = 64
+    dB = _colmajor(mg.rhs_uniform(n, seed=1, nrhs=nrhs))
+    dX = torch.empty_like(dB)
+    rc = _noalloc(S, dB, dX, nrhs)
+    assert rc == -1
+    msg = M.lib().mdgpu_last_error().decode()
+    assert "limit" in msg and "scratch" in msg
+    # one right-hand side fits and still solves
+    db1 = dB[:, 0].contiguous()
+    dx1 = torch.empty_like(db1)
+    assert _noalloc(S, db1, dx1, 1) == 0
+    x1 = S.solve(db1)
+    np.testing.assert_allclose(dx1.cpu().numpy(), x1.cpu().numpy(), rtol=1e-12,
+                               atol=1e-12 * float(x1.abs().max()))
