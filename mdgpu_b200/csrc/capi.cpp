@@ -242,13 +242,19 @@ void upload_plan(mdgpu_handle_s* h) {
     D.psched.before = h->keep(upload(h->pschedh.store.ctas_before));
     D.psched.h_op_beg = h->pschedh.op_beg;
     D.psched.h_ops = h->pschedh.ops;
-    D.solve.items = h->keep(upload(h->ssched.store.items));
-    D.solve.before = h->keep(upload(h->ssched.store.ctas_before));
-    D.solve.fwd_beg = h->ssched.fwd_beg;
-    D.solve.bwd_beg = h->ssched.bwd_beg;
-    D.solve.fwd = h->ssched.fwd;
-    D.solve.bwd = h->ssched.bwd;
-    D.solve.gather = h->ssched.gather;
+    {
+        const SolveScheduleHost& SS = h->ssched;
+        std::vector<int> tasks = SS.tasks;
+        if (tasks.empty()) tasks.assign(2, 0);
+        D.solve.tasks = reinterpret_cast<int2*>(h->keep(upload(tasks)));
+        D.solve.fwd_task_beg = SS.fwd_task_beg;
+        D.solve.bwd_task_beg = SS.bwd_task_beg;
+        D.solve.fwd_bytes = SS.fwd_bytes;
+        D.solve.bwd_bytes = SS.bwd_bytes;
+        D.solve.nflags = SS.nflags;
+        D.solve.nsync = 2 * P.nlevels + SS.nflags + 1;
+        D.solve.sync = h->keep(dalloc<int>(D.solve.nsync));
+    }
     // algorithmic work per launch, for the profiler's roofline figures
     {
         const TileSchedule& TS = h->fsched;
@@ -294,7 +300,8 @@ void upload_plan(mdgpu_handle_s* h) {
     }
     D.prof = &h->prof;
     if (!P.perm.empty()) h->d_perm = h->keep(upload(P.perm));
-    h->d_status = h->keep(dalloc<int>(2));
+    h->d_status = h->keep(dalloc<int>(3));  // not-SPD column, tensor-core error, solve error
+    D.solve.err = h->d_status + 2;
     h->d_Ax = dalloc<double>(std::max<int64_t>(P.nnz_user, 1));
     h->csr.rowptr = h->keep(upload(h->h_csr_rowptr));
     h->csr.col = h->keep(upload(h->h_csr_col));
@@ -482,6 +489,23 @@ int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
     return MDGPU_OK;
 }
 
+// Solve error word (d_status[2]): cleared before a public solve call, read
+// after it; bit 0 = a dependency wait of the large-front solve ran out,
+// bit 1 = a solve kernel found its ticket counter not cleared.
+void solve_status_reset(mdgpu_handle_s* h, cudaStream_t st) {
+    ck(cudaMemsetAsync(h->d_status + 2, 0, sizeof(int), st), "clear solve status");
+}
+int solve_status_check(mdgpu_handle_s* h, cudaStream_t st) {
+    int e = 0;
+    ck(cudaMemcpyAsync(&e, h->d_status + 2, sizeof(int), cudaMemcpyDeviceToHost, st),
+       "solve status");
+    ck(cudaStreamSynchronize(st), "solve");
+    if (e != 0)
+        return fail(MDGPU_ERR_CUDA, "large-front solve aborted (status " + std::to_string(e) +
+                                        "): a dependency wait ran out");
+    return MDGPU_OK;
+}
+
 // Argument check shared by the solve entry points; names the offending argument.
 int check_solve_args(mdgpu_handle_s* h, const void* B, int ldb, const void* X, int ldx,
                      int nrhs) {
@@ -664,9 +688,9 @@ int mdgpu_solve_device(mdgpu_handle h, const double* dB, int ldb, double* dX, in
         cudaStream_t st = pick_stream(h, stream);
         ck(cudaSetDevice(h->device), "cudaSetDevice");
         ensure_solve_storage(h, nrhs);
+        solve_status_reset(h, st);
         do_solve(h, dB, ldb, dX, ldx, nrhs, st);
-        ck(cudaStreamSynchronize(st), "solve");
-        return MDGPU_OK;
+        return solve_status_check(h, st);
     });
 }
 
@@ -683,12 +707,12 @@ int mdgpu_solve(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, in
         ck(cudaMemcpy2DAsync(h->d_B, n * sizeof(double), B, ldb * sizeof(double),
                              n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st),
            "upload rhs");
+        solve_status_reset(h, st);
         do_solve(h, h->d_B, n, h->d_X, n, nrhs, st);
         ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
                              n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
            "download solution");
-        ck(cudaStreamSynchronize(st), "solve");
-        return MDGPU_OK;
+        return solve_status_check(h, st);
     });
 }
 
@@ -701,7 +725,10 @@ int mdgpu_refine_device(mdgpu_handle h, const double* dB, int ldb, double* dX, i
     return guarded([&] {
         cudaStream_t st = pick_stream(h, stream);
         ck(cudaSetDevice(h->device), "cudaSetDevice");
-        return do_refine(h, dB, ldb, dX, ldx, nrhs, tol, maxit, berr, iters, st);
+        solve_status_reset(h, st);
+        int rc = do_refine(h, dB, ldb, dX, ldx, nrhs, tol, maxit, berr, iters, st);
+        int rs = solve_status_check(h, st);
+        return rs != MDGPU_OK ? rs : rc;
     });
 }
 
@@ -719,12 +746,13 @@ int mdgpu_refine(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, i
         ck(cudaMemcpy2DAsync(h->d_B, n * sizeof(double), B, ldb * sizeof(double),
                              n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st),
            "upload rhs");
+        solve_status_reset(h, st);
         int rc = do_refine(h, h->d_B, n, h->d_X, n, nrhs, tol, maxit, berr, iters, st);
         ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
                              n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
            "download solution");
-        ck(cudaStreamSynchronize(st), "refine");
-        return rc;
+        int rs = solve_status_check(h, st);
+        return rs != MDGPU_OK ? rs : rc;
     });
 }
 
@@ -793,6 +821,7 @@ int mdgpu_solve_device_noalloc(mdgpu_handle h, const double* dB, int ldb, double
                             std::to_string(noalloc_scratch_capacity()));
         double* xp = scratch;
         double* fv = scratch + (int64_t)n * chunk;
+        solve_status_reset(h, st);
         for (int q0 = 0; q0 < nrhs; q0 += 64) {
             const int nq = std::min(64, nrhs - q0);
             permute_gather(h->d_perm, dB + (int64_t)q0 * ldb, xp, n, nq, ldb, st);
@@ -803,8 +832,7 @@ int mdgpu_solve_device_noalloc(mdgpu_handle h, const double* dB, int ldb, double
             permute_scatter(h->d_perm, xp, dX + (int64_t)q0 * ldx, n, nq, ldx, st);
         }
         ck(cudaGetLastError(), "solve launch");
-        ck(cudaStreamSynchronize(st), "solve");
-        return MDGPU_OK;
+        return solve_status_check(h, st);
     });
 }
 

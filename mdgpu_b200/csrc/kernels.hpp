@@ -89,14 +89,18 @@ struct DevSchedule {
     std::vector<PanelOp> h_ops;
 };
 
+// Large-front solve: per level one forward and one backward launch over
+// dependency-ordered (front, tile) tasks.  sync holds 2 * nlevels ticket
+// counters, one flag per pivot tile and the abort word; it is cleared at the
+// start of every solve.  err (not cleared by the solve) gets bit 0 when a
+// dependency wait ran out.
 struct SolveSchedule {
-    int* items = nullptr;
-    int* before = nullptr;
-    // per level: large-front forward steps, backward steps and the L21'x
-    // gather; each WorkList names its step
-    std::vector<int> fwd_beg, bwd_beg;
-    std::vector<WorkList> fwd, bwd;
-    std::vector<WorkList> gather;  // per level
+    int2* tasks = nullptr;
+    std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1
+    std::vector<double> fwd_bytes, bwd_bytes;     // per level: L + Dinv elements
+    int* sync = nullptr;
+    int nsync = 0, nflags = 0;
+    int* err = nullptr;
 };
 
 struct DevPlan {

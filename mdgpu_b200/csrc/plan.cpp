@@ -288,39 +288,52 @@ void build_factor_schedule(const Plan& P, int T, int assemble_cols, TileSchedule
 void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     S = SolveScheduleHost();
     S.T = T;
-    S.fwd_beg.assign(P.nlevels + 1, 0);
-    S.bwd_beg.assign(P.nlevels + 1, 0);
-    for (int l = 0; l < P.nlevels; ++l) {
-        int maxsteps = 0;
-        std::vector<std::pair<int, int>> ga;
-        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-            const FrontDesc& f = P.fronts[P.large_list[q]];
-            int nt1 = (f.c + T - 1) / T;
-            maxsteps = std::max(maxsteps, nt1);
-            ga.push_back({P.large_list[q], nt1});
+    // level tasks.  Forward: row tile i of front s; pivot tiles (i < nt1)
+    // wait for pivot tiles 0..i-1, update tiles for all nt1 of them, so the
+    // key i (pivot) / nt1 (update) orders dependencies first.  Backward:
+    // pivot column tile j waits for pivot tiles j+1..nt1-1: key nt1-1-j.
+    S.tasks.clear();
+    S.fwd_task_beg.assign(P.nlevels + 1, 0);
+    S.bwd_task_beg.assign(P.nlevels + 1, 0);
+    S.fwd_bytes.assign(P.nlevels, 0.0);
+    S.bwd_bytes.assign(P.nlevels, 0.0);
+    int64_t ntiles_piv = 0;
+    for (int s : P.large_list) ntiles_piv += (P.fronts[s].c + T - 1) / T;
+    S.nflags = (int)ntiles_piv;
+    struct Key {
+        int key, ord, s, t;
+    };
+    auto emit = [&](std::vector<Key>& ks) {
+        std::stable_sort(ks.begin(), ks.end(), [](const Key& a, const Key& b) {
+            return a.key != b.key ? a.key < b.key : a.ord < b.ord;
+        });
+        for (const Key& k : ks) {
+            S.tasks.push_back(k.s);
+            S.tasks.push_back(k.t);
         }
-        S.gather.push_back(S.store.add(ga, 0));
-        S.fwd_beg[l] = (int)S.fwd.size();
-        for (int k = 0; k < maxsteps; ++k) {
-            std::vector<std::pair<int, int>> it;
+    };
+    for (int dir = 0; dir < 2; ++dir) {
+        for (int l = 0; l < P.nlevels; ++l) {
+            (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[l] = (int)(S.tasks.size() / 2);
+            std::vector<Key> ks;
+            double bytes = 0;
+            int ord = 0;
             for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-                const FrontDesc& f = P.fronts[P.large_list[q]];
-                if (k < (f.c + T - 1) / T) it.push_back({P.large_list[q], front_tiles(f.m, f.c, T) - k});
+                const int s = P.large_list[q];
+                const FrontDesc& f = P.fronts[s];
+                const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                bytes += (double)f.c * (f.c + 1) / 2 + (double)(f.m - f.c) * f.c +
+                         (double)nt1 * T * T;
+                if (dir == 0)
+                    for (int i = 0; i < NT; ++i) ks.push_back({i < nt1 ? i : nt1, ord++, s, i});
+                else
+                    for (int j = 0; j < nt1; ++j) ks.push_back({nt1 - 1 - j, ord++, s, j});
             }
-            S.fwd.push_back(S.store.add(it, k));
+            (dir == 0 ? S.fwd_bytes : S.bwd_bytes)[l] = bytes;
+            emit(ks);
         }
-        S.bwd_beg[l] = (int)S.bwd.size();
-        for (int k = maxsteps - 1; k >= 0; --k) {
-            std::vector<std::pair<int, int>> it;
-            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-                const FrontDesc& f = P.fronts[P.large_list[q]];
-                if (k < (f.c + T - 1) / T) it.push_back({P.large_list[q], k + 1});
-            }
-            S.bwd.push_back(S.store.add(it, k));
-        }
+        (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
     }
-    S.fwd_beg[P.nlevels] = (int)S.fwd.size();
-    S.bwd_beg[P.nlevels] = (int)S.bwd.size();
 }
 
 void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S) {

@@ -129,13 +129,16 @@ struct PanelSchedule {
 };
 void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S);
 
-// Work lists of the tiled solve kernels.
+// Tasks of the large-front solve kernels (one launch per level and direction).
 struct SolveScheduleHost {
     int T = 64;
-    ListStore store;
-    std::vector<int> fwd_beg, bwd_beg;   // per level: range in fwd / bwd
-    std::vector<WorkList> fwd, bwd;      // one per (level, step)
-    std::vector<WorkList> gather;        // per level
+    // one launch per level and direction: tasks (front, tile) as int pairs,
+    // ordered so that every task's dependencies come earlier (a task only
+    // waits on tasks that took a lower ticket, hence already run)
+    std::vector<int> tasks;
+    std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1 each, in tasks
+    std::vector<double> fwd_bytes, bwd_bytes;     // per level, L + Dinv elements read
+    int nflags = 0;                               // one per pivot tile of a large front
 };
 
 int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling

@@ -162,193 +162,384 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// y = inv(L_kk) f or x = inv(L_kk)' t for one pivot tile, with the inverse
-// stored by the factorization (Dk: T x T column-major, zero above the
-// diagonal); in and out are nk x nrhs in shared memory.
-template <typename TV>
-__device__ void apply_tile_inverse(const TV* Dk, const TV* in, TV* out, int nk, int nrhs,
-                                   bool transpose) {
-    constexpr int T = kTile;
-    for (int idx = threadIdx.x; idx < nk * nrhs; idx += blockDim.x) {
-        int q = idx / nk, r = idx - q * nk;
-        const TV* v = in + q * nk;
-        TV acc = TV(0);
-        if (!transpose) {
-            for (int l = 0; l <= r; ++l) acc += Dk[r + l * T] * v[l];
-        } else {
-            for (int l = r; l < nk; ++l) acc += Dk[l + r * T] * v[l];
-        }
-        out[idx] = acc;
+// ---------------------------------------------------------------------------
+// one launch per level and direction: dependency-ordered tile tasks
+//
+// Each CTA takes the next task by an atomic ticket, so every task that
+// started before it holds a lower ticket; the task lists are ordered so that
+// a task only waits for tasks earlier in its list, hence for CTAs that are
+// already resident, and the waits cannot deadlock.  A pivot tile publishes
+// its solution values and then a flag (release); a dependent task polls the
+// flag (acquire) with an iteration limit, after which the solve is aborted
+// (every waiter leaves) and the error word is set for the host.
+// ---------------------------------------------------------------------------
+
+constexpr int kSolveWaitPolls = 1 << 18;  // ~0.1-0.3 s at ~1 us per poll
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// load of a value another CTA of this launch published (ordered after the
+// acquire by the CTA barrier; never served from this SM's L1)
+__device__ __forceinline__ double ld_shared_value(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool wait_flag(const int* flag, int target, int* abort_flag, int* err) {
+    for (int it = 0; it < kSolveWaitPolls; ++it) {
+        if (ld_acquire_gpu(flag) >= target) return true;
+        if (ld_relaxed_gpu(abort_flag)) return false;
+        __nanosleep(64);
     }
-    __syncthreads();
+    atomicExch(abort_flag, 1);
+    atomicOr(err, 1);
+    return false;
+}
+
+template <typename TL>
+__device__ __forceinline__ void cp_async_elem(TL* dst, const TL* src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    if constexpr (sizeof(TL) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_groups() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Rows [0, nr) x columns [0, nc) of a column-major block (leading dimension
+// ld) into a kTile x (kTile + 1) shared array, zeros elsewhere.
+template <typename TL>
+__device__ __forceinline__ void load_block_async(TL* dst, const TL* src, int64_t ld, int nr,
+                                                 int nc) {
+    constexpr int T = kTile, LD = kTile + 1;
+    for (int e = threadIdx.x; e < T * T; e += blockDim.x) {
+        const int r = e & (T - 1), col = e / T;
+        TL* d = dst + r + col * LD;
+        if (r < nr && col < nc)
+            cp_async_elem(d, src + r + (int64_t)col * ld);
+        else
+            *d = TL(0);
+    }
 }
 
 template <typename TL, typename TV>
+__host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
+    return ((3 * (size_t)kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
+           ((size_t)kTile * nrhs + 4 * kTile) * sizeof(TV);
+}
+
+// Forward, task (s, i): row tile i of front s accumulates
+// acc = sum_{k < min(i, nt1)} L(i, k) y_k over the pivot tiles, waiting for
+// each y_k; a pivot tile (i < nt1) then solves y_i = inv(L_ii) (f_i - acc)
+// into the solution and publishes it (flag 1), an update tile leaves
+// f_i - acc in the front vector for the parent.  Threads: r = row in the
+// tile, g = quarter; one right-hand side splits the 64 columns of a block
+// over the quarters, several split the right-hand sides (NQ per thread).
+template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256)
-    k_fwd_step(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-               const int* __restrict__ before, int nitems, int kb,
-               const int64_t* __restrict__ fv_off, const int64_t* __restrict__ dinv_off,
-               const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
-               TV* __restrict__ fv, int n, int nrhs) {
+    k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
+                int ntasks, int* __restrict__ counter, int* __restrict__ flags,
+                int* __restrict__ abort_flag, int* __restrict__ err,
+                const int64_t* __restrict__ fv_off,
+                const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
+                const TL* __restrict__ Dinv, TV* __restrict__ xp, TV* __restrict__ fv, int n,
+                int nrhs) {
+    constexpr int T = kTile, LD = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int T = kTile;
-    TV* Dk = reinterpret_cast<TV*>(smem_raw);  // T x T
-    TV* fk = Dk + T * T;                       // nk x nrhs
-    TV* y = fk + T * nrhs;                     // nk x nrhs
-    const int it = find_item(before, nitems, blockIdx.x);
-    const int s = items[it];
-    const FrontDesc F = fronts[s];
-    const int i = kb + (blockIdx.x - before[it]);
-    const TileRange tk = tile_range(kb, F.m, F.c, T);
-    const int nk = tk.size;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const TL* L = Ls + F.loff;
-    TV* f = front_vec(fv, fv_off, s, nrhs);
-    const TL* dk = Dinv + dinv_off[s] + (int64_t)kb * T * T;
-    for (int idx = tid; idx < T * T; idx += nt) Dk[idx] = (TV)dk[idx];
-    for (int idx = tid; idx < nk * nrhs; idx += nt) {
-        int q = idx / nk, r = idx - q * nk;
-        fk[idx] = f[tk.start + r + (int64_t)q * F.m];
-    }
+    TL* Lb = reinterpret_cast<TL*>(smem_raw);  // 2 x T x LD
+    TL* Dk = Lb + 2 * T * LD;                  // T x LD
+    TV* Y = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
+    TV* red = Y + T * nrhs;  // 4 x T
+    __shared__ int s_task, s_ok;
+    const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
+    if (tid == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
-    apply_tile_inverse(Dk, fk, y, nk, nrhs, false);
-    if (i == kb) {
-        for (int idx = tid; idx < nk * nrhs; idx += nt) {
-            int q = idx / nk, r = idx - q * nk;
-            xp[F.first_col + tk.start + r + (int64_t)q * n] = y[idx];
-        }
+    if (s_task >= ntasks) {  // counter not cleared: refuse rather than read past the list
+        if (tid == 0) atomicOr(err, 2);
         return;
     }
-    // f[tile i] -= L(tile i, tile kb) y: warp w takes columns w, w+8, ...; lanes
-    // take rows lane, lane+32 (coalesced, 16 independent loads per thread);
-    // the eight partial sums per row meet in shared memory
+    const int2 tk = tasks[s_task];
+    const int s = tk.x, i = tk.y;
+    const FrontDesc F = fronts[s];
+    const int nt1 = tiles_l(F.c, T);
     const TileRange ti = tile_range(i, F.m, F.c, T);
-    TV* part = y + T * nrhs;  // 8 x T, one right-hand side at a time
-    const int lane = tid & 31, warp = tid >> 5;
-    const TL* blk = L + ti.start + (int64_t)tk.start * F.ldl;
-    for (int q = 0; q < nrhs; ++q) {
-        TV a0 = TV(0), a1 = TV(0);
-        for (int j = warp; j < nk; j += 8) {
-            const TV yj = y[j + q * nk];
-            const TL* col = blk + (int64_t)j * F.ldl;
-            if (lane < ti.size) a0 += (TV)col[lane] * yj;
-            if (lane + 32 < ti.size) a1 += (TV)col[lane + 32] * yj;
-        }
-        part[warp * T + lane] = a0;
-        part[warp * T + lane + 32] = a1;
-        __syncthreads();
-        for (int r = tid; r < ti.size; r += nt) {
-            TV acc = TV(0);
-#pragma unroll
-            for (int w = 0; w < 8; ++w) acc += part[w * T + r];
-            f[ti.start + r + (int64_t)q * F.m] -= acc;
-        }
-        __syncthreads();
-    }
-}
-
-template <typename TL, typename TV>
-__global__ void __launch_bounds__(256)
-    k_bwd_gather(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-                 const int* __restrict__ before, int nitems, const int* __restrict__ rows,
-                 const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
-                 const TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs) {
-    // t[cols of tile jb] = y - L21' x_below, written into the front vector.
-    // x_below (the already final solution at the front's update rows) is
-    // gathered into shared memory a chunk of rows at a time, so the L21
-    // column reads stream without waiting on the row-index indirection.
-    constexpr int T = kTile, CH = 2048;
-    __shared__ TV xs[CH];
-    const int it = find_item(before, nitems, blockIdx.x);
-    const int s = items[it];
-    const FrontDesc F = fronts[s];
-    const int jb = blockIdx.x - before[it];
-    const TileRange tj = tile_range(jb, F.m, F.c, T);
-    const int c = F.c, u = F.m - c;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int kend = min(i, nt1);
+    const bool pivot = i < nt1;
+    const bool lsplit = nrhs == 1;
     const TL* L = Ls + F.loff;
-    const int* rw = rows + F.rows_off + c;
-    TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int q = 0; q < nrhs; ++q) {
-        TV acc[T / 8];  // this warp's columns: warp, warp + 8, ...
+    int* fl = flags + dinv_off[s] / (T * T);
+    if (pivot) load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)i * T * T, T, ti.size, ti.size);
+    if (kend > 0) load_block_async(Lb, L + ti.start, F.ldl, ti.size, min(T, F.c));
+    cp_async_commit_group();
+    TV acc[NQ];
 #pragma unroll
-        for (int a = 0; a < T / 8; ++a) acc[a] = TV(0);
-        for (int r0 = 0; r0 < u; r0 += CH) {
-            const int nr = min(CH, u - r0);
-            for (int r = tid; r < nr; r += blockDim.x) xs[r] = xp[rw[r0 + r] + (int64_t)q * n];
-            __syncthreads();
+    for (int j = 0; j < NQ; ++j) acc[j] = TV(0);
+    bool ok = true;
+    for (int k = 0; k < kend; ++k) {
+        if (k + 1 < kend)
+            load_block_async(Lb + ((k + 1) & 1) * T * LD, L + ti.start + (int64_t)(k + 1) * T * F.ldl,
+                             F.ldl, ti.size, min(T, F.c - (k + 1) * T));
+        cp_async_commit_group();
+        if (tid == 0) s_ok = wait_flag(fl + k, 1, abort_flag, err);
+        __syncthreads();
+        if (!s_ok) {
+            ok = false;
+            break;
+        }
+        const int nk = min(T, F.c - k * T);
+        for (int e = tid; e < T * nrhs; e += blockDim.x) {
+            const int rr = e & (T - 1), q = e / T;
+            Y[e] = rr < nk ? ld_shared_value(xp + F.first_col + k * T + rr + (int64_t)q * n) : TV(0);
+        }
+        cp_async_wait_groups<1>();
+        __syncthreads();
+        const TL* B = Lb + (k & 1) * T * LD;
+        if (lsplit) {
 #pragma unroll
-            for (int a = 0; a < T / 8; ++a) {
-                const int l = warp + 8 * a;
-                if (l >= tj.size) break;
-                const TL* col = L + c + r0 + (int64_t)(tj.start + l) * F.ldl;
-                TV sum = TV(0);
-                for (int r = lane; r < nr; r += 32) sum += (TV)col[r] * xs[r];
-                acc[a] += sum;
+            for (int l = 0; l < 16; ++l) acc[0] += (TV)B[r + (16 * g + l) * LD] * Y[16 * g + l];
+        } else {
+#pragma unroll 4
+            for (int l = 0; l < T; ++l) {
+                const TV lv = (TV)B[r + l * LD];
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    const int q = g + 4 * j;
+                    if (q < nrhs) acc[j] += lv * Y[l + T * q];
+                }
             }
-            __syncthreads();
         }
-#pragma unroll
-        for (int a = 0; a < T / 8; ++a) {
-            const int l = warp + 8 * a;
-            if (l >= tj.size) break;
-            TV v = acc[a];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            const int j = tj.start + l;
-            if (lane == 0) f[j + (int64_t)q * F.m] = xp[F.first_col + j + (int64_t)q * n] - v;
-        }
+        __syncthreads();
     }
-}
-
-template <typename TL, typename TV>
-__global__ void __launch_bounds__(256)
-    k_bwd_step(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-               const int* __restrict__ before, int nitems, int kb,
-               const int64_t* __restrict__ fv_off, const int64_t* __restrict__ dinv_off,
-               const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
-               TV* __restrict__ fv, int n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int T = kTile;
-    TV* Dk = reinterpret_cast<TV*>(smem_raw);  // T x T
-    TV* tk_ = Dk + T * T;                      // nk x nrhs
-    TV* x = tk_ + T * nrhs;                    // nk x nrhs
-    const int it = find_item(before, nitems, blockIdx.x);
-    const int s = items[it];
-    const FrontDesc F = fronts[s];
-    const int jb = blockIdx.x - before[it];
-    const TileRange tk = tile_range(kb, F.m, F.c, T);
-    const int nk = tk.size;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    const TL* L = Ls + F.loff;
+    cp_async_wait_groups<0>();
+    if (!ok) return;
+    if (lsplit) {
+        red[g * T + r] = acc[0];
+        __syncthreads();
+        acc[0] = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
+        __syncthreads();
+    }
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    const TL* dk = Dinv + dinv_off[s] + (int64_t)kb * T * T;
-    for (int idx = tid; idx < T * T; idx += nt) Dk[idx] = (TV)dk[idx];
-    for (int idx = tid; idx < nk * nrhs; idx += nt) {
-        int q = idx / nk, r = idx - q * nk;
-        tk_[idx] = f[tk.start + r + (int64_t)q * F.m];
-    }
-    __syncthreads();
-    apply_tile_inverse(Dk, tk_, x, nk, nrhs, true);
-    if (jb == kb) {
-        for (int idx = tid; idx < nk * nrhs; idx += nt) {
-            int q = idx / nk, r = idx - q * nk;
-            xp[F.first_col + tk.start + r + (int64_t)q * n] = x[idx];
+    if (!pivot) {
+        if (r < ti.size) {
+            if (lsplit) {
+                if (g == 0) f[ti.start + r] -= acc[0];
+            } else {
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    const int q = g + 4 * j;
+                    if (q < nrhs) f[ti.start + r + (int64_t)q * F.m] -= acc[j];
+                }
+            }
         }
         return;
     }
-    const TileRange tj = tile_range(jb, F.m, F.c, T);
-    for (int l = warp; l < tj.size; l += nw) {
-        const TL* col = L + tk.start + (int64_t)(tj.start + l) * F.ldl;  // L[kb rows, col]
-        for (int q = 0; q < nrhs; ++q) {
-            TV acc = TV(0);
-            for (int r = lane; r < nk; r += 32) acc += (TV)col[r] * x[r + q * nk];
+    // F = f_i - acc (zero beyond the tile), then y = Dk F
+    if (lsplit) {
+        if (g == 0) Y[r] = r < ti.size ? f[ti.start + r] - acc[0] : TV(0);
+    } else {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) f[tj.start + l + (int64_t)q * F.m] -= acc;
+        for (int j = 0; j < NQ; ++j) {
+            const int q = g + 4 * j;
+            if (q < nrhs)
+                Y[r + T * q] = r < ti.size ? f[ti.start + r + (int64_t)q * F.m] - acc[j] : TV(0);
         }
     }
+    __syncthreads();
+    if (lsplit) {
+        TV y = TV(0);
+#pragma unroll
+        for (int l = 0; l < 16; ++l) y += (TV)Dk[r + (16 * g + l) * LD] * Y[16 * g + l];
+        red[g * T + r] = y;
+        __syncthreads();
+        if (g == 0 && r < ti.size)
+            xp[F.first_col + ti.start + r] = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
+    } else {
+        TV y[NQ];
+#pragma unroll
+        for (int j = 0; j < NQ; ++j) y[j] = TV(0);
+#pragma unroll 4
+        for (int l = 0; l < T; ++l) {
+            const TV dv = (TV)Dk[r + l * LD];
+#pragma unroll
+            for (int j = 0; j < NQ; ++j) {
+                const int q = g + 4 * j;
+                if (q < nrhs) y[j] += dv * Y[l + T * q];
+            }
+        }
+        if (r < ti.size) {
+#pragma unroll
+            for (int j = 0; j < NQ; ++j) {
+                const int q = g + 4 * j;
+                if (q < nrhs) xp[F.first_col + ti.start + r + (int64_t)q * n] = y[j];
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release_gpu(fl + i, 1);
+}
+
+// Backward, task (s, j): pivot column tile j of front s accumulates
+// acc = sum_{k > j} L(k, j)' x_k over all row tiles below it -- the update
+// rows first (their x is final: ancestors, read through the row list), then
+// the pivot tiles nt1-1 .. j+1 of this front as they publish (flag 2) -- and
+// solves x_j = inv(L_jj)' (y_j - acc).  Threads: l = column in the tile.
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256)
+    k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
+                int ntasks, int* __restrict__ counter, int* __restrict__ flags,
+                int* __restrict__ abort_flag, int* __restrict__ err, const int* __restrict__ rows,
+                const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
+                const TL* __restrict__ Dinv, TV* __restrict__ xp, int n, int nrhs) {
+    constexpr int T = kTile, LD = kTile + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TL* Lb = reinterpret_cast<TL*>(smem_raw);
+    TL* Dk = Lb + 2 * T * LD;
+    TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
+    TV* red = X + T * nrhs;
+    __shared__ int s_task, s_ok;
+    const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
+    if (tid == 0) s_task = atomicAdd(counter, 1);
+    __syncthreads();
+    if (s_task >= ntasks) {  // counter not cleared: refuse rather than read past the list
+        if (tid == 0) atomicOr(err, 2);
+        return;
+    }
+    const int2 tk = tasks[s_task];
+    const int s = tk.x, j = tk.y;
+    const FrontDesc F = fronts[s];
+    const int nt1 = tiles_l(F.c, T), NT = nt1 + tiles_l(F.m - F.c, T);
+    const TileRange tj = tile_range(j, F.m, F.c, T);
+    const bool lsplit = nrhs == 1;
+    const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;  // column tile j
+    const int* rw = rows + F.rows_off;
+    int* fl = flags + dinv_off[s] / (T * T);
+    const int nblk = NT - 1 - j;  // row tiles k = NT-1 down to j+1
+    load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
+    if (nblk > 0) {
+        const TileRange t0 = tile_range(NT - 1, F.m, F.c, T);
+        load_block_async(Lb, Lc + t0.start, F.ldl, t0.size, tj.size);
+    }
+    cp_async_commit_group();
+    TV acc[NQ];
+#pragma unroll
+    for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
+    bool ok = true;
+    for (int b = 0; b < nblk; ++b) {
+        const int k = NT - 1 - b;
+        if (b + 1 < nblk) {
+            const TileRange tn = tile_range(k - 1, F.m, F.c, T);
+            load_block_async(Lb + ((b + 1) & 1) * T * LD, Lc + tn.start, F.ldl, tn.size, tj.size);
+        }
+        cp_async_commit_group();
+        const TileRange tkr = tile_range(k, F.m, F.c, T);
+        if (k < nt1) {
+            if (tid == 0) s_ok = wait_flag(fl + k, 2, abort_flag, err);
+            __syncthreads();
+            if (!s_ok) {
+                ok = false;
+                break;
+            }
+            for (int e = tid; e < T * nrhs; e += blockDim.x) {
+                const int rr = e & (T - 1), q = e / T;
+                X[e] = rr < tkr.size
+                           ? ld_shared_value(xp + F.first_col + tkr.start + rr + (int64_t)q * n)
+                           : TV(0);
+            }
+        } else {
+            for (int e = tid; e < T * nrhs; e += blockDim.x) {
+                const int rr = e & (T - 1), q = e / T;
+                X[e] = rr < tkr.size ? xp[rw[tkr.start + rr] + (int64_t)q * n] : TV(0);
+            }
+        }
+        cp_async_wait_groups<1>();
+        __syncthreads();
+        const TL* B = Lb + (b & 1) * T * LD;
+        if (lsplit) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r) acc[0] += (TV)B[(16 * g + r) + l * LD] * X[16 * g + r];
+        } else {
+#pragma unroll 4
+            for (int r = 0; r < T; ++r) {
+                const TV lv = (TV)B[r + l * LD];
+#pragma unroll
+                for (int a = 0; a < NQ; ++a) {
+                    const int q = g + 4 * a;
+                    if (q < nrhs) acc[a] += lv * X[r + T * q];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    cp_async_wait_groups<0>();
+    if (!ok) return;
+    if (lsplit) {
+        red[g * T + l] = acc[0];
+        __syncthreads();
+        acc[0] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+        __syncthreads();
+    }
+    // t = y_j - acc (y_j: this front's forward solution), then x_j = Dk' t
+    const int64_t xj = F.first_col + tj.start;
+    if (lsplit) {
+        if (g == 0) X[l] = l < tj.size ? xp[xj + l] - acc[0] : TV(0);
+    } else {
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) {
+            const int q = g + 4 * a;
+            if (q < nrhs) X[l + T * q] = l < tj.size ? xp[xj + l + (int64_t)q * n] - acc[a] : TV(0);
+        }
+    }
+    __syncthreads();
+    if (lsplit) {
+        TV x = TV(0);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) x += (TV)Dk[(16 * g + r) + l * LD] * X[16 * g + r];
+        red[g * T + l] = x;
+        __syncthreads();
+        if (g == 0 && l < tj.size) xp[xj + l] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+    } else {
+        TV x[NQ];
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) x[a] = TV(0);
+#pragma unroll 4
+        for (int r = 0; r < T; ++r) {
+            const TV dv = (TV)Dk[r + l * LD];
+#pragma unroll
+            for (int a = 0; a < NQ; ++a) {
+                const int q = g + 4 * a;
+                if (q < nrhs) x[a] += dv * X[r + T * q];
+            }
+        }
+        if (l < tj.size) {
+#pragma unroll
+            for (int a = 0; a < NQ; ++a) {
+                const int q = g + 4 * a;
+                if (q < nrhs) xp[xj + l + (int64_t)q * n] = x[a];
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release_gpu(fl + j, 2);
 }
 
 // ---------------------------------------------------------------------------
@@ -399,10 +590,13 @@ static void set_solve_attributes() {
                          200 * 1024);
     cudaFuncSetAttribute(k_bwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
-    cudaFuncSetAttribute(k_fwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    cudaFuncSetAttribute(k_bwd_step<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
+    const int lv = (int)level_smem_bytes<TL, TV>(64);
+    cudaFuncSetAttribute(k_fwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_fwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_fwd_level<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_level<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
 }
 
 void init_solve_kernels() {
@@ -410,13 +604,45 @@ void init_solve_kernels() {
     set_solve_attributes<float, double>();
 }
 
+template <typename TL, typename TV, int NQ>
+static void launch_level_tasks(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
+                               TV* xp, TV* fv, int nrhs, cudaStream_t st) {
+    const SolveSchedule& S = D.solve;
+    const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
+    const int t0 = beg[l], nt = beg[l + 1] - beg[l];
+    if (nt == 0) return;
+    const size_t smem = level_smem_bytes<TL, TV>(nrhs);
+    int* counter = S.sync + 2 * l + (forward ? 0 : 1);
+    int* flags = S.sync + 2 * D.nlevels;
+    int* abort_flag = flags + S.nflags;
+    if (forward)
+        k_fwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
+                                                     abort_flag, S.err, D.fv_off, D.dinv_off, Ls,
+                                                     Dinv, xp, fv, D.n, nrhs);
+    else
+        k_bwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
+                                                     abort_flag, S.err, D.rows, D.dinv_off, Ls,
+                                                     Dinv, xp, D.n, nrhs);
+}
+
+template <typename TL, typename TV>
+static void launch_level(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
+                         TV* xp, TV* fv, int nrhs, cudaStream_t st) {
+    if (nrhs <= 4)
+        launch_level_tasks<TL, TV, 1>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
+    else if (nrhs <= 16)
+        launch_level_tasks<TL, TV, 4>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
+    else
+        launch_level_tasks<TL, TV, 16>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
+}
+
 template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st) {
     const int n = D.n;
     const int msmall = Plan::small_limit[kSmallBuckets - 1];
-    const size_t step_smem = (size_t)(kTile * kTile + 2 * kTile * nrhs + 8 * kTile) * sizeof(TV);
     const SolveSchedule& S = D.solve;
+    cudaMemsetAsync(S.sync, 0, (size_t)S.nsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
@@ -426,34 +652,17 @@ void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv
         }
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st);
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.fwd_bytes[l] * sizeof(TL));
             k_fwd_assemble<TV><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, D.child,
                                                         D.relmap, D.fv_off, xp, fv, n, nrhs);
-            for (int q = S.fwd_beg[l]; q < S.fwd_beg[l + 1]; ++q) {
-                const WorkList& w = S.fwd[q];
-                if (w.nctas == 0) continue;
-                k_fwd_step<TL, TV><<<w.nctas, 256, step_smem, st>>>(
-                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off,
-                    D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
-            }
+            launch_level<TL, TV>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
         }
     }
     for (int l = D.nlevels - 1; l >= 0; --l) {
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st);
-            const WorkList& g = S.gather[l];
-            if (g.nctas > 0)
-                k_bwd_gather<TL, TV><<<g.nctas, 256, 0, st>>>(D.fronts, S.items + g.off,
-                                                              S.before + g.off, g.nitems, D.rows,
-                                                              D.fv_off, Ls, xp, fv, n, nrhs);
-            for (int q = S.bwd_beg[l]; q < S.bwd_beg[l + 1]; ++q) {
-                const WorkList& w = S.bwd[q];
-                if (w.nctas == 0) continue;
-                k_bwd_step<TL, TV><<<w.nctas, 256, step_smem, st>>>(
-                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, w.step, D.fv_off,
-                    D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
-            }
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.bwd_bytes[l] * sizeof(TL));
+            launch_level<TL, TV>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
         }
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
