@@ -249,8 +249,9 @@ void upload_plan(mdgpu_handle_s* h) {
         D.solve.tasks = reinterpret_cast<int2*>(h->keep(upload(tasks)));
         D.solve.fwd_task_beg = SS.fwd_task_beg;
         D.solve.bwd_task_beg = SS.bwd_task_beg;
-        D.solve.fwd_bytes = SS.fwd_bytes;
-        D.solve.bwd_bytes = SS.bwd_bytes;
+        D.solve.fwd_elems = SS.fwd_elems;
+        D.solve.bwd_elems = SS.bwd_elems;
+        D.solve.small_elems = SS.small_elems;
         D.solve.nflags = SS.nflags;
         D.solve.nsync = 2 * P.nlevels + SS.nflags + 1;
         D.solve.sync = h->keep(dalloc<int>(D.solve.nsync));

@@ -186,106 +186,25 @@ __global__ void __launch_bounds__(256)
 // large fronts: tiles
 // ---------------------------------------------------------------------------
 
-// In-place Cholesky of an n x n lower tile held in shared memory (ld = LDS).
-template <typename T>
-__device__ void tile_potrf_smem(T* S, int LDS, int n, int* status, int col0) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int k = 0; k < n; ++k) {
-        const T dkk = S[k + k * LDS];
-        const T d = sqrt(dkk);
-        if (tid == 0 && !(dkk > T(0))) flag_pivot(status, col0 + k);
-        const T inv = T(1) / d;
-        for (int i = k + 1 + tid; i < n; i += nt) S[i + k * LDS] *= inv;
-        __syncthreads();
-        if (tid == 0) S[k + k * LDS] = d;
-        const int r = n - k - 1;
-        for (int idx = tid; idx < r * r; idx += nt) {
-            int jj = idx / r, ii = idx - jj * r;
-            if (ii >= jj) S[(k + 1 + ii) + (k + 1 + jj) * LDS] -= S[(k + 1 + ii) + k * LDS] * S[(k + 1 + jj) + k * LDS];
-        }
-        __syncthreads();
-    }
-}
-
-// In-place inverse of an n x n lower-triangular tile in shared memory (ld =
-// LDS), columns right to left: column j of inv(L) is -inv(L_jj) times the
-// already inverted trailing block applied to L's column j.  tmp: n entries.
-template <typename T>
-__device__ void tile_trtri_smem(T* S, int LDS, int n, T* tmp) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int j = n - 1; j >= 0; --j) {
-        for (int i = j + 1 + tid; i < n; i += nt) tmp[i] = S[i + j * LDS];
-        __syncthreads();
-        const T djj = T(1) / S[j + j * LDS];
-        for (int i = j + 1 + tid; i < n; i += nt) {
-            T acc = T(0);
-            for (int l = j + 1; l <= i; ++l) acc += S[i + l * LDS] * tmp[l];
-            S[i + j * LDS] = -djj * acc;
-        }
-        __syncthreads();
-        if (tid == 0) S[j + j * LDS] = djj;
-        __syncthreads();
-    }
-}
-
-// Cholesky of a 32 x 32 SPD block held one column per lane in registers
-// (lane j owns column j; rows i >= j are meaningful), in place.  Pivots are
-// broadcast by shuffles: no barriers.  A non-positive pivot is recorded at
-// global column col0 + k.
-template <typename T>
-__device__ __forceinline__ void warp_chol32(T (&a)[32], int lane, int* status, int col0) {
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-        const T piv = __shfl_sync(0xffffffffu, a[k], k);
-        if (lane == 0 && !(piv > T(0))) flag_pivot(status, col0 + k);
-        const T d = sqrt(piv);
-        const T inv = T(1) / d;
-        if (lane == k) {
-            a[k] = d;
-#pragma unroll
-            for (int i = k + 1; i < 32; ++i) a[i] *= inv;
-        }
-        T ljk = T(0);
-#pragma unroll
-        for (int i = k + 1; i < 32; ++i) {
-            const T v = __shfl_sync(0xffffffffu, a[i], k);  // L(i, k)
-            if (lane == i) ljk = v;
-            if (lane > k && i >= lane) a[i] -= v * ljk;
-        }
-    }
-}
-
-// Column `lane` of inv(L) for a 32 x 32 lower-triangular L in shared memory
-// (element (i, l) at L[i + l * ld]), by forward substitution; written to X.
-template <typename T>
-__device__ __forceinline__ void warp_trinv32(const T* L, int ld, T* X, int ldx, int lane) {
-    T x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        T acc = (i == lane) ? T(1) : T(0);
-#pragma unroll
-        for (int l = 0; l < i; ++l)
-            if (l >= lane) acc -= L[i + l * ld] * x[l];
-        x[i] = (i >= lane) ? acc / L[i + i * ld] : T(0);
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) X[i + lane * ldx] = x[i];
-}
-
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
-// column-major, zero above the diagonal) at Dk.  2 x 2 blocks of 32:
-//   L11 = chol(A11)             warp 0, registers          X11 = inv(L11)
-//   L21 = A21 X11'              all threads
-//   A22 -= L21 L21'             all threads
-//   L22 = chol(A22)             warp 0, registers          X22 = inv(L22)
-//   X21 = -X22 (L21 X11)        all threads
-// A partial tile (n < 64) is padded with the identity.  S, W: 64 x 65 each.
+// column-major, zero above the diagonal) at Dk.  Every thread of the CTA
+// works on every step, one barrier per step:
+//   1. right-looking elimination with unscaled pivot columns:
+//        S(i, j) -= S(i, p) S(j, p) / S(p, p)   for p < j <= i
+//      (column p is only read during step p, so one barrier per pivot);
+//   2. L(i, j) = S(i, j) / sqrt(S(j, j)), L(j, j) = sqrt(S(j, j)) into W;
+//   3. X = inv(L) by row elimination with rows left unscaled,
+//        X(i, c) -= L(i, p) X(p, c) / L(p, p)   for i > p, c <= p,
+//      and each row divided by its diagonal on output.
+// A partial tile (n < 64) is padded with the identity.  S, W: TB x (TB + 1);
+// 256 threads: row r = tid % 64 of the tile, column group tid / 64 (stride 4).
 template <typename T, int TB>
 __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
                                 int* status) {
-    static_assert(TB == 64, "2 x 2 blocks of 32");
+    static_assert(TB == 64, "row = tid % 64 over 256 threads");
     constexpr int LD = TB + 1;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int r = tid & (TB - 1), cg = tid >> 6;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
     const int col0 = f.first_col + tk.start;
@@ -297,73 +216,45 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
         S[i + j * LD] = v;
     }
     __syncthreads();
-    if (warp == 0) {  // L11, X11
-        T a[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) a[i] = S[i + lane * LD];
-        warp_chol32(a, lane, status, col0);
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i >= lane) S[i + lane * LD] = a[i];
-        __syncwarp();
-        warp_trinv32(S, LD, W, LD, lane);
-    }
-    __syncthreads();
-    // L21 = A21 X11' into W rows 32..63, columns 0..31
-    for (int idx = tid; idx < 32 * 32; idx += nt) {
-        int c = idx >> 5, r = idx & 31;
-        T acc = T(0);
-#pragma unroll 8
-        for (int l = 0; l <= c; ++l) acc += S[(32 + r) + l * LD] * W[c + l * LD];
-        W[(32 + r) + c * LD] = acc;
-    }
-    __syncthreads();
-    // A22 -= L21 L21' (lower), and L21 into its final place in S
-    for (int idx = tid; idx < 32 * 32; idx += nt) {
-        int c = idx >> 5, r = idx & 31;
-        S[(32 + r) + c * LD] = W[(32 + r) + c * LD];
-        if (r >= c) {
-            T acc = T(0);
-#pragma unroll 8
-            for (int l = 0; l < 32; ++l) acc += W[(32 + r) + l * LD] * W[(32 + c) + l * LD];
-            S[(32 + r) + (32 + c) * LD] -= acc;
+#pragma unroll 1
+    for (int p = 0; p < TB; ++p) {
+        const T dp = S[p + p * LD];
+        if (tid == 0 && p < n && !(dp > T(0))) flag_pivot(status, col0 + p);
+        if (r > p) {
+            const T sip = S[r + p * LD] / dp;
+#pragma unroll 4
+            for (int j = p + 1 + cg; j <= r; j += 4) S[r + j * LD] -= sip * S[j + p * LD];
         }
+        __syncthreads();
     }
-    __syncthreads();
-    if (warp == 0) {  // L22, X22
-        T a[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) a[i] = S[(32 + i) + (32 + lane) * LD];
-        warp_chol32(a, lane, status, col0 + 32);
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i >= lane) S[(32 + i) + (32 + lane) * LD] = a[i];
-        __syncwarp();
-        warp_trinv32(S + 32 + 32 * LD, LD, W + 32 + 32 * LD, LD, lane);
-    }
-    __syncthreads();
-    // T1 = L21 X11 into W rows 0..31, columns 32..63
-    for (int idx = tid; idx < 32 * 32; idx += nt) {
-        int c = idx >> 5, r = idx & 31;
-        T acc = T(0);
-#pragma unroll 8
-        for (int l = c; l < 32; ++l) acc += S[(32 + r) + l * LD] * W[l + c * LD];
-        W[r + (32 + c) * LD] = acc;
-    }
-    __syncthreads();
-    // X21 = -X22 T1 into W rows 32..63, columns 0..31
-    for (int idx = tid; idx < 32 * 32; idx += nt) {
-        int c = idx >> 5, r = idx & 31;
-        T acc = T(0);
-#pragma unroll 8
-        for (int l = 0; l <= r; ++l) acc += W[(32 + r) + (32 + l) * LD] * W[l + (32 + c) * LD];
-        W[(32 + r) + c * LD] = -acc;
+    for (int idx = tid; idx < TB * TB; idx += nt) {
+        int j = idx / TB, i = idx - j * TB;
+        T v = T(0);
+        if (i >= j) {
+            const T d = sqrt(S[j + j * LD]);
+            v = (i == j) ? d : S[i + j * LD] / d;
+        }
+        W[i + j * LD] = v;
     }
     __syncthreads();
     for (int idx = tid; idx < TB * TB; idx += nt) {
         int j = idx / TB, i = idx - j * TB;
-        if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * LD];
-        Dk[idx] = (i >= j && i < n && j < n) ? W[i + j * LD] : T(0);
+        S[i + j * LD] = (i == j) ? T(1) : T(0);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int p = 0; p < TB - 1; ++p) {
+        if (r > p) {
+            const T lip = W[r + p * LD] / W[p + p * LD];
+#pragma unroll 4
+            for (int c2 = cg; c2 <= p; c2 += 4) S[r + c2 * LD] -= lip * S[p + c2 * LD];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < TB * TB; idx += nt) {
+        int j = idx / TB, i = idx - j * TB;
+        if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = W[i + j * LD];
+        Dk[idx] = (i >= j && i < n && j < n) ? S[i + j * LD] / W[i + i * LD] : T(0);
     }
 }
 
@@ -602,7 +493,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
         if (w.nctas == 0) continue;
         switch (op.kind) {
             case OP_ASSEMBLE: {
-                ProfScope ps(D.prof, KC_ASSEMBLE, st);
+                ProfScope ps(D.prof, KC_ASSEMBLE, st, 0, op.elems * sizeof(T) + op.xbytes);
                 k_big_assemble<T><<<w.nctas, 256, D.max_u * sizeof(int), st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols, D.child,
                     D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off, D.asm_off, D.asm_range,
@@ -610,27 +501,27 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 break;
             }
             case OP_POTRF: {
-                ProfScope ps(D.prof, KC_POTRF, st);
+                ProfScope ps(D.prof, KC_POTRF, st, op.flops, op.elems * sizeof(T));
                 k_tile_potrf<T, kTile><<<w.nitems, 256, diag_smem<T>(), st>>>(
                     D.fronts, S.items + w.off, op.arg, D.dinv_off, Ls, Dinv, status);
                 break;
             }
             case OP_TRSM: {
-                ProfScope ps(D.prof, KC_TRSM, st);
+                ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
                 k_tile_trsm<T, kTile><<<w.nctas, 256, gsm, st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, D.dinv_off, Ls,
                     Dinv);
                 break;
             }
             case OP_UPDATE_PANEL: {
-                ProfScope ps(D.prof, KC_TRSM, st);
+                ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
                 k_tile_update<T, kTile><<<w.nctas, 256, gsm, st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, op.arg2,
                     D.dinv_off, Ls, Us, Dinv, status);
                 break;
             }
             case OP_SCHUR_TC: {
-                ProfScope ps(D.prof, KC_SCHUR, st, op.flops);
+                ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
                 if constexpr (sizeof(T) == 4)
                     launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, st);
                 else

@@ -97,7 +97,8 @@ struct DevSchedule {
 struct SolveSchedule {
     int2* tasks = nullptr;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1
-    std::vector<double> fwd_bytes, bwd_bytes;     // per level: L + Dinv elements
+    std::vector<double> fwd_elems, bwd_elems;     // per level: L + Dinv elements
+    std::vector<double> small_elems;              // per level: L elements of small fronts
     int* sync = nullptr;
     int nsync = 0, nflags = 0;
     int* err = nullptr;

@@ -295,8 +295,14 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     S.tasks.clear();
     S.fwd_task_beg.assign(P.nlevels + 1, 0);
     S.bwd_task_beg.assign(P.nlevels + 1, 0);
-    S.fwd_bytes.assign(P.nlevels, 0.0);
-    S.bwd_bytes.assign(P.nlevels, 0.0);
+    S.fwd_elems.assign(P.nlevels, 0.0);
+    S.bwd_elems.assign(P.nlevels, 0.0);
+    S.small_elems.assign(P.nlevels, 0.0);
+    for (int l = 0; l < P.nlevels; ++l)
+        for (int q = P.small_ptr[l * kSmallBuckets]; q < P.small_ptr[(l + 1) * kSmallBuckets]; ++q) {
+            const FrontDesc& f = P.fronts[P.small_list[q]];
+            S.small_elems[l] += (double)f.c * (f.c + 1) / 2 + (double)(f.m - f.c) * f.c;
+        }
     int64_t ntiles_piv = 0;
     for (int s : P.large_list) ntiles_piv += (P.fronts[s].c + T - 1) / T;
     S.nflags = (int)ntiles_piv;
@@ -329,7 +335,7 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
                 else
                     for (int j = 0; j < nt1; ++j) ks.push_back({nt1 - 1 - j, ord++, s, j});
             }
-            (dir == 0 ? S.fwd_bytes : S.bwd_bytes)[l] = bytes;
+            (dir == 0 ? S.fwd_elems : S.bwd_elems)[l] = bytes;
             emit(ks);
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
@@ -352,39 +358,74 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
         if (fr.empty()) continue;
         std::vector<std::pair<int, int>> as, po;
         int maxpanels = 0;
+        double asm_el = 0, asm_x = 0, po_fl = 0, po_el = 0;
+        // diagonal tile t of f: factor (n^3/3), read + write its lower part,
+        // write the T x T inverse
+        auto potrf_cost = [&](const FrontDesc& f, int t, double& fl, double& el) {
+            double nn = tsize(f, t);
+            fl += nn * nn * nn / 3.0;
+            el += nn * (nn + 1) + (double)T * T;
+        };
         for (int s : fr) {
             const FrontDesc& f = P.fronts[s];
             as.push_back({s, (f.m + CB - 1) / CB});
             po.push_back({s, 1});
             maxpanels = std::max(maxpanels, (f.c + PW - 1) / PW);
+            // assembly: write the L panel and the U store, read every child's
+            // update matrix; FP64 values with their source index and position
+            double u = f.m - f.c;
+            asm_el += (double)f.m * f.c + u * (u + 1) / 2;
+            for (int h = f.child_beg; h < f.child_end; ++h) {
+                const FrontDesc& g = P.fronts[P.child[h]];
+                double uc = g.m - g.c;
+                asm_el += uc * (uc + 1) / 2;
+                asm_x += 4.0 * uc;  // relative map
+            }
+            asm_x += 16.0 * (f.a_end - f.a_beg);
+            potrf_cost(f, 0, po_fl, po_el);
         }
-        S.ops.push_back({OP_ASSEMBLE, 0, 0, S.store.add(as, 0), 0});
-        S.ops.push_back({OP_POTRF, 0, 0, S.store.add(po, 0), 0});
+        S.ops.push_back({OP_ASSEMBLE, 0, 0, S.store.add(as, 0), 0, asm_el, asm_x});
+        S.ops.push_back({OP_POTRF, 0, 0, S.store.add(po, 0), po_fl, po_el, 0});
         for (int p = 0; p < maxpanels; ++p) {
             for (int k = p * TPP; k < (p + 1) * TPP; ++k) {
                 std::vector<std::pair<int, int>> tr, up;
-                double upfl = 0;
+                double upfl = 0, upel = 0, trfl = 0, trel = 0;
                 for (int s : fr) {
                     const FrontDesc& f = P.fronts[s];
                     int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
                     if (k >= nt1) continue;
                     if (NT - k - 1 > 0) tr.push_back({s, NT - k - 1});
+                    const double K = tsize(f, k);
+                    for (int i = k + 1; i < NT; ++i) {
+                        // X = A inv(L_kk)': triangular solve flops, read A and
+                        // the inverse, write X
+                        double ri = tsize(f, i);
+                        trfl += ri * K * K;
+                        trel += 2.0 * ri * K + K * K;
+                    }
                     int jl = std::min((p + 1) * TPP - 1, nt1 - 1);
                     int cnt = 0;
                     for (int j = k + 1; j <= jl; ++j) {
                         cnt += NT - j;
-                        double K = tsize(f, k), rj = tsize(f, j);
+                        double rj = tsize(f, j);
                         upfl += K * rj * (rj + 1);
-                        for (int i = j + 1; i < NT; ++i) upfl += 2.0 * K * tsize(f, i) * rj;
+                        upel += K * rj + rj * (rj + 1);
+                        for (int i = j + 1; i < NT; ++i) {
+                            double ri = tsize(f, i);
+                            upfl += 2.0 * K * ri * rj;
+                            upel += K * (ri + rj) + 2.0 * ri * rj;
+                        }
+                        if (j == k + 1) potrf_cost(f, j, upfl, upel);  // fused next diagonal
                     }
                     if (cnt > 0) up.push_back({s, cnt});
                 }
-                if (!tr.empty()) S.ops.push_back({OP_TRSM, k, 0, S.store.add(tr, k), 0});
+                if (!tr.empty()) S.ops.push_back({OP_TRSM, k, 0, S.store.add(tr, k), trfl, trel, 0});
                 if (!up.empty())
-                    S.ops.push_back({OP_UPDATE_PANEL, k, (p + 1) * TPP - 1, S.store.add(up, k), upfl});
+                    S.ops.push_back({OP_UPDATE_PANEL, k, (p + 1) * TPP - 1, S.store.add(up, k),
+                                     upfl, upel, 0});
             }
             std::vector<std::pair<int, int>> big, nextp;
-            double fl = 0;
+            double fl = 0, el = 0, np_fl = 0, np_el = 0;
             for (int s : fr) {
                 const FrontDesc& f = P.fronts[s];
                 int k0 = p * PW;
@@ -397,12 +438,16 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
                     big.push_back({s, nb * (nb + 1) / 2});
                     double tr = f.m - cbeg;
                     fl += (double)K * tr * (tr + 1);  // lower trailing part, 2 flops per FMA
+                    el += (double)K * tr + tr * (tr + 1);  // read the panel, update the trailing part
                 }
-                if ((p + 1) * PW < f.c) nextp.push_back({s, 1});
+                if ((p + 1) * PW < f.c) {
+                    nextp.push_back({s, 1});
+                    potrf_cost(f, (p + 1) * TPP, np_fl, np_el);
+                }
             }
-            if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), fl});
+            if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), fl, el, 0});
             if (!nextp.empty())
-                S.ops.push_back({OP_POTRF, (p + 1) * TPP, 0, S.store.add(nextp, 0), 0});
+                S.ops.push_back({OP_POTRF, (p + 1) * TPP, 0, S.store.add(nextp, 0), np_fl, np_el, 0});
         }
     }
     S.op_beg[P.nlevels] = (int)S.ops.size();

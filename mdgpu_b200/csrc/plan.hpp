@@ -120,7 +120,9 @@ struct PanelOp {
     int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_TC)
     int arg2;     // UPDATE_PANEL: last tile index of the panel
     WorkList w;
-    double flops;  // algorithmic flops of SCHUR_TC / UPDATE_PANEL launches
+    double flops;  // algorithmic flops of the launch
+    double elems;  // algorithmic factor-scalar traffic (elements read + written)
+    double xbytes; // other algorithmic traffic in bytes (FP64 values, indices)
 };
 struct PanelSchedule {
     ListStore store;
@@ -137,7 +139,8 @@ struct SolveScheduleHost {
     // waits on tasks that took a lower ticket, hence already run)
     std::vector<int> tasks;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1 each, in tasks
-    std::vector<double> fwd_bytes, bwd_bytes;     // per level, L + Dinv elements read
+    std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read
+    std::vector<double> small_elems;              // per level: L elements of its small fronts
     int nflags = 0;                               // one per pivot tile of a large front
 };
 

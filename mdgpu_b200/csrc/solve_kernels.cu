@@ -646,13 +646,13 @@ void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv
     for (int l = 0; l < D.nlevels; ++l) {
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
-            ProfScope ps(D.prof, KC_SOLVE_SMALL, st);
+            ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
             k_fwd_small<TL, TV><<<end - beg, 128, (size_t)msmall * nrhs * sizeof(TV), st>>>(
                 D.fronts, D.small_list + beg, D.child, D.relmap, D.fv_off, Ls, xp, fv, n, nrhs);
         }
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.fwd_bytes[l] * sizeof(TL));
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.fwd_elems[l] * sizeof(TL));
             k_fwd_assemble<TV><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, D.child,
                                                         D.relmap, D.fv_off, xp, fv, n, nrhs);
             launch_level<TL, TV>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
@@ -661,14 +661,14 @@ void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv
     for (int l = D.nlevels - 1; l >= 0; --l) {
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.bwd_bytes[l] * sizeof(TL));
+            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.bwd_elems[l] * sizeof(TL));
             launch_level<TL, TV>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
         }
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
             int umax = msmall;
             size_t smem = (size_t)(umax + msmall) * nrhs * sizeof(TV);
-            ProfScope ps(D.prof, KC_SOLVE_SMALL, st);
+            ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
             k_bwd_small<TL, TV><<<end - beg, 128, smem, st>>>(D.fronts, D.small_list + beg,
                                                               D.rows, Ls, xp, n, nrhs, umax);
         }
