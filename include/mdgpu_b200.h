@@ -117,8 +117,9 @@ MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, doub
  * implicit synchronization -- the work vectors come from a fixed 32 MiB
  * device array that every GPU loading this library holds until exit (the
  * handle's plan and factor were allocated earlier by mdgpu_analyze and
- * mdgpu_factor).  A call needs (n + sum of front rows) x min(nrhs, 64)
- * doubles; larger requests return MDGPU_ERR_INVALID.  All calls share the
+ * mdgpu_factor).  A call needs (n + w) x min(nrhs, 64) doubles, w =
+ * mdgpu_info(h, "solve_work_rows") (front vector rows plus backward partial
+ * sums); larger requests return MDGPU_ERR_INVALID.  All calls share the
  * array: calls whose work overlaps on one GPU race and must be serialized by
  * the caller.  The first call on a device looks up the array's address; make
  * it before any stream capture.

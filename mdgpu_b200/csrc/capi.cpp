@@ -226,7 +226,8 @@ void upload_plan(mdgpu_handle_s* h) {
         fvo[s] = acc;
         acc += P.fronts[s].m;
     }
-    D.fv_total = acc;
+    D.fv_fronts = acc;
+    D.fv_total = acc + h->ssched.gather_vecs * kTile;
     D.fv_off = h->keep(upload(fvo));
     D.dinv_off = h->keep(upload(P.dinv_off));
     D.asm_off = h->keep(upload(P.asm_off));
@@ -252,6 +253,9 @@ void upload_plan(mdgpu_handle_s* h) {
         D.solve.fwd_elems = SS.fwd_elems;
         D.solve.bwd_elems = SS.bwd_elems;
         D.solve.small_elems = SS.small_elems;
+        D.solve.gather_task_beg = SS.gather_task_beg;
+        D.solve.gather_nch = h->keep(upload(SS.gather_nch));
+        D.solve.gather_off = h->keep(upload(SS.gather_off));
         D.solve.nflags = SS.nflags;
         D.solve.nsync = 2 * P.nlevels + SS.nflags + 1;
         D.solve.sync = h->keep(dalloc<int>(D.solve.nsync));
@@ -613,6 +617,7 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "nchild") *value = (long long)P.child.size();
     else if (k == "large_fronts") *value = (long long)P.large_list.size();
     else if (k == "on_device") *value = h->on_device;
+    else if (k == "solve_work_rows") *value = h->D.fv_total;
     else return fail(MDGPU_ERR_INVALID, "unknown key " + k);
     return MDGPU_OK;
 }
@@ -818,7 +823,7 @@ int mdgpu_solve_device_noalloc(mdgpu_handle h, const double* dB, int ldb, double
         if (need > noalloc_scratch_capacity())
             return fail(MDGPU_ERR_INVALID,
                         "no-allocation solve needs " + std::to_string(need) +
-                            " scratch doubles ((n + sum of front rows) x min(nrhs, 64)), limit " +
+                            " scratch doubles ((n + solve_work_rows) x min(nrhs, 64)), limit " +
                             std::to_string(noalloc_scratch_capacity()));
         double* xp = scratch;
         double* fv = scratch + (int64_t)n * chunk;

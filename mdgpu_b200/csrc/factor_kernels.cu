@@ -187,24 +187,26 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
-// column-major, zero above the diagonal) at Dk.  Every thread of the CTA
-// works on every step, one barrier per step:
-//   1. right-looking elimination with unscaled pivot columns:
-//        S(i, j) -= S(i, p) S(j, p) / S(p, p)   for p < j <= i
-//      (column p is only read during step p, so one barrier per pivot);
-//   2. L(i, j) = S(i, j) / sqrt(S(j, j)), L(j, j) = sqrt(S(j, j)) into W;
-//   3. X = inv(L) by row elimination with rows left unscaled,
-//        X(i, c) -= L(i, p) X(p, c) / L(p, p)   for i > p, c <= p,
-//      and each row divided by its diagonal on output.
-// A partial tile (n < 64) is padded with the identity.  S, W: TB x (TB + 1);
-// 256 threads: row r = tid % 64 of the tile, column group tid / 64 (stride 4).
+// column-major, zero above the diagonal) at Dk.  The 256 threads form a
+// 16 x 16 grid; thread (tr, tc), tr >= tc, keeps the 4 x 4 block (tr, tc) of
+// the tile in registers.  Sixteen blocked steps of right-looking Cholesky:
+//   (a) the diagonal owner factors its 4 x 4 block in registers;
+//   (b) the owners below it solve X L_kk' = A (their block of the panel);
+//   (c) every lower block right of the panel takes the rank-4 update;
+// with L going to S block by block (two barriers per step).  Then the
+// inverse by block rows: owners of block row kb apply inv(L_kk) to their
+// accumulated blocks (final rows of inv(L), to W), and the blocks below
+// subtract L(tr, kb) X(kb, tc) (one barrier per step).  One division per
+// pivot: its reciprocal waits in S's padding row (row TB) for the solves.
+// A partial tile (n < 64) is padded with the identity.  S, W: TB x (TB + 1).
 template <typename T, int TB>
 __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
                                 int* status) {
-    static_assert(TB == 64, "row = tid % 64 over 256 threads");
-    constexpr int LD = TB + 1;
+    static_assert(TB == 64, "16 x 16 grid of 4 x 4 blocks over 256 threads");
+    constexpr int LD = TB + 1, B = 4, NB = TB / B;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int r = tid & (TB - 1), cg = tid >> 6;
+    const int tr = tid & (NB - 1), tc = tid >> 4;
+    const bool low = tr >= tc;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
     const int col0 = f.first_col + tk.start;
@@ -216,45 +218,129 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
         S[i + j * LD] = v;
     }
     __syncthreads();
+    T a[B][B];
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+        for (int c = 0; c < B; ++c) a[r][c] = low ? S[(B * tr + r) + (B * tc + c) * LD] : T(0);
+    __syncthreads();
 #pragma unroll 1
-    for (int p = 0; p < TB; ++p) {
-        const T dp = S[p + p * LD];
-        if (tid == 0 && p < n && !(dp > T(0))) flag_pivot(status, col0 + p);
-        if (r > p) {
-            const T sip = S[r + p * LD] / dp;
-#pragma unroll 4
-            for (int j = p + 1 + cg; j <= r; j += 4) S[r + j * LD] -= sip * S[j + p * LD];
+    for (int kb = 0; kb < NB; ++kb) {
+        if (tr == kb && tc == kb) {  // (a)
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                const T piv = a[i][i];
+                if (B * kb + i < n && !(piv > T(0))) flag_pivot(status, col0 + B * kb + i);
+                const T d = sqrt(piv);
+                const T rd = T(1) / d;
+                a[i][i] = d;
+                S[TB + (B * kb + i) * LD] = rd;  // padding row: reciprocal pivots
+#pragma unroll
+                for (int r = i + 1; r < B; ++r) a[r][i] *= rd;
+#pragma unroll
+                for (int r = i + 1; r < B; ++r)
+#pragma unroll
+                    for (int c = i + 1; c <= r; ++c) a[r][c] -= a[r][i] * a[c][i];
+            }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c)
+                    S[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? a[r][c] : T(0);
         }
         __syncthreads();
-    }
-    for (int idx = tid; idx < TB * TB; idx += nt) {
-        int j = idx / TB, i = idx - j * TB;
-        T v = T(0);
-        if (i >= j) {
-            const T d = sqrt(S[j + j * LD]);
-            v = (i == j) ? d : S[i + j * LD] / d;
+        if (tc == kb && tr > kb) {  // (b)
+            T lk[B][B], rd[B];
+#pragma unroll
+            for (int r = 0; r < B; ++r) {
+                rd[r] = S[TB + (B * kb + r) * LD];
+#pragma unroll
+                for (int c = 0; c < r; ++c) lk[r][c] = S[(B * kb + r) + (B * kb + c) * LD];
+            }
+#pragma unroll
+            for (int c = 0; c < B; ++c)
+#pragma unroll
+                for (int r = 0; r < B; ++r) {
+                    T v = a[r][c];
+#pragma unroll
+                    for (int m = 0; m < c; ++m) v -= a[r][m] * lk[c][m];
+                    a[r][c] = v * rd[c];
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) S[(B * tr + r) + (B * kb + c) * LD] = a[r][c];
         }
-        W[i + j * LD] = v;
+        __syncthreads();
+        if (tc > kb && low) {  // (c)
+            T p[B][B], q[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int m = 0; m < B; ++m) {
+                    p[r][m] = S[(B * tr + r) + (B * kb + m) * LD];
+                    q[r][m] = S[(B * tc + r) + (B * kb + m) * LD];
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c)
+#pragma unroll
+                    for (int m = 0; m < B; ++m) a[r][c] -= p[r][m] * q[c][m];
+        }
+    }
+    // inverse: a becomes this thread's block of X = inv(L)
+#pragma unroll
+    for (int r = 0; r < B; ++r)
+#pragma unroll
+        for (int c = 0; c < B; ++c) a[r][c] = (tr == tc && r == c) ? T(1) : T(0);
+#pragma unroll 1
+    for (int kb = 0; kb < NB; ++kb) {
+        if (tr == kb && tc <= kb) {
+            T lk[B][B], rd[B];
+#pragma unroll
+            for (int r = 0; r < B; ++r) {
+                rd[r] = S[TB + (B * kb + r) * LD];
+#pragma unroll
+                for (int c = 0; c < r; ++c) lk[r][c] = S[(B * kb + r) + (B * kb + c) * LD];
+            }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) {
+                    T v = a[r][c];
+#pragma unroll
+                    for (int m = 0; m < r; ++m) v -= lk[r][m] * a[m][c];
+                    a[r][c] = v * rd[r];
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) W[(B * kb + r) + (B * tc + c) * LD] = a[r][c];
+        }
+        __syncthreads();
+        if (tr > kb && tc <= kb) {
+            T p[B][B], q[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int m = 0; m < B; ++m) {
+                    p[r][m] = S[(B * tr + r) + (B * kb + m) * LD];
+                    q[m][r] = W[(B * kb + m) + (B * tc + r) * LD];
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c)
+#pragma unroll
+                    for (int m = 0; m < B; ++m) a[r][c] -= p[r][m] * q[m][c];
+        }
     }
     __syncthreads();
     for (int idx = tid; idx < TB * TB; idx += nt) {
         int j = idx / TB, i = idx - j * TB;
-        S[i + j * LD] = (i == j) ? T(1) : T(0);
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int p = 0; p < TB - 1; ++p) {
-        if (r > p) {
-            const T lip = W[r + p * LD] / W[p + p * LD];
-#pragma unroll 4
-            for (int c2 = cg; c2 <= p; c2 += 4) S[r + c2 * LD] -= lip * S[p + c2 * LD];
-        }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < TB * TB; idx += nt) {
-        int j = idx / TB, i = idx - j * TB;
-        if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = W[i + j * LD];
-        Dk[idx] = (i >= j && i < n && j < n) ? S[i + j * LD] / W[i + i * LD] : T(0);
+        if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * LD];
+        Dk[idx] = (i >= j && i < n && j < n) ? W[i + j * LD] : T(0);
     }
 }
 

@@ -102,6 +102,10 @@ struct SolveSchedule {
     int* sync = nullptr;
     int nsync = 0, nflags = 0;
     int* err = nullptr;
+    // backward update-row partial sums (see SolveScheduleHost)
+    std::vector<int> gather_task_beg;
+    int* gather_nch = nullptr;
+    int* gather_off = nullptr;
 };
 
 struct DevPlan {
@@ -131,7 +135,10 @@ struct DevPlan {
     std::vector<WorkList> h_assemble;  // per level, offsets into sched64 arrays
     DevSchedule sched64;
     SolveSchedule solve;
-    int64_t fv_total = 0;  // sum of m over supernodes
+    // work vectors per right-hand side: the front vectors (sum of m over
+    // supernodes) followed by the backward gather partials (T rows each)
+    int64_t fv_fronts = 0;
+    int64_t fv_total = 0;
     std::vector<double> h_update_flops;  // per update work list (algorithmic)
     std::vector<double> h_small_bytes;   // per (level, bucket) small-front launch
     Profiler* prof = nullptr;

@@ -340,6 +340,31 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
     }
+    const int GC = SolveScheduleHost::kGatherTiles;
+    S.gather_task_beg.assign(P.nlevels + 1, 0);
+    S.gather_nch.assign(P.nsuper, 0);
+    S.gather_off.assign(P.nsuper, 0);
+    S.gather_vecs = 0;
+    for (int l = 0; l < P.nlevels; ++l) {
+        S.gather_task_beg[l] = (int)(S.tasks.size() / 2);
+        int64_t vecs = 0;
+        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+            const int s = P.large_list[q];
+            const FrontDesc& f = P.fronts[s];
+            const int nt1 = (f.c + T - 1) / T, nu = (f.m - f.c + T - 1) / T;
+            const int nch = (nu + GC - 1) / GC;
+            S.gather_nch[s] = nch;
+            S.gather_off[s] = (int)vecs;
+            vecs += (int64_t)nt1 * nch;
+            for (int j = 0; j < nt1; ++j)
+                for (int h = 0; h < nch; ++h) {
+                    S.tasks.push_back(s);
+                    S.tasks.push_back(j | (h << 16));
+                }
+        }
+        S.gather_vecs = std::max(S.gather_vecs, vecs);
+    }
+    S.gather_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
 }
 
 void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S) {

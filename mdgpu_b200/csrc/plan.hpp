@@ -142,6 +142,15 @@ struct SolveScheduleHost {
     std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read
     std::vector<double> small_elems;              // per level: L elements of its small fronts
     int nflags = 0;                               // one per pivot tile of a large front
+    // backward, update rows: one task per (front, pivot column tile j,
+    // chunk of kGatherTiles update row tiles), packed (s, j | chunk << 16);
+    // each writes a T x nrhs partial sum of L(chunk, j)' x; per front the
+    // chunk count and the first partial (pivot tile j, chunk h at
+    // gather_off + j * gather_nch + h), counted within its level
+    static constexpr int kGatherTiles = 16;
+    std::vector<int> gather_task_beg;   // nlevels + 1, in tasks
+    std::vector<int> gather_nch, gather_off;  // per supernode
+    int64_t gather_vecs = 0;            // partial vectors the largest level needs
 };
 
 int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling

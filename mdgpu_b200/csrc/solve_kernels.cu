@@ -397,18 +397,100 @@ __global__ void __launch_bounds__(256)
     if (tid == 0) st_release_gpu(fl + i, 1);
 }
 
+// Backward, update rows, task (s, j | h << 16): the partial sum
+// L(k, j)' x_k over the update row tiles k of chunk h (kGatherTiles tiles;
+// x final: ancestors, read through the row list) for pivot column tile j,
+// written as a T x nrhs vector for the pivot task to add in chunk order.
+// Threads: l = column in the tile, g = quarter (as in k_bwd_level).
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256)
+    k_bwd_gather(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
+                 const int* __restrict__ rows, const int* __restrict__ gather_nch,
+                 const int* __restrict__ gather_off, const TL* __restrict__ Ls,
+                 const TV* __restrict__ xp, TV* __restrict__ part, int n, int nrhs) {
+    constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TL* Lb = reinterpret_cast<TL*>(smem_raw);
+    TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
+    TV* red = X + T * nrhs;
+    const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
+    const int2 tk = tasks[blockIdx.x];
+    const int s = tk.x, j = tk.y & 0xffff, h = tk.y >> 16;
+    const FrontDesc F = fronts[s];
+    const int nt1 = tiles_l(F.c, T), NT = nt1 + tiles_l(F.m - F.c, T);
+    const TileRange tj = tile_range(j, F.m, F.c, T);
+    const bool lsplit = nrhs == 1;
+    const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;
+    const int* rw = rows + F.rows_off;
+    const int k0 = nt1 + h * GC, k1 = min(NT, k0 + GC);
+    {
+        const TileRange t0 = tile_range(k0, F.m, F.c, T);
+        load_block_async(Lb, Lc + t0.start, F.ldl, t0.size, tj.size);
+    }
+    cp_async_commit_group();
+    TV acc[NQ];
+#pragma unroll
+    for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
+    for (int k = k0; k < k1; ++k) {
+        const int b = k - k0;
+        if (k + 1 < k1) {
+            const TileRange tn = tile_range(k + 1, F.m, F.c, T);
+            load_block_async(Lb + ((b + 1) & 1) * T * LD, Lc + tn.start, F.ldl, tn.size, tj.size);
+        }
+        cp_async_commit_group();
+        const TileRange tkr = tile_range(k, F.m, F.c, T);
+        for (int e = tid; e < T * nrhs; e += blockDim.x) {
+            const int rr = e & (T - 1), q = e / T;
+            X[e] = rr < tkr.size ? xp[rw[tkr.start + rr] + (int64_t)q * n] : TV(0);
+        }
+        cp_async_wait_groups<1>();
+        __syncthreads();
+        const TL* Bk = Lb + (b & 1) * T * LD;
+        if (lsplit) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r) acc[0] += (TV)Bk[(16 * g + r) + l * LD] * X[16 * g + r];
+        } else {
+#pragma unroll 4
+            for (int r = 0; r < T; ++r) {
+                const TV lv = (TV)Bk[r + l * LD];
+#pragma unroll
+                for (int a = 0; a < NQ; ++a) {
+                    const int q = g + 4 * a;
+                    if (q < nrhs) acc[a] += lv * X[r + T * q];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    cp_async_wait_groups<0>();
+    TV* out = part + ((int64_t)gather_off[s] + (int64_t)j * gather_nch[s] + h) * T * nrhs;
+    if (lsplit) {
+        red[g * T + l] = acc[0];
+        __syncthreads();
+        if (g == 0) out[l] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+    } else {
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) {
+            const int q = g + 4 * a;
+            if (q < nrhs) out[l + T * q] = acc[a];
+        }
+    }
+}
+
 // Backward, task (s, j): pivot column tile j of front s accumulates
-// acc = sum_{k > j} L(k, j)' x_k over all row tiles below it -- the update
-// rows first (their x is final: ancestors, read through the row list), then
-// the pivot tiles nt1-1 .. j+1 of this front as they publish (flag 2) -- and
-// solves x_j = inv(L_jj)' (y_j - acc).  Threads: l = column in the tile.
+// acc = sum_{k > j} L(k, j)' x_k over the pivot tiles nt1-1 .. j+1 of this
+// front as they publish (flag 2), adds the update-row partial sums of
+// k_bwd_gather in chunk order, and solves x_j = inv(L_jj)' (y_j - acc).
+// Threads: l = column in the tile.
 template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256)
     k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
                 int ntasks, int* __restrict__ counter, int* __restrict__ flags,
-                int* __restrict__ abort_flag, int* __restrict__ err, const int* __restrict__ rows,
-                const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
-                const TL* __restrict__ Dinv, TV* __restrict__ xp, int n, int nrhs) {
+                int* __restrict__ abort_flag, int* __restrict__ err,
+                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
+                const TV* __restrict__ part, const int64_t* __restrict__ dinv_off,
+                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp, int n,
+                int nrhs) {
     constexpr int T = kTile, LD = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL* Lb = reinterpret_cast<TL*>(smem_raw);
@@ -426,16 +508,15 @@ __global__ void __launch_bounds__(256)
     const int2 tk = tasks[s_task];
     const int s = tk.x, j = tk.y;
     const FrontDesc F = fronts[s];
-    const int nt1 = tiles_l(F.c, T), NT = nt1 + tiles_l(F.m - F.c, T);
+    const int nt1 = tiles_l(F.c, T);
     const TileRange tj = tile_range(j, F.m, F.c, T);
     const bool lsplit = nrhs == 1;
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;  // column tile j
-    const int* rw = rows + F.rows_off;
     int* fl = flags + dinv_off[s] / (T * T);
-    const int nblk = NT - 1 - j;  // row tiles k = NT-1 down to j+1
+    const int nblk = nt1 - 1 - j;  // pivot row tiles k = nt1-1 down to j+1
     load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
     if (nblk > 0) {
-        const TileRange t0 = tile_range(NT - 1, F.m, F.c, T);
+        const TileRange t0 = tile_range(nt1 - 1, F.m, F.c, T);
         load_block_async(Lb, Lc + t0.start, F.ldl, t0.size, tj.size);
     }
     cp_async_commit_group();
@@ -444,31 +525,24 @@ __global__ void __launch_bounds__(256)
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
     bool ok = true;
     for (int b = 0; b < nblk; ++b) {
-        const int k = NT - 1 - b;
+        const int k = nt1 - 1 - b;
         if (b + 1 < nblk) {
             const TileRange tn = tile_range(k - 1, F.m, F.c, T);
             load_block_async(Lb + ((b + 1) & 1) * T * LD, Lc + tn.start, F.ldl, tn.size, tj.size);
         }
         cp_async_commit_group();
         const TileRange tkr = tile_range(k, F.m, F.c, T);
-        if (k < nt1) {
-            if (tid == 0) s_ok = wait_flag(fl + k, 2, abort_flag, err);
-            __syncthreads();
-            if (!s_ok) {
-                ok = false;
-                break;
-            }
-            for (int e = tid; e < T * nrhs; e += blockDim.x) {
-                const int rr = e & (T - 1), q = e / T;
-                X[e] = rr < tkr.size
-                           ? ld_shared_value(xp + F.first_col + tkr.start + rr + (int64_t)q * n)
-                           : TV(0);
-            }
-        } else {
-            for (int e = tid; e < T * nrhs; e += blockDim.x) {
-                const int rr = e & (T - 1), q = e / T;
-                X[e] = rr < tkr.size ? xp[rw[tkr.start + rr] + (int64_t)q * n] : TV(0);
-            }
+        if (tid == 0) s_ok = wait_flag(fl + k, 2, abort_flag, err);
+        __syncthreads();
+        if (!s_ok) {
+            ok = false;
+            break;
+        }
+        for (int e = tid; e < T * nrhs; e += blockDim.x) {
+            const int rr = e & (T - 1), q = e / T;
+            X[e] = rr < tkr.size
+                       ? ld_shared_value(xp + F.first_col + tkr.start + rr + (int64_t)q * n)
+                       : TV(0);
         }
         cp_async_wait_groups<1>();
         __syncthreads();
@@ -496,6 +570,21 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         acc[0] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
         __syncthreads();
+    }
+    {  // update-row partial sums, in chunk order
+        const int nch = gather_nch[s];
+        const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
+        for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
+            if (lsplit) {
+                acc[0] += pj[l];
+            } else {
+#pragma unroll
+                for (int a = 0; a < NQ; ++a) {
+                    const int q = g + 4 * a;
+                    if (q < nrhs) acc[a] += pj[l + T * q];
+                }
+            }
+        }
     }
     // t = y_j - acc (y_j: this front's forward solution), then x_j = Dk' t
     const int64_t xj = F.first_col + tj.start;
@@ -597,6 +686,9 @@ static void set_solve_attributes() {
     cudaFuncSetAttribute(k_bwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
     cudaFuncSetAttribute(k_bwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
     cudaFuncSetAttribute(k_bwd_level<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
 }
 
 void init_solve_kernels() {
@@ -619,10 +711,18 @@ static void launch_level_tasks(bool forward, const DevPlan& D, int l, const TL* 
         k_fwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
                                                      abort_flag, S.err, D.fv_off, D.dinv_off, Ls,
                                                      Dinv, xp, fv, D.n, nrhs);
-    else
+    else {
+        TV* part = fv + D.fv_fronts * nrhs;
+        const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
+        if (ng > 0)
+            k_bwd_gather<TL, TV, NQ><<<ng, 256, smem, st>>>(D.fronts, S.tasks + gb, D.rows,
+                                                          S.gather_nch, S.gather_off, Ls, xp,
+                                                          part, D.n, nrhs);
         k_bwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
-                                                     abort_flag, S.err, D.rows, D.dinv_off, Ls,
-                                                     Dinv, xp, D.n, nrhs);
+                                                     abort_flag, S.err, S.gather_nch,
+                                                     S.gather_off, part, D.dinv_off, Ls, Dinv,
+                                                     xp, D.n, nrhs);
+    }
 }
 
 template <typename TL, typename TV>
