@@ -68,6 +68,7 @@ struct mdgpu_handle_s {
     Plan plan;
     TileSchedule fsched;
     SolveScheduleHost ssched;
+    std::vector<int64_t> pscr_off;  // panel scratch offset per supernode
     PanelSchedule pschedh;
     bool use_tensor_cores = true;
     DevPlan D;
@@ -230,6 +231,21 @@ void upload_plan(mdgpu_handle_s* h) {
     D.fv_total = acc + h->ssched.gather_vecs * kTile;
     D.fv_off = h->keep(upload(fvo));
     D.dinv_off = h->keep(upload(P.dinv_off));
+    {
+        // panel scratch: fronts of one level side by side, levels reuse it
+        h->pscr_off.assign(P.nsuper, -1);
+        D.pscr_total = 0;
+        for (int l = 0; l < P.nlevels; ++l) {
+            int64_t off = 0;
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                const int s = P.large_list[q];
+                h->pscr_off[s] = off;
+                off += 2 * (int64_t)panel_mpad(P.fronts[s].m) * kPanel;
+            }
+            D.pscr_total = std::max(D.pscr_total, off);
+        }
+        D.pscr_off = h->keep(upload(h->pscr_off));
+    }
     D.asm_off = h->keep(upload(P.asm_off));
     D.asm_range = h->keep(upload(P.asm_range));
     D.dinv_total = P.dinv_total;
@@ -344,11 +360,12 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
     } else {
         if (!h->dL32) {
             h->dL32 = dalloc<float>(P.lstore);
-            // TMA descriptors of every large front's FP32 panel (tensor-core path)
+            // split panel scratch and its TMA descriptors (tensor-core path)
             if (h->use_tensor_cores && !P.large_list.empty()) {
+                h->D.pscr = h->keep(dalloc<float>(h->D.pscr_total));
                 std::vector<CUtensorMap> maps;
                 std::vector<int> idx;
-                if (build_panel_maps(P, h->dL32, maps, idx) == 0) {
+                if (build_panel_maps(P, h->D.pscr, h->pscr_off, kPanel, maps, idx) == 0) {
                     h->D.tmaps = h->keep(upload(maps));
                     h->D.tmap_idx = h->keep(upload(idx));
                 }

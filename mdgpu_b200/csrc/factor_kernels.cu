@@ -383,12 +383,18 @@ __device__ void tile_gemm_nt_acc(const T* As, const T* Bs, int K, T (&acc)[4][4]
 }
 
 // X = A_ik inv(L_kk)' in place, CTA per row tile below the panel tile.
+// With a panel scratch (FP32 tensor-core path) X also goes there split for
+// the 3xTF32 Schur update: hi = X with the low 13 mantissa bits cleared (an
+// exact TF32 value), lo = X - hi (exact in FP32); the tile's columns past
+// the last pivot column are written as zeros there, so the update's last
+// K chunk adds nothing.
 template <typename T, int TB>
 __global__ void __launch_bounds__(256)
     k_tile_trsm(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                 const int* __restrict__ before, int nitems, int k,
                 const int64_t* __restrict__ dinv_off, T* __restrict__ Ls,
-                const T* __restrict__ Dinv) {
+                const T* __restrict__ Dinv, float* __restrict__ pscr,
+                const int64_t* __restrict__ pscr_off) {
     static_assert(TB == 64, "4x4 register tile over 256 threads assumes TB = 64");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* As = reinterpret_cast<T*>(smem_raw);  // [K][TB]
@@ -420,6 +426,27 @@ __global__ void __launch_bounds__(256)
         for (int a = 0; a < 4; ++a) {
             int rr = r0 + a;
             if (rr < ti.size) aik[rr + (int64_t)cc * f.ldl] = acc[a][b];
+        }
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (pscr) {
+            const int mpad = panel_mpad(f.m);
+            const int kk0 = (k % (kPanel / TB)) * TB;  // panel column of the tile's first
+            float* hi = pscr + pscr_off[s] + (int64_t)kk0 * (2 * mpad) + ti.start;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int cc = c0 + b;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const int rr = r0 + a;
+                    if (rr >= ti.size) continue;
+                    const float x = cc < K ? acc[a][b] : 0.f;
+                    const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+                    float* p = hi + (int64_t)cc * (2 * mpad) + rr;
+                    p[0] = h;
+                    p[mpad] = x - h;
+                }
+            }
         }
     }
 }
@@ -552,7 +579,7 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
             ProfScope ps(D.prof, KC_TRSM, st);
             k_tile_trsm<T, kTile><<<tr.nctas, 256, gsm, st>>>(
                 D.fronts, S.items + tr.off, S.before + tr.off, tr.nitems, tr.step, D.dinv_off, Ls,
-                Dinv);
+                Dinv, nullptr, nullptr);
         }
         if (up.nctas > 0) {
             ProfScope ps(D.prof, KC_SCHUR, st, D.h_update_flops[q]);
@@ -596,7 +623,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
                 k_tile_trsm<T, kTile><<<w.nctas, 256, gsm, st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, D.dinv_off, Ls,
-                    Dinv);
+                    Dinv, sizeof(T) == 4 ? D.pscr : nullptr, D.pscr_off);
                 break;
             }
             case OP_UPDATE_PANEL: {

@@ -130,6 +130,14 @@ struct DevPlan {
     // panel-wise schedule whose Schur updates run on the tensor cores
     CUtensorMap* tmaps = nullptr;
     int* tmap_idx = nullptr;
+    // FP32 path: the current panel of every large front of a level, split
+    // for the 3xTF32 products: per front 2 * mpad x kPanel floats (column
+    // kk: rows [0, mpad) the TF32 part hi, rows [mpad, 2 mpad) lo = x - hi),
+    // mpad = m rounded up to 128; written by the panel's TRSMs, read by the
+    // tensor-core Schur update through tmaps
+    float* pscr = nullptr;
+    int64_t* pscr_off = nullptr;  // per supernode (-1 if small)
+    int64_t pscr_total = 0;
     DevSchedule psched;
     std::vector<int> h_small_ptr, h_large_ptr;
     std::vector<WorkList> h_assemble;  // per level, offsets into sched64 arrays
@@ -162,8 +170,10 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st);
 
-int build_panel_maps(const Plan& P, const float* Ls, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx);
+// panel scratch rows of a large front (m rounded up to the 128-row tile)
+__host__ __device__ inline int panel_mpad(int m) { return (m + 127) & ~127; }
+int build_panel_maps(const Plan& P, const float* pscr, const std::vector<int64_t>& pscr_off,
+                     int PW, std::vector<CUtensorMap>& maps, std::vector<int>& idx);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,

@@ -5,21 +5,23 @@
 // One CTA computes one 128 x 128 tile (I, J), I >= J, of the trailing part of
 // a large front after a pivot panel of K <= PW (256) columns:
 //     C(I, J) -= A_I * A_J'      A_I = rows 128I.. of the panel columns
-// A_I and A_J are read straight from the column-major FP32 L panel: a 32 x 32
-// TMA box (rows contiguous, 128 bytes per panel column) lands MN-major.  For
-// 32-bit MN-major operands the only UMMA shared-memory layout is the 128-byte
-// swizzle with 32-byte atoms (32-byte chunks of each 128-byte row permuted by
-// row mod 4, atoms of 4 K-rows); the TMA writes exactly that pattern with
-// CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.  Four boxes make a 128-row x 32-column
-// stage of each operand; the K loop runs over 32-column chunks through a
-// 3-stage ring of shared-memory buffers.
+// in 3xTF32: A = hi + lo with hi an exact TF32 value and lo = A - hi, and
+// C -= hi*hi' + hi*lo' + lo*hi' (close to FP32 accuracy, which keeps the
+// iterative refinement short).  The panel's TRSMs write hi and lo into a
+// per-front scratch (column-major, rows hi then lo), so A_I and A_J arrive
+// split: a 32 x 32 TMA box (rows contiguous, 128 bytes per panel column)
+// lands MN-major.  For 32-bit MN-major operands the only UMMA shared-memory
+// layout is the 128-byte swizzle with 32-byte atoms (32-byte chunks of each
+// 128-byte row permuted by row mod 4, atoms of 4 K-rows); the TMA writes
+// exactly that pattern with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.  Four boxes
+// make a 128-row x 32-column operand; a stage holds A_hi, B_hi, A_lo, B_lo,
+// and the K loop runs over 32-column chunks through a 3-stage ring.
 //
-// Roles: thread 0 issues the TMA loads and the MMAs (one thread, the MMA
-// instruction is single-issued per CTA); all 128 threads split each landed
-// stage into TF32 high and low parts (3xTF32: hi*hi + hi*lo + lo*hi, close to
-// FP32 accuracy, which keeps iterative refinement short), then read the
-// accumulator out of TMEM (warp w owns TMEM lanes 32w..32w+31 = tile rows)
-// and subtract it from C in place -- coalesced along the column.
+// Roles: thread 0 issues the TMA loads (refilling a stage once the MMAs that
+// read it have completed), thread 32 issues the MMAs (single-issued per
+// CTA) and commits each stage back to the producer; then all 128 threads
+// read the accumulator out of TMEM (warp w owns TMEM lanes 32w..32w+31 =
+// tile rows) and subtract it from C in place -- coalesced along the column.
 //
 // Every wait on an mbarrier is bounded: on timeout the CTA records an error
 // code in *err, drains what it issued (bounded again), frees its TMEM and
@@ -41,8 +43,8 @@ namespace tc {
 constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3;
 constexpr int BOX = 32;                                   // TMA box: 32 rows x 32 columns (fp32)
 constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes
-constexpr int STAGE_TMA = STAGE_A + STAGE_B;              // bytes the TMA writes per stage
-// per stage: A_hi, B_hi (TMA destination, split in place), A_lo, B_lo
+constexpr int STAGE_TMA = STAGE_A + STAGE_B;              // one of hi / lo: A and B
+// per stage: A_hi, B_hi, then A_lo, B_lo at the same offsets + STAGE_TMA
 constexpr int STAGE_BYTES = 2 * STAGE_TMA;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack
 constexpr uint32_t TMEM_COLS = 128;
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(128, 1)
     __shared__ __align__(8) uint64_t empty_bar[STAGES];
     __shared__ __align__(8) uint64_t done_bar;
     __shared__ uint32_t tmem_base_sh;
-    __shared__ int abort_sh;
+    __shared__ volatile int abort_sh;
 
     // 1024-byte aligned in the shared window (the 128-byte swizzle phase)
     unsigned char* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -173,6 +175,7 @@ __global__ void __launch_bounds__(128, 1)
     const int s = items[it];
     const FrontDesc f = fronts[s];
     const CUtensorMap* map = maps + tmap_idx[s];
+    const int mpad = panel_mpad(f.m);
     // panel columns [k0, k0 + K); trailing columns start at cbeg
     const int k0 = panel * PW;
     const int K = min(PW, f.c - k0);
@@ -203,57 +206,53 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
 
-    // Thread 0 issues TMA loads and MMAs.  Every thread takes part in the
-    // split of each landed stage: x = hi + lo with hi the exact TF32 value
-    // (low 13 mantissa bits cleared, written back in place) and lo = x - hi
-    // (exact in FP32).  The three products hi*hi + hi*lo + lo*hi then give
-    // close to FP32 accuracy on the TF32 tensor pipe ("3xTF32").
-    auto load_chunk = [&](int c) {
-        const int st = c % STAGES;
-        unsigned char* a = smem + st * STAGE_BYTES;
-        unsigned char* b = a + STAGE_A;
-        tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
-        const int col = k0 + c * BK;
-#pragma unroll
-        for (int q = 0; q < BM / BOX; ++q) {
-            tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st], I * BM + q * BOX, col);
-            tc::tma_load_2d(b + q * BOX * BK * 4, map, &full_bar[st], J * BN + q * BOX, col);
-        }
-    };
-    int issued = 0, committed = 0;
-    bool ok = true;
-    if (tid == 0)
-        for (; issued < nk && issued < STAGES; ++issued) load_chunk(issued);
-    for (int c = 0; c < nk; ++c) {
-        const int st = c % STAGES;
-        if (!tc::mbar_wait(&full_bar[st], (c / STAGES) & 1)) ok = false;
-        if (__syncthreads_or(!ok)) {
-            ok = false;
-            break;
-        }
-        // split the landed stage (same swizzled positions in the lo buffers)
-        {
-            float4* hi = reinterpret_cast<float4*>(smem + st * STAGE_BYTES);
-            float4* lo = reinterpret_cast<float4*>(smem + st * STAGE_BYTES + STAGE_TMA);
-#pragma unroll 4
-            for (int v = tid; v < STAGE_TMA / 16; v += 128) {
-                float4 x = hi[v], h, l;
-                h.x = __uint_as_float(__float_as_uint(x.x) & 0xffffe000u);
-                h.y = __uint_as_float(__float_as_uint(x.y) & 0xffffe000u);
-                h.z = __uint_as_float(__float_as_uint(x.z) & 0xffffe000u);
-                h.w = __uint_as_float(__float_as_uint(x.w) & 0xffffe000u);
-                l.x = x.x - h.x;
-                l.y = x.y - h.y;
-                l.z = x.z - h.z;
-                l.w = x.w - h.w;
-                hi[v] = h;
-                lo[v] = l;
+    if (tid == 0) {
+        // producer: A_hi, B_hi, A_lo, B_lo of each 32-column chunk
+        int issued = 0;
+        bool ok = true;
+        for (int ch = 0; ch < nk; ++ch) {
+            const int st = ch % STAGES;
+            if (ch >= STAGES && !tc::mbar_wait(&empty_bar[st], ((ch / STAGES) - 1) & 1)) {
+                ok = false;
+                break;
             }
+            if (abort_sh) break;
+            unsigned char* a = smem + st * STAGE_BYTES;
+            unsigned char* b = a + STAGE_A;
+            tc::mbar_expect_tx(&full_bar[st], STAGE_BYTES);
+            const int col = ch * BK;
+#pragma unroll
+            for (int q = 0; q < BM / BOX; ++q) {
+                const int ra = I * BM + q * BOX, rb = J * BN + q * BOX;
+                tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st], ra, col);
+                tc::tma_load_2d(b + q * BOX * BK * 4, map, &full_bar[st], rb, col);
+                tc::tma_load_2d(a + STAGE_TMA + q * BOX * BK * 4, map, &full_bar[st], mpad + ra,
+                                col);
+                tc::tma_load_2d(b + STAGE_TMA + q * BOX * BK * 4, map, &full_bar[st], mpad + rb,
+                                col);
+            }
+            issued = ch + 1;
         }
-        // make the generic-proxy stores visible to the tensor core's reads
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+        if (!ok) {
+            atomicExch(err, 1);
+            abort_sh = 1;
+        }
+        if (!ok || abort_sh) {
+            // drain: wait (bounded) for the loads already issued
+            for (int ch = 0; ch < issued; ++ch)
+                tc::mbar_wait(&full_bar[ch % STAGES], (ch / STAGES) & 1);
+        }
+    } else if (tid == 32) {
+        // MMA issuer
+        int committed = 0;
+        bool ok = true;
+        for (int ch = 0; ch < nk; ++ch) {
+            const int st = ch % STAGES;
+            if (!tc::mbar_wait(&full_bar[st], (ch / STAGES) & 1)) {
+                ok = false;
+                break;
+            }
+            if (abort_sh) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
             const uint32_t bh = ah + STAGE_A;
@@ -262,37 +261,25 @@ __global__ void __launch_bounds__(128, 1)
             for (int t = 0; t < BK / 8; ++t) {
                 const uint32_t o = t * 1024;
                 tc::mma_tf32(tmem, tc::make_desc(al + o), tc::make_desc(bh + o),
-                             (c > 0 || t > 0) ? 1u : 0u);
+                             (ch > 0 || t > 0) ? 1u : 0u);
                 tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
                 tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
             }
             tc::mma_commit(&empty_bar[st]);
-            committed = c + 1;
-            // refill the stage of the previous chunk once its MMAs are done
-            if (c >= 1 && issued < nk) {
-                const int pc = c - 1, pst = pc % STAGES;
-                if (!tc::mbar_wait(&empty_bar[pst], (pc / STAGES) & 1))
-                    ok = false;
-                else
-                    load_chunk(issued++);
-            }
+            committed = ch + 1;
         }
-    }
-    if (tid == 0) {
-        if (ok) {
-            tc::mma_commit(&done_bar);
-        } else {
+        if (!ok) {
             atomicExch(err, 1);
             abort_sh = 1;
-            // drain: wait (bounded) for the loads already issued
-            for (int c = 0; c < issued; ++c) tc::mbar_wait(&full_bar[c % STAGES], (c / STAGES) & 1);
-            if (committed > 0) tc::mma_commit(&done_bar);
         }
+        // completes once every MMA issued above has (a partial accumulator
+        // after an abort is not written back)
+        if (committed > 0) tc::mma_commit(&done_bar);
     }
     __syncthreads();
-    const bool have_acc = tc::mbar_wait(&done_bar, 0);
+    const bool have_acc = nk > 0 && tc::mbar_wait(&done_bar, 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!have_acc && tid == 0) atomicExch(err, 2);
+    if (!have_acc && nk > 0 && tid == 0) atomicExch(err, 2);
     if (have_acc && !abort_sh) {
         const int row = I * BM + warp * 32 + lane;
 #pragma unroll 1
@@ -347,22 +334,23 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// One tensor map per large front over its FP32 L panel (rows x pivot columns).
-int build_panel_maps(const Plan& P, const float* Ls, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx) {
+// One tensor map per large front over its split panel scratch: 2 * mpad rows
+// (hi then lo) x PW panel columns, column-major.
+int build_panel_maps(const Plan& P, const float* pscr, const std::vector<int64_t>& pscr_off,
+                     int PW, std::vector<CUtensorMap>& maps, std::vector<int>& idx) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return -1;
     maps.resize(P.large_list.size());
     idx.assign(P.nsuper, -1);
     for (size_t q = 0; q < P.large_list.size(); ++q) {
         int s = P.large_list[q];
-        const FrontDesc& f = P.fronts[s];
+        const int mpad = panel_mpad(P.fronts[s].m);
         idx[s] = (int)q;
-        cuuint64_t dims[2] = {(cuuint64_t)f.m, (cuuint64_t)f.c};
-        cuuint64_t strides[1] = {(cuuint64_t)f.ldl * 4};
+        cuuint64_t dims[2] = {(cuuint64_t)(2 * mpad), (cuuint64_t)PW};
+        cuuint64_t strides[1] = {(cuuint64_t)(2 * mpad) * 4};
         cuuint32_t box[2] = {tc::BOX, tc::BK};
         cuuint32_t estr[2] = {1, 1};
-        void* base = const_cast<float*>(Ls + f.loff);
+        void* base = const_cast<float*>(pscr + pscr_off[s]);
         CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
