@@ -9,13 +9,15 @@
 // C -= hi*hi' + hi*lo' + lo*hi' (close to FP32 accuracy, which keeps the
 // iterative refinement short).  The panel's TRSMs write hi and lo into a
 // per-front scratch (column-major, rows hi then lo), so A_I and A_J arrive
-// split: a 32 x 32 TMA box (rows contiguous, 128 bytes per panel column)
+// split: a 32-row x 16-column TMA box (rows contiguous, 128 bytes per panel column)
 // lands MN-major.  For 32-bit MN-major operands the only UMMA shared-memory
 // layout is the 128-byte swizzle with 32-byte atoms (32-byte chunks of each
 // 128-byte row permuted by row mod 4, atoms of 4 K-rows); the TMA writes
 // exactly that pattern with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.  Four boxes
-// make a 128-row x 32-column operand; a stage holds A_hi, B_hi, A_lo, B_lo,
-// and the K loop runs over 32-column chunks through a 3-stage ring.
+// make a 128-row x 16-column operand; a stage holds A_hi, B_hi, A_lo, B_lo
+// (32 KB), and the K loop runs over 16-column chunks through a 3-stage ring
+// (97 KB of shared memory: two CTAs per SM, so one CTA's epilogue overlaps
+// the other's MMAs).
 //
 // Roles: thread 0 issues the TMA loads (refilling a stage once the MMAs that
 // read it have completed), thread 32 issues the MMAs (single-issued per
@@ -40,8 +42,8 @@ namespace mdgpu {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3;
-constexpr int BOX = 32;                                   // TMA box: 32 rows x 32 columns (fp32)
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
+constexpr int BOX = 32;                                   // TMA box: 32 rows x BK columns (fp32)
 constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes
 constexpr int STAGE_TMA = STAGE_A + STAGE_B;              // one of hi / lo: A and B
 // per stage: A_hi, B_hi, then A_lo, B_lo at the same offsets + STAGE_TMA
@@ -96,10 +98,10 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 
 // UMMA shared-memory descriptor: MN-major, 128-byte swizzle with 32-byte
 // atoms (layout type 1).  LBO = distance between 32-element (128 B) blocks
-// along M/N (one TMA box, 32 K-rows x 128 B), SBO = distance between groups
+// along M/N (one TMA box, BK K-rows x 128 B), SBO = distance between groups
 // of 4 K-rows (512 B); version 1 (sm_100).
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-    constexpr uint64_t LBO = 4096, SBO = 512;
+    constexpr uint64_t LBO = BOX * BK * 4, SBO = 512;
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
     d |= (uint64_t)((LBO >> 4) & 0x3FFF) << 16;
@@ -155,7 +157,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // items/before: one entry per large front; the CTAs of a front enumerate the
 // lower 128-tiles (I, J) with J >= J0 = cbeg / 128 in row-major order.
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, const int* __restrict__ tmap_idx,
                const CUtensorMap* __restrict__ maps, int panel, int PW,
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t tmem = tmem_base_sh;
 
     if (tid == 0) {
-        // producer: A_hi, B_hi, A_lo, B_lo of each 32-column chunk
+        // producer: A_hi, B_hi, A_lo, B_lo of each BK-column chunk
         int issued = 0;
         bool ok = true;
         for (int ch = 0; ch < nk; ++ch) {
