@@ -207,6 +207,10 @@ void upload_plan(mdgpu_handle_s* h) {
     D.nsuper = P.nsuper;
     D.nlevels = P.nlevels;
     D.max_u = std::max(P.max_u, 1);
+    for (int s : P.large_list) {
+        D.max_m_large = std::max(D.max_m_large, P.fronts[s].m);
+        D.max_nch_large = std::max(D.max_nch_large, P.fronts[s].child_end - P.fronts[s].child_beg);
+    }
     if ((size_t)D.max_u * sizeof(int) > 227 * 1024)
         throw std::runtime_error("update matrix order exceeds the assembly kernel's shared memory");
     D.fronts = h->keep(upload(P.fronts));

@@ -11,7 +11,7 @@
 
 namespace mdgpu {
 
-constexpr int kAssembleCols = 32;  // columns per CTA in the large-front assembly
+constexpr int kAssembleCols = 16;  // columns per CTA in the large-front assembly
 
 // Kernel classes timed by the profiler.
 enum KernelClass {
@@ -111,6 +111,7 @@ struct SolveSchedule {
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
     int max_u = 0;  // largest update-matrix order (child relative maps in shared memory)
+    int max_m_large = 0, max_nch_large = 0;  // largest large front, most children of one
     FrontDesc* fronts = nullptr;
     int* child = nullptr;
     int* rows = nullptr;
