@@ -37,7 +37,25 @@ import numpy as np  # noqa: E402
 METRIC = "factor+solve time & GFLOP/s, FP32+IR vs FP64 on B200 at backward error <=1e-14"
 UNIT = "GFLOP/s"
 REF_SIDE = 28  # CPU sample of the reference arm (the full 64^3 takes ~12 min on one core)
-CPU_BASELINE_SIDE = 32
+CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, one ncu pass
+# over every launch) of each kernel class in one FP32 bench step at side 64,
+# bytes per step; profiles/dram_traffic_fp32_step_3d64.md holds the capture
+# and its command.  The roofline line divides it by the class's launches.
+TRAFFIC_PER_STEP_3D64 = {
+    "small_front": 501836544, "assemble": 7711001856, "potrf": 12777216, "trsm": 2304483328,
+    "schur_update": 15847656960, "solve_small": 822050816, "solve_large": 6241783296,
+}
+# the kernels behind each profiler class (one class launch = one timed group)
+CLASS_KERNELS = {
+    "small_front": ["k_small_front"],
+    "assemble": ["k_big_assemble_cols"],
+    "potrf": ["k_tile_potrf"],
+    "trsm": ["k_tile_trsm", "k_tile_update"],
+    "schur_update": ["k_schur_tc"],
+    "solve_small": ["k_fwd_small", "k_bwd_small"],
+    "solve_large": ["k_fwd_assemble", "k_fwd_level", "k_bwd_gather", "k_bwd_level"],
+}
 
 
 def parse():
@@ -362,10 +380,19 @@ def run_gpu_arm(args):
             achieved = c["bytes"] / c["launches"] / (c["ms"] / c["launches"] * 1e-3) / 1e9
             unit = "GB/s"
             note = "%s HBM copy bandwidth" % peak_src
-        line["roofline"] = {"kernel": dom, "bound": c["bound"], "achieved": achieved,
+        traffic = None
+        if side == 64 and dom in TRAFFIC_PER_STEP_3D64:
+            traffic = TRAFFIC_PER_STEP_3D64[dom] / c["launches"]
+        line["roofline"] = {"kernel": dom, "kernels": CLASS_KERNELS.get(dom, []),
+                            "bound": c["bound"], "achieved": achieved,
                             "peak": peak, "unit": unit, "frac": achieved / peak,
-                            "traffic": c.get("traffic"), "peak_source": note,
-                            "launches": c["launches"], "ms_total": c["ms"]}
+                            "traffic": traffic,
+                            "algorithmic_bytes_per_launch": c["bytes"] / c["launches"],
+                            "flops_per_launch": c["flops"] / c["launches"],
+                            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                              "one pass over the same workload (bytes per launch)",
+                            "peak_source": note, "launches": c["launches"],
+                            "ms_total": c["ms"]}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = reference_cpu_sample(CPU_BASELINE_SIDE)
     print(json.dumps(line), flush=True)

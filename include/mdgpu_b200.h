@@ -112,9 +112,10 @@ MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, doub
 /*
  * mdgpu_solve_device without any device allocation.  No counterpart in the
  * reference.  For callers that cannot allocate device memory when they solve
- * -- code running while a CUDA graph is captured, host frameworks whose own
- * allocator owns the device memory, loops that cannot afford cudaMalloc's
- * implicit synchronization -- the work vectors come from a fixed 32 MiB
+ * -- host frameworks whose own caching allocator owns the device memory (a
+ * cudaMalloc behind its back can fail or fragment its pool), loops that
+ * cannot afford cudaMalloc's implicit device synchronization -- the work
+ * vectors come from a fixed 32 MiB
  * device array that every GPU loading this library holds until exit (the
  * handle's plan and factor were allocated earlier by mdgpu_analyze and
  * mdgpu_factor).  A call needs (n + w) x min(nrhs, 64) doubles, w =

@@ -2,10 +2,10 @@
 //
 // mdgpu_solve_device allocates its work vectors (permuted right-hand sides and
 // the per-front vectors of the multifrontal sweep) on first use.  Some callers
-// cannot do that at solve time: code running while a CUDA graph is being
-// captured, host frameworks whose own allocator owns all device memory, and
-// latency-bound loops that cannot afford cudaMalloc's implicit device
-// synchronization.  This variant takes its work vectors from a fixed
+// cannot do that at solve time: host frameworks whose own caching allocator
+// owns the device memory (an allocation behind its back can fail or fragment
+// its pool), and latency-bound loops that cannot afford cudaMalloc's
+// implicit device synchronization.  This variant takes its work vectors from a fixed
 // file-scope device array instead.
 //
 // Limits and sharing:

@@ -1,8 +1,8 @@
 """The solve that allocates no device memory (mdgpu_solve_device_noalloc).
 
-For callers that cannot allocate at solve time (inside a CUDA graph capture,
-under a framework whose allocator owns the device memory, or in loops that
-cannot pay cudaMalloc's synchronization), the work vectors come from a fixed
+For callers that cannot allocate at solve time (under a framework whose
+caching allocator owns the device memory, or in loops that cannot pay
+cudaMalloc's implicit synchronization), the work vectors come from a fixed
 32 MiB device array instead of cudaMalloc.  Checked through the C ABI against
 mdgpu_solve_device on two calls in a row (the array keeps the previous call's
 contents), and the size limit is enforced with a clear error.
