@@ -23,112 +23,6 @@ __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) 
 }
 
 // ---------------------------------------------------------------------------
-// small fronts
-// ---------------------------------------------------------------------------
-
-template <typename TL, typename TV>
-__global__ void __launch_bounds__(128)
-    k_fwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
-                const int* __restrict__ child, const int* __restrict__ relmap,
-                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
-                TV* __restrict__ fv, int n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TV* f = reinterpret_cast<TV*>(smem_raw);
-    const int s = list[blockIdx.x];
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const TL* L = Ls + F.loff;
-    for (int idx = tid; idx < m * nrhs; idx += nt) {
-        int q = idx / m, r = idx - q * m;
-        f[idx] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
-    }
-    __syncthreads();
-    for (int h = F.child_beg; h < F.child_end; ++h) {
-        const int ch = child[h];
-        const FrontDesc g = fronts[ch];
-        const int uc = g.m - g.c;
-        const TV* w = front_vec(fv, fv_off, ch, nrhs);
-        const int* rm = relmap + g.rows_off + g.c;
-        for (int idx = tid; idx < uc * nrhs; idx += nt) {
-            int q = idx / uc, r = idx - q * uc;
-            f[rm[r] + q * m] += w[g.c + r + q * g.m];
-        }
-        __syncthreads();
-    }
-    for (int j = 0; j < c; ++j) {
-        const TV inv = TV(1) / (TV)L[j + (int64_t)j * F.ldl];
-        for (int q = tid; q < nrhs; q += nt) f[j + q * m] *= inv;
-        __syncthreads();
-        const int rows = m - j - 1;
-        for (int idx = tid; idx < rows * nrhs; idx += nt) {
-            int q = idx / rows, r = j + 1 + (idx - q * rows);
-            f[r + q * m] -= (TV)L[r + (int64_t)j * F.ldl] * f[j + q * m];
-        }
-        __syncthreads();
-    }
-    TV* out = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < m * nrhs; idx += nt) {
-        int q = idx / m, r = idx - q * m;
-        if (r < c)
-            xp[F.first_col + r + (int64_t)q * n] = f[idx];
-        else
-            out[idx] = f[idx];
-    }
-}
-
-template <typename TL, typename TV>
-__global__ void __launch_bounds__(128)
-    k_bwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
-                const int* __restrict__ rows, const TL* __restrict__ Ls, TV* __restrict__ xp, int n,
-                int nrhs, int umax) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TV* xb = reinterpret_cast<TV*>(smem_raw);  // u x nrhs
-    TV* t = xb + (size_t)umax * nrhs;          // c x nrhs
-    const int s = list[blockIdx.x];
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c, u = m - c;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    const TL* L = Ls + F.loff;
-    const int* rw = rows + F.rows_off + c;
-    for (int idx = tid; idx < u * nrhs; idx += nt) {
-        int q = idx / u, r = idx - q * u;
-        xb[idx] = xp[rw[r] + (int64_t)q * n];
-    }
-    for (int idx = tid; idx < c * nrhs; idx += nt) {
-        int q = idx / c, j = idx - q * c;
-        t[idx] = xp[F.first_col + j + (int64_t)q * n];
-    }
-    __syncthreads();
-    for (int j = warp; j < c; j += nw) {
-        const TL* col = L + c + (int64_t)j * F.ldl;
-        for (int q = 0; q < nrhs; ++q) {
-            TV acc = TV(0);
-            for (int r = lane; r < u; r += 32) acc += (TV)col[r] * xb[r + q * u];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) t[j + q * c] -= acc;
-        }
-    }
-    __syncthreads();
-    for (int j = c - 1; j >= 0; --j) {
-        const TV inv = TV(1) / (TV)L[j + (int64_t)j * F.ldl];
-        for (int q = tid; q < nrhs; q += nt) t[j + q * c] *= inv;
-        __syncthreads();
-        for (int idx = tid; idx < j * nrhs; idx += nt) {
-            int q = idx / j, l = idx - q * j;
-            t[l + q * c] -= (TV)L[j + (int64_t)l * F.ldl] * t[j + q * c];
-        }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < c * nrhs; idx += nt) {
-        int q = idx / c, j = idx - q * c;
-        xp[F.first_col + j + (int64_t)q * n] = t[idx];
-    }
-}
-
-// ---------------------------------------------------------------------------
 // large fronts
 // ---------------------------------------------------------------------------
 
@@ -237,6 +131,196 @@ __device__ __forceinline__ void load_block_async(TL* dst, const TL* src, int64_t
             cp_async_elem(d, src + r + (int64_t)col * ld);
         else
             *d = TL(0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small fronts: CTA per front, the L panel staged in shared memory in blocks
+// of kSmallSolveCols columns (a block of a column-major panel is one
+// contiguous range: 16-byte cp.async, the next block loading while the
+// current one is used)
+// ---------------------------------------------------------------------------
+
+constexpr int kSmallSolveCols = 16;
+
+template <typename TL>
+__device__ __forceinline__ void load_panel_cols_async(TL* dst, const TL* src, int ncols, int ldl) {
+    const int nchunk = (int)((size_t)ncols * ldl * sizeof(TL) / 16);
+    const char* s = reinterpret_cast<const char*>(src);
+    char* d = reinterpret_cast<char*>(dst);
+    for (int q = threadIdx.x; q < nchunk; q += blockDim.x) {
+        const uint32_t da = static_cast<uint32_t>(__cvta_generic_to_shared(d + 16 * (size_t)q));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(da), "l"(s + 16 * (size_t)q)
+                     : "memory");
+    }
+}
+
+// shared memory: front vector (msmall x nrhs) + two panel blocks
+template <typename TL, typename TV>
+__host__ __device__ constexpr size_t small_fwd_smem(int msmall, int nrhs) {
+    return (((size_t)msmall * nrhs * sizeof(TV) + 15) / 16) * 16 +
+           2 * (size_t)kSmallSolveCols * ((msmall + 7) & ~7) * sizeof(TL);
+}
+// shared memory: update-row solution (umax x nrhs) + pivot part (msmall x
+// nrhs) + two panel blocks
+template <typename TL, typename TV>
+__host__ __device__ constexpr size_t small_bwd_smem(int msmall, int umax, int nrhs) {
+    return ((((size_t)umax + msmall) * nrhs * sizeof(TV) + 15) / 16) * 16 +
+           2 * (size_t)kSmallSolveCols * ((msmall + 7) & ~7) * sizeof(TL);
+}
+
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(128)
+    k_fwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
+                const int* __restrict__ child, const int* __restrict__ relmap,
+                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
+                TV* __restrict__ fv, int n, int nrhs, int msmall) {
+    constexpr int CB = kSmallSolveCols;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TV* f = reinterpret_cast<TV*>(smem_raw);
+    TL* Lb = reinterpret_cast<TL*>(smem_raw + (((size_t)msmall * nrhs * sizeof(TV) + 15) / 16) * 16);
+    const int s = list[blockIdx.x];
+    const FrontDesc F = fronts[s];
+    const int m = F.m, c = F.c, ldl = F.ldl;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const TL* L = Ls + F.loff;
+    const int nb = (c + CB - 1) / CB;
+    load_panel_cols_async(Lb, L, min(CB, c), ldl);
+    cp_async_commit_group();
+    for (int idx = tid; idx < m * nrhs; idx += nt) {
+        int q = idx / m, r = idx - q * m;
+        f[idx] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
+    }
+    __syncthreads();
+    for (int h = F.child_beg; h < F.child_end; ++h) {
+        const int ch = child[h];
+        const FrontDesc g = fronts[ch];
+        const int uc = g.m - g.c;
+        const TV* w = front_vec(fv, fv_off, ch, nrhs);
+        const int* rm = relmap + g.rows_off + g.c;
+        for (int idx = tid; idx < uc * nrhs; idx += nt) {
+            int q = idx / uc, r = idx - q * uc;
+            f[rm[r] + q * m] += w[g.c + r + q * g.m];
+        }
+        __syncthreads();
+    }
+    for (int b = 0; b < nb; ++b) {
+        const int j0 = b * CB, j1 = min(c, j0 + CB);
+        if (b + 1 < nb)
+            load_panel_cols_async(Lb + ((b + 1) & 1) * CB * ldl, L + (int64_t)(j0 + CB) * ldl,
+                                  min(CB, c - j0 - CB), ldl);
+        cp_async_commit_group();
+        cp_async_wait_groups<1>();
+        __syncthreads();
+        const TL* Bk = Lb + (b & 1) * CB * ldl;
+        for (int j = j0; j < j1; ++j) {
+            const TL* col = Bk + (j - j0) * ldl;
+            const TV inv = TV(1) / (TV)col[j];
+            for (int q = tid; q < nrhs; q += nt) f[j + q * m] *= inv;
+            __syncthreads();
+            const int rows = m - j - 1;
+            for (int idx = tid; idx < rows * nrhs; idx += nt) {
+                int q = idx / rows, r = j + 1 + (idx - q * rows);
+                f[r + q * m] -= (TV)col[r] * f[j + q * m];
+            }
+            __syncthreads();
+        }
+    }
+    cp_async_wait_groups<0>();
+    TV* out = front_vec(fv, fv_off, s, nrhs);
+    for (int idx = tid; idx < m * nrhs; idx += nt) {
+        int q = idx / m, r = idx - q * m;
+        if (r < c)
+            xp[F.first_col + r + (int64_t)q * n] = f[idx];
+        else
+            out[idx] = f[idx];
+    }
+}
+
+// Backward: t = y - L21' x_u (x_u: the already final update rows), then
+// column blocks from the last: t_B -= L(rows below B in the pivot part, B)'
+// x (dot products, a warp per column), then the block's own triangle from
+// the last column (row j of the block read from the staged columns).
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(128)
+    k_bwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
+                const int* __restrict__ rows, const TL* __restrict__ Ls, TV* __restrict__ xp, int n,
+                int nrhs, int umax, int msmall) {
+    constexpr int CB = kSmallSolveCols;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TV* xb = reinterpret_cast<TV*>(smem_raw);  // u x nrhs
+    TV* t = xb + (size_t)umax * nrhs;          // c x nrhs
+    TL* Lb = reinterpret_cast<TL*>(smem_raw +
+                                   ((((size_t)umax + msmall) * nrhs * sizeof(TV) + 15) / 16) * 16);
+    const int s = list[blockIdx.x];
+    const FrontDesc F = fronts[s];
+    const int m = F.m, c = F.c, u = m - c, ldl = F.ldl;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    const TL* L = Ls + F.loff;
+    const int* rw = rows + F.rows_off + c;
+    const int nb = (c + CB - 1) / CB;
+    {  // last block first
+        const int j0 = (nb - 1) * CB;
+        load_panel_cols_async(Lb + ((nb - 1) & 1) * CB * ldl, L + (int64_t)j0 * ldl, c - j0, ldl);
+    }
+    cp_async_commit_group();
+    for (int idx = tid; idx < u * nrhs; idx += nt) {
+        int q = idx / u, r = idx - q * u;
+        xb[idx] = xp[rw[r] + (int64_t)q * n];
+    }
+    for (int idx = tid; idx < c * nrhs; idx += nt) {
+        int q = idx / c, j = idx - q * c;
+        t[idx] = xp[F.first_col + j + (int64_t)q * n];
+    }
+    __syncthreads();
+    for (int j = warp; j < c; j += nw) {
+        const TL* col = L + c + (int64_t)j * ldl;
+        for (int q = 0; q < nrhs; ++q) {
+            TV acc = TV(0);
+            for (int r = lane; r < u; r += 32) acc += (TV)col[r] * xb[r + q * u];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) t[j + q * c] -= acc;
+        }
+    }
+    for (int b = nb - 1; b >= 0; --b) {
+        const int j0 = b * CB, j1 = min(c, j0 + CB);
+        if (b > 0)
+            load_panel_cols_async(Lb + ((b - 1) & 1) * CB * ldl, L + (int64_t)(j0 - CB) * ldl, CB,
+                                  ldl);
+        cp_async_commit_group();
+        cp_async_wait_groups<1>();
+        __syncthreads();
+        const TL* Bk = Lb + (b & 1) * CB * ldl;
+        // rows [j1, c) of the pivot part are final
+        for (int j = j0 + warp; j < j1; j += nw) {
+            const TL* col = Bk + (j - j0) * ldl;
+            for (int q = 0; q < nrhs; ++q) {
+                TV acc = TV(0);
+                for (int r = j1 + lane; r < c; r += 32) acc += (TV)col[r] * t[r + q * c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) t[j + q * c] -= acc;
+            }
+        }
+        __syncthreads();
+        for (int j = j1 - 1; j >= j0; --j) {
+            const TV inv = TV(1) / (TV)Bk[j + (j - j0) * ldl];
+            for (int q = tid; q < nrhs; q += nt) t[j + q * c] *= inv;
+            __syncthreads();
+            const int w = j - j0;
+            for (int idx = tid; idx < w * nrhs; idx += nt) {
+                int q = idx / w, l = j0 + (idx - q * w);
+                t[l + q * c] -= (TV)Bk[j + (l - j0) * ldl] * t[j + q * c];
+            }
+            __syncthreads();
+        }
+    }
+    cp_async_wait_groups<0>();
+    for (int idx = tid; idx < c * nrhs; idx += nt) {
+        int q = idx / c, j = idx - q * c;
+        xp[F.first_col + j + (int64_t)q * n] = t[idx];
     }
 }
 
@@ -675,10 +759,11 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 
 template <typename TL, typename TV>
 static void set_solve_attributes() {
+    const int ms = Plan::small_limit[kSmallBuckets - 1];
     cudaFuncSetAttribute(k_fwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
+                         (int)small_fwd_smem<TL, TV>(ms, 64));
     cudaFuncSetAttribute(k_bwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
+                         (int)small_bwd_smem<TL, TV>(ms, ms, 64));
     const int lv = (int)level_smem_bytes<TL, TV>(64);
     cudaFuncSetAttribute(k_fwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
     cudaFuncSetAttribute(k_fwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
@@ -740,15 +825,25 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st) {
     const int n = D.n;
-    const int msmall = Plan::small_limit[kSmallBuckets - 1];
     const SolveSchedule& S = D.solve;
+    // rows of the largest small front of a level (its highest non-empty
+    // bucket): sizes the shared memory of that level's small-front launches
+    auto level_msmall = [&](int l) {
+        int ms = Plan::small_limit[0];
+        for (int b = 0; b < kSmallBuckets; ++b)
+            if (D.h_small_ptr[l * kSmallBuckets + b + 1] > D.h_small_ptr[l * kSmallBuckets + b])
+                ms = Plan::small_limit[b];
+        return ms;
+    };
     cudaMemsetAsync(S.sync, 0, (size_t)S.nsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
+        const int msmall = level_msmall(l);
         if (end > beg) {
             ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
-            k_fwd_small<TL, TV><<<end - beg, 128, (size_t)msmall * nrhs * sizeof(TV), st>>>(
-                D.fronts, D.small_list + beg, D.child, D.relmap, D.fv_off, Ls, xp, fv, n, nrhs);
+            k_fwd_small<TL, TV><<<end - beg, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
+                D.fronts, D.small_list + beg, D.child, D.relmap, D.fv_off, Ls, xp, fv, n, nrhs,
+                msmall);
         }
         int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
         if (le > lb) {
@@ -766,11 +861,11 @@ void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv
         }
         int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
         if (end > beg) {
-            int umax = msmall;
-            size_t smem = (size_t)(umax + msmall) * nrhs * sizeof(TV);
+            const int msmall = level_msmall(l);
+            const int umax = msmall;  // u = m - c <= m
             ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
-            k_bwd_small<TL, TV><<<end - beg, 128, smem, st>>>(D.fronts, D.small_list + beg,
-                                                              D.rows, Ls, xp, n, nrhs, umax);
+            k_bwd_small<TL, TV><<<end - beg, 128, small_bwd_smem<TL, TV>(msmall, umax, nrhs), st>>>(
+                D.fronts, D.small_list + beg, D.rows, Ls, xp, n, nrhs, umax, msmall);
         }
     }
 }
