@@ -12,6 +12,8 @@
 // 64-row block of the diagonal block, many CTAs per launch; every CTA applies
 // the block's inverse (stored by the factorization) redundantly -- a 64 x 64
 // product, no serial substitution -- so no launch needs a second phase.
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "kernels.hpp"
 
@@ -27,12 +29,10 @@ __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) 
 // ---------------------------------------------------------------------------
 
 template <typename TV>
-__global__ void __launch_bounds__(256)
-    k_fwd_assemble(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
-                   const int* __restrict__ child, const int* __restrict__ relmap,
-                   const int64_t* __restrict__ fv_off, const TV* __restrict__ xp,
-                   TV* __restrict__ fv, int n, int nrhs) {
-    const int s = list[blockIdx.x];
+__device__ void fwd_assemble_front(int s, const FrontDesc* __restrict__ fronts,
+                                   const int* __restrict__ child, const int* __restrict__ relmap,
+                                   const int64_t* __restrict__ fv_off, const TV* __restrict__ xp,
+                                   TV* __restrict__ fv, int n, int nrhs) {
     const FrontDesc F = fronts[s];
     const int m = F.m, c = F.c;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -170,16 +170,15 @@ __host__ __device__ constexpr size_t small_bwd_smem(int msmall, int umax, int nr
 }
 
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(128)
-    k_fwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
-                const int* __restrict__ child, const int* __restrict__ relmap,
-                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
-                TV* __restrict__ fv, int n, int nrhs, int msmall) {
+__device__ void fwd_small_front(int s, const FrontDesc* __restrict__ fronts,
+                                const int* __restrict__ child, const int* __restrict__ relmap,
+                                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                                TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
+                                int msmall) {
     constexpr int CB = kSmallSolveCols;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TV* f = reinterpret_cast<TV*>(smem_raw);
     TL* Lb = reinterpret_cast<TL*>(smem_raw + (((size_t)msmall * nrhs * sizeof(TV) + 15) / 16) * 16);
-    const int s = list[blockIdx.x];
     const FrontDesc F = fronts[s];
     const int m = F.m, c = F.c, ldl = F.ldl;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -242,17 +241,15 @@ __global__ void __launch_bounds__(128)
 // x (dot products, a warp per column), then the block's own triangle from
 // the last column (row j of the block read from the staged columns).
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(128)
-    k_bwd_small(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
-                const int* __restrict__ rows, const TL* __restrict__ Ls, TV* __restrict__ xp, int n,
-                int nrhs, int umax, int msmall) {
+__device__ void bwd_small_front(int s, const FrontDesc* __restrict__ fronts,
+                                const int* __restrict__ rows, const TL* __restrict__ Ls,
+                                TV* __restrict__ xp, int n, int nrhs, int umax, int msmall) {
     constexpr int CB = kSmallSolveCols;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TV* xb = reinterpret_cast<TV*>(smem_raw);  // u x nrhs
     TV* t = xb + (size_t)umax * nrhs;          // c x nrhs
     TL* Lb = reinterpret_cast<TL*>(smem_raw +
                                    ((((size_t)umax + msmall) * nrhs * sizeof(TV) + 15) / 16) * 16);
-    const int s = list[blockIdx.x];
     const FrontDesc F = fronts[s];
     const int m = F.m, c = F.c, u = m - c, ldl = F.ldl;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -487,18 +484,17 @@ __global__ void __launch_bounds__(256)
 // written as a T x nrhs vector for the pivot task to add in chunk order.
 // Threads: l = column in the tile, g = quarter (as in k_bwd_level).
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
-    k_bwd_gather(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
-                 const int* __restrict__ rows, const int* __restrict__ gather_nch,
-                 const int* __restrict__ gather_off, const TL* __restrict__ Ls,
-                 const TV* __restrict__ xp, TV* __restrict__ part, int n, int nrhs) {
+__device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
+                                const int* __restrict__ rows, const int* __restrict__ gather_nch,
+                                const int* __restrict__ gather_off, const TL* __restrict__ Ls,
+                                const TV* __restrict__ xp, TV* __restrict__ part, int n,
+                                int nrhs) {
     constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL* Lb = reinterpret_cast<TL*>(smem_raw);
     TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = X + T * nrhs;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
-    const int2 tk = tasks[blockIdx.x];
     const int s = tk.x, j = tk.y & 0xffff, h = tk.y >> 16;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T), NT = nt1 + tiles_l(F.m - F.c, T);
@@ -559,6 +555,42 @@ __global__ void __launch_bounds__(256)
             if (q < nrhs) out[l + T * q] = acc[a];
         }
     }
+}
+
+// One launch per level before the large-front chain, forward: the small
+// fronts (CTA each) and the large fronts' vector assembly (CTA each) -- both
+// depend only on lower levels.  Backward: the update-row partial sums of the
+// large fronts and the small fronts -- both depend only on ancestors.
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(256)
+    k_fwd_prep(const FrontDesc* __restrict__ fronts, const int* __restrict__ small_list,
+               int nsmall, const int* __restrict__ large_list, const int* __restrict__ child,
+               const int* __restrict__ relmap, const int64_t* __restrict__ fv_off,
+               const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
+               int msmall) {
+    const int b = blockIdx.x;
+    if (b < nsmall)
+        fwd_small_front<TL, TV>(small_list[b], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
+                                msmall);
+    else
+        fwd_assemble_front<TV>(large_list[b - nsmall], fronts, child, relmap, fv_off, xp, fv, n,
+                               nrhs);
+}
+
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256)
+    k_bwd_prep(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
+               const int* __restrict__ small_list, const int* __restrict__ rows,
+               const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
+               const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ part, int n,
+               int nrhs, int umax, int msmall) {
+    const int b = blockIdx.x;
+    if (b < ngather)
+        bwd_gather_task<TL, TV, NQ>(gtasks[b], fronts, rows, gather_nch, gather_off, Ls, xp, part,
+                                    n, nrhs);
+    else
+        bwd_small_front<TL, TV>(small_list[b - ngather], fronts, rows, Ls, xp, n, nrhs, umax,
+                                msmall);
 }
 
 // Backward, task (s, j): pivot column tile j of front s accumulates
@@ -757,23 +789,24 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 // launch sequence
 // ---------------------------------------------------------------------------
 
+template <typename TL, typename TV, int NQ>
+static void set_solve_attributes_nq() {
+    const int ms = Plan::small_limit[kSmallBuckets - 1];
+    const int lv = (int)level_smem_bytes<TL, TV>(64);
+    const int bp = std::max(lv, (int)small_bwd_smem<TL, TV>(ms, ms, 64));
+    cudaFuncSetAttribute(k_fwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    cudaFuncSetAttribute(k_bwd_prep<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, bp);
+}
+
 template <typename TL, typename TV>
 static void set_solve_attributes() {
     const int ms = Plan::small_limit[kSmallBuckets - 1];
-    cudaFuncSetAttribute(k_fwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_fwd_prep<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)small_fwd_smem<TL, TV>(ms, 64));
-    cudaFuncSetAttribute(k_bwd_small<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)small_bwd_smem<TL, TV>(ms, ms, 64));
-    const int lv = (int)level_smem_bytes<TL, TV>(64);
-    cudaFuncSetAttribute(k_fwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_fwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_fwd_level<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_level<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_level<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_level<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_gather<TL, TV, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
+    set_solve_attributes_nq<TL, TV, 1>();
+    set_solve_attributes_nq<TL, TV, 4>();
+    set_solve_attributes_nq<TL, TV, 16>();
 }
 
 void init_solve_kernels() {
@@ -781,93 +814,82 @@ void init_solve_kernels() {
     set_solve_attributes<float, double>();
 }
 
+// rows of the largest small front of a level (its highest non-empty bucket):
+// sizes the shared memory of that level's small-front work
+static int level_msmall(const DevPlan& D, int l) {
+    int ms = Plan::small_limit[0];
+    for (int b = 0; b < kSmallBuckets; ++b)
+        if (D.h_small_ptr[l * kSmallBuckets + b + 1] > D.h_small_ptr[l * kSmallBuckets + b])
+            ms = Plan::small_limit[b];
+    return ms;
+}
+
+// One level of the solve: forward -- small fronts with the large fronts'
+// assembly, then the large-front chain; backward -- update-row gathers with
+// the small fronts, then the large-front chain.
 template <typename TL, typename TV, int NQ>
-static void launch_level_tasks(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
-                               TV* xp, TV* fv, int nrhs, cudaStream_t st) {
+static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
+                        TV* xp, TV* fv, int nrhs, cudaStream_t st) {
     const SolveSchedule& S = D.solve;
+    const int n = D.n;
+    const int sb = D.h_small_ptr[l * kSmallBuckets], se = D.h_small_ptr[(l + 1) * kSmallBuckets];
+    const int ns = se - sb;
+    const int lb = D.h_large_ptr[l], nl = D.h_large_ptr[l + 1] - lb;
+    const int msmall = level_msmall(D, l);
+    const size_t lsm = level_smem_bytes<TL, TV>(nrhs);
     const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
-    if (nt == 0) return;
-    const size_t smem = level_smem_bytes<TL, TV>(nrhs);
     int* counter = S.sync + 2 * l + (forward ? 0 : 1);
     int* flags = S.sync + 2 * D.nlevels;
     int* abort_flag = flags + S.nflags;
-    if (forward)
-        k_fwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
-                                                     abort_flag, S.err, D.fv_off, D.dinv_off, Ls,
-                                                     Dinv, xp, fv, D.n, nrhs);
-    else {
+    const double bytes =
+        (S.small_elems[l] + (forward ? S.fwd_elems[l] : S.bwd_elems[l])) * sizeof(TL);
+    ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
+    if (forward) {
+        if (ns + nl > 0)
+            k_fwd_prep<TL, TV><<<ns + nl, 256, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
+                D.fronts, D.small_list + sb, ns, D.large_list + lb, D.child, D.relmap, D.fv_off,
+                Ls, xp, fv, n, nrhs, msmall);
+        if (nt > 0)
+            k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
+                                                        flags, abort_flag, S.err, D.fv_off,
+                                                        D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
+    } else {
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
-        if (ng > 0)
-            k_bwd_gather<TL, TV, NQ><<<ng, 256, smem, st>>>(D.fronts, S.tasks + gb, D.rows,
-                                                          S.gather_nch, S.gather_off, Ls, xp,
-                                                          part, D.n, nrhs);
-        k_bwd_level<TL, TV, NQ><<<nt, 256, smem, st>>>(D.fronts, S.tasks + t0, nt, counter, flags,
-                                                     abort_flag, S.err, S.gather_nch,
-                                                     S.gather_off, part, D.dinv_off, Ls, Dinv,
-                                                     xp, D.n, nrhs);
+        if (ng + ns > 0) {
+            size_t sm = small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
+            if (ng > 0) sm = std::max(sm, lsm);
+            k_bwd_prep<TL, TV, NQ><<<ng + ns, 256, sm, st>>>(
+                D.fronts, S.tasks + gb, ng, D.small_list + sb, D.rows, S.gather_nch, S.gather_off,
+                Ls, xp, part, n, nrhs, msmall, msmall);
+        }
+        if (nt > 0)
+            k_bwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
+                                                        flags, abort_flag, S.err, S.gather_nch,
+                                                        S.gather_off, part, D.dinv_off, Ls, Dinv,
+                                                        xp, n, nrhs);
     }
 }
 
-template <typename TL, typename TV>
-static void launch_level(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
-                         TV* xp, TV* fv, int nrhs, cudaStream_t st) {
-    if (nrhs <= 4)
-        launch_level_tasks<TL, TV, 1>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
-    else if (nrhs <= 16)
-        launch_level_tasks<TL, TV, 4>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
-    else
-        launch_level_tasks<TL, TV, 16>(forward, D, l, Ls, Dinv, xp, fv, nrhs, st);
+template <typename TL, typename TV, int NQ>
+static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv,
+                            int nrhs, cudaStream_t st) {
+    cudaMemsetAsync(D.solve.sync, 0, (size_t)D.solve.nsync * sizeof(int), st);
+    for (int l = 0; l < D.nlevels; ++l) solve_level<TL, TV, NQ>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
+    for (int l = D.nlevels - 1; l >= 0; --l)
+        solve_level<TL, TV, NQ>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
 }
 
 template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st) {
-    const int n = D.n;
-    const SolveSchedule& S = D.solve;
-    // rows of the largest small front of a level (its highest non-empty
-    // bucket): sizes the shared memory of that level's small-front launches
-    auto level_msmall = [&](int l) {
-        int ms = Plan::small_limit[0];
-        for (int b = 0; b < kSmallBuckets; ++b)
-            if (D.h_small_ptr[l * kSmallBuckets + b + 1] > D.h_small_ptr[l * kSmallBuckets + b])
-                ms = Plan::small_limit[b];
-        return ms;
-    };
-    cudaMemsetAsync(S.sync, 0, (size_t)S.nsync * sizeof(int), st);
-    for (int l = 0; l < D.nlevels; ++l) {
-        int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
-        const int msmall = level_msmall(l);
-        if (end > beg) {
-            ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
-            k_fwd_small<TL, TV><<<end - beg, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
-                D.fronts, D.small_list + beg, D.child, D.relmap, D.fv_off, Ls, xp, fv, n, nrhs,
-                msmall);
-        }
-        int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
-        if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.fwd_elems[l] * sizeof(TL));
-            k_fwd_assemble<TV><<<le - lb, 256, 0, st>>>(D.fronts, D.large_list + lb, D.child,
-                                                        D.relmap, D.fv_off, xp, fv, n, nrhs);
-            launch_level<TL, TV>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
-        }
-    }
-    for (int l = D.nlevels - 1; l >= 0; --l) {
-        int lb = D.h_large_ptr[l], le = D.h_large_ptr[l + 1];
-        if (le > lb) {
-            ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, S.bwd_elems[l] * sizeof(TL));
-            launch_level<TL, TV>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
-        }
-        int beg = D.h_small_ptr[l * kSmallBuckets], end = D.h_small_ptr[(l + 1) * kSmallBuckets];
-        if (end > beg) {
-            const int msmall = level_msmall(l);
-            const int umax = msmall;  // u = m - c <= m
-            ProfScope ps(D.prof, KC_SOLVE_SMALL, st, 0, S.small_elems[l] * sizeof(TL));
-            k_bwd_small<TL, TV><<<end - beg, 128, small_bwd_smem<TL, TV>(msmall, umax, nrhs), st>>>(
-                D.fronts, D.small_list + beg, D.rows, Ls, xp, n, nrhs, umax, msmall);
-        }
-    }
+    if (nrhs <= 4)
+        solve_levels_nq<TL, TV, 1>(D, Ls, Dinv, xp, fv, nrhs, st);
+    else if (nrhs <= 16)
+        solve_levels_nq<TL, TV, 4>(D, Ls, Dinv, xp, fv, nrhs, st);
+    else
+        solve_levels_nq<TL, TV, 16>(D, Ls, Dinv, xp, fv, nrhs, st);
 }
 
 template void solve_levels<double, double>(const DevPlan&, const double*, const double*, double*,
