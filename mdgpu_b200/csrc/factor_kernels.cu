@@ -270,16 +270,19 @@ __global__ void __launch_bounds__(256)
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
 // column-major, zero above the diagonal) at Dk.  The 256 threads form a
 // 16 x 16 grid; thread (tr, tc), tr >= tc, keeps the 4 x 4 block (tr, tc) of
-// the tile in registers.  Sixteen blocked steps of right-looking Cholesky:
-//   (a) the diagonal owner factors its 4 x 4 block in registers;
-//   (b) the owners below it solve X L_kk' = A (their block of the panel);
-//   (c) every lower block right of the panel takes the rank-4 update;
-// with L going to S block by block (two barriers per step).  Then the
-// inverse by block rows: owners of block row kb apply inv(L_kk) to their
-// accumulated blocks (final rows of inv(L), to W), and the blocks below
-// subtract L(tr, kb) X(kb, tc) (one barrier per step).  One division per
-// pivot: its reciprocal waits in S's padding row (row TB) for the solves.
+// the tile in registers, and its block of X = inv(L).  Sixteen blocked steps
+// (two barriers each) of right-looking Cholesky with the inverse alongside:
+//   (a) the diagonal owner factors its 4 x 4 block and inverts it (Y);
+//   (b) the owners below it form their panel block A Y'; at the same time
+//       the owners of block row kb of X finalise it, X(kb, tc) = Y x;
+//   (c) every lower block right of the panel takes the rank-4 update; at the
+//       same time the X blocks below take x -= L(tr, kb) X(kb, tc);
+// with L going to S and X to W block by block.  One reciprocal square root
+// per pivot.
 // A partial tile (n < 64) is padded with the identity.  S, W: TB x (TB + 1).
+__device__ __forceinline__ float recip_sqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double recip_sqrt(double x) { return rsqrt(x); }
+
 template <typename T, int TB>
 __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
                                 int* status) {
@@ -299,23 +302,27 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
         S[i + j * LD] = v;
     }
     __syncthreads();
-    T a[B][B];
+    T a[B][B], x[B][B];  // this thread's block of A -> L, and of inv(L)
 #pragma unroll
     for (int r = 0; r < B; ++r)
 #pragma unroll
-        for (int c = 0; c < B; ++c) a[r][c] = low ? S[(B * tr + r) + (B * tc + c) * LD] : T(0);
+        for (int c = 0; c < B; ++c) {
+            a[r][c] = low ? S[(B * tr + r) + (B * tc + c) * LD] : T(0);
+            x[r][c] = (tr == tc && r == c) ? T(1) : T(0);
+        }
     __syncthreads();
 #pragma unroll 1
     for (int kb = 0; kb < NB; ++kb) {
-        if (tr == kb && tc == kb) {  // (a)
+        if (tr == kb && tc == kb) {  // (a) L_kk and its inverse Y = X(kb, kb)
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 const T piv = a[i][i];
                 if (B * kb + i < n && !(piv > T(0))) flag_pivot(status, col0 + B * kb + i);
-                const T d = sqrt(piv);
-                const T rd = T(1) / d;
+                // one reciprocal square root per pivot: d = piv / sqrt(piv)
+                const T rd = recip_sqrt(piv);
+                const T d = piv * rd;
                 a[i][i] = d;
-                S[TB + (B * kb + i) * LD] = rd;  // padding row: reciprocal pivots
+                x[i][i] = rd;  // diagonal of Y
 #pragma unroll
                 for (int r = i + 1; r < B; ++r) a[r][i] *= rd;
 #pragma unroll
@@ -323,37 +330,74 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
 #pragma unroll
                     for (int c = i + 1; c <= r; ++c) a[r][c] -= a[r][i] * a[c][i];
             }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c)
-                    S[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? a[r][c] : T(0);
-        }
-        __syncthreads();
-        if (tc == kb && tr > kb) {  // (b)
-            T lk[B][B], rd[B];
-#pragma unroll
-            for (int r = 0; r < B; ++r) {
-                rd[r] = S[TB + (B * kb + r) * LD];
-#pragma unroll
-                for (int c = 0; c < r; ++c) lk[r][c] = S[(B * kb + r) + (B * kb + c) * LD];
-            }
+            // Y = inv(L_kk) by forward substitution, column by column
 #pragma unroll
             for (int c = 0; c < B; ++c)
 #pragma unroll
-                for (int r = 0; r < B; ++r) {
-                    T v = a[r][c];
+                for (int r = c + 1; r < B; ++r) {
+                    T v = T(0);
 #pragma unroll
-                    for (int m = 0; m < c; ++m) v -= a[r][m] * lk[c][m];
-                    a[r][c] = v * rd[c];
+                    for (int m = c; m < r; ++m) v -= a[r][m] * x[m][c];
+                    x[r][c] = v * x[r][r];
                 }
 #pragma unroll
             for (int r = 0; r < B; ++r)
 #pragma unroll
-                for (int c = 0; c < B; ++c) S[(B * tr + r) + (B * kb + c) * LD] = a[r][c];
+                for (int c = 0; c < B; ++c) {
+                    S[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? a[r][c] : T(0);
+                    W[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? x[r][c] : T(0);
+                }
         }
         __syncthreads();
-        if (tc > kb && low) {  // (c)
+        if (tc == kb && tr > kb) {  // (b) panel block: A Y'
+            T y[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) y[r][c] = W[(B * kb + r) + (B * kb + c) * LD];
+            T o[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) {
+                    T v = T(0);
+#pragma unroll
+                    for (int m = 0; m <= c; ++m) v += a[r][m] * y[c][m];
+                    o[r][c] = v;
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) {
+                    a[r][c] = o[r][c];
+                    S[(B * tr + r) + (B * kb + c) * LD] = o[r][c];
+                }
+        } else if (tr == kb && tc < kb) {  // (b) inverse block row kb: X = Y x
+            T y[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) y[r][c] = W[(B * kb + r) + (B * kb + c) * LD];
+            T o[B][B];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) {
+                    T v = T(0);
+#pragma unroll
+                    for (int m = 0; m <= r; ++m) v += y[r][m] * x[m][c];
+                    o[r][c] = v;
+                }
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B; ++c) {
+                    x[r][c] = o[r][c];
+                    W[(B * kb + r) + (B * tc + c) * LD] = o[r][c];
+                }
+        }
+        __syncthreads();
+        if (tc > kb && low) {  // (c) trailing update with the panel
             T p[B][B], q[B][B];
 #pragma unroll
             for (int r = 0; r < B; ++r)
@@ -368,39 +412,7 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
                 for (int c = 0; c < B; ++c)
 #pragma unroll
                     for (int m = 0; m < B; ++m) a[r][c] -= p[r][m] * q[c][m];
-        }
-    }
-    // inverse: a becomes this thread's block of X = inv(L)
-#pragma unroll
-    for (int r = 0; r < B; ++r)
-#pragma unroll
-        for (int c = 0; c < B; ++c) a[r][c] = (tr == tc && r == c) ? T(1) : T(0);
-#pragma unroll 1
-    for (int kb = 0; kb < NB; ++kb) {
-        if (tr == kb && tc <= kb) {
-            T lk[B][B], rd[B];
-#pragma unroll
-            for (int r = 0; r < B; ++r) {
-                rd[r] = S[TB + (B * kb + r) * LD];
-#pragma unroll
-                for (int c = 0; c < r; ++c) lk[r][c] = S[(B * kb + r) + (B * kb + c) * LD];
-            }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    T v = a[r][c];
-#pragma unroll
-                    for (int m = 0; m < r; ++m) v -= lk[r][m] * a[m][c];
-                    a[r][c] = v * rd[r];
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) W[(B * kb + r) + (B * tc + c) * LD] = a[r][c];
-        }
-        __syncthreads();
-        if (tr > kb && tc <= kb) {
+        } else if (tr > kb && tc <= kb) {  // (c) inverse rows below: x -= L(tr, kb) X(kb, tc)
             T p[B][B], q[B][B];
 #pragma unroll
             for (int r = 0; r < B; ++r)
@@ -414,7 +426,7 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
 #pragma unroll
                 for (int c = 0; c < B; ++c)
 #pragma unroll
-                    for (int m = 0; m < B; ++m) a[r][c] -= p[r][m] * q[m][c];
+                    for (int m = 0; m < B; ++m) x[r][c] -= p[r][m] * q[m][c];
         }
     }
     __syncthreads();
