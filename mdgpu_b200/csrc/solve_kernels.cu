@@ -321,6 +321,13 @@ __device__ void bwd_small_front(int s, const FrontDesc* __restrict__ fronts,
     }
 }
 
+// the update-row gather: two L blocks (double buffer), x rows, partials
+template <typename TL, typename TV>
+__host__ __device__ constexpr size_t gather_smem_bytes(int nrhs) {
+    return ((2 * (size_t)kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
+           ((size_t)kTile * nrhs + 4 * kTile) * sizeof(TV);
+}
+
 template <typename TL, typename TV>
 __host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
     return ((3 * (size_t)kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
@@ -492,7 +499,7 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL* Lb = reinterpret_cast<TL*>(smem_raw);
-    TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
+    TV* X = reinterpret_cast<TV*>(smem_raw + ((2 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = X + T * nrhs;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
     const int s = tk.x, j = tk.y & 0xffff, h = tk.y >> 16;
@@ -557,7 +564,8 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
 }
 
-// One launch per level before the large-front chain, forward: the small
+// One launch per level before the large-front chain (128 threads, 256 when
+// it holds gather tasks), forward: the small
 // fronts (CTA each) and the large fronts' vector assembly (CTA each) -- both
 // depend only on lower levels.  Backward: the update-row partial sums of the
 // large fronts and the small fronts -- both depend only on ancestors.
@@ -847,7 +855,7 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
     if (forward) {
         if (ns + nl > 0)
-            k_fwd_prep<TL, TV><<<ns + nl, 256, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
+            k_fwd_prep<TL, TV><<<ns + nl, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
                 D.fronts, D.small_list + sb, ns, D.large_list + lb, D.child, D.relmap, D.fv_off,
                 Ls, xp, fv, n, nrhs, msmall);
         if (nt > 0)
@@ -859,8 +867,9 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
         if (ng + ns > 0) {
             size_t sm = small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
-            if (ng > 0) sm = std::max(sm, lsm);
-            k_bwd_prep<TL, TV, NQ><<<ng + ns, 256, sm, st>>>(
+            if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
+            // the gather's thread layout needs 256 threads; small fronts alone run on 128
+            k_bwd_prep<TL, TV, NQ><<<ng + ns, ng > 0 ? 256 : 128, sm, st>>>(
                 D.fronts, S.tasks + gb, ng, D.small_list + sb, D.rows, S.gather_nch, S.gather_off,
                 Ls, xp, part, n, nrhs, msmall, msmall);
         }
