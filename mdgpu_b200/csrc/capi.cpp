@@ -207,6 +207,10 @@ void upload_plan(mdgpu_handle_s* h) {
     D.nsuper = P.nsuper;
     D.nlevels = P.nlevels;
     D.max_u = std::max(P.max_u, 1);
+    D.h_level_max_m.assign(P.nlevels, 0);
+    for (int l = 0; l < P.nlevels; ++l)
+        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q)
+            D.h_level_max_m[l] = std::max(D.h_level_max_m[l], P.fronts[P.large_list[q]].m);
     for (int s : P.large_list) {
         D.max_m_large = std::max(D.max_m_large, P.fronts[s].m);
         D.max_nch_large = std::max(D.max_nch_large, P.fronts[s].child_end - P.fronts[s].child_beg);

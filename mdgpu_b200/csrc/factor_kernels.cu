@@ -263,6 +263,83 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Warp-per-column variant, for levels whose fronts are short enough that
+// every warp of the CTA holds a column of its own in shared memory: no block
+// barriers, only warp syncs.  A child's columns landing in the CTA's block
+// are at most CB (the relative map is injective), so the child column that
+// lands in parent column jj is found by one ballot over the child's range.
+// Same sums in the same order as k_big_assemble_cols.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_big_assemble_warp(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+                        const int* __restrict__ before, int nitems, int CB,
+                        const int* __restrict__ child, const int* __restrict__ relmap,
+                        const int* __restrict__ a_src, const int* __restrict__ a_pos,
+                        const int* __restrict__ a_colptr, const int* __restrict__ a_colptr_off,
+                        const int* __restrict__ asm_off, const int* __restrict__ asm_range,
+                        const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
+                        int ldbuf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    T* colbuf = reinterpret_cast<T*>(smem_raw) + (size_t)warp * ldbuf;
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it];
+    const int blk = blockIdx.x - before[it];
+    const FrontDesc f = fronts[s];
+    const int j0 = blk * CB, j1 = min(j0 + CB, f.m);
+    const int nch = f.child_end - f.child_beg;
+    const int* ranges = asm_range + asm_off[s] + blk * nch * 2;
+    const int* cp = j0 < f.c ? a_colptr + a_colptr_off[s] : nullptr;
+    for (int jj = j0 + warp; jj < j1; jj += nw) {
+        const bool inL = jj < f.c;
+        const int rlo = inL ? 0 : jj;
+        for (int r = rlo + lane; r < f.m; r += 32) colbuf[r] = T(0);
+        __syncwarp();
+        if (inL) {
+            const int e0 = f.a_beg + cp[jj], e1 = f.a_beg + cp[jj + 1];
+            for (int e = e0 + lane; e < e1; e += 32) {
+                const int src = a_src[e];
+                if (src >= 0) colbuf[a_pos[e] & 0xffff] = (T)Ax[src];
+            }
+            __syncwarp();
+        }
+        for (int h = 0; h < nch; ++h) {
+            const int jlo = ranges[2 * h], jhi = ranges[2 * h + 1];
+            if (jlo == jhi) continue;
+            const FrontDesc g = fronts[child[f.child_beg + h]];
+            const int* rm = relmap + g.rows_off + g.c;
+            const int cand = jlo + lane;
+            const unsigned hit = __ballot_sync(0xffffffffu, cand < jhi && __ldg(rm + cand) == jj);
+            if (!hit) continue;
+            const int jc = jlo + __ffs(hit) - 1;
+            const int uc = g.m - g.c;
+            const T* ucol = Us + g.uoff + (int64_t)jc * g.ldu;
+            for (int ic0 = jc + lane; ic0 < uc; ic0 += 8 * 32) {
+                int pr[8];
+                T v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int ic = ic0 + u * 32;
+                    pr[u] = ic < uc ? __ldg(rm + ic) : -1;
+                    v[u] = ic < uc ? __ldg(ucol + ic) : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (pr[u] >= 0) colbuf[pr[u]] += v[u];
+            }
+            __syncwarp();
+        }
+        if (inL) {
+            T* col = Ls + f.loff + (int64_t)jj * f.ldl;
+            for (int r = lane; r < f.m; r += 32) col[r] = colbuf[r];
+        } else {
+            T* col = Us + f.uoff + (int64_t)(jj - f.c) * f.ldu;
+            for (int r = jj + lane; r < f.m; r += 32) col[r - f.c] = colbuf[r];
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // large fronts: tiles
 // ---------------------------------------------------------------------------
@@ -709,7 +786,17 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
             case OP_ASSEMBLE: {
                 ProfScope ps(D.prof, KC_ASSEMBLE, st, 0, op.elems * sizeof(T) + op.xbytes);
                 const size_t csm = assemble_cols_smem<T>(D);
-                if (csm <= kAssembleColsSmemMax)
+                // warps per CTA that get a column buffer of this level's tallest front
+                const int ldbuf = (D.h_level_max_m[level] + 3) & ~3;
+                const int nwarps = (int)std::min<size_t>(
+                    8, kAssembleColsSmemMax / ((size_t)ldbuf * sizeof(T)));
+                if (nwarps >= 4)
+                    k_big_assemble_warp<T><<<w.nctas, 32 * nwarps,
+                                             (size_t)nwarps * ldbuf * sizeof(T), st>>>(
+                        D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols,
+                        D.child, D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off,
+                        D.asm_off, D.asm_range, Ax, Ls, Us, ldbuf);
+                else if (csm <= kAssembleColsSmemMax)
                     k_big_assemble_cols<T><<<w.nctas, 256, csm, st>>>(
                         D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols,
                         D.child, D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off,
@@ -766,6 +853,8 @@ static void set_factor_attributes() {
     cudaFuncSetAttribute(k_big_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          227 * 1024);
     cudaFuncSetAttribute(k_big_assemble_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kAssembleColsSmemMax);
+    cudaFuncSetAttribute(k_big_assemble_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kAssembleColsSmemMax);
 }
 

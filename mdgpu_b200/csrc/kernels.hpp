@@ -112,6 +112,7 @@ struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
     int max_u = 0;  // largest update-matrix order (child relative maps in shared memory)
     int max_m_large = 0, max_nch_large = 0;  // largest large front, most children of one
+    std::vector<int> h_level_max_m;          // per level: largest large front
     FrontDesc* fronts = nullptr;
     int* child = nullptr;
     int* rows = nullptr;
