@@ -236,7 +236,8 @@ void upload_plan(mdgpu_handle_s* h) {
         acc += P.fronts[s].m;
     }
     D.fv_fronts = acc;
-    D.fv_total = acc + h->ssched.gather_vecs * kTile;
+    D.fv_pub_off = acc + h->ssched.gather_vecs * kTile;
+    D.fv_total = D.fv_pub_off + 2 * (int64_t)h->ssched.nflags * kTile;
     D.fv_off = h->keep(upload(fvo));
     D.dinv_off = h->keep(upload(P.dinv_off));
     {

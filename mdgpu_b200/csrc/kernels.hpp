@@ -146,8 +146,10 @@ struct DevPlan {
     DevSchedule sched64;
     SolveSchedule solve;
     // work vectors per right-hand side: the front vectors (sum of m over
-    // supernodes) followed by the backward gather partials (T rows each)
+    // supernodes), the backward gather partials (T rows each), then the
+    // publication slots of the pivot tiles (T rows each, forward then backward)
     int64_t fv_fronts = 0;
+    int64_t fv_pub_off = 0;
     int64_t fv_total = 0;
     std::vector<double> h_update_flops;  // per update work list (algorithmic)
     std::vector<double> h_small_bytes;   // per (level, bucket) small-front launch

@@ -102,6 +102,51 @@ __device__ bool wait_flag(const int* flag, int target, int* abort_flag, int* err
     return false;
 }
 
+// Published pivot-tile values: every slot starts as the all-ones bit pattern
+// (a NaN that arithmetic never produces), and a producer stores final values
+// only (aligned 8-byte stores are single-copy atomic), so a consumer that
+// sees no sentinel has the data: one round trip instead of flag then data.
+// All threads poll together (uniform result); iteration limit as wait_flag.
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ bool is_unpublished(double v) {
+    return __double_as_longlong(v) == -1ll;
+}
+__device__ bool poll_published(double* dst, const double* src, int nk, int nrhs, int* abort_flag,
+                               int* err) {
+    constexpr int T = kTile;
+    __shared__ int s_abort[2];
+    for (int it = 0; it < kSolveWaitPolls; ++it) {
+        bool mine = true;
+        for (int e = threadIdx.x; e < T * nrhs; e += blockDim.x) {
+            if ((e & (T - 1)) < nk) {
+                const double v = ld_relaxed_f64(src + e);
+                if (is_unpublished(v))
+                    mine = false;
+                else
+                    dst[e] = v;
+            } else {
+                dst[e] = 0.0;
+            }
+        }
+        if (threadIdx.x == 0) s_abort[it & 1] = ld_relaxed_gpu(abort_flag);
+        if (__syncthreads_and(mine)) return true;
+        if (s_abort[it & 1]) return false;
+        __nanosleep(32);
+    }
+    if (threadIdx.x == 0) {
+        atomicExch(abort_flag, 1);
+        atomicOr(err, 1);
+    }
+    return false;
+}
+
 template <typename TL>
 __device__ __forceinline__ void cp_async_elem(TL* dst, const TL* src) {
     const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
@@ -344,7 +389,7 @@ __host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
 template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256)
     k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
-                int ntasks, int* __restrict__ counter, int* __restrict__ flags,
+                int ntasks, int* __restrict__ counter, double* __restrict__ pub,
                 int* __restrict__ abort_flag, int* __restrict__ err,
                 const int64_t* __restrict__ fv_off,
                 const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
@@ -356,7 +401,7 @@ __global__ void __launch_bounds__(256)
     TL* Dk = Lb + 2 * T * LD;                  // T x LD
     TV* Y = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = Y + T * nrhs;  // 4 x T
-    __shared__ int s_task, s_ok;
+    __shared__ int s_task;
     const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
     if (tid == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
@@ -373,7 +418,7 @@ __global__ void __launch_bounds__(256)
     const bool pivot = i < nt1;
     const bool lsplit = nrhs == 1;
     const TL* L = Ls + F.loff;
-    int* fl = flags + dinv_off[s] / (T * T);
+    double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
     if (pivot) load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)i * T * T, T, ti.size, ti.size);
     if (kend > 0) load_block_async(Lb, L + ti.start, F.ldl, ti.size, min(T, F.c));
     cp_async_commit_group();
@@ -386,16 +431,10 @@ __global__ void __launch_bounds__(256)
             load_block_async(Lb + ((k + 1) & 1) * T * LD, L + ti.start + (int64_t)(k + 1) * T * F.ldl,
                              F.ldl, ti.size, min(T, F.c - (k + 1) * T));
         cp_async_commit_group();
-        if (tid == 0) s_ok = wait_flag(fl + k, 1, abort_flag, err);
-        __syncthreads();
-        if (!s_ok) {
+        if (!poll_published(Y, pb + (int64_t)k * T * nrhs, min(T, F.c - k * T), nrhs, abort_flag,
+                            err)) {
             ok = false;
             break;
-        }
-        const int nk = min(T, F.c - k * T);
-        for (int e = tid; e < T * nrhs; e += blockDim.x) {
-            const int rr = e & (T - 1), q = e / T;
-            Y[e] = rr < nk ? ld_shared_value(xp + F.first_col + k * T + rr + (int64_t)q * n) : TV(0);
         }
         cp_async_wait_groups<1>();
         __syncthreads();
@@ -457,8 +496,11 @@ __global__ void __launch_bounds__(256)
         for (int l = 0; l < 16; ++l) y += (TV)Dk[r + (16 * g + l) * LD] * Y[16 * g + l];
         red[g * T + r] = y;
         __syncthreads();
-        if (g == 0 && r < ti.size)
-            xp[F.first_col + ti.start + r] = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
+        if (g == 0 && r < ti.size) {
+            const TV v = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
+            xp[F.first_col + ti.start + r] = v;
+            st_relaxed_f64(pb + (int64_t)i * T + r, v);
+        }
     } else {
         TV y[NQ];
 #pragma unroll
@@ -476,13 +518,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int j = 0; j < NQ; ++j) {
                 const int q = g + 4 * j;
-                if (q < nrhs) xp[F.first_col + ti.start + r + (int64_t)q * n] = y[j];
+                if (q < nrhs) {
+                    xp[F.first_col + ti.start + r + (int64_t)q * n] = y[j];
+                    st_relaxed_f64(pb + ((int64_t)i * nrhs + q) * T + r, y[j]);
+                }
             }
         }
     }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) st_release_gpu(fl + i, 1);
 }
 
 // Backward, update rows, task (s, j | h << 16): the partial sum
@@ -609,7 +651,7 @@ __global__ void __launch_bounds__(256)
 template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256)
     k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
-                int ntasks, int* __restrict__ counter, int* __restrict__ flags,
+                int ntasks, int* __restrict__ counter, double* __restrict__ pub,
                 int* __restrict__ abort_flag, int* __restrict__ err,
                 const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
                 const TV* __restrict__ part, const int64_t* __restrict__ dinv_off,
@@ -621,7 +663,7 @@ __global__ void __launch_bounds__(256)
     TL* Dk = Lb + 2 * T * LD;
     TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = X + T * nrhs;
-    __shared__ int s_task, s_ok;
+    __shared__ int s_task;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
     if (tid == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
@@ -636,7 +678,7 @@ __global__ void __launch_bounds__(256)
     const TileRange tj = tile_range(j, F.m, F.c, T);
     const bool lsplit = nrhs == 1;
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;  // column tile j
-    int* fl = flags + dinv_off[s] / (T * T);
+    double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
     const int nblk = nt1 - 1 - j;  // pivot row tiles k = nt1-1 down to j+1
     load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
     if (nblk > 0) {
@@ -656,17 +698,9 @@ __global__ void __launch_bounds__(256)
         }
         cp_async_commit_group();
         const TileRange tkr = tile_range(k, F.m, F.c, T);
-        if (tid == 0) s_ok = wait_flag(fl + k, 2, abort_flag, err);
-        __syncthreads();
-        if (!s_ok) {
+        if (!poll_published(X, pb + (int64_t)k * T * nrhs, tkr.size, nrhs, abort_flag, err)) {
             ok = false;
             break;
-        }
-        for (int e = tid; e < T * nrhs; e += blockDim.x) {
-            const int rr = e & (T - 1), q = e / T;
-            X[e] = rr < tkr.size
-                       ? ld_shared_value(xp + F.first_col + tkr.start + rr + (int64_t)q * n)
-                       : TV(0);
         }
         cp_async_wait_groups<1>();
         __syncthreads();
@@ -728,7 +762,11 @@ __global__ void __launch_bounds__(256)
         for (int r = 0; r < 16; ++r) x += (TV)Dk[(16 * g + r) + l * LD] * X[16 * g + r];
         red[g * T + l] = x;
         __syncthreads();
-        if (g == 0 && l < tj.size) xp[xj + l] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+        if (g == 0 && l < tj.size) {
+            const TV v = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+            xp[xj + l] = v;
+            st_relaxed_f64(pb + (int64_t)j * T + l, v);
+        }
     } else {
         TV x[NQ];
 #pragma unroll
@@ -746,13 +784,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int a = 0; a < NQ; ++a) {
                 const int q = g + 4 * a;
-                if (q < nrhs) xp[xj + l + (int64_t)q * n] = x[a];
+                if (q < nrhs) {
+                    xp[xj + l + (int64_t)q * n] = x[a];
+                    st_relaxed_f64(pb + ((int64_t)j * nrhs + q) * T + l, x[a]);
+                }
             }
         }
     }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) st_release_gpu(fl + j, 2);
 }
 
 // ---------------------------------------------------------------------------
@@ -860,8 +898,9 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
                 Ls, xp, fv, n, nrhs, msmall);
         if (nt > 0)
             k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
-                                                        flags, abort_flag, S.err, D.fv_off,
-                                                        D.dinv_off, Ls, Dinv, xp, fv, n, nrhs);
+                                                        fv + D.fv_pub_off * nrhs, abort_flag,
+                                                        S.err, D.fv_off, D.dinv_off, Ls, Dinv, xp,
+                                                        fv, n, nrhs);
     } else {
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
@@ -875,7 +914,8 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
         }
         if (nt > 0)
             k_bwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
-                                                        flags, abort_flag, S.err, S.gather_nch,
+                                                        fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs,
+                                                        abort_flag, S.err, S.gather_nch,
                                                         S.gather_off, part, D.dinv_off, Ls, Dinv,
                                                         xp, n, nrhs);
     }
@@ -885,6 +925,9 @@ template <typename TL, typename TV, int NQ>
 static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv,
                             int nrhs, cudaStream_t st) {
     cudaMemsetAsync(D.solve.sync, 0, (size_t)D.solve.nsync * sizeof(int), st);
+    // publication slots of the forward and backward pivot tiles: all-ones bits
+    cudaMemsetAsync(fv + D.fv_pub_off * nrhs, 0xff,
+                    (size_t)2 * D.solve.nflags * kTile * nrhs * sizeof(TV), st);
     for (int l = 0; l < D.nlevels; ++l) solve_level<TL, TV, NQ>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
     for (int l = D.nlevels - 1; l >= 0; --l)
         solve_level<TL, TV, NQ>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
