@@ -279,6 +279,12 @@ void upload_plan(mdgpu_handle_s* h) {
         D.solve.bwd_elems = SS.bwd_elems;
         D.solve.small_elems = SS.small_elems;
         D.solve.gather_task_beg = SS.gather_task_beg;
+        {
+            std::vector<int> at = SS.asm_tasks;
+            if (at.empty()) at.assign(2, 0);
+            D.solve.asm_tasks = reinterpret_cast<int2*>(h->keep(upload(at)));
+            D.solve.asm_task_beg = SS.asm_task_beg;
+        }
         D.solve.gather_nch = h->keep(upload(SS.gather_nch));
         D.solve.gather_off = h->keep(upload(SS.gather_off));
         D.solve.nflags = SS.nflags;

@@ -106,6 +106,9 @@ struct SolveSchedule {
     std::vector<int> gather_task_beg;
     int* gather_nch = nullptr;
     int* gather_off = nullptr;
+    // forward assembly chunks of the large fronts
+    int2* asm_tasks = nullptr;
+    std::vector<int> asm_task_beg;
 };
 
 struct DevPlan {

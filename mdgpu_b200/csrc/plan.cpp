@@ -340,6 +340,20 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
     }
+    S.asm_tasks.clear();
+    S.asm_task_beg.assign(P.nlevels + 1, 0);
+    for (int l = 0; l < P.nlevels; ++l) {
+        S.asm_task_beg[l] = (int)(S.asm_tasks.size() / 2);
+        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+            const int s = P.large_list[q];
+            const int nc = (P.fronts[s].m + SolveScheduleHost::kAsmRows - 1) / SolveScheduleHost::kAsmRows;
+            for (int h = 0; h < nc; ++h) {
+                S.asm_tasks.push_back(s);
+                S.asm_tasks.push_back(h);
+            }
+        }
+    }
+    S.asm_task_beg[P.nlevels] = (int)(S.asm_tasks.size() / 2);
     const int GC = SolveScheduleHost::kGatherTiles;
     S.gather_task_beg.assign(P.nlevels + 1, 0);
     S.gather_nch.assign(P.nsuper, 0);

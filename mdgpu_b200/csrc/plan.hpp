@@ -148,6 +148,11 @@ struct SolveScheduleHost {
     // chunk count and the first partial (pivot tile j, chunk h at
     // gather_off + j * gather_nch + h), counted within its level
     static constexpr int kGatherTiles = 16;
+    // forward assembly of the large fronts' vectors: tasks (front, chunk of
+    // kAsmRows rows) per level, packed (s, chunk)
+    static constexpr int kAsmRows = 1024;
+    std::vector<int> asm_tasks;
+    std::vector<int> asm_task_beg;      // nlevels + 1, in tasks
     std::vector<int> gather_task_beg;   // nlevels + 1, in tasks
     std::vector<int> gather_nch, gather_off;  // per supernode
     int64_t gather_vecs = 0;            // partial vectors the largest level needs

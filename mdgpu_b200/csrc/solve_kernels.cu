@@ -28,29 +28,42 @@ __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) 
 // large fronts
 // ---------------------------------------------------------------------------
 
+// Rows [ch * kAsmRows, ...) of large front s's vector: the pivot rows from
+// the right-hand side, then every child's update rows that land there, child
+// by child (deterministic sums).  A child's rows landing in a row range are
+// contiguous (increasing relative map); the factor's assembly ranges (per
+// kAssembleCols-row block) give them.
 template <typename TV>
-__device__ void fwd_assemble_front(int s, const FrontDesc* __restrict__ fronts,
+__device__ void fwd_assemble_chunk(int s, int ch, const FrontDesc* __restrict__ fronts,
                                    const int* __restrict__ child, const int* __restrict__ relmap,
+                                   const int* __restrict__ asm_off, const int* __restrict__ asm_range,
                                    const int64_t* __restrict__ fv_off, const TV* __restrict__ xp,
                                    TV* __restrict__ fv, int n, int nrhs) {
     const FrontDesc F = fronts[s];
     const int m = F.m, c = F.c;
+    const int r0 = ch * SolveScheduleHost::kAsmRows, r1 = min(m, r0 + SolveScheduleHost::kAsmRows);
+    const int nr = r1 - r0;
     const int tid = threadIdx.x, nt = blockDim.x;
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < m * nrhs; idx += nt) {
-        int q = idx / m, r = idx - q * m;
-        f[idx] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
+    for (int idx = tid; idx < nr * nrhs; idx += nt) {
+        int q = idx / nr, r = r0 + (idx - q * nr);
+        f[r + (int64_t)q * m] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
     }
     __syncthreads();
-    for (int h = F.child_beg; h < F.child_end; ++h) {
-        const int ch = child[h];
-        const FrontDesc g = fronts[ch];
-        const int uc = g.m - g.c;
-        const TV* w = front_vec(fv, fv_off, ch, nrhs);
+    const int nch = F.child_end - F.child_beg;
+    const int b0 = r0 / kAssembleCols, b1 = (r1 + kAssembleCols - 1) / kAssembleCols;
+    const int* rng = asm_range + asm_off[s];
+    for (int h = 0; h < nch; ++h) {
+        const int lo = rng[(b0 * nch + h) * 2], hi = rng[((b1 - 1) * nch + h) * 2 + 1];
+        if (lo >= hi) continue;
+        const int cs = child[F.child_beg + h];
+        const FrontDesc g = fronts[cs];
+        const TV* w = front_vec(fv, fv_off, cs, nrhs);
         const int* rm = relmap + g.rows_off + g.c;
-        for (int idx = tid; idx < uc * nrhs; idx += nt) {
-            int q = idx / uc, r = idx - q * uc;
-            f[rm[r] + q * m] += w[g.c + r + q * g.m];
+        const int cnt = hi - lo;
+        for (int idx = tid; idx < cnt * nrhs; idx += nt) {
+            int q = idx / cnt, rr = lo + (idx - q * cnt);
+            f[rm[rr] + (int64_t)q * m] += w[g.c + rr + (int64_t)q * g.m];
         }
         __syncthreads();
     }
@@ -425,6 +438,17 @@ __global__ void __launch_bounds__(256)
     TV acc[NQ];
 #pragma unroll
     for (int j = 0; j < NQ; ++j) acc[j] = TV(0);
+    // this tile's rows of the front vector (assembled by an earlier launch):
+    // loaded now, off the chain's critical path
+    TV* f = front_vec(fv, fv_off, s, nrhs);
+    TV fpre[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+        const int q = lsplit ? 0 : g + 4 * j;
+        fpre[j] = (r < ti.size && q < nrhs && (!lsplit || (g == 0 && j == 0)))
+                      ? f[ti.start + r + (int64_t)q * F.m]
+                      : TV(0);
+    }
     bool ok = true;
     for (int k = 0; k < kend; ++k) {
         if (k + 1 < kend)
@@ -463,16 +487,15 @@ __global__ void __launch_bounds__(256)
         acc[0] = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
         __syncthreads();
     }
-    TV* f = front_vec(fv, fv_off, s, nrhs);
     if (!pivot) {
         if (r < ti.size) {
             if (lsplit) {
-                if (g == 0) f[ti.start + r] -= acc[0];
+                if (g == 0) f[ti.start + r] = fpre[0] - acc[0];
             } else {
 #pragma unroll
                 for (int j = 0; j < NQ; ++j) {
                     const int q = g + 4 * j;
-                    if (q < nrhs) f[ti.start + r + (int64_t)q * F.m] -= acc[j];
+                    if (q < nrhs) f[ti.start + r + (int64_t)q * F.m] = fpre[j] - acc[j];
                 }
             }
         }
@@ -480,13 +503,12 @@ __global__ void __launch_bounds__(256)
     }
     // F = f_i - acc (zero beyond the tile), then y = Dk F
     if (lsplit) {
-        if (g == 0) Y[r] = r < ti.size ? f[ti.start + r] - acc[0] : TV(0);
+        if (g == 0) Y[r] = r < ti.size ? fpre[0] - acc[0] : TV(0);
     } else {
 #pragma unroll
         for (int j = 0; j < NQ; ++j) {
             const int q = g + 4 * j;
-            if (q < nrhs)
-                Y[r + T * q] = r < ti.size ? f[ti.start + r + (int64_t)q * F.m] - acc[j] : TV(0);
+            if (q < nrhs) Y[r + T * q] = r < ti.size ? fpre[j] - acc[j] : TV(0);
         }
     }
     __syncthreads();
@@ -614,17 +636,20 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(256)
     k_fwd_prep(const FrontDesc* __restrict__ fronts, const int* __restrict__ small_list,
-               int nsmall, const int* __restrict__ large_list, const int* __restrict__ child,
-               const int* __restrict__ relmap, const int64_t* __restrict__ fv_off,
+               int nsmall, const int2* __restrict__ asm_tasks, const int* __restrict__ child,
+               const int* __restrict__ relmap, const int* __restrict__ asm_off,
+               const int* __restrict__ asm_range, const int64_t* __restrict__ fv_off,
                const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
                int msmall) {
     const int b = blockIdx.x;
-    if (b < nsmall)
+    if (b < nsmall) {
         fwd_small_front<TL, TV>(small_list[b], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
                                 msmall);
-    else
-        fwd_assemble_front<TV>(large_list[b - nsmall], fronts, child, relmap, fv_off, xp, fv, n,
-                               nrhs);
+    } else {
+        const int2 t = asm_tasks[b - nsmall];
+        fwd_assemble_chunk<TV>(t.x, t.y, fronts, child, relmap, asm_off, asm_range, fv_off, xp, fv,
+                               n, nrhs);
+    }
 }
 
 template <typename TL, typename TV, int NQ>
@@ -689,6 +714,32 @@ __global__ void __launch_bounds__(256)
     TV acc[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
+    // off the chain's critical path, before the first wait: the update-row
+    // partial sums (earlier launch, in chunk order) and this tile's y_j
+    const int64_t xj = F.first_col + tj.start;
+    TV ypre[NQ];
+    {
+        const int nch = gather_nch[s];
+        const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
+        for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
+            if (lsplit) {
+                if (g == 0) acc[0] += pj[l];
+            } else {
+#pragma unroll
+                for (int a = 0; a < NQ; ++a) {
+                    const int q = g + 4 * a;
+                    if (q < nrhs) acc[a] += pj[l + T * q];
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) {
+            const int q = lsplit ? 0 : g + 4 * a;
+            ypre[a] = (l < tj.size && q < nrhs && (!lsplit || (g == 0 && a == 0)))
+                          ? xp[xj + l + (int64_t)q * n]
+                          : TV(0);
+        }
+    }
     bool ok = true;
     for (int b = 0; b < nblk; ++b) {
         const int k = nt1 - 1 - b;
@@ -729,30 +780,14 @@ __global__ void __launch_bounds__(256)
         acc[0] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
         __syncthreads();
     }
-    {  // update-row partial sums, in chunk order
-        const int nch = gather_nch[s];
-        const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
-        for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
-            if (lsplit) {
-                acc[0] += pj[l];
-            } else {
-#pragma unroll
-                for (int a = 0; a < NQ; ++a) {
-                    const int q = g + 4 * a;
-                    if (q < nrhs) acc[a] += pj[l + T * q];
-                }
-            }
-        }
-    }
     // t = y_j - acc (y_j: this front's forward solution), then x_j = Dk' t
-    const int64_t xj = F.first_col + tj.start;
     if (lsplit) {
-        if (g == 0) X[l] = l < tj.size ? xp[xj + l] - acc[0] : TV(0);
+        if (g == 0) X[l] = l < tj.size ? ypre[0] - acc[0] : TV(0);
     } else {
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
             const int q = g + 4 * a;
-            if (q < nrhs) X[l + T * q] = l < tj.size ? xp[xj + l + (int64_t)q * n] - acc[a] : TV(0);
+            if (q < nrhs) X[l + T * q] = l < tj.size ? ypre[a] - acc[a] : TV(0);
         }
     }
     __syncthreads();
@@ -892,10 +927,11 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
         (S.small_elems[l] + (forward ? S.fwd_elems[l] : S.bwd_elems[l])) * sizeof(TL);
     ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
     if (forward) {
-        if (ns + nl > 0)
-            k_fwd_prep<TL, TV><<<ns + nl, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
-                D.fronts, D.small_list + sb, ns, D.large_list + lb, D.child, D.relmap, D.fv_off,
-                Ls, xp, fv, n, nrhs, msmall);
+        const int ab = S.asm_task_beg[l], na = S.asm_task_beg[l + 1] - ab;
+        if (ns + na > 0)
+            k_fwd_prep<TL, TV><<<ns + na, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
+                D.fronts, D.small_list + sb, ns, S.asm_tasks + ab, D.child, D.relmap, D.asm_off,
+                D.asm_range, D.fv_off, Ls, xp, fv, n, nrhs, msmall);
         if (nt > 0)
             k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
                                                         fv + D.fv_pub_off * nrhs, abort_flag,
