@@ -69,6 +69,8 @@ def parse():
     # profiling helpers: run only one arm of the step (for ncu launch lists)
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-rhs64", action="store_true",
+                    help="skip the 64-right-hand-side measurement")
     return ap.parse_args()
 
 
@@ -233,6 +235,7 @@ def run_gpu_arm(args):
     import torch
 
     import mdgpu_b200 as M
+    from mdgpu_b200 import matgen as mg
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -332,6 +335,25 @@ def run_gpu_arm(args):
             e2e_t.append(time.perf_counter() - t0)
     e2e_ms = allmax(1e3 * statistics.mean(e2e_t)) if e2e_t else float("nan")
 
+    # the same step with 64 right-hand sides (FP32 factor + FP64 refinement of
+    # all 64 columns; device-resident, column-major)
+    rhs64 = None
+    if not args.no_rhs64:
+        B64 = mg.rhs_uniform(n, seed=1, nrhs=64)
+        dB64 = torch.from_numpy(np.asfortranarray(B64)).cuda().t().contiguous().t()
+        dX64 = torch.empty((64, n), dtype=torch.float64, device="cuda").t()
+
+        def step_fp32_64():
+            S.factor(dAx, M.FP32, stream=sptr)
+            return S.refine_device(dB64, dX64, tol=1e-14, maxit=30, stream=sptr)
+
+        t64, (be64, it64) = timed(step_fp32_64, max(1, min(args.steps, 3)), 1)
+        ms64r = allmax(statistics.mean(t64))
+        rhs64 = {"nrhs": 64, "ms_per_step": ms64r,
+                 "max_backward_error": float(np.max(be64)), "ir_iterations": int(it64),
+                 "solve_flops_per_rhs_sweep_pair": 4.0 * S.info("lnz"),
+                 "note": "FP32 factor + FP64 refinement of 64 columns at once"}
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -357,6 +379,7 @@ def run_gpu_arm(args):
                 "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(Ax.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes)},
+        "rhs64": rhs64,
         "gpu_launches": prof["launches_per_step"],
         "clocks": clocks,
         "roofline": None,
