@@ -43,18 +43,18 @@ CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
 # bytes per step; profiles/dram_traffic_fp32_step_3d64.md holds the capture
 # and its command.  The roofline line divides it by the class's launches.
 TRAFFIC_PER_STEP_3D64 = {
-    "small_front": 501836544, "assemble": 7711001856, "potrf": 12777216, "trsm": 2304483328,
-    "schur_update": 15847656960, "solve_small": 822050816, "solve_large": 6241783296,
+    "small_front": 501853696, "assemble": 7651057408, "potrf": 12498944, "trsm": 2300320000,
+    "schur_update": 15858723072, "solve_small": 671831040, "solve_large": 6392204800,
 }
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
     "small_front": ["k_small_front"],
-    "assemble": ["k_big_assemble_cols"],
+    "assemble": ["k_big_assemble_warp", "k_big_assemble_cols"],
     "potrf": ["k_tile_potrf"],
     "trsm": ["k_tile_trsm", "k_tile_update"],
     "schur_update": ["k_schur_tc"],
-    "solve_small": ["k_fwd_small", "k_bwd_small"],
-    "solve_large": ["k_fwd_assemble", "k_fwd_level", "k_bwd_gather", "k_bwd_level"],
+    "solve_small": ["k_fwd_prep", "k_bwd_prep"],
+    "solve_large": ["k_fwd_prep", "k_fwd_level", "k_bwd_prep", "k_bwd_level"],
 }
 
 
