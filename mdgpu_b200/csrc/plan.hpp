@@ -85,6 +85,7 @@ struct Plan {
     std::vector<int> large_list;
 
     static const int small_limit[kSmallBuckets];
+    static constexpr int kTinyBuckets = 2;  // buckets of fronts with m <= 32
 };
 
 // Largest m handled by the fused one-CTA-per-front kernel for a scalar size.

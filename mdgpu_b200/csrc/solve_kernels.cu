@@ -628,6 +628,71 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
 }
 
+// ---------------------------------------------------------------------------
+// tiny fronts (m <= 32, one right-hand side): a warp per front, one row per
+// lane; pivots by shuffles, dot products by warp reductions, no barriers
+// ---------------------------------------------------------------------------
+
+constexpr int kTinyRows = 32;
+
+template <typename TL, typename TV>
+__device__ void fwd_tiny_front(int s, const FrontDesc* __restrict__ fronts,
+                               const int* __restrict__ child, const int* __restrict__ relmap,
+                               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                               TV* __restrict__ xp, TV* __restrict__ fv, TV* wbuf) {
+    const int lane = threadIdx.x & 31;
+    const FrontDesc F = fronts[s];
+    const int m = F.m, c = F.c;
+    const TL* L = Ls + F.loff;
+    wbuf[lane] = lane < c ? xp[F.first_col + lane] : TV(0);
+    __syncwarp();
+    for (int h = F.child_beg; h < F.child_end; ++h) {  // children in order
+        const int ch = child[h];
+        const FrontDesc g = fronts[ch];
+        const int uc = g.m - g.c;
+        const TV* w = front_vec(fv, fv_off, ch, 1);
+        const int* rm = relmap + g.rows_off + g.c;
+        for (int rr = lane; rr < uc; rr += 32) wbuf[rm[rr]] += w[g.c + rr];
+        __syncwarp();
+    }
+    TV v = wbuf[lane];
+    __syncwarp();
+    for (int j = 0; j < c; ++j) {
+        if (lane == j) v = v / (TV)L[j + (int64_t)j * F.ldl];
+        const TV yj = __shfl_sync(0xffffffffu, v, j);
+        if (lane > j && lane < m) v -= (TV)L[lane + (int64_t)j * F.ldl] * yj;
+    }
+    if (lane < c)
+        xp[F.first_col + lane] = v;
+    else if (lane < m)
+        front_vec(fv, fv_off, s, 1)[lane] = v;
+}
+
+template <typename TL, typename TV>
+__device__ void bwd_tiny_front(int s, const FrontDesc* __restrict__ fronts,
+                               const int* __restrict__ rows, const TL* __restrict__ Ls,
+                               TV* __restrict__ xp) {
+    const int lane = threadIdx.x & 31;
+    const FrontDesc F = fronts[s];
+    const int m = F.m, c = F.c;
+    const TL* L = Ls + F.loff;
+    // pivot lanes: y; update lanes: the final x of their (ancestor) rows
+    TV v = lane < c ? xp[F.first_col + lane]
+                    : (lane < m ? xp[rows[F.rows_off + lane]] : TV(0));
+    for (int j = 0; j < c; ++j) {  // t_j = y_j - L(u, j)' x_u
+        TV p = (lane >= c && lane < m) ? (TV)L[lane + (int64_t)j * F.ldl] * v : TV(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        if (lane == j) v -= p;
+    }
+    for (int j = c - 1; j >= 0; --j) {  // L11' x = t, last pivot first
+        if (lane == j) v = v / (TV)L[j + (int64_t)j * F.ldl];
+        const TV xj = __shfl_sync(0xffffffffu, v, j);
+        if (lane < j) v -= (TV)L[j + (int64_t)lane * F.ldl] * xj;
+    }
+    if (lane < c) xp[F.first_col + lane] = v;
+}
+
 // One launch per level before the large-front chain (128 threads, 256 when
 // it holds gather tasks), forward: the small
 // fronts (CTA each) and the large fronts' vector assembly (CTA each) -- both
@@ -636,17 +701,28 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(256)
     k_fwd_prep(const FrontDesc* __restrict__ fronts, const int* __restrict__ small_list,
-               int nsmall, const int2* __restrict__ asm_tasks, const int* __restrict__ child,
+               int nsmall, int ntiny, const int2* __restrict__ asm_tasks, const int* __restrict__ child,
                const int* __restrict__ relmap, const int* __restrict__ asm_off,
                const int* __restrict__ asm_range, const int64_t* __restrict__ fv_off,
                const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
                int msmall) {
-    const int b = blockIdx.x;
-    if (b < nsmall) {
-        fwd_small_front<TL, TV>(small_list[b], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
-                                msmall);
+    const int wpb = blockDim.x >> 5;
+    const int tb = (ntiny + wpb - 1) / wpb;  // blocks of tiny fronts (a warp each)
+    int b = blockIdx.x;
+    if (b < tb) {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        const int w = threadIdx.x >> 5, q = b * wpb + w;
+        if (q < ntiny)
+            fwd_tiny_front<TL, TV>(small_list[q], fronts, child, relmap, fv_off, Ls, xp, fv,
+                                   reinterpret_cast<TV*>(smem_raw) + w * kTinyRows);
+        return;
+    }
+    b -= tb;
+    if (b < nsmall - ntiny) {
+        fwd_small_front<TL, TV>(small_list[ntiny + b], fronts, child, relmap, fv_off, Ls, xp, fv,
+                                n, nrhs, msmall);
     } else {
-        const int2 t = asm_tasks[b - nsmall];
+        const int2 t = asm_tasks[b - (nsmall - ntiny)];
         fwd_assemble_chunk<TV>(t.x, t.y, fronts, child, relmap, asm_off, asm_range, fv_off, xp, fv,
                                n, nrhs);
     }
@@ -655,17 +731,26 @@ __global__ void __launch_bounds__(256)
 template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256)
     k_bwd_prep(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
-               const int* __restrict__ small_list, const int* __restrict__ rows,
+               const int* __restrict__ small_list, int ntiny, const int* __restrict__ rows,
                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
                const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ part, int n,
                int nrhs, int umax, int msmall) {
     const int b = blockIdx.x;
-    if (b < ngather)
+    if (b < ngather) {
         bwd_gather_task<TL, TV, NQ>(gtasks[b], fronts, rows, gather_nch, gather_off, Ls, xp, part,
                                     n, nrhs);
-    else
-        bwd_small_front<TL, TV>(small_list[b - ngather], fronts, rows, Ls, xp, n, nrhs, umax,
-                                msmall);
+        return;
+    }
+    const int wpb = blockDim.x >> 5;
+    const int tb = (ntiny + wpb - 1) / wpb;  // blocks of tiny fronts (a warp each)
+    const int bb = b - ngather;
+    if (bb < tb) {
+        const int q = bb * wpb + (threadIdx.x >> 5);
+        if (q < ntiny) bwd_tiny_front<TL, TV>(small_list[q], fronts, rows, Ls, xp);
+        return;
+    }
+    bwd_small_front<TL, TV>(small_list[ntiny + bb - tb], fronts, rows, Ls, xp, n, nrhs, umax,
+                            msmall);
 }
 
 // Backward, task (s, j): pivot column tile j of front s accumulates
@@ -917,6 +1002,11 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     const int ns = se - sb;
     const int lb = D.h_large_ptr[l], nl = D.h_large_ptr[l + 1] - lb;
     const int msmall = level_msmall(D, l);
+    // small fronts of at most kTinyRows rows (the first two buckets) take the
+    // warp path when there is one right-hand side
+    static_assert(Plan::kTinyBuckets == 2, "buckets 0 and 1 hold m <= 16 and m <= 32");
+    const int ntiny =
+        nrhs == 1 ? D.h_small_ptr[l * kSmallBuckets + Plan::kTinyBuckets] - sb : 0;
     const size_t lsm = level_smem_bytes<TL, TV>(nrhs);
     const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
@@ -928,10 +1018,12 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
     if (forward) {
         const int ab = S.asm_task_beg[l], na = S.asm_task_beg[l + 1] - ab;
+        const int tb = (ntiny + 3) / 4;  // 128 threads: four tiny fronts per CTA
         if (ns + na > 0)
-            k_fwd_prep<TL, TV><<<ns + na, 128, small_fwd_smem<TL, TV>(msmall, nrhs), st>>>(
-                D.fronts, D.small_list + sb, ns, S.asm_tasks + ab, D.child, D.relmap, D.asm_off,
-                D.asm_range, D.fv_off, Ls, xp, fv, n, nrhs, msmall);
+            k_fwd_prep<TL, TV><<<tb + (ns - ntiny) + na, 128, small_fwd_smem<TL, TV>(msmall, nrhs),
+                                 st>>>(D.fronts, D.small_list + sb, ns, ntiny, S.asm_tasks + ab,
+                                       D.child, D.relmap, D.asm_off, D.asm_range, D.fv_off, Ls, xp,
+                                       fv, n, nrhs, msmall);
         if (nt > 0)
             k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
                                                         fv + D.fv_pub_off * nrhs, abort_flag,
@@ -944,9 +1036,11 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
             size_t sm = small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
             if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
             // the gather's thread layout needs 256 threads; small fronts alone run on 128
-            k_bwd_prep<TL, TV, NQ><<<ng + ns, ng > 0 ? 256 : 128, sm, st>>>(
-                D.fronts, S.tasks + gb, ng, D.small_list + sb, D.rows, S.gather_nch, S.gather_off,
-                Ls, xp, part, n, nrhs, msmall, msmall);
+            const int threads = ng > 0 ? 256 : 128;
+            const int tb = (ntiny + threads / 32 - 1) / (threads / 32);
+            k_bwd_prep<TL, TV, NQ><<<ng + tb + (ns - ntiny), threads, sm, st>>>(
+                D.fronts, S.tasks + gb, ng, D.small_list + sb, ntiny, D.rows, S.gather_nch,
+                S.gather_off, Ls, xp, part, n, nrhs, msmall, msmall);
         }
         if (nt > 0)
             k_bwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
