@@ -103,6 +103,85 @@ __global__ void k_small_front(const FrontDesc* __restrict__ fronts, const int* _
     }
 }
 
+// Fronts of at most 32 rows: a warp per front (four per CTA), the front in the
+// warp's own 32 x 33 shared slice; the same steps and sums in the same order
+// as k_small_front, with warp syncs only.
+constexpr int kTinyFrontRows = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+    k_tiny_fronts(const FrontDesc* __restrict__ fronts, const int* __restrict__ list, int nfronts,
+                  const int* __restrict__ child, const int* __restrict__ relmap,
+                  const int* __restrict__ a_src, const int* __restrict__ a_pos,
+                  const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
+                  int* __restrict__ status) {
+    constexpr int LD = kTinyFrontRows + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (q >= nfronts) return;
+    T* Fm = reinterpret_cast<T*>(smem_raw) + (size_t)warp * kTinyFrontRows * LD;
+    const int s = list[q];
+    const FrontDesc f = fronts[s];
+    const int m = f.m, c = f.c, u = m - c;
+    for (int idx = lane; idx < m * LD; idx += 32) Fm[idx] = T(0);
+    __syncwarp();
+    for (int e = f.a_beg + lane; e < f.a_end; e += 32) {
+        const int src = a_src[e];
+        if (src >= 0) {
+            const int pos = a_pos[e];
+            Fm[(pos & 0xffff) + (pos >> 16) * LD] = (T)Ax[src];
+        }
+    }
+    __syncwarp();
+    for (int h = f.child_beg; h < f.child_end; ++h) {
+        const FrontDesc g = fronts[child[h]];
+        const int uc = g.m - g.c;
+        if (uc <= 0) continue;
+        const int* rm = relmap + g.rows_off + g.c;
+        const T* U = Us + g.uoff;
+        for (int idx = lane; idx < uc * uc; idx += 32) {
+            const int j = idx / uc, i = idx - j * uc;
+            if (i >= j) Fm[rm[i] + rm[j] * LD] += U[i + (int64_t)j * g.ldu];
+        }
+        __syncwarp();
+    }
+    // partial Cholesky of the c pivot columns (right-looking, panel only):
+    // lane i owns row i and touches only it; the multipliers of the other
+    // rows arrive by shuffles
+    for (int k = 0; k < c; ++k) {
+        const T dkk = Fm[k + k * LD];
+        if (lane == 0 && !(dkk > T(0))) flag_pivot(status, f.first_col + k);
+        const T d = sqrt(dkk);
+        const T inv = T(1) / d;
+        const T lik = (lane > k && lane < m) ? Fm[lane + k * LD] * inv : T(0);
+        if (lane == k) Fm[k + k * LD] = d;
+        if (lane > k && lane < m) Fm[lane + k * LD] = lik;
+        for (int j = k + 1; j < c; ++j) {
+            const T ljk = __shfl_sync(0xffffffffu, lik, j);
+            if (lane >= j && lane < m) Fm[lane + j * LD] -= lik * ljk;
+        }
+        __syncwarp();
+    }
+    // Schur complement straight to the update store
+    if (f.uoff >= 0) {
+        T* Ud = Us + f.uoff;
+        for (int idx = lane; idx < u * u; idx += 32) {
+            const int j = idx / u, i = idx - j * u;
+            if (i >= j) {
+                T acc = Fm[(c + i) + (c + j) * LD];
+                for (int k = 0; k < c; ++k) acc -= Fm[(c + i) + k * LD] * Fm[(c + j) + k * LD];
+                Ud[i + (int64_t)j * f.ldu] = acc;
+            }
+        }
+    }
+    T* Ld = Ls + f.loff;
+    for (int idx = lane; idx < m * c; idx += 32) {
+        const int j = idx / m, i = idx - j * m;
+        Ld[i + (int64_t)j * f.ldl] = (i >= j) ? Fm[i + j * LD] : T(0);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // large fronts: assembly
 // ---------------------------------------------------------------------------
@@ -713,7 +792,21 @@ static size_t diag_smem() {
 template <typename T>
 void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax,
                          int* status, cudaStream_t st) {
-    for (int b = 0; b < kSmallBuckets; ++b) {
+    {  // fronts of at most 32 rows (the first two buckets): a warp each
+        const int beg = D.h_small_ptr[level * kSmallBuckets];
+        const int end = D.h_small_ptr[level * kSmallBuckets + Plan::kTinyBuckets];
+        if (end > beg) {
+            double by = 0;
+            for (int b = 0; b < Plan::kTinyBuckets; ++b)
+                by += D.h_small_bytes[level * kSmallBuckets + b];
+            ProfScope ps(D.prof, KC_SMALL_FRONT, st, 0, by * sizeof(T) / 8.0);
+            const size_t smem = (size_t)4 * kTinyFrontRows * (kTinyFrontRows + 1) * sizeof(T);
+            k_tiny_fronts<T><<<(end - beg + 3) / 4, 128, smem, st>>>(
+                D.fronts, D.small_list + beg, end - beg, D.child, D.relmap, D.a_src, D.a_pos, Ax,
+                Ls, Us, status);
+        }
+    }
+    for (int b = Plan::kTinyBuckets; b < kSmallBuckets; ++b) {
         int beg = D.h_small_ptr[level * kSmallBuckets + b];
         int end = D.h_small_ptr[level * kSmallBuckets + b + 1];
         if (end == beg) continue;
