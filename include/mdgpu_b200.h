@@ -59,6 +59,22 @@ MDGPU_API int mdgpu_analyze(int n, const int *Ap, const int *Ai, int ordering, i
                   mdgpu_handle *out);
 
 /*
+ * Many independent SPD systems under one handle (the batched mode of the
+ * many-systems workload; the reference handles one system per run).  System
+ * b is the lower triangle (n[b], Ap[b], Ai[b]); each is analysed on its own
+ * exactly as mdgpu_analyze would, then the systems are numbered one after
+ * another as one block-diagonal matrix, so one factor / solve call works on
+ * all of them in the same level-scheduled launches.  Values and right-hand
+ * sides are the systems' arrays concatenated in order; mdgpu_get_array
+ * "sys_row_off" and "sys_val_off" (nsys + 1 entries, mdgpu_info "nsys") give
+ * each system's first row and first value.  MDGPU_ERR_NOT_TREE names a
+ * system whose elimination tree is a forest.
+ */
+MDGPU_API int mdgpu_analyze_batch(int nsys, const int *n, const int *const *Ap,
+                                  const int *const *Ai, int ordering, int tree, int relax_zeros,
+                                  mdgpu_handle *out);
+
+/*
  * Analysis from an already permuted lower triangle and a given assembly tree,
  * the inputs of the reference's Factor(cs *A, cs *spL, ETree **listaNodos,
  * int cantNodos) (mdgpu.cu:1394): supernode s eliminates columns

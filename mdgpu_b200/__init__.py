@@ -24,7 +24,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
           -7: "no CUDA device"}
 
 # every entry point declared in include/mdgpu_b200.h
-EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
+EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
            "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
            "mdgpu_refine_device",
@@ -69,6 +69,8 @@ def lib():
         L.mdgpu_analyze.argtypes = [C.c_int, ip, ip, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
         L.mdgpu_analyze_tree.argtypes = [C.c_int, ip, ip, C.c_int, ip, ip, ip, ip, ip,
                                          C.POINTER(vp)]
+        L.mdgpu_analyze_batch.argtypes = [C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.c_int,
+                                          C.c_int, C.c_int, C.POINTER(vp)]
         L.mdgpu_destroy.argtypes = [vp]
         L.mdgpu_destroy.restype = None
         L.mdgpu_info.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
@@ -131,6 +133,31 @@ class Solver:
                                int(relax_zeros), C.byref(self._h)))
 
     @classmethod
+    def batch(cls, systems, ordering=ORDER_AMD, tree=TREE_SUPER, relax_zeros=0):
+        """Many independent systems [(n, Ap, Ai), ...] under one solver: each
+        analysed on its own, numbered one after another (block-diagonal).
+        Values and right-hand sides are the systems' arrays concatenated;
+        ``row_off`` / ``val_off`` give each system's slice."""
+        self = cls.__new__(cls)
+        L = lib()
+        ns = len(systems)
+        nn = np.array([int(s[0]) for s in systems], dtype=np.int32)
+        Aps = [np.ascontiguousarray(s[1], dtype=np.int32) for s in systems]
+        Ais = [np.ascontiguousarray(s[2], dtype=np.int32) for s in systems]
+        self._keep = (nn, Aps, Ais)
+        pa = (C.c_void_p * ns)(*[a.ctypes.data for a in Aps])
+        pi = (C.c_void_p * ns)(*[a.ctypes.data for a in Ais])
+        self._h = C.c_void_p()
+        _check(L.mdgpu_analyze_batch(ns, _ptr(nn), pa, pi, int(ordering), int(tree),
+                                     int(relax_zeros), C.byref(self._h)))
+        self.n = int(nn.sum())
+        self.Ap = None
+        self.Ai = None
+        self.row_off = self.array("sys_row_off")
+        self.val_off = self.array("sys_val_off")
+        return self
+
+    @classmethod
     def from_tree(cls, n, Ap, Ai, first_col, ncols, child_ptr, child, count):
         self = cls.__new__(cls)
         L = lib()
@@ -167,7 +194,8 @@ class Solver:
                  "sn_first": ns, "sn_ncols": ns, "child_ptr": ns + 1,
                  "child": self.info("nchild"), "rows_ptr": ns + 1,
                  "rows": self.info("rows_total"), "relmap": self.info("rows_total"),
-                 "level": ns}
+                 "level": ns, "sys_row_off": self.info("nsys") + 1,
+                 "sys_val_off": self.info("nsys") + 1}
         if name == "Lp":
             a = np.zeros(n + 1, np.int64)
         else:

@@ -68,6 +68,9 @@ struct mdgpu_handle_s {
     Plan plan;
     TileSchedule fsched;
     SolveScheduleHost ssched;
+    // batch of independent systems (mdgpu_analyze_batch): per system its first
+    // row and its first entry in the concatenated lower-triangle values
+    std::vector<int> sys_row_off, sys_val_off;
     std::vector<int64_t> pscr_off;  // panel scratch offset per supernode
     PanelSchedule pschedh;
     bool use_tensor_cores = true;
@@ -526,6 +529,75 @@ int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
     return MDGPU_OK;
 }
 
+// One symbolic result for independent systems: the block-diagonal matrix of
+// their lower triangles, each system analysed on its own (so each keeps its
+// own bit-exact ordering and tree); rows, supernodes, L columns and the
+// value sources are offset system by system.  The assembly forest has one
+// tree per system.
+void combine_symbolic(const std::vector<Symbolic>& parts, const std::vector<int>& val_off,
+                      Symbolic& S) {
+    S = Symbolic();
+    int n = 0, ns = 0;
+    int64_t nnz = 0, lnz = 0;
+    for (const Symbolic& p : parts) {
+        n += p.n;
+        ns += p.tree.size();
+        nnz += p.lower.nnz();
+        lnz += p.Lp.back();
+    }
+    if (nnz > INT_MAX) throw std::runtime_error("batch too large for 32-bit entry indices");
+    S.n = n;
+    S.lower.nrows = S.lower.ncols = n;
+    S.lower.colptr.assign(1, 0);
+    S.tree.child_ptr.assign(1, 0);
+    S.Lp.assign(1, 0);
+    const bool any_perm = std::any_of(parts.begin(), parts.end(), [](const Symbolic& p) {
+        return !p.perm.empty();
+    });
+    const bool any_relax = std::any_of(parts.begin(), parts.end(), [](const Symbolic& p) {
+        return !p.relax_perm.empty();
+    });
+    int ro = 0, so = 0;
+    int64_t eo = 0;
+    for (size_t b = 0; b < parts.size(); ++b) {
+        const Symbolic& p = parts[b];
+        auto shift = [](const std::vector<int>& v, int o, std::vector<int>& out, bool keep_neg) {
+            for (int x : v) out.push_back(keep_neg && x < 0 ? x : x + o);
+        };
+        if (any_perm) {
+            if (p.perm.empty())
+                for (int i = 0; i < p.n; ++i) S.perm.push_back(ro + i);
+            else
+                shift(p.perm, ro, S.perm, false);
+        }
+        if (any_relax) {
+            if (p.relax_perm.empty())
+                for (int i = 0; i < p.n; ++i) S.relax_perm.push_back(ro + i);
+            else
+                shift(p.relax_perm, ro, S.relax_perm, false);
+        }
+        shift(p.parent, ro, S.parent, true);
+        shift(p.post, ro, S.post, false);
+        S.count0.insert(S.count0.end(), p.count0.begin(), p.count0.end());
+        S.count.insert(S.count.end(), p.count.begin(), p.count.end());
+        for (int j = 0; j < p.n; ++j) S.lower.colptr.push_back((int)(eo + p.lower.colptr[j + 1]));
+        shift(p.lower.rowidx, ro, S.lower.rowidx, false);
+        S.lower.val.insert(S.lower.val.end(), p.lower.val.begin(), p.lower.val.end());
+        shift(p.lower_src, val_off[b], S.lower_src, true);
+        shift(p.tree.first_col, ro, S.tree.first_col, false);
+        S.tree.ncols.insert(S.tree.ncols.end(), p.tree.ncols.begin(), p.tree.ncols.end());
+        const int cbase = (int)S.tree.child.size();
+        for (int s = 0; s < p.tree.size(); ++s) S.tree.child_ptr.push_back(cbase + p.tree.child_ptr[s + 1]);
+        shift(p.tree.child, so, S.tree.child, false);
+        const int64_t lb = S.Lp.back();
+        for (int j = 0; j < p.n; ++j) S.Lp.push_back(lb + p.Lp[j + 1]);
+        ro += p.n;
+        so += p.tree.size();
+        eo += p.lower.nnz();
+    }
+    (void)lnz;
+}
+
 // Solve error word (d_status[2]): cleared before a public solve call, read
 // after it; bit 0 = a dependency wait of the large-front solve ran out,
 // bit 1 = a solve kernel found its ticket counter not cleared.
@@ -593,6 +665,63 @@ int mdgpu_analyze(int n, const int* Ap, const int* Ai, int ordering, int tree, i
     });
 }
 
+int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int* const* Ai,
+                        int ordering, int tree, int relax_zeros, mdgpu_handle* out) {
+    if (!out || nsys <= 0 || !n || !Ap || !Ai) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (tree < 0 || tree > 2 || ordering < 0 || ordering > 1)
+        return fail(MDGPU_ERR_INVALID, "bad ordering or tree kind");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        std::vector<Symbolic> parts(nsys);
+        std::vector<int> row_off(nsys + 1, 0), val_off(nsys + 1, 0);
+        for (int b = 0; b < nsys; ++b) {
+            const int nb = n[b];
+            if (nb <= 0 || !Ap[b] || !Ai[b])
+                return fail(MDGPU_ERR_INVALID, "bad arguments of system " + std::to_string(b));
+            for (int j = 0; j < nb; ++j) {
+                if (Ap[b][j + 1] < Ap[b][j])
+                    return fail(MDGPU_ERR_INVALID,
+                                "column pointers decrease in system " + std::to_string(b));
+                for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p)
+                    if (Ai[b][p] < j || Ai[b][p] >= nb)
+                        return fail(MDGPU_ERR_INVALID, "entry outside the lower triangle in system " +
+                                                           std::to_string(b));
+            }
+            if (analyze(nb, Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD, (TreeKind)tree,
+                        relax_zeros, parts[b]) != 0)
+                return fail(MDGPU_ERR_NOT_TREE,
+                            "the elimination tree of system " + std::to_string(b) + " is a forest");
+            if ((int64_t)row_off[b] + nb > INT_MAX || (int64_t)val_off[b] + Ap[b][nb] > INT_MAX)
+                return fail(MDGPU_ERR_INVALID, "batch too large for 32-bit indices");
+            row_off[b + 1] = row_off[b] + nb;
+            val_off[b + 1] = val_off[b] + Ap[b][nb];
+        }
+        auto* h = new mdgpu_handle_s();
+        try {
+            combine_symbolic(parts, val_off, h->sym);
+            h->sys_row_off = row_off;
+            h->sys_val_off = val_off;
+            // the block-diagonal lower triangle in the caller's ordering
+            const int N = row_off[nsys];
+            std::vector<int> Apc(1, 0), Aic;
+            Aic.reserve(val_off[nsys]);
+            for (int b = 0; b < nsys; ++b)
+                for (int j = 0; j < n[b]; ++j) {
+                    for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p) Aic.push_back(Ai[b][p] + row_off[b]);
+                    Apc.push_back((int)Aic.size());
+                }
+            finish_plan(h);
+            build_csr(h, N, Apc.data(), Aic.data());
+            upload_plan(h);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return MDGPU_OK;
+    });
+}
+
 int mdgpu_analyze_tree(int n, const int* Ap, const int* Ai, int nsuper, const int* first_col,
                        const int* ncols, const int* child_ptr, const int* child, const int* count,
                        mdgpu_handle* out) {
@@ -650,6 +779,7 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "large_fronts") *value = (long long)P.large_list.size();
     else if (k == "on_device") *value = h->on_device;
     else if (k == "solve_work_rows") *value = h->D.fv_total;
+    else if (k == "nsys") *value = h->sys_row_off.empty() ? 1 : (long long)h->sys_row_off.size() - 1;
     else return fail(MDGPU_ERR_INVALID, "unknown key " + k);
     return MDGPU_OK;
 }
@@ -681,6 +811,8 @@ int mdgpu_get_array(mdgpu_handle h, const char* name, void* dst) {
     if (k == "child_ptr") return put(S.tree.child_ptr);
     if (k == "child") return put(S.tree.child);
     if (k == "level") return put(h->level);
+    if (k == "sys_row_off") return put(h->sys_row_off);
+    if (k == "sys_val_off") return put(h->sys_val_off);
     if (k == "rows") return put(P.rows);
     if (k == "relmap") return put(P.relmap);
     if (k == "rows_ptr") {
