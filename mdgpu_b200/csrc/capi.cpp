@@ -3,12 +3,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <map>
 #include <cstring>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ir.hpp"
@@ -687,14 +689,43 @@ int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int*
                         return fail(MDGPU_ERR_INVALID, "entry outside the lower triangle in system " +
                                                            std::to_string(b));
             }
-            if (analyze(nb, Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD, (TreeKind)tree,
-                        relax_zeros, parts[b]) != 0)
-                return fail(MDGPU_ERR_NOT_TREE,
-                            "the elimination tree of system " + std::to_string(b) + " is a forest");
             if ((int64_t)row_off[b] + nb > INT_MAX || (int64_t)val_off[b] + Ap[b][nb] > INT_MAX)
                 return fail(MDGPU_ERR_INVALID, "batch too large for 32-bit indices");
             row_off[b + 1] = row_off[b] + nb;
             val_off[b + 1] = val_off[b] + Ap[b][nb];
+        }
+        // the systems' analyses are independent: one host thread per core,
+        // systems taken in order from a shared counter; the first failing
+        // system (lowest index) is reported
+        std::vector<int> rc(nsys, 0);
+        std::vector<std::string> what(nsys);
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            for (int b = next.fetch_add(1); b < nsys; b = next.fetch_add(1)) {
+                try {
+                    rc[b] = analyze(n[b], Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD,
+                                    (TreeKind)tree, relax_zeros, parts[b]) != 0
+                                ? 1
+                                : 0;
+                } catch (const std::bad_alloc&) {
+                    rc[b] = 2;
+                } catch (const std::exception& e) {
+                    rc[b] = 3;
+                    what[b] = e.what();
+                }
+            }
+        };
+        const int nthr = std::max(1, std::min<int>(nsys, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (int b = 0; b < nsys; ++b) {
+            if (rc[b] == 1)
+                return fail(MDGPU_ERR_NOT_TREE,
+                            "the elimination tree of system " + std::to_string(b) + " is a forest");
+            if (rc[b] == 2) throw std::bad_alloc();
+            if (rc[b] == 3) throw std::runtime_error("system " + std::to_string(b) + ": " + what[b]);
         }
         auto* h = new mdgpu_handle_s();
         try {

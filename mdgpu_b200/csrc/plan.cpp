@@ -2,11 +2,59 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <exception>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace mdgpu {
+
+// The trees of an assembly forest (a batch of independent systems) as
+// contiguous supernode ranges [beg, end): each tree ends at its root and holds
+// only its own descendants.  A single range when that does not hold.
+static std::vector<std::pair<int, int>> tree_ranges(const AssemblyTree& t,
+                                                    const std::vector<int>& parent) {
+    const int ns = t.size();
+    std::vector<std::pair<int, int>> r;
+    int beg = 0;
+    for (int s = 0; s < ns; ++s) {
+        for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h)
+            if (t.child[h] < beg || t.child[h] >= s) return {{0, ns}};
+        if (parent[s] < 0) {
+            r.push_back({beg, s + 1});
+            beg = s + 1;
+        }
+    }
+    if (beg != ns || r.empty()) return {{0, ns}};
+    return r;
+}
+
+// fn(beg, end) on every range, ranges shared out to the host's cores; the
+// first exception (lowest range) is rethrown.
+template <typename F>
+static void for_each_range(const std::vector<std::pair<int, int>>& rg, F&& fn) {
+    const int nr = (int)rg.size();
+    std::vector<std::exception_ptr> ex(nr);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int i = next.fetch_add(1); i < nr; i = next.fetch_add(1)) {
+            try {
+                fn(rg[i].first, rg[i].second);
+            } catch (...) {
+                ex[i] = std::current_exception();
+            }
+        }
+    };
+    const int nthr = std::max(1, std::min(nr, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int k = 1; k < nthr; ++k) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (auto& e : ex)
+        if (e) std::rethrow_exception(e);
+}
 
 const int Plan::small_limit[kSmallBuckets] = {16, 32, 64, 96, 128, 160};
 
@@ -33,9 +81,6 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
     P.lnz = S.Lp[n];
     for (int j = 0; j < n; ++j) P.flops += (double)S.count[j] * S.count[j] + 1.0;
 
-    std::vector<int> col2sn(n);
-    for (int s = 0; s < ns; ++s)
-        for (int j = 0; j < t.ncols[s]; ++j) col2sn[t.first_col[s] + j] = s;
     std::vector<int> parent(ns, -1);
     for (int s = 0; s < ns; ++s)
         for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h) parent[t.child[h]] = s;
@@ -44,61 +89,69 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
     // sorted union of A's rows below the supernode and the children's update
     // rows.  This is the row set the reference builds with MatrizGetFk_3 and
     // VectorMerge (mdgpu.cu:180-291,1456,1489-1508,1566).
+    // The row count of front s is the column count of its first column, so
+    // the sets go straight into one flat array (checked as they are formed).
     const SparseCol& A = S.lower;
     std::vector<int64_t> rows_off(ns + 1, 0);
-    std::vector<std::vector<int>> rows(ns);
-    std::vector<int> scratch;
     for (int s = 0; s < ns; ++s) {
-        int k = t.first_col[s], c = t.ncols[s];
-        scratch.clear();
-        for (int j = k; j < k + c; ++j)
-            for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
-                if (A.rowidx[p] >= k + c) scratch.push_back(A.rowidx[p]);
-        for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h) {
-            int ch = t.child[h];
-            const auto& rc = rows[ch];
-            for (size_t i = t.ncols[ch]; i < rc.size(); ++i) {
-                if (rc[i] < k) throw std::runtime_error("child update row below its parent");
-                if (rc[i] >= k + c) scratch.push_back(rc[i]);
-            }
-        }
-        std::sort(scratch.begin(), scratch.end());
-        scratch.erase(std::unique(scratch.begin(), scratch.end()), scratch.end());
-        auto& r = rows[s];
-        r.resize(c + scratch.size());
-        for (int i = 0; i < c; ++i) r[i] = k + i;
-        std::copy(scratch.begin(), scratch.end(), r.begin() + c);
-        int m = (int)r.size();
-        if (m != S.count[k])
-            throw std::runtime_error("front " + std::to_string(s) + " has " + std::to_string(m) +
-                                     " rows but column count " + std::to_string(S.count[k]));
-        rows_off[s + 1] = rows_off[s] + m;
+        const int cnt = S.count[t.first_col[s]];
+        if (cnt < t.ncols[s] || cnt > n - t.first_col[s])
+            throw std::runtime_error("front " + std::to_string(s) + ": column count " +
+                                     std::to_string(cnt) + " out of range");
+        rows_off[s + 1] = rows_off[s] + cnt;
     }
     if (rows_off[ns] > INT32_MAX) throw std::runtime_error("row arrays exceed 2^31 entries");
     P.rows.resize(rows_off[ns]);
     P.relmap.assign(rows_off[ns], -1);
-    for (int s = 0; s < ns; ++s)
-        std::copy(rows[s].begin(), rows[s].end(), P.rows.begin() + rows_off[s]);
-    // relative maps: position of each update row of s inside its parent's rows
-    for (int s = 0; s < ns; ++s) {
-        int p = parent[s];
-        if (p < 0) continue;
-        const auto& rs = rows[s];
-        const auto& rp = rows[p];
-        size_t q = 0;
-        for (size_t i = t.ncols[s]; i < rs.size(); ++i) {
-            while (q < rp.size() && rp[q] < rs[i]) ++q;
-            if (q == rp.size() || rp[q] != rs[i]) throw std::runtime_error("row not in parent");
-            P.relmap[rows_off[s] + i] = (int)q;
+    const auto ranges = tree_ranges(t, parent);
+    for_each_range(ranges, [&](int s0, int s1) {
+        std::vector<int> scratch;
+        for (int s = s0; s < s1; ++s) {
+            int k = t.first_col[s], c = t.ncols[s];
+            scratch.clear();
+            for (int j = k; j < k + c; ++j)
+                for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
+                    if (A.rowidx[p] >= k + c) scratch.push_back(A.rowidx[p]);
+            for (int h = t.child_ptr[s]; h < t.child_ptr[s + 1]; ++h) {
+                int ch = t.child[h];
+                for (int64_t i = rows_off[ch] + t.ncols[ch]; i < rows_off[ch + 1]; ++i) {
+                    const int rc = P.rows[i];
+                    if (rc < k) throw std::runtime_error("child update row below its parent");
+                    if (rc >= k + c) scratch.push_back(rc);
+                }
+            }
+            std::sort(scratch.begin(), scratch.end());
+            scratch.erase(std::unique(scratch.begin(), scratch.end()), scratch.end());
+            const int64_t m = c + (int64_t)scratch.size();
+            if (m != rows_off[s + 1] - rows_off[s])
+                throw std::runtime_error("front " + std::to_string(s) + " has " + std::to_string(m) +
+                                         " rows but column count " + std::to_string(S.count[k]));
+            int* r = P.rows.data() + rows_off[s];
+            for (int i = 0; i < c; ++i) r[i] = k + i;
+            std::copy(scratch.begin(), scratch.end(), r + c);
         }
-    }
+        // relative maps: position of each update row of s inside its parent's rows
+        for (int s = s0; s < s1; ++s) {
+            int p = parent[s];
+            if (p < 0) continue;
+            const int* rs = P.rows.data() + rows_off[s];
+            const int* rp = P.rows.data() + rows_off[p];
+            const int64_t ms = rows_off[s + 1] - rows_off[s], mp = rows_off[p + 1] - rows_off[p];
+            int64_t q = 0;
+            for (int64_t i = t.ncols[s]; i < ms; ++i) {
+                while (q < mp && rp[q] < rs[i]) ++q;
+                if (q == mp || rp[q] != rs[i]) throw std::runtime_error("row not in parent");
+                P.relmap[rows_off[s] + i] = (int)q;
+            }
+        }
+    });
 
     // storage offsets and descriptors
     P.fronts.resize(ns);
     int64_t lo = 0, uo = 0;
     for (int s = 0; s < ns; ++s) {
         FrontDesc& f = P.fronts[s];
-        f.m = (int)rows[s].size();
+        f.m = (int)(rows_off[s + 1] - rows_off[s]);
         f.c = t.ncols[s];
         f.ldl = round8(f.m);
         int u = f.m - f.c;
