@@ -290,6 +290,8 @@ void upload_plan(mdgpu_handle_s* h) {
             D.solve.asm_tasks = reinterpret_cast<int2*>(h->keep(upload(at)));
             D.solve.asm_task_beg = SS.asm_task_beg;
         }
+        D.solve.warp_list = h->keep(upload(SS.warp_list));
+        D.solve.warp_cnt = SS.warp_cnt;
         D.solve.gather_nch = h->keep(upload(SS.gather_nch));
         D.solve.gather_off = h->keep(upload(SS.gather_off));
         D.solve.nflags = SS.nflags;

@@ -109,6 +109,10 @@ struct SolveSchedule {
     // forward assembly chunks of the large fronts
     int2* asm_tasks = nullptr;
     std::vector<int> asm_task_beg;
+    // small fronts per level by rows descending, and per level the counts
+    // taking one, two and four fronts per warp (see SolveScheduleHost)
+    int* warp_list = nullptr;
+    std::vector<int> warp_cnt;
 };
 
 struct DevPlan {

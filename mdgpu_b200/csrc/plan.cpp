@@ -67,6 +67,9 @@ int front_tiles(int m, int c, int T) { return (c + T - 1) / T + (m - c + T - 1) 
 
 void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& P) {
     P = Plan();
+    if (large_threshold > Plan::kSmallMaxRows ||
+        Plan::small_limit[kSmallBuckets - 1] != Plan::kSmallMaxRows)
+        throw std::runtime_error("small fronts must have at most 160 rows");
     const AssemblyTree& t = S.tree;
     int n = S.n, ns = t.size();
     P.n = n;
@@ -392,6 +395,19 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
             emit(ks);
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
+    }
+    S.warp_list.clear();
+    S.warp_cnt.assign(3 * (size_t)P.nlevels, 0);
+    for (int l = 0; l < P.nlevels; ++l) {
+        const int b = P.small_ptr[l * kSmallBuckets], e = P.small_ptr[(l + 1) * kSmallBuckets];
+        std::vector<int> w(P.small_list.begin() + b, P.small_list.begin() + e);
+        std::stable_sort(w.begin(), w.end(),
+                         [&](int x, int y) { return P.fronts[x].m > P.fronts[y].m; });
+        for (int s : w) {
+            const int m = P.fronts[s].m;
+            S.warp_cnt[3 * l + (m > 16 ? 0 : (m > 8 ? 1 : 2))]++;
+        }
+        S.warp_list.insert(S.warp_list.end(), w.begin(), w.end());
     }
     S.asm_tasks.clear();
     S.asm_task_beg.assign(P.nlevels + 1, 0);

@@ -86,6 +86,7 @@ struct Plan {
 
     static const int small_limit[kSmallBuckets];
     static constexpr int kTinyBuckets = 2;  // buckets of fronts with m <= 32
+    static constexpr int kSmallMaxRows = 160;  // small_limit[kSmallBuckets - 1]
 };
 
 // Largest m handled by the fused one-CTA-per-front kernel for a scalar size.
@@ -157,6 +158,12 @@ struct SolveScheduleHost {
     std::vector<int> gather_task_beg;   // nlevels + 1, in tasks
     std::vector<int> gather_nch, gather_off;  // per supernode
     int64_t gather_vecs = 0;            // partial vectors the largest level needs
+    // small fronts of each level for the warp-per-front sweeps, by rows
+    // descending (same level ranges as small_list): warp_cnt[3 l + k] fronts
+    // of more than 16 rows (k = 0, a warp each), of 9..16 rows (k = 1, two
+    // per warp) and of at most 8 rows (k = 2, four per warp)
+    std::vector<int> warp_list;
+    std::vector<int> warp_cnt;
 };
 
 int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling

@@ -629,128 +629,422 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 }
 
 // ---------------------------------------------------------------------------
-// tiny fronts (m <= 32, one right-hand side): a warp per front, one row per
-// lane; pivots by shuffles, dot products by warp reductions, no barriers
+// small fronts with at most kWarpSolveRhs right-hand sides: a warp per front,
+// lane l holding rows l, l + 32, ... (R slots, m <= 32 R) of NQ right-hand
+// sides in registers.  Forward: the pivot value is broadcast by a shuffle and
+// every lane updates its rows below it; backward: a warp reduction per pivot
+// column (dot product with the final rows below it).  No block barriers; the
+// children's update parts are summed into a per-warp shared buffer (child by
+// child, deterministic) before the rows are taken into registers.
 // ---------------------------------------------------------------------------
 
-constexpr int kTinyRows = 32;
+constexpr int kWarpSolveRhs = 4;  // right-hand sides per pass of the warp path
 
-template <typename TL, typename TV>
-__device__ void fwd_tiny_front(int s, const FrontDesc* __restrict__ fronts,
-                               const int* __restrict__ child, const int* __restrict__ relmap,
-                               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
-                               TV* __restrict__ xp, TV* __restrict__ fv, TV* wbuf) {
-    const int lane = threadIdx.x & 31;
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c;
-    const TL* L = Ls + F.loff;
-    wbuf[lane] = lane < c ? xp[F.first_col + lane] : TV(0);
-    __syncwarp();
-    for (int h = F.child_beg; h < F.child_end; ++h) {  // children in order
-        const int ch = child[h];
-        const FrontDesc g = fronts[ch];
-        const int uc = g.m - g.c;
-        const TV* w = front_vec(fv, fv_off, ch, 1);
-        const int* rm = relmap + g.rows_off + g.c;
-        for (int rr = lane; rr < uc; rr += 32) wbuf[rm[rr]] += w[g.c + rr];
-        __syncwarp();
-    }
-    TV v = wbuf[lane];
-    __syncwarp();
-    for (int j = 0; j < c; ++j) {
-        if (lane == j) v = v / (TV)L[j + (int64_t)j * F.ldl];
-        const TV yj = __shfl_sync(0xffffffffu, v, j);
-        if (lane > j && lane < m) v -= (TV)L[lane + (int64_t)j * F.ldl] * yj;
-    }
-    if (lane < c)
-        xp[F.first_col + lane] = v;
-    else if (lane < m)
-        front_vec(fv, fv_off, s, 1)[lane] = v;
+// Fronts of at most W rows (W = 8, 16, 32) on a group of W lanes of a warp
+// (32 / W fronts per warp), one row per lane.  mask: the group's lanes; the
+// group's rows of the warp buffer are wbuf[q * 32 + r].
+template <int W>
+__device__ __forceinline__ unsigned group_mask() {
+    return W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1)));
 }
 
-template <typename TL, typename TV>
-__device__ void bwd_tiny_front(int s, const FrontDesc* __restrict__ fronts,
-                               const int* __restrict__ rows, const TL* __restrict__ Ls,
-                               TV* __restrict__ xp) {
-    const int lane = threadIdx.x & 31;
-    const FrontDesc F = fronts[s];
+template <typename TL, typename TV, int W, int NQ>
+__device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict__ fronts,
+                                const int* __restrict__ child, const int* __restrict__ relmap,
+                                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                                TV* __restrict__ xp, TV* __restrict__ out, TV* __restrict__ fv,
+                                int n, int nrhs, TV* wbuf) {
+    const unsigned mask = group_mask<W>();
+    const int r = threadIdx.x & (W - 1);
     const int m = F.m, c = F.c;
+    const int64_t ldl = F.ldl;
     const TL* L = Ls + F.loff;
-    // pivot lanes: y; update lanes: the final x of their (ancestor) rows
-    TV v = lane < c ? xp[F.first_col + lane]
-                    : (lane < m ? xp[rows[F.rows_off + lane]] : TV(0));
-    for (int j = 0; j < c; ++j) {  // t_j = y_j - L(u, j)' x_u
-        TV p = (lane >= c && lane < m) ? (TV)L[lane + (int64_t)j * F.ldl] * v : TV(0);
+    for (int q0 = 0; q0 < nrhs; q0 += NQ) {
+        const int nq = min(NQ, nrhs - q0);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-        if (lane == j) v -= p;
+        for (int q = 0; q < NQ; ++q)
+            if (q < nq && r < m)
+                wbuf[q * 32 + r] = r < c ? xp[F.first_col + r + (int64_t)(q0 + q) * n] : TV(0);
+        __syncwarp(mask);
+        for (int h = F.child_beg; h < F.child_end; ++h) {  // children in order
+            const int ch = child[h];
+            const FrontDesc g = fronts[ch];
+            const int uc = g.m - g.c;
+            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c + (int64_t)q0 * g.m;
+            if (r < uc) {  // uc < m <= W
+                const int p = relmap[g.rows_off + g.c + r];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    if (q < nq) wbuf[q * 32 + p] += w[r + (int64_t)q * g.m];
+            }
+            __syncwarp(mask);
+        }
+        TV v[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) v[q] = (q < nq && r < m) ? wbuf[q * 32 + r] : TV(0);
+        __syncwarp(mask);
+        // column j of L for this lane's row, one column ahead of its use
+        TV lc = (r > 0 && r < m) ? (TV)L[r] : TV(0), d = (TV)L[0];
+        for (int j = 0; j < c; ++j) {
+            TV ln = TV(0), dn = TV(1);
+            if (j + 1 < c) {
+                const TL* cn = L + (j + 1) * ldl;
+                dn = (TV)cn[j + 1];
+                ln = (r > j + 1 && r < m) ? (TV)cn[r] : TV(0);
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const TV y = __shfl_sync(mask, v[q], j, W) / d;
+                if (r == j)
+                    v[q] = y;
+                else if (r > j)
+                    v[q] -= lc * y;
+            }
+            lc = ln;
+            d = dn;
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            if (q >= nq || r >= m) continue;
+            if (r < c)
+                xp[F.first_col + r + (int64_t)(q0 + q) * n] = v[q];
+            else
+                out[r + (int64_t)(q0 + q) * m] = v[q];
+        }
     }
-    for (int j = c - 1; j >= 0; --j) {  // L11' x = t, last pivot first
-        if (lane == j) v = v / (TV)L[j + (int64_t)j * F.ldl];
-        const TV xj = __shfl_sync(0xffffffffu, v, j);
-        if (lane < j) v -= (TV)L[j + (int64_t)lane * F.ldl] * xj;
+}
+
+template <typename TL, typename TV, int W, int NQ>
+__device__ void bwd_group_front(const FrontDesc& F, const int* __restrict__ rows,
+                                const TL* __restrict__ Ls, TV* __restrict__ xp, int n, int nrhs) {
+    const unsigned mask = group_mask<W>();
+    const int r = threadIdx.x & (W - 1);
+    const int m = F.m, c = F.c;
+    const int64_t ldl = F.ldl;
+    const TL* L = Ls + F.loff;
+    // this lane's row in the solution: a pivot row, else an ancestor's
+    const int src = r < c ? F.first_col + r : (r < m ? rows[F.rows_off + r] : 0);
+    for (int q0 = 0; q0 < nrhs; q0 += NQ) {
+        const int nq = min(NQ, nrhs - q0);
+        TV v[NQ];  // y on the pivot rows (x once solved), final x on the others
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            v[q] = (q < nq && r < m) ? xp[src + (int64_t)(q0 + q) * n] : TV(0);
+        const int jl = c - 1;
+        TV lc = (r > jl && r < m) ? (TV)L[r + jl * ldl] : TV(0), d = (TV)L[jl + jl * ldl];
+        for (int j = jl; j >= 0; --j) {
+            TV ln = TV(0), dn = TV(1);
+            if (j > 0) {
+                const TL* cn = L + (j - 1) * ldl;
+                dn = (TV)cn[j - 1];
+                ln = (r > j - 1 && r < m) ? (TV)cn[r] : TV(0);
+            }
+            TV p[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) p[q] = lc * v[q];
+#pragma unroll
+            for (int o = W / 2; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) p[q] += __shfl_xor_sync(mask, p[q], o, W);
+            if (r == j) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) v[q] = (v[q] - p[q]) / d;
+            }
+            lc = ln;
+            d = dn;
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            if (q < nq && r < c) xp[F.first_col + r + (int64_t)(q0 + q) * n] = v[q];
     }
-    if (lane < c) xp[F.first_col + lane] = v;
+}
+
+// Fronts of 33..160 rows: the same sweeps with the front vector kept in the
+// warp's shared buffer (ld MR rows per right-hand side) instead of registers.
+template <typename TL, typename TV, int NQ>
+__device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restrict__ fronts,
+                                    const int* __restrict__ child, const int* __restrict__ relmap,
+                                    const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                                    TV* __restrict__ xp, TV* __restrict__ out, TV* __restrict__ fv,
+                                    int n, int nrhs, TV* f, int MR) {
+    const int lane = threadIdx.x & 31;
+    const int m = F.m, c = F.c;
+    const int64_t ldl = F.ldl;
+    const TL* L = Ls + F.loff;
+    for (int q0 = 0; q0 < nrhs; q0 += NQ) {
+        const int nq = min(NQ, nrhs - q0);
+        for (int r = lane; r < m; r += 32)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                if (q < nq)
+                    f[q * MR + r] = r < c ? xp[F.first_col + r + (int64_t)(q0 + q) * n] : TV(0);
+        __syncwarp();
+        for (int h = F.child_beg; h < F.child_end; ++h) {  // children in order
+            const int ch = child[h];
+            const FrontDesc g = fronts[ch];
+            const int uc = g.m - g.c;
+            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c + (int64_t)q0 * g.m;
+            const int* rm = relmap + g.rows_off + g.c;
+            for (int rr = lane; rr < uc; rr += 32) {
+                const int p = rm[rr];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    if (q < nq) f[q * MR + p] += w[rr + (int64_t)q * g.m];
+            }
+            __syncwarp();
+        }
+        for (int j = 0; j < c; ++j) {
+            const TL* col = L + j * ldl;
+            const TV d = (TV)col[j];
+            TV y[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) y[q] = f[q * MR + j] / d;
+            if (lane == (j & 31)) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    if (q < nq) xp[F.first_col + j + (int64_t)(q0 + q) * n] = y[q];
+            }
+            for (int r = j + 1 + lane; r < m; r += 32) {
+                const TV l = (TV)col[r];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) f[q * MR + r] -= l * y[q];
+            }
+            __syncwarp();
+        }
+        for (int r = c + lane; r < m; r += 32)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                if (q < nq) out[r + (int64_t)(q0 + q) * m] = f[q * MR + r];
+        __syncwarp();
+    }
+}
+
+template <typename TL, typename TV, int NQ>
+__device__ void bwd_warp_front_smem(const FrontDesc& F, const int* __restrict__ rows,
+                                    const TL* __restrict__ Ls, TV* __restrict__ xp, int n,
+                                    int nrhs, TV* x, int MR) {
+    const int lane = threadIdx.x & 31;
+    const int m = F.m, c = F.c;
+    const int64_t ldl = F.ldl;
+    const TL* L = Ls + F.loff;
+    const int* rw = rows + F.rows_off;
+    for (int q0 = 0; q0 < nrhs; q0 += NQ) {
+        const int nq = min(NQ, nrhs - q0);
+        for (int r = lane; r < m; r += 32) {
+            const int src = r < c ? F.first_col + r : rw[r];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                x[q * MR + r] = q < nq ? xp[src + (int64_t)(q0 + q) * n] : TV(0);
+        }
+        __syncwarp();
+        for (int j = c - 1; j >= 0; --j) {
+            const TL* col = L + j * ldl;
+            TV p[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) p[q] = TV(0);
+            for (int r = j + 1 + lane; r < m; r += 32) {
+                const TV l = (TV)col[r];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) p[q] += l * x[q * MR + r];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) p[q] += __shfl_xor_sync(0xffffffffu, p[q], o);
+            const TV d = (TV)col[j];
+            if (lane == (j & 31)) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const TV v = (x[q * MR + j] - p[q]) / d;
+                    x[q * MR + j] = v;
+                    if (q < nq) xp[F.first_col + j + (int64_t)(q0 + q) * n] = v;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// dispatch on the front's rows: registers up to 32, the shared buffer above
+template <typename TL, typename TV, int NQ>
+__device__ void fwd_warp_front(int s, const FrontDesc* __restrict__ fronts,
+                               const int* __restrict__ child, const int* __restrict__ relmap,
+                               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                               TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
+                               TV* wbuf, int MR) {
+    const FrontDesc F = fronts[s];
+    TV* out = front_vec(fv, fv_off, s, nrhs);
+    if (F.m <= 32)
+        fwd_group_front<TL, TV, 32, NQ>(F, fronts, child, relmap, fv_off, Ls, xp, out, fv, n, nrhs,
+                                        wbuf);
+    else
+        fwd_warp_front_smem<TL, TV, NQ>(F, fronts, child, relmap, fv_off, Ls, xp, out, fv, n, nrhs,
+                                        wbuf, MR);
+}
+
+template <typename TL, typename TV, int NQ>
+__device__ void bwd_warp_front(int s, const FrontDesc* __restrict__ fronts,
+                               const int* __restrict__ rows, const TL* __restrict__ Ls,
+                               TV* __restrict__ xp, int n, int nrhs, TV* wbuf, int MR) {
+    const FrontDesc F = fronts[s];
+    if (F.m <= 32)
+        bwd_group_front<TL, TV, 32, NQ>(F, rows, Ls, xp, n, nrhs);
+    else
+        bwd_warp_front_smem<TL, TV, NQ>(F, rows, Ls, xp, n, nrhs, wbuf, MR);
+}
+
+// per-warp shared buffer of the warp path: MR = rows rounded up to 32, times
+// the right-hand sides of one pass
+__host__ __device__ constexpr int warp_rows(int msmall) { return ((msmall + 31) / 32) * 32; }
+__host__ __device__ constexpr int warp_buf_stride(int msmall, int nrhs) {
+    return warp_rows(msmall) * (nrhs == 1 ? 1 : kWarpSolveRhs);
+}
+
+// Warp tasks of one level's small fronts (the level's slice of the rows-
+// descending warp list): tasks [0, n1) one front each, then two fronts of
+// 9..16 rows per task, then four of at most 8 rows.
+struct WarpTasks {
+    const int* list;
+    int n1, n2, n4;
+    __host__ __device__ int count() const { return n1 + (n2 + 1) / 2 + (n4 + 3) / 4; }
+};
+
+// Blocks that run warp tasks: at most kWarpTaskBlocks, each warp looping over
+// tasks with the grid's warp count as stride.
+constexpr int kWarpTaskBlocks = 148 * 8;
+
+template <typename TL, typename TV, int NQ>
+__device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __restrict__ fronts,
+                              const int* __restrict__ child, const int* __restrict__ relmap,
+                              const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
+                              TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs, TV* wbuf,
+                              int MR) {
+    const int lane = threadIdx.x & 31;
+    if (t < wt.n1) {
+        fwd_warp_front<TL, TV, NQ>(wt.list[t], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
+                                   wbuf, MR);
+        return;
+    }
+    t -= wt.n1;
+    const int t2 = (wt.n2 + 1) / 2;
+    if (t < t2) {
+        const int k = 2 * t + (lane >> 4);
+        if (k < wt.n2) {
+            const int s = wt.list[wt.n1 + k];
+            const FrontDesc F = fronts[s];
+            fwd_group_front<TL, TV, 16, NQ>(F, fronts, child, relmap, fv_off, Ls, xp,
+                                            front_vec(fv, fv_off, s, nrhs), fv, n, nrhs,
+                                            wbuf + (lane & 16));
+        }
+        return;
+    }
+    const int k = 4 * (t - t2) + (lane >> 3);
+    if (k < wt.n4) {
+        const int s = wt.list[wt.n1 + wt.n2 + k];
+        const FrontDesc F = fronts[s];
+        fwd_group_front<TL, TV, 8, NQ>(F, fronts, child, relmap, fv_off, Ls, xp,
+                                       front_vec(fv, fv_off, s, nrhs), fv, n, nrhs,
+                                       wbuf + (lane & 24));
+    }
+}
+
+template <typename TL, typename TV, int NQ>
+__device__ void bwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __restrict__ fronts,
+                              const int* __restrict__ rows, const TL* __restrict__ Ls,
+                              TV* __restrict__ xp, int n, int nrhs, TV* wbuf, int MR) {
+    const int lane = threadIdx.x & 31;
+    if (t < wt.n1) {
+        bwd_warp_front<TL, TV, NQ>(wt.list[t], fronts, rows, Ls, xp, n, nrhs, wbuf, MR);
+        return;
+    }
+    t -= wt.n1;
+    const int t2 = (wt.n2 + 1) / 2;
+    if (t < t2) {
+        const int k = 2 * t + (lane >> 4);
+        if (k < wt.n2) bwd_group_front<TL, TV, 16, NQ>(fronts[wt.list[wt.n1 + k]], rows, Ls, xp, n, nrhs);
+        return;
+    }
+    const int k = 4 * (t - t2) + (lane >> 3);
+    if (k < wt.n4)
+        bwd_group_front<TL, TV, 8, NQ>(fronts[wt.list[wt.n1 + wt.n2 + k]], rows, Ls, xp, n, nrhs);
 }
 
 // One launch per level before the large-front chain (128 threads, 256 when
-// it holds gather tasks), forward: the small
-// fronts (CTA each) and the large fronts' vector assembly (CTA each) -- both
-// depend only on lower levels.  Backward: the update-row partial sums of the
-// large fronts and the small fronts -- both depend only on ancestors.
+// it holds gather tasks), forward: the small fronts and the large fronts'
+// vector assembly (CTA each) -- both depend only on lower levels.  Backward:
+// the update-row partial sums of the large fronts and the small fronts --
+// both depend only on ancestors.  With at most kWarpSolveRhs right-hand sides
+// the small fronts are warp tasks on the first wblocks blocks (wt.count() > 0),
+// else a CTA each (small_list, nsmall of them; wt empty).
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(256)
-    k_fwd_prep(const FrontDesc* __restrict__ fronts, const int* __restrict__ small_list,
-               int nsmall, int ntiny, const int2* __restrict__ asm_tasks, const int* __restrict__ child,
-               const int* __restrict__ relmap, const int* __restrict__ asm_off,
-               const int* __restrict__ asm_range, const int64_t* __restrict__ fv_off,
-               const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
-               int msmall) {
-    const int wpb = blockDim.x >> 5;
-    const int tb = (ntiny + wpb - 1) / wpb;  // blocks of tiny fronts (a warp each)
+__global__ void __launch_bounds__(256, 4)
+    k_fwd_prep(const FrontDesc* __restrict__ fronts, WarpTasks wt, int wblocks,
+               const int* __restrict__ small_list, int nsmall, const int2* __restrict__ asm_tasks,
+               const int* __restrict__ child, const int* __restrict__ relmap,
+               const int* __restrict__ asm_off, const int* __restrict__ asm_range,
+               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
+               TV* __restrict__ fv, int n, int nrhs, int msmall) {
     int b = blockIdx.x;
-    if (b < tb) {
+    if (b < wblocks) {
         extern __shared__ __align__(16) unsigned char smem_raw[];
-        const int w = threadIdx.x >> 5, q = b * wpb + w;
-        if (q < ntiny)
-            fwd_tiny_front<TL, TV>(small_list[q], fronts, child, relmap, fv_off, Ls, xp, fv,
-                                   reinterpret_cast<TV*>(smem_raw) + w * kTinyRows);
+        const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
+        TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
+        const int ntask = wt.count();
+        for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
+            if (nrhs == 1)
+                fwd_warp_task<TL, TV, 1>(wt, t, fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
+                                         wbuf, warp_rows(msmall));
+            else
+                fwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, child, relmap, fv_off, Ls, xp,
+                                                     fv, n, nrhs, wbuf, warp_rows(msmall));
+            __syncwarp();
+        }
         return;
     }
-    b -= tb;
-    if (b < nsmall - ntiny) {
-        fwd_small_front<TL, TV>(small_list[ntiny + b], fronts, child, relmap, fv_off, Ls, xp, fv,
-                                n, nrhs, msmall);
+    b -= wblocks;
+    if (b < nsmall) {
+        fwd_small_front<TL, TV>(small_list[b], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
+                                msmall);
     } else {
-        const int2 t = asm_tasks[b - (nsmall - ntiny)];
+        const int2 t = asm_tasks[b - nsmall];
         fwd_assemble_chunk<TV>(t.x, t.y, fronts, child, relmap, asm_off, asm_range, fv_off, xp, fv,
                                n, nrhs);
     }
 }
 
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_bwd_prep(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
-               const int* __restrict__ small_list, int ntiny, const int* __restrict__ rows,
-               const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
-               const TL* __restrict__ Ls, TV* __restrict__ xp, TV* __restrict__ part, int n,
-               int nrhs, int umax, int msmall) {
+               WarpTasks wt, int wblocks, const int* __restrict__ small_list, int nsmall,
+               const int* __restrict__ rows, const int* __restrict__ gather_nch,
+               const int* __restrict__ gather_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
+               TV* __restrict__ part, int n, int nrhs, int umax, int msmall) {
     const int b = blockIdx.x;
     if (b < ngather) {
         bwd_gather_task<TL, TV, NQ>(gtasks[b], fronts, rows, gather_nch, gather_off, Ls, xp, part,
                                     n, nrhs);
         return;
     }
-    const int wpb = blockDim.x >> 5;
-    const int tb = (ntiny + wpb - 1) / wpb;  // blocks of tiny fronts (a warp each)
     const int bb = b - ngather;
-    if (bb < tb) {
-        const int q = bb * wpb + (threadIdx.x >> 5);
-        if (q < ntiny) bwd_tiny_front<TL, TV>(small_list[q], fronts, rows, Ls, xp);
+    if (bb < wblocks) {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
+        TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
+        const int ntask = wt.count();
+        for (int t = bb * wpb + w; t < ntask; t += wblocks * wpb) {
+            if (nrhs == 1)
+                bwd_warp_task<TL, TV, 1>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
+                                         warp_rows(msmall));
+            else
+                bwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
+                                                     warp_rows(msmall));
+            __syncwarp();
+        }
         return;
     }
-    bwd_small_front<TL, TV>(small_list[ntiny + bb - tb], fronts, rows, Ls, xp, n, nrhs, umax,
-                            msmall);
+    if (bb - wblocks < nsmall)
+        bwd_small_front<TL, TV>(small_list[bb - wblocks], fronts, rows, Ls, xp, n, nrhs, umax,
+                                msmall);
 }
 
 // Backward, task (s, j): pivot column tile j of front s accumulates
@@ -1002,11 +1296,16 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     const int ns = se - sb;
     const int lb = D.h_large_ptr[l], nl = D.h_large_ptr[l + 1] - lb;
     const int msmall = level_msmall(D, l);
-    // small fronts of at most kTinyRows rows (the first two buckets) take the
-    // warp path when there is one right-hand side
-    static_assert(Plan::kTinyBuckets == 2, "buckets 0 and 1 hold m <= 16 and m <= 32");
-    const int ntiny =
-        nrhs == 1 ? D.h_small_ptr[l * kSmallBuckets + Plan::kTinyBuckets] - sb : 0;
+    // with at most kWarpSolveRhs right-hand sides every small front takes the
+    // warp path
+    static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 5 rows per lane");
+    const int nwarp = nrhs <= kWarpSolveRhs ? ns : 0;
+    WarpTasks wt{S.warp_list + sb, 0, 0, 0};
+    if (nwarp > 0) {
+        wt.n1 = S.warp_cnt[3 * l];
+        wt.n2 = S.warp_cnt[3 * l + 1];
+        wt.n4 = S.warp_cnt[3 * l + 2];
+    }
     const size_t lsm = level_smem_bytes<TL, TV>(nrhs);
     const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
@@ -1018,12 +1317,14 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
     if (forward) {
         const int ab = S.asm_task_beg[l], na = S.asm_task_beg[l + 1] - ab;
-        const int tb = (ntiny + 3) / 4;  // 128 threads: four tiny fronts per CTA
+        const int nsm = ns - nwarp;  // small fronts on a CTA each
+        const int wblocks = std::min((wt.count() + 3) / 4, kWarpTaskBlocks);  // 4 warps a block
+        const size_t sm = nwarp > 0 ? 4 * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV)
+                                    : small_fwd_smem<TL, TV>(msmall, nrhs);
         if (ns + na > 0)
-            k_fwd_prep<TL, TV><<<tb + (ns - ntiny) + na, 128, small_fwd_smem<TL, TV>(msmall, nrhs),
-                                 st>>>(D.fronts, D.small_list + sb, ns, ntiny, S.asm_tasks + ab,
-                                       D.child, D.relmap, D.asm_off, D.asm_range, D.fv_off, Ls, xp,
-                                       fv, n, nrhs, msmall);
+            k_fwd_prep<TL, TV><<<wblocks + nsm + na, 128, sm, st>>>(
+                D.fronts, wt, wblocks, D.small_list + sb, nsm, S.asm_tasks + ab, D.child, D.relmap,
+                D.asm_off, D.asm_range, D.fv_off, Ls, xp, fv, n, nrhs, msmall);
         if (nt > 0)
             k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
                                                         fv + D.fv_pub_off * nrhs, abort_flag,
@@ -1033,14 +1334,17 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
         if (ng + ns > 0) {
-            size_t sm = small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
-            if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
             // the gather's thread layout needs 256 threads; small fronts alone run on 128
             const int threads = ng > 0 ? 256 : 128;
-            const int tb = (ntiny + threads / 32 - 1) / (threads / 32);
-            k_bwd_prep<TL, TV, NQ><<<ng + tb + (ns - ntiny), threads, sm, st>>>(
-                D.fronts, S.tasks + gb, ng, D.small_list + sb, ntiny, D.rows, S.gather_nch,
-                S.gather_off, Ls, xp, part, n, nrhs, msmall, msmall);
+            const int nsm = ns - nwarp;
+            const int wpb = threads / 32;
+            const int wblocks = std::min((wt.count() + wpb - 1) / wpb, kWarpTaskBlocks);
+            size_t sm = nwarp > 0 ? wpb * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV)
+                                  : small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
+            if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
+            k_bwd_prep<TL, TV, NQ><<<ng + wblocks + nsm, threads, sm, st>>>(
+                D.fronts, S.tasks + gb, ng, wt, wblocks, D.small_list + sb, nsm, D.rows,
+                S.gather_nch, S.gather_off, Ls, xp, part, n, nrhs, msmall, msmall);
         }
         if (nt > 0)
             k_bwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,

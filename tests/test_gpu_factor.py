@@ -81,6 +81,31 @@ def test_multiple_rhs_and_device_api():
     np.testing.assert_allclose(dX.cpu().numpy(), X, rtol=0, atol=1e-12 * np.abs(X).max())
 
 
+@pytest.mark.parametrize("name", ["2d100_amd_sn", "3d16_amd_rn4", "rnd300_amd_sn"])
+def test_solves_with_each_rhs_count_match_oracle(name):
+    """Small fronts take a warp each (rows in registers up to 32, in the warp's
+    shared buffer up to 160) with at most 4 right-hand sides, a CTA each with
+    more; every count must give the oracle's solution column by column."""
+    _, gen, amd, mode, z = next(c for c in CASES if c[0] == name)
+    n, Ap, Ai, Ax = gen()
+    P = O.Plan(n, Ap, Ai, Ax, amd=amd, mode=mode, rn_zeros=z)
+    ref = P.factor()
+    S = M.Solver(n, Ap, Ai, ordering=int(amd), tree=TREE[mode], relax_zeros=z)
+    assert S.array("rows_ptr").size > 1
+    S.factor(Ax, M.FP64)
+    B = mg.rhs_uniform(n, seed=9, nrhs=9)
+    xr = [P.solve(ref["Li"], ref["Lx"], B[:, q]) for q in range(9)]
+    for k in (1, 2, 3, 4, 5, 9):
+        X = S.solve(B[:, :k]).reshape(n, k)
+        for q in range(k):
+            assert np.abs(X[:, q] - xr[q]).max() / np.abs(xr[q]).max() <= 1e-10, (k, q)
+    S.factor(Ax, M.FP32)
+    for k in (1, 3, 4, 5):
+        X = S.solve(B[:, :k]).reshape(n, k)
+        for q in range(k):
+            assert np.abs(X[:, q] - xr[q]).max() / np.abs(xr[q]).max() <= 1e-3, (k, q)
+
+
 @pytest.mark.parametrize("side", [16, 24])
 def test_fp32_factor_with_refinement_reaches_fp64_accuracy(side):
     n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(side, seed=0)
