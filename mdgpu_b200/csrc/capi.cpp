@@ -234,16 +234,11 @@ void upload_plan(mdgpu_handle_s* h) {
     D.large_list = h->keep(upload(P.large_list));
     D.h_small_ptr = P.small_ptr;
     D.h_large_ptr = P.large_ptr;
-    std::vector<int64_t> fvo(P.nsuper);
-    int64_t acc = 0;
-    for (int s = 0; s < P.nsuper; ++s) {
-        fvo[s] = acc;
-        acc += P.fronts[s].m;
-    }
+    const int64_t acc = h->ssched.fv_rows;
     D.fv_fronts = acc;
     D.fv_pub_off = acc + h->ssched.gather_vecs * kTile;
     D.fv_total = D.fv_pub_off + 2 * (int64_t)h->ssched.nflags * kTile;
-    D.fv_off = h->keep(upload(fvo));
+    D.fv_off = h->keep(upload(h->ssched.fv_off));
     D.dinv_off = h->keep(upload(P.dinv_off));
     {
         // panel scratch: fronts of one level side by side, levels reuse it
@@ -284,12 +279,9 @@ void upload_plan(mdgpu_handle_s* h) {
         D.solve.bwd_elems = SS.bwd_elems;
         D.solve.small_elems = SS.small_elems;
         D.solve.gather_task_beg = SS.gather_task_beg;
-        {
-            std::vector<int> at = SS.asm_tasks;
-            if (at.empty()) at.assign(2, 0);
-            D.solve.asm_tasks = reinterpret_cast<int2*>(h->keep(upload(at)));
-            D.solve.asm_task_beg = SS.asm_task_beg;
-        }
+        D.solve.amap_off = h->keep(upload(SS.amap_off));
+        D.solve.amap_row = h->keep(upload(SS.amap_row));
+        D.solve.amap_ent = h->keep(upload(SS.amap_ent));
         D.solve.warp_list = h->keep(upload(SS.warp_list));
         D.solve.warp_cnt = SS.warp_cnt;
         D.solve.gather_nch = h->keep(upload(SS.gather_nch));

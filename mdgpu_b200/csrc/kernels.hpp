@@ -106,9 +106,10 @@ struct SolveSchedule {
     std::vector<int> gather_task_beg;
     int* gather_nch = nullptr;
     int* gather_off = nullptr;
-    // forward assembly chunks of the large fronts
-    int2* asm_tasks = nullptr;
-    std::vector<int> asm_task_beg;
+    // forward assembly of the large fronts as a gather (see SolveScheduleHost)
+    int* amap_off = nullptr;
+    int* amap_row = nullptr;
+    int* amap_ent = nullptr;
     // small fronts per level by rows descending, and per level the counts
     // taking one, two and four fronts per warp (see SolveScheduleHost)
     int* warp_list = nullptr;

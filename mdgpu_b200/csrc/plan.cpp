@@ -409,20 +409,40 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         }
         S.warp_list.insert(S.warp_list.end(), w.begin(), w.end());
     }
-    S.asm_tasks.clear();
-    S.asm_task_beg.assign(P.nlevels + 1, 0);
-    for (int l = 0; l < P.nlevels; ++l) {
-        S.asm_task_beg[l] = (int)(S.asm_tasks.size() / 2);
-        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-            const int s = P.large_list[q];
-            const int nc = (P.fronts[s].m + SolveScheduleHost::kAsmRows - 1) / SolveScheduleHost::kAsmRows;
-            for (int h = 0; h < nc; ++h) {
-                S.asm_tasks.push_back(s);
-                S.asm_tasks.push_back(h);
-            }
+    S.fv_off.assign(P.nsuper, 0);
+    S.fv_rows = 0;
+    for (int s = 0; s < P.nsuper; ++s) {
+        S.fv_off[s] = S.fv_rows;
+        S.fv_rows += P.fronts[s].m;
+    }
+    if (S.fv_rows > INT32_MAX) throw std::runtime_error("front vectors exceed 2^31 rows");
+    S.amap_off.assign(P.nsuper, -1);
+    S.amap_row.clear();
+    S.amap_ent.clear();
+    std::vector<int> cnt;
+    for (int s : P.large_list) {
+        const FrontDesc& f = P.fronts[s];
+        cnt.assign(f.m + 1, 0);
+        for (int h = f.child_beg; h < f.child_end; ++h) {
+            const FrontDesc& g = P.fronts[P.child[h]];
+            const int* rm = P.relmap.data() + g.rows_off + g.c;
+            for (int rr = 0; rr < g.m - g.c; ++rr) cnt[rm[rr] + 1]++;
+        }
+        for (int r = 0; r < f.m; ++r) cnt[r + 1] += cnt[r];
+        const int64_t base = (int64_t)S.amap_ent.size();
+        if (base + cnt[f.m] > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 entries");
+        S.amap_off[s] = (int)S.amap_row.size();
+        for (int r = 0; r <= f.m; ++r) S.amap_row.push_back((int)(base + cnt[r]));
+        S.amap_ent.resize(base + cnt[f.m]);
+        for (int h = f.child_beg; h < f.child_end; ++h) {  // child order kept per row
+            const int ch = P.child[h];
+            const FrontDesc& g = P.fronts[ch];
+            const int* rm = P.relmap.data() + g.rows_off + g.c;
+            for (int rr = 0; rr < g.m - g.c; ++rr)
+                S.amap_ent[base + cnt[rm[rr]]++] = (int)(S.fv_off[ch] + g.c + rr);
         }
     }
-    S.asm_task_beg[P.nlevels] = (int)(S.asm_tasks.size() / 2);
+    if (S.amap_row.size() > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 rows");
     const int GC = SolveScheduleHost::kGatherTiles;
     S.gather_task_beg.assign(P.nlevels + 1, 0);
     S.gather_nch.assign(P.nsuper, 0);

@@ -150,11 +150,6 @@ struct SolveScheduleHost {
     // chunk count and the first partial (pivot tile j, chunk h at
     // gather_off + j * gather_nch + h), counted within its level
     static constexpr int kGatherTiles = 16;
-    // forward assembly of the large fronts' vectors: tasks (front, chunk of
-    // kAsmRows rows) per level, packed (s, chunk)
-    static constexpr int kAsmRows = 1024;
-    std::vector<int> asm_tasks;
-    std::vector<int> asm_task_beg;      // nlevels + 1, in tasks
     std::vector<int> gather_task_beg;   // nlevels + 1, in tasks
     std::vector<int> gather_nch, gather_off;  // per supernode
     int64_t gather_vecs = 0;            // partial vectors the largest level needs
@@ -164,6 +159,17 @@ struct SolveScheduleHost {
     // per warp) and of at most 8 rows (k = 2, four per warp)
     std::vector<int> warp_list;
     std::vector<int> warp_cnt;
+    // front vectors: front s holds rows fv_off[s] .. fv_off[s] + m_s - 1 of
+    // one array (a row holds the right-hand sides side by side)
+    std::vector<int64_t> fv_off;
+    int64_t fv_rows = 0;
+    // forward assembly of the large fronts as a gather: row r of large front
+    // s sums the front-vector rows amap_ent[amap_row[amap_off[s] + r] ..
+    // amap_row[amap_off[s] + r + 1] - 1] (children's update rows, in child
+    // order, so the sums are those of a child-by-child scatter)
+    std::vector<int> amap_off;  // per supernode, -1 for small fronts
+    std::vector<int> amap_row;
+    std::vector<int> amap_ent;
 };
 
 int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling

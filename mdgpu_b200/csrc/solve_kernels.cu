@@ -19,54 +19,12 @@
 
 namespace mdgpu {
 
+// Front vector of supernode s: rows fv_off[s] .. fv_off[s] + m - 1 of one
+// array whose row holds the nrhs right-hand sides side by side, so row r,
+// right-hand side q is front_vec(...)[r * nrhs + q].
 template <typename TV>
 __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) {
     return fv + fv_off[s] * nrhs;
-}
-
-// ---------------------------------------------------------------------------
-// large fronts
-// ---------------------------------------------------------------------------
-
-// Rows [ch * kAsmRows, ...) of large front s's vector: the pivot rows from
-// the right-hand side, then every child's update rows that land there, child
-// by child (deterministic sums).  A child's rows landing in a row range are
-// contiguous (increasing relative map); the factor's assembly ranges (per
-// kAssembleCols-row block) give them.
-template <typename TV>
-__device__ void fwd_assemble_chunk(int s, int ch, const FrontDesc* __restrict__ fronts,
-                                   const int* __restrict__ child, const int* __restrict__ relmap,
-                                   const int* __restrict__ asm_off, const int* __restrict__ asm_range,
-                                   const int64_t* __restrict__ fv_off, const TV* __restrict__ xp,
-                                   TV* __restrict__ fv, int n, int nrhs) {
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c;
-    const int r0 = ch * SolveScheduleHost::kAsmRows, r1 = min(m, r0 + SolveScheduleHost::kAsmRows);
-    const int nr = r1 - r0;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    TV* f = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < nr * nrhs; idx += nt) {
-        int q = idx / nr, r = r0 + (idx - q * nr);
-        f[r + (int64_t)q * m] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
-    }
-    __syncthreads();
-    const int nch = F.child_end - F.child_beg;
-    const int b0 = r0 / kAssembleCols, b1 = (r1 + kAssembleCols - 1) / kAssembleCols;
-    const int* rng = asm_range + asm_off[s];
-    for (int h = 0; h < nch; ++h) {
-        const int lo = rng[(b0 * nch + h) * 2], hi = rng[((b1 - 1) * nch + h) * 2 + 1];
-        if (lo >= hi) continue;
-        const int cs = child[F.child_beg + h];
-        const FrontDesc g = fronts[cs];
-        const TV* w = front_vec(fv, fv_off, cs, nrhs);
-        const int* rm = relmap + g.rows_off + g.c;
-        const int cnt = hi - lo;
-        for (int idx = tid; idx < cnt * nrhs; idx += nt) {
-            int q = idx / cnt, rr = lo + (idx - q * cnt);
-            f[rm[rr] + (int64_t)q * m] += w[g.c + rr + (int64_t)q * g.m];
-        }
-        __syncthreads();
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -257,7 +215,7 @@ __device__ void fwd_small_front(int s, const FrontDesc* __restrict__ fronts,
         const int* rm = relmap + g.rows_off + g.c;
         for (int idx = tid; idx < uc * nrhs; idx += nt) {
             int q = idx / uc, r = idx - q * uc;
-            f[rm[r] + q * m] += w[g.c + r + q * g.m];
+            f[rm[r] + q * m] += w[(g.c + r) * nrhs + q];
         }
         __syncthreads();
     }
@@ -290,7 +248,7 @@ __device__ void fwd_small_front(int s, const FrontDesc* __restrict__ fronts,
         if (r < c)
             xp[F.first_col + r + (int64_t)q * n] = f[idx];
         else
-            out[idx] = f[idx];
+            out[r * nrhs + q] = f[idx];
     }
 }
 
@@ -392,37 +350,31 @@ __host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
            ((size_t)kTile * nrhs + 4 * kTile) * sizeof(TV);
 }
 
-// Forward, task (s, i): row tile i of front s accumulates
-// acc = sum_{k < min(i, nt1)} L(i, k) y_k over the pivot tiles, waiting for
-// each y_k; a pivot tile (i < nt1) then solves y_i = inv(L_ii) (f_i - acc)
-// into the solution and publishes it (flag 1), an update tile leaves
-// f_i - acc in the front vector for the parent.  Threads: r = row in the
-// tile, g = quarter; one right-hand side splits the 64 columns of a block
-// over the quarters, several split the right-hand sides (NQ per thread).
+// Forward, task (s, i): row tile i of front s gathers its rows of the front
+// vector (right-hand side on the pivot rows plus the children's update rows,
+// child by child) and accumulates acc = sum_{k < min(i, nt1)} L(i, k) y_k
+// over the pivot tiles, waiting for each y_k; a pivot tile (i < nt1) then
+// solves y_i = inv(L_ii) (f_i - acc) into the solution and publishes it, an
+// update tile leaves f_i - acc in the front vector for the parent.
+// Threads: r = row in the tile, g = quarter; one right-hand side splits the
+// 64 columns of a block over the quarters, several split the right-hand
+// sides (NQ per thread).
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
-    k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
-                int ntasks, int* __restrict__ counter, double* __restrict__ pub,
-                int* __restrict__ abort_flag, int* __restrict__ err,
-                const int64_t* __restrict__ fv_off,
-                const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
-                const TL* __restrict__ Dinv, TV* __restrict__ xp, TV* __restrict__ fv, int n,
-                int nrhs) {
+__device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
+                              double* __restrict__ pub, int* __restrict__ abort_flag,
+                              int* __restrict__ err, const int64_t* __restrict__ fv_off,
+                              const int* __restrict__ amap_off, const int* __restrict__ amap_row,
+                              const int* __restrict__ amap_ent,
+                              const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
+                              const TL* __restrict__ Dinv, TV* __restrict__ xp,
+                              TV* __restrict__ fv, int n, int nrhs) {
     constexpr int T = kTile, LD = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL* Lb = reinterpret_cast<TL*>(smem_raw);  // 2 x T x LD
     TL* Dk = Lb + 2 * T * LD;                  // T x LD
     TV* Y = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = Y + T * nrhs;  // 4 x T
-    __shared__ int s_task;
     const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
-    if (tid == 0) s_task = atomicAdd(counter, 1);
-    __syncthreads();
-    if (s_task >= ntasks) {  // counter not cleared: refuse rather than read past the list
-        if (tid == 0) atomicOr(err, 2);
-        return;
-    }
-    const int2 tk = tasks[s_task];
     const int s = tk.x, i = tk.y;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T);
@@ -438,16 +390,28 @@ __global__ void __launch_bounds__(256)
     TV acc[NQ];
 #pragma unroll
     for (int j = 0; j < NQ; ++j) acc[j] = TV(0);
-    // this tile's rows of the front vector (assembled by an earlier launch):
-    // loaded now, off the chain's critical path
+    // this tile's rows of the front vector, gathered now (children are
+    // final: lower levels), off the chain's critical path
     TV* f = front_vec(fv, fv_off, s, nrhs);
     TV fpre[NQ];
+    {
+        const int R = ti.start + r;
+        int e0 = 0, e1 = 0;
+        if (r < ti.size) {
+            const int* ar = amap_row + amap_off[s] + R;
+            e0 = ar[0];
+            e1 = ar[1];
+        }
 #pragma unroll
-    for (int j = 0; j < NQ; ++j) {
-        const int q = lsplit ? 0 : g + 4 * j;
-        fpre[j] = (r < ti.size && q < nrhs && (!lsplit || (g == 0 && j == 0)))
-                      ? f[ti.start + r + (int64_t)q * F.m]
-                      : TV(0);
+        for (int j = 0; j < NQ; ++j) {
+            const int q = lsplit ? 0 : g + 4 * j;
+            TV v = TV(0);
+            if (r < ti.size && q < nrhs && (!lsplit || (g == 0 && j == 0))) {
+                if (R < F.c) v = xp[F.first_col + R + (int64_t)q * n];
+                for (int e = e0; e < e1; ++e) v += fv[(int64_t)amap_ent[e] * nrhs + q];
+            }
+            fpre[j] = v;
+        }
     }
     bool ok = true;
     for (int k = 0; k < kend; ++k) {
@@ -495,7 +459,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
                 for (int j = 0; j < NQ; ++j) {
                     const int q = g + 4 * j;
-                    if (q < nrhs) f[ti.start + r + (int64_t)q * F.m] = fpre[j] - acc[j];
+                    if (q < nrhs) f[(int64_t)(ti.start + r) * nrhs + q] = fpre[j] - acc[j];
                 }
             }
         }
@@ -557,7 +521,8 @@ __global__ void __launch_bounds__(256)
 template <typename TL, typename TV, int NQ>
 __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                 const int* __restrict__ rows, const int* __restrict__ gather_nch,
-                                const int* __restrict__ gather_off, const TL* __restrict__ Ls,
+                                const int* __restrict__ gather_off, int* __restrict__ gcount,
+                                const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
                                 const TV* __restrict__ xp, TV* __restrict__ part, int n,
                                 int nrhs) {
     constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
@@ -626,6 +591,13 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
             if (q < nrhs) out[l + T * q] = acc[a];
         }
     }
+    // count this chunk in for the pivot task (s, j): the CTA's stores, then
+    // a device-scope fence, then the increment
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        atomicAdd(gcount + dinv_off[s] / (T * T) + j, 1);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -670,12 +642,12 @@ __device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict_
             const int ch = child[h];
             const FrontDesc g = fronts[ch];
             const int uc = g.m - g.c;
-            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c + (int64_t)q0 * g.m;
+            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c * nrhs + q0;
             if (r < uc) {  // uc < m <= W
                 const int p = relmap[g.rows_off + g.c + r];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    if (q < nq) wbuf[q * 32 + p] += w[r + (int64_t)q * g.m];
+                    if (q < nq) wbuf[q * 32 + p] += w[r * nrhs + q];
             }
             __syncwarp(mask);
         }
@@ -709,7 +681,7 @@ __device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict_
             if (r < c)
                 xp[F.first_col + r + (int64_t)(q0 + q) * n] = v[q];
             else
-                out[r + (int64_t)(q0 + q) * m] = v[q];
+                out[r * nrhs + q0 + q] = v[q];
         }
     }
 }
@@ -783,13 +755,13 @@ __device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restr
             const int ch = child[h];
             const FrontDesc g = fronts[ch];
             const int uc = g.m - g.c;
-            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c + (int64_t)q0 * g.m;
+            const TV* w = front_vec(fv, fv_off, ch, nrhs) + g.c * nrhs + q0;
             const int* rm = relmap + g.rows_off + g.c;
             for (int rr = lane; rr < uc; rr += 32) {
                 const int p = rm[rr];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    if (q < nq) f[q * MR + p] += w[rr + (int64_t)q * g.m];
+                    if (q < nq) f[q * MR + p] += w[rr * nrhs + q];
             }
             __syncwarp();
         }
@@ -814,7 +786,7 @@ __device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restr
         for (int r = c + lane; r < m; r += 32)
 #pragma unroll
             for (int q = 0; q < NQ; ++q)
-                if (q < nq) out[r + (int64_t)(q0 + q) * m] = f[q * MR + r];
+                if (q < nq) out[r * nrhs + q0 + q] = f[q * MR + r];
         __syncwarp();
     }
 }
@@ -969,120 +941,35 @@ __device__ void bwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __res
         bwd_group_front<TL, TV, 8, NQ>(fronts[wt.list[wt.n1 + wt.n2 + k]], rows, Ls, xp, n, nrhs);
 }
 
-// One launch per level before the large-front chain (128 threads, 256 when
-// it holds gather tasks), forward: the small fronts and the large fronts'
-// vector assembly (CTA each) -- both depend only on lower levels.  Backward:
-// the update-row partial sums of the large fronts and the small fronts --
-// both depend only on ancestors.  With at most kWarpSolveRhs right-hand sides
-// the small fronts are warp tasks on the first wblocks blocks (wt.count() > 0),
-// else a CTA each (small_list, nsmall of them; wt empty).
-template <typename TL, typename TV>
-__global__ void __launch_bounds__(256, 4)
-    k_fwd_prep(const FrontDesc* __restrict__ fronts, WarpTasks wt, int wblocks,
-               const int* __restrict__ small_list, int nsmall, const int2* __restrict__ asm_tasks,
-               const int* __restrict__ child, const int* __restrict__ relmap,
-               const int* __restrict__ asm_off, const int* __restrict__ asm_range,
-               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
-               TV* __restrict__ fv, int n, int nrhs, int msmall) {
-    int b = blockIdx.x;
-    if (b < wblocks) {
-        extern __shared__ __align__(16) unsigned char smem_raw[];
-        const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
-        TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
-        const int ntask = wt.count();
-        for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
-            if (nrhs == 1)
-                fwd_warp_task<TL, TV, 1>(wt, t, fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
-                                         wbuf, warp_rows(msmall));
-            else
-                fwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, child, relmap, fv_off, Ls, xp,
-                                                     fv, n, nrhs, wbuf, warp_rows(msmall));
-            __syncwarp();
-        }
-        return;
-    }
-    b -= wblocks;
-    if (b < nsmall) {
-        fwd_small_front<TL, TV>(small_list[b], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
-                                msmall);
-    } else {
-        const int2 t = asm_tasks[b - nsmall];
-        fwd_assemble_chunk<TV>(t.x, t.y, fronts, child, relmap, asm_off, asm_range, fv_off, xp, fv,
-                               n, nrhs);
-    }
-}
-
-template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256, 4)
-    k_bwd_prep(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
-               WarpTasks wt, int wblocks, const int* __restrict__ small_list, int nsmall,
-               const int* __restrict__ rows, const int* __restrict__ gather_nch,
-               const int* __restrict__ gather_off, const TL* __restrict__ Ls, TV* __restrict__ xp,
-               TV* __restrict__ part, int n, int nrhs, int umax, int msmall) {
-    const int b = blockIdx.x;
-    if (b < ngather) {
-        bwd_gather_task<TL, TV, NQ>(gtasks[b], fronts, rows, gather_nch, gather_off, Ls, xp, part,
-                                    n, nrhs);
-        return;
-    }
-    const int bb = b - ngather;
-    if (bb < wblocks) {
-        extern __shared__ __align__(16) unsigned char smem_raw[];
-        const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
-        TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
-        const int ntask = wt.count();
-        for (int t = bb * wpb + w; t < ntask; t += wblocks * wpb) {
-            if (nrhs == 1)
-                bwd_warp_task<TL, TV, 1>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
-                                         warp_rows(msmall));
-            else
-                bwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
-                                                     warp_rows(msmall));
-            __syncwarp();
-        }
-        return;
-    }
-    if (bb - wblocks < nsmall)
-        bwd_small_front<TL, TV>(small_list[bb - wblocks], fronts, rows, Ls, xp, n, nrhs, umax,
-                                msmall);
-}
-
 // Backward, task (s, j): pivot column tile j of front s accumulates
 // acc = sum_{k > j} L(k, j)' x_k over the pivot tiles nt1-1 .. j+1 of this
-// front as they publish (flag 2), adds the update-row partial sums of
-// k_bwd_gather in chunk order, and solves x_j = inv(L_jj)' (y_j - acc).
-// Threads: l = column in the tile.
+// front as they publish, then (once the update-row gathers of (s, j) have
+// all counted in) their partial sums in chunk order, and solves
+// x_j = inv(L_jj)' (y_j - acc).  Threads: l = column in the tile.
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
-    k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks,
-                int ntasks, int* __restrict__ counter, double* __restrict__ pub,
-                int* __restrict__ abort_flag, int* __restrict__ err,
-                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
-                const TV* __restrict__ part, const int64_t* __restrict__ dinv_off,
-                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp, int n,
-                int nrhs) {
+__device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
+                               double* __restrict__ pub, int* __restrict__ abort_flag,
+                               int* __restrict__ err, const int* __restrict__ gather_nch,
+                               const int* __restrict__ gather_off, const int* __restrict__ gcount,
+                               const TV* __restrict__ part, const int64_t* __restrict__ dinv_off,
+                               const TL* __restrict__ Ls, const TL* __restrict__ Dinv,
+                               TV* __restrict__ xp, int n, int nrhs) {
     constexpr int T = kTile, LD = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL* Lb = reinterpret_cast<TL*>(smem_raw);
     TL* Dk = Lb + 2 * T * LD;
     TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
     TV* red = X + T * nrhs;
-    __shared__ int s_task;
+    __shared__ int s_ok;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
-    if (tid == 0) s_task = atomicAdd(counter, 1);
-    __syncthreads();
-    if (s_task >= ntasks) {  // counter not cleared: refuse rather than read past the list
-        if (tid == 0) atomicOr(err, 2);
-        return;
-    }
-    const int2 tk = tasks[s_task];
     const int s = tk.x, j = tk.y;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T);
     const TileRange tj = tile_range(j, F.m, F.c, T);
     const bool lsplit = nrhs == 1;
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;  // column tile j
-    double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
+    const int64_t tile0 = dinv_off[s] / (T * T);               // this front's first pivot tile
+    double* pb = pub + tile0 * T * nrhs;
     const int nblk = nt1 - 1 - j;  // pivot row tiles k = nt1-1 down to j+1
     load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
     if (nblk > 0) {
@@ -1093,31 +980,15 @@ __global__ void __launch_bounds__(256)
     TV acc[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
-    // off the chain's critical path, before the first wait: the update-row
-    // partial sums (earlier launch, in chunk order) and this tile's y_j
+    // this tile's y_j, before the first wait
     const int64_t xj = F.first_col + tj.start;
     TV ypre[NQ];
-    {
-        const int nch = gather_nch[s];
-        const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
-        for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
-            if (lsplit) {
-                if (g == 0) acc[0] += pj[l];
-            } else {
 #pragma unroll
-                for (int a = 0; a < NQ; ++a) {
-                    const int q = g + 4 * a;
-                    if (q < nrhs) acc[a] += pj[l + T * q];
-                }
-            }
-        }
-#pragma unroll
-        for (int a = 0; a < NQ; ++a) {
-            const int q = lsplit ? 0 : g + 4 * a;
-            ypre[a] = (l < tj.size && q < nrhs && (!lsplit || (g == 0 && a == 0)))
-                          ? xp[xj + l + (int64_t)q * n]
-                          : TV(0);
-        }
+    for (int a = 0; a < NQ; ++a) {
+        const int q = lsplit ? 0 : g + 4 * a;
+        ypre[a] = (l < tj.size && q < nrhs && (!lsplit || (g == 0 && a == 0)))
+                      ? xp[xj + l + (int64_t)q * n]
+                      : TV(0);
     }
     bool ok = true;
     for (int b = 0; b < nblk; ++b) {
@@ -1153,6 +1024,27 @@ __global__ void __launch_bounds__(256)
     }
     cp_async_wait_groups<0>();
     if (!ok) return;
+    // the update-row partial sums of (s, j), in chunk order, once all counted in
+    {
+        const int nch = gather_nch[s];
+        if (nch > 0) {
+            if (tid == 0) s_ok = wait_flag(gcount + tile0 + j, nch, abort_flag, err) ? 1 : 0;
+            __syncthreads();
+            if (!s_ok) return;
+            const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
+            for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
+                if (lsplit) {
+                    if (g == 0) acc[0] += ld_shared_value(pj + l);
+                } else {
+#pragma unroll
+                    for (int a = 0; a < NQ; ++a) {
+                        const int q = g + 4 * a;
+                        if (q < nrhs) acc[a] += ld_shared_value(pj + l + T * q);
+                    }
+                }
+            }
+        }
+    }
     if (lsplit) {
         red[g * T + l] = acc[0];
         __syncthreads();
@@ -1207,6 +1099,122 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+
+// One launch per level and direction.  Blocks [0, ntile) take tickets for
+// the dependency-ordered tile tasks of the large fronts; the blocks after
+// them run the small fronts: warp tasks (at most kWarpSolveRhs right-hand
+// sides; wblocks blocks looping over wt) or a CTA each (small_list, nsm of
+// them).  Small fronts depend only on lower levels (forward) or ancestors
+// (backward), never on this launch's tile tasks.  Backward tickets first
+// hand out the ngather update-row gathers (no waits), then the pivot tasks.
+
+template <typename TL, typename TV, int NQ>
+__device__ void small_fronts_fwd(int b, WarpTasks wt, int wblocks, const int* small_list,
+                                 const FrontDesc* __restrict__ fronts, const int* __restrict__ child,
+                                 const int* __restrict__ relmap, const int64_t* __restrict__ fv_off,
+                                 const TL* __restrict__ Ls, TV* __restrict__ xp,
+                                 TV* __restrict__ fv, int n, int nrhs, int msmall) {
+    if (b < wblocks) {
+        if constexpr (NQ == 1) {  // nrhs <= kWarpSolveRhs
+            extern __shared__ __align__(16) unsigned char smem_raw[];
+            const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
+            TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
+            const int ntask = wt.count();
+            for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
+                if (nrhs == 1)
+                    fwd_warp_task<TL, TV, 1>(wt, t, fronts, child, relmap, fv_off, Ls, xp, fv, n,
+                                             nrhs, wbuf, warp_rows(msmall));
+                else
+                    fwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, child, relmap, fv_off, Ls,
+                                                         xp, fv, n, nrhs, wbuf, warp_rows(msmall));
+                __syncwarp();
+            }
+        }
+        return;
+    }
+    fwd_small_front<TL, TV>(small_list[b - wblocks], fronts, child, relmap, fv_off, Ls, xp, fv, n,
+                            nrhs, msmall);
+}
+
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256)
+    k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks, int ntile,
+                int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
+                int* __restrict__ err, const int64_t* __restrict__ fv_off,
+                const int* __restrict__ amap_off, const int* __restrict__ amap_row,
+                const int* __restrict__ amap_ent, const int64_t* __restrict__ dinv_off,
+                WarpTasks wt, int wblocks, const int* __restrict__ small_list,
+                const int* __restrict__ child, const int* __restrict__ relmap,
+                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
+                TV* __restrict__ fv, int n, int nrhs, int msmall) {
+    if ((int)blockIdx.x >= ntile) {
+        small_fronts_fwd<TL, TV, NQ>(blockIdx.x - ntile, wt, wblocks, small_list, fronts, child,
+                                     relmap, fv_off, Ls, xp, fv, n, nrhs, msmall);
+        return;
+    }
+    __shared__ int s_task;
+    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
+    __syncthreads();
+    if (s_task >= ntile) {  // counter not cleared: refuse rather than read past the list
+        if (threadIdx.x == 0) atomicOr(err, 2);
+        return;
+    }
+    fwd_tile_task<TL, TV, NQ>(tasks[s_task], fronts, pub, abort_flag, err, fv_off, amap_off,
+                              amap_row, amap_ent, dinv_off, Ls, Dinv, xp, fv, n, nrhs);
+}
+
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256)
+    k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
+                const int2* __restrict__ tasks, int ntile, int* __restrict__ counter,
+                double* __restrict__ pub, int* __restrict__ abort_flag, int* __restrict__ err,
+                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
+                int* __restrict__ gcount, TV* __restrict__ part,
+                const int64_t* __restrict__ dinv_off, WarpTasks wt, int wblocks,
+                const int* __restrict__ small_list, const int* __restrict__ rows,
+                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp, int n,
+                int nrhs, int msmall) {
+    const int ntk = ngather + ntile;
+    if ((int)blockIdx.x >= ntk) {
+        const int b = blockIdx.x - ntk;
+        if (b < wblocks) {
+            if constexpr (NQ == 1) {  // nrhs <= kWarpSolveRhs
+                extern __shared__ __align__(16) unsigned char smem_raw[];
+                const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
+                TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
+                const int ntask = wt.count();
+                for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
+                    if (nrhs == 1)
+                        bwd_warp_task<TL, TV, 1>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
+                                                 warp_rows(msmall));
+                    else
+                        bwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, rows, Ls, xp, n, nrhs,
+                                                             wbuf, warp_rows(msmall));
+                    __syncwarp();
+                }
+            }
+            return;
+        }
+        bwd_small_front<TL, TV>(small_list[b - wblocks], fronts, rows, Ls, xp, n, nrhs, msmall,
+                                msmall);
+        return;
+    }
+    __shared__ int s_task;
+    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
+    __syncthreads();
+    if (s_task >= ntk) {  // counter not cleared: refuse rather than read past the list
+        if (threadIdx.x == 0) atomicOr(err, 2);
+        return;
+    }
+    if (s_task < ngather) {
+        bwd_gather_task<TL, TV, NQ>(gtasks[s_task], fronts, rows, gather_nch, gather_off, gcount,
+                                    dinv_off, Ls, xp, part, n, nrhs);
+        return;
+    }
+    bwd_chain_task<TL, TV, NQ>(tasks[s_task - ngather], fronts, pub, abort_flag, err, gather_nch,
+                               gather_off, gcount, part, dinv_off, Ls, Dinv, xp, n, nrhs);
+}
+
 // ---------------------------------------------------------------------------
 // permutations
 // ---------------------------------------------------------------------------
@@ -1249,21 +1257,27 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 // launch sequence
 // ---------------------------------------------------------------------------
 
+// the largest dynamic shared memory any launch of the level kernels asks for
+template <typename TL, typename TV>
+static int solve_smem_max() {
+    const int ms = Plan::kSmallMaxRows;
+    size_t m = level_smem_bytes<TL, TV>(64);
+    m = std::max(m, small_fwd_smem<TL, TV>(ms, 64));
+    m = std::max(m, small_bwd_smem<TL, TV>(ms, ms, 64));
+    m = std::max(m, gather_smem_bytes<TL, TV>(64));
+    m = std::max(m, 8 * (size_t)warp_buf_stride(ms, kWarpSolveRhs) * sizeof(TV));
+    return (int)m;
+}
+
 template <typename TL, typename TV, int NQ>
 static void set_solve_attributes_nq() {
-    const int ms = Plan::small_limit[kSmallBuckets - 1];
-    const int lv = (int)level_smem_bytes<TL, TV>(64);
-    const int bp = std::max(lv, (int)small_bwd_smem<TL, TV>(ms, ms, 64));
-    cudaFuncSetAttribute(k_fwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, lv);
-    cudaFuncSetAttribute(k_bwd_prep<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, bp);
+    const int sm = solve_smem_max<TL, TV>();
+    cudaFuncSetAttribute(k_fwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_bwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
 template <typename TL, typename TV>
 static void set_solve_attributes() {
-    const int ms = Plan::small_limit[kSmallBuckets - 1];
-    cudaFuncSetAttribute(k_fwd_prep<TL, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)small_fwd_smem<TL, TV>(ms, 64));
     set_solve_attributes_nq<TL, TV, 1>();
     set_solve_attributes_nq<TL, TV, 4>();
     set_solve_attributes_nq<TL, TV, 16>();
@@ -1284,9 +1298,7 @@ static int level_msmall(const DevPlan& D, int l) {
     return ms;
 }
 
-// One level of the solve: forward -- small fronts with the large fronts'
-// assembly, then the large-front chain; backward -- update-row gathers with
-// the small fronts, then the large-front chain.
+// One level of the solve: one launch per direction (see k_fwd_level).
 template <typename TL, typename TV, int NQ>
 static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
                         TV* xp, TV* fv, int nrhs, cudaStream_t st) {
@@ -1294,64 +1306,53 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     const int n = D.n;
     const int sb = D.h_small_ptr[l * kSmallBuckets], se = D.h_small_ptr[(l + 1) * kSmallBuckets];
     const int ns = se - sb;
-    const int lb = D.h_large_ptr[l], nl = D.h_large_ptr[l + 1] - lb;
+    const int nl = D.h_large_ptr[l + 1] - D.h_large_ptr[l];
     const int msmall = level_msmall(D, l);
-    // with at most kWarpSolveRhs right-hand sides every small front takes the
-    // warp path
-    static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 5 rows per lane");
-    const int nwarp = nrhs <= kWarpSolveRhs ? ns : 0;
+    // with at most kWarpSolveRhs right-hand sides (NQ == 1) every small front
+    // is a warp task, else a CTA
+    static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 160 rows in shared memory");
+    const bool warp = NQ == 1 && nrhs <= kWarpSolveRhs;
     WarpTasks wt{S.warp_list + sb, 0, 0, 0};
-    if (nwarp > 0) {
+    if (warp) {
         wt.n1 = S.warp_cnt[3 * l];
         wt.n2 = S.warp_cnt[3 * l + 1];
         wt.n4 = S.warp_cnt[3 * l + 2];
     }
-    const size_t lsm = level_smem_bytes<TL, TV>(nrhs);
+    const int nsm = warp ? 0 : ns;  // small fronts on a CTA each
+    // warp-task blocks: 8 warps each, at most 4 blocks per SM
+    const int wblocks = warp ? std::min((wt.count() + 7) / 8, 148 * 4) : 0;
+    size_t sm = 0;
+    if (warp && wt.count() > 0) sm = 8 * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV);
+    if (nsm > 0)
+        sm = std::max(sm, forward ? small_fwd_smem<TL, TV>(msmall, nrhs)
+                                  : small_bwd_smem<TL, TV>(msmall, msmall, nrhs));
     const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
+    if (nt > 0) sm = std::max(sm, level_smem_bytes<TL, TV>(nrhs));
     int* counter = S.sync + 2 * l + (forward ? 0 : 1);
-    int* flags = S.sync + 2 * D.nlevels;
-    int* abort_flag = flags + S.nflags;
+    int* gcount = S.sync + 2 * D.nlevels;  // one per pivot tile of a large front
+    int* abort_flag = gcount + S.nflags;
     const double bytes =
         (S.small_elems[l] + (forward ? S.fwd_elems[l] : S.bwd_elems[l])) * sizeof(TL);
     ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
     if (forward) {
-        const int ab = S.asm_task_beg[l], na = S.asm_task_beg[l + 1] - ab;
-        const int nsm = ns - nwarp;  // small fronts on a CTA each
-        const int wblocks = std::min((wt.count() + 3) / 4, kWarpTaskBlocks);  // 4 warps a block
-        const size_t sm = nwarp > 0 ? 4 * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV)
-                                    : small_fwd_smem<TL, TV>(msmall, nrhs);
-        if (ns + na > 0)
-            k_fwd_prep<TL, TV><<<wblocks + nsm + na, 128, sm, st>>>(
-                D.fronts, wt, wblocks, D.small_list + sb, nsm, S.asm_tasks + ab, D.child, D.relmap,
-                D.asm_off, D.asm_range, D.fv_off, Ls, xp, fv, n, nrhs, msmall);
-        if (nt > 0)
-            k_fwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
-                                                        fv + D.fv_pub_off * nrhs, abort_flag,
-                                                        S.err, D.fv_off, D.dinv_off, Ls, Dinv, xp,
-                                                        fv, n, nrhs);
+        const int grid = nt + wblocks + nsm;
+        if (grid > 0)
+            k_fwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
+                D.fronts, S.tasks + t0, nt, counter, fv + D.fv_pub_off * nrhs, abort_flag, S.err,
+                D.fv_off, S.amap_off, S.amap_row, S.amap_ent, D.dinv_off, wt, wblocks,
+                D.small_list + sb, D.child, D.relmap, Ls, Dinv, xp, fv, n, nrhs, msmall);
     } else {
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
-        if (ng + ns > 0) {
-            // the gather's thread layout needs 256 threads; small fronts alone run on 128
-            const int threads = ng > 0 ? 256 : 128;
-            const int nsm = ns - nwarp;
-            const int wpb = threads / 32;
-            const int wblocks = std::min((wt.count() + wpb - 1) / wpb, kWarpTaskBlocks);
-            size_t sm = nwarp > 0 ? wpb * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV)
-                                  : small_bwd_smem<TL, TV>(msmall, msmall, nrhs);
-            if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
-            k_bwd_prep<TL, TV, NQ><<<ng + wblocks + nsm, threads, sm, st>>>(
-                D.fronts, S.tasks + gb, ng, wt, wblocks, D.small_list + sb, nsm, D.rows,
-                S.gather_nch, S.gather_off, Ls, xp, part, n, nrhs, msmall, msmall);
-        }
-        if (nt > 0)
-            k_bwd_level<TL, TV, NQ><<<nt, 256, lsm, st>>>(D.fronts, S.tasks + t0, nt, counter,
-                                                        fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs,
-                                                        abort_flag, S.err, S.gather_nch,
-                                                        S.gather_off, part, D.dinv_off, Ls, Dinv,
-                                                        xp, n, nrhs);
+        if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
+        const int grid = ng + nt + wblocks + nsm;
+        if (grid > 0)
+            k_bwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
+                D.fronts, S.tasks + gb, ng, S.tasks + t0, nt, counter,
+                fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs, abort_flag, S.err,
+                S.gather_nch, S.gather_off, gcount, part, D.dinv_off, wt, wblocks,
+                D.small_list + sb, D.rows, Ls, Dinv, xp, n, nrhs, msmall);
     }
 }
 
