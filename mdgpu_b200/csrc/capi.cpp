@@ -236,7 +236,8 @@ void upload_plan(mdgpu_handle_s* h) {
     D.h_large_ptr = P.large_ptr;
     const int64_t acc = h->ssched.fv_rows;
     D.fv_fronts = acc;
-    D.fv_pub_off = acc + h->ssched.gather_vecs * kTile;
+    // publication slots start on 16 bytes (copied with 16-byte cp.async)
+    D.fv_pub_off = (acc + h->ssched.gather_vecs * kTile + 1) & ~(int64_t)1;
     D.fv_total = D.fv_pub_off + 2 * (int64_t)h->ssched.nflags * kTile;
     D.fv_off = h->keep(upload(h->ssched.fv_off));
     D.dinv_off = h->keep(upload(P.dinv_off));

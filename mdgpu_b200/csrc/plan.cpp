@@ -386,9 +386,15 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
                 const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
                 bytes += (double)f.c * (f.c + 1) / 2 + (double)(f.m - f.c) * f.c +
                          (double)nt1 * T * T;
-                if (dir == 0)
-                    for (int i = 0; i < NT; ++i) ks.push_back({i < nt1 ? i : nt1, ord++, s, i});
-                else
+                if (dir == 0) {
+                    // pivot tiles one per task; update tiles in groups of
+                    // kFwdGroupBlocks / nt1 (streamed by one CTA)
+                    for (int i = 0; i < nt1; ++i) ks.push_back({i, ord++, s, i | (1 << 16)});
+                    const int G = std::max(1, std::min(SolveScheduleHost::kFwdGroupBlocks / nt1,
+                                                       SolveScheduleHost::kFwdGroupBlocks));
+                    for (int i = nt1; i < NT; i += G)
+                        ks.push_back({nt1, ord++, s, i | (std::min(G, NT - i) << 16)});
+                } else
                     for (int j = 0; j < nt1; ++j) ks.push_back({nt1 - 1 - j, ord++, s, j});
             }
             (dir == 0 ? S.fwd_elems : S.bwd_elems)[l] = bytes;

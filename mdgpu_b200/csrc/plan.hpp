@@ -139,6 +139,10 @@ struct SolveScheduleHost {
     // one launch per level and direction: tasks (front, tile) as int pairs,
     // ordered so that every task's dependencies come earlier (a task only
     // waits on tasks that took a lower ticket, hence already run)
+    // forward task (s, i | cnt << 16): row tiles i .. i + cnt - 1 of front s
+    // (a pivot tile alone; update tiles grouped to about kFwdGroupBlocks L
+    // blocks per task); backward task (s, j): pivot column tile j
+    static constexpr int kFwdGroupBlocks = 8;
     std::vector<int> tasks;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1 each, in tasks
     std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read

@@ -337,28 +337,96 @@ __device__ void bwd_small_front(int s, const FrontDesc* __restrict__ fronts,
     }
 }
 
-// the update-row gather: two L blocks (double buffer), x rows, partials
-template <typename TL, typename TV>
-__host__ __device__ constexpr size_t gather_smem_bytes(int nrhs) {
-    return ((2 * (size_t)kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
-           ((size_t)kTile * nrhs + 4 * kTile) * sizeof(TV);
+// ---------------------------------------------------------------------------
+// large-front tile tasks: a pipeline of `stg` stages streams the L blocks a
+// task multiplies, each with the vector block it is multiplied by (a pivot
+// tile's published solution, or gathered solution rows), by cp.async; the
+// block in use is consumed while the next ones load.  Published vectors come
+// through L2 (16-byte cp.async.cg); a stage whose copy still holds a
+// sentinel falls back to polling that slot.
+// ---------------------------------------------------------------------------
+
+template <typename TL>
+__host__ __device__ constexpr int level_stages(int nrhs) {
+    return 2;
 }
 
+// shared memory: diagonal inverse block, stg L blocks, stg vector blocks, a
+// vector, the quarter reduction, the gather's row indices
 template <typename TL, typename TV>
 __host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
-    return ((3 * (size_t)kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
-           ((size_t)kTile * nrhs + 4 * kTile) * sizeof(TV);
+    return (((1 + (size_t)level_stages<TL>(nrhs)) * kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
+           (((size_t)level_stages<TL>(nrhs) + 1) * kTile * nrhs + 4 * kTile) * sizeof(TV) +
+           (size_t)SolveScheduleHost::kGatherTiles * kTile * sizeof(int);
 }
 
-// Forward, task (s, i): row tile i of front s gathers its rows of the front
-// vector (right-hand side on the pivot rows plus the children's update rows,
-// child by child) and accumulates acc = sum_{k < min(i, nt1)} L(i, k) y_k
-// over the pivot tiles, waiting for each y_k; a pivot tile (i < nt1) then
-// solves y_i = inv(L_ii) (f_i - acc) into the solution and publishes it, an
-// update tile leaves f_i - acc in the front vector for the parent.
-// Threads: r = row in the tile, g = quarter; one right-hand side splits the
-// 64 columns of a block over the quarters, several split the right-hand
-// sides (NQ per thread).
+template <typename TL, typename TV>
+struct LevelSmem {
+    TL* Dk;   // T x LD
+    TL* Lst;  // stg x T x LD
+    TV* Vst;  // stg x T x nrhs
+    TV* Y;    // T x nrhs
+    TV* red;  // 4 x T
+    int* idx; // kGatherTiles x T
+    int stg;
+    __device__ explicit LevelSmem(int nrhs) {
+        constexpr int T = kTile, LD = kTile + 1;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        stg = level_stages<TL>(nrhs);
+        Dk = reinterpret_cast<TL*>(smem_raw);
+        Lst = Dk + T * LD;
+        Vst = reinterpret_cast<TV*>(smem_raw +
+                                    (((1 + (size_t)stg) * T * LD * sizeof(TL) + 15) / 16) * 16);
+        Y = Vst + (size_t)stg * T * nrhs;
+        red = Y + T * nrhs;
+        idx = reinterpret_cast<int*>(red + 4 * T);
+    }
+    __device__ TL* lb(int p) const { return Lst + (p % stg) * kTile * (kTile + 1); }
+    __device__ TV* vb(int p, int nrhs) const { return Vst + (size_t)(p % stg) * kTile * nrhs; }
+};
+
+__device__ __forceinline__ void cp_async_wait_stages(int stg) {
+    if (stg >= 3)
+        cp_async_wait_groups<2>();
+    else
+        cp_async_wait_groups<1>();
+}
+
+// a published T x nrhs slot into a stage (16-byte copies through L2; T * nrhs
+// is even and slots start on 16 bytes)
+__device__ __forceinline__ void load_slot_async(double* dst, const double* src, int nrhs) {
+    for (int q = threadIdx.x; q < kTile * nrhs / 2; q += blockDim.x) {
+        const uint32_t da = static_cast<uint32_t>(__cvta_generic_to_shared(dst + 2 * q));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(da), "l"(src + 2 * q)
+                     : "memory");
+    }
+}
+
+// After the stage's copy landed: rows >= nk zeroed, rows < nk checked for
+// the sentinel; an unpublished row sends the CTA to poll the slot.  Uniform
+// result; false = the solve was aborted.
+__device__ __forceinline__ bool settle_slot(double* v, const double* src, int nk, int nrhs,
+                                            int* abort_flag, int* err) {
+    bool mine = true;
+    for (int e = threadIdx.x; e < kTile * nrhs; e += blockDim.x) {
+        if ((e & (kTile - 1)) >= nk)
+            v[e] = 0.0;
+        else if (is_unpublished(v[e]))
+            mine = false;
+    }
+    if (__syncthreads_and(mine)) return true;
+    return poll_published(v, src, nk, nrhs, abort_flag, err);
+}
+
+// Forward, task (s, i0 | cnt << 16): row tiles i0 .. i0 + cnt - 1 of front s.
+// Each gathers its rows of the front vector (right-hand side on the pivot
+// rows plus the children's update rows, child by child; one tile ahead) and
+// accumulates acc = sum_{k < min(i, nt1)} L(i, k) y_k over the pivot tiles.
+// A pivot tile (i0 < nt1, cnt = 1) then solves y_i = inv(L_ii) (f_i - acc)
+// into the solution and publishes it; an update tile leaves f_i - acc in the
+// front vector for the parent.  Threads: r = row in the tile, g = quarter;
+// one right-hand side splits the 64 columns of a block over the quarters,
+// several split the right-hand sides (NQ per thread).
 template <typename TL, typename TV, int NQ>
 __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
                               double* __restrict__ pub, int* __restrict__ abort_flag,
@@ -368,68 +436,80 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
                               const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
                               const TL* __restrict__ Dinv, TV* __restrict__ xp,
                               TV* __restrict__ fv, int n, int nrhs) {
+    static_assert(sizeof(TV) == 8, "solve vectors are double");
     constexpr int T = kTile, LD = kTile + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TL* Lb = reinterpret_cast<TL*>(smem_raw);  // 2 x T x LD
-    TL* Dk = Lb + 2 * T * LD;                  // T x LD
-    TV* Y = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
-    TV* red = Y + T * nrhs;  // 4 x T
+    const LevelSmem<TL, TV> sm(nrhs);
     const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
-    const int s = tk.x, i = tk.y;
+    const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T);
-    const TileRange ti = tile_range(i, F.m, F.c, T);
-    const int kend = min(i, nt1);
-    const bool pivot = i < nt1;
+    const bool pivot = i0 < nt1;
+    const int kend = pivot ? i0 : nt1;  // L blocks per tile
+    const int P = cnt * kend;
     const bool lsplit = nrhs == 1;
     const TL* L = Ls + F.loff;
     double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
-    if (pivot) load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)i * T * T, T, ti.size, ti.size);
-    if (kend > 0) load_block_async(Lb, L + ti.start, F.ldl, ti.size, min(T, F.c));
-    cp_async_commit_group();
-    TV acc[NQ];
-#pragma unroll
-    for (int j = 0; j < NQ; ++j) acc[j] = TV(0);
-    // this tile's rows of the front vector, gathered now (children are
-    // final: lower levels), off the chain's critical path
     TV* f = front_vec(fv, fv_off, s, nrhs);
-    TV fpre[NQ];
-    {
+    const int aoff = amap_off[s];
+    // rows of tile i of the front vector into v (this thread's share)
+    auto gather_rows = [&](int i, TV (&v)[NQ]) {
+        const TileRange ti = tile_range(i, F.m, F.c, T);
         const int R = ti.start + r;
         int e0 = 0, e1 = 0;
         if (r < ti.size) {
-            const int* ar = amap_row + amap_off[s] + R;
-            e0 = ar[0];
-            e1 = ar[1];
+            e0 = amap_row[aoff + R];
+            e1 = amap_row[aoff + R + 1];
         }
 #pragma unroll
         for (int j = 0; j < NQ; ++j) {
             const int q = lsplit ? 0 : g + 4 * j;
-            TV v = TV(0);
+            TV x = TV(0);
             if (r < ti.size && q < nrhs && (!lsplit || (g == 0 && j == 0))) {
-                if (R < F.c) v = xp[F.first_col + R + (int64_t)q * n];
-                for (int e = e0; e < e1; ++e) v += fv[(int64_t)amap_ent[e] * nrhs + q];
+                if (R < F.c) x = xp[F.first_col + R + (int64_t)q * n];
+                for (int e = e0; e < e1; ++e) x += fv[(int64_t)amap_ent[e] * nrhs + q];
             }
-            fpre[j] = v;
+            v[j] = x;
         }
-    }
-    bool ok = true;
-    for (int k = 0; k < kend; ++k) {
-        if (k + 1 < kend)
-            load_block_async(Lb + ((k + 1) & 1) * T * LD, L + ti.start + (int64_t)(k + 1) * T * F.ldl,
-                             F.ldl, ti.size, min(T, F.c - (k + 1) * T));
+    };
+    auto issue = [&](int p) {
+        if (p < P) {
+            const int i = i0 + p / kend, k = p % kend;
+            const TileRange ti = tile_range(i, F.m, F.c, T);
+            load_block_async(sm.lb(p), L + ti.start + (int64_t)k * T * F.ldl, F.ldl, ti.size,
+                             min(T, F.c - k * T));
+            load_slot_async(sm.vb(p, nrhs), pb + (int64_t)k * T * nrhs, nrhs);
+        }
         cp_async_commit_group();
-        if (!poll_published(Y, pb + (int64_t)k * T * nrhs, min(T, F.c - k * T), nrhs, abort_flag,
-                            err)) {
+    };
+    if (pivot) {
+        const TileRange ti = tile_range(i0, F.m, F.c, T);
+        load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)i0 * T * T, T, ti.size, ti.size);
+    }
+    for (int p = 0; p < sm.stg - 1; ++p) issue(p);
+    TV fcur[NQ], fnext[NQ], acc[NQ];
+    gather_rows(i0, fcur);
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+        fnext[j] = TV(0);
+        acc[j] = TV(0);
+    }
+    if (cnt > 1) gather_rows(i0 + 1, fnext);
+    bool ok = true;
+    for (int p = 0; p < P; ++p) {
+        issue(p + sm.stg - 1);
+        cp_async_wait_stages(sm.stg);
+        __syncthreads();
+        const int i = i0 + p / kend, k = p % kend;
+        TV* Yk = sm.vb(p, nrhs);
+        if (!settle_slot(Yk, pb + (int64_t)k * T * nrhs, min(T, F.c - k * T), nrhs, abort_flag,
+                         err)) {
             ok = false;
             break;
         }
-        cp_async_wait_groups<1>();
-        __syncthreads();
-        const TL* B = Lb + (k & 1) * T * LD;
+        const TL* B = sm.lb(p);
         if (lsplit) {
 #pragma unroll
-            for (int l = 0; l < 16; ++l) acc[0] += (TV)B[r + (16 * g + l) * LD] * Y[16 * g + l];
+            for (int l = 0; l < 16; ++l) acc[0] += (TV)B[r + (16 * g + l) * LD] * Yk[16 * g + l];
         } else {
 #pragma unroll 4
             for (int l = 0; l < T; ++l) {
@@ -437,42 +517,53 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
 #pragma unroll
                 for (int j = 0; j < NQ; ++j) {
                     const int q = g + 4 * j;
-                    if (q < nrhs) acc[j] += lv * Y[l + T * q];
+                    if (q < nrhs) acc[j] += lv * Yk[l + T * q];
                 }
             }
+        }
+        if (!pivot && k == kend - 1) {  // update tile i complete: f_i - acc to the front vector
+            const TileRange ti = tile_range(i, F.m, F.c, T);
+            if (lsplit) {
+                sm.red[g * T + r] = acc[0];
+                __syncthreads();
+                if (g == 0 && r < ti.size)
+                    f[ti.start + r] =
+                        fcur[0] - (sm.red[r] + sm.red[T + r] + sm.red[2 * T + r] + sm.red[3 * T + r]);
+            } else if (r < ti.size) {
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    const int q = g + 4 * j;
+                    if (q < nrhs) f[(int64_t)(ti.start + r) * nrhs + q] = fcur[j] - acc[j];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NQ; ++j) {
+                acc[j] = TV(0);
+                fcur[j] = fnext[j];
+            }
+            if (i + 2 < i0 + cnt) gather_rows(i + 2, fnext);
         }
         __syncthreads();
     }
     cp_async_wait_groups<0>();
-    if (!ok) return;
+    if (!ok || !pivot) return;
+    __syncthreads();
+    // pivot tile: F = f_i - acc (zero beyond the tile), then y = Dk F
+    const TileRange ti = tile_range(i0, F.m, F.c, T);
+    TV* Y = sm.Y;
+    TV* red = sm.red;
+    const TL* Dk = sm.Dk;
     if (lsplit) {
         red[g * T + r] = acc[0];
         __syncthreads();
-        acc[0] = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
-        __syncthreads();
-    }
-    if (!pivot) {
-        if (r < ti.size) {
-            if (lsplit) {
-                if (g == 0) f[ti.start + r] = fpre[0] - acc[0];
-            } else {
-#pragma unroll
-                for (int j = 0; j < NQ; ++j) {
-                    const int q = g + 4 * j;
-                    if (q < nrhs) f[(int64_t)(ti.start + r) * nrhs + q] = fpre[j] - acc[j];
-                }
-            }
-        }
-        return;
-    }
-    // F = f_i - acc (zero beyond the tile), then y = Dk F
-    if (lsplit) {
-        if (g == 0) Y[r] = r < ti.size ? fpre[0] - acc[0] : TV(0);
+        if (g == 0)
+            Y[r] = r < ti.size ? fcur[0] - (red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r])
+                               : TV(0);
     } else {
 #pragma unroll
         for (int j = 0; j < NQ; ++j) {
             const int q = g + 4 * j;
-            if (q < nrhs) Y[r + T * q] = r < ti.size ? fpre[j] - acc[j] : TV(0);
+            if (q < nrhs) Y[r + T * q] = r < ti.size ? fcur[j] - acc[j] : TV(0);
         }
     }
     __syncthreads();
@@ -485,7 +576,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         if (g == 0 && r < ti.size) {
             const TV v = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
             xp[F.first_col + ti.start + r] = v;
-            st_relaxed_f64(pb + (int64_t)i * T + r, v);
+            st_relaxed_f64(pb + (int64_t)i0 * T + r, v);
         }
     } else {
         TV y[NQ];
@@ -506,7 +597,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
                 const int q = g + 4 * j;
                 if (q < nrhs) {
                     xp[F.first_col + ti.start + r + (int64_t)q * n] = y[j];
-                    st_relaxed_f64(pb + ((int64_t)i * nrhs + q) * T + r, y[j]);
+                    st_relaxed_f64(pb + ((int64_t)i0 * nrhs + q) * T + r, y[j]);
                 }
             }
         }
@@ -516,8 +607,8 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
 // Backward, update rows, task (s, j | h << 16): the partial sum
 // L(k, j)' x_k over the update row tiles k of chunk h (kGatherTiles tiles;
 // x final: ancestors, read through the row list) for pivot column tile j,
-// written as a T x nrhs vector for the pivot task to add in chunk order.
-// Threads: l = column in the tile, g = quarter (as in k_bwd_level).
+// written as a T x nrhs vector for the pivot task to add in chunk order, then
+// counted in.  Threads: l = column in the tile, g = quarter.
 template <typename TL, typename TV, int NQ>
 __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                 const int* __restrict__ rows, const int* __restrict__ gather_nch,
@@ -526,10 +617,7 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                 const TV* __restrict__ xp, TV* __restrict__ part, int n,
                                 int nrhs) {
     constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TL* Lb = reinterpret_cast<TL*>(smem_raw);
-    TV* X = reinterpret_cast<TV*>(smem_raw + ((2 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
-    TV* red = X + T * nrhs;
+    const LevelSmem<TL, TV> sm(nrhs);
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
     const int s = tk.x, j = tk.y & 0xffff, h = tk.y >> 16;
     const FrontDesc F = fronts[s];
@@ -538,30 +626,39 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     const bool lsplit = nrhs == 1;
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;
     const int* rw = rows + F.rows_off;
-    const int k0 = nt1 + h * GC, k1 = min(NT, k0 + GC);
-    {
-        const TileRange t0 = tile_range(k0, F.m, F.c, T);
-        load_block_async(Lb, Lc + t0.start, F.ldl, t0.size, tj.size);
+    const int k0 = nt1 + h * GC, P = min(NT, k0 + GC) - k0;
+    // the chunk's solution rows (ancestors), then the pipeline
+    for (int e = tid; e < P * T; e += blockDim.x) {
+        const TileRange tkr = tile_range(k0 + e / T, F.m, F.c, T);
+        const int rr = e & (T - 1);
+        sm.idx[e] = rr < tkr.size ? rw[tkr.start + rr] : -1;
     }
-    cp_async_commit_group();
+    __syncthreads();
+    auto issue = [&](int p) {
+        if (p < P) {
+            const TileRange tkr = tile_range(k0 + p, F.m, F.c, T);
+            load_block_async(sm.lb(p), Lc + tkr.start, F.ldl, tkr.size, tj.size);
+            TV* v = sm.vb(p, nrhs);
+            for (int e = tid; e < T * nrhs; e += blockDim.x) {
+                const int row = sm.idx[p * T + (e & (T - 1))], q = e / T;
+                if (row >= 0)
+                    cp_async_elem(v + e, xp + row + (int64_t)q * n);
+                else
+                    v[e] = TV(0);
+            }
+        }
+        cp_async_commit_group();
+    };
+    for (int p = 0; p < sm.stg - 1; ++p) issue(p);
     TV acc[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
-    for (int k = k0; k < k1; ++k) {
-        const int b = k - k0;
-        if (k + 1 < k1) {
-            const TileRange tn = tile_range(k + 1, F.m, F.c, T);
-            load_block_async(Lb + ((b + 1) & 1) * T * LD, Lc + tn.start, F.ldl, tn.size, tj.size);
-        }
-        cp_async_commit_group();
-        const TileRange tkr = tile_range(k, F.m, F.c, T);
-        for (int e = tid; e < T * nrhs; e += blockDim.x) {
-            const int rr = e & (T - 1), q = e / T;
-            X[e] = rr < tkr.size ? xp[rw[tkr.start + rr] + (int64_t)q * n] : TV(0);
-        }
-        cp_async_wait_groups<1>();
+    for (int p = 0; p < P; ++p) {
+        issue(p + sm.stg - 1);
+        cp_async_wait_stages(sm.stg);
         __syncthreads();
-        const TL* Bk = Lb + (b & 1) * T * LD;
+        const TL* Bk = sm.lb(p);
+        const TV* X = sm.vb(p, nrhs);
         if (lsplit) {
 #pragma unroll
             for (int r = 0; r < 16; ++r) acc[0] += (TV)Bk[(16 * g + r) + l * LD] * X[16 * g + r];
@@ -581,9 +678,9 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     cp_async_wait_groups<0>();
     TV* out = part + ((int64_t)gather_off[s] + (int64_t)j * gather_nch[s] + h) * T * nrhs;
     if (lsplit) {
-        red[g * T + l] = acc[0];
+        sm.red[g * T + l] = acc[0];
         __syncthreads();
-        if (g == 0) out[l] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
+        if (g == 0) out[l] = sm.red[l] + sm.red[T + l] + sm.red[2 * T + l] + sm.red[3 * T + l];
     } else {
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
@@ -941,10 +1038,10 @@ __device__ void bwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __res
         bwd_group_front<TL, TV, 8, NQ>(fronts[wt.list[wt.n1 + wt.n2 + k]], rows, Ls, xp, n, nrhs);
 }
 
-// Backward, task (s, j): pivot column tile j of front s accumulates
-// acc = sum_{k > j} L(k, j)' x_k over the pivot tiles nt1-1 .. j+1 of this
-// front as they publish, then (once the update-row gathers of (s, j) have
-// all counted in) their partial sums in chunk order, and solves
+// Backward, task (s, j): pivot column tile j of front s accumulates, once
+// the update-row gathers of (s, j) have all counted in, their partial sums
+// in chunk order, then acc += sum_{k > j} L(k, j)' x_k over the pivot tiles
+// nt1-1 .. j+1 of this front as they publish, and solves
 // x_j = inv(L_jj)' (y_j - acc).  Threads: l = column in the tile.
 template <typename TL, typename TV, int NQ>
 __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
@@ -954,12 +1051,9 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                const TV* __restrict__ part, const int64_t* __restrict__ dinv_off,
                                const TL* __restrict__ Ls, const TL* __restrict__ Dinv,
                                TV* __restrict__ xp, int n, int nrhs) {
+    static_assert(sizeof(TV) == 8, "solve vectors are double");
     constexpr int T = kTile, LD = kTile + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TL* Lb = reinterpret_cast<TL*>(smem_raw);
-    TL* Dk = Lb + 2 * T * LD;
-    TV* X = reinterpret_cast<TV*>(smem_raw + ((3 * (size_t)T * LD * sizeof(TL) + 15) / 16) * 16);
-    TV* red = X + T * nrhs;
+    const LevelSmem<TL, TV> sm(nrhs);
     __shared__ int s_ok;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
     const int s = tk.x, j = tk.y;
@@ -970,13 +1064,17 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;  // column tile j
     const int64_t tile0 = dinv_off[s] / (T * T);               // this front's first pivot tile
     double* pb = pub + tile0 * T * nrhs;
-    const int nblk = nt1 - 1 - j;  // pivot row tiles k = nt1-1 down to j+1
-    load_block_async(Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
-    if (nblk > 0) {
-        const TileRange t0 = tile_range(nt1 - 1, F.m, F.c, T);
-        load_block_async(Lb, Lc + t0.start, F.ldl, t0.size, tj.size);
-    }
-    cp_async_commit_group();
+    const int P = nt1 - 1 - j;  // pivot row tiles k = nt1-1 down to j+1
+    auto issue = [&](int p) {
+        if (p < P) {
+            const TileRange tkr = tile_range(nt1 - 1 - p, F.m, F.c, T);
+            load_block_async(sm.lb(p), Lc + tkr.start, F.ldl, tkr.size, tj.size);
+            load_slot_async(sm.vb(p, nrhs), pb + (int64_t)(nt1 - 1 - p) * T * nrhs, nrhs);
+        }
+        cp_async_commit_group();
+    };
+    load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
+    for (int p = 0; p < sm.stg - 1; ++p) issue(p);
     TV acc[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
@@ -990,22 +1088,44 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
                       ? xp[xj + l + (int64_t)q * n]
                       : TV(0);
     }
-    bool ok = true;
-    for (int b = 0; b < nblk; ++b) {
-        const int k = nt1 - 1 - b;
-        if (b + 1 < nblk) {
-            const TileRange tn = tile_range(k - 1, F.m, F.c, T);
-            load_block_async(Lb + ((b + 1) & 1) * T * LD, Lc + tn.start, F.ldl, tn.size, tj.size);
+    // the update-row partial sums of (s, j) (gathers hold lower tickets), in
+    // chunk order, before the chain's first wait
+    {
+        const int nch = gather_nch[s];
+        if (nch > 0) {
+            if (tid == 0) s_ok = wait_flag(gcount + tile0 + j, nch, abort_flag, err) ? 1 : 0;
+            __syncthreads();
+            if (!s_ok) {
+                cp_async_wait_groups<0>();
+                return;
+            }
+            const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
+            for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
+                if (lsplit) {
+                    if (g == 0) acc[0] += __ldcg(pj + l);
+                } else {
+#pragma unroll
+                    for (int a = 0; a < NQ; ++a) {
+                        const int q = g + 4 * a;
+                        if (q < nrhs) acc[a] += __ldcg(pj + l + T * q);
+                    }
+                }
+            }
         }
-        cp_async_commit_group();
-        const TileRange tkr = tile_range(k, F.m, F.c, T);
-        if (!poll_published(X, pb + (int64_t)k * T * nrhs, tkr.size, nrhs, abort_flag, err)) {
+    }
+    bool ok = true;
+    for (int p = 0; p < P; ++p) {
+        issue(p + sm.stg - 1);
+        cp_async_wait_stages(sm.stg);
+        __syncthreads();
+        const int k = nt1 - 1 - p;
+        TV* X = sm.vb(p, nrhs);
+        if (!settle_slot(X, pb + (int64_t)k * T * nrhs, tile_range(k, F.m, F.c, T).size, nrhs,
+                         abort_flag, err)) {
             ok = false;
             break;
         }
-        cp_async_wait_groups<1>();
-        __syncthreads();
-        const TL* B = Lb + (b & 1) * T * LD;
+        const TL* B = sm.lb(p);
         if (lsplit) {
 #pragma unroll
             for (int r = 0; r < 16; ++r) acc[0] += (TV)B[(16 * g + r) + l * LD] * X[16 * g + r];
@@ -1024,27 +1144,10 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
     cp_async_wait_groups<0>();
     if (!ok) return;
-    // the update-row partial sums of (s, j), in chunk order, once all counted in
-    {
-        const int nch = gather_nch[s];
-        if (nch > 0) {
-            if (tid == 0) s_ok = wait_flag(gcount + tile0 + j, nch, abort_flag, err) ? 1 : 0;
-            __syncthreads();
-            if (!s_ok) return;
-            const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
-            for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
-                if (lsplit) {
-                    if (g == 0) acc[0] += ld_shared_value(pj + l);
-                } else {
-#pragma unroll
-                    for (int a = 0; a < NQ; ++a) {
-                        const int q = g + 4 * a;
-                        if (q < nrhs) acc[a] += ld_shared_value(pj + l + T * q);
-                    }
-                }
-            }
-        }
-    }
+    __syncthreads();
+    TV* X = sm.Y;
+    TV* red = sm.red;
+    const TL* Dk = sm.Dk;
     if (lsplit) {
         red[g * T + l] = acc[0];
         __syncthreads();
@@ -1099,7 +1202,6 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
 }
 
-
 // One launch per level and direction.  Blocks [0, ntile) take tickets for
 // the dependency-ordered tile tasks of the large fronts; the blocks after
 // them run the small fronts: warp tasks (at most kWarpSolveRhs right-hand
@@ -1137,7 +1239,7 @@ __device__ void small_fronts_fwd(int b, WarpTasks wt, int wblocks, const int* sm
 }
 
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
     k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks, int ntile,
                 int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
                 int* __restrict__ err, const int64_t* __restrict__ fv_off,
@@ -1164,7 +1266,7 @@ __global__ void __launch_bounds__(256)
 }
 
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
     k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
                 const int2* __restrict__ tasks, int ntile, int* __restrict__ counter,
                 double* __restrict__ pub, int* __restrict__ abort_flag, int* __restrict__ err,
@@ -1264,7 +1366,6 @@ static int solve_smem_max() {
     size_t m = level_smem_bytes<TL, TV>(64);
     m = std::max(m, small_fwd_smem<TL, TV>(ms, 64));
     m = std::max(m, small_bwd_smem<TL, TV>(ms, ms, 64));
-    m = std::max(m, gather_smem_bytes<TL, TV>(64));
     m = std::max(m, 8 * (size_t)warp_buf_stride(ms, kWarpSolveRhs) * sizeof(TV));
     return (int)m;
 }
@@ -1345,7 +1446,7 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     } else {
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
-        if (ng > 0) sm = std::max(sm, gather_smem_bytes<TL, TV>(nrhs));
+        if (ng > 0) sm = std::max(sm, level_smem_bytes<TL, TV>(nrhs));
         const int grid = ng + nt + wblocks + nsm;
         if (grid > 0)
             k_bwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
