@@ -391,7 +391,7 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
                     // kFwdGroupBlocks / nt1 (streamed by one CTA)
                     for (int i = 0; i < nt1; ++i) ks.push_back({i, ord++, s, i | (1 << 16)});
                     const int G = std::max(1, std::min(SolveScheduleHost::kFwdGroupBlocks / nt1,
-                                                       SolveScheduleHost::kFwdGroupBlocks));
+                                                       SolveScheduleHost::kFwdGroupTiles));
                     for (int i = nt1; i < NT; i += G)
                         ks.push_back({nt1, ord++, s, i | (std::min(G, NT - i) << 16)});
                 } else

@@ -143,6 +143,7 @@ struct SolveScheduleHost {
     // (a pivot tile alone; update tiles grouped to about kFwdGroupBlocks L
     // blocks per task); backward task (s, j): pivot column tile j
     static constexpr int kFwdGroupBlocks = 8;
+    static constexpr int kFwdGroupTiles = 4;  // at most 256 rows: a thread per row
     std::vector<int> tasks;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1 each, in tasks
     std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read

@@ -1202,6 +1202,84 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
 }
 
+// ---------------------------------------------------------------------------
+// forward update tiles with one right-hand side: L read straight from global
+// memory into registers, coalesced (a thread per row), the next columns'
+// loads issued before the current ones are used, no block barrier per L
+// block.  The pivot tiles' published vectors come through poll_published
+// into a shared double buffer (a buffer is rewritten two polls later, after
+// the barrier of the poll between).
+// ---------------------------------------------------------------------------
+
+constexpr int kRt1MaxPivotTiles = 4;
+
+struct Rt1Smem {
+    double* Ys;  // 2 x T: published slots
+    __device__ Rt1Smem() {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        Ys = reinterpret_cast<double*>(smem_raw);
+    }
+};
+template <typename TL>
+__host__ __device__ constexpr size_t rt1_smem_bytes() {
+    return 2 * (size_t)kTile * sizeof(double);
+}
+
+template <typename TL>
+__device__ __forceinline__ TL ldL(const TL* p) {
+    return __ldg(p);
+}
+
+// Forward update rows [R0, R1) of front s (at most 256; one right-hand side):
+// thread = row; columns in groups of 16, the next group's loads issued
+// before the current group's products.
+template <typename TL>
+__device__ void fwd_update_rt1(int s, int R0, int R1, const FrontDesc& F, double* __restrict__ pb,
+                               int* __restrict__ abort_flag, int* __restrict__ err,
+                               const int* __restrict__ amap_off, const int* __restrict__ amap_row,
+                               const int* __restrict__ amap_ent, const TL* __restrict__ Ls,
+                               const double* __restrict__ xp, double* __restrict__ f,
+                               const double* __restrict__ fv) {
+    constexpr int T = kTile;
+    const Rt1Smem sm;
+    const int R = R0 + threadIdx.x;
+    const bool rv = R < R1;
+    const TL* Lr = Ls + F.loff + R;
+    double f0 = 0.0;
+    if (rv) {
+        const int* ar = amap_row + amap_off[s] + R;
+        const int e0 = ar[0], e1 = ar[1];
+        for (int e = e0; e < e1; ++e) f0 += fv[amap_ent[e]];
+    }
+    constexpr int GW = sizeof(TL) == 4 ? 16 : 8;  // columns per group (registers)
+    constexpr int GPB = T / GW;                     // groups per 64-column block
+    const int ng = (F.c + GW - 1) / GW;
+    auto load = [&](int cg, TL (&v)[GW]) {
+#pragma unroll
+        for (int l = 0; l < GW; ++l) {
+            const int col = GW * cg + l;
+            v[l] = (rv && col < F.c) ? ldL(Lr + (int64_t)col * F.ldl) : TL(0);
+        }
+    };
+    double acc = 0.0;
+    TL lv[GW], ln[GW];
+    load(0, lv);
+    for (int cg = 0; cg < ng; ++cg) {
+        if (cg + 1 < ng) load(cg + 1, ln);
+        const int k = cg / GPB;
+        double* Yk = sm.Ys + (k & 1) * T;
+        if (cg % GPB == 0 &&
+            !poll_published(Yk, pb + (int64_t)k * T, min(T, F.c - k * T), 1, abort_flag, err))
+            return;
+        const double* y = Yk + GW * (cg % GPB);
+#pragma unroll
+        for (int l = 0; l < GW; ++l) acc += (double)lv[l] * y[l];
+#pragma unroll
+        for (int l = 0; l < GW; ++l) lv[l] = ln[l];
+    }
+    if (rv) f[R] = f0 - acc;
+}
+
 // One launch per level and direction.  Blocks [0, ntile) take tickets for
 // the dependency-ordered tile tasks of the large fronts; the blocks after
 // them run the small fronts: warp tasks (at most kWarpSolveRhs right-hand
@@ -1261,8 +1339,28 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
         if (threadIdx.x == 0) atomicOr(err, 2);
         return;
     }
-    fwd_tile_task<TL, TV, NQ>(tasks[s_task], fronts, pub, abort_flag, err, fv_off, amap_off,
-                              amap_row, amap_ent, dinv_off, Ls, Dinv, xp, fv, n, nrhs);
+    const int2 tk = tasks[s_task];
+    if constexpr (NQ == 1) {
+        // update tiles of fronts with at most kRt1MaxPivotTiles pivot tiles,
+        // one right-hand side: registers straight from L (measured faster
+        // there; the staged pipeline streams long column ranges better)
+        constexpr int T = kTile;
+        const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
+        const FrontDesc F = fronts[s];
+        const int nt1 = tiles_l(F.c, T);
+        if (nrhs == 1 && i0 >= nt1 && nt1 <= kRt1MaxPivotTiles) {
+            double* pb = pub + (dinv_off[s] / (T * T)) * T;
+            {
+                const TileRange a = tile_range(i0, F.m, F.c, T);
+                const TileRange b = tile_range(i0 + cnt - 1, F.m, F.c, T);
+                fwd_update_rt1<TL>(s, a.start, b.start + b.size, F, pb, abort_flag, err, amap_off,
+                                   amap_row, amap_ent, Ls, xp, front_vec(fv, fv_off, s, 1), fv);
+            }
+            return;
+        }
+    }
+    fwd_tile_task<TL, TV, NQ>(tk, fronts, pub, abort_flag, err, fv_off, amap_off, amap_row,
+                              amap_ent, dinv_off, Ls, Dinv, xp, fv, n, nrhs);
 }
 
 template <typename TL, typename TV, int NQ>
@@ -1429,7 +1527,10 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
                                   : small_bwd_smem<TL, TV>(msmall, msmall, nrhs));
     const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
-    if (nt > 0) sm = std::max(sm, level_smem_bytes<TL, TV>(nrhs));
+    // tile tasks: registers straight from L with one right-hand side
+    const size_t tile_sm = std::max(level_smem_bytes<TL, TV>(nrhs),
+                                    (NQ == 1 && nrhs == 1) ? rt1_smem_bytes<TL>() : (size_t)0);
+    if (nt > 0) sm = std::max(sm, tile_sm);
     int* counter = S.sync + 2 * l + (forward ? 0 : 1);
     int* gcount = S.sync + 2 * D.nlevels;  // one per pivot tile of a large front
     int* abort_flag = gcount + S.nflags;
@@ -1446,7 +1547,7 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     } else {
         TV* part = fv + D.fv_fronts * nrhs;
         const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
-        if (ng > 0) sm = std::max(sm, level_smem_bytes<TL, TV>(nrhs));
+        if (ng > 0) sm = std::max(sm, tile_sm);
         const int grid = ng + nt + wblocks + nsm;
         if (grid > 0)
             k_bwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
