@@ -128,6 +128,9 @@ struct mdgpu_handle_s {
                         (void*)dD64, (void*)dD32,
                         (void*)d_xp, (void*)d_fv, (void*)d_B, (void*)d_X, (void*)d_R, (void*)d_D})
             if (p) cudaFree(p);
+        if (D.fork_ev) cudaEventDestroy(D.fork_ev);
+        if (D.join_ev) cudaEventDestroy(D.join_ev);
+        if (D.aux) cudaStreamDestroy(D.aux);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -206,6 +209,9 @@ void upload_plan(mdgpu_handle_s* h) {
     ck(cudaGetDevice(&h->device), "cudaGetDevice");
     h->on_device = true;
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    ck(cudaStreamCreateWithFlags(&h->D.aux, cudaStreamNonBlocking), "stream");
+    ck(cudaEventCreateWithFlags(&h->D.fork_ev, cudaEventDisableTiming), "event");
+    ck(cudaEventCreateWithFlags(&h->D.join_ev, cudaEventDisableTiming), "event");
     const Plan& P = h->plan;
     DevPlan& D = h->D;
     D.n = P.n;

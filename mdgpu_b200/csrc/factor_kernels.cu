@@ -956,17 +956,35 @@ void init_factor_kernels() {
     set_factor_attributes<float>();
 }
 
+// Level by level.  A level's small and large fronts depend only on lower
+// levels, so where a level has both, its small fronts run on the second
+// stream beside the large fronts (fork and join by events; inside a stream
+// capture these become parallel graph branches).  Serial while the profiler
+// records, so each class keeps its own time.
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
                    cudaStream_t st) {
+    const bool fork = D.aux && D.fork_ev && D.join_ev && !(D.prof && D.prof->on);
     for (int l = 0; l < D.nlevels; ++l) {
-        launch_small_fronts<T>(D, l, Ls, Us, Ax, status, st);
+        const bool has_small =
+            D.h_small_ptr[(l + 1) * kSmallBuckets] > D.h_small_ptr[l * kSmallBuckets];
+        const bool has_large = D.h_large_ptr[l + 1] > D.h_large_ptr[l];
+        const bool par = fork && has_small && has_large;
+        if (par) {
+            cudaEventRecord(D.fork_ev, st);
+            cudaStreamWaitEvent(D.aux, D.fork_ev, 0);
+            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, D.aux);
+            cudaEventRecord(D.join_ev, D.aux);
+        } else {
+            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, st);
+        }
         // FP32 needs the TMA descriptors of the tensor-core path; without them
         // (descriptor encoding unavailable) it keeps the 64-wide tile schedule
         if (sizeof(T) == 8 || D.tmaps)
             launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, st);
         else
             launch_large_level<T>(D, l, Ls, Us, Dinv, Ax, status, st);
+        if (par) cudaStreamWaitEvent(st, D.join_ev, 0);
     }
 }
 

@@ -118,6 +118,10 @@ struct SolveSchedule {
 
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
+    // a second stream and two events: the factor runs a level's small fronts
+    // beside its large fronts (both depend only on lower levels)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     int max_u = 0;  // largest update-matrix order (child relative maps in shared memory)
     int max_m_large = 0, max_nch_large = 0;  // largest large front, most children of one
     std::vector<int> h_level_max_m;          // per level: largest large front

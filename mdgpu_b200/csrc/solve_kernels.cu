@@ -707,7 +707,8 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 // child, deterministic) before the rows are taken into registers.
 // ---------------------------------------------------------------------------
 
-constexpr int kWarpSolveRhs = 4;  // right-hand sides per pass of the warp path
+constexpr int kWarpSolveRhs = 4;   // right-hand sides per pass of the warp path
+constexpr int kSolvePassRhs = 32;  // right-hand sides per pass of the level kernels
 
 // Fronts of at most W rows (W = 8, 16, 32) on a group of W lanes of a warp
 // (32 / W fronts per warp), one row per lane.  mask: the group's lanes; the
@@ -1461,9 +1462,9 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 template <typename TL, typename TV>
 static int solve_smem_max() {
     const int ms = Plan::kSmallMaxRows;
-    size_t m = level_smem_bytes<TL, TV>(64);
-    m = std::max(m, small_fwd_smem<TL, TV>(ms, 64));
-    m = std::max(m, small_bwd_smem<TL, TV>(ms, ms, 64));
+    size_t m = level_smem_bytes<TL, TV>(kSolvePassRhs);
+    m = std::max(m, small_fwd_smem<TL, TV>(ms, kSolvePassRhs));
+    m = std::max(m, small_bwd_smem<TL, TV>(ms, ms, kSolvePassRhs));
     m = std::max(m, 8 * (size_t)warp_buf_stride(ms, kWarpSolveRhs) * sizeof(TV));
     return (int)m;
 }
@@ -1479,7 +1480,7 @@ template <typename TL, typename TV>
 static void set_solve_attributes() {
     set_solve_attributes_nq<TL, TV, 1>();
     set_solve_attributes_nq<TL, TV, 4>();
-    set_solve_attributes_nq<TL, TV, 16>();
+    set_solve_attributes_nq<TL, TV, 8>();
 }
 
 void init_solve_kernels() {
@@ -1573,12 +1574,18 @@ static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* 
 template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st) {
-    if (nrhs <= 4)
-        solve_levels_nq<TL, TV, 1>(D, Ls, Dinv, xp, fv, nrhs, st);
-    else if (nrhs <= 16)
-        solve_levels_nq<TL, TV, 4>(D, Ls, Dinv, xp, fv, nrhs, st);
-    else
-        solve_levels_nq<TL, TV, 16>(D, Ls, Dinv, xp, fv, nrhs, st);
+    // passes of at most kSolvePassRhs right-hand sides (xp columns q0 ..;
+    // the work vectors, sized for more, are reused with the pass's count)
+    for (int q0 = 0; q0 < nrhs; q0 += kSolvePassRhs) {
+        const int nq = std::min(kSolvePassRhs, nrhs - q0);
+        TV* x = xp + (int64_t)q0 * D.n;
+        if (nq <= 4)
+            solve_levels_nq<TL, TV, 1>(D, Ls, Dinv, x, fv, nq, st);
+        else if (nq <= 16)
+            solve_levels_nq<TL, TV, 4>(D, Ls, Dinv, x, fv, nq, st);
+        else
+            solve_levels_nq<TL, TV, 8>(D, Ls, Dinv, x, fv, nq, st);
+    }
 }
 
 template void solve_levels<double, double>(const DevPlan&, const double*, const double*, double*,
