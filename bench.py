@@ -48,13 +48,13 @@ TRAFFIC_PER_STEP_3D64 = {
 }
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
-    "small_front": ["k_small_front"],
-    "assemble": ["k_big_assemble_warp", "k_big_assemble_cols"],
+    "small_front": ["k_tiny_fronts", "k_small_front"],
+    "assemble": ["k_big_assemble_warp"],
     "potrf": ["k_tile_potrf"],
     "trsm": ["k_tile_trsm", "k_tile_update"],
     "schur_update": ["k_schur_tc"],
-    "solve_small": ["k_fwd_prep", "k_bwd_prep"],
-    "solve_large": ["k_fwd_prep", "k_fwd_level", "k_bwd_prep", "k_bwd_level"],
+    "solve_small": ["k_fwd_level", "k_bwd_level"],
+    "solve_large": ["k_fwd_level", "k_bwd_level"],
 }
 
 

@@ -90,7 +90,8 @@ MDGPU_API void mdgpu_destroy(mdgpu_handle h);
 
 /* Scalars: "n", "nsuper", "lnz", "nlevels", "nnz", "max_front", "flops"
  * (the reference's own count, mdgpu.cu:1354-1359), "lstore_bytes",
- * "ustore_bytes", "rows_total", "nchild", "large_fronts". */
+ * "ustore_bytes", "rows_total", "nchild", "large_fronts", "small_fronts",
+ * "nsys", "solve_work_rows", "amap_rows", "amap_entries". */
 MDGPU_API int mdgpu_info(mdgpu_handle h, const char *key, long long *value);
 
 /* Copy a symbolic array out: "perm" (n, new->old; identity if natural),
@@ -99,7 +100,13 @@ MDGPU_API int mdgpu_info(mdgpu_handle h, const char *key, long long *value);
  * "sn_first", "sn_ncols" (nsuper), "child_ptr" (nsuper+1), "child",
  * "Lp" (n+1, as long long), "rows_ptr" (nsuper+1), "rows" (front row sets),
  * "relmap" (per front row: its position in the parent's front, -1 for pivot
- * rows and the root), "level" (nsuper). */
+ * rows and the root), "level" (nsuper).  Solve plan (diagnostics):
+ * "warp_list" (small fronts per level by rows descending), "warp_cnt" (per
+ * level the counts of more than 16, 9..16 and at most 8 rows), "amap_off"
+ * (nsuper; -1 for small fronts), "amap_row", "amap_ent" (forward assembly
+ * of the large fronts: front-vector rows summed into each front row, child
+ * order; a front's vector starts at the sum of the rows of the supernodes
+ * before it). */
 MDGPU_API int mdgpu_get_array(mdgpu_handle h, const char *name, void *dst);
 
 /*

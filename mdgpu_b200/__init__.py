@@ -195,7 +195,10 @@ class Solver:
                  "child": self.info("nchild"), "rows_ptr": ns + 1,
                  "rows": self.info("rows_total"), "relmap": self.info("rows_total"),
                  "level": ns, "sys_row_off": self.info("nsys") + 1,
-                 "sys_val_off": self.info("nsys") + 1}
+                 "sys_val_off": self.info("nsys") + 1,
+                 "warp_list": self.info("small_fronts"), "warp_cnt": 3 * self.info("nlevels"),
+                 "amap_off": ns, "amap_row": self.info("amap_rows"),
+                 "amap_ent": self.info("amap_entries")}
         if name == "Lp":
             a = np.zeros(n + 1, np.int64)
         else:

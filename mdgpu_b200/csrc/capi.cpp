@@ -812,6 +812,9 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "on_device") *value = h->on_device;
     else if (k == "solve_work_rows") *value = h->D.fv_total;
     else if (k == "nsys") *value = h->sys_row_off.empty() ? 1 : (long long)h->sys_row_off.size() - 1;
+    else if (k == "small_fronts") *value = (long long)P.small_list.size();
+    else if (k == "amap_rows") *value = (long long)h->ssched.amap_row.size();
+    else if (k == "amap_entries") *value = (long long)h->ssched.amap_ent.size();
     else return fail(MDGPU_ERR_INVALID, "unknown key " + k);
     return MDGPU_OK;
 }
@@ -846,6 +849,11 @@ int mdgpu_get_array(mdgpu_handle h, const char* name, void* dst) {
     if (k == "sys_row_off") return put(h->sys_row_off);
     if (k == "sys_val_off") return put(h->sys_val_off);
     if (k == "rows") return put(P.rows);
+    if (k == "warp_list") return put(h->ssched.warp_list);
+    if (k == "warp_cnt") return put(h->ssched.warp_cnt);
+    if (k == "amap_off") return put(h->ssched.amap_off);
+    if (k == "amap_row") return put(h->ssched.amap_row);
+    if (k == "amap_ent") return put(h->ssched.amap_ent);
     if (k == "relmap") return put(P.relmap);
     if (k == "rows_ptr") {
         int* d = static_cast<int*>(dst);

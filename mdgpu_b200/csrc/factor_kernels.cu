@@ -261,93 +261,16 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Column-at-a-time variant (used when a front column fits in shared memory):
-// CTA per (front, block of CB columns); each parent column is built in
-// shared memory -- zeros, its A entries, then the matching column of every
-// child in child order (each child's columns landing in the block are
-// consumed in order, the relative maps being increasing) -- and written to
-// the panel / update store once, coalesced.  Same sums in the same order as
-// k_big_assemble.  Shared memory: maxm scalars + per child its next column.
-template <typename T>
-__global__ void __launch_bounds__(256)
-    k_big_assemble_cols(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-                        const int* __restrict__ before, int nitems, int CB,
-                        const int* __restrict__ child, const int* __restrict__ relmap,
-                        const int* __restrict__ a_src, const int* __restrict__ a_pos,
-                        const int* __restrict__ a_colptr, const int* __restrict__ a_colptr_off,
-                        const int* __restrict__ asm_off, const int* __restrict__ asm_range,
-                        const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
-                        int maxm) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* colbuf = reinterpret_cast<T*>(smem_raw);
-    int* cur = reinterpret_cast<int*>(smem_raw + (((size_t)maxm * sizeof(T) + 15) & ~(size_t)15));
-    const int it = find_item(before, nitems, blockIdx.x);
-    const int s = items[it];
-    const int blk = blockIdx.x - before[it];
-    const FrontDesc f = fronts[s];
-    const int j0 = blk * CB, j1 = min(j0 + CB, f.m);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int nch = f.child_end - f.child_beg;
-    const int* ranges = asm_range + asm_off[s] + blk * nch * 2;
-    const int* cp = j0 < f.c ? a_colptr + a_colptr_off[s] : nullptr;
-    for (int h = tid; h < nch; h += nt) cur[h] = ranges[2 * h];
-    __syncthreads();
-    for (int jj = j0; jj < j1; ++jj) {
-        const bool inL = jj < f.c;
-        const int rlo = inL ? 0 : jj;
-        for (int r = rlo + tid; r < f.m; r += nt) colbuf[r] = T(0);
-        __syncthreads();
-        if (inL) {
-            const int e0 = f.a_beg + cp[jj], e1 = f.a_beg + cp[jj + 1];
-            for (int e = e0 + tid; e < e1; e += nt) {
-                const int src = a_src[e];
-                if (src >= 0) colbuf[a_pos[e] & 0xffff] = (T)Ax[src];
-            }
-            __syncthreads();
-        }
-        for (int h = 0; h < nch; ++h) {
-            const int jc = cur[h];
-            if (jc >= ranges[2 * h + 1]) continue;
-            const FrontDesc g = fronts[child[f.child_beg + h]];
-            const int* rm = relmap + g.rows_off + g.c;
-            if (rm[jc] != jj) continue;  // uniform across the CTA
-            const int uc = g.m - g.c;
-            const T* ucol = Us + g.uoff + (int64_t)jc * g.ldu;
-            // eight independent load pairs in flight per thread, then the adds
-            // (rows of one child column land on distinct parent rows)
-            for (int ic0 = jc + tid; ic0 < uc; ic0 += 8 * nt) {
-                int pr[8];
-                T v[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int ic = ic0 + u * nt;
-                    pr[u] = ic < uc ? __ldg(rm + ic) : -1;
-                    v[u] = ic < uc ? __ldg(ucol + ic) : T(0);
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (pr[u] >= 0) colbuf[pr[u]] += v[u];
-            }
-            __syncthreads();
-            if (tid == 0) cur[h] = jc + 1;
-        }
-        if (inL) {
-            T* col = Ls + f.loff + (int64_t)jj * f.ldl;
-            for (int r = tid; r < f.m; r += nt) col[r] = colbuf[r];
-        } else {
-            T* col = Us + f.uoff + (int64_t)(jj - f.c) * f.ldu;
-            for (int r = jj + tid; r < f.m; r += nt) col[r - f.c] = colbuf[r];
-        }
-        __syncthreads();
-    }
-}
-
-// Warp-per-column variant, for levels whose fronts are short enough that
-// every warp of the CTA holds a column of its own in shared memory: no block
-// barriers, only warp syncs.  A child's columns landing in the CTA's block
-// are at most CB (the relative map is injective), so the child column that
-// lands in parent column jj is found by one ballot over the child's range.
-// Same sums in the same order as k_big_assemble_cols.
+// Warp-per-column variant: no block barriers, only warp syncs.  Each warp
+// builds its column in windows of W rows (W a multiple of 16) in its own
+// shared slice, so the slice does not grow with the front.  A child's columns
+// landing in the CTA's block of CB columns are at most CB (the relative map
+// is injective): the child column that lands in parent column jj is found by
+// one ballot over the child's range.  The child rows landing in a window are
+// one contiguous range (increasing relative map), read from the per-16-row
+// block table asm_range.  Every front entry gets its A value (or zero), then
+// the children's contributions in child order: the sums of a child-by-child
+// extend-add.
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_big_assemble_warp(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
@@ -357,65 +280,73 @@ __global__ void __launch_bounds__(256)
                         const int* __restrict__ a_colptr, const int* __restrict__ a_colptr_off,
                         const int* __restrict__ asm_off, const int* __restrict__ asm_range,
                         const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
-                        int ldbuf) {
+                        int W) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    T* colbuf = reinterpret_cast<T*>(smem_raw) + (size_t)warp * ldbuf;
+    T* colbuf = reinterpret_cast<T*>(smem_raw) + (size_t)warp * W;
     const int it = find_item(before, nitems, blockIdx.x);
     const int s = items[it];
     const int blk = blockIdx.x - before[it];
     const FrontDesc f = fronts[s];
     const int j0 = blk * CB, j1 = min(j0 + CB, f.m);
     const int nch = f.child_end - f.child_beg;
-    const int* ranges = asm_range + asm_off[s] + blk * nch * 2;
+    const int* rtab = asm_range + asm_off[s];  // [16-row block][child] -> [lo, hi)
+    const int* ranges = rtab + blk * nch * 2;
     const int* cp = j0 < f.c ? a_colptr + a_colptr_off[s] : nullptr;
     for (int jj = j0 + warp; jj < j1; jj += nw) {
         const bool inL = jj < f.c;
         const int rlo = inL ? 0 : jj;
-        for (int r = rlo + lane; r < f.m; r += 32) colbuf[r] = T(0);
-        __syncwarp();
-        if (inL) {
-            const int e0 = f.a_beg + cp[jj], e1 = f.a_beg + cp[jj + 1];
-            for (int e = e0 + lane; e < e1; e += 32) {
-                const int src = a_src[e];
-                if (src >= 0) colbuf[a_pos[e] & 0xffff] = (T)Ax[src];
-            }
+        for (int R0 = (rlo / W) * W; R0 < f.m; R0 += W) {
+            const int R1 = min(R0 + W, f.m), w0 = max(R0, rlo);
+            for (int r = w0 + lane; r < R1; r += 32) colbuf[r - R0] = T(0);
             __syncwarp();
-        }
-        for (int h = 0; h < nch; ++h) {
-            const int jlo = ranges[2 * h], jhi = ranges[2 * h + 1];
-            if (jlo == jhi) continue;
-            const FrontDesc g = fronts[child[f.child_beg + h]];
-            const int* rm = relmap + g.rows_off + g.c;
-            const int cand = jlo + lane;
-            const unsigned hit = __ballot_sync(0xffffffffu, cand < jhi && __ldg(rm + cand) == jj);
-            if (!hit) continue;
-            const int jc = jlo + __ffs(hit) - 1;
-            const int uc = g.m - g.c;
-            const T* ucol = Us + g.uoff + (int64_t)jc * g.ldu;
-            for (int ic0 = jc + lane; ic0 < uc; ic0 += 8 * 32) {
-                int pr[8];
-                T v[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int ic = ic0 + u * 32;
-                    pr[u] = ic < uc ? __ldg(rm + ic) : -1;
-                    v[u] = ic < uc ? __ldg(ucol + ic) : T(0);
+            if (inL) {
+                const int e0 = f.a_beg + cp[jj], e1 = f.a_beg + cp[jj + 1];
+                for (int e = e0 + lane; e < e1; e += 32) {
+                    const int src = a_src[e], row = a_pos[e] & 0xffff;
+                    if (src >= 0 && row >= R0 && row < R1) colbuf[row - R0] = (T)Ax[src];
                 }
+                __syncwarp();
+            }
+            const int b0 = R0 / 16, b1 = (R1 - 1) / 16;
+            for (int h = 0; h < nch; ++h) {
+                const int jlo = ranges[2 * h], jhi = ranges[2 * h + 1];
+                if (jlo == jhi) continue;
+                const FrontDesc g = fronts[child[f.child_beg + h]];
+                const int* rm = relmap + g.rows_off + g.c;
+                const int cand = jlo + lane;
+                const unsigned hit =
+                    __ballot_sync(0xffffffffu, cand < jhi && __ldg(rm + cand) == jj);
+                if (!hit) continue;
+                const int jc = jlo + __ffs(hit) - 1;
+                // child rows >= jc landing in rows [R0, R1) of the parent
+                const int ilo = max(jc, rtab[(b0 * nch + h) * 2]);
+                const int ihi = rtab[(b1 * nch + h) * 2 + 1];
+                const T* ucol = Us + g.uoff + (int64_t)jc * g.ldu;
+                for (int ic0 = ilo + lane; ic0 < ihi; ic0 += 8 * 32) {
+                    int pr[8];
+                    T v[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (pr[u] >= 0) colbuf[pr[u]] += v[u];
+                    for (int u = 0; u < 8; ++u) {
+                        const int ic = ic0 + u * 32;
+                        pr[u] = ic < ihi ? __ldg(rm + ic) : -1;
+                        v[u] = ic < ihi ? __ldg(ucol + ic) : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (pr[u] >= 0) colbuf[pr[u] - R0] += v[u];
+                }
+                __syncwarp();
+            }
+            if (inL) {
+                T* col = Ls + f.loff + (int64_t)jj * f.ldl;
+                for (int r = w0 + lane; r < R1; r += 32) col[r] = colbuf[r - R0];
+            } else {
+                T* col = Us + f.uoff + (int64_t)(jj - f.c) * f.ldu;
+                for (int r = w0 + lane; r < R1; r += 32) col[r - f.c] = colbuf[r - R0];
             }
             __syncwarp();
         }
-        if (inL) {
-            T* col = Ls + f.loff + (int64_t)jj * f.ldl;
-            for (int r = lane; r < f.m; r += 32) col[r] = colbuf[r];
-        } else {
-            T* col = Us + f.uoff + (int64_t)(jj - f.c) * f.ldu;
-            for (int r = jj + lane; r < f.m; r += 32) col[r - f.c] = colbuf[r];
-        }
-        __syncwarp();
     }
 }
 
@@ -774,13 +705,9 @@ __global__ void __launch_bounds__(256)
 // host launchers
 // ---------------------------------------------------------------------------
 
-// column-at-a-time assembly: one front column plus a cursor per child
-constexpr size_t kAssembleColsSmemMax = 220 * 1024;
-template <typename T>
-static size_t assemble_cols_smem(const DevPlan& D) {
-    return (((size_t)D.max_m_large * sizeof(T) + 15) & ~(size_t)15) +
-           (size_t)std::max(D.max_nch_large, 1) * sizeof(int);
-}
+// rows per window of the warp-per-column assembly's column buffers
+constexpr int kAssembleWindow = 1024;
+constexpr size_t kAssembleColsSmemMax = 8 * kAssembleWindow * sizeof(double);
 
 // shared memory of the tile kernels: two 64 x 65 buffers (operands of the
 // tile products, or S and W of the diagonal-tile factorization)
@@ -878,27 +805,13 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
         switch (op.kind) {
             case OP_ASSEMBLE: {
                 ProfScope ps(D.prof, KC_ASSEMBLE, st, 0, op.elems * sizeof(T) + op.xbytes);
-                const size_t csm = assemble_cols_smem<T>(D);
-                // warps per CTA that get a column buffer of this level's tallest front
-                const int ldbuf = (D.h_level_max_m[level] + 3) & ~3;
-                const int nwarps = (int)std::min<size_t>(
-                    8, kAssembleColsSmemMax / ((size_t)ldbuf * sizeof(T)));
-                if (nwarps >= 4)
-                    k_big_assemble_warp<T><<<w.nctas, 32 * nwarps,
-                                             (size_t)nwarps * ldbuf * sizeof(T), st>>>(
-                        D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols,
-                        D.child, D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off,
-                        D.asm_off, D.asm_range, Ax, Ls, Us, ldbuf);
-                else if (csm <= kAssembleColsSmemMax)
-                    k_big_assemble_cols<T><<<w.nctas, 256, csm, st>>>(
-                        D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols,
-                        D.child, D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off,
-                        D.asm_off, D.asm_range, Ax, Ls, Us, D.max_m_large);
-                else
-                    k_big_assemble<T><<<w.nctas, 256, D.max_u * sizeof(int), st>>>(
-                        D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols,
-                        D.child, D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off,
-                        D.asm_off, D.asm_range, Ax, Ls, Us);
+                // a warp per column, 8 warps, columns built in windows of
+                // kAssembleWindow rows (the whole column when shorter)
+                const int W = std::min(kAssembleWindow, (D.h_level_max_m[level] + 15) & ~15);
+                k_big_assemble_warp<T><<<w.nctas, 256, (size_t)8 * W * sizeof(T), st>>>(
+                    D.fronts, S.items + w.off, S.before + w.off, w.nitems, kAssembleCols, D.child,
+                    D.relmap, D.a_src, D.a_pos, D.a_colptr, D.a_colptr_off, D.asm_off,
+                    D.asm_range, Ax, Ls, Us, W);
                 break;
             }
             case OP_POTRF: {
@@ -945,8 +858,6 @@ static void set_factor_attributes() {
                          (int)diag_smem<T>());
     cudaFuncSetAttribute(k_big_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          227 * 1024);
-    cudaFuncSetAttribute(k_big_assemble_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kAssembleColsSmemMax);
     cudaFuncSetAttribute(k_big_assemble_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kAssembleColsSmemMax);
 }
