@@ -143,7 +143,8 @@ MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, doub
  * handle's plan and factor were allocated earlier by mdgpu_analyze and
  * mdgpu_factor).  A call needs (n + w) x min(nrhs, 64) doubles, w =
  * mdgpu_info(h, "solve_work_rows") (front vector rows plus backward partial
- * sums); larger requests return MDGPU_ERR_INVALID.  All calls share the
+ * sums), one more when n x min(nrhs, 64) is odd; larger requests return
+ * MDGPU_ERR_INVALID.  All calls share the
  * array: calls whose work overlaps on one GPU race and must be serialized by
  * the caller.  The first call on a device looks up the array's address; make
  * it before any stream capture.

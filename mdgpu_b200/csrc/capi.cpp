@@ -1023,14 +1023,19 @@ int mdgpu_solve_device_noalloc(mdgpu_handle h, const double* dB, int ldb, double
         if (!scratch) return fail(MDGPU_ERR_CUDA, msg);
         const int n = h->plan.n;
         const int chunk = std::min(nrhs, 64);
-        const long long need = ((long long)n + h->D.fv_total) * chunk;
+        // the work vectors start on 16 bytes (the solve copies published
+        // vectors from them in 16-byte pieces): the permuted right-hand sides
+        // take an even number of doubles
+        const long long xrows = ((long long)n * chunk + 1) & ~1ll;
+        const long long need = xrows + h->D.fv_total * chunk;
         if (need > noalloc_scratch_capacity())
             return fail(MDGPU_ERR_INVALID,
                         "no-allocation solve needs " + std::to_string(need) +
-                            " scratch doubles ((n + solve_work_rows) x min(nrhs, 64)), limit " +
+                            " scratch doubles ((n + solve_work_rows) x min(nrhs, 64), n x "
+                            "min(nrhs, 64) rounded up to even), limit " +
                             std::to_string(noalloc_scratch_capacity()));
         double* xp = scratch;
-        double* fv = scratch + (int64_t)n * chunk;
+        double* fv = scratch + xrows;
         solve_status_reset(h, st);
         for (int q0 = 0; q0 < nrhs; q0 += 64) {
             const int nq = std::min(64, nrhs - q0);

@@ -12,8 +12,10 @@
 //   * the array holds kNoAllocScratchDoubles doubles (32 MiB) on every GPU
 //     that loads this library, for the life of the process;
 //   * one call needs (n + solve_work_rows) * min(nrhs, 64) doubles (work
-//     rows: front vectors and backward partial sums); larger requests
-//     are rejected with MDGPU_ERR_INVALID and a message giving both numbers;
+//     rows: front vectors and backward partial sums), one more when
+//     n * min(nrhs, 64) is odd (the work rows start on 16 bytes); larger
+//     requests are rejected with MDGPU_ERR_INVALID and a message giving both
+//     numbers;
 //   * all calls share the array, and it keeps the last call's contents: calls
 //     whose kernels overlap on the GPU (different streams, threads or
 //     handles on one device) race on it and must be serialized by the caller;

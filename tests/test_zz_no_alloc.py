@@ -35,9 +35,15 @@ def _colmajor(a):
     return t.t().contiguous().t() if t.dim() == 2 else t
 
 
-@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
-def test_noalloc_solve_matches_regular_solve_twice(prec):
-    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(14, seed=2)
+@pytest.mark.parametrize("prec,gen", [
+    (M.FP64, lambda: mg.laplacian_3d_varcoef(14, seed=2)),
+    (M.FP32, lambda: mg.laplacian_3d_varcoef(14, seed=2)),
+    # odd n with an odd right-hand-side count: the work vectors after the
+    # permuted right-hand sides still start on 16 bytes
+    (M.FP32, lambda: mg.laplacian_3d_varcoef(13, seed=4)),
+], ids=["fp64", "fp32", "fp32_odd_n"])
+def test_noalloc_solve_matches_regular_solve_twice(prec, gen):
+    n, Ap, Ai, Ax = gen()
     S = M.Solver(n, Ap, Ai)
     S.factor(Ax, prec)
     for call, (seed, nrhs) in enumerate([(10, 3), (11, 1)]):
