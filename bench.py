@@ -43,8 +43,8 @@ CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
 # bytes per step; profiles/dram_traffic_fp32_step_3d64.md holds the capture
 # and its command.  The roofline line divides it by the class's launches.
 TRAFFIC_PER_STEP_3D64 = {
-    "small_front": 501853696, "assemble": 7651057408, "potrf": 12498944, "trsm": 2300320000,
-    "schur_update": 15858723072, "solve_small": 671831040, "solve_large": 6392204800,
+    "small_front": 508384768, "assemble": 7675335936, "potrf": 12537856, "trsm": 2306070016,
+    "schur_update": 15846390528, "solve_small": 672630528, "solve_large": 6322322944,
 }
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
