@@ -979,9 +979,6 @@ struct WarpTasks {
     __host__ __device__ int count() const { return n1 + (n2 + 1) / 2 + (n4 + 3) / 4; }
 };
 
-// Blocks that run warp tasks: at most kWarpTaskBlocks, each warp looping over
-// tasks with the grid's warp count as stride.
-constexpr int kWarpTaskBlocks = 148 * 8;
 
 template <typename TL, typename TV, int NQ>
 __device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __restrict__ fronts,
