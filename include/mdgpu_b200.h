@@ -59,6 +59,24 @@ MDGPU_API int mdgpu_analyze(int n, const int *Ap, const int *Ai, int ordering, i
                   mdgpu_handle *out);
 
 /*
+ * Read a matrix file, the reference's cs_load + cs_compress (cs.cpp:4-27,
+ * 251-270, as its driver calls them, mdgpu.cu:1725-1729).  format 0: the
+ * reference's own input, 1-based "i j x" triples read until the first line
+ * that is not one (an index below 1 is an error, as in cs_entry); format 1:
+ * a Matrix Market real coordinate file ('%' lines skipped, then the
+ * "rows cols entries" line, whose sizes are used and checked).  *m, *n: the
+ * largest indices (format 0) or the stated sizes; *nnz: the entries read.
+ * With Ap (n + 1 entries) non-NULL, also the compressed columns: Ai (row
+ * indices, 0-based) and Ax (values) receive nnz entries each (either may be
+ * NULL), a column's entries in file order, as cs_compress leaves them.  Call
+ * once with Ap = NULL for the sizes, then with arrays of those sizes.  For
+ * mdgpu_analyze the file holds the lower triangle (a Matrix Market
+ * "symmetric" file does) with rows ascending within each column.
+ */
+MDGPU_API int mdgpu_load_triplet(const char *path, int format, int *m, int *n, int *nnz, int *Ap,
+                                 int *Ai, double *Ax);
+
+/*
  * Many independent SPD systems under one handle (the batched mode of the
  * many-systems workload; the reference handles one system per run).  System
  * b is the lower triangle (n[b], Ap[b], Ai[b]); each is analysed on its own

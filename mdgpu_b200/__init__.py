@@ -29,7 +29,7 @@ EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
            "mdgpu_refine_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
-           "mdgpu_last_error")
+           "mdgpu_last_error", "mdgpu_load_triplet")
 
 KERNEL_CLASSES = ("small_front", "assemble", "potrf", "trsm", "schur_update", "solve_small",
                   "solve_large", "other")
@@ -87,6 +87,7 @@ def lib():
         L.mdgpu_get_L.argtypes = [vp, vp, vp, vp]
         L.mdgpu_profile.argtypes = [vp, C.c_int]
         L.mdgpu_profile_read.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+        L.mdgpu_load_triplet.argtypes = [C.c_char_p, C.c_int, ip, ip, ip, vp, vp, vp]
         L.mdgpu_status_string.argtypes = [C.c_int]
         L.mdgpu_status_string.restype = C.c_char_p
         L.mdgpu_last_error.restype = C.c_char_p
@@ -113,6 +114,25 @@ def _ptr(a):
 
 def _tensor_ptr(t):
     return C.c_void_p(t.data_ptr())
+
+
+def load_triplet(path, matrix_market=False):
+    """Read a matrix file as the reference's cs_load + cs_compress do
+    (1-based "i j x" triples until the first line that is not one), or a
+    Matrix Market real coordinate file.  Returns (m, n, Ap, Ai, Ax): int32
+    column pointers and 0-based rows, float64 values, a column's entries in
+    file order."""
+    L = lib()
+    m, n, nnz = C.c_int(), C.c_int(), C.c_int()
+    fmt = 1 if matrix_market else 0
+    p = str(path).encode()
+    _check(L.mdgpu_load_triplet(p, fmt, C.byref(m), C.byref(n), C.byref(nnz), None, None, None))
+    Ap = np.zeros(n.value + 1, np.int32)
+    Ai = np.zeros(max(nnz.value, 1), np.int32)
+    Ax = np.zeros(max(nnz.value, 1), np.float64)
+    _check(L.mdgpu_load_triplet(p, fmt, C.byref(m), C.byref(n), C.byref(nnz), _ptr(Ap), _ptr(Ai),
+                                _ptr(Ax)))
+    return m.value, n.value, Ap, Ai[: nnz.value], Ax[: nnz.value]
 
 
 class Solver:

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cstdio>
 #include <map>
 #include <cstring>
 #include <new>
@@ -664,6 +665,83 @@ int mdgpu_analyze(int n, const int* Ap, const int* Ai, int ordering, int tree, i
             throw;
         }
         *out = h;
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_load_triplet(const char* path, int format, int* m, int* n, int* nnz, int* Ap, int* Ai,
+                       double* Ax) {
+    if (!path || !m || !n || !nnz || (format != 0 && format != 1))
+        return fail(MDGPU_ERR_INVALID, "bad arguments");
+    return guarded([&]() -> int {
+        FILE* f = std::fopen(path, "r");
+        if (!f) return fail(MDGPU_ERR_INVALID, std::string("cannot open ") + path);
+        long long msize = -1, nsize = -1;
+        if (format == 1) {  // Matrix Market: '%' lines, then "rows cols entries"
+            char line[4096];
+            bool have = false;
+            while (std::fgets(line, sizeof line, f)) {
+                if (line[0] == '%') continue;
+                long long a, b, c;
+                if (std::sscanf(line, "%lld %lld %lld", &a, &b, &c) != 3 || a < 0 || b < 0 ||
+                    a > INT_MAX || b > INT_MAX) {
+                    std::fclose(f);
+                    return fail(MDGPU_ERR_INVALID, "bad Matrix Market size line");
+                }
+                msize = a;
+                nsize = b;
+                have = true;
+                break;
+            }
+            if (!have) {
+                std::fclose(f);
+                return fail(MDGPU_ERR_INVALID, "no Matrix Market size line");
+            }
+        }
+        // 1-based "i j x" triples, read until the first that does not parse
+        std::vector<int> ti, tj;
+        std::vector<double> tx;
+        int i, j;
+        double x;
+        while (std::fscanf(f, "%d %d %lg", &i, &j, &x) == 3) {
+            if (i < 1 || j < 1) {
+                std::fclose(f);
+                return fail(MDGPU_ERR_INVALID, "index below 1 in entry " + std::to_string(ti.size()));
+            }
+            if ((msize >= 0 && i > msize) || (nsize >= 0 && j > nsize)) {
+                std::fclose(f);
+                return fail(MDGPU_ERR_INVALID,
+                            "entry " + std::to_string(ti.size()) + " outside the stated size");
+            }
+            ti.push_back(i - 1);
+            tj.push_back(j - 1);
+            tx.push_back(x);
+        }
+        std::fclose(f);
+        int mm = 0, nn = 0;
+        for (size_t k = 0; k < ti.size(); ++k) {
+            mm = std::max(mm, ti[k] + 1);
+            nn = std::max(nn, tj[k] + 1);
+        }
+        if (msize >= 0) {
+            mm = (int)msize;
+            nn = (int)nsize;
+        }
+        if (ti.size() > (size_t)INT_MAX) return fail(MDGPU_ERR_INVALID, "too many entries");
+        *m = mm;
+        *n = nn;
+        *nnz = (int)ti.size();
+        if (Ap) {  // compressed columns, entries of a column in file order
+            std::vector<int> w(nn + 1, 0);
+            for (int c : tj) w[c + 1]++;
+            for (int c = 0; c < nn; ++c) w[c + 1] += w[c];
+            std::copy(w.begin(), w.end(), Ap);
+            for (size_t k = 0; k < ti.size(); ++k) {
+                const int p = w[tj[k]]++;
+                if (Ai) Ai[p] = ti[k];
+                if (Ax) Ax[p] = tx[k];
+            }
+        }
         return MDGPU_OK;
     });
 }
