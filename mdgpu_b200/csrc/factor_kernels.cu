@@ -103,70 +103,67 @@ __global__ void k_small_front(const FrontDesc* __restrict__ fronts, const int* _
     }
 }
 
-// Fronts of at most 32 rows: a warp per front (four per CTA), the front in the
-// warp's own 32 x 33 shared slice; the same steps and sums in the same order
-// as k_small_front, with warp syncs only.
+// Fronts of at most 32 rows: a group of W lanes per front (W = 32, 16, 8:
+// one, two or four fronts per warp), the front in the group's own W x (W + 1)
+// shared slice; the same steps and sums in the same order as k_small_front,
+// with group syncs only.
 constexpr int kTinyFrontRows = 32;
 
-template <typename T>
-__global__ void __launch_bounds__(128)
-    k_tiny_fronts(const FrontDesc* __restrict__ fronts, const int* __restrict__ list, int nfronts,
-                  const int* __restrict__ child, const int* __restrict__ relmap,
-                  const int* __restrict__ a_src, const int* __restrict__ a_pos,
-                  const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
-                  int* __restrict__ status) {
-    constexpr int LD = kTinyFrontRows + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (q >= nfronts) return;
-    T* Fm = reinterpret_cast<T*>(smem_raw) + (size_t)warp * kTinyFrontRows * LD;
-    const int s = list[q];
+template <typename T, int W>
+__device__ void tiny_front_group(int s, const FrontDesc* __restrict__ fronts,
+                                 const int* __restrict__ child, const int* __restrict__ relmap,
+                                 const int* __restrict__ a_src, const int* __restrict__ a_pos,
+                                 const double* __restrict__ Ax, T* __restrict__ Ls,
+                                 T* __restrict__ Us, int* __restrict__ status, T* Fm) {
+    constexpr int LD = W + 1;
+    const unsigned mask =
+        W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1)));
+    const int gl = threadIdx.x & (W - 1);
     const FrontDesc f = fronts[s];
     const int m = f.m, c = f.c, u = m - c;
-    for (int idx = lane; idx < m * LD; idx += 32) Fm[idx] = T(0);
-    __syncwarp();
-    for (int e = f.a_beg + lane; e < f.a_end; e += 32) {
+    for (int idx = gl; idx < m * LD; idx += W) Fm[idx] = T(0);
+    __syncwarp(mask);
+    for (int e = f.a_beg + gl; e < f.a_end; e += W) {
         const int src = a_src[e];
         if (src >= 0) {
             const int pos = a_pos[e];
             Fm[(pos & 0xffff) + (pos >> 16) * LD] = (T)Ax[src];
         }
     }
-    __syncwarp();
+    __syncwarp(mask);
     for (int h = f.child_beg; h < f.child_end; ++h) {
         const FrontDesc g = fronts[child[h]];
         const int uc = g.m - g.c;
         if (uc <= 0) continue;
         const int* rm = relmap + g.rows_off + g.c;
         const T* U = Us + g.uoff;
-        for (int idx = lane; idx < uc * uc; idx += 32) {
+        for (int idx = gl; idx < uc * uc; idx += W) {
             const int j = idx / uc, i = idx - j * uc;
             if (i >= j) Fm[rm[i] + rm[j] * LD] += U[i + (int64_t)j * g.ldu];
         }
-        __syncwarp();
+        __syncwarp(mask);
     }
     // partial Cholesky of the c pivot columns (right-looking, panel only):
-    // lane i owns row i and touches only it; the multipliers of the other
-    // rows arrive by shuffles
+    // lane i of the group owns row i and touches only it; the multipliers of
+    // the other rows arrive by shuffles
     for (int k = 0; k < c; ++k) {
         const T dkk = Fm[k + k * LD];
-        if (lane == 0 && !(dkk > T(0))) flag_pivot(status, f.first_col + k);
+        if (gl == 0 && !(dkk > T(0))) flag_pivot(status, f.first_col + k);
         const T d = sqrt(dkk);
         const T inv = T(1) / d;
-        const T lik = (lane > k && lane < m) ? Fm[lane + k * LD] * inv : T(0);
-        if (lane == k) Fm[k + k * LD] = d;
-        if (lane > k && lane < m) Fm[lane + k * LD] = lik;
+        const T lik = (gl > k && gl < m) ? Fm[gl + k * LD] * inv : T(0);
+        if (gl == k) Fm[k + k * LD] = d;
+        if (gl > k && gl < m) Fm[gl + k * LD] = lik;
         for (int j = k + 1; j < c; ++j) {
-            const T ljk = __shfl_sync(0xffffffffu, lik, j);
-            if (lane >= j && lane < m) Fm[lane + j * LD] -= lik * ljk;
+            const T ljk = __shfl_sync(mask, lik, j, W);
+            if (gl >= j && gl < m) Fm[gl + j * LD] -= lik * ljk;
         }
-        __syncwarp();
+        __syncwarp(mask);
     }
     // Schur complement straight to the update store
     if (f.uoff >= 0) {
         T* Ud = Us + f.uoff;
-        for (int idx = lane; idx < u * u; idx += 32) {
+        for (int idx = gl; idx < u * u; idx += W) {
             const int j = idx / u, i = idx - j * u;
             if (i >= j) {
                 T acc = Fm[(c + i) + (c + j) * LD];
@@ -176,9 +173,45 @@ __global__ void __launch_bounds__(128)
         }
     }
     T* Ld = Ls + f.loff;
-    for (int idx = lane; idx < m * c; idx += 32) {
+    for (int idx = gl; idx < m * c; idx += W) {
         const int j = idx / m, i = idx - j * m;
         Ld[i + (int64_t)j * f.ldl] = (i >= j) ? Fm[i + j * LD] : T(0);
+    }
+    __syncwarp(mask);  // the slice is reused by the group's next front
+}
+
+// One level's fronts of at most 32 rows as warp tasks over a rows-descending
+// list: tasks [0, n32) one front each (17..32 rows), then two fronts of 9..16
+// rows per task, then four of at most 8; persistent warps take tasks with
+// the grid's warp count as stride.
+template <typename T>
+__global__ void __launch_bounds__(128)
+    k_tiny_fronts(const FrontDesc* __restrict__ fronts, const int* __restrict__ list, int n32,
+                  int n16, int n8, const int* __restrict__ child, const int* __restrict__ relmap,
+                  const int* __restrict__ a_src, const int* __restrict__ a_pos,
+                  const double* __restrict__ Ax, T* __restrict__ Ls, T* __restrict__ Us,
+                  int* __restrict__ status) {
+    constexpr int LD = kTinyFrontRows + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    T* slice = reinterpret_cast<T*>(smem_raw) + (size_t)warp * kTinyFrontRows * LD;
+    const int t16 = (n16 + 1) / 2, t8 = (n8 + 3) / 4, ntask = n32 + t16 + t8;
+    for (int t = blockIdx.x * wpb + warp; t < ntask; t += gridDim.x * wpb) {
+        if (t < n32) {
+            tiny_front_group<T, 32>(list[t], fronts, child, relmap, a_src, a_pos, Ax, Ls, Us,
+                                    status, slice);
+        } else if (t < n32 + t16) {
+            const int k = 2 * (t - n32) + (lane >> 4);
+            if (k < n16)
+                tiny_front_group<T, 16>(list[n32 + k], fronts, child, relmap, a_src, a_pos, Ax,
+                                        Ls, Us, status, slice + (lane >> 4) * 16 * 17);
+        } else {
+            const int k = 4 * (t - n32 - t16) + (lane >> 3);
+            if (k < n8)
+                tiny_front_group<T, 8>(list[n32 + n16 + k], fronts, child, relmap, a_src, a_pos,
+                                       Ax, Ls, Us, status, slice + (lane >> 3) * 8 * 9);
+        }
+        __syncwarp();
     }
 }
 
@@ -719,7 +752,7 @@ static size_t diag_smem() {
 template <typename T>
 void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax,
                          int* status, cudaStream_t st) {
-    {  // fronts of at most 32 rows (the first two buckets): a warp each
+    {  // fronts of at most 32 rows (the first two buckets): one, two or four per warp
         const int beg = D.h_small_ptr[level * kSmallBuckets];
         const int end = D.h_small_ptr[level * kSmallBuckets + Plan::kTinyBuckets];
         if (end > beg) {
@@ -728,9 +761,17 @@ void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double
                 by += D.h_small_bytes[level * kSmallBuckets + b];
             ProfScope ps(D.prof, KC_SMALL_FRONT, st, 0, by * sizeof(T) / 8.0);
             const size_t smem = (size_t)4 * kTinyFrontRows * (kTinyFrontRows + 1) * sizeof(T);
-            k_tiny_fronts<T><<<(end - beg + 3) / 4, 128, smem, st>>>(
-                D.fronts, D.small_list + beg, end - beg, D.child, D.relmap, D.a_src, D.a_pos, Ax,
-                Ls, Us, status);
+            // the level's slice of the rows-descending warp list: its fronts
+            // of 17..32 rows end the part above 16 rows, then 9..16, then <= 8
+            const int* cnt = D.solve.warp_cnt.data() + 3 * level;
+            const int n32 = D.h_small_ptr[level * kSmallBuckets + 2] -
+                            D.h_small_ptr[level * kSmallBuckets + 1];
+            const int n16 = cnt[1], n8 = cnt[2];
+            const int ntask = n32 + (n16 + 1) / 2 + (n8 + 3) / 4;
+            const int blocks = std::min((ntask + 3) / 4, 148 * 8);
+            k_tiny_fronts<T><<<blocks, 128, smem, st>>>(
+                D.fronts, D.solve.warp_list + beg + (cnt[0] - n32), n32, n16, n8, D.child,
+                D.relmap, D.a_src, D.a_pos, Ax, Ls, Us, status);
         }
     }
     for (int b = Plan::kTinyBuckets; b < kSmallBuckets; ++b) {
