@@ -43,8 +43,8 @@ CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
 # bytes per step; profiles/dram_traffic_fp32_step_3d64.md holds the capture
 # and its command.  The roofline line divides it by the class's launches.
 TRAFFIC_PER_STEP_3D64 = {
-    "small_front": 508384768, "assemble": 7675335936, "potrf": 12537856, "trsm": 2306070016,
-    "schur_update": 15846390528, "solve_small": 672630528, "solve_large": 6322322944,
+    "small_front": 509384192, "assemble": 7672552960, "potrf": 12531456, "trsm": 2301383680,
+    "schur_update": 15850466816, "solve_small": 672695552, "solve_large": 6323437056,
 }
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
