@@ -183,6 +183,26 @@ MDGPU_API int mdgpu_refine_device(mdgpu_handle h, const double *dB, int ldb, dou
                         double tol, int maxit, double *berr, int *iters, void *stream);
 
 /*
+ * Differentiation (no counterpart in the reference, whose driver only
+ * factors and solves).  mdgpu_logdet: log det A = 2 sum log L(j, j) of the
+ * current factor (FP64 or FP32).  mdgpu_selinv: the selected inverse
+ * Z = A^-1 on the pattern of L of the current FP64 factor (Takahashi's
+ * recurrence over the fronts from the root down; it reuses the factor's
+ * update-matrix storage, so call it after the factor and before the next
+ * one).  mdgpu_grad_lower: the gradient of loss = log det A + b' A^-1 b with
+ * respect to the caller's lower-triangle values Ax, given x = A^-1 b in the
+ * caller's ordering (x = NULL: the gradient of log det A alone): an
+ * off-diagonal entry, which stands for A(i,j) and A(j,i), gets
+ * 2 (Z(i,j) - x_i x_j), a diagonal entry Z(i,i) - x_i^2; dropped duplicates
+ * get 0.  G has nnz (Ap[n]) entries; the gradient with respect to b is 2 x.
+ * _device: x and G in device memory.
+ */
+MDGPU_API int mdgpu_logdet(mdgpu_handle h, double *logdet, void *stream);
+MDGPU_API int mdgpu_selinv(mdgpu_handle h, void *stream);
+MDGPU_API int mdgpu_grad_lower(mdgpu_handle h, const double *x, double *G, void *stream);
+MDGPU_API int mdgpu_grad_lower_device(mdgpu_handle h, const double *dx, double *dG, void *stream);
+
+/*
  * Copy L out as compressed columns, the spL contract of the reference
  * (mdgpu.cu:1346-1352, 1859-1875): Lp[n+1] (long long), Li[lnz] row indices
  * ascending with the diagonal first, Lx[lnz] values (FP64; an FP32 factor is

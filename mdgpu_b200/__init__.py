@@ -29,7 +29,8 @@ EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
            "mdgpu_refine_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
-           "mdgpu_last_error", "mdgpu_load_triplet")
+           "mdgpu_last_error", "mdgpu_load_triplet", "mdgpu_logdet", "mdgpu_selinv",
+           "mdgpu_grad_lower", "mdgpu_grad_lower_device")
 
 KERNEL_CLASSES = ("small_front", "assemble", "potrf", "trsm", "schur_update", "solve_small",
                   "solve_large", "other")
@@ -88,6 +89,10 @@ def lib():
         L.mdgpu_profile.argtypes = [vp, C.c_int]
         L.mdgpu_profile_read.argtypes = [vp, C.c_int, vp, vp, vp, vp]
         L.mdgpu_load_triplet.argtypes = [C.c_char_p, C.c_int, ip, ip, ip, vp, vp, vp]
+        L.mdgpu_logdet.argtypes = [vp, vp, vp]
+        L.mdgpu_selinv.argtypes = [vp, vp]
+        L.mdgpu_grad_lower.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_grad_lower_device.argtypes = [vp, vp, vp, vp]
         L.mdgpu_status_string.argtypes = [C.c_int]
         L.mdgpu_status_string.restype = C.c_char_p
         L.mdgpu_last_error.restype = C.c_char_p
@@ -315,6 +320,36 @@ class Solver:
                 total_launches += n.value
         dom = max(classes, key=lambda k: classes[k]["ms"]) if classes else None
         return {"classes": classes, "dominant": dom, "launches_per_step": total_launches}
+
+    # ---- differentiation ----------------------------------------------
+    def logdet(self, stream=None):
+        """log det A from the current factor."""
+        v = C.c_double()
+        _check(lib().mdgpu_logdet(self._h, C.byref(v), stream), self._h)
+        return v.value
+
+    def selinv(self, stream=None):
+        """Selected inverse of the current FP64 factor (kept on the device)."""
+        _check(lib().mdgpu_selinv(self._h, stream), self._h)
+
+    def grad_lower(self, x=None, stream=None):
+        """d(log det A + b' A^-1 b) / d Ax for the caller's lower-triangle
+        values, x = A^-1 b (None: the gradient of log det A alone); numpy x
+        gives a numpy G, a CUDA tensor x (or x None with device=True) a CUDA
+        tensor."""
+        nnz = self.info("nnz")
+        if x is not None and hasattr(x, "data_ptr"):
+            import torch
+
+            G = torch.empty(nnz, dtype=torch.float64, device=x.device)
+            _check(lib().mdgpu_grad_lower_device(self._h, _tensor_ptr(x), _tensor_ptr(G), stream),
+                   self._h)
+            return G
+        G = np.zeros(max(nnz, 1))
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        _check(lib().mdgpu_grad_lower(self._h, None if xa is None else _ptr(xa), _ptr(G), stream),
+               self._h)
+        return G[:nnz]
 
     def get_L(self, values=True):
         """L as (Lp int64, Li int32, Lx float64) -- the reference's spL."""

@@ -103,6 +103,12 @@ struct mdgpu_handle_s {
     cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
     std::map<int, cudaGraphExec_t> sgraph;  // key: precision * 1024 + rhs count
     int factored = -1;  // precision of the current factor, -1 none
+    bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dU64
+    double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
+    double* d_Y = nullptr;         // its Y scratch
+    double* d_logdet = nullptr;    // logdet partial sums, then the result
+    double* d_gx = nullptr;        // gradient: x and G on the device (host entry)
+    double* d_gG = nullptr;
     int status_init[2] = {0, 0};
     int not_spd = -1;
     Profiler prof;
@@ -125,6 +131,8 @@ struct mdgpu_handle_s {
             if (g) cudaGraphExecDestroy(g);
         drop_solve_graphs();
         for (void* p : owned) cudaFree(p);
+        for (void* p : {(void*)dZ64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG})
+            if (p) cudaFree(p);
         for (void* p : {(void*)d_Ax, (void*)dL64, (void*)dU64, (void*)dL32, (void*)dU32,
                         (void*)dD64, (void*)dD32,
                         (void*)d_xp, (void*)d_fv, (void*)d_B, (void*)d_X, (void*)d_R, (void*)d_D})
@@ -266,6 +274,32 @@ void upload_plan(mdgpu_handle_s* h) {
     D.asm_off = h->keep(upload(P.asm_off));
     D.asm_range = h->keep(upload(P.asm_range));
     D.dinv_total = P.dinv_total;
+    {
+        // selected inverse: supernodes by level, Y scratch per level's fronts
+        // side by side (levels reuse it), each lower entry's front
+        const std::vector<int>& lv = h->level;
+        D.h_level_ptr.assign(P.nlevels + 1, 0);
+        for (int s = 0; s < P.nsuper; ++s) D.h_level_ptr[lv[s] + 1]++;
+        for (int l = 0; l < P.nlevels; ++l) D.h_level_ptr[l + 1] += D.h_level_ptr[l];
+        std::vector<int> ll(std::max(P.nsuper, 1)), nxt(D.h_level_ptr.begin(), D.h_level_ptr.end() - 1);
+        for (int s = 0; s < P.nsuper; ++s) ll[nxt[lv[s]]++] = s;
+        D.level_list = h->keep(upload(ll));
+        std::vector<int64_t> yo(P.nsuper, 0);
+        D.yscr_total = 0;
+        for (int l = 0; l < P.nlevels; ++l) {
+            int64_t off = 0;
+            for (int q = D.h_level_ptr[l]; q < D.h_level_ptr[l + 1]; ++q) {
+                yo[ll[q]] = off;
+                off += (int64_t)P.fronts[ll[q]].m * selinv_block();
+            }
+            D.yscr_total = std::max(D.yscr_total, off);
+        }
+        D.yoff = h->keep(upload(yo));
+        std::vector<int> af(std::max<size_t>(P.a_src.size(), 1), 0);
+        for (int s = 0; s < P.nsuper; ++s)
+            for (int e = P.fronts[s].a_beg; e < P.fronts[s].a_end; ++e) af[e] = s;
+        D.a_front = h->keep(upload(af));
+    }
     D.sched64.items = h->keep(upload(h->fsched.store.items));
     D.sched64.before = h->keep(upload(h->fsched.store.ctas_before));
     D.sched64.h_level_beg = h->fsched.level_beg;
@@ -427,6 +461,7 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
         return fail(MDGPU_ERR_INVALID, "unknown precision");
     ck(cudaSetDevice(h->device), "cudaSetDevice");
     ensure_factor_storage(h, precision);
+    h->selinv_done = false;
     if (dAx != h->d_Ax)
         ck(cudaMemcpyAsync(h->d_Ax, dAx, h->plan.nnz_user * sizeof(double),
                            cudaMemcpyDeviceToDevice, st),
@@ -460,6 +495,7 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
                                         std::to_string(stat[1]) + ")");
     }
     h->factored = precision;
+    h->selinv_done = false;
     h->not_spd = (col == big) ? -1 : col;
     if (h->not_spd >= 0) {
         h->factored = -1;
@@ -1041,6 +1077,76 @@ int mdgpu_refine(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, i
            "download solution");
         int rs = solve_status_check(h, st);
         return rs != MDGPU_OK ? rs : rc;
+    });
+}
+
+int mdgpu_logdet(mdgpu_handle h, double* logdet, void* stream) {
+    if (!h || !logdet) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        if (!h->d_logdet) h->d_logdet = dalloc<double>(logdet_partials() + 1);
+        double* out = h->d_logdet + logdet_partials();
+        if (h->factored == MDGPU_FP64)
+            launch_logdet<double>(h->D, h->dL64, h->d_logdet, out, st);
+        else
+            launch_logdet<float>(h->D, h->dL32, h->d_logdet, out, st);
+        ck(cudaGetLastError(), "logdet launch");
+        ck(cudaMemcpyAsync(logdet, out, sizeof(double), cudaMemcpyDeviceToHost, st), "logdet");
+        ck(cudaStreamSynchronize(st), "logdet");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_selinv(mdgpu_handle h, void* stream) {
+    if (!h) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored != MDGPU_FP64) return fail(MDGPU_ERR_STATE, "the selected inverse needs an FP64 factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        if (!h->dZ64) h->dZ64 = dalloc<double>(h->plan.lstore);
+        if (!h->d_Y) h->d_Y = dalloc<double>(std::max<int64_t>(h->D.yscr_total, 1));
+        launch_selinv(h->D, h->dL64, h->dZ64, h->dU64, h->d_Y, st);
+        ck(cudaGetLastError(), "selected inverse launch");
+        ck(cudaStreamSynchronize(st), "selected inverse");
+        h->selinv_done = true;
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_grad_lower_device(mdgpu_handle h, const double* dx, double* dG, void* stream) {
+    if (!h || !dG) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (!h->selinv_done) return fail(MDGPU_ERR_STATE, "no selected inverse of the current factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ck(cudaMemsetAsync(dG, 0, (size_t)h->plan.nnz_user * sizeof(double), st), "zero G");
+        launch_grad_lower(h->D, (int)h->plan.a_src.size(), h->d_perm, h->dZ64, dx, dG, st);
+        ck(cudaGetLastError(), "gradient launch");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_grad_lower(mdgpu_handle h, const double* x, double* G, void* stream) {
+    if (!h || !G) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (!h->selinv_done) return fail(MDGPU_ERR_STATE, "no selected inverse of the current factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        const int64_t n = h->plan.n, nnz = h->plan.nnz_user;
+        if (!h->d_gx) h->d_gx = dalloc<double>(n);
+        if (!h->d_gG) h->d_gG = dalloc<double>(std::max<int64_t>(nnz, 1));
+        if (x) ck(cudaMemcpyAsync(h->d_gx, x, n * sizeof(double), cudaMemcpyHostToDevice, st), "x");
+        int rc = mdgpu_grad_lower_device(h, x ? h->d_gx : nullptr, h->d_gG, stream);
+        if (rc != MDGPU_OK) return rc;
+        ck(cudaMemcpyAsync(G, h->d_gG, nnz * sizeof(double), cudaMemcpyDeviceToHost, st), "G");
+        ck(cudaStreamSynchronize(st), "gradient");
+        return MDGPU_OK;
     });
 }
 

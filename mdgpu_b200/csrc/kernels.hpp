@@ -131,6 +131,13 @@ struct DevPlan {
     int* relmap = nullptr;
     int* a_src = nullptr;
     int* a_pos = nullptr;
+    // selected inverse: every supernode by level (root level last), the
+    // Y scratch offset per supernode, and per lower-triangle entry its front
+    int* level_list = nullptr;
+    std::vector<int> h_level_ptr;  // nlevels + 1
+    int64_t* yoff = nullptr;
+    int64_t yscr_total = 0;
+    int* a_front = nullptr;
     int* a_colptr = nullptr;
     int* a_colptr_off = nullptr;
     int* small_list = nullptr;
@@ -204,5 +211,15 @@ void permute_gather(const int* perm, const double* b, double* xp, int n, int nrh
                     cudaStream_t st);
 void permute_scatter(const int* perm, const double* xp, double* x, int n, int nrhs, int ldx,
                      cudaStream_t st);
+
+// selected inverse and adjoint (selinv.cu)
+void launch_selinv(const DevPlan& D, const double* Ls, double* Zs, double* Zu, double* Yscr,
+                   cudaStream_t st);
+void launch_grad_lower(const DevPlan& D, int nnz, const int* perm, const double* Zs,
+                       const double* x, double* G, cudaStream_t st);
+template <typename T>
+void launch_logdet(const DevPlan& D, const T* Ls, double* partial, double* out, cudaStream_t st);
+int logdet_partials();
+int selinv_block();
 
 }  // namespace mdgpu

@@ -185,3 +185,25 @@ def load_dir(d):
             with open(p) as fh:
                 out["meta"] = json.load(fh)
     return out
+
+
+def selected_inverse(n, Lp, Li, Lx):
+    """Z = A^-1 on the pattern of L (and its transpose) from the CSC factor
+    A = L L' (rows ascending, diagonal first): the Takahashi recurrence,
+    column by column from the last --
+        y = L(R, j) / L(j, j),  Z(R, j) = -Z(R, R) y,
+        Z(j, j) = 1 / L(j, j)^2 - y' Z(R, j)
+    with R the rows below the diagonal of column j (a clique of the filled
+    graph, so Z(R, R) lies on the pattern).  Dense n x n storage: for the
+    small test sizes only.  TEST INFRASTRUCTURE ONLY."""
+    Z = np.zeros((n, n))
+    for j in range(n - 1, -1, -1):
+        p0, p1 = int(Lp[j]), int(Lp[j + 1])
+        d = Lx[p0]
+        R = np.asarray(Li[p0 + 1:p1], dtype=np.int64)
+        y = Lx[p0 + 1:p1] / d
+        zr = -Z[np.ix_(R, R)] @ y
+        Z[R, j] = zr
+        Z[j, R] = zr
+        Z[j, j] = 1.0 / (d * d) - y @ zr
+    return Z
