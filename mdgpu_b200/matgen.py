@@ -90,6 +90,27 @@ def laplacian_grid(dims, *, seed=None, sigma=1.0, shift=0.0, const=None):
     return _assemble_lower(n, rows, cols, vals)
 
 
+def laplacian_grid_edges(dims, *, seed=None, sigma=1.0, shift=0.0):
+    """laplacian_grid with its edges: (n, Ap, Ai, Ax, lo, hi, cond), edge e
+    joining unknowns lo[e] < hi[e] with conductance cond[e] (the same draws
+    as laplacian_grid for the same arguments)."""
+    dims = tuple(int(d) for d in dims)
+    n = int(np.prod(dims))
+    los, his = _edges_grid(dims)
+    lo = np.concatenate(los)
+    hi = np.concatenate(his)
+    rng = np.random.default_rng(seed)
+    cond = np.concatenate([rng.lognormal(0.0, sigma, size=len(l)) for l in los])
+    diag = np.full(n, float(shift))
+    np.add.at(diag, lo, cond)
+    np.add.at(diag, hi, cond)
+    rows = np.concatenate([np.arange(n), hi])
+    cols = np.concatenate([np.arange(n), lo])
+    vals = np.concatenate([diag, -cond])
+    n, Ap, Ai, Ax = _assemble_lower(n, rows, cols, vals)
+    return n, Ap, Ai, Ax, lo, hi, cond
+
+
 def laplacian_2d_5pt(side=100):
     """2D 5-point Dirichlet Laplacian: diagonal 4, off-diagonals -1."""
     return laplacian_grid((side, side), const=(4.0, -1.0))
