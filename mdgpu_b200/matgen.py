@@ -165,3 +165,87 @@ def write_triplets(path, n, Ap, Ai, Ax):
             for i, j, x in zip(Ai, cols, Ax)
         ]
         f.writelines(lines)
+
+
+def elasticity_3dof(side=40, seed=0, sigma=1.0, shift=1e-2):
+    """3 unknowns per node of a side^3 node grid with 27-point connectivity,
+    elasticity-like: for an edge (i, j) with stencil offset unit vector e,
+    B_ij = w_ij (I_3 + 0.5 e e') with w_ij ~ lognormal(0, sigma); the
+    off-diagonal block is -B_ij and the diagonal block sum_j B_ij + shift I_3
+    (a sum of positive semidefinite edge terms plus shift I: SPD).  Unknown
+    3 k + c is component c of node k.  Lower CSC of the 3 side^3 system."""
+    side = int(side)
+    nn = side ** 3
+    idx = np.arange(nn, dtype=np.int64).reshape(side, side, side)  # [z][y][x]
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    diag = np.zeros((nn, 3, 3))
+    # the 13 offsets with a positive first nonzero component: each edge once
+    offs = [(dz, dy, dx) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+            if (dz, dy, dx) > (0, 0, 0)]
+    for dz, dy, dx in offs:
+        e = np.array([dx, dy, dz], dtype=np.float64)
+        e /= np.linalg.norm(e)
+        K = np.eye(3) + 0.5 * np.outer(e, e)
+        sz = slice(max(0, -dz), side - max(0, dz))
+        sy = slice(max(0, -dy), side - max(0, dy))
+        sx = slice(max(0, -dx), side - max(0, dx))
+        a = idx[sz, sy, sx].ravel()
+        b = idx[sz.start + dz:sz.stop + dz, sy.start + dy:sy.stop + dy,
+                sx.start + dx:sx.stop + dx].ravel()
+        w = rng.lognormal(0.0, sigma, size=a.size)
+        Bs = w[:, None, None] * K[None]
+        np.add.at(diag, a, Bs)
+        np.add.at(diag, b, Bs)
+        lo, hi = np.minimum(a, b), np.maximum(a, b)
+        for ci in range(3):
+            for cj in range(3):
+                rows.append(3 * hi + ci)
+                cols.append(3 * lo + cj)
+                vals.append(-Bs[:, ci, cj])
+    diag += shift * np.eye(3)[None]
+    k = np.arange(nn)
+    for ci in range(3):
+        for cj in range(ci + 1):
+            rows.append(3 * k + ci)
+            cols.append(3 * k + cj)
+            vals.append(diag[:, ci, cj])
+    return _assemble_lower(3 * nn, np.concatenate(rows), np.concatenate(cols),
+                           np.concatenate(vals))
+
+
+def node_graph_lower(side=40):
+    """Pattern of the side^3 node grid with 27-point connectivity (lower CSC,
+    unit values): the graph the 3-unknown systems are ordered on."""
+    side = int(side)
+    nn = side ** 3
+    idx = np.arange(nn, dtype=np.int64).reshape(side, side, side)
+    rows, cols = [np.arange(nn)], [np.arange(nn)]
+    for dz, dy, dx in [(dz, dy, dx) for dz in (-1, 0, 1) for dy in (-1, 0, 1)
+                       for dx in (-1, 0, 1) if (dz, dy, dx) > (0, 0, 0)]:
+        sz = slice(max(0, -dz), side - max(0, dz))
+        sy = slice(max(0, -dy), side - max(0, dy))
+        sx = slice(max(0, -dx), side - max(0, dx))
+        a = idx[sz, sy, sx].ravel()
+        b = idx[sz.start + dz:sz.stop + dz, sy.start + dy:sy.stop + dy,
+                sx.start + dx:sx.stop + dx].ravel()
+        rows.append(np.maximum(a, b))
+        cols.append(np.minimum(a, b))
+    r, c = np.concatenate(rows), np.concatenate(cols)
+    return _assemble_lower(nn, r, c, np.ones(r.size))
+
+
+def expand_node_perm(perm, dof=3):
+    """A node permutation (new -> old) as one of the node's unknowns."""
+    perm = np.asarray(perm, dtype=np.int64)
+    return (dof * perm[:, None] + np.arange(dof)[None, :]).ravel().astype(np.int32)
+
+
+def permute_lower(n, Ap, Ai, Ax, perm):
+    """Lower CSC of P A P' (perm: new -> old) from the lower CSC of A."""
+    perm = np.asarray(perm, dtype=np.int64)
+    inv = np.empty(n, dtype=np.int64)
+    inv[perm] = np.arange(n)
+    cols = np.repeat(np.arange(n), np.diff(Ap))
+    r, c = inv[np.asarray(Ai, dtype=np.int64)], inv[cols]
+    return _assemble_lower(n, np.maximum(r, c), np.minimum(r, c), np.asarray(Ax, dtype=np.float64))
