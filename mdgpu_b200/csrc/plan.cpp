@@ -189,40 +189,42 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
     int nnz = A.nnz();
     P.a_src.resize(nnz);
     P.a_pos.resize(nnz);
-    std::vector<int> last_at;  // per local position of the current front
-    for (int s = 0; s < ns; ++s) {
-        const FrontDesc& f = P.fronts[s];
-        const int* r = P.rows.data() + f.rows_off;
-        for (int jj = 0; jj < f.c; ++jj) {
-            int j = f.first_col + jj;
-            for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p) {
-                int row = A.rowidx[p];
-                int pos = (int)(std::lower_bound(r, r + f.m, row) - r);
-                if (pos >= f.m || r[pos] != row) throw std::runtime_error("A entry outside front");
-                if (f.m >= 65536) throw std::runtime_error("front too large for packed A map");
-                P.a_src[p] = S.lower_src[p];
-                P.a_pos[p] = pos | (jj << 16);
-            }
-        }
-        // duplicates: keep the last in storage order
-        bool dup = false;
-        for (int jj = 0; jj < f.c && !dup; ++jj) {
-            int j = f.first_col + jj;
-            for (int p = A.colptr[j] + 1; p < A.colptr[j + 1]; ++p)
-                if (A.rowidx[p] <= A.rowidx[p - 1]) dup = true;
-        }
-        if (dup) {
+    for_each_range(ranges, [&](int s0, int s1) {
+        for (int s = s0; s < s1; ++s) {
+            const FrontDesc& f = P.fronts[s];
+            const int* r = P.rows.data() + f.rows_off;
             for (int jj = 0; jj < f.c; ++jj) {
                 int j = f.first_col + jj;
-                for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
-                    for (int q = p + 1; q < A.colptr[j + 1]; ++q)
-                        if (A.rowidx[q] == A.rowidx[p]) {
-                            P.a_src[p] = -1;
-                            break;
-                        }
+                for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p) {
+                    int row = A.rowidx[p];
+                    int pos = (int)(std::lower_bound(r, r + f.m, row) - r);
+                    if (pos >= f.m || r[pos] != row)
+                        throw std::runtime_error("A entry outside front");
+                    if (f.m >= 65536) throw std::runtime_error("front too large for packed A map");
+                    P.a_src[p] = S.lower_src[p];
+                    P.a_pos[p] = pos | (jj << 16);
+                }
+            }
+            // duplicates: keep the last in storage order
+            bool dup = false;
+            for (int jj = 0; jj < f.c && !dup; ++jj) {
+                int j = f.first_col + jj;
+                for (int p = A.colptr[j] + 1; p < A.colptr[j + 1]; ++p)
+                    if (A.rowidx[p] <= A.rowidx[p - 1]) dup = true;
+            }
+            if (dup) {
+                for (int jj = 0; jj < f.c; ++jj) {
+                    int j = f.first_col + jj;
+                    for (int p = A.colptr[j]; p < A.colptr[j + 1]; ++p)
+                        for (int q = p + 1; q < A.colptr[j + 1]; ++q)
+                            if (A.rowidx[q] == A.rowidx[p]) {
+                                P.a_src[p] = -1;
+                                break;
+                            }
+                }
             }
         }
-    }
+    });
 
     // levels
     std::vector<int> level(ns, 0);
@@ -402,18 +404,28 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
     }
-    S.warp_list.clear();
+    S.warp_list.assign(P.small_list.size(), 0);
     S.warp_cnt.assign(3 * (size_t)P.nlevels, 0);
-    for (int l = 0; l < P.nlevels; ++l) {
-        const int b = P.small_ptr[l * kSmallBuckets], e = P.small_ptr[(l + 1) * kSmallBuckets];
-        std::vector<int> w(P.small_list.begin() + b, P.small_list.begin() + e);
-        std::stable_sort(w.begin(), w.end(),
-                         [&](int x, int y) { return P.fronts[x].m > P.fronts[y].m; });
-        for (int s : w) {
-            const int m = P.fronts[s].m;
-            S.warp_cnt[3 * l + (m > 16 ? 0 : (m > 8 ? 1 : 2))]++;
+    {
+        // per level a stable counting sort of the small fronts by rows,
+        // descending (small fronts have at most kSmallMaxRows rows)
+        constexpr int MX = Plan::kSmallMaxRows;
+        std::vector<int> at(MX + 2);
+        for (int l = 0; l < P.nlevels; ++l) {
+            const int b = P.small_ptr[l * kSmallBuckets], e = P.small_ptr[(l + 1) * kSmallBuckets];
+            std::fill(at.begin(), at.end(), 0);
+            for (int q = b; q < e; ++q) {
+                const int m = P.fronts[P.small_list[q]].m;
+                if (m < 1 || m > MX) throw std::runtime_error("small front of unexpected size");
+                at[MX - m + 1]++;  // slot of m: fronts with more rows first
+                S.warp_cnt[3 * l + (m > 16 ? 0 : (m > 8 ? 1 : 2))]++;
+            }
+            for (int k = 0; k <= MX; ++k) at[k + 1] += at[k];
+            for (int q = b; q < e; ++q) {
+                const int s = P.small_list[q];
+                S.warp_list[b + at[MX - P.fronts[s].m]++] = s;
+            }
         }
-        S.warp_list.insert(S.warp_list.end(), w.begin(), w.end());
     }
     S.fv_off.assign(P.nsuper, 0);
     S.fv_rows = 0;
