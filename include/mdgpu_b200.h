@@ -183,6 +183,27 @@ MDGPU_API int mdgpu_refine_device(mdgpu_handle h, const double *dB, int ldb, dou
                         double tol, int maxit, double *berr, int *iters, void *stream);
 
 /*
+ * Solve with GMRES-based iterative refinement (GMRES-IR; no counterpart in the
+ * reference): x = M^-1 b, then while the backward error (as for
+ * mdgpu_refine) is above tol and fewer than maxit corrections were made,
+ * r = b - A x with the caller's FP64 values and the correction d solves
+ * M^-1 A d = M^-1 r by GMRES in FP64 from d = 0 (at most `restart` steps,
+ * 1..64; stop when the preconditioned residual is inner_tol times its start),
+ * x += d.  M^-1 is the solve with the current factor (FP32 or FP64).  Plain
+ * refinement needs cond(A) u_factor < 1; GMRES-IR converges for cond(A) up to
+ * about u_factor^-2.  Right-hand sides are refined one after another.
+ * berr[nrhs], iters[nrhs] (corrections) and inner[nrhs] (GMRES steps, one
+ * factor solve and one product with A each) are optional outputs.  Device
+ * memory: (restart + 2) n doubles, kept with the handle.
+ */
+MDGPU_API int mdgpu_gmres_ir(mdgpu_handle h, const double *B, int ldb, double *X, int ldx, int nrhs,
+                             double tol, int maxit, int restart, double inner_tol, double *berr,
+                             int *iters, int *inner, void *stream);
+MDGPU_API int mdgpu_gmres_ir_device(mdgpu_handle h, const double *dB, int ldb, double *dX, int ldx,
+                                    int nrhs, double tol, int maxit, int restart, double inner_tol,
+                                    double *berr, int *iters, int *inner, void *stream);
+
+/*
  * Differentiation (no counterpart in the reference, whose driver only
  * factors and solves).  mdgpu_logdet: log det A = 2 sum log L(j, j) of the
  * current factor (FP64 or FP32).  mdgpu_selinv: the selected inverse

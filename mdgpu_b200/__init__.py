@@ -27,7 +27,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
 EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
            "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
-           "mdgpu_refine_device",
+           "mdgpu_refine_device", "mdgpu_gmres_ir", "mdgpu_gmres_ir_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
            "mdgpu_last_error", "mdgpu_load_triplet", "mdgpu_logdet", "mdgpu_selinv",
            "mdgpu_grad_lower", "mdgpu_grad_lower_device")
@@ -85,6 +85,9 @@ def lib():
         L.mdgpu_refine.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, C.c_double, C.c_int,
                                    dp, vp, vp]
         L.mdgpu_refine_device.argtypes = L.mdgpu_refine.argtypes
+        L.mdgpu_gmres_ir.argtypes = [vp, dp, C.c_int, dp, C.c_int, C.c_int, C.c_double, C.c_int,
+                                     C.c_int, C.c_double, dp, vp, vp, vp]
+        L.mdgpu_gmres_ir_device.argtypes = L.mdgpu_gmres_ir.argtypes
         L.mdgpu_get_L.argtypes = [vp, vp, vp, vp]
         L.mdgpu_profile.argtypes = [vp, C.c_int]
         L.mdgpu_profile_read.argtypes = [vp, C.c_int, vp, vp, vp, vp]
@@ -301,6 +304,42 @@ class Solver:
                                          float(tol), int(maxit), _ptr(berr), C.byref(it),
                                          stream))
         return berr, it.value
+
+    def gmres_ir(self, B, tol=1e-14, maxit=10, restart=30, inner_tol=1e-8, stream=None):
+        """Solve with GMRES-based iterative refinement (the factor's solve as
+        the preconditioner of GMRES in FP64); returns (x, berr, iters, inner)
+        with one backward error, correction count and GMRES step count per
+        right-hand side."""
+        B = np.asarray(B, dtype=np.float64)
+        one = B.ndim == 1
+        Bf = np.asfortranarray(B.reshape(self.n, -1))
+        X = np.zeros_like(Bf, order="F")
+        k = Bf.shape[1]
+        berr = np.zeros(k)
+        it = np.zeros(k, np.int32)
+        inner = np.zeros(k, np.int32)
+        _check(lib().mdgpu_gmres_ir(self._h, _ptr(Bf), self.n, _ptr(X), self.n, k, float(tol),
+                                    int(maxit), int(restart), float(inner_tol), _ptr(berr),
+                                    _ptr(it), _ptr(inner), stream))
+        if one:
+            return X[:, 0], berr[0], int(it[0]), int(inner[0])
+        return X, berr, it, inner
+
+    def gmres_ir_device(self, B, X, tol=1e-14, maxit=10, restart=30, inner_tol=1e-8,
+                        stream=None):
+        """GMRES-IR on CUDA tensors (column-major); returns (berr, iters, inner)."""
+        nrhs, ldb = self._device_layout(B)
+        nx, ldx = self._device_layout(X)
+        if nx != nrhs:
+            raise ValueError("B and X hold different numbers of right-hand sides")
+        berr = np.zeros(nrhs)
+        it = np.zeros(nrhs, np.int32)
+        inner = np.zeros(nrhs, np.int32)
+        _check(lib().mdgpu_gmres_ir_device(self._h, _tensor_ptr(B), ldb, _tensor_ptr(X), ldx,
+                                           nrhs, float(tol), int(maxit), int(restart),
+                                           float(inner_tol), _ptr(berr), _ptr(it), _ptr(inner),
+                                           stream))
+        return berr, it, inner
 
     def profile_step(self, fn):
         """Run fn() once with per-launch event timing on; return per-class

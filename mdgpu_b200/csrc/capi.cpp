@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "gmres_ir.hpp"
 #include "ir.hpp"
 #include "kernels.hpp"
 #include "mdgpu_b200.h"
@@ -109,6 +110,8 @@ struct mdgpu_handle_s {
     double* d_logdet = nullptr;    // logdet partial sums, then the result
     double* d_gx = nullptr;        // gradient: x and G on the device (host entry)
     double* d_gG = nullptr;
+    double* d_gm = nullptr;  // GMRES-IR basis, scratch vector, slots, partial sums
+    int64_t gm_cap = 0;      // its size in doubles
     int status_init[2] = {0, 0};
     int not_spd = -1;
     Profiler prof;
@@ -131,7 +134,8 @@ struct mdgpu_handle_s {
             if (g) cudaGraphExecDestroy(g);
         drop_solve_graphs();
         for (void* p : owned) cudaFree(p);
-        for (void* p : {(void*)dZ64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG})
+        for (void* p : {(void*)dZ64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG,
+                        (void*)d_gm})
             if (p) cudaFree(p);
         for (void* p : {(void*)d_Ax, (void*)dL64, (void*)dU64, (void*)dL32, (void*)dU32,
                         (void*)dD64, (void*)dD32,
@@ -569,6 +573,96 @@ int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
     return MDGPU_OK;
 }
 
+// GMRES-IR on the device: the vector backend of gmres_ir() over one
+// right-hand side; the preconditioner is the solve with the current factor.
+struct DeviceGmresOps {
+    mdgpu_handle_s* h;
+    cudaStream_t st;
+    int n, kmax;
+    double anorm;
+    double *V, *tmp, *slots, *coef, *partial;
+
+    double* basis(int k) { return V + (int64_t)k * n; }
+    double* scratch() { return tmp; }
+    void residual(const double* x, const double* b, double* r) {
+        launch_residual(h->csr, h->d_Ax, x, n, b, n, r, n, 1, st);
+    }
+    double backward_error(const double* r, const double* x, const double* b) {
+        launch_absmax3(n, 1, r, n, x, n, b, n, h->d_norms + 1, st);
+        unsigned long long raw[3];
+        ck(cudaMemcpyAsync(raw, h->d_norms + 1, sizeof(raw), cudaMemcpyDeviceToHost, st), "norms");
+        ck(cudaStreamSynchronize(st), "gmres-ir");
+        double nr, nx, nb;
+        std::memcpy(&nr, &raw[0], sizeof(double));
+        std::memcpy(&nx, &raw[1], sizeof(double));
+        std::memcpy(&nb, &raw[2], sizeof(double));
+        const double den = anorm * nx + nb;
+        return den > 0 ? nr / den : 0.0;
+    }
+    void precond(const double* r, double* z) { do_solve(h, r, n, z, n, 1, st); }
+    void spmv(const double* v, double* w) { launch_spmv(h->csr, h->d_Ax, v, w, st); }
+    void dots(int k, const double* w, int s) {
+        launch_dots(n, k, V, n, w, partial, slots + (int64_t)s * kmax, st);
+    }
+    void sub(int k, int s, double* w) {
+        launch_gemv_acc(n, k, V, n, slots + (int64_t)s * kmax, -1.0, w, st);
+    }
+    void norm2_to_slot(const double* w) {
+        launch_dots(n, 1, w, n, w, partial, slots + 2 * (int64_t)kmax, st);
+    }
+    void fetch(double* host) {
+        ck(cudaMemcpyAsync(host, slots, (2 * (size_t)kmax + 1) * sizeof(double),
+                           cudaMemcpyDeviceToHost, st),
+           "gmres slots");
+        ck(cudaStreamSynchronize(st), "gmres-ir");
+    }
+    void scale(double alpha, double* w) { launch_scale(n, alpha, w, st); }
+    void add(int k, const double* y, double* x) {
+        ck(cudaMemcpyAsync(coef, y, k * sizeof(double), cudaMemcpyHostToDevice, st), "gmres y");
+        launch_gemv_acc(n, k, V, n, coef, 1.0, x, st);
+    }
+};
+
+int do_gmres_ir(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
+                const GmresIrParams& prm, double* berr, int* outer, int* inner, cudaStream_t st) {
+    const int n = h->plan.n, kmax = prm.restart;
+    ensure_solve_storage(h, 1);
+    // basis (kmax + 1 vectors), one scratch vector, the slots (2 kmax + 1) and
+    // the correction's coefficients (kmax), the partial sums of the dots
+    const int64_t need = (int64_t)n * (kmax + 2) + 3 * (int64_t)kGmresMaxRestart + 1 +
+                         dots_partial_size(kGmresMaxRestart);
+    if (need > h->gm_cap) {
+        if (h->d_gm) cudaFree(h->d_gm);
+        h->d_gm = nullptr;
+        h->gm_cap = 0;
+        h->d_gm = dalloc<double>(need);
+        h->gm_cap = need;
+    }
+    DeviceGmresOps ops;
+    ops.h = h;
+    ops.st = st;
+    ops.n = n;
+    ops.kmax = kmax;
+    ops.V = h->d_gm;
+    ops.tmp = ops.V + (int64_t)n * (kmax + 1);
+    ops.slots = ops.tmp + n;
+    ops.coef = ops.slots + 2 * kGmresMaxRestart + 1;
+    ops.partial = ops.coef + kGmresMaxRestart;
+    launch_anorm(h->csr, h->d_Ax, h->d_norms, st);
+    unsigned long long raw;
+    ck(cudaMemcpyAsync(&raw, h->d_norms, sizeof(raw), cudaMemcpyDeviceToHost, st), "norm");
+    ck(cudaStreamSynchronize(st), "gmres-ir");
+    std::memcpy(&ops.anorm, &raw, sizeof(double));
+    for (int q = 0; q < nrhs; ++q) {
+        const GmresIrResult r =
+            gmres_ir(ops, dX + (int64_t)q * ldx, dB + (int64_t)q * ldb, prm);
+        if (berr) berr[q] = r.berr;
+        if (outer) outer[q] = r.outer;
+        if (inner) inner[q] = r.inner;
+    }
+    return MDGPU_OK;
+}
+
 // One symbolic result for independent systems: the block-diagonal matrix of
 // their lower triangles, each system analysed on its own (so each keeps its
 // own bit-exact ordering and tree); rows, supernodes, L columns and the
@@ -652,6 +746,15 @@ int solve_status_check(mdgpu_handle_s* h, cudaStream_t st) {
     if (e != 0)
         return fail(MDGPU_ERR_CUDA, "large-front solve aborted (status " + std::to_string(e) +
                                         "): a dependency wait ran out");
+    return MDGPU_OK;
+}
+
+// Argument check of the GMRES-IR entry points.
+int check_gmres_args(int maxit, int restart, double inner_tol) {
+    if (maxit < 0) return fail(MDGPU_ERR_INVALID, "maxit must be >= 0");
+    if (restart < 1 || restart > kGmresMaxRestart)
+        return fail(MDGPU_ERR_INVALID, "restart must be in 1..64");
+    if (!(inner_tol >= 0.0)) return fail(MDGPU_ERR_INVALID, "inner_tol must be >= 0");
     return MDGPU_OK;
 }
 
@@ -1072,6 +1175,50 @@ int mdgpu_refine(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, i
            "upload rhs");
         solve_status_reset(h, st);
         int rc = do_refine(h, h->d_B, n, h->d_X, n, nrhs, tol, maxit, berr, iters, st);
+        ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
+           "download solution");
+        int rs = solve_status_check(h, st);
+        return rs != MDGPU_OK ? rs : rc;
+    });
+}
+
+int mdgpu_gmres_ir_device(mdgpu_handle h, const double* dB, int ldb, double* dX, int ldx,
+                          int nrhs, double tol, int maxit, int restart, double inner_tol,
+                          double* berr, int* iters, int* inner, void* stream) {
+    if (int rc = check_solve_args(h, dB, ldb, dX, ldx, nrhs)) return rc;
+    if (int rc = check_gmres_args(maxit, restart, inner_tol)) return rc;
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        solve_status_reset(h, st);
+        const GmresIrParams prm{tol, maxit, restart, inner_tol};
+        int rc = do_gmres_ir(h, dB, ldb, dX, ldx, nrhs, prm, berr, iters, inner, st);
+        int rs = solve_status_check(h, st);
+        return rs != MDGPU_OK ? rs : rc;
+    });
+}
+
+int mdgpu_gmres_ir(mdgpu_handle h, const double* B, int ldb, double* X, int ldx, int nrhs,
+                   double tol, int maxit, int restart, double inner_tol, double* berr, int* iters,
+                   int* inner, void* stream) {
+    if (int rc = check_solve_args(h, B, ldb, X, ldx, nrhs)) return rc;
+    if (int rc = check_gmres_args(maxit, restart, inner_tol)) return rc;
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored < 0) return fail(MDGPU_ERR_STATE, "no valid factor");
+    return guarded([&] {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        ensure_solve_storage(h, nrhs);
+        const int n = h->plan.n;
+        ck(cudaMemcpy2DAsync(h->d_B, n * sizeof(double), B, ldb * sizeof(double),
+                             n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st),
+           "upload rhs");
+        solve_status_reset(h, st);
+        const GmresIrParams prm{tol, maxit, restart, inner_tol};
+        int rc = do_gmres_ir(h, h->d_B, n, h->d_X, n, nrhs, prm, berr, iters, inner, st);
         ck(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->d_X, n * sizeof(double),
                              n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st),
            "download solution");

@@ -207,3 +207,84 @@ def selected_inverse(n, Lp, Li, Lx):
         Z[j, R] = zr
         Z[j, j] = 1.0 / (d * d) - y @ zr
     return Z
+
+
+def gmres_ir(matvec, precond, b, anorm, tol=1e-14, maxit=10, restart=30, inner_tol=1e-10):
+    """GMRES-based iterative refinement, restated from Carson & Higham,
+    "Accelerating the solution of linear systems by iterative refinement in
+    three precisions", SIAM J. Sci. Comput. 40(2), A817-A847 (2018),
+    Algorithm 3.1, with the working and residual precisions both FP64:
+
+        x = M^-1 b
+        repeat: r = b - A x;  stop when ||r||inf / (anorm ||x||inf + ||b||inf)
+                <= tol or after maxit corrections;
+                solve M^-1 A d = M^-1 r by GMRES (zero start, at most
+                `restart` steps, stop when the preconditioned residual falls
+                to inner_tol times its start);  x += d
+
+    where M^-1 applies the low-precision factor.  The Arnoldi basis is
+    orthogonalised by classical Gram-Schmidt applied twice, the Hessenberg
+    matrix reduced by Givens rotations as it grows.  matvec(v) = A v and
+    precond(r) = M^-1 r take and return FP64 vectors.  Returns (x, berr
+    history, inner step counts).  TEST INFRASTRUCTURE ONLY."""
+    b = np.asarray(b, np.float64)
+    n = b.size
+    x = precond(b)
+    hist, inner = [], []
+    for outer in range(maxit + 1):
+        r = b - matvec(x)
+        den = anorm * np.abs(x).max() + np.abs(b).max()
+        be = np.abs(r).max() / den if den > 0 else 0.0
+        hist.append(be)
+        if be <= tol or outer == maxit:
+            break
+        z = precond(r)
+        beta = np.sqrt(z @ z)
+        if beta == 0.0:
+            break
+        V = np.zeros((n, restart + 1))
+        H = np.zeros((restart + 1, restart))
+        cs, sn = np.zeros(restart), np.zeros(restart)
+        g = np.zeros(restart + 1)
+        g[0] = beta
+        V[:, 0] = z / beta
+        k = 0
+        for j in range(restart):
+            w = precond(matvec(V[:, j]))
+            h1 = V[:, :j + 1].T @ w
+            w = w - V[:, :j + 1] @ h1
+            h2 = V[:, :j + 1].T @ w
+            w = w - V[:, :j + 1] @ h2
+            H[:j + 1, j] = h1 + h2
+            hn = np.sqrt(w @ w)
+            H[j + 1, j] = hn
+            for i in range(j):
+                t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                H[i, j] = t
+            den2 = np.hypot(H[j, j], H[j + 1, j])
+            cs[j], sn[j] = H[j, j] / den2, H[j + 1, j] / den2
+            H[j, j] = den2
+            H[j + 1, j] = 0.0
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            k = j + 1
+            if abs(g[j + 1]) <= inner_tol * beta or hn == 0.0:
+                break
+            V[:, j + 1] = w / hn
+        y = np.zeros(k)
+        for i in range(k - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1:k] @ y[i + 1:k]) / H[i, i]
+        x = x + V[:, :k] @ y
+        inner.append(k)
+    return x, hist, inner
+
+
+def round_bf16(a):
+    """Round FP64 values to the nearest BF16 (8 significant bits, ties to
+    even), returned as FP64: the factor a BF16 tensor-core path would keep.
+    TEST INFRASTRUCTURE ONLY."""
+    u = np.asarray(a, np.float32).copy().view(np.uint32)
+    u += np.uint32(0x7FFF) + ((u >> np.uint32(16)) & np.uint32(1))
+    u &= np.uint32(0xFFFF0000)
+    return u.view(np.float32).astype(np.float64)
