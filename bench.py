@@ -71,9 +71,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-rhs64", action="store_true",
                     help="skip the 64-right-hand-side measurement")
-    ap.add_argument("--workload", choices=["grid3d", "batch", "adjoint"], default="grid3d",
+    ap.add_argument("--workload", choices=["grid3d", "batch", "adjoint", "elasticity"],
+                    default="grid3d",
                     help="batch: 1024 independent systems (512 2D, 512 3D) under one handle; "
-                         "adjoint: gradient of log det A + b'A^-1 b on the 48^3 grid")
+                         "adjoint: gradient of log det A + b'A^-1 b on the 48^3 grid; "
+                         "elasticity: 3 unknowns per node on a 40^3 27-point node grid, "
+                         "FP32 factor + GMRES-IR vs + plain refinement vs FP64")
     return ap.parse_args()
 
 
@@ -607,6 +610,90 @@ def run_adjoint_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_elasticity_arm(args):
+    """The multi-unknown system: 3 unknowns per node of a 40^3 node grid with
+    27-point connectivity (n = 192000), blocks w (I + 0.5 e e'), w
+    lognormal(0, 1), shift 1e-2, AMD on the node graph expanded to the
+    unknowns.  One step = factor + solve to backward error 1e-14 of one
+    right-hand side: FP32 factor + GMRES-IR, FP32 factor + plain refinement,
+    FP64 factor + solve."""
+    import torch
+
+    import mdgpu_b200 as M
+    from mdgpu_b200 import matgen as mg
+
+    side = 40
+    n, Ap, Ai, Ax = mg.elasticity_3dof(side, seed=0, sigma=1.0, shift=1e-2)
+    nn, gp, gi, _ = mg.node_graph_lower(side)
+    perm = mg.expand_node_perm(M.Solver(nn, gp, gi, ordering=M.ORDER_AMD).array("perm"))
+    n, Ap, Ai, Ax = mg.permute_lower(n, Ap, Ai, Ax, perm)
+    t0 = time.perf_counter()
+    S = M.Solver(n, Ap, Ai, ordering=M.ORDER_NATURAL)
+    t_an = time.perf_counter() - t0
+    flops = float(S.info("flops"))
+    b = mg.rhs_uniform(n, seed=1)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    dAx = torch.from_numpy(Ax).cuda()
+    dB = torch.from_numpy(b).cuda()
+    dX = torch.empty(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        ts, extra = [], None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            extra = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts), extra
+
+    def step_gmres():
+        S.factor(dAx, M.FP32, stream=sptr)
+        return S.gmres_ir_device(dB, dX, tol=1e-14, maxit=10, stream=sptr)
+
+    def step_ir():
+        S.factor(dAx, M.FP32, stream=sptr)
+        return S.refine_device(dB, dX, tol=1e-14, maxit=30, stream=sptr)
+
+    def step64():
+        S.factor(dAx, M.FP64, stream=sptr)
+        return S.refine_device(dB, dX, tol=1e-14, maxit=0, stream=sptr)
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    ms_g, (be_g, it_g, in_g) = timed(step_gmres, args.steps, args.warmup)
+    clocks = sampler.stop()
+    ms_ir, (be_ir, it_ir) = timed(step_ir, max(1, min(args.steps, 3)), 1)
+    ms64, (be64, _) = timed(step64, max(1, min(args.steps, 3)), 1)
+    line = {"metric": METRIC, "value": flops / (ms_g * 1e-3) / 1e9, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_g,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 factor (tf32 tensor-core Schur) + f64 GMRES-IR", "data": "synthetic",
+            "config": {"workload": "3 unknowns per node, 40^3 node grid, 27-point, blocks "
+                                   "w(I+0.5ee'), w lognormal(0,1), shift 1e-2, node-graph AMD, "
+                                   "1 RHS U(-1,1)",
+                       "n": n, "nsuper": S.info("nsuper"), "lnz": S.info("lnz"),
+                       "flops_per_step": flops, "analyze_s": t_an,
+                       "l2": "flushed between steps (256 MiB write)"},
+            "backward_error": float(np.max(be_g)), "corrections": int(np.max(it_g)),
+            "gmres_steps": int(np.sum(in_g)),
+            "fp32_plain_ir": {"ms_per_step": ms_ir, "backward_error": float(np.max(be_ir)),
+                              "corrections": int(it_ir)},
+            "fp64": {"ms_per_step": ms64, "value": flops / (ms64 * 1e-3) / 1e9,
+                     "backward_error": float(np.max(be64)),
+                     "speedup_fp32_gmres_ir_over_fp64": ms64 / ms_g},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "batch" and args.impl != "reference":
@@ -614,6 +701,9 @@ def main():
         return
     if args.workload == "adjoint" and args.impl != "reference":
         run_adjoint_arm(args)
+        return
+    if args.workload == "elasticity" and args.impl != "reference":
+        run_elasticity_arm(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)
