@@ -93,6 +93,16 @@ MDGPU_API int mdgpu_analyze_batch(int nsys, const int *n, const int *const *Ap,
                                   mdgpu_handle *out);
 
 /*
+ * Cost estimate of independent systems without a handle or a device (no
+ * counterpart in the reference): the same symbolic analysis as
+ * mdgpu_analyze_batch for each system (on all host cores), reduced to its
+ * flop count (as mdgpu_info "flops") in flops[nsys] and its L entries in
+ * lnz[nsys] (optional).  For partitioning systems across GPUs.
+ */
+MDGPU_API int mdgpu_estimate_batch(int nsys, const int *n, const int *const *Ap,
+                                   const int *const *Ai, int ordering, int tree, int relax_zeros,
+                                   double *flops, long long *lnz);
+/*
  * Analysis from an already permuted lower triangle and a given assembly tree,
  * the inputs of the reference's Factor(cs *A, cs *spL, ETree **listaNodos,
  * int cantNodos) (mdgpu.cu:1394): supernode s eliminates columns

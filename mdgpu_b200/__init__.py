@@ -25,7 +25,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
 
 # every entry point declared in include/mdgpu_b200.h
 EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
-           "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
+           "mdgpu_estimate_batch", "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
            "mdgpu_refine_device", "mdgpu_gmres_ir", "mdgpu_gmres_ir_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
@@ -72,6 +72,8 @@ def lib():
                                          C.POINTER(vp)]
         L.mdgpu_analyze_batch.argtypes = [C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.c_int,
                                           C.c_int, C.c_int, C.POINTER(vp)]
+        L.mdgpu_estimate_batch.argtypes = [C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.c_int,
+                                           C.c_int, C.c_int, dp, vp]
         L.mdgpu_destroy.argtypes = [vp]
         L.mdgpu_destroy.restype = None
         L.mdgpu_info.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
@@ -141,6 +143,23 @@ def load_triplet(path, matrix_market=False):
     _check(L.mdgpu_load_triplet(p, fmt, C.byref(m), C.byref(n), C.byref(nnz), _ptr(Ap), _ptr(Ai),
                                 _ptr(Ax)))
     return m.value, n.value, Ap, Ai[: nnz.value], Ax[: nnz.value]
+
+
+def estimate_batch(systems, ordering=ORDER_AMD, tree=TREE_SUPER, relax_zeros=0):
+    """Flop count and L entries of each of the independent systems
+    [(n, Ap, Ai), ...] from their symbolic analyses (host only, all cores);
+    returns (flops, lnz) arrays."""
+    ns = len(systems)
+    nn = np.array([int(s[0]) for s in systems], dtype=np.int32)
+    Aps = [np.ascontiguousarray(s[1], dtype=np.int32) for s in systems]
+    Ais = [np.ascontiguousarray(s[2], dtype=np.int32) for s in systems]
+    pa = (C.c_void_p * ns)(*[a.ctypes.data for a in Aps])
+    pi = (C.c_void_p * ns)(*[a.ctypes.data for a in Ais])
+    flops = np.zeros(ns)
+    lnz = np.zeros(ns, np.int64)
+    _check(lib().mdgpu_estimate_batch(ns, _ptr(nn), pa, pi, int(ordering), int(tree),
+                                      int(relax_zeros), _ptr(flops), _ptr(lnz)))
+    return flops, lnz
 
 
 class Solver:

@@ -749,6 +749,82 @@ int solve_status_check(mdgpu_handle_s* h, cudaStream_t st) {
     return MDGPU_OK;
 }
 
+// Validation and symbolic analysis of independent systems, shared by the
+// batch analysis and the cost estimate.  The analyses are independent: one
+// host thread per core, systems taken in order from a shared counter; the
+// first failing system (lowest index) is reported.  With offsets, row_off /
+// val_off receive the systems' first row and first value in the
+// concatenation (32-bit, checked); given flops, each system's analysis is
+// reduced to its flop count (sum over columns of count^2 + 1, as the plan's)
+// and its L entries (lnz, optional), then dropped, and parts stays empty.
+int analyze_systems(int nsys, const int* n, const int* const* Ap, const int* const* Ai,
+                    int ordering, int tree, int relax_zeros, bool offsets,
+                    std::vector<Symbolic>& parts, std::vector<int>& row_off,
+                    std::vector<int>& val_off, double* flops, long long* lnz) {
+    row_off.assign(nsys + 1, 0);
+    val_off.assign(nsys + 1, 0);
+    for (int b = 0; b < nsys; ++b) {
+        const int nb = n[b];
+        if (nb <= 0 || !Ap[b] || !Ai[b])
+            return fail(MDGPU_ERR_INVALID, "bad arguments of system " + std::to_string(b));
+        for (int j = 0; j < nb; ++j) {
+            if (Ap[b][j + 1] < Ap[b][j])
+                return fail(MDGPU_ERR_INVALID,
+                            "column pointers decrease in system " + std::to_string(b));
+            for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p)
+                if (Ai[b][p] < j || Ai[b][p] >= nb)
+                    return fail(MDGPU_ERR_INVALID,
+                                "entry outside the lower triangle in system " + std::to_string(b));
+        }
+        if (offsets) {
+            if ((int64_t)row_off[b] + nb > INT_MAX || (int64_t)val_off[b] + Ap[b][nb] > INT_MAX)
+                return fail(MDGPU_ERR_INVALID, "batch too large for 32-bit indices");
+            row_off[b + 1] = row_off[b] + nb;
+            val_off[b + 1] = val_off[b] + Ap[b][nb];
+        }
+    }
+    const bool keep = flops == nullptr;
+    std::vector<int> rc(nsys, 0);
+    std::vector<std::string> what(nsys);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        Symbolic one;
+        for (int b = next.fetch_add(1); b < nsys; b = next.fetch_add(1)) {
+            Symbolic& S = keep ? parts[b] : one;
+            try {
+                rc[b] = analyze(n[b], Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD,
+                                (TreeKind)tree, relax_zeros, S) != 0
+                            ? 1
+                            : 0;
+                if (!keep && rc[b] == 0) {
+                    double f = 0.0;
+                    for (int j = 0; j < n[b]; ++j) f += (double)S.count[j] * S.count[j] + 1.0;
+                    flops[b] = f;
+                    if (lnz) lnz[b] = (long long)S.Lp[n[b]];
+                }
+            } catch (const std::bad_alloc&) {
+                rc[b] = 2;
+            } catch (const std::exception& e) {
+                rc[b] = 3;
+                what[b] = e.what();
+            }
+        }
+    };
+    const int nthr = std::max(1, std::min<int>(nsys, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (int b = 0; b < nsys; ++b) {
+        if (rc[b] == 1)
+            return fail(MDGPU_ERR_NOT_TREE,
+                        "the elimination tree of system " + std::to_string(b) + " is a forest");
+        if (rc[b] == 2) throw std::bad_alloc();
+        if (rc[b] == 3) throw std::runtime_error("system " + std::to_string(b) + ": " + what[b]);
+    }
+    return MDGPU_OK;
+}
+
 // Argument check of the GMRES-IR entry points.
 int check_gmres_args(int maxit, int restart, double inner_tol) {
     if (maxit < 0) return fail(MDGPU_ERR_INVALID, "maxit must be >= 0");
@@ -885,6 +961,20 @@ int mdgpu_load_triplet(const char* path, int format, int* m, int* n, int* nnz, i
     });
 }
 
+int mdgpu_estimate_batch(int nsys, const int* n, const int* const* Ap, const int* const* Ai,
+                         int ordering, int tree, int relax_zeros, double* flops,
+                         long long* lnz) {
+    if (nsys <= 0 || !n || !Ap || !Ai || !flops) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (tree < 0 || tree > 2 || ordering < 0 || ordering > 1)
+        return fail(MDGPU_ERR_INVALID, "bad ordering or tree kind");
+    return guarded([&]() -> int {
+        std::vector<Symbolic> parts;
+        std::vector<int> row_off, val_off;
+        return analyze_systems(nsys, n, Ap, Ai, ordering, tree, relax_zeros, false, parts,
+                               row_off, val_off, flops, lnz);
+    });
+}
+
 int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int* const* Ai,
                         int ordering, int tree, int relax_zeros, mdgpu_handle* out) {
     if (!out || nsys <= 0 || !n || !Ap || !Ai) return fail(MDGPU_ERR_INVALID, "bad arguments");
@@ -893,58 +983,10 @@ int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int*
     *out = nullptr;
     return guarded([&]() -> int {
         std::vector<Symbolic> parts(nsys);
-        std::vector<int> row_off(nsys + 1, 0), val_off(nsys + 1, 0);
-        for (int b = 0; b < nsys; ++b) {
-            const int nb = n[b];
-            if (nb <= 0 || !Ap[b] || !Ai[b])
-                return fail(MDGPU_ERR_INVALID, "bad arguments of system " + std::to_string(b));
-            for (int j = 0; j < nb; ++j) {
-                if (Ap[b][j + 1] < Ap[b][j])
-                    return fail(MDGPU_ERR_INVALID,
-                                "column pointers decrease in system " + std::to_string(b));
-                for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p)
-                    if (Ai[b][p] < j || Ai[b][p] >= nb)
-                        return fail(MDGPU_ERR_INVALID, "entry outside the lower triangle in system " +
-                                                           std::to_string(b));
-            }
-            if ((int64_t)row_off[b] + nb > INT_MAX || (int64_t)val_off[b] + Ap[b][nb] > INT_MAX)
-                return fail(MDGPU_ERR_INVALID, "batch too large for 32-bit indices");
-            row_off[b + 1] = row_off[b] + nb;
-            val_off[b + 1] = val_off[b] + Ap[b][nb];
-        }
-        // the systems' analyses are independent: one host thread per core,
-        // systems taken in order from a shared counter; the first failing
-        // system (lowest index) is reported
-        std::vector<int> rc(nsys, 0);
-        std::vector<std::string> what(nsys);
-        std::atomic<int> next{0};
-        auto work = [&]() {
-            for (int b = next.fetch_add(1); b < nsys; b = next.fetch_add(1)) {
-                try {
-                    rc[b] = analyze(n[b], Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD,
-                                    (TreeKind)tree, relax_zeros, parts[b]) != 0
-                                ? 1
-                                : 0;
-                } catch (const std::bad_alloc&) {
-                    rc[b] = 2;
-                } catch (const std::exception& e) {
-                    rc[b] = 3;
-                    what[b] = e.what();
-                }
-            }
-        };
-        const int nthr = std::max(1, std::min<int>(nsys, (int)std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
-        work();
-        for (auto& t : pool) t.join();
-        for (int b = 0; b < nsys; ++b) {
-            if (rc[b] == 1)
-                return fail(MDGPU_ERR_NOT_TREE,
-                            "the elimination tree of system " + std::to_string(b) + " is a forest");
-            if (rc[b] == 2) throw std::bad_alloc();
-            if (rc[b] == 3) throw std::runtime_error("system " + std::to_string(b) + ": " + what[b]);
-        }
+        std::vector<int> row_off, val_off;
+        if (int rc = analyze_systems(nsys, n, Ap, Ai, ordering, tree, relax_zeros, true, parts,
+                                     row_off, val_off, nullptr, nullptr))
+            return rc;
         auto* h = new mdgpu_handle_s();
         try {
             combine_symbolic(parts, val_off, h->sym);
