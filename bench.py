@@ -269,9 +269,13 @@ def run_gpu_arm(args):
 
     side = args.side
     n, Ap, Ai, Ax, b = workload(side)
+    # device memory the handle holds: driver-level free memory before and
+    # after each stage (the library allocates with cudaMalloc, outside torch)
+    free_a, _ = torch.cuda.mem_get_info()
     t0 = time.perf_counter()
     S = M.Solver(n, Ap, Ai)
     t_analyze = time.perf_counter() - t0
+    free_b, _ = torch.cuda.mem_get_info()
     flops = float(S.info("flops"))
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -315,11 +319,20 @@ def run_gpu_arm(args):
             dist.destroy_process_group()
         return
 
+    free_c, _ = torch.cuda.mem_get_info()
     sampler = ClockSampler(local)
     sampler.start()
     t32, (berr32, it32) = timed(step_fp32, args.steps, args.warmup)
     clocks = sampler.stop()
+    free_d, _ = torch.cuda.mem_get_info()
     t64, (berr64, _) = timed(step_fp64, max(1, min(args.steps, 3)), 1)
+    free_e, _ = torch.cuda.mem_get_info()
+    hbm = {"plan": int(free_a - free_b), "fp32_factor_and_solve": int(free_c - free_d),
+           "fp64_factor_added": int(free_d - free_e),
+           "handle_total": int((free_a - free_b) + (free_c - free_e)),
+           "lstore_bytes_fp64": int(S.info("lstore_bytes")),
+           "ustore_bytes_fp64": int(S.info("ustore_bytes")),
+           "note": "cudaMemGetInfo deltas (2 MiB granularity)"}
     ms32 = allmax(statistics.mean(t32))
     ms64 = allmax(statistics.mean(t64))
 
@@ -386,6 +399,7 @@ def run_gpu_arm(args):
                 "h2d_bytes_per_step": int(Ax.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes)},
         "rhs64": rhs64,
+        "hbm_bytes": hbm,
         "gpu_launches": prof["launches_per_step"],
         "clocks": clocks,
         "roofline": None,
