@@ -1,6 +1,7 @@
 // C ABI implementation (include/mdgpu_b200.h): symbolic on the host, plan
 // resident on the device, numeric factor / solve / refinement on the GPU.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -26,6 +27,17 @@ using namespace mdgpu;
 namespace {
 
 thread_local std::string g_last_error;
+
+// An NVTX range over one API-level phase (factor, solve, refinement, ...),
+// so a profiler can select a phase's kernels by name (ncu --nvtx
+// --nvtx-include "mdgpu_factor/").  Header-only NVTX: without a tool
+// attached each call returns at once.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct CudaError : std::runtime_error {
     cudaError_t code;
@@ -461,6 +473,7 @@ void ensure_solve_storage(mdgpu_handle_s* h, int nrhs) {
 }
 
 int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
+    NvtxRange nvtx("mdgpu_factor");
     if (precision != MDGPU_FP64 && precision != MDGPU_FP32)
         return fail(MDGPU_ERR_INVALID, "unknown precision");
     ck(cudaSetDevice(h->device), "cudaSetDevice");
@@ -512,6 +525,7 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
 // dB, dX device, original ordering; chunks of at most 64 right-hand sides
 void do_solve(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
               cudaStream_t st) {
+    NvtxRange nvtx("mdgpu_solve");
     const int n = h->plan.n;
     for (int q0 = 0; q0 < nrhs; q0 += 64) {
         int nq = std::min(64, nrhs - q0);
@@ -537,6 +551,7 @@ void do_solve(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
 
 int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
               double tol, int maxit, double* berr, int* iters, cudaStream_t st) {
+    NvtxRange nvtx("mdgpu_refine");
     const int n = h->plan.n;
     ensure_solve_storage(h, nrhs);
     launch_anorm(h->csr, h->d_Ax, h->d_norms, st);
@@ -625,6 +640,7 @@ struct DeviceGmresOps {
 
 int do_gmres_ir(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx, int nrhs,
                 const GmresIrParams& prm, double* berr, int* outer, int* inner, cudaStream_t st) {
+    NvtxRange nvtx("mdgpu_gmres_ir");
     const int n = h->plan.n, kmax = prm.restart;
     ensure_solve_storage(h, 1);
     // basis (kmax + 1 vectors), one scratch vector, the slots (2 kmax + 1) and
@@ -1298,6 +1314,7 @@ int mdgpu_selinv(mdgpu_handle h, void* stream) {
         ck(cudaSetDevice(h->device), "cudaSetDevice");
         if (!h->dZ64) h->dZ64 = dalloc<double>(h->plan.lstore);
         if (!h->d_Y) h->d_Y = dalloc<double>(std::max<int64_t>(h->D.yscr_total, 1));
+        NvtxRange nvtx("mdgpu_selinv");
         launch_selinv(h->D, h->dL64, h->dZ64, h->dU64, h->d_Y, st);
         ck(cudaGetLastError(), "selected inverse launch");
         ck(cudaStreamSynchronize(st), "selected inverse");
