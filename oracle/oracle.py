@@ -288,3 +288,33 @@ def round_bf16(a):
     u += np.uint32(0x7FFF) + ((u >> np.uint32(16)) & np.uint32(1))
     u &= np.uint32(0xFFFF0000)
     return u.view(np.float32).astype(np.float64)
+
+
+def bf16_update_cholesky(A, nb=64, pow2_scale=False):
+    """Dense right-looking blocked Cholesky in FP32 whose trailing (Schur)
+    updates take their operands rounded to BF16 and accumulate in FP32 -- the
+    arithmetic of a BF16 tensor-core Schur update (A22 -= L21 L21' with BF16
+    inputs, FP32 accumulators); the diagonal-block factor and the panel solve
+    stay in FP32.  pow2_scale: before rounding, each panel is multiplied by
+    the power of two that brings its largest magnitude into [1, 2) and the
+    product is scaled back (per-front power-of-two scaling).  Returns the
+    lower factor in FP64.  TEST INFRASTRUCTURE ONLY."""
+    import scipy.linalg as sl
+
+    W = np.array(A, dtype=np.float32)
+    n = W.shape[0]
+    for k in range(0, n, nb):
+        e = min(k + nb, n)
+        L11 = np.linalg.cholesky(W[k:e, k:e].astype(np.float64)).astype(np.float32)
+        W[k:e, k:e] = L11
+        if e < n:
+            L21 = sl.solve_triangular(L11, W[e:, k:e].T, lower=True).T.astype(np.float32)
+            W[e:, k:e] = L21
+            s = 1.0
+            if pow2_scale:
+                mx = float(np.abs(L21).max())
+                if mx > 0:
+                    s = 2.0 ** -np.floor(np.log2(mx))
+            Q = (round_bf16(L21 * np.float32(s))).astype(np.float32)
+            W[e:, e:] -= (Q @ Q.T) * np.float32(1.0 / (s * s))
+    return np.tril(W).astype(np.float64)
