@@ -190,13 +190,14 @@ def test_gmres_ir_on_the_multi_unknown_system(precision):
     B = np.random.default_rng(5).uniform(-1, 1, (n, 3))
     X, berr, it, inner = S.gmres_ir(B, tol=1e-14, maxit=10)
     Xe = np.linalg.solve(A, B)
+    # forward error <= cond(A) (~2e4) x backward error (<= 1e-14)
     for q in range(3):
         assert berr[q] <= 1e-14 and it[q] <= 3, (berr, it, inner)
         assert _berr(A, X[:, q], B[:, q]) <= 2e-14
-        assert np.abs(X[:, q] - Xe[:, q]).max() <= 1e-11 * np.abs(Xe[:, q]).max()
+        assert np.abs(X[:, q] - Xe[:, q]).max() <= 1e-9 * np.abs(Xe[:, q]).max()
     # a single right-hand side, and device buffers with a leading dimension > n
     x1, b1, i1, k1 = S.gmres_ir(B[:, 1])
-    assert b1 <= 1e-14 and np.abs(x1 - Xe[:, 1]).max() <= 1e-11 * np.abs(Xe[:, 1]).max()
+    assert b1 <= 1e-14 and np.abs(x1 - Xe[:, 1]).max() <= 1e-9 * np.abs(Xe[:, 1]).max()
     ld = n + 3
     dB = torch.zeros((3, ld), dtype=torch.float64, device="cuda")
     dB[:, :n] = torch.from_numpy(B.T.copy()).cuda()
@@ -204,7 +205,7 @@ def test_gmres_ir_on_the_multi_unknown_system(precision):
     berr_d, it_d, inner_d = S.gmres_ir_device(dB[:, :n].t(), dX[:, :n].t())
     Xd = dX[:, :n].cpu().numpy().T
     assert np.all(berr_d <= 1e-14)
-    assert np.abs(Xd - Xe).max() <= 1e-11 * np.abs(Xe).max()
+    assert np.abs(Xd - Xe).max() <= 1e-9 * np.abs(Xe).max()
     assert torch.all(dX[:, n:] == 0)  # nothing written past n in a column
 
 
