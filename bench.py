@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-rhs64", action="store_true",
                     help="skip the 64-right-hand-side measurement")
+    ap.add_argument("--no-gmres", action="store_true",
+                    help="skip the FP32 factor + GMRES-IR measurement")
     ap.add_argument("--workload", choices=["grid3d", "batch", "adjoint", "elasticity"],
                     default="grid3d",
                     help="batch: 1024 independent systems (512 2D, 512 3D) under one handle; "
@@ -373,6 +375,24 @@ def run_gpu_arm(args):
                  "solve_flops_per_rhs_sweep_pair": 4.0 * S.info("lnz"),
                  "note": "FP32 factor + FP64 refinement of 64 columns at once"}
 
+    # the same step with GMRES-based refinement in place of plain refinement
+    # (same FP32 factor, mdgpu_gmres_ir_device); an error here is reported in
+    # the line rather than ending the run
+    gmres = None
+    if not args.no_gmres:
+        def step_fp32_gmres():
+            S.factor(dAx, M.FP32, stream=sptr)
+            return S.gmres_ir_device(db, dx, tol=1e-14, maxit=10, stream=sptr)
+
+        try:
+            tg, (beg, itg, ing) = timed(step_fp32_gmres, max(1, min(args.steps, 3)), 1)
+            gmres = {"ms_per_step": allmax(statistics.mean(tg)),
+                     "backward_error": float(np.max(beg)), "corrections": int(np.max(itg)),
+                     "gmres_steps": int(np.sum(ing)),
+                     "note": "FP32 factor + GMRES-IR (restart 30, inner tolerance 1e-8)"}
+        except Exception as e:  # noqa: BLE001
+            gmres = {"error": str(e)[:300]}
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -399,6 +419,7 @@ def run_gpu_arm(args):
                 "h2d_bytes_per_step": int(Ax.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes)},
         "rhs64": rhs64,
+        "gmres_ir": gmres,
         "hbm_bytes": hbm,
         "gpu_launches": prof["launches_per_step"],
         "clocks": clocks,
