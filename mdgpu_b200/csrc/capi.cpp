@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <map>
 #include <cstring>
+#include <exception>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -61,8 +62,8 @@ T* dalloc(size_t count) {
     return static_cast<T*>(p);
 }
 
-template <typename T>
-T* upload(const std::vector<T>& v) {
+template <typename T, typename A>
+T* upload(const std::vector<T, A>& v) {
     T* d = dalloc<T>(v.size());
     if (!v.empty()) ck(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
     return d;
@@ -203,6 +204,8 @@ void finish_plan(mdgpu_handle_s* h) {
     build_panel_schedule(h->plan, kTile, kPanel, kAssembleCols, h->pschedh);
     h->level = front_levels(h->plan);
 }
+
+
 
 void init_kernels_once() {
     static bool done = false;
@@ -679,6 +682,73 @@ int do_gmres_ir(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ld
     return MDGPU_OK;
 }
 
+// fn(i) for i in [0, count) on all host cores; the first exception (lowest
+// index) is rethrown.
+template <typename F>
+void parallel_for(int count, F&& fn) {
+    std::vector<std::exception_ptr> ex(count);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) {
+            try {
+                fn(i);
+            } catch (...) {
+                ex[i] = std::current_exception();
+            }
+        }
+    };
+    const int nthr = std::max(1, std::min(count, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (auto& x : ex)
+        if (x) std::rethrow_exception(x);
+}
+
+// The same full symmetric CSR for independent systems given one by one: the
+// block-diagonal matrix's rows hold only their own system's entries, in the
+// same order as build_csr over the concatenation; the systems are filled in
+// parallel.
+void build_csr_batch(mdgpu_handle_s* h, int nsys, const int* n, const int* const* Ap,
+                     const int* const* Ai, const std::vector<int>& row_off,
+                     const std::vector<int>& val_off) {
+    const int N = row_off[nsys];
+    std::vector<int> cnt(N, 0);
+    parallel_for(nsys, [&](int b) {
+        int* cb = cnt.data() + row_off[b];
+        for (int j = 0; j < n[b]; ++j)
+            for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p) {
+                const int i = Ai[b][p];
+                cb[i]++;
+                if (i != j) cb[j]++;
+            }
+    });
+    h->h_csr_rowptr.assign(N + 1, 0);
+    for (int i = 0; i < N; ++i) h->h_csr_rowptr[i + 1] = h->h_csr_rowptr[i] + cnt[i];
+    const int64_t nnz = h->h_csr_rowptr[N];
+    h->h_csr_col.resize(nnz);
+    h->h_csr_src.resize(nnz);
+    parallel_for(nsys, [&](int b) {
+        const int r0 = row_off[b];
+        std::vector<int> next(h->h_csr_rowptr.begin() + r0, h->h_csr_rowptr.begin() + r0 + n[b]);
+        for (int j = 0; j < n[b]; ++j)
+            for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p) {
+                const int i = Ai[b][p];
+                int q = next[i]++;
+                h->h_csr_col[q] = j + r0;
+                h->h_csr_src[q] = p + val_off[b];
+                if (i != j) {
+                    q = next[j]++;
+                    h->h_csr_col[q] = i + r0;
+                    h->h_csr_src[q] = p + val_off[b];
+                }
+            }
+    });
+    h->csr.n = N;
+    h->csr.nnz = nnz;
+}
+
 // One symbolic result for independent systems: the block-diagonal matrix of
 // their lower triangles, each system analysed on its own (so each keeps its
 // own bit-exact ordering and tree); rows, supernodes, L columns and the
@@ -687,65 +757,76 @@ int do_gmres_ir(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ld
 void combine_symbolic(const std::vector<Symbolic>& parts, const std::vector<int>& val_off,
                       Symbolic& S) {
     S = Symbolic();
-    int n = 0, ns = 0;
-    int64_t nnz = 0, lnz = 0;
-    for (const Symbolic& p : parts) {
-        n += p.n;
-        ns += p.tree.size();
-        nnz += p.lower.nnz();
-        lnz += p.Lp.back();
+    const int nsys = (int)parts.size();
+    // each system's first row, supernode, lower entry, child entry, L entry
+    // and value in the concatenated arrays
+    std::vector<int64_t> ro(nsys + 1, 0), so(nsys + 1, 0), eo(nsys + 1, 0), co(nsys + 1, 0),
+        lo(nsys + 1, 0), vo(nsys + 1, 0);
+    bool any_perm = false, any_relax = false;
+    for (int b = 0; b < nsys; ++b) {
+        const Symbolic& p = parts[b];
+        ro[b + 1] = ro[b] + p.n;
+        so[b + 1] = so[b] + p.tree.size();
+        eo[b + 1] = eo[b] + p.lower.nnz();
+        co[b + 1] = co[b] + (int64_t)p.tree.child.size();
+        lo[b + 1] = lo[b] + p.Lp.back();
+        vo[b + 1] = vo[b] + (int64_t)p.lower.val.size();
+        any_perm = any_perm || !p.perm.empty();
+        any_relax = any_relax || !p.relax_perm.empty();
     }
-    if (nnz > INT_MAX) throw std::runtime_error("batch too large for 32-bit entry indices");
+    if (eo[nsys] > INT_MAX) throw std::runtime_error("batch too large for 32-bit entry indices");
+    const int n = (int)ro[nsys];
+    const int ns = (int)so[nsys];
     S.n = n;
     S.lower.nrows = S.lower.ncols = n;
-    S.lower.colptr.assign(1, 0);
-    S.tree.child_ptr.assign(1, 0);
-    S.Lp.assign(1, 0);
-    const bool any_perm = std::any_of(parts.begin(), parts.end(), [](const Symbolic& p) {
-        return !p.perm.empty();
-    });
-    const bool any_relax = std::any_of(parts.begin(), parts.end(), [](const Symbolic& p) {
-        return !p.relax_perm.empty();
-    });
-    int ro = 0, so = 0;
-    int64_t eo = 0;
-    for (size_t b = 0; b < parts.size(); ++b) {
+    if (any_perm) S.perm.resize(n);
+    if (any_relax) S.relax_perm.resize(n);
+    S.parent.resize(n);
+    S.post.resize(n);
+    S.count0.resize(n);
+    S.count.resize(n);
+    S.lower.colptr.resize(n + 1);
+    S.lower.rowidx.resize(eo[nsys]);
+    S.lower.val.resize(vo[nsys]);
+    S.lower_src.resize(eo[nsys]);
+    S.tree.first_col.resize(ns);
+    S.tree.ncols.resize(ns);
+    S.tree.child_ptr.resize(ns + 1);
+    S.tree.child.resize(co[nsys]);
+    S.Lp.resize(n + 1);
+    S.lower.colptr[0] = 0;
+    S.tree.child_ptr[0] = 0;
+    S.Lp[0] = 0;
+    // the systems' slices are disjoint: filled in parallel
+    parallel_for(nsys, [&](int b) {
         const Symbolic& p = parts[b];
-        auto shift = [](const std::vector<int>& v, int o, std::vector<int>& out, bool keep_neg) {
-            for (int x : v) out.push_back(keep_neg && x < 0 ? x : x + o);
-        };
-        if (any_perm) {
-            if (p.perm.empty())
-                for (int i = 0; i < p.n; ++i) S.perm.push_back(ro + i);
-            else
-                shift(p.perm, ro, S.perm, false);
+        const int r0 = (int)ro[b], s0 = (int)so[b];
+        const int64_t e0 = eo[b], c0 = co[b], l0 = lo[b];
+        for (int i = 0; i < p.n; ++i) {
+            if (any_perm) S.perm[r0 + i] = p.perm.empty() ? r0 + i : p.perm[i] + r0;
+            if (any_relax)
+                S.relax_perm[r0 + i] = p.relax_perm.empty() ? r0 + i : p.relax_perm[i] + r0;
+            S.parent[r0 + i] = p.parent[i] < 0 ? p.parent[i] : p.parent[i] + r0;
+            S.post[r0 + i] = p.post[i] + r0;
+            S.count0[r0 + i] = p.count0[i];
+            S.count[r0 + i] = p.count[i];
+            S.lower.colptr[r0 + i + 1] = (int)(e0 + p.lower.colptr[i + 1]);
+            S.Lp[r0 + i + 1] = l0 + p.Lp[i + 1];
         }
-        if (any_relax) {
-            if (p.relax_perm.empty())
-                for (int i = 0; i < p.n; ++i) S.relax_perm.push_back(ro + i);
-            else
-                shift(p.relax_perm, ro, S.relax_perm, false);
+        for (int64_t q = 0; q < p.lower.nnz(); ++q) {
+            S.lower.rowidx[e0 + q] = p.lower.rowidx[q] + r0;
+            const int src = p.lower_src[q];
+            S.lower_src[e0 + q] = src < 0 ? src : src + val_off[b];
         }
-        shift(p.parent, ro, S.parent, true);
-        shift(p.post, ro, S.post, false);
-        S.count0.insert(S.count0.end(), p.count0.begin(), p.count0.end());
-        S.count.insert(S.count.end(), p.count.begin(), p.count.end());
-        for (int j = 0; j < p.n; ++j) S.lower.colptr.push_back((int)(eo + p.lower.colptr[j + 1]));
-        shift(p.lower.rowidx, ro, S.lower.rowidx, false);
-        S.lower.val.insert(S.lower.val.end(), p.lower.val.begin(), p.lower.val.end());
-        shift(p.lower_src, val_off[b], S.lower_src, true);
-        shift(p.tree.first_col, ro, S.tree.first_col, false);
-        S.tree.ncols.insert(S.tree.ncols.end(), p.tree.ncols.begin(), p.tree.ncols.end());
-        const int cbase = (int)S.tree.child.size();
-        for (int s = 0; s < p.tree.size(); ++s) S.tree.child_ptr.push_back(cbase + p.tree.child_ptr[s + 1]);
-        shift(p.tree.child, so, S.tree.child, false);
-        const int64_t lb = S.Lp.back();
-        for (int j = 0; j < p.n; ++j) S.Lp.push_back(lb + p.Lp[j + 1]);
-        ro += p.n;
-        so += p.tree.size();
-        eo += p.lower.nnz();
-    }
-    (void)lnz;
+        std::copy(p.lower.val.begin(), p.lower.val.end(), S.lower.val.begin() + vo[b]);
+        for (int s = 0; s < p.tree.size(); ++s) {
+            S.tree.first_col[s0 + s] = p.tree.first_col[s] + r0;
+            S.tree.ncols[s0 + s] = p.tree.ncols[s];
+            S.tree.child_ptr[s0 + s + 1] = (int)(c0 + p.tree.child_ptr[s + 1]);
+        }
+        for (size_t k = 0; k < p.tree.child.size(); ++k)
+            S.tree.child[c0 + k] = p.tree.child[k] + s0;
+    });
 }
 
 // Solve error word (d_status[2]): cleared before a public solve call, read
@@ -1008,17 +1089,8 @@ int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int*
             combine_symbolic(parts, val_off, h->sym);
             h->sys_row_off = row_off;
             h->sys_val_off = val_off;
-            // the block-diagonal lower triangle in the caller's ordering
-            const int N = row_off[nsys];
-            std::vector<int> Apc(1, 0), Aic;
-            Aic.reserve(val_off[nsys]);
-            for (int b = 0; b < nsys; ++b)
-                for (int j = 0; j < n[b]; ++j) {
-                    for (int p = Ap[b][j]; p < Ap[b][j + 1]; ++p) Aic.push_back(Ai[b][p] + row_off[b]);
-                    Apc.push_back((int)Aic.size());
-                }
             finish_plan(h);
-            build_csr(h, N, Apc.data(), Aic.data());
+            build_csr_batch(h, nsys, n, Ap, Ai, row_off, val_off);
             upload_plan(h);
         } catch (...) {
             delete h;
@@ -1099,7 +1171,7 @@ int mdgpu_get_array(mdgpu_handle h, const char* name, void* dst) {
     const Plan& P = h->plan;
     const Symbolic& S = h->sym;
     std::string k(name);
-    auto put = [&](const std::vector<int>& v) {
+    auto put = [&](const auto& v) {
         if (!v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int));
         return MDGPU_OK;
     };

@@ -31,29 +31,34 @@ static std::vector<std::pair<int, int>> tree_ranges(const AssemblyTree& t,
     return r;
 }
 
-// fn(beg, end) on every range, ranges shared out to the host's cores; the
-// first exception (lowest range) is rethrown.
+// fn(i) for i in [0, count), indices shared out to the host's cores; the
+// first exception (lowest index) is rethrown.
 template <typename F>
-static void for_each_range(const std::vector<std::pair<int, int>>& rg, F&& fn) {
-    const int nr = (int)rg.size();
-    std::vector<std::exception_ptr> ex(nr);
+static void for_each_index(int count, F&& fn) {
+    std::vector<std::exception_ptr> ex(count);
     std::atomic<int> next{0};
     auto work = [&]() {
-        for (int i = next.fetch_add(1); i < nr; i = next.fetch_add(1)) {
+        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) {
             try {
-                fn(rg[i].first, rg[i].second);
+                fn(i);
             } catch (...) {
                 ex[i] = std::current_exception();
             }
         }
     };
-    const int nthr = std::max(1, std::min(nr, (int)std::thread::hardware_concurrency()));
+    const int nthr = std::max(1, std::min(count, (int)std::thread::hardware_concurrency()));
     std::vector<std::thread> pool;
     for (int k = 1; k < nthr; ++k) pool.emplace_back(work);
     work();
     for (auto& th : pool) th.join();
     for (auto& e : ex)
         if (e) std::rethrow_exception(e);
+}
+
+// fn(beg, end) on every range, ranges shared out to the host's cores
+template <typename F>
+static void for_each_range(const std::vector<std::pair<int, int>>& rg, F&& fn) {
+    for_each_index((int)rg.size(), [&](int i) { fn(rg[i].first, rg[i].second); });
 }
 
 const int Plan::small_limit[kSmallBuckets] = {16, 32, 64, 96, 128, 160};
@@ -104,8 +109,8 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
         rows_off[s + 1] = rows_off[s] + cnt;
     }
     if (rows_off[ns] > INT32_MAX) throw std::runtime_error("row arrays exceed 2^31 entries");
-    P.rows.resize(rows_off[ns]);
-    P.relmap.assign(rows_off[ns], -1);
+    P.rows.resize(rows_off[ns]);    // every entry is written below
+    P.relmap.resize(rows_off[ns]);  // likewise (-1 where there is no parent row)
     const auto ranges = tree_ranges(t, parent);
     for_each_range(ranges, [&](int s0, int s1) {
         std::vector<int> scratch;
@@ -133,9 +138,12 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
             for (int i = 0; i < c; ++i) r[i] = k + i;
             std::copy(scratch.begin(), scratch.end(), r + c);
         }
-        // relative maps: position of each update row of s inside its parent's rows
+        // relative maps: position of each update row of s inside its parent's
+        // rows; -1 for the pivot rows and for a root's rows
         for (int s = s0; s < s1; ++s) {
             int p = parent[s];
+            int* rm = P.relmap.data() + rows_off[s];
+            std::fill(rm, rm + (p < 0 ? rows_off[s + 1] - rows_off[s] : t.ncols[s]), -1);
             if (p < 0) continue;
             const int* rs = P.rows.data() + rows_off[s];
             const int* rp = P.rows.data() + rows_off[p];
@@ -149,35 +157,70 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
         }
     });
 
-    // storage offsets and descriptors
-    P.fronts.resize(ns);
-    int64_t lo = 0, uo = 0;
-    for (int s = 0; s < ns; ++s) {
-        FrontDesc& f = P.fronts[s];
-        f.m = (int)(rows_off[s + 1] - rows_off[s]);
-        f.c = t.ncols[s];
-        f.ldl = round8(f.m);
-        int u = f.m - f.c;
-        f.ldu = round8(u);
-        f.loff = lo;
-        lo = align_up(lo + (int64_t)f.ldl * f.c, 32);
-        if (parent[s] >= 0 && u > 0) {
-            f.uoff = uo;
-            uo = align_up(uo + (int64_t)f.ldu * u, 32);
-        } else {
-            f.uoff = -1;
+    // storage offsets and descriptors.  The offsets are prefix sums of the
+    // 32-aligned panel and update sizes (offsets start at 0 and stay aligned,
+    // so align_up(off + size) = off + align_up(size)): sums per range, then
+    // the ranges filled in parallel from their bases.
+    P.fronts.resize(ns);  // every descriptor is written below
+    const int nrg = (int)ranges.size();
+    std::vector<int64_t> rg_l(nrg + 1, 0), rg_u(nrg + 1, 0);
+    std::vector<int> rg_maxm(nrg, 0), rg_maxu(nrg, 0);
+    auto panel_size = [&](int s, int64_t& lsz, int64_t& usz) {
+        const int m = (int)(rows_off[s + 1] - rows_off[s]), c = t.ncols[s], u = m - c;
+        lsz = align_up((int64_t)round8(m) * c, 32);
+        usz = (parent[s] >= 0 && u > 0) ? align_up((int64_t)round8(u) * u, 32) : -1;
+    };
+    for_each_index(nrg, [&](int r) {
+        int64_t sl = 0, su = 0;
+        for (int s = ranges[r].first; s < ranges[r].second; ++s) {
+            int64_t lsz, usz;
+            panel_size(s, lsz, usz);
+            sl += lsz;
+            if (usz >= 0) su += usz;
         }
-        f.rows_off = (int)rows_off[s];
-        f.first_col = t.first_col[s];
-        f.child_beg = t.child_ptr[s];
-        f.child_end = t.child_ptr[s + 1];
-        f.a_beg = A.colptr[f.first_col];
-        f.a_end = A.colptr[f.first_col + f.c];
-        f.parent = parent[s];
-        f.pad_ = 0;
-        P.max_m = std::max(P.max_m, f.m);
-        P.max_u = std::max(P.max_u, u);
+        rg_l[r + 1] = sl;
+        rg_u[r + 1] = su;
+    });
+    for (int r = 0; r < nrg; ++r) {
+        rg_l[r + 1] += rg_l[r];
+        rg_u[r + 1] += rg_u[r];
     }
+    for_each_index(nrg, [&](int r) {
+        int64_t lo = rg_l[r], uo = rg_u[r];
+        for (int s = ranges[r].first; s < ranges[r].second; ++s) {
+            int64_t lsz, usz;
+            panel_size(s, lsz, usz);
+            FrontDesc& f = P.fronts[s];
+            f.m = (int)(rows_off[s + 1] - rows_off[s]);
+            f.c = t.ncols[s];
+            f.ldl = round8(f.m);
+            const int u = f.m - f.c;
+            f.ldu = round8(u);
+            f.loff = lo;
+            lo += lsz;
+            if (usz >= 0) {
+                f.uoff = uo;
+                uo += usz;
+            } else {
+                f.uoff = -1;
+            }
+            f.rows_off = (int)rows_off[s];
+            f.first_col = t.first_col[s];
+            f.child_beg = t.child_ptr[s];
+            f.child_end = t.child_ptr[s + 1];
+            f.a_beg = A.colptr[f.first_col];
+            f.a_end = A.colptr[f.first_col + f.c];
+            f.parent = parent[s];
+            f.pad_ = 0;
+            rg_maxm[r] = std::max(rg_maxm[r], f.m);
+            rg_maxu[r] = std::max(rg_maxu[r], u);
+        }
+    });
+    for (int r = 0; r < nrg; ++r) {
+        P.max_m = std::max(P.max_m, rg_maxm[r]);
+        P.max_u = std::max(P.max_u, rg_maxu[r]);
+    }
+    const int64_t lo = rg_l[nrg], uo = rg_u[nrg];
     P.lstore = std::max<int64_t>(lo, 32);
     P.ustore = std::max<int64_t>(uo, 32);
     P.child = t.child;

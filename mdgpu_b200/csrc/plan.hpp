@@ -16,11 +16,39 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "symbolic.hpp"
 
 namespace mdgpu {
+
+// std::allocator whose resize() leaves new elements default-initialised
+// (for int and plain structs: untouched), so a plan's large arrays are first
+// written -- and their pages first touched -- by the threads that fill them.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <typename T>
+using HostArray = std::vector<T, UninitAlloc<T>>;
 
 // Per-supernode record mirrored on the device.
 struct FrontDesc {
@@ -54,12 +82,12 @@ struct Plan {
     int64_t nnz_user = 0;       // entries of the caller's lower triangle
     std::vector<int> perm;      // new -> old (empty: natural)
     std::vector<int> iperm;     // old -> new
-    std::vector<FrontDesc> fronts;
+    HostArray<FrontDesc> fronts;
     std::vector<int> child;     // children lists
-    std::vector<int> rows;      // front row sets, concatenated
-    std::vector<int> relmap;    // per row r >= c_s of front s: position in the parent's front
-    std::vector<int> a_src;     // per A entry: index in the caller's value array
-    std::vector<int> a_pos;     // per A entry: local (row | col << 16) inside the front
+    HostArray<int> rows;        // front row sets, concatenated
+    HostArray<int> relmap;      // per row r >= c_s of front s: position in the parent's front
+    HostArray<int> a_src;       // per A entry: index in the caller's value array
+    HostArray<int> a_pos;       // per A entry: local (row | col << 16) inside the front
     std::vector<int> a_colptr;  // per large front: c+1 offsets into its A entries
     std::vector<int> a_colptr_off;  // per supernode: offset into a_colptr (-1 if small)
     // large fronts: inverted diagonal tiles (T x T each, one per pivot tile)
