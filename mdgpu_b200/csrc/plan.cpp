@@ -477,24 +477,38 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         S.fv_rows += P.fronts[s].m;
     }
     if (S.fv_rows > INT32_MAX) throw std::runtime_error("front vectors exceed 2^31 rows");
+    // assembly maps of the large fronts: sizes first (rows m + 1, entries =
+    // the children's update rows), then each front filled on its own
     S.amap_off.assign(P.nsuper, -1);
-    S.amap_row.clear();
-    S.amap_ent.clear();
-    std::vector<int> cnt;
-    for (int s : P.large_list) {
+    const int nlarge = (int)P.large_list.size();
+    std::vector<int64_t> row_base(nlarge + 1, 0), ent_base(nlarge + 1, 0);
+    for (int k = 0; k < nlarge; ++k) {
+        const FrontDesc& f = P.fronts[P.large_list[k]];
+        int64_t ent = 0;
+        for (int h = f.child_beg; h < f.child_end; ++h) {
+            const FrontDesc& g = P.fronts[P.child[h]];
+            ent += g.m - g.c;
+        }
+        row_base[k + 1] = row_base[k] + f.m + 1;
+        ent_base[k + 1] = ent_base[k] + ent;
+    }
+    if (ent_base[nlarge] > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 entries");
+    if (row_base[nlarge] > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 rows");
+    S.amap_row.resize(row_base[nlarge]);  // every entry is written below
+    S.amap_ent.resize(ent_base[nlarge]);
+    for_each_index(nlarge, [&](int k) {
+        const int s = P.large_list[k];
         const FrontDesc& f = P.fronts[s];
-        cnt.assign(f.m + 1, 0);
+        std::vector<int> cnt(f.m + 1, 0);
         for (int h = f.child_beg; h < f.child_end; ++h) {
             const FrontDesc& g = P.fronts[P.child[h]];
             const int* rm = P.relmap.data() + g.rows_off + g.c;
             for (int rr = 0; rr < g.m - g.c; ++rr) cnt[rm[rr] + 1]++;
         }
         for (int r = 0; r < f.m; ++r) cnt[r + 1] += cnt[r];
-        const int64_t base = (int64_t)S.amap_ent.size();
-        if (base + cnt[f.m] > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 entries");
-        S.amap_off[s] = (int)S.amap_row.size();
-        for (int r = 0; r <= f.m; ++r) S.amap_row.push_back((int)(base + cnt[r]));
-        S.amap_ent.resize(base + cnt[f.m]);
+        const int64_t base = ent_base[k];
+        S.amap_off[s] = (int)row_base[k];
+        for (int r = 0; r <= f.m; ++r) S.amap_row[row_base[k] + r] = (int)(base + cnt[r]);
         for (int h = f.child_beg; h < f.child_end; ++h) {  // child order kept per row
             const int ch = P.child[h];
             const FrontDesc& g = P.fronts[ch];
@@ -502,8 +516,7 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
             for (int rr = 0; rr < g.m - g.c; ++rr)
                 S.amap_ent[base + cnt[rm[rr]]++] = (int)(S.fv_off[ch] + g.c + rr);
         }
-    }
-    if (S.amap_row.size() > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 rows");
+    });
     const int GC = SolveScheduleHost::kGatherTiles;
     S.gather_task_beg.assign(P.nlevels + 1, 0);
     S.gather_nch.assign(P.nsuper, 0);

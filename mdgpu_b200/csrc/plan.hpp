@@ -201,8 +201,8 @@ struct SolveScheduleHost {
     // amap_row[amap_off[s] + r + 1] - 1] (children's update rows, in child
     // order, so the sums are those of a child-by-child scatter)
     std::vector<int> amap_off;  // per supernode, -1 for small fronts
-    std::vector<int> amap_row;
-    std::vector<int> amap_ent;
+    HostArray<int> amap_row;
+    HostArray<int> amap_ent;
 };
 
 int front_tiles(int m, int c, int T);  // tiles in the [0,c) + [c,m) tiling
