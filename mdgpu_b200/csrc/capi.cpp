@@ -94,7 +94,8 @@ struct mdgpu_handle_s {
     DevPlan D;
     std::vector<int> level;
     SymCsr csr;
-    std::vector<int> h_csr_rowptr, h_csr_col, h_csr_src;
+    std::vector<int> h_csr_rowptr;
+    HostArray<int> h_csr_col, h_csr_src;  // every entry written by the CSR build
     bool on_device = false;
     int device = 0;
     cudaStream_t stream = nullptr;
