@@ -20,6 +20,7 @@
 #include "ir.hpp"
 #include "kernels.hpp"
 #include "mdgpu_b200.h"
+#include "parallel.hpp"
 #include "plan.hpp"
 #include "symbolic.hpp"
 
@@ -205,8 +206,6 @@ void finish_plan(mdgpu_handle_s* h) {
     build_panel_schedule(h->plan, kTile, kPanel, kAssembleCols, h->pschedh);
     h->level = front_levels(h->plan);
 }
-
-
 
 void init_kernels_once() {
     static bool done = false;
@@ -683,30 +682,6 @@ int do_gmres_ir(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ld
     return MDGPU_OK;
 }
 
-// fn(i) for i in [0, count) on all host cores; the first exception (lowest
-// index) is rethrown.
-template <typename F>
-void parallel_for(int count, F&& fn) {
-    std::vector<std::exception_ptr> ex(count);
-    std::atomic<int> next{0};
-    auto work = [&]() {
-        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) {
-            try {
-                fn(i);
-            } catch (...) {
-                ex[i] = std::current_exception();
-            }
-        }
-    };
-    const int nthr = std::max(1, std::min(count, (int)std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
-    work();
-    for (auto& t : pool) t.join();
-    for (auto& x : ex)
-        if (x) std::rethrow_exception(x);
-}
-
 // The same full symmetric CSR for independent systems given one by one: the
 // block-diagonal matrix's rows hold only their own system's entries, in the
 // same order as build_csr over the concatenation; the systems are filled in
@@ -884,35 +859,27 @@ int analyze_systems(int nsys, const int* n, const int* const* Ap, const int* con
     const bool keep = flops == nullptr;
     std::vector<int> rc(nsys, 0);
     std::vector<std::string> what(nsys);
-    std::atomic<int> next{0};
-    auto work = [&]() {
+    parallel_for(nsys, [&](int b) {
         Symbolic one;
-        for (int b = next.fetch_add(1); b < nsys; b = next.fetch_add(1)) {
-            Symbolic& S = keep ? parts[b] : one;
-            try {
-                rc[b] = analyze(n[b], Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD,
-                                (TreeKind)tree, relax_zeros, S) != 0
-                            ? 1
-                            : 0;
-                if (!keep && rc[b] == 0) {
-                    double f = 0.0;
-                    for (int j = 0; j < n[b]; ++j) f += (double)S.count[j] * S.count[j] + 1.0;
-                    flops[b] = f;
-                    if (lnz) lnz[b] = (long long)S.Lp[n[b]];
-                }
-            } catch (const std::bad_alloc&) {
-                rc[b] = 2;
-            } catch (const std::exception& e) {
-                rc[b] = 3;
-                what[b] = e.what();
+        Symbolic& S = keep ? parts[b] : one;
+        try {
+            rc[b] = analyze(n[b], Ap[b], Ai[b], nullptr, ordering == MDGPU_ORDER_AMD,
+                            (TreeKind)tree, relax_zeros, S) != 0
+                        ? 1
+                        : 0;
+            if (!keep && rc[b] == 0) {
+                double f = 0.0;
+                for (int j = 0; j < n[b]; ++j) f += (double)S.count[j] * S.count[j] + 1.0;
+                flops[b] = f;
+                if (lnz) lnz[b] = (long long)S.Lp[n[b]];
             }
+        } catch (const std::bad_alloc&) {
+            rc[b] = 2;
+        } catch (const std::exception& e) {
+            rc[b] = 3;
+            what[b] = e.what();
         }
-    };
-    const int nthr = std::max(1, std::min<int>(nsys, (int)std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
-    work();
-    for (auto& t : pool) t.join();
+    });
     for (int b = 0; b < nsys; ++b) {
         if (rc[b] == 1)
             return fail(MDGPU_ERR_NOT_TREE,

@@ -9,6 +9,8 @@
 #include <string>
 #include <thread>
 
+#include "parallel.hpp"
+
 namespace mdgpu {
 
 // The trees of an assembly forest (a batch of independent systems) as
@@ -31,34 +33,10 @@ static std::vector<std::pair<int, int>> tree_ranges(const AssemblyTree& t,
     return r;
 }
 
-// fn(i) for i in [0, count), indices shared out to the host's cores; the
-// first exception (lowest index) is rethrown.
-template <typename F>
-static void for_each_index(int count, F&& fn) {
-    std::vector<std::exception_ptr> ex(count);
-    std::atomic<int> next{0};
-    auto work = [&]() {
-        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) {
-            try {
-                fn(i);
-            } catch (...) {
-                ex[i] = std::current_exception();
-            }
-        }
-    };
-    const int nthr = std::max(1, std::min(count, (int)std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int k = 1; k < nthr; ++k) pool.emplace_back(work);
-    work();
-    for (auto& th : pool) th.join();
-    for (auto& e : ex)
-        if (e) std::rethrow_exception(e);
-}
-
 // fn(beg, end) on every range, ranges shared out to the host's cores
 template <typename F>
 static void for_each_range(const std::vector<std::pair<int, int>>& rg, F&& fn) {
-    for_each_index((int)rg.size(), [&](int i) { fn(rg[i].first, rg[i].second); });
+    parallel_for((int)rg.size(), [&](int i) { fn(rg[i].first, rg[i].second); });
 }
 
 const int Plan::small_limit[kSmallBuckets] = {16, 32, 64, 96, 128, 160};
@@ -170,7 +148,7 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
         lsz = align_up((int64_t)round8(m) * c, 32);
         usz = (parent[s] >= 0 && u > 0) ? align_up((int64_t)round8(u) * u, 32) : -1;
     };
-    for_each_index(nrg, [&](int r) {
+    parallel_for(nrg, [&](int r) {
         int64_t sl = 0, su = 0;
         for (int s = ranges[r].first; s < ranges[r].second; ++s) {
             int64_t lsz, usz;
@@ -185,7 +163,7 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
         rg_l[r + 1] += rg_l[r];
         rg_u[r + 1] += rg_u[r];
     }
-    for_each_index(nrg, [&](int r) {
+    parallel_for(nrg, [&](int r) {
         int64_t lo = rg_l[r], uo = rg_u[r];
         for (int s = ranges[r].first; s < ranges[r].second; ++s) {
             int64_t lsz, usz;
@@ -496,7 +474,7 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     if (row_base[nlarge] > INT32_MAX) throw std::runtime_error("assembly map exceeds 2^31 rows");
     S.amap_row.resize(row_base[nlarge]);  // every entry is written below
     S.amap_ent.resize(ent_base[nlarge]);
-    for_each_index(nlarge, [&](int k) {
+    parallel_for(nlarge, [&](int k) {
         const int s = P.large_list[k];
         const FrontDesc& f = P.fronts[s];
         std::vector<int> cnt(f.m + 1, 0);
