@@ -144,6 +144,80 @@ def reference_cpu_sample(side, timeout=600):
                 "sample": "oracle port of the reference CPU path on the %d^3 grid" % side}
 
 
+def reference_cpu_system(n, Ap, Ai, Ax, b, timeout=600):
+    """The reference's own CPU Factor + cs_lsolve/cs_ltsolve (-amd -sn, one
+    core) on one system: (flops, seconds of factor + solve, kind)."""
+    from mdgpu_b200 import matgen as mg
+    from oracle import oracle as O
+
+    with tempfile.TemporaryDirectory() as d:
+        mf = os.path.join(d, "A.txt")
+        bf = os.path.join(d, "b.f64")
+        mg.write_triplets(mf, n, Ap, Ai, Ax)
+        np.asarray(b, np.float64).tofile(bf)
+        if os.path.exists(O.REF_HARNESS):
+            out = os.path.join(d, "out")
+            os.makedirs(out)
+            cmd = ["taskset", "-c", "0", O.REF_HARNESS, "-amd", "-sn", "-bfile", bf, mf, out]
+            try:
+                subprocess.run(cmd, check=True, capture_output=True, timeout=timeout)
+            except FileNotFoundError:
+                subprocess.run(cmd[3:], check=True, capture_output=True, timeout=timeout)
+            meta = O.load_dir(out)["meta"]
+            return meta["flops"], meta["t_factor"] + meta["t_solve"], "reference"
+        P = O.Plan(n, Ap, Ai, Ax, amd=True, mode="sn")
+        t0 = time.perf_counter()
+        F = P.factor()
+        P.solve(F["Li"], F["Lx"], b)
+        return F["flops"], time.perf_counter() - t0, "port"
+
+
+def run_reference_workload_arm(args):
+    """The reference's CPU path on a bounded sample of the batch or
+    elasticity workload (the reference factors one system per run, on one
+    core): batch -- every 64th of the 1024 systems (8 2D + 8 3D), one after
+    another; elasticity -- the same generator at 12^3 nodes, cs_amd on the
+    scalar matrix (the reference's -amd)."""
+    from mdgpu_b200 import matgen as mg
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if args.workload == "batch":
+        syss = batch_systems()[::64]
+        sample = ("every 64th of the 1024 systems (%d systems, n = %d), one after another"
+                  % (len(syss), sum(s[0] for s in syss)))
+        work = [(n, Ap, Ai, Ax, mg.rhs_uniform(n, seed=3)) for (n, Ap, Ai, Ax) in syss]
+    else:
+        n, Ap, Ai, Ax = mg.elasticity_3dof(12, seed=0, sigma=1.0, shift=1e-2)
+        sample = "3 unknowns per node, 12^3 nodes (n = %d), -amd on the scalar matrix" % n
+        work = [(n, Ap, Ai, Ax, mg.rhs_uniform(n, seed=1))]
+    for _ in range(args.warmup):
+        reference_cpu_system(*work[0])
+    rates, secs = [], []
+    kind = "reference"
+    for _ in range(args.steps):
+        fl, t = 0.0, 0.0
+        for w in work:
+            f1, t1, kind = reference_cpu_system(*w)
+            fl += f1
+            t += t1
+        rates.append(fl / t / 1e9)
+        secs.append(t)
+    v = statistics.median(rates)
+    base = {"value": v, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+            "seconds": statistics.median(secs)}
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "sample": sample, "cpu": cpu_info(),
+                       "nproc": os.cpu_count(),
+                       "note": "single-threaded reference Factor + cs_lsolve + cs_ltsolve"},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def cpu_info():
     try:
         for line in open("/proc/cpuinfo"):
@@ -790,7 +864,9 @@ def main():
     if args.workload == "elasticity" and args.impl != "reference":
         run_elasticity_arm(args)
         return
-    if args.impl == "reference":
+    if args.impl == "reference" and args.workload in ("batch", "elasticity"):
+        run_reference_workload_arm(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_gpu_arm(args)
