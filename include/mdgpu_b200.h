@@ -116,6 +116,17 @@ MDGPU_API int mdgpu_analyze_tree(int n, const int *Ap, const int *Ai, int nsuper
 
 MDGPU_API void mdgpu_destroy(mdgpu_handle h);
 
+/*
+ * Diagnostic (no counterpart in the reference): check on the host every
+ * invariant the device kernels rely on when they index the handle's tables
+ * -- front row sets strictly increasing and inside n, relative maps pointing
+ * at the same row of the parent, every A entry at its row and column, level
+ * and warp lists holding each front once, assembly maps and solve task
+ * order, the residual's CSR in range.  MDGPU_OK, or MDGPU_ERR_INVALID with
+ * the failed invariant and its front in mdgpu_last_error().  Host only.
+ */
+MDGPU_API int mdgpu_check_plan(mdgpu_handle h);
+
 /* Scalars: "n", "nsuper", "lnz", "nlevels", "nnz", "max_front", "flops"
  * (the reference's own count, mdgpu.cu:1354-1359), "lstore_bytes",
  * "ustore_bytes", "rows_total", "nchild", "large_fronts", "small_fronts",

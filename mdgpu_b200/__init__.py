@@ -24,7 +24,7 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "not positive definite", -3: "out
           -7: "no CUDA device"}
 
 # every entry point declared in include/mdgpu_b200.h
-EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_info",
+EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_destroy", "mdgpu_check_plan", "mdgpu_info",
            "mdgpu_estimate_batch", "mdgpu_get_array", "mdgpu_factor", "mdgpu_factor_device", "mdgpu_not_spd_column",
            "mdgpu_solve", "mdgpu_solve_device", "mdgpu_solve_device_noalloc", "mdgpu_refine",
            "mdgpu_refine_device", "mdgpu_gmres_ir", "mdgpu_gmres_ir_device",
@@ -75,6 +75,7 @@ def lib():
         L.mdgpu_estimate_batch.argtypes = [C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.c_int,
                                            C.c_int, C.c_int, dp, vp]
         L.mdgpu_destroy.argtypes = [vp]
+        L.mdgpu_check_plan.argtypes = [vp]
         L.mdgpu_destroy.restype = None
         L.mdgpu_info.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
         L.mdgpu_get_array.argtypes = [vp, C.c_char_p, vp]
@@ -229,6 +230,11 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def check_plan(self):
+        """Host check of every invariant of the plan's tables (raises
+        MdgpuError naming the failed invariant)."""
+        _check(lib().mdgpu_check_plan(self._h))
 
     def info(self, key):
         v = C.c_longlong()

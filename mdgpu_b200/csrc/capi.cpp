@@ -22,6 +22,7 @@
 #include "mdgpu_b200.h"
 #include "parallel.hpp"
 #include "plan.hpp"
+#include "plan_check.hpp"
 #include "symbolic.hpp"
 
 using namespace mdgpu;
@@ -1199,6 +1200,17 @@ int mdgpu_factor(mdgpu_handle h, const double* Ax, int precision, void* stream) 
                            cudaMemcpyHostToDevice, st),
            "upload values");
         return do_factor(h, h->d_Ax, precision, st);
+    });
+}
+
+int mdgpu_check_plan(mdgpu_handle h) {
+    if (!h) return fail(MDGPU_ERR_INVALID, "null handle");
+    return guarded([&]() -> int {
+        const std::string why =
+            check_plan(h->plan, h->sym, h->ssched, h->level, h->h_csr_rowptr, h->h_csr_col.data(),
+                       h->h_csr_src.data(), (int64_t)h->h_csr_col.size());
+        if (!why.empty()) return fail(MDGPU_ERR_INVALID, "plan check: " + why);
+        return MDGPU_OK;
     });
 }
 
