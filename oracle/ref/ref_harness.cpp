@@ -11,9 +11,8 @@
  *   numeric factor            mdgpu.cu:1888-1890  (Factor with GPU = false)
  *   solve + residual          mdgpu.cu:1941-1973  (cs_pvec, cs_lsolve, cs_ltsolve,
  *                                                  cs_ipvec, cs_gaxpy, cs_norm)
- * with three fixes that make the reference's CPU path usable as an oracle, each
- * applied here rather than in the
- * reference sources:
+ * with three fixes that make the reference's CPU path usable as an oracle,
+ * each applied here rather than in the reference sources:
  *   - spL->x is allocated (its allocation is commented out at mdgpu.cu:1873,
  *     yet FactorAux_CPU_3 writes it at mdgpu.cu:1350);
  *   - the children of every supernode are put back in postorder after
