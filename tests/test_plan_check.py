@@ -74,3 +74,36 @@ def test_each_broken_invariant_is_caught(tmp_path):
     assert set(got) == set(EXPECT)
     for k, v in EXPECT.items():
         assert v in got[k], (k, got[k])
+
+
+def _random_connected_lower(n, extra, rng):
+    """Lower CSC of a random connected pattern: a random spanning tree plus
+    `extra` random edges (so the elimination tree is one tree)."""
+    edges = set()
+    order = rng.permutation(n)
+    for k in range(1, n):
+        a, b = order[k], order[rng.integers(0, k)]
+        edges.add((max(a, b), min(a, b)))
+    for _ in range(extra):
+        a, b = rng.integers(0, n, 2)
+        if a != b:
+            edges.add((max(a, b), min(a, b)))
+    cols = [[j] for j in range(n)]
+    for i, j in edges:
+        cols[j].append(i)
+    Ap, Ai = [0], []
+    for j in range(n):
+        Ai.extend(sorted(cols[j]))
+        Ap.append(len(Ai))
+    return n, np.array(Ap, np.int32), np.array(Ai, np.int32)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_patterns_pass_the_check(seed):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(1, 400))
+    n, Ap, Ai = _random_connected_lower(n, int(rng.integers(0, 6 * n + 1)), rng)
+    for kw in ({}, {"tree": M.TREE_NODAL}, {"tree": M.TREE_RELAXED, "relax_zeros": 6},
+               {"ordering": M.ORDER_NATURAL}):
+        S = M.Solver(n, Ap, Ai, **kw)
+        S.check_plan()
