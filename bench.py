@@ -73,6 +73,8 @@ def parse():
                     help="skip the 64-right-hand-side measurement")
     ap.add_argument("--no-gmres", action="store_true",
                     help="skip the FP32 factor + GMRES-IR measurement")
+    ap.add_argument("--elastic-side", type=int, default=40,
+                    help="nodes per side of the elasticity workload (40: the full size)")
     ap.add_argument("--workload", choices=["grid3d", "batch", "adjoint", "elasticity"],
                     default="grid3d",
                     help="batch: 1024 independent systems (512 2D, 512 3D) under one handle; "
@@ -797,7 +799,7 @@ def run_elasticity_arm(args):
     import mdgpu_b200 as M
     from mdgpu_b200 import matgen as mg
 
-    side = 40
+    side = args.elastic_side
     n, Ap, Ai, Ax = mg.elasticity_3dof(side, seed=0, sigma=1.0, shift=1e-2)
     nn, gp, gi, _ = mg.node_graph_lower(side)
     perm = mg.expand_node_perm(M.Solver(nn, gp, gi, ordering=M.ORDER_AMD).array("perm"))
@@ -852,9 +854,9 @@ def run_elasticity_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_g,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 factor (tf32 tensor-core Schur) + f64 GMRES-IR", "data": "synthetic",
-            "config": {"workload": "3 unknowns per node, 40^3 node grid, 27-point, blocks "
+            "config": {"workload": "3 unknowns per node, %d^3 node grid, 27-point, blocks "
                                    "w(I+0.5ee'), w lognormal(0,1), shift 1e-2, node-graph AMD, "
-                                   "1 RHS U(-1,1)",
+                                   "1 RHS U(-1,1)" % side,
                        "n": n, "nsuper": S.info("nsuper"), "lnz": S.info("lnz"),
                        "flops_per_step": flops, "analyze_s": t_an,
                        "l2": "flushed between steps (256 MiB write)"},
