@@ -788,8 +788,9 @@ def run_adjoint_arm(args):
 
 
 def run_elasticity_arm(args):
-    """The multi-unknown system: 3 unknowns per node of a 40^3 node grid with
-    27-point connectivity (n = 192000), blocks w (I + 0.5 e e'), w
+    """The multi-unknown system: 3 unknowns per node of a side^3 node grid
+    (--elastic-side, 40 by default: n = 192000) with 27-point connectivity,
+    blocks w (I + 0.5 e e'), w
     lognormal(0, 1), shift 1e-2, AMD on the node graph expanded to the
     unknowns.  One step = factor + solve to backward error 1e-14 of one
     right-hand side: FP32 factor + GMRES-IR, FP32 factor + plain refinement,
