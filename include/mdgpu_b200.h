@@ -124,6 +124,8 @@ MDGPU_API void mdgpu_destroy(mdgpu_handle h);
  * and warp lists holding each front once, assembly maps and solve task
  * order, the residual's CSR in range.  MDGPU_OK, or MDGPU_ERR_INVALID with
  * the failed invariant and its front in mdgpu_last_error().  Host only.
+ * With the environment variable MDGPU_CHECK_PLAN=1 every analysis runs the
+ * same check before its tables reach the device, and fails if it fails.
  */
 MDGPU_API int mdgpu_check_plan(mdgpu_handle h);
 

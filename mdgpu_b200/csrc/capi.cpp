@@ -8,6 +8,7 @@
 #include <climits>
 #include <cstdio>
 #include <map>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -233,6 +234,14 @@ cudaGraphExec_t capture(mdgpu_handle_s* h, F&& fn) {
 }
 
 void upload_plan(mdgpu_handle_s* h) {
+    // MDGPU_CHECK_PLAN=1: check every table the kernels index by before any
+    // of it reaches the device (the analysis fails with the broken invariant)
+    if (const char* e = std::getenv("MDGPU_CHECK_PLAN"); e && e[0] == '1') {
+        const std::string why =
+            check_plan(h->plan, h->sym, h->ssched, h->level, h->h_csr_rowptr, h->h_csr_col.data(),
+                       h->h_csr_src.data(), (int64_t)h->h_csr_col.size());
+        if (!why.empty()) throw std::runtime_error("plan check: " + why);
+    }
     if (!device_available()) return;
     init_kernels_once();
     ck(cudaGetDevice(&h->device), "cudaGetDevice");

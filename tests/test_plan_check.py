@@ -107,3 +107,18 @@ def test_random_patterns_pass_the_check(seed):
                {"ordering": M.ORDER_NATURAL}):
         S = M.Solver(n, Ap, Ai, **kw)
         S.check_plan()
+
+
+def test_check_before_upload_when_asked():
+    """MDGPU_CHECK_PLAN=1 runs the check inside every analysis, before the
+    tables would reach the device."""
+    import sys
+
+    code = ("import mdgpu_b200 as M; from mdgpu_b200 import matgen as mg; "
+            "M.Solver(*mg.laplacian_3d_varcoef(14, seed=1)[:3]); "
+            "M.Solver.batch([mg.laplacian_2d_5pt(9)[:3], mg.laplacian_2d_5pt(6)[:3]]); "
+            "print('analysed')")
+    env = dict(os.environ, MDGPU_CHECK_PLAN="1", PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                         timeout=300, check=True).stdout
+    assert "analysed" in out
