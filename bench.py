@@ -38,24 +38,24 @@ METRIC = "factor+solve time & GFLOP/s, FP32+IR vs FP64 on B200 at backward error
 UNIT = "GFLOP/s"
 REF_SIDE = 28  # CPU sample of the reference arm (the full 64^3 takes ~12 min on one core)
 CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, one ncu pass
-# over every launch) of each kernel class in one FP32 bench step at side 64,
-# bytes per step; profiles/dram_traffic_fp32_step_3d64.md holds the capture
-# and its command.  The roofline line divides it by the class's launches.
-TRAFFIC_PER_STEP_3D64 = {
-    "small_front": 509384192, "assemble": 7672552960, "potrf": 12531456, "trsm": 2301383680,
-    "schur_update": 15850466816, "solve_small": 672695552, "solve_large": 6323437056,
-}
+# DRAM traffic per algorithmic byte of each kernel class's dominant kernel:
+# dram__bytes_read.sum + dram__bytes_write.sum of single launches captured by
+# ncu on a 48^3 step (one kernel, a few launches, --clock-control none),
+# divided by the same launches' algorithmic bytes.  The roofline line scales
+# the class's algorithmic bytes per launch at the bench size by it (traffic
+# grows with the units processed); None where no capture exists.
+TRAFFIC_PER_ALGO_BYTE = {}
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
     "small_front": ["k_tiny_fronts", "k_small_front"],
     "assemble": ["k_big_assemble_warp"],
     "potrf": ["k_tile_potrf"],
-    "trsm": ["k_tile_trsm", "k_tile_update"],
+    "panel": ["k_panel"],
     "schur_update": ["k_schur_tc"],
     "solve_small": ["k_fwd_level", "k_bwd_level"],
     "solve_large": ["k_fwd_level", "k_bwd_level"],
 }
+CLASS_KERNELS_FP64 = dict(CLASS_KERNELS, schur_update=["k_schur_f64"])
 
 
 def parse():
@@ -331,6 +331,69 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def measure_fp64_gemm_tflops():
+    """Dense FP64 throughput of this GPU, measured: a cuBLAS DGEMM (torch,
+    8192^3) timed with CUDA events after warm-up (the denominator of the FP64
+    Schur update's roofline; the measured-peaks file holds HBM and bf16
+    figures only)."""
+    import torch
+
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    bm = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, bm)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(a, bm)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, bm
+    return 2.0 * 8192 ** 3 / (ms * 1e-3) / 1e12
+
+
+def roofline(prof, cls, peaks, peak_src, fp64_peak, class_kernels):
+    """Roofline figures of one kernel class from a profiled step: achieved =
+    algorithmic flops (tensor- or FP64-bound classes) or bytes per launch /
+    the class's mean launch time (CUDA events on the launching stream).
+    Peaks: 3xTF32 = sustained dense bf16 / 2 (TF32 rate) / 3 (three products
+    per FP32 product); FP64 = the measured DGEMM rate; HBM = measured copy
+    bandwidth."""
+    if cls is None or cls not in prof["classes"]:
+        return None
+    c = prof["classes"][cls]
+    per_launch_s = c["ms"] / c["launches"] * 1e-3
+    if fp64_peak is not None and cls == "schur_update":
+        peak, unit, bound = fp64_peak, "TFLOP/s", "fp64"
+        achieved = c["flops"] / c["launches"] / per_launch_s / 1e12
+        note = "measured cuBLAS DGEMM (8192^3) on this GPU; algorithmic FP64 flops"
+    elif c["bound"] == "tensor":
+        bf16 = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+        peak, unit, bound = bf16 / 2.0 / 3.0, "TFLOP/s", "tensor"
+        achieved = c["flops"] / c["launches"] / per_launch_s / 1e12
+        note = ("3xTF32 ceiling = %s sustained dense bf16 / 2 / 3; algorithmic FP32 flops"
+                % peak_src)
+    else:
+        peak, unit, bound = peaks["hbm_gbs"], "GB/s", "hbm"
+        achieved = c["bytes"] / c["launches"] / per_launch_s / 1e9
+        note = "%s HBM copy bandwidth; algorithmic bytes" % peak_src
+    ratio = TRAFFIC_PER_ALGO_BYTE.get(cls)
+    traffic = ratio * c["bytes"] / c["launches"] if ratio is not None else None
+    return {"kernel": cls, "kernels": class_kernels.get(cls, []), "bound": bound,
+            "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": c["bytes"] / c["launches"],
+            "flops_per_launch": c["flops"] / c["launches"],
+            "traffic_source": ("ncu DRAM bytes per algorithmic byte of single launches on a "
+                               "48^3 step, times this launch's algorithmic bytes"
+                               if ratio is not None else None),
+            "peak_source": note, "launches": c["launches"], "ms_total": c["ms"]}
+
+
 def run_gpu_arm(args):
     import torch
 
@@ -418,21 +481,44 @@ def run_gpu_arm(args):
     sampler.start()
     t32, (berr32, it32) = timed(step_fp32, args.steps, args.warmup)
     clocks = sampler.stop()
+    x32 = dx.cpu().numpy()
     free_d, _ = torch.cuda.mem_get_info()
-    t64, (berr64, _) = timed(step_fp64, max(1, min(args.steps, 3)), 1)
+    # the plain FP64 factor + solve: the same steps, warm-up and clock record
+    sampler64 = ClockSampler(local)
+    sampler64.start()
+    t64, (berr64, _) = timed(step_fp64, args.steps, args.warmup)
+    clocks64 = sampler64.stop()
+    x64 = dx.cpu().numpy()
     free_e, _ = torch.cuda.mem_get_info()
     hbm = {"plan": int(free_a - free_b), "fp32_factor_and_solve": int(free_c - free_d),
            "fp64_factor_added": int(free_d - free_e),
            "handle_total": int((free_a - free_b) + (free_c - free_e)),
            "lstore_bytes_fp64": int(S.info("lstore_bytes")),
            "ustore_bytes_fp64": int(S.info("ustore_bytes")),
-           "note": "cudaMemGetInfo deltas (2 MiB granularity)"}
+           "ustore_bytes_fp64_without_reuse": int(S.info("ustore_total_bytes")),
+           "note": "cudaMemGetInfo deltas (2 MiB granularity); the update-matrix store "
+                   "is reused over the matrices' lifetimes in the level schedule"}
     ms32 = allmax(statistics.mean(t32))
     ms64 = allmax(statistics.mean(t64))
 
-    # kernel-level evidence for the roofline: the dominant kernel class, timed
-    # with CUDA events around each of its launches during one extra step
+    # kernel-level evidence for the roofline: every kernel class, timed with
+    # CUDA events around each of its launches during one extra step of each
+    # precision
     prof = S.profile_step(lambda: step_fp32())
+    prof64 = S.profile_step(lambda: step_fp64())
+
+    # accuracy on the host, independent of the library's residual kernel:
+    # backward error ||b - A x||inf / (||A||inf ||x||inf + ||b||inf) by a
+    # scipy product with the caller's values, forward error against the
+    # plain FP64 GPU solution
+    A_full = mg.lower_to_full_scipy(n, Ap, Ai, Ax)
+    a_inf = float(abs(A_full).sum(axis=1).max())
+
+    def host_berr(x):
+        return float(np.abs(b - A_full @ x).max() / (a_inf * np.abs(x).max() + np.abs(b).max()))
+
+    def fwd_err(x):
+        return float(np.abs(x - x64).max() / np.abs(x64).max())
 
     # end to end through the public API with host buffers
     Axh = np.ascontiguousarray(Ax)
@@ -460,10 +546,15 @@ def run_gpu_arm(args):
             S.factor(dAx, M.FP32, stream=sptr)
             return S.refine_device(dB64, dX64, tol=1e-14, maxit=30, stream=sptr)
 
-        t64, (be64, it64) = timed(step_fp32_64, max(1, min(args.steps, 3)), 1)
-        ms64r = allmax(statistics.mean(t64))
+        t64r, (be64, it64) = timed(step_fp32_64, max(1, min(args.steps, 3)), 1)
+        ms64r = allmax(statistics.mean(t64r))
+        X64 = dX64.cpu().numpy()
+        R = B64 - A_full @ X64
+        be_host = (np.abs(R).max(axis=0) /
+                   (a_inf * np.abs(X64).max(axis=0) + np.abs(B64).max(axis=0)))
         rhs64 = {"nrhs": 64, "ms_per_step": ms64r,
-                 "max_backward_error": float(np.max(be64)), "ir_iterations": int(it64),
+                 "max_backward_error": float(np.max(be64)),
+                 "max_backward_error_host": float(be_host.max()), "ir_iterations": int(it64),
                  "solve_flops_per_rhs_sweep_pair": 4.0 * S.info("lnz"),
                  "note": "FP32 factor + FP64 refinement of 64 columns at once"}
 
@@ -478,9 +569,11 @@ def run_gpu_arm(args):
 
         try:
             tg, (beg, itg, ing) = timed(step_fp32_gmres, max(1, min(args.steps, 3)), 1)
+            xg = dx.cpu().numpy()
             gmres = {"ms_per_step": allmax(statistics.mean(tg)),
-                     "backward_error": float(np.max(beg)), "corrections": int(np.max(itg)),
-                     "gmres_steps": int(np.sum(ing)),
+                     "backward_error": float(np.max(beg)),
+                     "backward_error_host": host_berr(xg), "forward_error": fwd_err(xg),
+                     "corrections": int(np.max(itg)), "gmres_steps": int(np.sum(ing)),
                      "note": "FP32 factor + GMRES-IR (restart 30, inner tolerance 1e-8)"}
         except Exception as e:  # noqa: BLE001
             gmres = {"error": str(e)[:300]}
@@ -490,8 +583,8 @@ def run_gpu_arm(args):
             dist.destroy_process_group()
         return
     peaks, peak_src = measured_peaks()
+    fp64_peak = measure_fp64_gemm_tflops()
     value = world * flops / (ms32 * 1e-3) / 1e9
-    dom = prof["dominant"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
@@ -502,10 +595,15 @@ def run_gpu_arm(args):
                                 "parallelism": "replicas x%d (a single system does not shard)"
                                                % world,
                                 "analyze_s": t_analyze}),
-        "backward_error": float(berr32[0]), "ir_iterations": int(it32),
+        "backward_error": float(berr32[0]), "backward_error_host": host_berr(x32),
+        "forward_error": fwd_err(x32), "ir_iterations": int(it32),
         "fp64": {"ms_per_step": ms64, "value": world * flops / (ms64 * 1e-3) / 1e9,
-                 "backward_error": float(berr64[0]),
-                 "speedup_fp32_ir_over_fp64": ms64 / ms32},
+                 "steps": args.steps, "warmup": args.warmup,
+                 "backward_error": float(berr64[0]), "backward_error_host": host_berr(x64),
+                 "speedup_fp32_ir_over_fp64": ms64 / ms32, "clocks": clocks64,
+                 "kernels": prof64["classes"],
+                 "roofline": roofline(prof64, "schur_update", peaks, peak_src, fp64_peak,
+                                      CLASS_KERNELS_FP64)},
         "e2e": {"value": world * flops / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
                 "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(Ax.nbytes + b.nbytes),
@@ -515,40 +613,9 @@ def run_gpu_arm(args):
         "hbm_bytes": hbm,
         "gpu_launches": prof["launches_per_step"],
         "clocks": clocks,
-        "roofline": None,
+        "roofline": roofline(prof, prof["dominant"], peaks, peak_src, None, CLASS_KERNELS),
         "kernels": prof["classes"],
     }
-    if dom is not None:
-        c = prof["classes"][dom]
-        if c["bound"] == "tensor":
-            # FP32 products as three TF32 MMAs (hi*hi + hi*lo + lo*hi): the
-            # ceiling for delivered FP32 flops is the TF32 rate / 3, and the
-            # TF32 dense rate is half the bf16 rate; sustained figure (the
-            # kernel runs inside a long step)
-            bf16 = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
-            peak = bf16 / 2.0 / 3.0
-            achieved = c["flops"] / c["launches"] / (c["ms"] / c["launches"] * 1e-3) / 1e12
-            unit = "TFLOP/s"
-            note = ("3xTF32 ceiling = %s sustained dense bf16 / 2 / 3; algorithmic FP32 flops"
-                    % peak_src)
-        else:
-            peak = peaks["hbm_gbs"]
-            achieved = c["bytes"] / c["launches"] / (c["ms"] / c["launches"] * 1e-3) / 1e9
-            unit = "GB/s"
-            note = "%s HBM copy bandwidth" % peak_src
-        traffic = None
-        if side == 64 and dom in TRAFFIC_PER_STEP_3D64:
-            traffic = TRAFFIC_PER_STEP_3D64[dom] / c["launches"]
-        line["roofline"] = {"kernel": dom, "kernels": CLASS_KERNELS.get(dom, []),
-                            "bound": c["bound"], "achieved": achieved,
-                            "peak": peak, "unit": unit, "frac": achieved / peak,
-                            "traffic": traffic,
-                            "algorithmic_bytes_per_launch": c["bytes"] / c["launches"],
-                            "flops_per_launch": c["flops"] / c["launches"],
-                            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                              "one pass over the same workload (bytes per launch)",
-                            "peak_source": note, "launches": c["launches"],
-                            "ms_total": c["ms"]}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = reference_cpu_sample(CPU_BASELINE_SIDE)
     print(json.dumps(line), flush=True)
@@ -782,8 +849,10 @@ def run_adjoint_arm(args):
             "fd_edges": 64, "fd_max_rel_err": worst,
             "hbm_bytes": {"after_forward": int(free0 - free1),
                           "backward_extra": int(free1 - free2),
-                          "note": "the selected inverse's update part reuses the factor's "
-                                  "update-matrix store; nothing is recomputed"}}
+                          "zustore_bytes": int(S.info("zustore_bytes")),
+                          "note": "the selected inverse's update parts have their own store, "
+                                  "reused over their top-down lifetimes; nothing is "
+                                  "recomputed"}}
     print(json.dumps(line), flush=True)
 
 

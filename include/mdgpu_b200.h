@@ -131,7 +131,10 @@ MDGPU_API int mdgpu_check_plan(mdgpu_handle h);
 
 /* Scalars: "n", "nsuper", "lnz", "nlevels", "nnz", "max_front", "flops"
  * (the reference's own count, mdgpu.cu:1354-1359), "lstore_bytes",
- * "ustore_bytes", "rows_total", "nchild", "large_fronts", "small_fronts",
+ * "ustore_bytes" (the update-matrix store, reused over the matrices'
+ * lifetimes), "ustore_total_bytes" (the sum of every update matrix: the store
+ * without reuse), "zustore_bytes" (the selected inverse's update parts),
+ * "rows_total", "nchild", "large_fronts", "small_fronts",
  * "nsys", "solve_work_rows", "amap_rows", "amap_entries". */
 MDGPU_API int mdgpu_info(mdgpu_handle h, const char *key, long long *value);
 
@@ -187,8 +190,11 @@ MDGPU_API int mdgpu_solve_device(mdgpu_handle h, const double *dB, int ldb, doub
  * sums), one more when n x min(nrhs, 64) is odd; larger requests return
  * MDGPU_ERR_INVALID.  All calls share the
  * array: calls whose work overlaps on one GPU race and must be serialized by
- * the caller.  The first call on a device looks up the array's address; make
- * it before any stream capture.
+ * the caller.  The analysis (mdgpu_analyze and the other analyze entries)
+ * looks up the array's address on the handle's device, which loads the
+ * array's module and commits its memory then, so a solve does no module
+ * load; should that look-up fail there, the first call on the device makes
+ * it: make that first call before any stream capture.
  */
 MDGPU_API int mdgpu_solve_device_noalloc(mdgpu_handle h, const double *dB, int ldb, double *dX,
                                          int ldx, int nrhs, void *stream);

@@ -32,13 +32,13 @@ EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_
            "mdgpu_last_error", "mdgpu_load_triplet", "mdgpu_logdet", "mdgpu_selinv",
            "mdgpu_grad_lower", "mdgpu_grad_lower_device")
 
-KERNEL_CLASSES = ("small_front", "assemble", "potrf", "trsm", "schur_update", "solve_small",
+KERNEL_CLASSES = ("small_front", "assemble", "potrf", "panel", "schur_update", "solve_small",
                   "solve_large", "other")
 # the roofline each class is measured against: the tensor pipes for the
 # trailing (Schur) updates, HBM for the rest -- the diagonal-tile factor and
 # the in-panel tile steps read and write 64 x 64 tiles, and their distance
 # from streaming speed is the latency of the dependency chain
-KERNEL_BOUND = {"small_front": "hbm", "assemble": "hbm", "potrf": "hbm", "trsm": "hbm",
+KERNEL_BOUND = {"small_front": "hbm", "assemble": "hbm", "potrf": "hbm", "panel": "hbm",
                 "schur_update": "tensor", "solve_small": "hbm", "solve_large": "hbm",
                 "other": "hbm"}
 

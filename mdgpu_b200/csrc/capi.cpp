@@ -91,7 +91,6 @@ struct mdgpu_handle_s {
     // batch of independent systems (mdgpu_analyze_batch): per system its first
     // row and its first entry in the concatenated lower-triangle values
     std::vector<int> sys_row_off, sys_val_off;
-    std::vector<int64_t> pscr_off;  // panel scratch offset per supernode
     PanelSchedule pschedh;
     bool use_tensor_cores = true;
     DevPlan D;
@@ -121,8 +120,9 @@ struct mdgpu_handle_s {
     cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
     std::map<int, cudaGraphExec_t> sgraph;  // key: precision * 1024 + rhs count
     int factored = -1;  // precision of the current factor, -1 none
-    bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dU64
+    bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dZu64
     double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
+    double* dZu64 = nullptr;       // its update parts (plan.zuoff offsets)
     double* d_Y = nullptr;         // its Y scratch
     double* d_logdet = nullptr;    // logdet partial sums, then the result
     double* d_gx = nullptr;        // gradient: x and G on the device (host entry)
@@ -151,7 +151,7 @@ struct mdgpu_handle_s {
             if (g) cudaGraphExecDestroy(g);
         drop_solve_graphs();
         for (void* p : owned) cudaFree(p);
-        for (void* p : {(void*)dZ64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG,
+        for (void* p : {(void*)dZ64, (void*)dZu64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG,
                         (void*)d_gm})
             if (p) cudaFree(p);
         for (void* p : {(void*)d_Ax, (void*)dL64, (void*)dU64, (void*)dL32, (void*)dU32,
@@ -216,6 +216,7 @@ void init_kernels_once() {
     init_solve_kernels();
     init_schur_tc();
     init_schur_f64();
+    init_panel_kernels();
     done = true;
 }
 
@@ -233,18 +234,30 @@ cudaGraphExec_t capture(mdgpu_handle_s* h, F&& fn) {
     return ex;
 }
 
-void upload_plan(mdgpu_handle_s* h) {
-    // MDGPU_CHECK_PLAN=1: check every table the kernels index by before any
-    // of it reaches the device (the analysis fails with the broken invariant)
-    if (const char* e = std::getenv("MDGPU_CHECK_PLAN"); e && e[0] == '1') {
-        const std::string why =
+void upload_plan(mdgpu_handle_s* h, bool check = false) {
+    // check (or MDGPU_CHECK_PLAN=1): check every table the kernels index by
+    // before any of it reaches the device (the analysis fails with the
+    // broken invariant)
+    const char* e = std::getenv("MDGPU_CHECK_PLAN");
+    if (check || (e && e[0] == '1')) {
+        std::string why =
             check_plan(h->plan, h->sym, h->ssched, h->level, h->h_csr_rowptr, h->h_csr_col.data(),
                        h->h_csr_src.data(), (int64_t)h->h_csr_col.size());
+        if (why.empty()) why = check_panel_schedule(h->plan, h->pschedh, h->level, kTile, kPanel);
         if (!why.empty()) throw std::runtime_error("plan check: " + why);
     }
     if (!device_available()) return;
     init_kernels_once();
     ck(cudaGetDevice(&h->device), "cudaGetDevice");
+    ck(cudaDeviceGetAttribute(&h->D.num_sms, cudaDevAttrMultiProcessorCount, h->device),
+       "SM count");
+    {
+        // the no-allocation solve's scratch array: its address on this device
+        // now, so that no solve loads its module (a failure here is reported
+        // by that solve, which retries the look-up)
+        std::string msg;
+        if (!noalloc_scratch(msg)) cudaGetLastError();
+    }
     h->on_device = true;
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
     ck(cudaStreamCreateWithFlags(&h->D.aux, cudaStreamNonBlocking), "stream");
@@ -285,21 +298,6 @@ void upload_plan(mdgpu_handle_s* h) {
     D.fv_total = D.fv_pub_off + 2 * (int64_t)h->ssched.nflags * kTile;
     D.fv_off = h->keep(upload(h->ssched.fv_off));
     D.dinv_off = h->keep(upload(P.dinv_off));
-    {
-        // panel scratch: fronts of one level side by side, levels reuse it
-        h->pscr_off.assign(P.nsuper, -1);
-        D.pscr_total = 0;
-        for (int l = 0; l < P.nlevels; ++l) {
-            int64_t off = 0;
-            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-                const int s = P.large_list[q];
-                h->pscr_off[s] = off;
-                off += 2 * (int64_t)panel_mpad(P.fronts[s].m) * kPanel;
-            }
-            D.pscr_total = std::max(D.pscr_total, off);
-        }
-        D.pscr_off = h->keep(upload(h->pscr_off));
-    }
     D.asm_off = h->keep(upload(P.asm_off));
     D.asm_range = h->keep(upload(P.asm_range));
     D.dinv_total = P.dinv_total;
@@ -324,6 +322,11 @@ void upload_plan(mdgpu_handle_s* h) {
             D.yscr_total = std::max(D.yscr_total, off);
         }
         D.yoff = h->keep(upload(yo));
+        {
+            std::vector<int64_t> zo = P.zuoff;
+            if (zo.empty()) zo.assign(1, -1);
+            D.zuoff = h->keep(upload(zo));
+        }
         std::vector<int> af(std::max<size_t>(P.a_src.size(), 1), 0);
         for (int s = 0; s < P.nsuper; ++s)
             for (int e = P.fronts[s].a_beg; e < P.fronts[s].a_end; ++e) af[e] = s;
@@ -339,6 +342,16 @@ void upload_plan(mdgpu_handle_s* h) {
     D.psched.before = h->keep(upload(h->pschedh.store.ctas_before));
     D.psched.h_op_beg = h->pschedh.op_beg;
     D.psched.h_ops = h->pschedh.ops;
+    {
+        std::vector<int> pt = h->pschedh.tasks;
+        if (pt.empty()) pt.assign(2, 0);
+        D.psched.tasks = reinterpret_cast<int2*>(h->keep(upload(pt)));
+        D.fsync_flags = h->pschedh.ncounters;
+        D.nflags_factor = (int)h->pschedh.nflags;
+        D.nfsync = D.fsync_flags + D.nflags_factor + 1;
+        D.fsync = h->keep(dalloc<int>(D.nfsync));
+        ck(cudaMemset(D.fsync, 0, (size_t)D.nfsync * sizeof(int)), "panel sync words");
+    }
     {
         const SolveScheduleHost& SS = h->ssched;
         std::vector<int> tasks = SS.tasks;
@@ -445,12 +458,11 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
     } else {
         if (!h->dL32) {
             h->dL32 = dalloc<float>(P.lstore);
-            // split panel scratch and its TMA descriptors (tensor-core path)
+            // TMA descriptors of the L panels (tensor-core Schur updates)
             if (h->use_tensor_cores && !P.large_list.empty()) {
-                h->D.pscr = h->keep(dalloc<float>(h->D.pscr_total));
                 std::vector<CUtensorMap> maps;
                 std::vector<int> idx;
-                if (build_panel_maps(P, h->D.pscr, h->pscr_off, kPanel, maps, idx) == 0) {
+                if (build_panel_maps(P, h->dL32, maps, idx) == 0) {
                     h->D.tmaps = h->keep(upload(maps));
                     h->D.tmap_idx = h->keep(upload(idx));
                 }
@@ -521,8 +533,9 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
     int col = stat[0];
     if (stat[1] != 0) {
         h->factored = -1;
-        return fail(MDGPU_ERR_CUDA, "tensor-core Schur update: pipeline wait timed out (code " +
-                                        std::to_string(stat[1]) + ")");
+        return fail(MDGPU_ERR_CUDA,
+                    "factor: a device wait timed out (code " + std::to_string(stat[1]) +
+                        ": 1-2 tensor-core pipeline, 3 panel dependency, 4 panel ticket)");
     }
     h->factored = precision;
     h->selinv_done = false;
@@ -1079,6 +1092,66 @@ int mdgpu_analyze_batch(int nsys, const int* n, const int* const* Ap, const int*
     });
 }
 
+namespace {
+
+// The caller's lower triangle and assembly tree, checked before any of it is
+// used as an index (O(n + nnz + nsuper)); empty when valid.  The tree must be
+// the reference's ETree list (etree.h:6-19) in the form Factor consumes it:
+// supernodes of consecutive columns that together cover 0..n-1 once each,
+// listed in postorder (every supernode but the root, the last, is the child
+// of exactly one later supernode), and column counts of a supernodal L
+// (count[j + i] = count[j] - i inside a supernode, count[j] <= n - j).
+std::string validate_tree(int n, const int* Ap, const int* Ai, int nsuper, const int* first_col,
+                          const int* ncols, const int* child_ptr, const int* child,
+                          const int* count) {
+    if (Ap[0] != 0) return "Ap[0] must be 0";
+    for (int j = 0; j < n; ++j) {
+        if (Ap[j + 1] < Ap[j]) return "column pointers decrease at column " + std::to_string(j);
+        for (int p = Ap[j]; p < Ap[j + 1]; ++p)
+            if (Ai[p] < j || Ai[p] >= n)
+                return "entry " + std::to_string(p) + " outside the lower triangle";
+    }
+    if (nsuper > n) return "more supernodes than columns";
+    std::vector<char> covered(n, 0);
+    for (int s = 0; s < nsuper; ++s) {
+        if (first_col[s] < 0 || first_col[s] >= n)
+            return "supernode " + std::to_string(s) + ": first column out of range";
+        if (ncols[s] < 1 || ncols[s] > n - first_col[s])
+            return "supernode " + std::to_string(s) + ": column count out of range";
+        for (int j = first_col[s]; j < first_col[s] + ncols[s]; ++j)
+            if (covered[j]++)
+                return "column " + std::to_string(j) + " belongs to two supernodes";
+    }
+    for (int j = 0; j < n; ++j)
+        if (!covered[j]) return "column " + std::to_string(j) + " belongs to no supernode";
+    for (int j = 0; j < n; ++j)
+        if (count[j] < 1 || count[j] > n - j)
+            return "count[" + std::to_string(j) + "] out of range";
+    for (int s = 0; s < nsuper; ++s)
+        for (int i = 1; i < ncols[s]; ++i)
+            if (count[first_col[s] + i] != count[first_col[s]] - i)
+                return "supernode " + std::to_string(s) + ": column counts are not those of a "
+                       "supernode";
+    if (child_ptr[0] != 0) return "child_ptr[0] must be 0";
+    for (int s = 0; s < nsuper; ++s)
+        if (child_ptr[s + 1] < child_ptr[s])
+            return "child_ptr decreases at supernode " + std::to_string(s);
+    if (child_ptr[nsuper] != nsuper - 1)
+        return "child lists must name every supernode but the root once";
+    std::vector<char> seen(nsuper, 0);
+    for (int s = 0; s < nsuper; ++s)
+        for (int h = child_ptr[s]; h < child_ptr[s + 1]; ++h) {
+            const int ch = child[h];
+            if (ch < 0 || ch >= s)
+                return "child " + std::to_string(ch) + " of supernode " + std::to_string(s) +
+                       " is not an earlier supernode (postorder)";
+            if (seen[ch]++) return "supernode " + std::to_string(ch) + " has two parents";
+        }
+    return std::string();
+}
+
+}  // namespace
+
 int mdgpu_analyze_tree(int n, const int* Ap, const int* Ai, int nsuper, const int* first_col,
                        const int* ncols, const int* child_ptr, const int* child, const int* count,
                        mdgpu_handle* out) {
@@ -1087,6 +1160,9 @@ int mdgpu_analyze_tree(int n, const int* Ap, const int* Ai, int nsuper, const in
         return fail(MDGPU_ERR_INVALID, "bad arguments");
     *out = nullptr;
     return guarded([&]() -> int {
+        const std::string why =
+            validate_tree(n, Ap, Ai, nsuper, first_col, ncols, child_ptr, child, count);
+        if (!why.empty()) return fail(MDGPU_ERR_INVALID, "bad assembly tree: " + why);
         auto* h = new mdgpu_handle_s();
         Symbolic& S = h->sym;
         S.n = n;
@@ -1106,7 +1182,9 @@ int mdgpu_analyze_tree(int n, const int* Ap, const int* Ai, int nsuper, const in
         try {
             finish_plan(h);
             build_csr(h, n, Ap, Ai);
-            upload_plan(h);
+            // a caller's tree: every table the kernels index by is checked
+            // on the host before any of it reaches the device
+            upload_plan(h, true);
         } catch (...) {
             delete h;
             throw;
@@ -1131,6 +1209,13 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "flops") *value = (long long)P.flops;
     else if (k == "lstore_bytes") *value = P.lstore * 8;
     else if (k == "ustore_bytes") *value = P.ustore * 8;
+    else if (k == "zustore_bytes") *value = P.zustore * 8;
+    else if (k == "ustore_total_bytes") {
+        long long t = 0;
+        for (const FrontDesc& f : P.fronts)
+            if (f.uoff >= 0) t += ((long long)f.ldu * (f.m - f.c) + 31) / 32 * 32;
+        *value = t * 8;
+    }
     else if (k == "rows_total") *value = (long long)P.rows.size();
     else if (k == "nchild") *value = (long long)P.child.size();
     else if (k == "large_fronts") *value = (long long)P.large_list.size();
@@ -1215,9 +1300,10 @@ int mdgpu_factor(mdgpu_handle h, const double* Ax, int precision, void* stream) 
 int mdgpu_check_plan(mdgpu_handle h) {
     if (!h) return fail(MDGPU_ERR_INVALID, "null handle");
     return guarded([&]() -> int {
-        const std::string why =
+        std::string why =
             check_plan(h->plan, h->sym, h->ssched, h->level, h->h_csr_rowptr, h->h_csr_col.data(),
                        h->h_csr_src.data(), (int64_t)h->h_csr_col.size());
+        if (why.empty()) why = check_panel_schedule(h->plan, h->pschedh, h->level, kTile, kPanel);
         if (!why.empty()) return fail(MDGPU_ERR_INVALID, "plan check: " + why);
         return MDGPU_OK;
     });
@@ -1374,9 +1460,10 @@ int mdgpu_selinv(mdgpu_handle h, void* stream) {
         cudaStream_t st = pick_stream(h, stream);
         ck(cudaSetDevice(h->device), "cudaSetDevice");
         if (!h->dZ64) h->dZ64 = dalloc<double>(h->plan.lstore);
+        if (!h->dZu64) h->dZu64 = dalloc<double>(h->plan.zustore);
         if (!h->d_Y) h->d_Y = dalloc<double>(std::max<int64_t>(h->D.yscr_total, 1));
         NvtxRange nvtx("mdgpu_selinv");
-        launch_selinv(h->D, h->dL64, h->dZ64, h->dU64, h->d_Y, st);
+        launch_selinv(h->D, h->dL64, h->dZ64, h->dZu64, h->d_Y, st);
         ck(cudaGetLastError(), "selected inverse launch");
         ck(cudaStreamSynchronize(st), "selected inverse");
         h->selinv_done = true;

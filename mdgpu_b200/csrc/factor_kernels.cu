@@ -20,6 +20,7 @@
 
 #include "device_common.cuh"
 #include "kernels.hpp"
+#include "tile_ops.cuh"
 
 namespace mdgpu {
 
@@ -388,32 +389,16 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
-// column-major, zero above the diagonal) at Dk.  The 256 threads form a
-// 16 x 16 grid; thread (tr, tc), tr >= tc, keeps the 4 x 4 block (tr, tc) of
-// the tile in registers, and its block of X = inv(L).  Sixteen blocked steps
-// (two barriers each) of right-looking Cholesky with the inverse alongside:
-//   (a) the diagonal owner factors its 4 x 4 block and inverts it (Y);
-//   (b) the owners below it form their panel block A Y'; at the same time
-//       the owners of block row kb of X finalise it, X(kb, tc) = Y x;
-//   (c) every lower block right of the panel takes the rank-4 update; at the
-//       same time the X blocks below take x -= L(tr, kb) X(kb, tc);
-// with L going to S and X to W block by block.  One reciprocal square root
-// per pivot.
-// A partial tile (n < 64) is padded with the identity.  S, W: TB x (TB + 1).
-__device__ __forceinline__ float recip_sqrt(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double recip_sqrt(double x) { return rsqrt(x); }
-
+// column-major, zero above the diagonal) at Dk (potrf_tile_core on a copy in
+// shared memory; a partial tile (n < 64) is padded with the identity).
+// S, W: TB x (TB + 1).
 template <typename T, int TB>
 __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
                                 int* status) {
-    static_assert(TB == 64, "16 x 16 grid of 4 x 4 blocks over 256 threads");
-    constexpr int LD = TB + 1, B = 4, NB = TB / B;
+    constexpr int LD = TB + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int tr = tid & (NB - 1), tc = tid >> 4;
-    const bool low = tr >= tc;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
-    const int col0 = f.first_col + tk.start;
     T* base = Ls + f.loff + tk.start + (int64_t)tk.start * f.ldl;
     for (int idx = tid; idx < TB * TB; idx += nt) {
         int j = idx / TB, i = idx - j * TB;
@@ -421,135 +406,7 @@ __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T
         if (i < n && j < n && i >= j) v = base[i + (int64_t)j * f.ldl];
         S[i + j * LD] = v;
     }
-    __syncthreads();
-    T a[B][B], x[B][B];  // this thread's block of A -> L, and of inv(L)
-#pragma unroll
-    for (int r = 0; r < B; ++r)
-#pragma unroll
-        for (int c = 0; c < B; ++c) {
-            a[r][c] = low ? S[(B * tr + r) + (B * tc + c) * LD] : T(0);
-            x[r][c] = (tr == tc && r == c) ? T(1) : T(0);
-        }
-    __syncthreads();
-#pragma unroll 1
-    for (int kb = 0; kb < NB; ++kb) {
-        if (tr == kb && tc == kb) {  // (a) L_kk and its inverse Y = X(kb, kb)
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-                const T piv = a[i][i];
-                if (B * kb + i < n && !(piv > T(0))) flag_pivot(status, col0 + B * kb + i);
-                // one reciprocal square root per pivot: d = piv / sqrt(piv)
-                const T rd = recip_sqrt(piv);
-                const T d = piv * rd;
-                a[i][i] = d;
-                x[i][i] = rd;  // diagonal of Y
-#pragma unroll
-                for (int r = i + 1; r < B; ++r) a[r][i] *= rd;
-#pragma unroll
-                for (int r = i + 1; r < B; ++r)
-#pragma unroll
-                    for (int c = i + 1; c <= r; ++c) a[r][c] -= a[r][i] * a[c][i];
-            }
-            // Y = inv(L_kk) by forward substitution, column by column
-#pragma unroll
-            for (int c = 0; c < B; ++c)
-#pragma unroll
-                for (int r = c + 1; r < B; ++r) {
-                    T v = T(0);
-#pragma unroll
-                    for (int m = c; m < r; ++m) v -= a[r][m] * x[m][c];
-                    x[r][c] = v * x[r][r];
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    S[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? a[r][c] : T(0);
-                    W[(B * kb + r) + (B * kb + c) * LD] = (c <= r) ? x[r][c] : T(0);
-                }
-        }
-        __syncthreads();
-        if (tc == kb && tr > kb) {  // (b) panel block: A Y'
-            T y[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) y[r][c] = W[(B * kb + r) + (B * kb + c) * LD];
-            T o[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    T v = T(0);
-#pragma unroll
-                    for (int m = 0; m <= c; ++m) v += a[r][m] * y[c][m];
-                    o[r][c] = v;
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    a[r][c] = o[r][c];
-                    S[(B * tr + r) + (B * kb + c) * LD] = o[r][c];
-                }
-        } else if (tr == kb && tc < kb) {  // (b) inverse block row kb: X = Y x
-            T y[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) y[r][c] = W[(B * kb + r) + (B * kb + c) * LD];
-            T o[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    T v = T(0);
-#pragma unroll
-                    for (int m = 0; m <= r; ++m) v += y[r][m] * x[m][c];
-                    o[r][c] = v;
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    x[r][c] = o[r][c];
-                    W[(B * kb + r) + (B * tc + c) * LD] = o[r][c];
-                }
-        }
-        __syncthreads();
-        if (tc > kb && low) {  // (c) trailing update with the panel
-            T p[B][B], q[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int m = 0; m < B; ++m) {
-                    p[r][m] = S[(B * tr + r) + (B * kb + m) * LD];
-                    q[r][m] = S[(B * tc + r) + (B * kb + m) * LD];
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c)
-#pragma unroll
-                    for (int m = 0; m < B; ++m) a[r][c] -= p[r][m] * q[c][m];
-        } else if (tr > kb && tc <= kb) {  // (c) inverse rows below: x -= L(tr, kb) X(kb, tc)
-            T p[B][B], q[B][B];
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int m = 0; m < B; ++m) {
-                    p[r][m] = S[(B * tr + r) + (B * kb + m) * LD];
-                    q[m][r] = W[(B * kb + m) + (B * tc + r) * LD];
-                }
-#pragma unroll
-            for (int r = 0; r < B; ++r)
-#pragma unroll
-                for (int c = 0; c < B; ++c)
-#pragma unroll
-                    for (int m = 0; m < B; ++m) x[r][c] -= p[r][m] * q[m][c];
-        }
-    }
-    __syncthreads();
+    potrf_tile_core<T, TB>(S, W, n, f.first_col + tk.start, status);
     for (int idx = tid; idx < TB * TB; idx += nt) {
         int j = idx / TB, i = idx - j * TB;
         if (i < n && j < n && i >= j) base[i + (int64_t)j * f.ldl] = S[i + j * LD];
@@ -571,43 +428,13 @@ __global__ void __launch_bounds__(256)
     potrf_diag_tile<T, TB>(f, k, Ls, Dinv + dinv_off[s] + (int64_t)k * TB * TB, S, W, status);
 }
 
-// C (TB x TB, tile (i, j) of front f) -= A B' with A = rows of tile i and
-// B = rows of tile j, both over the K columns of panel tile k; 256 threads,
-// 4 x 4 outputs each.  As/Bs: K x TB staging in shared memory.
-template <typename T, int TB>
-__device__ void tile_gemm_nt_acc(const T* As, const T* Bs, int K, T (&acc)[4][4]) {
-    const int tid = threadIdx.x;
-    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-    for (int q = 0; q < K; ++q) {
-        T av[4], bv[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) av[a] = As[q * TB + r0 + a];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = Bs[q * TB + c0 + b];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
-    }
-}
-
 // X = A_ik inv(L_kk)' in place, CTA per row tile below the panel tile.
-// With a panel scratch (FP32 tensor-core path) X also goes there split for
-// the 3xTF32 Schur update: hi = X with the low 13 mantissa bits cleared (an
-// exact TF32 value), lo = X - hi (exact in FP32); the tile's columns past
-// the last pivot column are written as zeros there, so the update's last
-// K chunk adds nothing.
 template <typename T, int TB>
 __global__ void __launch_bounds__(256)
     k_tile_trsm(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                 const int* __restrict__ before, int nitems, int k,
                 const int64_t* __restrict__ dinv_off, T* __restrict__ Ls,
-                const T* __restrict__ Dinv, float* __restrict__ pscr,
-                const int64_t* __restrict__ pscr_off) {
+                const T* __restrict__ Dinv) {
     static_assert(TB == 64, "4x4 register tile over 256 threads assumes TB = 64");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* As = reinterpret_cast<T*>(smem_raw);  // [K][TB]
@@ -639,27 +466,6 @@ __global__ void __launch_bounds__(256)
         for (int a = 0; a < 4; ++a) {
             int rr = r0 + a;
             if (rr < ti.size) aik[rr + (int64_t)cc * f.ldl] = acc[a][b];
-        }
-    }
-    if constexpr (sizeof(T) == 4) {
-        if (pscr) {
-            const int mpad = panel_mpad(f.m);
-            const int kk0 = (k % (kPanel / TB)) * TB;  // panel column of the tile's first
-            float* hi = pscr + pscr_off[s] + (int64_t)kk0 * (2 * mpad) + ti.start;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int cc = c0 + b;
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const int rr = r0 + a;
-                    if (rr >= ti.size) continue;
-                    const float x = cc < K ? acc[a][b] : 0.f;
-                    const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
-                    float* p = hi + (int64_t)cc * (2 * mpad) + rr;
-                    p[0] = h;
-                    p[mpad] = x - h;
-                }
-            }
         }
     }
 }
@@ -818,7 +624,7 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
             ProfScope ps(D.prof, KC_TRSM, st);
             k_tile_trsm<T, kTile><<<tr.nctas, 256, gsm, st>>>(
                 D.fronts, S.items + tr.off, S.before + tr.off, tr.nitems, tr.step, D.dinv_off, Ls,
-                Dinv, nullptr, nullptr);
+                Dinv);
         }
         if (up.nctas > 0) {
             ProfScope ps(D.prof, KC_SCHUR, st, D.h_update_flops[q]);
@@ -829,11 +635,13 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
     }
 }
 
-// Large fronts in 256-column panels: inside a panel the 64-wide tile steps
-// (TRSM, in-panel updates, fused diagonal POTRF); after it one wide Schur
-// update of the whole trailing part -- tcgen05 tensor cores (TF32) for FP32,
-// the register-tiled FP64 kernel for FP64.  status[1] receives the
-// tensor-core kernel's error code (pipeline wait timeout).
+// Large fronts in 256-column panels: per panel one launch of dependency-
+// ordered row-tile tasks (k_panel: diagonal tiles, triangular solves and the
+// panel's own updates), then one wide Schur update of the whole trailing
+// part -- tcgen05 tensor cores (TF32) for FP32, the register-tiled FP64
+// kernel for FP64.  status[1] receives a device wait's error code (1, 2:
+// the tensor-core pipeline; 3: a panel dependency wait; 4: a panel ticket
+// counter not cleared).
 template <typename T>
 static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv,
                                       const double* Ax, int* status, cudaStream_t st) {
@@ -842,7 +650,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
     for (int q = S.h_op_beg[level]; q < S.h_op_beg[level + 1]; ++q) {
         const PanelOp& op = S.h_ops[q];
         const WorkList& w = op.w;
-        if (w.nctas == 0) continue;
+        if (op.kind == OP_PANEL ? op.ntasks == 0 : w.nctas == 0) continue;
         switch (op.kind) {
             case OP_ASSEMBLE: {
                 ProfScope ps(D.prof, KC_ASSEMBLE, st, 0, op.elems * sizeof(T) + op.xbytes);
@@ -865,7 +673,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
                 k_tile_trsm<T, kTile><<<w.nctas, 256, gsm, st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, D.dinv_off, Ls,
-                    Dinv, sizeof(T) == 4 ? D.pscr : nullptr, D.pscr_off);
+                    Dinv);
                 break;
             }
             case OP_UPDATE_PANEL: {
@@ -873,6 +681,11 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 k_tile_update<T, kTile><<<w.nctas, 256, gsm, st>>>(
                     D.fronts, S.items + w.off, S.before + w.off, w.nitems, op.arg, op.arg2,
                     D.dinv_off, Ls, Us, Dinv, status);
+                break;
+            }
+            case OP_PANEL: {
+                ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
+                launch_panel<T>(D, op, Ls, Dinv, status, st);
                 break;
             }
             case OP_SCHUR_TC: {
@@ -917,6 +730,7 @@ template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
                    cudaStream_t st) {
     const bool fork = D.aux && D.fork_ev && D.join_ev && !(D.prof && D.prof->on);
+    if (D.fsync && D.nfsync > 0) cudaMemsetAsync(D.fsync, 0, (size_t)D.nfsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
         const bool has_small =
             D.h_small_ptr[(l + 1) * kSmallBuckets] > D.h_small_ptr[l * kSmallBuckets];

@@ -18,7 +18,7 @@ enum KernelClass {
     KC_SMALL_FRONT = 0,  // fused small-front factor
     KC_ASSEMBLE,         // large-front assembly
     KC_POTRF,            // first diagonal tile of large fronts
-    KC_TRSM,             // panel triangular solves
+    KC_TRSM,             // panel factorization (diagonal tiles, triangular solves, in-panel updates)
     KC_SCHUR,            // Schur-complement tile updates (dominant flops)
     KC_SOLVE_SMALL,      // small-front forward/backward sweeps
     KC_SOLVE_LARGE,      // large-front forward/backward steps
@@ -82,6 +82,7 @@ constexpr int kPanel = 256;        // FP32 path: pivot columns per tensor-core S
 struct DevSchedule {
     int* items = nullptr;
     int* before = nullptr;
+    int2* tasks = nullptr;  // OP_PANEL tasks (front, row tile)
     std::vector<int> h_level_beg;
     std::vector<WorkList> h_trsm, h_update;
     // panel schedule (FP32): per level a run of operations
@@ -118,6 +119,7 @@ struct SolveSchedule {
 
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
+    int num_sms = 0;  // of the handle's device (persistent grids)
     // a second stream and two events: the factor runs a level's small fronts
     // beside its large fronts (both depend only on lower levels)
     cudaStream_t aux = nullptr;
@@ -136,6 +138,7 @@ struct DevPlan {
     int* level_list = nullptr;
     std::vector<int> h_level_ptr;  // nlevels + 1
     int64_t* yoff = nullptr;
+    int64_t* zuoff = nullptr;  // per supernode: Z's update part in the selinv Zu store
     int64_t yscr_total = 0;
     int* a_front = nullptr;
     int* a_colptr = nullptr;
@@ -147,19 +150,19 @@ struct DevPlan {
     int* asm_off = nullptr;       // per supernode: child column ranges (large fronts)
     int* asm_range = nullptr;
     int64_t dinv_total = 0;
-    // FP32 path: per large front a TMA descriptor of its L panel, and the
-    // panel-wise schedule whose Schur updates run on the tensor cores
+    // FP32 path: per large front a TMA descriptor of its L panel (the
+    // operands of the tensor-core Schur updates)
     CUtensorMap* tmaps = nullptr;
     int* tmap_idx = nullptr;
-    // FP32 path: the current panel of every large front of a level, split
-    // for the 3xTF32 products: per front 2 * mpad x kPanel floats (column
-    // kk: rows [0, mpad) the TF32 part hi, rows [mpad, 2 mpad) lo = x - hi),
-    // mpad = m rounded up to 128; written by the panel's TRSMs, read by the
-    // tensor-core Schur update through tmaps
-    float* pscr = nullptr;
-    int64_t* pscr_off = nullptr;  // per supernode (-1 if small)
-    int64_t pscr_total = 0;
     DevSchedule psched;
+    // sync words of the panel launches, cleared at the start of every
+    // factor: one ticket counter per OP_PANEL launch, then one flag per pivot
+    // tile of the large fronts (flag of tile k of front s at fsync_flags +
+    // dinv_off[s] / kTile^2 + k), then the abort word
+    int* fsync = nullptr;
+    int nfsync = 0;
+    int fsync_flags = 0;
+    int nflags_factor = 0;
     std::vector<int> h_small_ptr, h_large_ptr;
     std::vector<WorkList> h_assemble;  // per level, offsets into sched64 arrays
     DevSchedule sched64;
@@ -181,6 +184,7 @@ void init_factor_kernels();
 void init_solve_kernels();
 void init_schur_tc();
 void init_schur_f64();
+void init_panel_kernels();
 
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
@@ -193,10 +197,12 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st);
 
-// panel scratch rows of a large front (m rounded up to the 128-row tile)
-__host__ __device__ inline int panel_mpad(int m) { return (m + 127) & ~127; }
-int build_panel_maps(const Plan& P, const float* pscr, const std::vector<int64_t>& pscr_off,
-                     int PW, std::vector<CUtensorMap>& maps, std::vector<int>& idx);
+int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
+                     std::vector<int>& idx);
+// one panel launch (OP_PANEL): every row-tile task of the panel's fronts
+template <typename T>
+void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status,
+                  cudaStream_t st);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,

@@ -23,8 +23,10 @@
 //     gather fills the permuted right-hand sides, each front vector is formed
 //     before use), so nothing needs clearing between calls.
 // The array's address is looked up once per device with
-// cudaGetSymbolAddress (the first call on a device does this set-up with
-// that device current; make that first call before any stream capture).
+// cudaGetSymbolAddress, with that device current: by the analysis that
+// uploads a plan to the device (so the module holding the array is loaded
+// and its memory committed then, not inside a solve), else by the first
+// no-allocation solve on the device (make it before any stream capture).
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -2,6 +2,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <map>
 #include <atomic>
 #include <cmath>
 #include <exception>
@@ -41,10 +42,80 @@ static void for_each_range(const std::vector<std::pair<int, int>>& rg, F&& fn) {
 
 const int Plan::small_limit[kSmallBuckets] = {16, 32, 64, 96, 128, 160};
 
-int small_front_limit(int scalar_bytes) { return scalar_bytes == 8 ? 160 : 160; }
-
 static int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 static int round8(int x) { return (x + 7) & ~7; }
+
+int64_t lifetime_alloc(const std::vector<int>& beg, const std::vector<int>& end,
+                       const std::vector<int64_t>& size, int nlev, std::vector<int64_t>& off) {
+    const int nb = (int)size.size();
+    off.assign(nb, -1);
+    std::vector<std::vector<int>> starts(std::max(nlev, 1)), ends(std::max(nlev, 1));
+    for (int i = 0; i < nb; ++i)
+        if (size[i] > 0) {
+            starts[beg[i]].push_back(i);
+            ends[end[i]].push_back(i);
+        }
+    std::map<int64_t, int64_t> by_off;        // free ranges: offset -> size
+    std::multimap<int64_t, int64_t> by_size;  // size -> offset
+    auto drop = [&](std::map<int64_t, int64_t>::iterator it) {
+        auto r = by_size.equal_range(it->second);
+        for (auto q = r.first; q != r.second; ++q)
+            if (q->second == it->first) {
+                by_size.erase(q);
+                break;
+            }
+        by_off.erase(it);
+    };
+    int64_t top = 0, peak = 0;
+    for (int l = 0; l < nlev; ++l) {
+        if (l > 0)
+            for (int i : ends[l - 1]) {
+                int64_t o = off[i], z = size[i];
+                auto nx = by_off.lower_bound(o);
+                if (nx != by_off.end() && nx->first == o + z) {
+                    z += nx->second;
+                    auto d = nx++;
+                    drop(d);
+                }
+                if (nx != by_off.begin()) {
+                    auto pv = std::prev(nx);
+                    if (pv->first + pv->second == o) {
+                        o = pv->first;
+                        z += pv->second;
+                        drop(pv);
+                    }
+                }
+                if (o + z == top) {
+                    top = o;
+                } else {
+                    by_off[o] = z;
+                    by_size.emplace(z, o);
+                }
+            }
+        std::vector<int>& st = starts[l];
+        std::sort(st.begin(), st.end(), [&](int a, int b) {
+            return size[a] != size[b] ? size[a] > size[b] : a < b;
+        });
+        for (int i : st) {
+            const int64_t z = size[i];
+            auto fit = by_size.lower_bound(z);
+            if (fit != by_size.end()) {
+                const int64_t o = fit->second, fz = fit->first;
+                drop(by_off.find(o));
+                off[i] = o;
+                if (fz > z) {
+                    by_off[o + z] = fz - z;
+                    by_size.emplace(fz - z, o + z);
+                }
+            } else {
+                off[i] = top;
+                top += z;
+                peak = std::max(peak, top);
+            }
+        }
+    }
+    return peak;
+}
 
 int front_tiles(int m, int c, int T) { return (c + T - 1) / T + (m - c + T - 1) / T; }
 
@@ -198,10 +269,33 @@ void build_plan(const Symbolic& S, int64_t nnz_user, int large_threshold, Plan& 
         P.max_m = std::max(P.max_m, rg_maxm[r]);
         P.max_u = std::max(P.max_u, rg_maxu[r]);
     }
-    const int64_t lo = rg_l[nrg], uo = rg_u[nrg];
+    const int64_t lo = rg_l[nrg];
     P.lstore = std::max<int64_t>(lo, 32);
-    P.ustore = std::max<int64_t>(uo, 32);
     P.child = t.child;
+    {
+        // update matrices over their lifetimes in the level schedule: the
+        // factor writes U_s at level lev(s) and its parent's assembly reads
+        // it at lev(parent); the selected inverse (top-down) writes Z_UU of s
+        // at lev(s) and its children read it down to their lowest level
+        const std::vector<int> lev = front_levels(P);
+        int nlev = 0;
+        for (int s = 0; s < ns; ++s) nlev = std::max(nlev, lev[s] + 1);
+        std::vector<int> fb(ns), fe(ns), zb(ns), ze(ns);
+        std::vector<int64_t> usz(ns, 0), uoff, zoff;
+        for (int s = 0; s < ns; ++s) {
+            const FrontDesc& f = P.fronts[s];
+            fb[s] = fe[s] = zb[s] = ze[s] = lev[s];
+            if (f.uoff < 0) continue;
+            usz[s] = align_up((int64_t)f.ldu * (f.m - f.c), 32);
+            fe[s] = lev[f.parent];
+            for (int h = f.child_beg; h < f.child_end; ++h)
+                zb[s] = std::min(zb[s], lev[P.child[h]]);
+        }
+        P.ustore = std::max<int64_t>(lifetime_alloc(fb, fe, usz, nlev, uoff), 32);
+        P.zustore = std::max<int64_t>(lifetime_alloc(zb, ze, usz, nlev, zoff), 32);
+        P.zuoff = zoff;
+        for (int s = 0; s < ns; ++s) P.fronts[s].uoff = usz[s] > 0 ? uoff[s] : -1;
+    }
 
     // A entries: the lower triangle's entries of the supernode's columns are
     // contiguous (columns are consecutive).  A repeated (row, col) keeps the
@@ -536,9 +630,9 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
         std::vector<int> fr(P.large_list.begin() + P.large_ptr[l],
                             P.large_list.begin() + P.large_ptr[l + 1]);
         if (fr.empty()) continue;
-        std::vector<std::pair<int, int>> as, po;
+        std::vector<std::pair<int, int>> as;
         int maxpanels = 0;
-        double asm_el = 0, asm_x = 0, po_fl = 0, po_el = 0;
+        double asm_el = 0, asm_x = 0;
         // diagonal tile t of f: factor (n^3/3), read + write its lower part,
         // write the T x T inverse
         auto potrf_cost = [&](const FrontDesc& f, int t, double& fl, double& el) {
@@ -549,7 +643,6 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
         for (int s : fr) {
             const FrontDesc& f = P.fronts[s];
             as.push_back({s, (f.m + CB - 1) / CB});
-            po.push_back({s, 1});
             maxpanels = std::max(maxpanels, (f.c + PW - 1) / PW);
             // assembly: write the L panel and the U store, read every child's
             // update matrix; FP64 values with their source index and position
@@ -562,50 +655,57 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
                 asm_x += 4.0 * uc;  // relative map
             }
             asm_x += 16.0 * (f.a_end - f.a_beg);
-            potrf_cost(f, 0, po_fl, po_el);
         }
         S.ops.push_back({OP_ASSEMBLE, 0, 0, S.store.add(as, 0), 0, asm_el, asm_x});
-        S.ops.push_back({OP_POTRF, 0, 0, S.store.add(po, 0), po_fl, po_el, 0});
         for (int p = 0; p < maxpanels; ++p) {
-            for (int k = p * TPP; k < (p + 1) * TPP; ++k) {
-                std::vector<std::pair<int, int>> tr, up;
-                double upfl = 0, upel = 0, trfl = 0, trel = 0;
+            // one launch for the whole panel: diagonal tasks first
+            const int64_t toff = (int64_t)S.tasks.size() / 2;
+            double fl = 0, el = 0;
+            for (int t = 0; t < TPP; ++t)
                 for (int s : fr) {
                     const FrontDesc& f = P.fronts[s];
-                    int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
-                    if (k >= nt1) continue;
-                    if (NT - k - 1 > 0) tr.push_back({s, NT - k - 1});
-                    const double K = tsize(f, k);
-                    for (int i = k + 1; i < NT; ++i) {
-                        // X = A inv(L_kk)': triangular solve flops, read A and
-                        // the inverse, write X
-                        double ri = tsize(f, i);
-                        trfl += ri * K * K;
-                        trel += 2.0 * ri * K + K * K;
+                    const int nt1 = (f.c + T - 1) / T;
+                    const int klo = p * TPP, khi = std::min(klo + TPP, nt1);
+                    if (klo + t < khi) {
+                        S.tasks.push_back(s);
+                        S.tasks.push_back(klo + t);
                     }
-                    int jl = std::min((p + 1) * TPP - 1, nt1 - 1);
-                    int cnt = 0;
-                    for (int j = k + 1; j <= jl; ++j) {
-                        cnt += NT - j;
-                        double rj = tsize(f, j);
-                        upfl += K * rj * (rj + 1);
-                        upel += K * rj + rj * (rj + 1);
-                        for (int i = j + 1; i < NT; ++i) {
-                            double ri = tsize(f, i);
-                            upfl += 2.0 * K * ri * rj;
-                            upel += K * (ri + rj) + 2.0 * ri * rj;
-                        }
-                        if (j == k + 1) potrf_cost(f, j, upfl, upel);  // fused next diagonal
-                    }
-                    if (cnt > 0) up.push_back({s, cnt});
                 }
-                if (!tr.empty()) S.ops.push_back({OP_TRSM, k, 0, S.store.add(tr, k), trfl, trel, 0});
-                if (!up.empty())
-                    S.ops.push_back({OP_UPDATE_PANEL, k, (p + 1) * TPP - 1, S.store.add(up, k),
-                                     upfl, upel, 0});
+            for (int s : fr) {
+                const FrontDesc& f = P.fronts[s];
+                const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                const int klo = p * TPP, khi = std::min(klo + TPP, nt1);
+                if (klo >= nt1) continue;
+                for (int i = khi; i < NT; ++i) {
+                    S.tasks.push_back(s);
+                    S.tasks.push_back(i);
+                }
+                // algorithmic work: per pivot tile k its factorization, the
+                // triangular solve of every row below it and the update of
+                // the panel's later columns; every panel element read and
+                // written once, every inverse written once
+                for (int k = klo; k < khi; ++k) {
+                    const double K = tsize(f, k);
+                    potrf_cost(f, k, fl, el);
+                    for (int i = k + 1; i < NT; ++i) fl += tsize(f, i) * K * K;
+                    for (int j = k + 1; j < khi; ++j) {
+                        const double rj = tsize(f, j);
+                        fl += K * rj * (rj + 1);
+                        for (int i = j + 1; i < NT; ++i) fl += 2.0 * K * tsize(f, i) * rj;
+                    }
+                    for (int i = k + 1; i < NT; ++i) el += 2.0 * tsize(f, i) * K;
+                }
             }
-            std::vector<std::pair<int, int>> big, nextp;
-            double fl = 0, el = 0, np_fl = 0, np_el = 0;
+            const int ntasks = (int)((int64_t)S.tasks.size() / 2 - toff);
+            if (ntasks > 0) {
+                PanelOp op{OP_PANEL, p, 0, WorkList{0, 0, 0, p}, fl, el, 0};
+                op.toff = toff;
+                op.ntasks = ntasks;
+                op.counter = S.ncounters++;
+                S.ops.push_back(op);
+            }
+            std::vector<std::pair<int, int>> big;
+            double sfl = 0, sel = 0;
             for (int s : fr) {
                 const FrontDesc& f = P.fronts[s];
                 int k0 = p * PW;
@@ -617,20 +717,15 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
                     int nb = NB - J0;
                     big.push_back({s, nb * (nb + 1) / 2});
                     double tr = f.m - cbeg;
-                    fl += (double)K * tr * (tr + 1);  // lower trailing part, 2 flops per FMA
-                    el += (double)K * tr + tr * (tr + 1);  // read the panel, update the trailing part
-                }
-                if ((p + 1) * PW < f.c) {
-                    nextp.push_back({s, 1});
-                    potrf_cost(f, (p + 1) * TPP, np_fl, np_el);
+                    sfl += (double)K * tr * (tr + 1);  // lower trailing part, 2 flops per FMA
+                    sel += (double)K * tr + tr * (tr + 1);  // read the panel, update the trailing part
                 }
             }
-            if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), fl, el, 0});
-            if (!nextp.empty())
-                S.ops.push_back({OP_POTRF, (p + 1) * TPP, 0, S.store.add(nextp, 0), np_fl, np_el, 0});
+            if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), sfl, sel, 0});
         }
     }
     S.op_beg[P.nlevels] = (int)S.ops.size();
+    S.nflags = (P.dinv_total + (int64_t)T * T - 1) / ((int64_t)T * T);
 }
 
 std::vector<int> front_levels(const Plan& P) {

@@ -8,8 +8,13 @@
 //             factor's final storage and the input of the solves.
 //   U store   one column-major u_s x u_s update matrix per non-root supernode
 //             (u_s = m_s - c_s, leading dimension ldu_s = u_s rounded up to 8),
-//             lower triangle only; written when s is factored, read when its
-//             parent is assembled.
+//             lower triangle only; written when s is factored (tree level
+//             lev(s)), read when its parent is assembled (level lev(parent)).
+//             Storage is reused over the matrices' lifetimes: two update
+//             matrices whose level intervals [lev(s), lev(parent)] overlap
+//             share no element, others may, so the store is about the
+//             largest sum of update matrices live at one level, not their
+//             total (the role of a postorder stack in a sequential code).
 // Front s is the m_s x m_s matrix [L panel | U]; its rows are the sorted
 // global (permuted) column indices rows_s, the first c_s of which are
 // first_col_s .. first_col_s + c_s - 1.
@@ -99,6 +104,10 @@ struct Plan {
     std::vector<int> asm_range;
     std::vector<int64_t> Lp;    // CSC column pointers of L (reference spL->p)
     int64_t lstore = 0, ustore = 0;  // element counts
+    // selected inverse: the update part Z_UU of every front with an update
+    // matrix, at zuoff[s] of a store of zustore elements (see build_plan)
+    std::vector<int64_t> zuoff;
+    int64_t zustore = 0;
     int64_t lnz = 0;
     double flops = 0;           // sum over columns of count^2 (the reference's count)
     int max_m = 0, max_u = 0;
@@ -117,8 +126,14 @@ struct Plan {
     static constexpr int kSmallMaxRows = 160;  // small_limit[kSmallBuckets - 1]
 };
 
-// Largest m handled by the fused one-CTA-per-front kernel for a scalar size.
-int small_front_limit(int scalar_bytes);
+// Offsets for blocks with inclusive lifetimes [beg_i, end_i] (levels 0 ..
+// nlev - 1): blocks whose lifetimes overlap get disjoint ranges.  Sweep over
+// the levels: the blocks whose lifetime ended at l - 1 are freed (coalesced),
+// then the blocks starting at l are placed, largest first, in the smallest
+// free range that holds them, else on top.  Blocks of size 0 get -1.
+// Returns the store size (the highest end reached).
+int64_t lifetime_alloc(const std::vector<int>& beg, const std::vector<int>& end,
+                       const std::vector<int64_t>& size, int nlev, std::vector<int64_t>& off);
 
 // Build the plan from a completed symbolic analysis.  `large_threshold` is
 // the row count above which a front takes the tiled multi-CTA path.
@@ -143,21 +158,35 @@ struct TileSchedule {
     std::vector<WorkList> assemble;      // per level: CTA per (front, column block)
 };
 
-// FP32 panel schedule: per level, operations in launch order.
-enum PanelOpKind { OP_ASSEMBLE = 0, OP_POTRF, OP_TRSM, OP_UPDATE_PANEL, OP_SCHUR_TC };
+// Panel schedule of the large fronts: per level, operations in launch order:
+// the assembly, then per 256-column panel one panel factorization (OP_PANEL)
+// and one Schur update of the trailing part (OP_SCHUR_TC).  OP_POTRF,
+// OP_TRSM and OP_UPDATE_PANEL are the 64-wide steps of the tile schedule.
+enum PanelOpKind { OP_ASSEMBLE = 0, OP_POTRF, OP_TRSM, OP_UPDATE_PANEL, OP_SCHUR_TC, OP_PANEL };
 struct PanelOp {
     int kind;
-    int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_TC)
+    int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_TC, PANEL)
     int arg2;     // UPDATE_PANEL: last tile index of the panel
     WorkList w;
     double flops;  // algorithmic flops of the launch
     double elems;  // algorithmic factor-scalar traffic (elements read + written)
     double xbytes; // other algorithmic traffic in bytes (FP64 values, indices)
+    // OP_PANEL: tasks [toff, toff + ntasks) of PanelSchedule::tasks (pairs),
+    // taken by ticket from counter number `counter`
+    int64_t toff = 0;
+    int ntasks = 0;
+    int counter = -1;
 };
 struct PanelSchedule {
     ListStore store;
     std::vector<int> op_beg;  // per level
     std::vector<PanelOp> ops;
+    // OP_PANEL tasks (front s, row tile i) as int pairs: per launch every
+    // diagonal task first (pivot tile by pivot tile), then the other row
+    // tiles front by front, so that a task waits only on lower tickets
+    std::vector<int> tasks;
+    int ncounters = 0;   // one ticket counter per OP_PANEL launch
+    int64_t nflags = 0;  // one flag per pivot tile of a large front (dinv_total / T^2)
 };
 void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S);
 

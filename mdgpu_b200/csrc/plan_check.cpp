@@ -5,6 +5,7 @@
 #include "plan_check.hpp"
 
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -32,7 +33,7 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
         if ((int)P.fronts.size() != ns || (int)level.size() != ns) bad("table sizes");
         // fronts: sizes, storage ranges, row sets, children, columns owned
         std::vector<int> owner(n, -1);
-        int64_t rows_next = 0, lprev = -1, uprev = -1;
+        int64_t rows_next = 0, lprev = -1;
         for (int s = 0; s < ns; ++s) {
             const FrontDesc& f = P.fronts[s];
             const int u = f.m - f.c;
@@ -42,11 +43,11 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                 bad("L panel offset", s);
             lprev = f.loff + (int64_t)f.ldl * f.c - 1;
             if ((f.parent >= 0 && u > 0) != (f.uoff >= 0)) bad("update matrix presence", s);
-            if (f.uoff >= 0) {
-                if (f.uoff % 32 || f.uoff <= uprev || f.uoff + (int64_t)f.ldu * u > P.ustore)
-                    bad("update matrix offset", s);
-                uprev = f.uoff + (int64_t)f.ldu * u - 1;
-            }
+            if (f.uoff >= 0 && (f.uoff % 32 || f.uoff + (int64_t)f.ldu * u > P.ustore))
+                bad("update matrix offset", s);
+            if (f.uoff >= 0 && ((int)P.zuoff.size() != ns || P.zuoff[s] < 0 || P.zuoff[s] % 32 ||
+                                P.zuoff[s] + (int64_t)f.ldu * u > P.zustore))
+                bad("selected-inverse update offset", s);
             if (f.rows_off != rows_next) bad("row set offset", s);
             rows_next += f.m;
             if (rows_next > (int64_t)P.rows.size()) bad("row set past the row array", s);
@@ -183,6 +184,43 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                 }
             }
         }
+        // update matrices sharing storage have disjoint lifetimes: at every
+        // level, the ranges of the matrices live there do not overlap (the
+        // factor's [lev(s), lev(parent)]; the selected inverse's [lowest
+        // child level, lev(s)])
+        {
+            int nlev = 0;
+            for (int s = 0; s < ns; ++s) nlev = std::max(nlev, level[s] + 1);
+            for (int pass = 0; pass < 2; ++pass) {
+                std::vector<std::vector<int>> live(nlev);
+                for (int s = 0; s < ns; ++s) {
+                    const FrontDesc& f = P.fronts[s];
+                    if (f.uoff < 0) continue;
+                    int b = level[s], e = level[s];
+                    if (pass == 0) {
+                        e = level[f.parent];
+                    } else {
+                        for (int h = f.child_beg; h < f.child_end; ++h)
+                            b = std::min(b, level[P.child[h]]);
+                    }
+                    for (int l = b; l <= e; ++l) live[l].push_back(s);
+                }
+                for (int l = 0; l < nlev; ++l) {
+                    std::vector<std::pair<int64_t, int64_t>> rg;
+                    for (int s : live[l]) {
+                        const FrontDesc& f = P.fronts[s];
+                        const int64_t o = pass == 0 ? f.uoff : P.zuoff[s];
+                        rg.push_back({o, o + (int64_t)f.ldu * (f.m - f.c)});
+                    }
+                    std::sort(rg.begin(), rg.end());
+                    for (size_t q = 1; q < rg.size(); ++q)
+                        if (rg[q].first < rg[q - 1].second)
+                            bad(pass == 0 ? "update matrices live together share storage"
+                                          : "selected-inverse update parts live together share "
+                                            "storage");
+                }
+            }
+        }
         // solve tasks: each tile of each large front once per direction, in
         // dependency order (forward pivot tiles ascending before the front's
         // update tiles; backward pivot tiles descending)
@@ -227,6 +265,60 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
         for (int64_t q = 0; q < csr_nnz; ++q)
             if (csr_col[q] < 0 || csr_col[q] >= n || csr_src[q] < 0 || csr_src[q] >= P.nnz_user)
                 bad("CSR entry out of range");
+    } catch (const Fail& f) {
+        return f.msg;
+    }
+    return std::string();
+}
+
+std::string check_panel_schedule(const Plan& P, const PanelSchedule& S,
+                                 const std::vector<int>& level, int T, int PW) {
+    try {
+        const int ns = P.nsuper, TPP = PW / T;
+        std::vector<char> is_large(ns, 0);
+        for (int s : P.large_list) is_large[s] = 1;
+        std::vector<char> counter_used(S.ncounters, 0);
+        for (int l = 0; l < P.nlevels; ++l) {
+            for (int q = S.op_beg[l]; q < S.op_beg[l + 1]; ++q) {
+                const PanelOp& op = S.ops[q];
+                if (op.kind != OP_PANEL) continue;
+                const int klo = op.arg * TPP;
+                if (op.counter < 0 || op.counter >= S.ncounters || counter_used[op.counter]++)
+                    bad("panel ticket counter");
+                if (op.toff < 0 || op.ntasks < 1 ||
+                    2 * (op.toff + op.ntasks) > (int64_t)S.tasks.size())
+                    bad("panel task range");
+                // every task's waits (the pivot tiles of the panel above its
+                // row) name diagonal tasks earlier in the list
+                std::map<int, std::vector<char>> done;
+                for (int64_t t = op.toff; t < op.toff + op.ntasks; ++t) {
+                    const int s = S.tasks[2 * t], i = S.tasks[2 * t + 1];
+                    if (s < 0 || s >= ns || !is_large[s] || level[s] != l) bad("panel task front");
+                    const FrontDesc& f = P.fronts[s];
+                    const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                    const int khi = std::min(klo + TPP, nt1);
+                    if (klo >= nt1 || i < klo || i >= NT) bad("panel task row tile", s);
+                    if (P.dinv_off[s] < 0 || P.dinv_off[s] % ((int64_t)T * T) ||
+                        P.dinv_off[s] / ((int64_t)T * T) + nt1 > S.nflags)
+                        bad("panel flag range", s);
+                    std::vector<char>& d = done[s];
+                    d.resize(NT, 0);
+                    for (int k = klo; k < std::min(i, khi); ++k)
+                        if (!d[k]) bad("panel task order", s);
+                    if (d[i]++) bad("panel task repeated", s);
+                }
+                for (int qq = P.large_ptr[l]; qq < P.large_ptr[l + 1]; ++qq) {
+                    const int s = P.large_list[qq];
+                    const FrontDesc& f = P.fronts[s];
+                    const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                    if (klo >= nt1) continue;
+                    auto it = done.find(s);
+                    for (int i = klo; i < NT; ++i)
+                        if (it == done.end() || !it->second[i])
+                            bad("panel tasks do not cover the front", s);
+                }
+            }
+        }
     } catch (const Fail& f) {
         return f.msg;
     }

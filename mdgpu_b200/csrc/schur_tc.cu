@@ -1,37 +1,49 @@
-// Tensor-core Schur-complement update for FP32 fronts (TF32 inputs, FP32
-// accumulation) on sm_100a: tcgen05.mma with the accumulator in TMEM,
-// operands staged in shared memory by TMA.
+// Tensor-core Schur-complement update for FP32 fronts (3xTF32 products, FP32
+// accumulation) on sm_100a: tcgen05.mma with the accumulators in TMEM,
+// operands brought into shared memory by TMA straight from the L panels.
 //
-// One CTA computes one 128 x 128 tile (I, J), I >= J, of the trailing part of
-// a large front after a pivot panel of K <= PW (256) columns:
-//     C(I, J) -= A_I * A_J'      A_I = rows 128I.. of the panel columns
-// in 3xTF32: A = hi + lo with hi an exact TF32 value and lo = A - hi, and
-// C -= hi*hi' + hi*lo' + lo*hi' (close to FP32 accuracy, which keeps the
-// iterative refinement short).  The panel's TRSMs write hi and lo into a
-// per-front scratch (column-major, rows hi then lo), so A_I and A_J arrive
-// split: a 32-row x 16-column TMA box (rows contiguous, 128 bytes per panel column)
-// lands MN-major.  For 32-bit MN-major operands the only UMMA shared-memory
-// layout is the 128-byte swizzle with 32-byte atoms (32-byte chunks of each
-// 128-byte row permuted by row mod 4, atoms of 4 K-rows); the TMA writes
-// exactly that pattern with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.  Four boxes
-// make a 128-row x 16-column operand; a stage holds A_hi, B_hi, A_lo, B_lo
-// (32 KB), and the K loop runs over 16-column chunks through a 3-stage ring
-// (97 KB of shared memory: two CTAs per SM, so one CTA's epilogue overlaps
-// the other's MMAs).
+// After pivot panel p (columns [k0, k0 + K), K <= 256) of a large front, the
+// trailing lower part is updated in 128 x 128 tiles (I, J), I >= J >= J0:
+//     C(I, J) -= A_I A_J'      A_I = rows 128 I .. of the panel's columns
+// in 3xTF32: A = hi + lo with hi = A with the low 13 mantissa bits cleared
+// (an exact TF32 value) and lo = A - hi (exact in FP32), and
+// C -= lo hi' + hi lo' + hi hi' (close to FP32 accuracy, which keeps the
+// iterative refinement short).
 //
-// Roles: thread 0 issues the TMA loads (refilling a stage once the MMAs that
-// read it have completed), thread 32 issues the MMAs (single-issued per
-// CTA) and commits each stage back to the producer; then all 128 threads
-// read the accumulator out of TMEM (warp w owns TMEM lanes 32w..32w+31 =
-// tile rows) and subtract it from C in place -- coalesced along the column.
+// One persistent CTA per SM takes tiles round-robin over the launch's tile
+// list and runs three roles (288 threads, nine warps):
+//   warps 0-3  load + split: lane 0 of warp 0 issues the TMA loads of each
+//              16-column chunk of A_I and A_J (32-row boxes from the front's
+//              L panel, rows and columns past the panel's end read as zeros),
+//              then all four warps split the chunk in shared memory (hi in
+//              place, lo beside it) and release it to the MMA warp;
+//   warp 4     MMA issue (one elected thread): per 8-column step three
+//              tcgen05.mma kind::tf32 (M = N = 128) into the tile's TMEM
+//              accumulator, the stage committed back to the loaders;
+//   warps 5-8  epilogue: tcgen05.ld of their 32 TMEM lanes (tile rows),
+//              C -= acc in place (coalesced along the columns), then the
+//              accumulator is handed back to the MMA warp.
+// The TMEM accumulator is double-buffered (2 x 128 columns), so tile t's
+// epilogue runs under tile t + 1's MMAs; the chunk ring has four stages.
+// Only the panel itself crosses L2 (the hi / lo split is made here, once per
+// chunk and CTA, instead of being stored and read twice).
+//
+// For 32-bit MN-major operands the only UMMA shared-memory layout is the
+// 128-byte swizzle with 32-byte atoms (32-byte chunks of each 128-byte row
+// permuted by row mod 4, atoms of 4 K-rows); the TMA writes exactly that
+// pattern with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, and the split is
+// elementwise, so lo lands in the same pattern.
 //
 // Every wait on an mbarrier is bounded: on timeout the CTA records an error
-// code in *err, drains what it issued (bounded again), frees its TMEM and
-// returns; the host reports the error.  The TMA loads never use cluster
-// multicast and only ever read this GPU's own memory.
+// code in *err and sets its abort word, every role leaves its loop, the
+// loaders wait (bounded) for their TMA loads in flight and the MMA warp for
+// its MMAs, then the TMEM is freed and the CTA returns; the host reports the
+// error.  The TMA loads never use cluster multicast and only ever read this
+// GPU's own memory.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -42,15 +54,16 @@ namespace mdgpu {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
-constexpr int BOX = 32;                                   // TMA box: 32 rows x BK columns (fp32)
-constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes
-constexpr int STAGE_TMA = STAGE_A + STAGE_B;              // one of hi / lo: A and B
-// per stage: A_hi, B_hi, then A_lo, B_lo at the same offsets + STAGE_TMA
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
+constexpr int BOX = 32;                                      // TMA box: 32 rows x BK columns
+constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes of one operand chunk
+constexpr int STAGE_TMA = STAGE_A + STAGE_B;                 // what the TMA brings per chunk
+// per stage: A, B as loaded (then hi in place), then A_lo, B_lo at + STAGE_TMA
 constexpr int STAGE_BYTES = 2 * STAGE_TMA;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack
-constexpr uint32_t TMEM_COLS = 128;
-constexpr long long WAIT_LIMIT = 1ll << 22;               // polls (with backoff) before giving up
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;      // + alignment slack
+constexpr uint32_t TMEM_COLS = 2 * BN;                       // two accumulators
+constexpr int NLOAD_WARPS = 4, MMA_WARP = 4, NTHREADS = 9 * 32;  // warps 5-8: epilogue
+constexpr long long WAIT_LIMIT = 1ll << 22;                  // polls (with backoff)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,6 +79,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     uint32_t ok;
     asm volatile(
@@ -78,15 +95,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
-// bounded wait; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+// bounded wait; false on timeout or when the CTA's abort word is set
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort) {
     for (long long i = 0; i < WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, phase)) return true;
-        if (i > 64) __nanosleep(64);
+        if (i > 64) {
+            if (*abort) return false;
+            __nanosleep(64);
+        }
     }
     return false;
 }
-
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int x, int y) {
     asm volatile(
@@ -153,51 +172,71 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Tile number b of the launch -> front s and tile (I, J); the CTAs of a front
+// enumerate the lower 128-tiles (I, J) with J >= J0 = cbeg / 128 row by row.
+struct TileJob {
+    int s, I, J, nk, k0, cbeg;
+};
+__device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts,
+                                            const int* __restrict__ items,
+                                            const int* __restrict__ before, int nitems, int b,
+                                            int panel, int PW) {
+    TileJob t;
+    const int it = find_item(before, nitems, b);
+    t.s = items[it];
+    const FrontDesc f = fronts[t.s];
+    t.k0 = panel * PW;
+    const int K = min(PW, f.c - t.k0);
+    t.cbeg = min(t.k0 + PW, f.c);
+    const int J0 = t.cbeg / BM;
+    int ii, jj;
+    lower_index(b - before[it], ii, jj);
+    t.I = J0 + ii;
+    t.J = J0 + jj;
+    t.nk = (K + BK - 1) / BK;
+    return t;
+}
+
 }  // namespace tc
 
-// items/before: one entry per large front; the CTAs of a front enumerate the
-// lower 128-tiles (I, J) with J >= J0 = cbeg / 128 in row-major order.
-__global__ void __launch_bounds__(128, 2)
+// items/before: one entry per large front (its tile count); ntiles: the
+// launch's total.  maps: per large front a tensor map over its FP32 L panel
+// (rows x pivot columns).
+__global__ void __launch_bounds__(tc::NTHREADS, 1)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
-               const int* __restrict__ before, int nitems, const int* __restrict__ tmap_idx,
-               const CUtensorMap* __restrict__ maps, int panel, int PW,
-               float* __restrict__ Ls, float* __restrict__ Us, int* __restrict__ err) {
+               const int* __restrict__ before, int nitems, int ntiles,
+               const int* __restrict__ tmap_idx, const CUtensorMap* __restrict__ maps, int panel,
+               int PW, float* __restrict__ Ls, float* __restrict__ Us, int* __restrict__ err) {
     using namespace tc;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[STAGES];
-    __shared__ __align__(8) uint64_t empty_bar[STAGES];
-    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ __align__(8) uint64_t full_bar[STAGES];   // TMA bytes landed
+    __shared__ __align__(8) uint64_t split_bar[STAGES];  // hi / lo written (4 warps)
+    __shared__ __align__(8) uint64_t empty_bar[STAGES];  // MMAs done reading the stage
+    __shared__ __align__(8) uint64_t accf_bar[2];        // accumulator complete
+    __shared__ __align__(8) uint64_t acce_bar[2];        // accumulator read out (4 warps)
+    __shared__ __align__(8) uint64_t drain_bar;          // every MMA issued has completed
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
 
     // 1024-byte aligned in the shared window (the 128-byte swizzle phase)
     unsigned char* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int it = find_item(before, nitems, blockIdx.x);
-    const int s = items[it];
-    const FrontDesc f = fronts[s];
-    const CUtensorMap* map = maps + tmap_idx[s];
-    const int mpad = panel_mpad(f.m);
-    // panel columns [k0, k0 + K); trailing columns start at cbeg
-    const int k0 = panel * PW;
-    const int K = min(PW, f.c - k0);
-    const int cbeg = min(k0 + PW, f.c);
-    const int J0 = cbeg / BM;
-    int ii, jj;
-    lower_index(blockIdx.x - before[it], ii, jj);
-    const int I = J0 + ii, J = J0 + jj;
-    const int nk = (K + BK - 1) / BK;
 
     if (tid == 0) {
         for (int q = 0; q < STAGES; ++q) {
             tc::mbar_init(&full_bar[q], 1);
+            tc::mbar_init(&split_bar[q], NLOAD_WARPS);
             tc::mbar_init(&empty_bar[q], 1);
         }
-        tc::mbar_init(&done_bar, 1);
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&accf_bar[a], 1);
+            tc::mbar_init(&acce_bar[a], 4);
+        }
+        tc::mbar_init(&drain_bar, 1);
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == MMA_WARP) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          tc::smem_u32(&tmem_base_sh)),
                      "r"(TMEM_COLS));
@@ -208,108 +247,162 @@ __global__ void __launch_bounds__(128, 2)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
 
-    if (tid == 0) {
-        // producer: A_hi, B_hi, A_lo, B_lo of each BK-column chunk
-        int issued = 0;
+    if (warp < NLOAD_WARPS) {
+        // ---- loaders: TMA (warp 0 lane 0), then the split by all four warps
+        long long g = 0;  // chunk counter over this CTA's tiles
+        long long issued = 0;
         bool ok = true;
-        for (int ch = 0; ch < nk; ++ch) {
-            const int st = ch % STAGES;
-            if (ch >= STAGES && !tc::mbar_wait(&empty_bar[st], ((ch / STAGES) - 1) & 1)) {
-                ok = false;
-                break;
-            }
-            if (abort_sh) break;
-            unsigned char* a = smem + st * STAGE_BYTES;
-            unsigned char* b = a + STAGE_A;
-            tc::mbar_expect_tx(&full_bar[st], STAGE_BYTES);
-            const int col = ch * BK;
+        for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+            const CUtensorMap* map = maps + tmap_idx[t.s];
+            for (int ch = 0; ch < t.nk; ++ch, ++g) {
+                const int st = (int)(g % STAGES);
+                const uint32_t use = (uint32_t)(g / STAGES);
+                unsigned char* a = smem + st * STAGE_BYTES;
+                if (tid == 0) {
+                    if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1, &abort_sh)) {
+                        ok = false;
+                    } else {
+                        tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
+                        const int col = t.k0 + ch * BK;
 #pragma unroll
-            for (int q = 0; q < BM / BOX; ++q) {
-                const int ra = I * BM + q * BOX, rb = J * BN + q * BOX;
-                tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st], ra, col);
-                tc::tma_load_2d(b + q * BOX * BK * 4, map, &full_bar[st], rb, col);
-                tc::tma_load_2d(a + STAGE_TMA + q * BOX * BK * 4, map, &full_bar[st], mpad + ra,
-                                col);
-                tc::tma_load_2d(b + STAGE_TMA + q * BOX * BK * 4, map, &full_bar[st], mpad + rb,
-                                col);
-            }
-            issued = ch + 1;
-        }
-        if (!ok) {
-            atomicExch(err, 1);
-            abort_sh = 1;
-        }
-        if (!ok || abort_sh) {
-            // drain: wait (bounded) for the loads already issued
-            for (int ch = 0; ch < issued; ++ch)
-                tc::mbar_wait(&full_bar[ch % STAGES], (ch / STAGES) & 1);
-        }
-    } else if (tid == 32) {
-        // MMA issuer
-        int committed = 0;
-        bool ok = true;
-        for (int ch = 0; ch < nk; ++ch) {
-            const int st = ch % STAGES;
-            if (!tc::mbar_wait(&full_bar[st], (ch / STAGES) & 1)) {
-                ok = false;
-                break;
-            }
-            if (abort_sh) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
-            const uint32_t bh = ah + STAGE_A;
-            const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
-#pragma unroll
-            for (int t = 0; t < BK / 8; ++t) {
-                const uint32_t o = t * 1024;
-                tc::mma_tf32(tmem, tc::make_desc(al + o), tc::make_desc(bh + o),
-                             (ch > 0 || t > 0) ? 1u : 0u);
-                tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
-                tc::mma_tf32(tmem, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
-            }
-            tc::mma_commit(&empty_bar[st]);
-            committed = ch + 1;
-        }
-        if (!ok) {
-            atomicExch(err, 1);
-            abort_sh = 1;
-        }
-        // completes once every MMA issued above has (a partial accumulator
-        // after an abort is not written back)
-        if (committed > 0) tc::mma_commit(&done_bar);
-    }
-    __syncthreads();
-    const bool have_acc = nk > 0 && tc::mbar_wait(&done_bar, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!have_acc && nk > 0 && tid == 0) atomicExch(err, 2);
-    if (have_acc && !abort_sh) {
-        const int row = I * BM + warp * 32 + lane;
-#pragma unroll 1
-        for (int cb = 0; cb < BN / 32; ++cb) {
-            float v[32];
-            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + cb * 32, v);
-            if (row < f.m) {
-                // gather all 32 addresses and old values first (independent
-                // loads in flight), then write
-                float* p[32];
-                float old[32];
-#pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int col = J * BN + cb * 32 + q;
-                    const bool ok = col >= cbeg && col < f.m && row >= col;
-                    p[q] = ok ? front_elem(Ls, Us, f, row, col) : nullptr;
+                        for (int q = 0; q < BM / BOX; ++q) {
+                            tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st],
+                                            t.I * BM + q * BOX, col);
+                            tc::tma_load_2d(a + STAGE_A + q * BOX * BK * 4, map, &full_bar[st],
+                                            t.J * BN + q * BOX, col);
+                        }
+                        issued = g + 1;
+                    }
                 }
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                // all four warps: wait for the bytes, split, release
+                if (ok && !tc::mbar_wait(&full_bar[st], use & 1, &abort_sh)) ok = false;
+                if (!ok) break;
+                float4* x = reinterpret_cast<float4*>(a);
+                float4* lo = reinterpret_cast<float4*>(a + STAGE_TMA);
 #pragma unroll
-                for (int q = 0; q < 32; ++q) old[q] = p[q] ? *p[q] : 0.f;
+                for (int u = 0; u < STAGE_TMA / 16 / 128; ++u) {
+                    const int e = tid + 128 * u;  // tid < 128 in the loader warps
+                    const float4 v = x[e];
+                    float4 h;
+                    h.x = __uint_as_float(__float_as_uint(v.x) & 0xffffe000u);
+                    h.y = __uint_as_float(__float_as_uint(v.y) & 0xffffe000u);
+                    h.z = __uint_as_float(__float_as_uint(v.z) & 0xffffe000u);
+                    h.w = __uint_as_float(__float_as_uint(v.w) & 0xffffe000u);
+                    x[e] = h;
+                    lo[e] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+                }
+                // generic-proxy writes, read next by the tensor core (async proxy)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&split_bar[st]);
+            }
+        }
+        if (!ok && tid == 0) {
+            atomicExch(err, 1);
+            abort_sh = 1;
+            // drain: wait (bounded, ignoring the abort word) for the loads issued
+            volatile int never = 0;
+            for (long long q = (issued > STAGES ? issued - STAGES : 0); q < issued; ++q)
+                tc::mbar_wait(&full_bar[q % STAGES], (uint32_t)(q / STAGES) & 1, &never);
+        }
+    } else if (warp == MMA_WARP) {
+        // ---- MMA issue
+        if (lane == 0) {
+            long long g = 0;
+            int tl = 0;  // tiles of this CTA
+            bool ok = true, any = false;
+            for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x, ++tl) {
+                const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+                const int acc = tl & 1;
+                const uint32_t use_acc = (uint32_t)(tl >> 1);
+                if (use_acc > 0 && !tc::mbar_wait(&acce_bar[acc], (use_acc - 1) & 1, &abort_sh)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(acc * BN);
+                for (int ch = 0; ch < t.nk; ++ch, ++g) {
+                    const int st = (int)(g % STAGES);
+                    if (!tc::mbar_wait(&split_bar[st], (uint32_t)(g / STAGES) & 1, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
+                    const uint32_t bh = ah + STAGE_A;
+                    const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
 #pragma unroll
-                for (int q = 0; q < 32; ++q)
-                    if (p[q]) *p[q] = old[q] - v[q];
+                    for (int k = 0; k < BK / 8; ++k) {
+                        const uint32_t o = k * 1024;
+                        tc::mma_tf32(d, tc::make_desc(al + o), tc::make_desc(bh + o),
+                                     (ch > 0 || k > 0) ? 1u : 0u);
+                        tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
+                        tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
+                    }
+                    tc::mma_commit(&empty_bar[st]);
+                    any = true;
+                }
+                if (!ok) break;
+                tc::mma_commit(&accf_bar[acc]);
+            }
+            if (!ok) {
+                atomicExch(err, 1);
+                abort_sh = 1;
+            }
+            // completes once every MMA issued above has
+            if (any) {
+                tc::mma_commit(&drain_bar);
+                volatile int never = 0;
+                if (!tc::mbar_wait(&drain_bar, 0, &never)) atomicExch(err, 2);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+        const int quarter = warp & 3;
+        int tl = 0;
+        for (int b = blockIdx.x; b < ntiles; b += gridDim.x, ++tl) {
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+            const FrontDesc f = fronts[t.s];
+            const int acc = tl & 1;
+            if (!tc::mbar_wait(&accf_bar[acc], (uint32_t)(tl >> 1) & 1, &abort_sh)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int row = t.I * BM + quarter * 32 + lane;
+#pragma unroll 1
+            for (int cb = 0; cb < BN / 32; ++cb) {
+                float v[32];
+                tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + acc * BN + cb * 32, v);
+                if (cb == BN / 32 - 1) {
+                    // every TMEM read of this accumulator is done: hand it back
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&acce_bar[acc]);
+                }
+                if (row < f.m) {
+                    // all 32 addresses and old values first (independent
+                    // loads in flight), then the stores
+                    float* p[32];
+                    float old[32];
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) {
+                        const int col = t.J * BN + cb * 32 + q;
+                        const bool in = col >= t.cbeg && col < f.m && row >= col;
+                        p[q] = in ? front_elem(Ls, Us, f, row, col) : nullptr;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) old[q] = p[q] ? *p[q] : 0.f;
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)
+                        if (p[q]) *p[q] = old[q] - v[q];
+                }
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == MMA_WARP)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(TMEM_COLS));
 }
@@ -336,23 +429,26 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// One tensor map per large front over its split panel scratch: 2 * mpad rows
-// (hi then lo) x PW panel columns, column-major.
-int build_panel_maps(const Plan& P, const float* pscr, const std::vector<int64_t>& pscr_off,
-                     int PW, std::vector<CUtensorMap>& maps, std::vector<int>& idx) {
+// One tensor map per large front over its FP32 L panel: m rows x c pivot
+// columns, column-major with leading dimension ldl (a multiple of 8, so the
+// column stride is a multiple of 16 bytes; the panel starts on 128 bytes).
+// Boxes of 32 rows x 16 columns; reads past the panel's rows or columns
+// return zeros.
+int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
+                     std::vector<int>& idx) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return -1;
     maps.resize(P.large_list.size());
     idx.assign(P.nsuper, -1);
     for (size_t q = 0; q < P.large_list.size(); ++q) {
-        int s = P.large_list[q];
-        const int mpad = panel_mpad(P.fronts[s].m);
+        const int s = P.large_list[q];
+        const FrontDesc& f = P.fronts[s];
         idx[s] = (int)q;
-        cuuint64_t dims[2] = {(cuuint64_t)(2 * mpad), (cuuint64_t)PW};
-        cuuint64_t strides[1] = {(cuuint64_t)(2 * mpad) * 4};
+        cuuint64_t dims[2] = {(cuuint64_t)f.m, (cuuint64_t)f.c};
+        cuuint64_t strides[1] = {(cuuint64_t)f.ldl * 4};
         cuuint32_t box[2] = {tc::BOX, tc::BK};
         cuuint32_t estr[2] = {1, 1};
-        void* base = const_cast<float*>(pscr + pscr_off[s]);
+        void* base = const_cast<float*>(L32 + f.loff);
         CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -367,10 +463,10 @@ void init_schur_tc() {
 
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, cudaStream_t st) {
-    k_schur_tc<<<w.nctas, 128, tc::SMEM_BYTES, st>>>(D.fronts, D.psched.items + w.off,
-                                                     D.psched.before + w.off, w.nitems,
-                                                     D.tmap_idx, D.tmaps, panel, PW, Ls, Us,
-                                                     err);
+    const int grid = std::min(w.nctas, D.num_sms > 0 ? D.num_sms : 148);
+    k_schur_tc<<<grid, tc::NTHREADS, tc::SMEM_BYTES, st>>>(
+        D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas, D.tmap_idx,
+        D.tmaps, panel, PW, Ls, Us, err);
 }
 
 }  // namespace mdgpu

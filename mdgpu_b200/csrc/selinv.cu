@@ -32,17 +32,19 @@ namespace mdgpu {
 constexpr int kSelBlock = 16;  // pivot columns per block of the recurrence
 
 // Z(r, col), r >= col, front-local indices of front f
-__device__ __forceinline__ double& zelem(double* Zs, double* Zu, const FrontDesc& f, int r,
-                                         int col) {
+// (Z's update part of front f at zoff in the Zu store)
+__device__ __forceinline__ double& zelem(double* Zs, double* Zu, const FrontDesc& f,
+                                         int64_t zoff, int r, int col) {
     if (col < f.c) return Zs[f.loff + r + (int64_t)col * f.ldl];
-    return Zu[f.uoff + (r - f.c) + (int64_t)(col - f.c) * f.ldu];
+    return Zu[zoff + (r - f.c) + (int64_t)(col - f.c) * f.ldu];
 }
 
 __global__ void __launch_bounds__(256, 2)
     k_selinv_front(const FrontDesc* __restrict__ fronts, const int* __restrict__ list,
                    const int* __restrict__ relmap, const double* __restrict__ Ls,
                    double* __restrict__ Zs, double* __restrict__ Zu,
-                   double* __restrict__ Yscr, const int64_t* __restrict__ yoff) {
+                   const int64_t* __restrict__ zuoff, double* __restrict__ Yscr,
+                   const int64_t* __restrict__ yoff) {
     constexpr int NB = kSelBlock;
     __shared__ double Lk[NB][NB + 1];
     __shared__ double Wk[NB][NB + 1];
@@ -50,14 +52,16 @@ __global__ void __launch_bounds__(256, 2)
     const int s = list[blockIdx.x];
     const FrontDesc f = fronts[s];
     const int m = f.m, c = f.c, u = m - c;
+    const int64_t zf = (f.parent >= 0 && u > 0) ? zuoff[s] : -1;
     // the update part: the parent's Z on this front's update rows
     if (f.parent >= 0 && u > 0) {
         const FrontDesc p = fronts[f.parent];
+        const int64_t zp = zuoff[f.parent];
         const int* rm = relmap + f.rows_off + c;
         for (int b = 0; b < u; ++b) {
             const int pb = rm[b];
             for (int a = b + tid; a < u; a += nt)
-                Zu[f.uoff + a + (int64_t)b * f.ldu] = zelem(Zs, Zu, p, rm[a], pb);
+                Zu[zf + a + (int64_t)b * f.ldu] = zelem(Zs, Zu, p, zp, rm[a], pb);
         }
         __syncthreads();
     }
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
             for (int j = 0; j < NB; ++j) acc[j] = 0.0;
             for (int b = k1; b < m; ++b) {
-                const double z = b <= a ? zelem(Zs, Zu, f, a, b) : zelem(Zs, Zu, f, b, a);
+                const double z = b <= a ? zelem(Zs, Zu, f, zf, a, b) : zelem(Zs, Zu, f, zf, b, a);
                 const double* y = Y + (int64_t)(b - k1) * NB;
 #pragma unroll
                 for (int j = 0; j < NB; ++j) acc[j] += z * y[j];
@@ -192,7 +196,7 @@ void launch_selinv(const DevPlan& D, const double* Ls, double* Zs, double* Zu, d
         const int b = D.h_level_ptr[l], e = D.h_level_ptr[l + 1];
         if (e > b)
             k_selinv_front<<<e - b, 256, 0, st>>>(D.fronts, D.level_list + b, D.relmap, Ls, Zs, Zu,
-                                                  Yscr, D.yoff);
+                                                  D.zuoff, Yscr, D.yoff);
     }
 }
 

@@ -290,6 +290,39 @@ def round_bf16(a):
     return u.view(np.float32).astype(np.float64)
 
 
+def truncate_tf32(a):
+    """FP32 values with the low 13 mantissa bits cleared (an exact TF32
+    value, rounded toward zero): the operand a TF32 tensor-core product reads
+    from an FP32 register, and the 'hi' part of a 3xTF32 split.  TEST
+    INFRASTRUCTURE ONLY."""
+    u = np.asarray(a, np.float32).copy().view(np.uint32)
+    u &= np.uint32(0xFFFFE000)
+    return u.view(np.float32)
+
+
+def rounded_update_cholesky(A, nb=64, rounding=None):
+    """Dense right-looking blocked Cholesky in FP32 whose trailing (Schur)
+    updates take their operands through `rounding` (an FP32 -> FP32 map; None:
+    plain FP32 products) and accumulate in FP32; the diagonal-block factor and
+    the panel solve stay in FP32.  rounding=truncate_tf32 is a 1xTF32
+    tensor-core Schur update, None the FP32 arithmetic a 3xTF32 update
+    approaches.  Returns the lower factor in FP64.  TEST INFRASTRUCTURE ONLY."""
+    import scipy.linalg as sl
+
+    W = np.array(A, dtype=np.float32)
+    n = W.shape[0]
+    for k in range(0, n, nb):
+        e = min(k + nb, n)
+        L11 = np.linalg.cholesky(W[k:e, k:e].astype(np.float64)).astype(np.float32)
+        W[k:e, k:e] = L11
+        if e < n:
+            L21 = sl.solve_triangular(L11, W[e:, k:e].T, lower=True).T.astype(np.float32)
+            W[e:, k:e] = L21
+            Q = L21 if rounding is None else rounding(L21)
+            W[e:, e:] -= Q @ Q.T
+    return np.tril(W).astype(np.float64)
+
+
 def bf16_update_cholesky(A, nb=64, pow2_scale=False):
     """Dense right-looking blocked Cholesky in FP32 whose trailing (Schur)
     updates take their operands rounded to BF16 and accumulate in FP32 -- the

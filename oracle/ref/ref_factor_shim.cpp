@@ -8,9 +8,15 @@
  * column counts' prefix sums, mdgpu.cu:1859-1875) and the postordered
  * supernode list; it must fill spL->i and spL->x.  Here the whole numeric
  * phase goes through the C ABI: mdgpu_analyze_tree builds the plan from the
- * given tree, mdgpu_factor factors on the GPU in FP64, mdgpu_get_L writes L
- * in the reference's layout (rows ascending, diagonal first).  Errors print
- * the library's message and exit, as the reference does (cutil.h:9-35).
+ * given tree, mdgpu_factor factors on the GPU, mdgpu_get_L writes L in the
+ * reference's layout (rows ascending, diagonal first).  Errors print the
+ * library's message and exit, as the reference does (cutil.h:9-35).
+ *
+ * The value type follows the reference's FLOTANTE (types.h:4-24).  In its
+ * FP64 build the values pass straight through and the factor is FP64.  In
+ * its default build (FLOTANTE float) the shim widens A->x to double for the
+ * C ABI, factors in FP32 (the reference's precision; 3xTF32 tensor-core Schur
+ * updates), and narrows L back to float into spL->x.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -30,6 +36,24 @@ static void check(int rc, const char* what) {
     }
 }
 
+// FP64 build: the values pass straight through, FP64 factor
+static void numeric(mdgpu_handle h, int nnz, const double* Ax, int lnz, int* Li, double* Lx,
+                    long long* Lp) {
+    (void)nnz;
+    (void)lnz;
+    check(mdgpu_factor(h, Ax, MDGPU_FP64, NULL), "mdgpu_factor");
+    check(mdgpu_get_L(h, Lp, Li, Lx), "mdgpu_get_L");
+}
+
+// default (FP32) build: widen A, FP32 factor, narrow L
+static void numeric(mdgpu_handle h, int nnz, const float* Ax, int lnz, int* Li, float* Lx,
+                    long long* Lp) {
+    std::vector<double> ax(Ax, Ax + nnz), lx(lnz > 0 ? lnz : 1);
+    check(mdgpu_factor(h, ax.data(), MDGPU_FP32, NULL), "mdgpu_factor");
+    check(mdgpu_get_L(h, Lp, Li, lx.data()), "mdgpu_get_L");
+    for (int q = 0; q < lnz; q++) Lx[q] = (float)lx[q];
+}
+
 void Factor(cs* A, cs* spL, struct ETree** lista, int cant) {
     std::map<struct ETree*, int> pos;
     for (int s = 0; s < cant; s++) pos[lista[s]] = s;
@@ -45,8 +69,7 @@ void Factor(cs* A, cs* spL, struct ETree** lista, int cant) {
     check(mdgpu_analyze_tree(A->n, A->p, A->i, cant, first.data(), ncols.data(), cptr.data(),
                              child.data(), count.data(), &h),
           "mdgpu_analyze_tree");
-    check(mdgpu_factor(h, A->x, MDGPU_FP64, NULL), "mdgpu_factor");
     std::vector<long long> Lp(A->n + 1);
-    check(mdgpu_get_L(h, Lp.data(), spL->i, spL->x), "mdgpu_get_L");
+    numeric(h, A->p[A->n], A->x, spL->p[A->n], spL->i, spL->x, Lp.data());
     mdgpu_destroy(h);
 }

@@ -25,6 +25,9 @@
  * Usage: mdgpu_ref_harness [-amd] [-sn | -rn z] [-b bs] [-nofactor] [-bfile f]
  *                          <matrix triplet file> <output dir>
  * Outputs raw little-endian arrays (.i32 / .f64) and meta.json in <output dir>.
+ * The scalar is the reference's FLOTANTE (types.h:4-24): double in the FP64
+ * build, float in the reference's default build; values are written as f64
+ * either way and the right-hand side file holds f64 values.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -51,7 +54,8 @@ static double now_s() {
 }
 
 /* make_sym is file-static in mdgpu.cu:1630-1638; same three CSparse calls. */
-static int keep_offdiag(int i, int j, double, void*) { return i != j; }
+typedef FLOTANTE Val;
+static int keep_offdiag(int i, int j, Val, void*) { return i != j; }
 static cs* sym_from_lower(cs* A) {
     cs* AT = cs_transpose(A, 1);
     cs_fkeep(AT, &keep_offdiag, NULL);
@@ -60,9 +64,9 @@ static cs* sym_from_lower(cs* A) {
     return C;
 }
 
-static double inf_norm(const double* x, int n) {
+static double inf_norm(const Val* x, int n) {
     double m = 0;
-    for (int i = 0; i < n; i++) m = std::max(m, fabs(x[i]));
+    for (int i = 0; i < n; i++) m = std::max(m, fabs((double)x[i]));
     return m;
 }
 
@@ -75,7 +79,10 @@ static void dump(const char* name, const void* data, size_t bytes) {
     fclose(f);
 }
 static void dump_i32(const char* name, const int* v, size_t n) { dump(name, v, n * sizeof(int)); }
-static void dump_f64(const char* name, const double* v, size_t n) { dump(name, v, n * sizeof(double)); }
+static void dump_f64(const char* name, const Val* v, size_t n) {
+    std::vector<double> d(v, v + n);
+    dump(name, d.data(), n * sizeof(double));
+}
 
 int main(int argc, char** argv) {
     bool amd = false, sn = false, rn = false, do_factor = true;
@@ -188,7 +195,7 @@ int main(int argc, char** argv) {
     spL->nzmax = (int)nz;
     spL->nz = -1;
     spL->i = (int*)calloc(nz > 0 ? nz : 1, sizeof(int));
-    spL->x = (double*)calloc(nz > 0 ? nz : 1, sizeof(double));
+    spL->x = (Val*)calloc(nz > 0 ? nz : 1, sizeof(Val));
     double t_symbolic = now_s() - t1;
 
     /* ---- dump symbolic ---- */
@@ -226,16 +233,18 @@ int main(int argc, char** argv) {
         dump_f64("Lx.f64", spL->x, nz);
 
         /* ---- solve + residual: mdgpu.cu:1941-1973 ---- */
-        std::vector<double> b(n), x(n), x2(n);
+        std::vector<Val> b(n), x(n), x2(n);
         if (bfile) {
+            std::vector<double> bd(n);
             FILE* fb = fopen(bfile, "rb");
-            if (!fb || fread(b.data(), sizeof(double), n, fb) != (size_t)n) {
+            if (!fb || fread(bd.data(), sizeof(double), n, fb) != (size_t)n) {
                 fprintf(stderr, "cannot read %s\n", bfile);
                 return 2;
             }
             fclose(fb);
+            for (int i = 0; i < n; i++) b[i] = (Val)bd[i];
         } else {
-            for (int i = 0; i < n; i++) b[i] = 1 + ((double)i) / n;
+            for (int i = 0; i < n; i++) b[i] = 1 + ((Val)i) / n;
         }
         double t3 = now_s();
         x = b;
@@ -245,7 +254,7 @@ int main(int argc, char** argv) {
         if (amd_perm) cs_ipvec(amd_perm, x.data(), x2.data(), n);
         else x2 = x;
         t_solve = now_s() - t3;
-        std::vector<double> r(n);
+        std::vector<Val> r(n);
         for (int i = 0; i < n; i++) r[i] = -b[i];
         cs* C = sym_from_lower(C_low);
         cs_gaxpy(C, x2.data(), r.data());

@@ -39,12 +39,14 @@ void grid(int side, int& n, std::vector<int>& Ap, std::vector<int>& Ai) {
 struct Case {
     Plan P;
     SolveScheduleHost Q;
+    PanelSchedule PS;
     std::vector<int> level, rowptr, col, src;
 };
 
 std::string run(const Case& c, const Symbolic& S) {
-    const std::string m = check_plan(c.P, S, c.Q, c.level, c.rowptr, c.col.data(), c.src.data(),
-                                     (int64_t)c.col.size());
+    std::string m = check_plan(c.P, S, c.Q, c.level, c.rowptr, c.col.data(), c.src.data(),
+                               (int64_t)c.col.size());
+    if (m.empty()) m = check_panel_schedule(c.P, c.PS, c.level, 64, 256);
     return m.empty() ? "ok" : m;
 }
 
@@ -60,6 +62,8 @@ int main(int argc, char** argv) {
     Case base;
     build_plan(S, Ap[n], Plan::kSmallMaxRows, base.P);
     build_solve_schedule(base.P, 64, base.Q);
+    build_large_tables(base.P, 64, 16);
+    build_panel_schedule(base.P, 64, 256, 16, base.PS);
     base.level = front_levels(base.P);
     // the residual's CSR: only its ranges are checked, so rows in order
     base.rowptr.assign(n + 1, 0);
@@ -144,6 +148,39 @@ int main(int argc, char** argv) {
         const int s = P.fronts[s_rel].parent;
         c.level[s_rel] = c.level[s];
         bad.push_back({"level", c});
+    }
+    {
+        // a front's second diagonal task moved behind a task that waits on it
+        Case c = base;
+        int64_t td = -1, tl = -1;
+        for (const PanelOp& o : c.PS.ops) {
+            if (o.kind != OP_PANEL || o.arg != 0) continue;
+            for (int64_t t = o.toff; t < o.toff + o.ntasks; ++t)
+                if (c.PS.tasks[2 * t] == s_piv && c.PS.tasks[2 * t + 1] == 1) td = t;
+            if (td >= 0) {
+                tl = o.toff + o.ntasks - 1;
+                break;
+            }
+        }
+        if (td < 0) return 6;
+        std::swap(c.PS.tasks[2 * td], c.PS.tasks[2 * tl]);
+        std::swap(c.PS.tasks[2 * td + 1], c.PS.tasks[2 * tl + 1]);
+        bad.push_back({"panel", c});
+    }
+    {
+        // two update matrices live at the same level given the same storage
+        Case c = base;
+        int a = -1, b = -1;
+        for (int s = 0; s < P.nsuper && b < 0; ++s)
+            if (P.fronts[s].uoff >= 0 && c.level[s] == 0) {
+                if (a < 0)
+                    a = s;
+                else
+                    b = s;
+            }
+        if (b < 0) return 7;
+        c.P.fronts[b].uoff = c.P.fronts[a].uoff;
+        bad.push_back({"uoff", c});
     }
     for (auto& b : bad) std::printf("%s: %s\n", b.first.c_str(), run(b.second, S).c_str());
     return 0;

@@ -90,3 +90,35 @@ def test_batch_factor_and_solve_match_each_system_alone():
         r = b[r0:r1] - A @ xr[r0:r1]
         den = abs(A).sum(axis=1).max() * np.abs(xr[r0:r1]).max() + np.abs(b[r0:r1]).max()
         assert np.abs(r).max() / den <= 1e-13
+
+
+@pytest.mark.gpu
+def test_batch_matches_the_oracle_system_by_system():
+    """Every system's block of the batch factor against the oracle (the
+    restatement of the reference's CPU path) run on that system alone: the
+    same L pattern, L within 1e-12 relative Frobenius, the solution within
+    1e-10 of the oracle's.  The mix includes 3D grids large enough for tiled
+    fronts, so the batch's panel launches hold fronts of several systems."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from oracle import oracle as O
+
+    syss = _systems(seed=2, k=6) + [mg.laplacian_3d_varcoef(14, seed=5, sigma=0.5, shift=1e-2),
+                                    mg.laplacian_3d_varcoef(12, seed=6)]
+    B = M.Solver.batch([(n, Ap, Ai) for (n, Ap, Ai, _) in syss])
+    assert B.info("large_fronts") > 0
+    Ax = np.concatenate([s[3] for s in syss])
+    b = np.concatenate([mg.rhs_uniform(s[0], seed=11 + q) for q, s in enumerate(syss)])
+    B.factor(Ax, M.FP64)
+    x = B.solve(b)
+    Lp, Li, Lx = B.get_L()
+    for q, (n, Ap, Ai, Axq) in enumerate(syss):
+        P = O.Plan(n, Ap, Ai, Axq, amd=True, mode="sn")
+        ref = P.factor()
+        r0, r1 = B.row_off[q], B.row_off[q + 1]
+        seg = slice(Lp[r0], Lp[r1])
+        np.testing.assert_array_equal(Li[seg] - r0, ref["Li"])
+        assert np.linalg.norm(Lx[seg] - ref["Lx"]) <= 1e-12 * np.linalg.norm(ref["Lx"]), q
+        xr = P.solve(ref["Li"], ref["Lx"], b[r0:r1])
+        assert np.abs(x[r0:r1] - xr).max() <= 1e-10 * np.abs(xr).max(), q

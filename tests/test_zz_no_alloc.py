@@ -77,3 +77,30 @@ def test_noalloc_solve_rejects_requests_beyond_its_scratch():
     x1 = S.solve(db1)
     np.testing.assert_allclose(dx1.cpu().numpy(), x1.cpu().numpy(), rtol=1e-12,
                                atol=1e-12 * float(x1.abs().max()))
+
+
+def test_noalloc_solve_allocates_nothing_and_chunks_more_than_64_rhs():
+    """After one warm-up call, further calls -- 70 and 65 right-hand sides
+    (two 64-column chunks reusing the same work vectors) and one -- leave the
+    device's free memory unchanged, and each matches the regular solve."""
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(10, seed=3)
+    S = M.Solver(n, Ap, Ai)
+    S.factor(Ax, M.FP32)
+    B = mg.rhs_uniform(n, seed=21, nrhs=70).reshape(n, 70)
+    dB = _colmajor(B)
+    refs = {k: S.solve(_colmajor(B[:, :k])).cpu().numpy().reshape(n, k) for k in (70, 65, 1)}
+    dX = torch.full_like(dB, float("nan"))
+    assert _noalloc(S, dB, dX, 70) == 0, M.lib().mdgpu_last_error().decode()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in (70, 65, 1, 70):
+        dX.fill_(float("nan"))
+        rc = _noalloc(S, dB, dX, k)
+        assert rc == 0, M.lib().mdgpu_last_error().decode()
+        torch.cuda.synchronize()
+        x = dX[:, :k].cpu().numpy()
+        xr = refs[k]
+        assert np.all(np.isfinite(x)), k
+        np.testing.assert_allclose(x, xr, rtol=1e-12, atol=1e-12 * np.abs(xr).max())
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
