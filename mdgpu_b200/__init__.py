@@ -261,13 +261,16 @@ class Solver:
 
     # ---- numeric -----------------------------------------------------
     def factor(self, Ax, precision=FP64, stream=None):
-        """Ax: numpy float64 (host) or a CUDA torch tensor (device)."""
+        """Ax: numpy float64 (host) or a CUDA torch tensor (device).  Every
+        successful factor advances self.generation (which factor the handle
+        holds: callers that keep results across factors compare it)."""
         if hasattr(Ax, "data_ptr"):
             _check(lib().mdgpu_factor_device(self._h, _tensor_ptr(Ax), int(precision), stream),
                    self._h)
         else:
             Ax = np.ascontiguousarray(Ax, dtype=np.float64)
             _check(lib().mdgpu_factor(self._h, _ptr(Ax), int(precision), stream), self._h)
+        self.generation = getattr(self, "generation", 0) + 1
 
     def _device_layout(self, T):
         """(nrhs, leading dimension) of a column-major float64 CUDA tensor of

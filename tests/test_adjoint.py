@@ -129,3 +129,31 @@ def test_autograd_front_end():
     np.testing.assert_allclose(tb.grad.cpu().numpy(), 2 * x, rtol=1e-10, atol=0)
     sign, ld = np.linalg.slogdet(_dense(n, Ap, Ai, Ax))
     assert abs(float(loss.detach()) - (ld + b @ x)) <= 1e-10 * abs(ld + b @ x)
+
+
+@pytest.mark.gpu
+def test_autograd_two_forwards_on_one_solver_then_backwards():
+    """Two forwards on one Solver (the second refactors it) before either
+    backward: each backward differentiates its own values (it refactors them
+    when the Solver's factor generation moved on), matching the dense
+    gradient of each."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from mdgpu_b200.autograd import logdet_quad
+
+    n, Ap, Ai, Ax1 = mg.laplacian_3d_varcoef(7, seed=11, sigma=0.5, shift=1e-2)
+    Ax2 = mg.laplacian_3d_varcoef(7, seed=12, sigma=0.5, shift=1e-2)[3]
+    b = mg.rhs_uniform(n, seed=13)
+    S = M.Solver(n, Ap, Ai)
+    t1 = torch.from_numpy(Ax1).cuda().requires_grad_(True)
+    t2 = torch.from_numpy(Ax2).cuda().requires_grad_(True)
+    tb = torch.from_numpy(b).cuda()
+    l1 = logdet_quad(S, t1, tb)
+    l2 = logdet_quad(S, t2, tb)
+    l1.backward()
+    l2.backward()
+    for t, A in ((t1, Ax1), (t2, Ax2)):
+        Gd = _dense_grad(n, Ap, Ai, A, b)
+        np.testing.assert_allclose(t.grad.cpu().numpy(), Gd, rtol=0,
+                                   atol=1e-10 * np.abs(Gd).max())

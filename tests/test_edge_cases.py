@@ -96,3 +96,34 @@ def test_repeated_entries_keep_the_last_value():
     S0 = M.Solver(n, Ap, Ai, ordering=M.ORDER_NATURAL)
     S0.factor(Ax)
     np.testing.assert_allclose(S.get_L()[2], S0.get_L()[2], rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA device")
+def test_nan_with_the_sentinel_payload_in_the_rhs_solves_to_nan_quickly():
+    """The solve marks unpublished pivot-tile slots with the all-ones bit
+    pattern (a NaN).  A right-hand side holding a NaN with exactly that
+    payload must come out as NaN in the solution, promptly and with status
+    OK, not stall the dependent tiles until their waits run out; the other
+    right-hand side of the same call is unaffected."""
+    import time
+
+    from mdgpu_b200 import matgen as mg
+
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(16, seed=0)  # large fronts: tile tasks
+    S = M.Solver(n, Ap, Ai)
+    assert S.info("large_fronts") > 0
+    S.factor(Ax, M.FP64)
+    B = mg.rhs_uniform(n, seed=2, nrhs=2).reshape(n, 2).copy()
+    ref = S.solve(B[:, 1].copy())
+    bad = np.array([-1], dtype=np.int64).view(np.float64)[0]
+    perm = S.array("perm")
+    B[perm[-1], 0] = bad  # the last pivot: the root's last tile
+    B[perm[n // 2], 0] = bad
+    for cols in ([0], [0, 1]):
+        t0 = time.perf_counter()
+        X = S.solve(np.asfortranarray(B[:, cols])).reshape(n, len(cols))
+        assert time.perf_counter() - t0 < 2.0
+        assert np.isnan(X[:, 0]).any()
+        if len(cols) == 2:
+            np.testing.assert_allclose(X[:, 1], ref, rtol=0, atol=1e-12 * np.abs(ref).max())
