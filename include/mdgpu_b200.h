@@ -43,7 +43,12 @@ enum mdgpu_ordering { MDGPU_ORDER_NATURAL = 0, MDGPU_ORDER_AMD = 1 };
 enum mdgpu_tree { MDGPU_TREE_NODAL = 0, MDGPU_TREE_SUPER = 1, MDGPU_TREE_RELAXED = 2 };
 enum mdgpu_precision {
     MDGPU_FP64 = 0, /* plain FP64 factor: the drop-in mode */
-    MDGPU_FP32 = 1  /* FP32 factor; Schur updates of large fronts on TF32 tensor cores */
+    MDGPU_FP32 = 1, /* FP32 factor; Schur updates of large fronts on the tensor cores in
+                       3xTF32 (close to FP32 accuracy) */
+    MDGPU_BF16 = 2  /* FP32 factor whose large-front Schur updates take BF16 operands (one
+                       tensor-core product, FP32 accumulation): for GMRES-IR
+                       (mdgpu_gmres_ir); a factorization that meets a non-positive pivot is
+                       redone in FP32 (mdgpu_info "bf16_fallbacks", "precision_used") */
 };
 
 /*
@@ -134,6 +139,10 @@ MDGPU_API int mdgpu_check_plan(mdgpu_handle h);
  * "ustore_bytes" (the update-matrix store, reused over the matrices'
  * lifetimes), "ustore_total_bytes" (the sum of every update matrix: the store
  * without reuse), "zustore_bytes" (the selected inverse's update parts),
+ * "fp64_diag_tiles" (diagonal tiles of the last FP32 / BF16 factor whose
+ * pivots were weak -- d^2 < a / 1024 or not positive -- and were factored
+ * again in FP64), "bf16_fallbacks", "precision_used" (the current factor's
+ * precision),
  * "rows_total", "nchild", "large_fronts", "small_fronts",
  * "nsys", "solve_work_rows", "amap_rows", "amap_entries". */
 MDGPU_API int mdgpu_info(mdgpu_handle h, const char *key, long long *value);

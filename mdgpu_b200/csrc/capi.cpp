@@ -117,9 +117,11 @@ struct mdgpu_handle_s {
     int nrhs_cap = 0;
     // CUDA graphs of the numeric launch sequences (captured once, replayed)
     bool use_graphs = true;
-    cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
+    cudaGraphExec_t fgraph[3] = {nullptr, nullptr, nullptr};  // per precision
     std::map<int, cudaGraphExec_t> sgraph;  // key: precision * 1024 + rhs count
     int factored = -1;  // precision of the current factor, -1 none
+    int fp64_diag_tiles = 0;  // of the last factor: diagonal tiles redone in FP64
+    int bf16_fallbacks = 0;   // BF16 factors redone in FP32 (non-positive pivot)
     bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dZu64
     double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
     double* dZu64 = nullptr;       // its update parts (plan.zuoff offsets)
@@ -419,7 +421,8 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
     }
     D.prof = &h->prof;
     if (!P.perm.empty()) h->d_perm = h->keep(upload(P.perm));
-    h->d_status = h->keep(dalloc<int>(3));  // not-SPD column, tensor-core error, solve error
+    // not-SPD column, device wait error, solve error, FP64 diagonal tiles
+    h->d_status = h->keep(dalloc<int>(4));
     D.solve.err = h->d_status + 2;
     h->d_Ax = dalloc<double>(std::max<int64_t>(P.nnz_user, 1));
     h->csr.rowptr = h->keep(upload(h->h_csr_rowptr));
@@ -462,7 +465,7 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
             if (h->use_tensor_cores && !P.large_list.empty()) {
                 std::vector<CUtensorMap> maps;
                 std::vector<int> idx;
-                if (build_panel_maps(P, h->dL32, maps, idx) == 0) {
+                if (build_panel_maps(P, h->dL32, maps, idx, false) == 0) {
                     h->D.tmaps = h->keep(upload(maps));
                     h->D.tmap_idx = h->keep(upload(idx));
                 }
@@ -470,6 +473,14 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
         }
         if (!h->dU32) h->dU32 = dalloc<float>(P.ustore);
         if (!h->dD32) h->dD32 = dalloc<float>(P.dinv_total);
+        // the same panels for the BF16 Schur update (64-column boxes)
+        if (precision == MDGPU_BF16 && !h->D.tmaps_bf16 && h->use_tensor_cores &&
+            !P.large_list.empty()) {
+            std::vector<CUtensorMap> maps;
+            std::vector<int> idx;
+            if (build_panel_maps(P, h->dL32, maps, idx, true) == 0)
+                h->D.tmaps_bf16 = h->keep(upload(maps));
+        }
     }
 }
 
@@ -497,9 +508,24 @@ void ensure_solve_storage(mdgpu_handle_s* h, int nrhs) {
     h->nrhs_cap = nrhs;
 }
 
+int do_factor_once(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st);
+
+// MDGPU_BF16 whose factorization meets a non-positive pivot (BF16 rounding
+// of the Schur updates can destroy definiteness when cond(A) u_bf16 is near
+// 1) is factored again in FP32; precision_used records which factor the
+// handle holds.
 int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
+    int rc = do_factor_once(h, dAx, precision, st);
+    if (rc == MDGPU_ERR_NOT_SPD && precision == MDGPU_BF16) {
+        rc = do_factor_once(h, h->d_Ax, MDGPU_FP32, st);
+        if (rc == MDGPU_OK) h->bf16_fallbacks++;
+    }
+    return rc;
+}
+
+int do_factor_once(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
     NvtxRange nvtx("mdgpu_factor");
-    if (precision != MDGPU_FP64 && precision != MDGPU_FP32)
+    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16)
         return fail(MDGPU_ERR_INVALID, "unknown precision");
     ck(cudaSetDevice(h->device), "cudaSetDevice");
     ensure_factor_storage(h, precision);
@@ -513,11 +539,13 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
     h->status_init[1] = 0;
     ck(cudaMemcpyAsync(h->d_status, h->status_init, 2 * sizeof(int), cudaMemcpyHostToDevice, st),
        "status");
+    ck(cudaMemsetAsync(h->d_status + 3, 0, sizeof(int), st), "status");
     auto run = [h, precision](cudaStream_t s) {
         if (precision == MDGPU_FP64)
             factor_levels<double>(h->D, h->dL64, h->dU64, h->dD64, h->d_Ax, h->d_status, s);
         else
-            factor_levels<float>(h->D, h->dL32, h->dU32, h->dD32, h->d_Ax, h->d_status, s);
+            factor_levels<float>(h->D, h->dL32, h->dU32, h->dD32, h->d_Ax, h->d_status, s,
+                                 precision == MDGPU_BF16);
     };
     if (h->use_graphs && !h->prof.on) {
         cudaGraphExec_t& g = h->fgraph[precision];
@@ -527,9 +555,10 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
         run(st);
     }
     ck(cudaGetLastError(), "factor launch");
-    int stat[2] = {big, 0};
-    ck(cudaMemcpyAsync(stat, h->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    int stat[4] = {big, 0, 0, 0};
+    ck(cudaMemcpyAsync(stat, h->d_status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st), "status");
     ck(cudaStreamSynchronize(st), "factor");
+    h->fp64_diag_tiles = stat[3];
     int col = stat[0];
     if (stat[1] != 0) {
         h->factored = -1;
@@ -1210,6 +1239,9 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "lstore_bytes") *value = P.lstore * 8;
     else if (k == "ustore_bytes") *value = P.ustore * 8;
     else if (k == "zustore_bytes") *value = P.zustore * 8;
+    else if (k == "fp64_diag_tiles") *value = h->fp64_diag_tiles;
+    else if (k == "bf16_fallbacks") *value = h->bf16_fallbacks;
+    else if (k == "precision_used") *value = h->factored;
     else if (k == "ustore_total_bytes") {
         long long t = 0;
         for (const FrontDesc& f : P.fronts)

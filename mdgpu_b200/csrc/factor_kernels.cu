@@ -644,7 +644,8 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
 // counter not cleared).
 template <typename T>
 static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv,
-                                      const double* Ax, int* status, cudaStream_t st) {
+                                      const double* Ax, int* status, bool bf16,
+                                      cudaStream_t st) {
     const DevSchedule& S = D.psched;
     const size_t gsm = diag_smem<T>();
     for (int q = S.h_op_beg[level]; q < S.h_op_beg[level + 1]; ++q) {
@@ -691,7 +692,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
             case OP_SCHUR_TC: {
                 ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
                 if constexpr (sizeof(T) == 4)
-                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, st);
+                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, bf16, st);
                 else
                     launch_schur_f64(D, w, op.arg, kPanel, Ls, Us, st);
                 break;
@@ -728,7 +729,7 @@ void init_factor_kernels() {
 // records, so each class keeps its own time.
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool bf16) {
     const bool fork = D.aux && D.fork_ev && D.join_ev && !(D.prof && D.prof->on);
     if (D.fsync && D.nfsync > 0) cudaMemsetAsync(D.fsync, 0, (size_t)D.nfsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
@@ -746,8 +747,8 @@ void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, in
         }
         // FP32 needs the TMA descriptors of the tensor-core path; without them
         // (descriptor encoding unavailable) it keeps the 64-wide tile schedule
-        if (sizeof(T) == 8 || D.tmaps)
-            launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, st);
+        if (sizeof(T) == 8 || (bf16 ? D.tmaps_bf16 != nullptr : D.tmaps != nullptr))
+            launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, bf16, st);
         else
             launch_large_level<T>(D, l, Ls, Us, Dinv, Ax, status, st);
         if (par) cudaStreamWaitEvent(st, D.join_ev, 0);
@@ -755,8 +756,8 @@ void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, in
 }
 
 template void factor_levels<double>(const DevPlan&, double*, double*, double*, const double*,
-                                    int*, cudaStream_t);
+                                    int*, cudaStream_t, bool);
 template void factor_levels<float>(const DevPlan&, float*, float*, float*, const double*, int*,
-                                   cudaStream_t);
+                                   cudaStream_t, bool);
 
 }  // namespace mdgpu

@@ -153,6 +153,7 @@ struct DevPlan {
     // FP32 path: per large front a TMA descriptor of its L panel (the
     // operands of the tensor-core Schur updates)
     CUtensorMap* tmaps = nullptr;
+    CUtensorMap* tmaps_bf16 = nullptr;  // the same panels for the BF16 Schur update
     int* tmap_idx = nullptr;
     DevSchedule psched;
     // sync words of the panel launches, cleared at the start of every
@@ -186,9 +187,13 @@ void init_schur_tc();
 void init_schur_f64();
 void init_panel_kernels();
 
+// bf16 (T = float only): the large fronts' Schur updates take BF16 operands
+// (the MDGPU_BF16 factor); else 3xTF32 (float) or FP64 (double).  status:
+// [0] smallest failing pivot column, [1] device wait error code, [3] count
+// of diagonal tiles refactored in FP64 (weak FP32 pivots)
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
-                   cudaStream_t st);
+                   cudaStream_t st, bool bf16 = false);
 
 // Solves with the factor L (scalar TL) on vectors of type TV.  xp holds the
 // permuted right-hand sides on entry (n x nrhs, ld n) and the permuted
@@ -197,14 +202,16 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st);
 
+// bf16: boxes of 64 columns without swizzle (the BF16 Schur update), else
+// 16 columns with the 128-byte / 32-byte-atom swizzle (3xTF32)
 int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx);
+                     std::vector<int>& idx, bool bf16);
 // one panel launch (OP_PANEL): every row-tile task of the panel's fronts
 template <typename T>
 void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status,
                   cudaStream_t st);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, cudaStream_t st);
+                     float* Us, int* err, bool bf16, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,
                       double* Us, cudaStream_t st);
 

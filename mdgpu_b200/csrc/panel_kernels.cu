@@ -27,6 +27,13 @@
 // trailing update, one TRSM product, one SYRK product and one 64 x 64
 // factorization behind the previous.  The panel's Schur update then reads
 // the finished panel straight from the L store.
+//
+// FP32 factors: each diagonal tile's pivots are compared with the tile's
+// diagonal before its factorization; if one lost more than ten bits to
+// cancellation (or is not positive) the tile is factored again in FP64 from
+// the same values (the FP64 safeguard for weak pivots; the count is
+// reported in status[3]).
+#include <climits>
 #include <cstdio>
 
 #include "device_common.cuh"
@@ -38,6 +45,9 @@ namespace mdgpu {
 namespace {
 
 constexpr int kPanelWaitPolls = 1 << 20;  // ~0.5-1 s at ~1 us per poll
+// FP32 diagonal tiles: a pivot d with d^2 < a / kWeakPivotInv (a: the
+// tile's diagonal entry before the factorization) sends the tile to FP64
+constexpr float kWeakPivotInv = 1024.f;
 
 __device__ __forceinline__ int pn_ld_acquire(const int* p) {
     int v;
@@ -210,6 +220,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     T* W = Bs + TB * LDS;
     const int n = ti.size;
     const T* Xi = Xs + (size_t)(i - klo) * TB * TB;
+    const int col0g = f.first_col + i * TB;
     __syncthreads();  // every reader of Bs and of the X blocks is done
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -220,15 +231,63 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             if (r < n && c < n) v = r >= c ? Xi[c * TB + r] - accd[a][b] : T(0);
             S[r + c * LDS] = v;
         }
-    potrf_tile_core<T, TB>(S, W, n, f.first_col + i * TB, status);
     T* base = Ls + f.loff + i * TB + (int64_t)(i * TB) * f.ldl;
     T* Di = Dinv + dinv_off[s] + (int64_t)i * TB * TB;
-    for (int idx = tid; idx < TB * TB; idx += 256) {
-        const int j = idx >> 6, r = idx & 63;
-        const bool in = r < n && j < n && r >= j;
-        if (in) base[r + (int64_t)j * f.ldl] = S[r + j * LDS];
-        Di[idx] = in ? W[r + j * LDS] : T(0);
+    bool redo64 = false;
+    if constexpr (sizeof(T) == 4) {
+        // FP32 pivots checked against the tile's diagonal before the
+        // factorization: a pivot that lost more than ten bits to
+        // cancellation (d^2 < a / 1024), or a non-positive one, and the tile
+        // is factored again in FP64 from the same updated values
+        __shared__ int s_stat;
+        if (tid == 0) s_stat = INT_MAX;
+        __syncthreads();
+        const float dpre = tid < n ? S[tid * (LDS + 1)] : 1.f;
+        potrf_tile_core<T, TB>(S, W, n, col0g, &s_stat);
+        bool weak = false;
+        if (tid < n) {
+            const float d = S[tid * (LDS + 1)];
+            weak = !(d * d >= dpre * (1.f / kWeakPivotInv));
+        }
+        redo64 = __syncthreads_or(weak || (tid == 0 && s_stat != INT_MAX)) != 0;
+        if (redo64) {
+            double sd[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int r = r0 + a, c = c0 + b;
+                    double v = (r == c) ? 1.0 : 0.0;
+                    if (r < n && c < n)
+                        v = r >= c ? (double)Xi[c * TB + r] - (double)accd[a][b] : 0.0;
+                    sd[a][b] = v;
+                }
+            __syncthreads();  // the row block and S, W are reused below
+            double* S64 = reinterpret_cast<double*>(Xs);  // 2 TB (TB + 1) doubles fit in
+            double* W64 = S64 + TB * LDS;                 // the row block + operand block
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) S64[(r0 + a) + (c0 + b) * LDS] = sd[a][b];
+            potrf_tile_core<double, TB>(S64, W64, n, col0g, status);
+            for (int idx = tid; idx < TB * TB; idx += 256) {
+                const int j = idx >> 6, r = idx & 63;
+                const bool in = r < n && j < n && r >= j;
+                if (in) base[r + (int64_t)j * f.ldl] = (T)S64[r + j * LDS];
+                Di[idx] = in ? (T)W64[r + j * LDS] : T(0);
+            }
+            if (tid == 0) atomicAdd(status + 3, 1);
+        }
+    } else {
+        potrf_tile_core<T, TB>(S, W, n, col0g, status);
     }
+    if (!redo64)
+        for (int idx = tid; idx < TB * TB; idx += 256) {
+            const int j = idx >> 6, r = idx & 63;
+            const bool in = r < n && j < n && r >= j;
+            if (in) base[r + (int64_t)j * f.ldl] = S[r + j * LDS];
+            Di[idx] = in ? W[r + j * LDS] : T(0);
+        }
     __threadfence();
     __syncthreads();
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);

@@ -1,6 +1,7 @@
-// Tensor-core Schur-complement update for FP32 fronts (3xTF32 products, FP32
-// accumulation) on sm_100a: tcgen05.mma with the accumulators in TMEM,
-// operands brought into shared memory by TMA straight from the L panels.
+// Tensor-core Schur-complement update for FP32 fronts (3xTF32 products, or
+// one BF16 product, FP32 accumulation) on sm_100a: tcgen05.mma with the
+// accumulators in TMEM, operands brought into shared memory by TMA straight
+// from the L panels.
 //
 // After pivot panel p (columns [k0, k0 + K), K <= 256) of a large front, the
 // trailing lower part is updated in 128 x 128 tiles (I, J), I >= J >= J0:
@@ -28,6 +29,13 @@
 // Only the panel itself crosses L2 (the hi / lo split is made here, once per
 // chunk and CTA, instead of being stored and read twice).
 //
+// BF16 mode (the MDGPU_BF16 factor): the loaders round each FP32 chunk to
+// BF16 (nearest even) into a K-major copy with the 128-byte swizzle, and one
+// tcgen05.mma kind::f16 per 16 columns replaces the three TF32 products.
+// Per-front power-of-two scaling is not applied: BF16 keeps FP32's 8-bit
+// exponent, so scaling by 2^k would only shift exponents and leave every
+// rounded bit as it is.
+//
 // For 32-bit MN-major operands the only UMMA shared-memory layout is the
 // 128-byte swizzle with 32-byte atoms (32-byte chunks of each 128-byte row
 // permuted by row mod 4, atoms of 4 K-rows); the TMA writes exactly that
@@ -41,6 +49,7 @@
 // error.  The TMA loads never use cluster multicast and only ever read this
 // GPU's own memory.
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,14 +63,23 @@ namespace mdgpu {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
-constexpr int BOX = 32;                                      // TMA box: 32 rows x BK columns
-constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;  // bytes of one operand chunk
-constexpr int STAGE_TMA = STAGE_A + STAGE_B;                 // what the TMA brings per chunk
-// per stage: A, B as loaded (then hi in place), then A_lo, B_lo at + STAGE_TMA
-constexpr int STAGE_BYTES = 2 * STAGE_TMA;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;      // + alignment slack
-constexpr uint32_t TMEM_COLS = 2 * BN;                       // two accumulators
+constexpr int BM = 128, BN = 128;
+constexpr int BOX = 32;               // TMA box: 32 rows x BK columns of FP32
+constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
+
+// Per-mode constants.  3xTF32: 16-column chunks; a stage holds A, B as
+// loaded (hi after the split, in place) and A_lo, B_lo beside them; four
+// stages.  BF16: 64-column chunks; a stage holds A, B as loaded (FP32, no
+// swizzle) and their BF16 copies (K-major, 128-byte swizzle); two stages.
+template <bool BF>
+struct Cfg {
+    static constexpr int BK = BF ? 64 : 16;       // K columns per chunk
+    static constexpr int STAGES = BF ? 2 : 4;
+    static constexpr int OPER = BM * BK * 4;      // bytes of one FP32 operand chunk
+    static constexpr int STAGE_TMA = 2 * OPER;    // what the TMA brings per chunk
+    static constexpr int STAGE_BYTES = BF ? STAGE_TMA + STAGE_TMA / 2 : 2 * STAGE_TMA;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+};
 constexpr int NLOAD_WARPS = 4, MMA_WARP = 4, NTHREADS = 9 * 32;  // warps 5-8: epilogue
 constexpr long long WAIT_LIMIT = 1ll << 22;                  // polls (with backoff)
 
@@ -120,7 +138,7 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 // along M/N (one TMA box, BK K-rows x 128 B), SBO = distance between groups
 // of 4 K-rows (512 B); version 1 (sm_100).
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-    constexpr uint64_t LBO = BOX * BK * 4, SBO = 512;
+    constexpr uint64_t LBO = BOX * 16 * 4, SBO = 512;
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
     d |= (uint64_t)((LBO >> 4) & 0x3FFF) << 16;
@@ -142,6 +160,36 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
             tmem_d),
         "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle (layout type 2):
+// rows of 64 BF16 K-values (128 B), 8-row atoms 1024 B apart (SBO); the
+// 16-byte chunks of row r of an atom sit at chunk ^ (r mod 8).  A K-step of
+// 16 inside the 128-byte row advances the start address by 32 B.
+__device__ __forceinline__ uint64_t make_desc_kmajor(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                   // LBO (unused for swizzled K-major)
+    d |= (uint64_t)((1024 >> 4) & 0x3FFF) << 32;  // SBO: 8 rows of 128 B
+    d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
+}
+
+// instruction descriptor: D f32, A/B bf16 (kind::f16), both K-major,
+// M = 128, N = 128
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) |
+                                ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(da), "l"(db), "r"(IDESC_BF16), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
         : "memory");
 }
 
@@ -180,7 +228,7 @@ struct TileJob {
 __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts,
                                             const int* __restrict__ items,
                                             const int* __restrict__ before, int nitems, int b,
-                                            int panel, int PW) {
+                                            int panel, int PW, int BK) {
     TileJob t;
     const int it = find_item(before, nitems, b);
     t.s = items[it];
@@ -202,15 +250,19 @@ __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts
 // items/before: one entry per large front (its tile count); ntiles: the
 // launch's total.  maps: per large front a tensor map over its FP32 L panel
 // (rows x pivot columns).
+template <bool BF>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int ntiles,
                const int* __restrict__ tmap_idx, const CUtensorMap* __restrict__ maps, int panel,
                int PW, float* __restrict__ Ls, float* __restrict__ Us, int* __restrict__ err) {
     using namespace tc;
+    using C = Cfg<BF>;
+    constexpr int BK = C::BK, STAGES = C::STAGES, OPER = C::OPER, STAGE_TMA = C::STAGE_TMA,
+                  STAGE_BYTES = C::STAGE_BYTES;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];   // TMA bytes landed
-    __shared__ __align__(8) uint64_t split_bar[STAGES];  // hi / lo written (4 warps)
+    __shared__ __align__(8) uint64_t split_bar[STAGES];  // operands prepared (4 warps)
     __shared__ __align__(8) uint64_t empty_bar[STAGES];  // MMAs done reading the stage
     __shared__ __align__(8) uint64_t accf_bar[2];        // accumulator complete
     __shared__ __align__(8) uint64_t acce_bar[2];        // accumulator read out (4 warps)
@@ -253,7 +305,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
         long long issued = 0;
         bool ok = true;
         for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
-            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
             const CUtensorMap* map = maps + tmap_idx[t.s];
             for (int ch = 0; ch < t.nk; ++ch, ++g) {
                 const int st = (int)(g % STAGES);
@@ -269,7 +321,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                         for (int q = 0; q < BM / BOX; ++q) {
                             tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st],
                                             t.I * BM + q * BOX, col);
-                            tc::tma_load_2d(a + STAGE_A + q * BOX * BK * 4, map, &full_bar[st],
+                            tc::tma_load_2d(a + OPER + q * BOX * BK * 4, map, &full_bar[st],
                                             t.J * BN + q * BOX, col);
                         }
                         issued = g + 1;
@@ -279,19 +331,48 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                 // all four warps: wait for the bytes, split, release
                 if (ok && !tc::mbar_wait(&full_bar[st], use & 1, &abort_sh)) ok = false;
                 if (!ok) break;
-                float4* x = reinterpret_cast<float4*>(a);
-                float4* lo = reinterpret_cast<float4*>(a + STAGE_TMA);
+                if constexpr (!BF) {
+                    // 3xTF32: hi in place, lo beside it
+                    float4* x = reinterpret_cast<float4*>(a);
+                    float4* lo = reinterpret_cast<float4*>(a + STAGE_TMA);
 #pragma unroll
-                for (int u = 0; u < STAGE_TMA / 16 / 128; ++u) {
-                    const int e = tid + 128 * u;  // tid < 128 in the loader warps
-                    const float4 v = x[e];
-                    float4 h;
-                    h.x = __uint_as_float(__float_as_uint(v.x) & 0xffffe000u);
-                    h.y = __uint_as_float(__float_as_uint(v.y) & 0xffffe000u);
-                    h.z = __uint_as_float(__float_as_uint(v.z) & 0xffffe000u);
-                    h.w = __uint_as_float(__float_as_uint(v.w) & 0xffffe000u);
-                    x[e] = h;
-                    lo[e] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+                    for (int u = 0; u < STAGE_TMA / 16 / 128; ++u) {
+                        const int e = tid + 128 * u;  // tid < 128 in the loader warps
+                        const float4 v = x[e];
+                        float4 h;
+                        h.x = __uint_as_float(__float_as_uint(v.x) & 0xffffe000u);
+                        h.y = __uint_as_float(__float_as_uint(v.y) & 0xffffe000u);
+                        h.z = __uint_as_float(__float_as_uint(v.z) & 0xffffe000u);
+                        h.w = __uint_as_float(__float_as_uint(v.w) & 0xffffe000u);
+                        x[e] = h;
+                        lo[e] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+                    }
+                } else {
+                    // BF16 (round to nearest even), K-major with the 128-byte
+                    // swizzle: thread (m, kc) converts K columns 8 kc .. 8 kc + 7
+                    // of row m into one 16-byte chunk
+#pragma unroll
+                    for (int o = 0; o < 2; ++o) {
+                        const float* src = reinterpret_cast<const float*>(a + o * OPER);
+                        unsigned char* dst = a + STAGE_TMA + o * (OPER / 2);
+#pragma unroll 2
+                        for (int u = 0; u < 8; ++u) {
+                            const int m = tid, kc = u;
+                            // FP32 staging: box m / 32, K column k at k * 32 + m % 32
+                            const float* sp = src + (m >> 5) * (BOX * BK) + (kc * 8) * BOX + (m & 31);
+                            uint32_t w[4];
+#pragma unroll
+                            for (int h = 0; h < 4; ++h) {
+                                const __nv_bfloat162 p =
+                                    __floats2bfloat162_rn(sp[(2 * h) * BOX], sp[(2 * h + 1) * BOX]);
+                                w[h] = *reinterpret_cast<const uint32_t*>(&p);
+                            }
+                            const int r = m & 7;
+                            *reinterpret_cast<uint4*>(dst + (m >> 3) * 1024 + r * 128 +
+                                                      ((kc ^ r) << 4)) =
+                                make_uint4(w[0], w[1], w[2], w[3]);
+                        }
+                    }
                 }
                 // generic-proxy writes, read next by the tensor core (async proxy)
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -314,7 +395,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
             int tl = 0;  // tiles of this CTA
             bool ok = true, any = false;
             for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x, ++tl) {
-                const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+                const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
                 const int acc = tl & 1;
                 const uint32_t use_acc = (uint32_t)(tl >> 1);
                 if (use_acc > 0 && !tc::mbar_wait(&acce_bar[acc], (use_acc - 1) & 1, &abort_sh)) {
@@ -330,16 +411,26 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
-                    const uint32_t bh = ah + STAGE_A;
-                    const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
+                    if constexpr (!BF) {
+                        const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
+                        const uint32_t bh = ah + OPER;
+                        const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
 #pragma unroll
-                    for (int k = 0; k < BK / 8; ++k) {
-                        const uint32_t o = k * 1024;
-                        tc::mma_tf32(d, tc::make_desc(al + o), tc::make_desc(bh + o),
-                                     (ch > 0 || k > 0) ? 1u : 0u);
-                        tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
-                        tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
+                        for (int k = 0; k < BK / 8; ++k) {
+                            const uint32_t o = k * 1024;
+                            tc::mma_tf32(d, tc::make_desc(al + o), tc::make_desc(bh + o),
+                                         (ch > 0 || k > 0) ? 1u : 0u);
+                            tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
+                            tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
+                        }
+                    } else {
+                        const uint32_t ab = tc::smem_u32(smem + st * STAGE_BYTES + STAGE_TMA);
+                        const uint32_t bb = ab + OPER / 2;
+#pragma unroll
+                        for (int k = 0; k < BK / 16; ++k)
+                            tc::mma_bf16(d, tc::make_desc_kmajor(ab + k * 32),
+                                         tc::make_desc_kmajor(bb + k * 32),
+                                         (ch > 0 || k > 0) ? 1u : 0u);
                     }
                     tc::mma_commit(&empty_bar[st]);
                     any = true;
@@ -364,7 +455,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
         const int quarter = warp & 3;
         int tl = 0;
         for (int b = blockIdx.x; b < ntiles; b += gridDim.x, ++tl) {
-            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW);
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
             const FrontDesc f = fronts[t.s];
             const int acc = tl & 1;
             if (!tc::mbar_wait(&accf_bar[acc], (uint32_t)(tl >> 1) & 1, &abort_sh)) break;
@@ -435,7 +526,7 @@ static EncodeTiledFn encode_fn() {
 // Boxes of 32 rows x 16 columns; reads past the panel's rows or columns
 // return zeros.
 int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx) {
+                     std::vector<int>& idx, bool bf16) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return -1;
     maps.resize(P.large_list.size());
@@ -446,11 +537,12 @@ int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& 
         idx[s] = (int)q;
         cuuint64_t dims[2] = {(cuuint64_t)f.m, (cuuint64_t)f.c};
         cuuint64_t strides[1] = {(cuuint64_t)f.ldl * 4};
-        cuuint32_t box[2] = {tc::BOX, tc::BK};
+        cuuint32_t box[2] = {tc::BOX, (cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK)};
         cuuint32_t estr[2] = {1, 1};
         void* base = const_cast<float*>(L32 + f.loff);
         CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         bf16 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return -2;
     }
@@ -458,15 +550,23 @@ int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& 
 }
 
 void init_schur_tc() {
-    cudaFuncSetAttribute(k_schur_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    cudaFuncSetAttribute(k_schur_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<false>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_schur_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<true>::SMEM_BYTES);
 }
 
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, cudaStream_t st) {
+                     float* Us, int* err, bool bf16, cudaStream_t st) {
     const int grid = std::min(w.nctas, D.num_sms > 0 ? D.num_sms : 148);
-    k_schur_tc<<<grid, tc::NTHREADS, tc::SMEM_BYTES, st>>>(
-        D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas, D.tmap_idx,
-        D.tmaps, panel, PW, Ls, Us, err);
+    if (bf16)
+        k_schur_tc<true><<<grid, tc::NTHREADS, tc::Cfg<true>::SMEM_BYTES, st>>>(
+            D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
+            D.tmap_idx, D.tmaps_bf16, panel, PW, Ls, Us, err);
+    else
+        k_schur_tc<false><<<grid, tc::NTHREADS, tc::Cfg<false>::SMEM_BYTES, st>>>(
+            D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
+            D.tmap_idx, D.tmaps, panel, PW, Ls, Us, err);
 }
 
 }  // namespace mdgpu
