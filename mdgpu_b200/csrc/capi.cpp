@@ -219,6 +219,7 @@ void init_kernels_once() {
     init_schur_tc();
     init_schur_f64();
     init_panel_kernels();
+    init_selinv();
     done = true;
 }
 
@@ -313,17 +314,61 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
         std::vector<int> ll(std::max(P.nsuper, 1)), nxt(D.h_level_ptr.begin(), D.h_level_ptr.end() - 1);
         for (int s = 0; s < P.nsuper; ++s) ll[nxt[lv[s]]++] = s;
         D.level_list = h->keep(upload(ll));
+        // Y scratch: m x 16 for a small front (one CTA), 2 m x 64 for a
+        // large one (Y and a row-major copy of Z_RK); a level's fronts side
+        // by side, levels reuse it
+        std::vector<char> large(P.nsuper, 0);
+        for (int s : P.large_list) large[s] = 1;
         std::vector<int64_t> yo(P.nsuper, 0);
         D.yscr_total = 0;
         for (int l = 0; l < P.nlevels; ++l) {
             int64_t off = 0;
             for (int q = D.h_level_ptr[l]; q < D.h_level_ptr[l + 1]; ++q) {
-                yo[ll[q]] = off;
-                off += (int64_t)P.fronts[ll[q]].m * selinv_block();
+                const int s = ll[q];
+                yo[s] = off;
+                off += (int64_t)P.fronts[s].m * (large[s] ? 2 * selinv_tile() : selinv_block());
             }
             D.yscr_total = std::max(D.yscr_total, off);
         }
         D.yoff = h->keep(upload(yo));
+        // the large fronts' selected-inverse work lists
+        {
+            const int T = selinv_tile();
+            ListStore st;
+            SelSchedule& SS = D.sel;
+            SS.h_gather.assign(P.nlevels, WorkList{0, 0, 0, 0});
+            SS.h_step_beg.assign(P.nlevels + 1, 0);
+            for (int l = 0; l < P.nlevels; ++l) {
+                SS.h_step_beg[l] = (int)SS.h_steps.size();
+                std::vector<std::pair<int, int>> g;
+                int maxb = 0;
+                for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                    const FrontDesc& f = P.fronts[P.large_list[q]];
+                    if (f.parent >= 0 && f.m > f.c) g.push_back({P.large_list[q], (f.m - f.c + 15) / 16});
+                    maxb = std::max(maxb, (f.c + T - 1) / T);
+                }
+                if (!g.empty()) SS.h_gather[l] = st.add(g, 0);
+                for (int t = 0; t < maxb; ++t) {
+                    std::vector<std::pair<int, int>> w;
+                    for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                        const int s = P.large_list[q];
+                        const FrontDesc& f = P.fronts[s];
+                        const int nblk = (f.c + T - 1) / T;
+                        if (t >= nblk) continue;
+                        const int k1 = std::min((nblk - t) * T, f.c);
+                        w.push_back({s, (f.m - k1 + T - 1) / T});
+                    }
+                    SS.h_steps.push_back(st.add(w, t));
+                }
+            }
+            SS.h_step_beg[P.nlevels] = (int)SS.h_steps.size();
+            if (st.items.empty()) {
+                st.items.assign(1, -1);
+                st.ctas_before.assign(1, 0);
+            }
+            SS.items = h->keep(upload(st.items));
+            SS.before = h->keep(upload(st.ctas_before));
+        }
         {
             std::vector<int64_t> zo = P.zuoff;
             if (zo.empty()) zo.assign(1, -1);
@@ -1495,7 +1540,7 @@ int mdgpu_selinv(mdgpu_handle h, void* stream) {
         if (!h->dZu64) h->dZu64 = dalloc<double>(h->plan.zustore);
         if (!h->d_Y) h->d_Y = dalloc<double>(std::max<int64_t>(h->D.yscr_total, 1));
         NvtxRange nvtx("mdgpu_selinv");
-        launch_selinv(h->D, h->dL64, h->dZ64, h->dZu64, h->d_Y, st);
+        launch_selinv(h->D, h->dL64, h->dD64, h->dZ64, h->dZu64, h->d_Y, st);
         ck(cudaGetLastError(), "selected inverse launch");
         ck(cudaStreamSynchronize(st), "selected inverse");
         h->selinv_done = true;

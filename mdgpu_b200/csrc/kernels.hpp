@@ -117,6 +117,18 @@ struct SolveSchedule {
     std::vector<int> warp_cnt;
 };
 
+// Selected inverse of the large fronts: per level a gather list (front, CTAs
+// = 16-column blocks of its update part) and per (level, block step) a list
+// (front, CTAs = 64-row tiles below the step's pivot block); WorkList.step
+// is the block step (0 = the front's last pivot block).
+struct SelSchedule {
+    int* items = nullptr;
+    int* before = nullptr;
+    std::vector<WorkList> h_gather;  // per level
+    std::vector<int> h_step_beg;     // nlevels + 1
+    std::vector<WorkList> h_steps;
+};
+
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
     int num_sms = 0;  // of the handle's device (persistent grids)
@@ -138,6 +150,7 @@ struct DevPlan {
     int* level_list = nullptr;
     std::vector<int> h_level_ptr;  // nlevels + 1
     int64_t* yoff = nullptr;
+    SelSchedule sel;
     int64_t* zuoff = nullptr;  // per supernode: Z's update part in the selinv Zu store
     int64_t yscr_total = 0;
     int* a_front = nullptr;
@@ -186,6 +199,7 @@ void init_solve_kernels();
 void init_schur_tc();
 void init_schur_f64();
 void init_panel_kernels();
+void init_selinv();
 
 // bf16 (T = float only): the large fronts' Schur updates take BF16 operands
 // (the MDGPU_BF16 factor); else 3xTF32 (float) or FP64 (double).  status:
@@ -226,13 +240,14 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
                      cudaStream_t st);
 
 // selected inverse and adjoint (selinv.cu)
-void launch_selinv(const DevPlan& D, const double* Ls, double* Zs, double* Zu, double* Yscr,
-                   cudaStream_t st);
+void launch_selinv(const DevPlan& D, const double* Ls, const double* Dinv, double* Zs,
+                   double* Zu, double* Yscr, cudaStream_t st);
 void launch_grad_lower(const DevPlan& D, int nnz, const int* perm, const double* Zs,
                        const double* x, double* G, cudaStream_t st);
 template <typename T>
 void launch_logdet(const DevPlan& D, const T* Ls, double* partial, double* out, cudaStream_t st);
 int logdet_partials();
-int selinv_block();
+int selinv_block();  // pivot columns per block of the one-CTA (small-front) kernel
+int selinv_tile();   // pivot columns per block step of the large fronts
 
 }  // namespace mdgpu

@@ -11,10 +11,11 @@
 // Z_RR lies inside the front: its pivot part was computed by the later
 // blocks, its update part Z_UU is the parent front's Z on the front's update
 // rows (gathered through the relative map -- the transpose of the
-// extend-add).  So the fronts are processed level by level from the root,
-// one CTA per front; Z of the pivot columns goes to a store laid out like the
-// L panels, Z_UU to the update store (the factor's update matrices are no
-// longer needed).
+// extend-add).  So the fronts are processed level by level from the root:
+// small fronts one CTA each (blocks of 16 columns), large fronts in blocks of
+// 64 columns over many CTAs per front (below); Z of the pivot columns goes to
+// a store laid out like the L panels, Z_UU to the selected inverse's own
+// update store.
 //
 // The gradient of loss = logdet A + b' A^-1 b with respect to the caller's
 // lower-triangle values: with x = A^-1 b, d loss / d A = Z - x x' (symmetric),
@@ -132,6 +133,218 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
+// ---------------------------------------------------------------------------
+// large fronts: the same recurrence in blocks of kSelT = 64 pivot columns
+// (the factor's diagonal tiles, whose inverses W it stored), one launch per
+// phase and block step over every large front of the level, many CTAs per
+// front:
+//   gather  Z_UU from the parent's Z (CTA per front and 16 columns)
+//   y       Y = L_RK W                (CTA per front and 64-row tile of R)
+//   zrk     Z_RK = -Z_RR Y            (CTA per front and 64-row tile of R)
+//   zkk     Z_KK = W'W - Y' Z_RK      (CTA per front)
+// Y and a row-major copy of Z_RK sit in the front's scratch (2 m x 64).
+// ---------------------------------------------------------------------------
+
+constexpr int kSelT = 64;
+// dynamic shared memory of the tiled phases: two 64 x 65 FP64 blocks
+constexpr int kSelSmem = 2 * kSelT * (kSelT + 1) * (int)sizeof(double);
+
+__device__ __forceinline__ double zget(const double* __restrict__ Zs,
+                                       const double* __restrict__ Zu, const FrontDesc& f,
+                                       int64_t zoff, int r, int col) {
+    if (r < col) {
+        const int t = r;
+        r = col;
+        col = t;
+    }
+    if (col < f.c) return Zs[f.loff + r + (int64_t)col * f.ldl];
+    return Zu[zoff + (r - f.c) + (int64_t)(col - f.c) * f.ldu];
+}
+
+// acc[a][b] += sum over q < K of As[q lda + r0 + a] Bs[q ldb + c0 + b]
+__device__ __forceinline__ void sel_gemm(const double* As, int lda, const double* Bs, int ldb,
+                                         int K, double (&acc)[4][4]) {
+    const int tid = threadIdx.x;
+    const int r0 = (tid & 15) * 4, c0 = (tid >> 4) * 4;
+    for (int q = 0; q < K; ++q) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = As[q * lda + r0 + a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = Bs[q * ldb + c0 + b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+}
+
+struct SelStep {
+    int kb, k0, k1, nb;
+};
+__device__ __forceinline__ SelStep sel_step(const FrontDesc& f, int step) {
+    SelStep t;
+    const int nblk = (f.c + kSelT - 1) / kSelT;
+    t.kb = nblk - 1 - step;
+    t.k0 = t.kb * kSelT;
+    t.k1 = min(t.k0 + kSelT, f.c);
+    t.nb = t.k1 - t.k0;
+    return t;
+}
+
+__global__ void __launch_bounds__(256)
+    k_sel_gather(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+                 const int* __restrict__ before, int nitems, const int* __restrict__ relmap,
+                 double* __restrict__ Zs, double* __restrict__ Zu,
+                 const int64_t* __restrict__ zuoff) {
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it], blk = blockIdx.x - before[it];
+    const FrontDesc f = fronts[s];
+    const FrontDesc p = fronts[f.parent];
+    const int u = f.m - f.c;
+    const int64_t zf = zuoff[s], zp = zuoff[f.parent];
+    const int* rm = relmap + f.rows_off + f.c;
+    for (int b = 16 * blk; b < min(16 * blk + 16, u); ++b) {
+        const int pb = rm[b];
+        for (int a = b + (int)threadIdx.x; a < u; a += blockDim.x)
+            Zu[zf + a + (int64_t)b * f.ldu] = zelem(Zs, Zu, p, zp, rm[a], pb);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    k_sel_y(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+            const int* __restrict__ before, int nitems, int step, const double* __restrict__ Ls,
+            const double* __restrict__ Dinv, const int64_t* __restrict__ dinv_off,
+            double* __restrict__ Yscr, const int64_t* __restrict__ yoff) {
+    extern __shared__ double sel_sm[];
+    double* As = sel_sm;                  // kSelT x kSelT
+    double* Bs = As + kSelT * kSelT;      // kSelT x (kSelT + 1)
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it], rt = blockIdx.x - before[it];
+    const FrontDesc f = fronts[s];
+    const SelStep t = sel_step(f, step);
+    const int a0 = t.k1 + kSelT * rt, rows = min(kSelT, f.m - a0);
+    const double* W = Dinv + dinv_off[s] + (int64_t)t.kb * kSelT * kSelT;
+    for (int idx = threadIdx.x; idx < kSelT * kSelT; idx += 256) {
+        const int r = idx & 63, q = idx >> 6;
+        As[q * kSelT + r] =
+            (r < rows && q < t.nb) ? Ls[f.loff + a0 + r + (int64_t)(t.k0 + q) * f.ldl] : 0.0;
+        // W(r, q) column-major: Bs[k][c] = W(k, c) with k = r, c = q
+        Bs[r * (kSelT + 1) + q] = W[r + q * kSelT];
+    }
+    __syncthreads();
+    double acc[4][4] = {};
+    sel_gemm(As, kSelT, Bs, kSelT + 1, t.nb, acc);
+    const int r0 = (threadIdx.x & 15) * 4, c0 = (threadIdx.x >> 4) * 4;
+    double* Y = Yscr + yoff[s];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+        if (r0 + a < rows)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) Y[(int64_t)(a0 + r0 + a - t.k1) * kSelT + c0 + b] = acc[a][b];
+}
+
+__global__ void __launch_bounds__(256)
+    k_sel_zrk(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
+              const int* __restrict__ before, int nitems, int step, double* __restrict__ Zs,
+              const double* __restrict__ Zu, const int64_t* __restrict__ zuoff,
+              double* __restrict__ Yscr, const int64_t* __restrict__ yoff) {
+    extern __shared__ double sel_sm[];
+    double* As = sel_sm;                      // kSelT x (kSelT + 1)
+    double* Bs = As + kSelT * (kSelT + 1);    // kSelT x kSelT
+    const int it = find_item(before, nitems, blockIdx.x);
+    const int s = items[it], rt = blockIdx.x - before[it];
+    const FrontDesc f = fronts[s];
+    const SelStep t = sel_step(f, step);
+    const int a0 = t.k1 + kSelT * rt, rows = min(kSelT, f.m - a0);
+    const int64_t zf = (f.parent >= 0 && f.m > f.c) ? zuoff[s] : -1;
+    double* Y = Yscr + yoff[s];
+    const int ylen = f.m - t.k1;
+    double* Zrk = Y + (int64_t)f.m * kSelT;
+    double acc[4][4] = {};
+    for (int b0 = t.k1; b0 < f.m; b0 += kSelT) {
+        const int cols = min(kSelT, f.m - b0);
+        // As[q][r] = Z(a0 + r, b0 + q): read along the stored columns
+        const bool upper = b0 >= a0 + kSelT;  // every b above every a
+        for (int idx = threadIdx.x; idx < kSelT * kSelT; idx += 256) {
+            const int fast = idx & 63, slow = idx >> 6;
+            const int r = upper ? slow : fast, q = upper ? fast : slow;
+            As[q * (kSelT + 1) + r] =
+                (r < rows && q < cols) ? zget(Zs, Zu, f, zf, a0 + r, b0 + q) : 0.0;
+        }
+        for (int idx = threadIdx.x; idx < kSelT * kSelT; idx += 256) {
+            const int c = idx & 63, q = idx >> 6;
+            Bs[q * kSelT + c] = q < cols ? Y[(int64_t)(b0 + q - t.k1) * kSelT + c] : 0.0;
+        }
+        __syncthreads();
+        sel_gemm(As, kSelT + 1, Bs, kSelT, kSelT, acc);
+        __syncthreads();
+    }
+    (void)ylen;
+    const int r0 = (threadIdx.x & 15) * 4, c0 = (threadIdx.x >> 4) * 4;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + a;
+        if (r >= rows) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = c0 + b;
+            const double v = -acc[a][b];
+            Zrk[(int64_t)(a0 + r - t.k1) * kSelT + c] = v;
+            if (c < t.nb) Zs[f.loff + a0 + r + (int64_t)(t.k0 + c) * f.ldl] = v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    k_sel_zkk(const FrontDesc* __restrict__ fronts, const int* __restrict__ items, int step,
+              double* __restrict__ Zs, const double* __restrict__ Dinv,
+              const int64_t* __restrict__ dinv_off, const double* __restrict__ Yscr,
+              const int64_t* __restrict__ yoff) {
+    extern __shared__ double sel_sm[];
+    double* As = sel_sm;                      // kSelT x (kSelT + 1) each
+    double* Bs = As + kSelT * (kSelT + 1);
+    const int s = items[blockIdx.x];
+    const FrontDesc f = fronts[s];
+    const SelStep t = sel_step(f, step);
+    const double* W = Dinv + dinv_off[s] + (int64_t)t.kb * kSelT * kSelT;
+    const double* Y = Yscr + yoff[s];
+    const double* Zrk = Y + (int64_t)f.m * kSelT;
+    // W'W: As[q][i] = W(q, i)
+    for (int idx = threadIdx.x; idx < kSelT * kSelT; idx += 256) {
+        const int q = idx & 63, i = idx >> 6;
+        const double w = W[q + i * kSelT];
+        As[q * (kSelT + 1) + i] = w;
+        Bs[q * (kSelT + 1) + i] = w;
+    }
+    __syncthreads();
+    double pos[4][4] = {}, neg[4][4] = {};
+    sel_gemm(As, kSelT + 1, Bs, kSelT + 1, t.nb, pos);
+    __syncthreads();
+    // Y' Z_RK over the rows of R
+    for (int a0 = t.k1; a0 < f.m; a0 += kSelT) {
+        const int rows = min(kSelT, f.m - a0);
+        for (int idx = threadIdx.x; idx < kSelT * kSelT; idx += 256) {
+            const int i = idx & 63, q = idx >> 6;
+            const int64_t o = (int64_t)(a0 + q - t.k1) * kSelT + i;
+            As[q * (kSelT + 1) + i] = q < rows ? Y[o] : 0.0;
+            Bs[q * (kSelT + 1) + i] = q < rows ? Zrk[o] : 0.0;
+        }
+        __syncthreads();
+        sel_gemm(As, kSelT + 1, Bs, kSelT + 1, kSelT, neg);
+        __syncthreads();
+    }
+    const int r0 = (threadIdx.x & 15) * 4, c0 = (threadIdx.x >> 4) * 4;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int i = r0 + a, j = c0 + b;
+            if (i < t.nb && j < t.nb && i >= j)
+                Zs[f.loff + (t.k0 + i) + (int64_t)(t.k0 + j) * f.ldl] = pos[a][b] - neg[a][b];
+        }
+}
+
 // G (caller order; zeroed by the caller) of every lower-triangle entry e:
 // its front position (a_pos: row | column << 16 within front a_front[e]).
 __global__ void k_grad_lower(int nnz, const FrontDesc* __restrict__ fronts,
@@ -190,13 +403,34 @@ __global__ void k_logdet_final(int nparts, const double* __restrict__ partial,
 
 constexpr int kLogdetBlocks = 148 * 2;
 
-void launch_selinv(const DevPlan& D, const double* Ls, double* Zs, double* Zu, double* Yscr,
-                   cudaStream_t st) {
+// Level by level from the root: the small fronts one CTA each
+// (k_selinv_front), the large fronts by the tiled phases above, block step
+// by block step (fronts with fewer pivot blocks join the later steps).
+void launch_selinv(const DevPlan& D, const double* Ls, const double* Dinv, double* Zs,
+                   double* Zu, double* Yscr, cudaStream_t st) {
+    const SelSchedule& S = D.sel;
     for (int l = D.nlevels - 1; l >= 0; --l) {
-        const int b = D.h_level_ptr[l], e = D.h_level_ptr[l + 1];
-        if (e > b)
-            k_selinv_front<<<e - b, 256, 0, st>>>(D.fronts, D.level_list + b, D.relmap, Ls, Zs, Zu,
-                                                  D.zuoff, Yscr, D.yoff);
+        const int sb = D.h_small_ptr[l * kSmallBuckets], se = D.h_small_ptr[(l + 1) * kSmallBuckets];
+        if (se > sb)
+            k_selinv_front<<<se - sb, 256, 0, st>>>(D.fronts, D.small_list + sb, D.relmap, Ls, Zs,
+                                                    Zu, D.zuoff, Yscr, D.yoff);
+        const WorkList& g = S.h_gather[l];
+        if (g.nctas > 0)
+            k_sel_gather<<<g.nctas, 256, 0, st>>>(D.fronts, S.items + g.off, S.before + g.off,
+                                                  g.nitems, D.relmap, Zs, Zu, D.zuoff);
+        for (int q = S.h_step_beg[l]; q < S.h_step_beg[l + 1]; ++q) {
+            const WorkList& w = S.h_steps[q];
+            if (w.nctas > 0) {
+                k_sel_y<<<w.nctas, 256, kSelSmem, st>>>(D.fronts, S.items + w.off,
+                                                        S.before + w.off, w.nitems, w.step, Ls,
+                                                        Dinv, D.dinv_off, Yscr, D.yoff);
+                k_sel_zrk<<<w.nctas, 256, kSelSmem, st>>>(D.fronts, S.items + w.off,
+                                                          S.before + w.off, w.nitems, w.step, Zs,
+                                                          Zu, D.zuoff, Yscr, D.yoff);
+            }
+            k_sel_zkk<<<w.nitems, 256, kSelSmem, st>>>(D.fronts, S.items + w.off, w.step, Zs,
+                                                       Dinv, D.dinv_off, Yscr, D.yoff);
+        }
     }
 }
 
@@ -217,5 +451,12 @@ template void launch_logdet<float>(const DevPlan&, const float*, double*, double
 
 int logdet_partials() { return kLogdetBlocks; }
 int selinv_block() { return kSelBlock; }
+
+void init_selinv() {
+    cudaFuncSetAttribute(k_sel_y, cudaFuncAttributeMaxDynamicSharedMemorySize, kSelSmem);
+    cudaFuncSetAttribute(k_sel_zrk, cudaFuncAttributeMaxDynamicSharedMemorySize, kSelSmem);
+    cudaFuncSetAttribute(k_sel_zkk, cudaFuncAttributeMaxDynamicSharedMemorySize, kSelSmem);
+}
+int selinv_tile() { return kSelT; }
 
 }  // namespace mdgpu
