@@ -92,6 +92,7 @@ struct mdgpu_handle_s {
     // row and its first entry in the concatenated lower-triangle values
     std::vector<int> sys_row_off, sys_val_off;
     PanelSchedule pschedh;
+    std::vector<int64_t> pscr_off;  // panel scratch offset per supernode
     bool use_tensor_cores = true;
     DevPlan D;
     std::vector<int> level;
@@ -301,6 +302,22 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
     D.fv_total = D.fv_pub_off + 2 * (int64_t)h->ssched.nflags * kTile;
     D.fv_off = h->keep(upload(h->ssched.fv_off));
     D.dinv_off = h->keep(upload(P.dinv_off));
+    {
+        // panel scratch (3xTF32 path): fronts of one level side by side,
+        // levels reuse it
+        h->pscr_off.assign(P.nsuper, -1);
+        D.pscr_total = 0;
+        for (int l = 0; l < P.nlevels; ++l) {
+            int64_t off = 0;
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
+                const int s = P.large_list[q];
+                h->pscr_off[s] = off;
+                off += 2 * (int64_t)panel_mpad(P.fronts[s].m) * kPanel;
+            }
+            D.pscr_total = std::max(D.pscr_total, off);
+        }
+        D.pscr_off = h->keep(upload(h->pscr_off));
+    }
     D.asm_off = h->keep(upload(P.asm_off));
     D.asm_range = h->keep(upload(P.asm_range));
     D.dinv_total = P.dinv_total;
@@ -506,11 +523,13 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
     } else {
         if (!h->dL32) {
             h->dL32 = dalloc<float>(P.lstore);
-            // TMA descriptors of the L panels (tensor-core Schur updates)
+            // the split panel scratch and its TMA descriptors (3xTF32
+            // tensor-core Schur updates)
             if (h->use_tensor_cores && !P.large_list.empty()) {
+                h->D.pscr = h->keep(dalloc<float>(std::max<int64_t>(h->D.pscr_total, 1)));
                 std::vector<CUtensorMap> maps;
                 std::vector<int> idx;
-                if (build_panel_maps(P, h->dL32, maps, idx, false) == 0) {
+                if (build_panel_maps(P, h->D.pscr, h->pscr_off, maps, idx, false) == 0) {
                     h->D.tmaps = h->keep(upload(maps));
                     h->D.tmap_idx = h->keep(upload(idx));
                 }
@@ -523,7 +542,7 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
             !P.large_list.empty()) {
             std::vector<CUtensorMap> maps;
             std::vector<int> idx;
-            if (build_panel_maps(P, h->dL32, maps, idx, true) == 0)
+            if (build_panel_maps(P, h->dL32, h->pscr_off, maps, idx, true) == 0)
                 h->D.tmaps_bf16 = h->keep(upload(maps));
         }
     }

@@ -686,7 +686,7 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
             }
             case OP_PANEL: {
                 ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
-                launch_panel<T>(D, op, Ls, Dinv, status, st);
+                launch_panel<T>(D, op, Ls, Dinv, status, !bf16, st);
                 break;
             }
             case OP_SCHUR_TC: {

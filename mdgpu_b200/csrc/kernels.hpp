@@ -166,7 +166,15 @@ struct DevPlan {
     // FP32 path: per large front a TMA descriptor of its L panel (the
     // operands of the tensor-core Schur updates)
     CUtensorMap* tmaps = nullptr;
-    CUtensorMap* tmaps_bf16 = nullptr;  // the same panels for the BF16 Schur update
+    CUtensorMap* tmaps_bf16 = nullptr;  // over the L panels, for the BF16 Schur update
+    // FP32 (3xTF32) path: the current panel of every large front of a level,
+    // split: per front 2 mpad x kPanel floats (column kk: rows [0, mpad) the
+    // TF32 part hi, rows [mpad, 2 mpad) lo = x - hi), mpad = m rounded up to
+    // 128; written by the panel kernel, read by the tensor-core Schur update
+    // through tmaps (fronts of a level side by side, levels reuse it)
+    float* pscr = nullptr;
+    int64_t* pscr_off = nullptr;  // per supernode (-1 if small)
+    int64_t pscr_total = 0;
     int* tmap_idx = nullptr;
     DevSchedule psched;
     // sync words of the panel launches, cleared at the start of every
@@ -201,6 +209,9 @@ void init_schur_f64();
 void init_panel_kernels();
 void init_selinv();
 
+// panel scratch rows of a large front (m rounded up to the 128-row tile)
+__host__ __device__ inline int panel_mpad(int m) { return (m + 127) & ~127; }
+
 // bf16 (T = float only): the large fronts' Schur updates take BF16 operands
 // (the MDGPU_BF16 factor); else 3xTF32 (float) or FP64 (double).  status:
 // [0] smallest failing pivot column, [1] device wait error code, [3] count
@@ -216,13 +227,16 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st);
 
-// bf16: boxes of 64 columns without swizzle (the BF16 Schur update), else
-// 16 columns with the 128-byte / 32-byte-atom swizzle (3xTF32)
-int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx, bool bf16);
+// bf16: per large front a map over its FP32 L panel (m x c), boxes of 64
+// columns without swizzle (the BF16 Schur update); else over its split
+// panel scratch (2 mpad x kPanel, base scr + scr_off[s]), boxes of 16 columns
+// with the 128-byte / 32-byte-atom swizzle (3xTF32)
+int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t>& scr_off,
+                     std::vector<CUtensorMap>& maps, std::vector<int>& idx, bool bf16);
 // one panel launch (OP_PANEL): every row-tile task of the panel's fronts
+// split: also write the panel split for 3xTF32 into the panel scratch
 template <typename T>
-void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status,
+void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, bool split,
                   cudaStream_t st);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, bool bf16, cudaStream_t st);

@@ -25,8 +25,11 @@
 // diagonal factorization as separate launches (about nine per panel): the
 // critical path of a panel is the chain of its diagonal tiles, each one
 // trailing update, one TRSM product, one SYRK product and one 64 x 64
-// factorization behind the previous.  The panel's Schur update then reads
-// the finished panel straight from the L store.
+// factorization behind the previous.  With a panel scratch (FP32 factors
+// with 3xTF32 Schur updates) each X(i, k) also goes there split (hi = X with
+// the low 13 mantissa bits cleared, lo = X - hi), columns past the last pivot
+// column as zeros, for the panel's Schur update; BF16 Schur updates read the
+// finished panel straight from the L store.
 //
 // FP32 factors: each diagonal tile's pivots are compared with the tile's
 // diagonal before its factorization; if one lost more than ten bits to
@@ -95,13 +98,25 @@ __device__ __forceinline__ void pn_store_block(T* Bs, const T (&pre)[16]) {
 }
 
 // one 64-column block of the task's row block (rows r < nrows, columns cc <
-// ncols) to the L panel
+// ncols) to the L panel and, with a panel scratch, split to it (all 64
+// columns: zeros past ncols)
 template <typename T>
 __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl, int nrows,
-                                               int ncols) {
+                                               int ncols, float* hi, int mpad) {
     for (int idx = threadIdx.x; idx < kTile * kTile; idx += 256) {
         const int q = idx >> 6, r = idx & 63;
-        if (r < nrows && q < ncols) dst[r + (int64_t)q * ldl] = Xk[idx];
+        if (r >= nrows) continue;
+        const T v = Xk[idx];
+        if (q < ncols) dst[r + (int64_t)q * ldl] = v;
+        if constexpr (sizeof(T) == 4) {
+            if (hi) {
+                const float x = q < ncols ? (float)v : 0.f;
+                const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+                float* p = hi + (int64_t)q * (2 * mpad) + r;
+                p[0] = h;
+                p[mpad] = x - h;
+            }
+        }
     }
 }
 
@@ -120,6 +135,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             int panel, int* __restrict__ counter, int* __restrict__ flags,
             int* __restrict__ abort_flag, int* __restrict__ err,
             const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
+            float* __restrict__ pscr, const int64_t* __restrict__ pscr_off,
             int* __restrict__ status) {
     constexpr int TB = kTile, PT = kPanel / kTile, LDS = TB + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -145,6 +161,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int ncol = (diag ? min((i + 1) * TB, f.c) : min(khi * TB, f.c)) - col0;
     const int64_t tile0 = dinv_off[s] / (TB * TB);  // flag of pivot tile k: flags[tile0 + k]
     T* rowp = Ls + f.loff + ti.start + (int64_t)col0 * f.ldl;
+    float* ps = nullptr;  // this task's rows of the split panel scratch
+    const int mpad = panel_mpad(f.m);
+    if constexpr (sizeof(T) == 4)
+        if (pscr) ps = pscr + pscr_off[s] + ti.start;
 
     for (int idx = tid; idx < kPanel * TB; idx += 256) {
         const int q = idx >> 6, r = idx & 63;
@@ -210,7 +230,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                 Xk[(c0 + b) * TB + r0 + a] = in ? acc[a][b] : T(0);
             }
         __syncthreads();
-        pn_write_block(Xk, rowp + (int64_t)(k - klo) * TB * f.ldl, f.ldl, ti.size, ksz);
+        pn_write_block(Xk, rowp + (int64_t)(k - klo) * TB * f.ldl, f.ldl, ti.size, ksz,
+                       ps ? ps + (int64_t)(k - klo) * TB * (2 * mpad) : nullptr, mpad);
         if (diag) tile_gemm_nt_add<T, TB>(Xk, Xk, accd);
     }
     if (!diag) return;
@@ -288,25 +309,41 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             if (in) base[r + (int64_t)j * f.ldl] = S[r + j * LDS];
             Di[idx] = in ? W[r + j * LDS] : T(0);
         }
+    if constexpr (sizeof(T) == 4) {
+        if (ps) {
+            // the split of L_ii (read back from the L store: this CTA wrote it),
+            // and zeros for the panel's later tiles, above the diagonal here
+            __syncthreads();
+            float* hi = ps + (int64_t)(i - klo) * TB * (2 * mpad);
+            for (int idx = tid; idx < (kPanel - (i - klo) * TB) * TB; idx += 256) {
+                const int q = idx >> 6, r = idx & 63;
+                if (r >= n) continue;
+                const float x = (q < n && r >= q) ? (float)base[r + (int64_t)q * f.ldl] : 0.f;
+                const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+                hi[(int64_t)q * (2 * mpad) + r] = h;
+                hi[(int64_t)q * (2 * mpad) + r + mpad] = x - h;
+            }
+        }
+    }
     __threadfence();
     __syncthreads();
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);
 }
 
 template <typename T>
-void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status,
+void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, bool split,
                   cudaStream_t st) {
     int* counter = D.fsync + op.counter;
     int* flags = D.fsync + D.fsync_flags;
     int* abort_flag = D.fsync + D.fsync_flags + D.nflags_factor;
     k_panel<T><<<op.ntasks, 256, panel_smem_bytes<T>(), st>>>(
         D.fronts, D.psched.tasks + op.toff, op.ntasks, op.arg, counter, flags, abort_flag,
-        status + 1, D.dinv_off, Ls, Dinv, status);
+        status + 1, D.dinv_off, Ls, Dinv, split ? D.pscr : nullptr, D.pscr_off, status);
 }
 
-template void launch_panel<float>(const DevPlan&, const PanelOp&, float*, float*, int*,
+template void launch_panel<float>(const DevPlan&, const PanelOp&, float*, float*, int*, bool,
                                   cudaStream_t);
-template void launch_panel<double>(const DevPlan&, const PanelOp&, double*, double*, int*,
+template void launch_panel<double>(const DevPlan&, const PanelOp&, double*, double*, int*, bool,
                                    cudaStream_t);
 
 void init_panel_kernels() {

@@ -67,20 +67,27 @@ constexpr int BM = 128, BN = 128;
 constexpr int BOX = 32;               // TMA box: 32 rows x BK columns of FP32
 constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
 
-// Per-mode constants.  3xTF32: 16-column chunks; a stage holds A, B as
-// loaded (hi after the split, in place) and A_lo, B_lo beside them; four
-// stages.  BF16: 64-column chunks; a stage holds A, B as loaded (FP32, no
-// swizzle) and their BF16 copies (K-major, 128-byte swizzle); two stages.
+// Per-mode constants.  3xTF32: 16-column chunks; a stage holds A_hi, B_hi,
+// A_lo, B_lo as the panel kernel split them; three stages, two CTAs per SM.
+// BF16: 64-column chunks; a stage holds A, B as loaded (FP32, no swizzle)
+// and their BF16 copies (K-major, 128-byte swizzle); two stages.
 template <bool BF>
 struct Cfg {
     static constexpr int BK = BF ? 64 : 16;       // K columns per chunk
-    static constexpr int STAGES = BF ? 2 : 4;
+    static constexpr int STAGES = BF ? 2 : 3;
     static constexpr int OPER = BM * BK * 4;      // bytes of one FP32 operand chunk
-    static constexpr int STAGE_TMA = 2 * OPER;    // what the TMA brings per chunk
-    static constexpr int STAGE_BYTES = BF ? STAGE_TMA + STAGE_TMA / 2 : 2 * STAGE_TMA;
+    // what the TMA brings per chunk: A, B (BF16: FP32, to be converted) or
+    // A_hi, B_hi, A_lo, B_lo (3xTF32: split by the panel kernel)
+    static constexpr int STAGE_TMA = BF ? 2 * OPER : 4 * OPER;
+    static constexpr int STAGE_BYTES = BF ? STAGE_TMA + STAGE_TMA / 2 : STAGE_TMA;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+    // warps: loaders (BF16: four, they convert; 3xTF32: one TMA warp), one
+    // MMA warp, four epilogue warps
+    static constexpr int NLOAD = BF ? 4 : 1;
+    static constexpr int MMA_WARP = NLOAD;
+    static constexpr int NTHREADS = (NLOAD + 5) * 32;
+    static constexpr int CTAS_PER_SM = BF ? 1 : 2;
 };
-constexpr int NLOAD_WARPS = 4, MMA_WARP = 4, NTHREADS = 9 * 32;  // warps 5-8: epilogue
 constexpr long long WAIT_LIMIT = 1ll << 22;                  // polls (with backoff)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -251,7 +258,7 @@ __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts
 // launch's total.  maps: per large front a tensor map over its FP32 L panel
 // (rows x pivot columns).
 template <bool BF>
-__global__ void __launch_bounds__(tc::NTHREADS, 1)
+__global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_SM)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int ntiles,
                const int* __restrict__ tmap_idx, const CUtensorMap* __restrict__ maps, int panel,
@@ -259,7 +266,8 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
     using namespace tc;
     using C = Cfg<BF>;
     constexpr int BK = C::BK, STAGES = C::STAGES, OPER = C::OPER, STAGE_TMA = C::STAGE_TMA,
-                  STAGE_BYTES = C::STAGE_BYTES;
+                  STAGE_BYTES = C::STAGE_BYTES, NLOAD_WARPS = C::NLOAD,
+                  MMA_WARP = C::MMA_WARP;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];   // TMA bytes landed
     __shared__ __align__(8) uint64_t split_bar[STAGES];  // operands prepared (4 warps)
@@ -300,13 +308,15 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
     const uint32_t tmem = tmem_base_sh;
 
     if (warp < NLOAD_WARPS) {
-        // ---- loaders: TMA (warp 0 lane 0), then the split by all four warps
+        // ---- loaders: TMA (warp 0 lane 0); BF16: then the conversion by all
+        // four loader warps
         long long g = 0;  // chunk counter over this CTA's tiles
         long long issued = 0;
         bool ok = true;
         for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
             const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
             const CUtensorMap* map = maps + tmap_idx[t.s];
+            const int mpad = panel_mpad(fronts[t.s].m);
             for (int ch = 0; ch < t.nk; ++ch, ++g) {
                 const int st = (int)(g % STAGES);
                 const uint32_t use = (uint32_t)(g / STAGES);
@@ -316,38 +326,35 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                         ok = false;
                     } else {
                         tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
-                        const int col = t.k0 + ch * BK;
 #pragma unroll
                         for (int q = 0; q < BM / BOX; ++q) {
-                            tc::tma_load_2d(a + q * BOX * BK * 4, map, &full_bar[st],
-                                            t.I * BM + q * BOX, col);
-                            tc::tma_load_2d(a + OPER + q * BOX * BK * 4, map, &full_bar[st],
-                                            t.J * BN + q * BOX, col);
+                            const int ra = t.I * BM + q * BOX, rb = t.J * BN + q * BOX;
+                            unsigned char* d = a + q * BOX * BK * 4;
+                            if constexpr (BF) {
+                                // the L panel: panel columns from k0
+                                const int col = t.k0 + ch * BK;
+                                tc::tma_load_2d(d, map, &full_bar[st], ra, col);
+                                tc::tma_load_2d(d + OPER, map, &full_bar[st], rb, col);
+                            } else {
+                                // the split scratch: hi rows, then lo rows from mpad
+                                const int col = ch * BK;
+                                tc::tma_load_2d(d, map, &full_bar[st], ra, col);
+                                tc::tma_load_2d(d + OPER, map, &full_bar[st], rb, col);
+                                tc::tma_load_2d(d + 2 * OPER, map, &full_bar[st], mpad + ra, col);
+                                tc::tma_load_2d(d + 3 * OPER, map, &full_bar[st], mpad + rb, col);
+                            }
                         }
                         issued = g + 1;
                     }
                 }
                 ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-                // all four warps: wait for the bytes, split, release
-                if (ok && !tc::mbar_wait(&full_bar[st], use & 1, &abort_sh)) ok = false;
                 if (!ok) break;
-                if constexpr (!BF) {
-                    // 3xTF32: hi in place, lo beside it
-                    float4* x = reinterpret_cast<float4*>(a);
-                    float4* lo = reinterpret_cast<float4*>(a + STAGE_TMA);
-#pragma unroll
-                    for (int u = 0; u < STAGE_TMA / 16 / 128; ++u) {
-                        const int e = tid + 128 * u;  // tid < 128 in the loader warps
-                        const float4 v = x[e];
-                        float4 h;
-                        h.x = __uint_as_float(__float_as_uint(v.x) & 0xffffe000u);
-                        h.y = __uint_as_float(__float_as_uint(v.y) & 0xffffe000u);
-                        h.z = __uint_as_float(__float_as_uint(v.z) & 0xffffe000u);
-                        h.w = __uint_as_float(__float_as_uint(v.w) & 0xffffe000u);
-                        x[e] = h;
-                        lo[e] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+                if constexpr (BF) {
+                    // all four warps: wait for the bytes, convert, release
+                    if (!tc::mbar_wait(&full_bar[st], use & 1, &abort_sh)) {
+                        ok = false;
+                        break;
                     }
-                } else {
                     // BF16 (round to nearest even), K-major with the 128-byte
                     // swizzle: thread (m, kc) converts K columns 8 kc .. 8 kc + 7
                     // of row m into one 16-byte chunk
@@ -359,12 +366,13 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                         for (int u = 0; u < 8; ++u) {
                             const int m = tid, kc = u;
                             // FP32 staging: box m / 32, K column k at k * 32 + m % 32
-                            const float* sp = src + (m >> 5) * (BOX * BK) + (kc * 8) * BOX + (m & 31);
+                            const float* sp =
+                                src + (m >> 5) * (BOX * BK) + (kc * 8) * BOX + (m & 31);
                             uint32_t w[4];
 #pragma unroll
                             for (int h = 0; h < 4; ++h) {
-                                const __nv_bfloat162 p =
-                                    __floats2bfloat162_rn(sp[(2 * h) * BOX], sp[(2 * h + 1) * BOX]);
+                                const __nv_bfloat162 p = __floats2bfloat162_rn(
+                                    sp[(2 * h) * BOX], sp[(2 * h + 1) * BOX]);
                                 w[h] = *reinterpret_cast<const uint32_t*>(&p);
                             }
                             const int r = m & 7;
@@ -373,11 +381,11 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                                 make_uint4(w[0], w[1], w[2], w[3]);
                         }
                     }
+                    // generic-proxy writes, read next by the tensor core (async proxy)
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&split_bar[st]);
                 }
-                // generic-proxy writes, read next by the tensor core (async proxy)
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&split_bar[st]);
             }
         }
         if (!ok && tid == 0) {
@@ -406,7 +414,8 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                 const uint32_t d = tmem + (uint32_t)(acc * BN);
                 for (int ch = 0; ch < t.nk; ++ch, ++g) {
                     const int st = (int)(g % STAGES);
-                    if (!tc::mbar_wait(&split_bar[st], (uint32_t)(g / STAGES) & 1, &abort_sh)) {
+                    if (!tc::mbar_wait(BF ? &split_bar[st] : &full_bar[st],
+                                       (uint32_t)(g / STAGES) & 1, &abort_sh)) {
                         ok = false;
                         break;
                     }
@@ -414,7 +423,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1)
                     if constexpr (!BF) {
                         const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
                         const uint32_t bh = ah + OPER;
-                        const uint32_t al = ah + STAGE_TMA, bl = bh + STAGE_TMA;
+                        const uint32_t al = ah + 2 * OPER, bl = bh + 2 * OPER;
 #pragma unroll
                         for (int k = 0; k < BK / 8; ++k) {
                             const uint32_t o = k * 1024;
@@ -520,13 +529,15 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// One tensor map per large front over its FP32 L panel: m rows x c pivot
-// columns, column-major with leading dimension ldl (a multiple of 8, so the
-// column stride is a multiple of 16 bytes; the panel starts on 128 bytes).
-// Boxes of 32 rows x 16 columns; reads past the panel's rows or columns
-// return zeros.
-int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& maps,
-                     std::vector<int>& idx, bool bf16) {
+// One tensor map per large front.  BF16: over its FP32 L panel, m rows x c
+// pivot columns, column-major with leading dimension ldl (a multiple of 8,
+// so the column stride is a multiple of 16 bytes; the panel starts on 128
+// bytes), boxes of 32 rows x 64 columns without swizzle.  3xTF32: over its
+// split panel scratch, 2 mpad rows (hi then lo) x kPanel columns, boxes of
+// 32 rows x 16 columns with the 128-byte / 32-byte-atom swizzle.  Reads
+// past the rows or columns return zeros.
+int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t>& scr_off,
+                     std::vector<CUtensorMap>& maps, std::vector<int>& idx, bool bf16) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return -1;
     maps.resize(P.large_list.size());
@@ -535,12 +546,24 @@ int build_panel_maps(const Plan& P, const float* L32, std::vector<CUtensorMap>& 
         const int s = P.large_list[q];
         const FrontDesc& f = P.fronts[s];
         idx[s] = (int)q;
-        cuuint64_t dims[2] = {(cuuint64_t)f.m, (cuuint64_t)f.c};
-        cuuint64_t strides[1] = {(cuuint64_t)f.ldl * 4};
-        cuuint32_t box[2] = {tc::BOX, (cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK)};
+        cuuint64_t dims[2], strides[1];
+        cuuint32_t box[2] = {tc::BOX,
+                             (cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK)};
         cuuint32_t estr[2] = {1, 1};
-        void* base = const_cast<float*>(L32 + f.loff);
-        CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box,
+        void* ptr;
+        if (bf16) {
+            dims[0] = (cuuint64_t)f.m;
+            dims[1] = (cuuint64_t)f.c;
+            strides[0] = (cuuint64_t)f.ldl * 4;
+            ptr = const_cast<float*>(base + f.loff);
+        } else {
+            const int mpad = panel_mpad(f.m);
+            dims[0] = (cuuint64_t)(2 * mpad);
+            dims[1] = (cuuint64_t)kPanel;
+            strides[0] = (cuuint64_t)(2 * mpad) * 4;
+            ptr = const_cast<float*>(base + scr_off[s]);
+        }
+        CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, ptr, dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          bf16 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -558,13 +581,15 @@ void init_schur_tc() {
 
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, bool bf16, cudaStream_t st) {
-    const int grid = std::min(w.nctas, D.num_sms > 0 ? D.num_sms : 148);
+    const int sms = D.num_sms > 0 ? D.num_sms : 148;
     if (bf16)
-        k_schur_tc<true><<<grid, tc::NTHREADS, tc::Cfg<true>::SMEM_BYTES, st>>>(
+        k_schur_tc<true><<<std::min(w.nctas, sms * tc::Cfg<true>::CTAS_PER_SM),
+                           tc::Cfg<true>::NTHREADS, tc::Cfg<true>::SMEM_BYTES, st>>>(
             D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
             D.tmap_idx, D.tmaps_bf16, panel, PW, Ls, Us, err);
     else
-        k_schur_tc<false><<<grid, tc::NTHREADS, tc::Cfg<false>::SMEM_BYTES, st>>>(
+        k_schur_tc<false><<<std::min(w.nctas, sms * tc::Cfg<false>::CTAS_PER_SM),
+                            tc::Cfg<false>::NTHREADS, tc::Cfg<false>::SMEM_BYTES, st>>>(
             D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
             D.tmap_idx, D.tmaps, panel, PW, Ls, Us, err);
 }

@@ -351,3 +351,27 @@ def bf16_update_cholesky(A, nb=64, pow2_scale=False):
             Q = (round_bf16(L21 * np.float32(s))).astype(np.float32)
             W[e:, e:] -= (Q @ Q.T) * np.float32(1.0 / (s * s))
     return np.tril(W).astype(np.float64)
+
+
+def cholesky_adjoint_dense(L, Lbar):
+    """Reverse mode of the Cholesky factorization A = L L' (dense, FP64):
+    given L and Lbar (the loss's gradient with respect to the entries of the
+    lower triangle of L), the gradient with respect to the entries of the
+    lower triangle of A, each stored entry a free variable (an off-diagonal
+    one stands for A(i, j) and A(j, i)).  With Phi(X) = the lower triangle
+    of X with its diagonal halved (Murray 2016, "Differentiation of the
+    Cholesky decomposition"):
+        P = Phi(L' Lbar),  S = L^-T P L^-1,
+        Abar = tril(S + S') with the diagonal S(i, i).
+    TEST INFRASTRUCTURE ONLY."""
+    import scipy.linalg as sl
+
+    L = np.asarray(L, dtype=np.float64)
+    Lb = np.tril(np.asarray(Lbar, dtype=np.float64))
+    P = np.tril(L.T @ Lb)
+    P[np.diag_indices_from(P)] *= 0.5
+    X = sl.solve_triangular(L, P.T, lower=True, trans="T").T  # X = P L^-1 (L' X' = P')
+    S = sl.solve_triangular(L, X, lower=True, trans="T")        # L^-T X
+    G = np.tril(S + S.T)
+    G[np.diag_indices_from(G)] = np.diag(S)
+    return G
