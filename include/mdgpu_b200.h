@@ -262,6 +262,23 @@ MDGPU_API int mdgpu_grad_lower(mdgpu_handle h, const double *x, double *G, void 
 MDGPU_API int mdgpu_grad_lower_device(mdgpu_handle h, const double *dx, double *dG, void *stream);
 
 /*
+ * General reverse mode of the factorization (no counterpart in the
+ * reference; the forward structure it reverses is Factor, mdgpu.cu:1394-1608):
+ * given Lbar, the gradient of a loss with respect to the values of L (lnz
+ * entries in the CSC order of mdgpu_get_L / the reference's spL), writes
+ * Abar, the gradient with respect to the caller's lower-triangle values
+ * (nnz entries, caller order; an off-diagonal value stands for A(i,j) and
+ * A(j,i); a repeated entry the assembly drops gets 0).  Needs a current FP64
+ * factor.  Front by front from the root: the adjoints of the Schur update,
+ * the triangular solve and the diagonal-block Cholesky, and the transpose of
+ * the extend-add; only L is read (no update matrix is stored or recomputed).
+ * _device: device pointers, asynchronous on the stream.
+ */
+MDGPU_API int mdgpu_adjoint(mdgpu_handle h, const double *Lbar, double *Abar, void *stream);
+MDGPU_API int mdgpu_adjoint_device(mdgpu_handle h, const double *dLbar, double *dAbar,
+                                   void *stream);
+
+/*
  * Copy L out as compressed columns, the spL contract of the reference
  * (mdgpu.cu:1346-1352, 1859-1875): Lp[n+1] (long long), Li[lnz] row indices
  * ascending with the diagonal first, Lx[lnz] values (FP64; an FP32 factor is

@@ -30,7 +30,8 @@ EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_
            "mdgpu_refine_device", "mdgpu_gmres_ir", "mdgpu_gmres_ir_device",
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
            "mdgpu_last_error", "mdgpu_load_triplet", "mdgpu_logdet", "mdgpu_selinv",
-           "mdgpu_grad_lower", "mdgpu_grad_lower_device")
+           "mdgpu_grad_lower", "mdgpu_grad_lower_device", "mdgpu_adjoint",
+           "mdgpu_adjoint_device")
 
 KERNEL_CLASSES = ("small_front", "assemble", "potrf", "panel", "schur_update", "solve_small",
                   "solve_large", "other")
@@ -99,6 +100,8 @@ def lib():
         L.mdgpu_selinv.argtypes = [vp, vp]
         L.mdgpu_grad_lower.argtypes = [vp, vp, vp, vp]
         L.mdgpu_grad_lower_device.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_adjoint.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_adjoint_device.argtypes = [vp, vp, vp, vp]
         L.mdgpu_status_string.argtypes = [C.c_int]
         L.mdgpu_status_string.restype = C.c_char_p
         L.mdgpu_last_error.restype = C.c_char_p
@@ -416,6 +419,25 @@ class Solver:
         xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
         _check(lib().mdgpu_grad_lower(self._h, None if xa is None else _ptr(xa), _ptr(G), stream),
                self._h)
+        return G[:nnz]
+
+    def adjoint(self, Lbar, stream=None):
+        """Reverse mode of the current FP64 factorization: Lbar, the gradient
+        of a loss with respect to L's values (lnz entries, get_L's order) ->
+        the gradient with respect to the caller's lower-triangle values (nnz
+        entries, caller order).  numpy in, numpy out; a CUDA tensor in, a
+        CUDA tensor out."""
+        nnz = self.info("nnz")
+        if hasattr(Lbar, "data_ptr"):
+            import torch
+
+            G = torch.empty(max(nnz, 1), dtype=torch.float64, device=Lbar.device)
+            _check(lib().mdgpu_adjoint_device(self._h, _tensor_ptr(Lbar.contiguous()),
+                                              _tensor_ptr(G), stream), self._h)
+            return G[:nnz]
+        Lb = np.ascontiguousarray(Lbar, dtype=np.float64)
+        G = np.zeros(max(nnz, 1))
+        _check(lib().mdgpu_adjoint(self._h, _ptr(Lb), _ptr(G), stream), self._h)
         return G[:nnz]
 
     def get_L(self, values=True):

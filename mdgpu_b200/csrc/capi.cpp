@@ -126,6 +126,9 @@ struct mdgpu_handle_s {
     bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dZu64
     double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
     double* dZu64 = nullptr;       // its update parts (plan.zuoff offsets)
+    // general reverse mode: Fbar panels, Ubar store, c x c scratch, Lbar / Abar
+    double *d_Fb = nullptr, *d_Fu = nullptr, *d_W = nullptr, *d_Lbar = nullptr,
+           *d_Abar = nullptr;
     double* d_Y = nullptr;         // its Y scratch
     double* d_logdet = nullptr;    // logdet partial sums, then the result
     double* d_gx = nullptr;        // gradient: x and G on the device (host entry)
@@ -154,6 +157,8 @@ struct mdgpu_handle_s {
             if (g) cudaGraphExecDestroy(g);
         drop_solve_graphs();
         for (void* p : owned) cudaFree(p);
+        for (void* p : {(void*)d_Fb, (void*)d_Fu, (void*)d_W, (void*)d_Lbar, (void*)d_Abar})
+            if (p) cudaFree(p);
         for (void* p : {(void*)dZ64, (void*)dZu64, (void*)d_Y, (void*)d_logdet, (void*)d_gx, (void*)d_gG,
                         (void*)d_gm})
             if (p) cudaFree(p);
@@ -385,6 +390,36 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
             }
             SS.items = h->keep(upload(st.items));
             SS.before = h->keep(upload(st.ctas_before));
+        }
+        // the general reverse mode: gather lists, L's column pointers, the
+        // c x c scratch of every front (a level's fronts side by side)
+        {
+            AdjSchedule& AS = D.adj;
+            ListStore st;
+            AS.h_gather.assign(P.nlevels, WorkList{0, 0, 0, 0});
+            std::vector<int64_t> wo(P.nsuper, 0);
+            AS.wtotal = 1;
+            for (int l = 0; l < P.nlevels; ++l) {
+                std::vector<std::pair<int, int>> g;
+                int64_t off = 0;
+                for (int q = D.h_level_ptr[l]; q < D.h_level_ptr[l + 1]; ++q) {
+                    const int s = ll[q];
+                    const FrontDesc& f = P.fronts[s];
+                    wo[s] = off;
+                    off += (int64_t)f.c * f.c;
+                    if (f.parent >= 0 && f.m > f.c) g.push_back({s, (f.m - f.c + 15) / 16});
+                }
+                AS.wtotal = std::max(AS.wtotal, off);
+                if (!g.empty()) AS.h_gather[l] = st.add(g, 0);
+            }
+            if (st.items.empty()) {
+                st.items.assign(1, -1);
+                st.ctas_before.assign(1, 0);
+            }
+            AS.items = h->keep(upload(st.items));
+            AS.before = h->keep(upload(st.ctas_before));
+            AS.woff = h->keep(upload(wo));
+            AS.Lp = h->keep(upload(P.Lp));
         }
         {
             std::vector<int64_t> zo = P.zuoff;
@@ -1596,6 +1631,46 @@ int mdgpu_grad_lower(mdgpu_handle h, const double* x, double* G, void* stream) {
         if (rc != MDGPU_OK) return rc;
         ck(cudaMemcpyAsync(G, h->d_gG, nnz * sizeof(double), cudaMemcpyDeviceToHost, st), "G");
         ck(cudaStreamSynchronize(st), "gradient");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_adjoint_device(mdgpu_handle h, const double* dLbar, double* dAbar, void* stream) {
+    if (!h || !dLbar || !dAbar) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored != MDGPU_FP64) return fail(MDGPU_ERR_STATE, "the adjoint needs an FP64 factor");
+    return guarded([&]() -> int {
+        NvtxRange nvtx("mdgpu_adjoint");
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        const Plan& P = h->plan;
+        if (!h->d_Fb) h->d_Fb = dalloc<double>(P.lstore);
+        if (!h->d_Fu) h->d_Fu = dalloc<double>(P.zustore);
+        if (!h->d_W) h->d_W = dalloc<double>(h->D.adj.wtotal);
+        launch_adjoint(h->D, (int)P.a_src.size(), h->dL64, dLbar, h->d_Fb, h->d_Fu, h->d_W,
+                       dAbar, st);
+        ck(cudaGetLastError(), "adjoint launch");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_adjoint(mdgpu_handle h, const double* Lbar, double* Abar, void* stream) {
+    if (!h || !Lbar || !Abar) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (h->factored != MDGPU_FP64) return fail(MDGPU_ERR_STATE, "the adjoint needs an FP64 factor");
+    return guarded([&]() -> int {
+        cudaStream_t st = pick_stream(h, stream);
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        const int64_t lnz = h->plan.lnz, nnz = h->plan.nnz_user;
+        if (!h->d_Lbar) h->d_Lbar = dalloc<double>(std::max<int64_t>(lnz, 1));
+        if (!h->d_Abar) h->d_Abar = dalloc<double>(std::max<int64_t>(nnz, 1));
+        ck(cudaMemcpyAsync(h->d_Lbar, Lbar, lnz * sizeof(double), cudaMemcpyHostToDevice, st),
+           "Lbar");
+        int rc = mdgpu_adjoint_device(h, h->d_Lbar, h->d_Abar, stream);
+        if (rc != MDGPU_OK) return rc;
+        ck(cudaMemcpyAsync(Abar, h->d_Abar, nnz * sizeof(double), cudaMemcpyDeviceToHost, st),
+           "Abar");
+        ck(cudaStreamSynchronize(st), "adjoint");
         return MDGPU_OK;
     });
 }

@@ -129,6 +129,19 @@ struct SelSchedule {
     std::vector<WorkList> h_steps;
 };
 
+// General reverse mode (adjoint.cu): per level the fronts with an update
+// part and a parent, for the gather of their Ubar (CTA per 16 columns); L's
+// column pointers; per front the offset of its c x c scratch (a level's
+// fronts side by side, levels reuse it).
+struct AdjSchedule {
+    int* items = nullptr;
+    int* before = nullptr;
+    std::vector<WorkList> h_gather;  // per level
+    int64_t* Lp = nullptr;
+    int64_t* woff = nullptr;
+    int64_t wtotal = 0;
+};
+
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
     int num_sms = 0;  // of the handle's device (persistent grids)
@@ -151,6 +164,7 @@ struct DevPlan {
     std::vector<int> h_level_ptr;  // nlevels + 1
     int64_t* yoff = nullptr;
     SelSchedule sel;
+    AdjSchedule adj;
     int64_t* zuoff = nullptr;  // per supernode: Z's update part in the selinv Zu store
     int64_t yscr_total = 0;
     int* a_front = nullptr;
@@ -261,6 +275,10 @@ void launch_grad_lower(const DevPlan& D, int nnz, const int* perm, const double*
 template <typename T>
 void launch_logdet(const DevPlan& D, const T* Ls, double* partial, double* out, cudaStream_t st);
 int logdet_partials();
+// Abar (nnz entries, caller order) from Lbar (L's CSC values) with the FP64
+// factor Ls: Fb, Fu, Wscr stores of plan lstore, zustore, adj.wtotal doubles
+void launch_adjoint(const DevPlan& D, int nnz, const double* Ls, const double* Lbar, double* Fb,
+                    double* Fu, double* Wscr, double* Abar, cudaStream_t st);
 int selinv_block();  // pivot columns per block of the one-CTA (small-front) kernel
 int selinv_tile();   // pivot columns per block step of the large fronts
 
