@@ -685,6 +685,11 @@ def run_batch_arm(args):
     SB = ShardedBatch(syss, rank, world)
     S = SB.solver
     t_an = time.perf_counter() - t0
+    tuned = None
+    if S is not None:
+        # launch shapes of the small-front kernels for these fronts (config 3:
+        # autotuned), chosen on the FP32 factor before anything is timed
+        tuned = S.autotune(SB.local_values([s[3] for s in syss]), FP32)
     n = SB.n
     flops = float(SB.costs.sum())  # every system's, all ranks together
     stream = torch.cuda.current_stream()
@@ -750,6 +755,7 @@ def run_batch_arm(args):
                            "flops_per_step": flops, "analyze_s_rank0": t_an,
                            "partition": "longest processing time first by estimated flops",
                            "load_gflop_per_rank": [float(v) / 1e9 for v in loads],
+                           "autotuned_shapes_rank0": tuned,
                            "l2": "flushed between steps (256 MiB write)"},
                 "backward_error": be32, "ir_iterations": it32,
                 "fp64": {"ms_per_step": ms64, "value": flops / (ms64 * 1e-3) / 1e9,

@@ -172,6 +172,20 @@ MDGPU_API int mdgpu_get_array(mdgpu_handle h, const char *name, void *dst);
  */
 MDGPU_API int mdgpu_factor(mdgpu_handle h, const double *Ax, int precision, void *stream);
 MDGPU_API int mdgpu_factor_device(mdgpu_handle h, const double *dAx, int precision, void *stream);
+
+/*
+ * Autotuner (no counterpart in the reference): chooses the launch shapes of
+ * the small-front factor kernels for this handle's fronts -- the tiny-front
+ * kernel's grid cap and the threads per CTA of each small-front size bucket
+ * (fronts of at most 64, 96, 128, 160 rows) -- by timing the whole factor of
+ * Ax (host values) in the given precision with CUDA events (median of three
+ * after one untimed run) over the candidates, one shape after another, the
+ * fastest kept.  The choice stays with the handle; the factor's CUDA graphs
+ * are captured again.  *ms_best (optional): the chosen shapes' factor time.
+ * mdgpu_info keys "tuned", "tune_tiny_blocks", "tune_threads_b2" ..
+ * "tune_threads_b5" report it.
+ */
+MDGPU_API int mdgpu_autotune(mdgpu_handle h, const double *Ax, int precision, double *ms_best);
 MDGPU_API int mdgpu_not_spd_column(mdgpu_handle h); /* first failing column (permuted), -1 if none */
 
 /*

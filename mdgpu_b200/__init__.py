@@ -31,7 +31,7 @@ EXPORTS = ("mdgpu_analyze", "mdgpu_analyze_batch", "mdgpu_analyze_tree", "mdgpu_
            "mdgpu_get_L", "mdgpu_profile", "mdgpu_profile_read", "mdgpu_status_string",
            "mdgpu_last_error", "mdgpu_load_triplet", "mdgpu_logdet", "mdgpu_selinv",
            "mdgpu_grad_lower", "mdgpu_grad_lower_device", "mdgpu_adjoint",
-           "mdgpu_adjoint_device")
+           "mdgpu_adjoint_device", "mdgpu_autotune")
 
 KERNEL_CLASSES = ("small_front", "assemble", "potrf", "panel", "schur_update", "solve_small",
                   "solve_large", "other")
@@ -102,6 +102,7 @@ def lib():
         L.mdgpu_grad_lower_device.argtypes = [vp, vp, vp, vp]
         L.mdgpu_adjoint.argtypes = [vp, vp, vp, vp]
         L.mdgpu_adjoint_device.argtypes = [vp, vp, vp, vp]
+        L.mdgpu_autotune.argtypes = [vp, vp, C.c_int, vp]
         L.mdgpu_status_string.argtypes = [C.c_int]
         L.mdgpu_status_string.restype = C.c_char_p
         L.mdgpu_last_error.restype = C.c_char_p
@@ -420,6 +421,18 @@ class Solver:
         _check(lib().mdgpu_grad_lower(self._h, None if xa is None else _ptr(xa), _ptr(G), stream),
                self._h)
         return G[:nnz]
+
+    def autotune(self, Ax, precision=FP64):
+        """Choose the small-front kernels' launch shapes for this handle by
+        timing the factor of Ax (numpy); returns the chosen shapes and the
+        factor time in ms."""
+        Ax = np.ascontiguousarray(Ax, dtype=np.float64)
+        ms = C.c_double()
+        _check(lib().mdgpu_autotune(self._h, _ptr(Ax), int(precision), C.byref(ms)), self._h)
+        out = {"tiny_blocks": self.info("tune_tiny_blocks"), "ms": ms.value}
+        for b in range(2, 6):
+            out["threads_b%d" % b] = self.info("tune_threads_b%d" % b)
+        return out
 
     def adjoint(self, Lbar, stream=None):
         """Reverse mode of the current FP64 factorization: Lbar, the gradient

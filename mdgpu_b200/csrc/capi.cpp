@@ -123,6 +123,7 @@ struct mdgpu_handle_s {
     int factored = -1;  // precision of the current factor, -1 none
     int fp64_diag_tiles = 0;  // of the last factor: diagonal tiles redone in FP64
     int bf16_fallbacks = 0;   // BF16 factors redone in FP32 (non-positive pivot)
+    bool tuned = false;       // launch shapes chosen by mdgpu_autotune
     bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dZu64
     double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
     double* dZu64 = nullptr;       // its update parts (plan.zuoff offsets)
@@ -1341,6 +1342,11 @@ int mdgpu_info(mdgpu_handle h, const char* key, long long* value) {
     else if (k == "fp64_diag_tiles") *value = h->fp64_diag_tiles;
     else if (k == "bf16_fallbacks") *value = h->bf16_fallbacks;
     else if (k == "precision_used") *value = h->factored;
+    else if (k == "tuned") *value = h->tuned;
+    else if (k == "tune_tiny_blocks") *value = h->D.tiny_blocks_cap;
+    else if (k.rfind("tune_threads_b", 0) == 0 && k.size() == 15 && k[14] >= '0' &&
+             k[14] < '0' + kSmallBuckets)
+        *value = h->D.small_threads[k[14] - '0'];
     else if (k == "ustore_total_bytes") {
         long long t = 0;
         for (const FrontDesc& f : P.fronts)
@@ -1631,6 +1637,88 @@ int mdgpu_grad_lower(mdgpu_handle h, const double* x, double* G, void* stream) {
         if (rc != MDGPU_OK) return rc;
         ck(cudaMemcpyAsync(G, h->d_gG, nnz * sizeof(double), cudaMemcpyDeviceToHost, st), "G");
         ck(cudaStreamSynchronize(st), "gradient");
+        return MDGPU_OK;
+    });
+}
+
+int mdgpu_autotune(mdgpu_handle h, const double* Ax, int precision, double* ms_best) {
+    if (!h || !Ax) return fail(MDGPU_ERR_INVALID, "bad arguments");
+    if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
+    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16)
+        return fail(MDGPU_ERR_INVALID, "unknown precision");
+    return guarded([&]() -> int {
+        NvtxRange nvtx("mdgpu_autotune");
+        ck(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = h->stream;
+        ck(cudaMemcpyAsync(h->d_Ax, Ax, h->plan.nnz_user * sizeof(double), cudaMemcpyHostToDevice,
+                           st),
+           "values");
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        DevPlan& D = h->D;
+        // the factor's device time with the current shapes: the graph is
+        // captured again, one untimed factor, then the median of three
+        auto measure = [&]() -> double {
+            for (auto& g : h->fgraph)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+            int rc = do_factor_once(h, h->d_Ax, precision, st);
+            if (rc != MDGPU_OK) throw std::runtime_error(std::string("autotune factor: ") +
+                                                         g_last_error);
+            float t[3];
+            for (float& x : t) {
+                ck(cudaEventRecord(e0, st), "event");
+                do_factor_once(h, h->d_Ax, precision, st);
+                ck(cudaEventRecord(e1, st), "event");
+                ck(cudaEventSynchronize(e1), "event");
+                ck(cudaEventElapsedTime(&x, e0, e1), "event");
+            }
+            std::sort(t, t + 3);
+            return t[1];
+        };
+        // coordinate descent, one pass: each shape over its candidates with
+        // the others held, the fastest kept
+        double best = measure();
+        {
+            const int cand[] = {148 * 4, 148 * 8, 148 * 16};
+            int keep = D.tiny_blocks_cap;
+            for (int c : cand) {
+                if (c == keep) continue;
+                D.tiny_blocks_cap = c;
+                const double t = measure();
+                if (t < best) {
+                    best = t;
+                    keep = c;
+                }
+            }
+            D.tiny_blocks_cap = keep;
+        }
+        for (int b = Plan::kTinyBuckets; b < kSmallBuckets; ++b) {
+            const int cand[] = {128, 256, 512};
+            int keep = D.small_threads[b];
+            for (int c : cand) {
+                if (c == keep) continue;
+                D.small_threads[b] = c;
+                const double t = measure();
+                if (t < best) {
+                    best = t;
+                    keep = c;
+                }
+            }
+            D.small_threads[b] = keep;
+        }
+        for (auto& g : h->fgraph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        h->tuned = true;
+        if (ms_best) *ms_best = best;
         return MDGPU_OK;
     });
 }

@@ -574,7 +574,7 @@ void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double
                             D.h_small_ptr[level * kSmallBuckets + 1];
             const int n16 = cnt[1], n8 = cnt[2];
             const int ntask = n32 + (n16 + 1) / 2 + (n8 + 3) / 4;
-            const int blocks = std::min((ntask + 3) / 4, 148 * 8);
+            const int blocks = std::min((ntask + 3) / 4, D.tiny_blocks_cap);
             k_tiny_fronts<T><<<blocks, 128, smem, st>>>(
                 D.fronts, D.solve.warp_list + beg + (cnt[0] - n32), n32, n16, n8, D.child,
                 D.relmap, D.a_src, D.a_pos, Ax, Ls, Us, status);
@@ -587,7 +587,7 @@ void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double
         int MB = Plan::small_limit[b];
         int LD = MB + 1;
         size_t smem = (size_t)MB * LD * sizeof(T) + (size_t)MB * sizeof(int);
-        int threads = MB <= 16 ? 64 : (MB <= 32 ? 128 : 256);
+        const int threads = D.small_threads[b];
         ProfScope ps(D.prof, KC_SMALL_FRONT, st, 0,
                      D.h_small_bytes[level * kSmallBuckets + b] * sizeof(T) / 8.0);
         k_small_front<T><<<end - beg, threads, smem, st>>>(D.fronts, D.small_list + beg, D.child,

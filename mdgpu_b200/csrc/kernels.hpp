@@ -145,6 +145,12 @@ struct AdjSchedule {
 struct DevPlan {
     int n = 0, nsuper = 0, nlevels = 0;
     int num_sms = 0;  // of the handle's device (persistent grids)
+    // launch shapes of the small-front factor kernels, chosen by
+    // mdgpu_autotune (these defaults otherwise): the tiny-front kernel's grid
+    // cap (blocks of four warps) and the threads of k_small_front per size
+    // bucket
+    int tiny_blocks_cap = 148 * 8;
+    int small_threads[kSmallBuckets] = {64, 128, 256, 256, 256, 256};
     // a second stream and two events: the factor runs a level's small fronts
     // beside its large fronts (both depend only on lower levels)
     cudaStream_t aux = nullptr;
