@@ -26,10 +26,11 @@
 // critical path of a panel is the chain of its diagonal tiles, each one
 // trailing update, one TRSM product, one SYRK product and one 64 x 64
 // factorization behind the previous.  With a panel scratch (FP32 factors
-// with 3xTF32 Schur updates) each X(i, k) also goes there split (hi = X with
-// the low 13 mantissa bits cleared, lo = X - hi), columns past the last pivot
-// column as zeros, for the panel's Schur update; BF16 Schur updates read the
-// finished panel straight from the L store.
+// with 3xTF32 Schur updates) every task finally writes its rows of the
+// finished panel there split (hi = X with the low 13 mantissa bits cleared,
+// lo = X - hi), columns past the last pivot column as zeros, for the panel's
+// Schur update -- a diagonal task after publishing its flag, so the split
+// stays off the chain; BF16 Schur updates read the panel from the L store.
 //
 // FP32 factors: each diagonal tile's pivots are compared with the tile's
 // diagonal before its factorization; if one lost more than ten bits to
@@ -98,25 +99,31 @@ __device__ __forceinline__ void pn_store_block(T* Bs, const T (&pre)[16]) {
 }
 
 // one 64-column block of the task's row block (rows r < nrows, columns cc <
-// ncols) to the L panel and, with a panel scratch, split to it (all 64
-// columns: zeros past ncols)
+// ncols) to the L panel
 template <typename T>
 __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl, int nrows,
-                                               int ncols, float* hi, int mpad) {
+                                               int ncols) {
     for (int idx = threadIdx.x; idx < kTile * kTile; idx += 256) {
         const int q = idx >> 6, r = idx & 63;
+        if (r < nrows && q < ncols) dst[r + (int64_t)q * ldl] = Xk[idx];
+    }
+}
+
+// The task's rows of the finished panel (read back from the L store, which
+// this CTA wrote: zeros above the diagonal and past the last pivot column)
+// split into the panel scratch for 3xTF32: hi = x with the low 13 mantissa
+// bits cleared, lo = x - hi; all kPanel columns.
+__device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, int nrows,
+                                              int ncols, float* ps, int mpad) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kPanel * kTile; idx += 256) {
+        const int q = idx >> 6, r = idx & 63;
         if (r >= nrows) continue;
-        const T v = Xk[idx];
-        if (q < ncols) dst[r + (int64_t)q * ldl] = v;
-        if constexpr (sizeof(T) == 4) {
-            if (hi) {
-                const float x = q < ncols ? (float)v : 0.f;
-                const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
-                float* p = hi + (int64_t)q * (2 * mpad) + r;
-                p[0] = h;
-                p[mpad] = x - h;
-            }
-        }
+        const float x = q < ncols ? rowp[r + (int64_t)q * ldl] : 0.f;
+        const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+        float* p = ps + (int64_t)q * (2 * mpad) + r;
+        p[0] = h;
+        p[mpad] = x - h;
     }
 }
 
@@ -230,11 +237,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                 Xk[(c0 + b) * TB + r0 + a] = in ? acc[a][b] : T(0);
             }
         __syncthreads();
-        pn_write_block(Xk, rowp + (int64_t)(k - klo) * TB * f.ldl, f.ldl, ti.size, ksz,
-                       ps ? ps + (int64_t)(k - klo) * TB * (2 * mpad) : nullptr, mpad);
+        pn_write_block(Xk, rowp + (int64_t)(k - klo) * TB * f.ldl, f.ldl, ti.size, ksz);
         if (diag) tile_gemm_nt_add<T, TB>(Xk, Xk, accd);
     }
-    if (!diag) return;
+    // columns of the panel this task's rows hold (beyond: zeros in the split)
+    const int pcols = min(kPanel, f.c - col0);
+    if (!diag) {
+        if constexpr (sizeof(T) == 4)
+            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad);
+        return;
+    }
 
     // diagonal tile (i, i): update, factor with its inverse, store, publish
     T* S = Bs;
@@ -309,25 +321,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             if (in) base[r + (int64_t)j * f.ldl] = S[r + j * LDS];
             Di[idx] = in ? W[r + j * LDS] : T(0);
         }
-    if constexpr (sizeof(T) == 4) {
-        if (ps) {
-            // the split of L_ii (read back from the L store: this CTA wrote it),
-            // and zeros for the panel's later tiles, above the diagonal here
-            __syncthreads();
-            float* hi = ps + (int64_t)(i - klo) * TB * (2 * mpad);
-            for (int idx = tid; idx < (kPanel - (i - klo) * TB) * TB; idx += 256) {
-                const int q = idx >> 6, r = idx & 63;
-                if (r >= n) continue;
-                const float x = (q < n && r >= q) ? (float)base[r + (int64_t)q * f.ldl] : 0.f;
-                const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
-                hi[(int64_t)q * (2 * mpad) + r] = h;
-                hi[(int64_t)q * (2 * mpad) + r + mpad] = x - h;
-            }
-        }
-    }
     __threadfence();
     __syncthreads();
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);
+    // the split for the Schur update, after the flag: off the panel's chain
+    if constexpr (sizeof(T) == 4)
+        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad);
 }
 
 template <typename T>

@@ -62,7 +62,7 @@ def test_bf16_factor_with_gmres_ir_reaches_fp64_accuracy():
     S.factor(Ax, M.BF16)
     b = mg.rhs_uniform(n, seed=4)
     x, berr, it, inner = S.gmres_ir(b, tol=1e-14, maxit=10)
-    assert berr[0] <= 1e-14, (berr, it, inner)
+    assert np.max(berr) <= 1e-14, (berr, it, inner)
     assert O.residual(n, Ap, Ai, Ax, x, b) <= 1e-14
     S64 = M.Solver(n, Ap, Ai)
     S64.factor(Ax, M.FP64)
@@ -78,7 +78,7 @@ def test_weak_pivots_refactored_in_fp64():
     assert S.info("fp64_diag_tiles") > 0
     b = mg.rhs_uniform(n, seed=5)
     x, berr, it, inner = S.gmres_ir(b, tol=1e-14, maxit=10)
-    assert berr[0] <= 1e-14, (berr, it, inner)
+    assert np.max(berr) <= 1e-14, (berr, it, inner)
     # a well-conditioned system keeps every diagonal tile in FP32
     n2, Ap2, Ai2, Ax2 = mg.laplacian_3d_varcoef(14, seed=1, sigma=0.5, shift=1.0)
     S2 = M.Solver(n2, Ap2, Ai2)
