@@ -553,7 +553,8 @@ def run_gpu_arm(args):
         R = B64 - A_full @ X64
         be_host = (np.abs(R).max(axis=0) /
                    (a_inf * np.abs(X64).max(axis=0) + np.abs(B64).max(axis=0)))
-        rhs64 = {"nrhs": 64, "ms_per_step": ms64r,
+        prof64r = S.profile_step(lambda: step_fp32_64())
+        rhs64 = {"nrhs": 64, "ms_per_step": ms64r, "kernels": prof64r["classes"],
                  "max_backward_error": float(np.max(be64)),
                  "max_backward_error_host": float(be_host.max()), "ir_iterations": int(it64),
                  "solve_flops_per_rhs_sweep_pair": 4.0 * S.info("lnz"),

@@ -448,7 +448,7 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
         D.psched.tasks = reinterpret_cast<int2*>(h->keep(upload(pt)));
         D.fsync_flags = h->pschedh.ncounters;
         D.nflags_factor = (int)h->pschedh.nflags;
-        D.nfsync = D.fsync_flags + D.nflags_factor + 1;
+        D.nfsync = D.fsync_flags + 2 * D.nflags_factor + 1;
         D.fsync = h->keep(dalloc<int>(D.nfsync));
         ck(cudaMemset(D.fsync, 0, (size_t)D.nfsync * sizeof(int)), "panel sync words");
     }

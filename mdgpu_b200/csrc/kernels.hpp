@@ -201,7 +201,8 @@ struct DevPlan {
     // sync words of the panel launches, cleared at the start of every
     // factor: one ticket counter per OP_PANEL launch, then one flag per pivot
     // tile of the large fronts (flag of tile k of front s at fsync_flags +
-    // dinv_off[s] / kTile^2 + k), then the abort word
+    // dinv_off[s] / kTile^2 + k), then the abort word, then one step count
+    // per pivot tile (the blocks X(k, .) its diagonal task has written)
     int* fsync = nullptr;
     int nfsync = 0;
     int fsync_flags = 0;

@@ -12,8 +12,13 @@
 //     tile(i, i) -= sum over k' in [klo, i) of X(i, k') X(i, k')'
 // (accumulated step by step as its X(i, k') appear), factors it with its
 // inverse (potrf_tile_core), stores L_ii and inv(L_ii), and publishes a flag.
-// Every task waits for the flag of pivot tile k before step k and reads the
-// published X(k, .) and inv(L_kk) through L2 (ld.cg: never a stale L1 line).
+// Every task reads the published X(k, .) and inv(L_kk) through L2 (ld.cg:
+// never a stale L1 line).  The update products of step k need only the
+// blocks X(k, k') that the diagonal task of tile k has written; it counts
+// them in a step word per tile as it goes, so every task runs them while the
+// diagonal tile is still being factored, and only the TRSM product waits for
+// the tile's flag.  Per pivot tile the chain is then one TRSM product, one
+// SYRK product and one 64 x 64 factorization.
 //
 // Tasks take atomic tickets; the list holds every front's diagonal tasks
 // first (tile by tile), then the rest, so a task only waits on tasks with a
@@ -67,11 +72,11 @@ __device__ __forceinline__ void pn_st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// bounded wait for a published pivot tile; false = aborted (this wait ran
-// out, or another one did)
-__device__ bool pn_wait(const int* flag, int* abort_flag, int* err) {
+// bounded wait for a published word to reach v (a pivot tile's flag: 1; a
+// step count); false = aborted (this wait ran out, or another one did)
+__device__ bool pn_wait(const int* flag, int* abort_flag, int* err, int v = 1) {
     for (int it = 0; it < kPanelWaitPolls; ++it) {
-        if (pn_ld_acquire(flag) != 0) return true;
+        if (pn_ld_acquire(flag) >= v) return true;
         if (pn_ld_relaxed(abort_flag)) return false;
         if (it > 8) __nanosleep(it < 256 ? 32 : 256);
     }
@@ -140,7 +145,7 @@ template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     k_panel(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks, int ntasks,
             int panel, int* __restrict__ counter, int* __restrict__ flags,
-            int* __restrict__ abort_flag, int* __restrict__ err,
+            int* __restrict__ steps, int* __restrict__ abort_flag, int* __restrict__ err,
             const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
             float* __restrict__ pscr, const int64_t* __restrict__ pscr_off,
             int* __restrict__ status) {
@@ -184,10 +189,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
         for (int b = 0; b < 4; ++b) accd[a][b] = T(0);
 
-    for (int k = klo; k < kend; ++k) {
-        if (tid == 0) s_ok = pn_wait(flags + tile0 + k, abort_flag, err) ? 1 : 0;
+    // tid 0 waits for a word to reach v; false (uniform) = aborted
+    auto wait_word = [&](const int* w, int v) -> bool {
+        if (tid == 0) s_ok = pn_wait(w, abort_flag, err, v) ? 1 : 0;
         __syncthreads();
-        if (!s_ok) return;
+        return s_ok != 0;
+    };
+    for (int k = klo; k < kend; ++k) {
         const int ksz = min(TB, f.c - k * TB);
         const T* Lk = Ls + f.loff + k * TB;  // rows of pivot tile k
         const T* Dk = Dinv + dinv_off[s] + (int64_t)k * TB * TB;
@@ -199,21 +207,26 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-        if (nupd > 0)
-            pn_load_block(pre, Lk + (int64_t)col0 * f.ldl, f.ldl, ksz);
-        else
-            pn_load_block(pre, Dk, TB, TB);
-        // tile(i, k) -= X(i, k') X(k, k')' over the panel's earlier tiles
+        // tile(i, k) -= X(i, k') X(k, k')' over the panel's earlier tiles,
+        // each block once the diagonal task of tile k has counted it in (the
+        // next block loads during a product)
         for (int j = 0; j < nupd; ++j) {
+            if (j == 0) {
+                if (!wait_word(steps + tile0 + k, 1)) return;
+                pn_load_block(pre, Lk + (int64_t)col0 * f.ldl, f.ldl, ksz);
+            }
             __syncthreads();  // the previous product is done with Bs
             pn_store_block(Bs, pre);
-            if (j + 1 < nupd)
+            if (j + 1 < nupd) {
+                if (!wait_word(steps + tile0 + k, j + 2)) return;
                 pn_load_block(pre, Lk + (int64_t)(col0 + (j + 1) * TB) * f.ldl, f.ldl, ksz);
-            else
-                pn_load_block(pre, Dk, TB, TB);
+            }
             __syncthreads();
             tile_gemm_nt_add<T, TB>(Xs + (size_t)j * TB * TB, Bs, acc);
         }
+        // the TRSM product waits for the diagonal tile
+        if (!wait_word(flags + tile0 + k, 1)) return;
+        pn_load_block(pre, Dk, TB, TB);
         __syncthreads();
         if (nupd > 0) {
 #pragma unroll
@@ -238,7 +251,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             }
         __syncthreads();
         pn_write_block(Xk, rowp + (int64_t)(k - klo) * TB * f.ldl, f.ldl, ti.size, ksz);
-        if (diag) tile_gemm_nt_add<T, TB>(Xk, Xk, accd);
+        if (diag) {
+            // X(i, k) counted in for the tasks' step-i updates
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) pn_st_release(steps + tile0 + i, k - klo + 1);
+            tile_gemm_nt_add<T, TB>(Xk, Xk, accd);
+        }
     }
     // columns of the panel this task's rows hold (beyond: zeros in the split)
     const int pcols = min(kPanel, f.c - col0);
@@ -335,8 +354,9 @@ void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* stat
     int* counter = D.fsync + op.counter;
     int* flags = D.fsync + D.fsync_flags;
     int* abort_flag = D.fsync + D.fsync_flags + D.nflags_factor;
+    int* steps = abort_flag + 1;
     k_panel<T><<<op.ntasks, 256, panel_smem_bytes<T>(), st>>>(
-        D.fronts, D.psched.tasks + op.toff, op.ntasks, op.arg, counter, flags, abort_flag,
+        D.fronts, D.psched.tasks + op.toff, op.ntasks, op.arg, counter, flags, steps, abort_flag,
         status + 1, D.dinv_off, Ls, Dinv, split ? D.pscr : nullptr, D.pscr_off, status);
 }
 
