@@ -945,6 +945,13 @@ def run_elasticity_arm(args):
     x_ir = dX.cpu().numpy()
     ms64, (be64, _) = timed(step64, max(1, min(args.steps, 3)), 1)
     x64 = dX.cpu().numpy()
+    # where the time goes: the factor alone per precision, and the kernel
+    # classes of one step of each precision mode
+    factor_ms = {}
+    for name, prec in (("bf16", M.BF16), ("fp32", M.FP32), ("fp64", M.FP64)):
+        factor_ms[name], _ = timed(lambda: S.factor(dAx, prec, stream=sptr), 2, 1)
+    kernels = {"bf16_gmres_ir": S.profile_step(step_bf16_gmres)["classes"],
+               "fp32_gmres_ir": S.profile_step(step_gmres)["classes"]}
 
     def fwd(x):
         return float(np.abs(x - x64).max() / np.abs(x64).max())
@@ -975,6 +982,7 @@ def run_elasticity_arm(args):
                      "backward_error": float(np.max(be64)), "backward_error_host": host_berr(x64),
                      "speedup_bf16_gmres_ir_over_fp64": ms64 / ms_b},
             "fp64_diag_tiles": int(S.info("fp64_diag_tiles")),
+            "factor_ms": factor_ms, "kernels": kernels,
             "clocks": clocks}
     print(json.dumps(line), flush=True)
 

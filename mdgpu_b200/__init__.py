@@ -131,6 +131,17 @@ def _tensor_ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+def _dev_stream(stream):
+    """The stream for a call on CUDA tensors: the caller's, else torch's
+    current stream, so the call is ordered with the torch work that made its
+    inputs and with the torch work that reads its outputs."""
+    if stream is not None:
+        return stream
+    import torch
+
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
 def load_triplet(path, matrix_market=False):
     """Read a matrix file as the reference's cs_load + cs_compress do
     (1-based "i j x" triples until the first line that is not one), or a
@@ -269,7 +280,8 @@ class Solver:
         successful factor advances self.generation (which factor the handle
         holds: callers that keep results across factors compare it)."""
         if hasattr(Ax, "data_ptr"):
-            _check(lib().mdgpu_factor_device(self._h, _tensor_ptr(Ax), int(precision), stream),
+            _check(lib().mdgpu_factor_device(self._h, _tensor_ptr(Ax), int(precision),
+                                             _dev_stream(stream)),
                    self._h)
         else:
             Ax = np.ascontiguousarray(Ax, dtype=np.float64)
@@ -303,7 +315,7 @@ class Solver:
             nrhs, ld = self._device_layout(B)
             X = torch.empty((nrhs, self.n), dtype=B.dtype, device=B.device).t()
             _check(lib().mdgpu_solve_device(self._h, _tensor_ptr(B), ld, _tensor_ptr(X),
-                                            self.n, nrhs, stream))
+                                            self.n, nrhs, _dev_stream(stream)))
             return X[:, 0] if B.dim() == 1 else X
         B = np.asarray(B, dtype=np.float64)
         one = B.ndim == 1
@@ -334,7 +346,7 @@ class Solver:
         it = C.c_int()
         _check(lib().mdgpu_refine_device(self._h, _tensor_ptr(B), ldb, _tensor_ptr(X), ldx, nrhs,
                                          float(tol), int(maxit), _ptr(berr), C.byref(it),
-                                         stream))
+                                         _dev_stream(stream)))
         return berr, it.value
 
     def gmres_ir(self, B, tol=1e-14, maxit=10, restart=30, inner_tol=1e-8, stream=None):
@@ -370,7 +382,7 @@ class Solver:
         _check(lib().mdgpu_gmres_ir_device(self._h, _tensor_ptr(B), ldb, _tensor_ptr(X), ldx,
                                            nrhs, float(tol), int(maxit), int(restart),
                                            float(inner_tol), _ptr(berr), _ptr(it), _ptr(inner),
-                                           stream))
+                                           _dev_stream(stream)))
         return berr, it, inner
 
     def profile_step(self, fn):
@@ -413,8 +425,8 @@ class Solver:
             import torch
 
             G = torch.empty(nnz, dtype=torch.float64, device=x.device)
-            _check(lib().mdgpu_grad_lower_device(self._h, _tensor_ptr(x), _tensor_ptr(G), stream),
-                   self._h)
+            _check(lib().mdgpu_grad_lower_device(self._h, _tensor_ptr(x), _tensor_ptr(G),
+                                                 _dev_stream(stream)), self._h)
             return G
         G = np.zeros(max(nnz, 1))
         xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
@@ -445,8 +457,9 @@ class Solver:
             import torch
 
             G = torch.empty(max(nnz, 1), dtype=torch.float64, device=Lbar.device)
-            _check(lib().mdgpu_adjoint_device(self._h, _tensor_ptr(Lbar.contiguous()),
-                                              _tensor_ptr(G), stream), self._h)
+            Lc = Lbar.contiguous()
+            _check(lib().mdgpu_adjoint_device(self._h, _tensor_ptr(Lc), _tensor_ptr(G),
+                                              _dev_stream(stream)), self._h)
             return G[:nnz]
         Lb = np.ascontiguousarray(Lbar, dtype=np.float64)
         G = np.zeros(max(nnz, 1))
