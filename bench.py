@@ -38,13 +38,15 @@ METRIC = "factor+solve time & GFLOP/s, FP32+IR vs FP64 on B200 at backward error
 UNIT = "GFLOP/s"
 REF_SIDE = 28  # CPU sample of the reference arm (the full 64^3 takes ~12 min on one core)
 CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
-# DRAM traffic per algorithmic byte of each kernel class's dominant kernel:
-# dram__bytes_read.sum + dram__bytes_write.sum of single launches captured by
-# ncu on a 48^3 step (one kernel, a few launches, --clock-control none),
-# divided by the same launches' algorithmic bytes.  The roofline line scales
-# the class's algorithmic bytes per launch at the bench size by it (traffic
-# grows with the units processed); None where no capture exists.
-TRAFFIC_PER_ALGO_BYTE = {}
+# DRAM traffic per algorithmic byte of each kernel class:
+# dram__bytes_read.sum + dram__bytes_write.sum of every launch of the class
+# over three FP32 steps of the 48^3 grid (one ncu pass, three metrics,
+# --clock-control none; cold caches per launch), per step, divided by the
+# class's algorithmic bytes of one profiled 48^3 step.  The roofline line
+# scales the class's algorithmic bytes per launch at the bench size by it
+# (traffic grows with the units processed).
+TRAFFIC_PER_ALGO_BYTE = {"panel": 0.80, "schur_update": 0.63, "solve_large": 1.12,
+                         "solve_small": 1.12, "small_front": 1.01, "assemble": 0.53}
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
     "small_front": ["k_tiny_fronts", "k_small_front"],
@@ -389,8 +391,8 @@ def roofline(prof, cls, peaks, peak_src, fp64_peak, class_kernels):
             "traffic": traffic,
             "algorithmic_bytes_per_launch": c["bytes"] / c["launches"],
             "flops_per_launch": c["flops"] / c["launches"],
-            "traffic_source": ("ncu DRAM bytes per algorithmic byte of single launches on a "
-                               "48^3 step, times this launch's algorithmic bytes"
+            "traffic_source": ("ncu DRAM bytes per algorithmic byte of the class over three "
+                               "48^3 steps, times this launch's algorithmic bytes"
                                if ratio is not None else None),
             "peak_source": note, "launches": c["launches"], "ms_total": c["ms"]}
 
