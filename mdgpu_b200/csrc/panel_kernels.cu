@@ -29,13 +29,15 @@
 // This replaces, per panel, the 64-wide steps of TRSM, in-panel update and
 // diagonal factorization as separate launches (about nine per panel): the
 // critical path of a panel is the chain of its diagonal tiles, each one
-// trailing update, one TRSM product, one SYRK product and one 64 x 64
-// factorization behind the previous.  With a panel scratch (FP32 factors
+// TRSM product, one SYRK product and one 64 x 64 factorization behind the
+// previous (the in-panel updates run ahead on the step words).  With a
+// panel scratch (FP32 factors
 // with 3xTF32 Schur updates) every task finally writes its rows of the
 // finished panel there split (hi = X with the low 13 mantissa bits cleared,
 // lo = X - hi), columns past the last pivot column as zeros, for the panel's
-// Schur update -- a diagonal task after publishing its flag, so the split
-// stays off the chain; BF16 Schur updates read the panel from the L store.
+// Schur update (row-major: the K-major operands of the tensor-core update)
+// -- a diagonal task after publishing its flag, so the split stays off the
+// chain; BF16 Schur updates read the panel from the L store.
 //
 // FP32 factors: each diagonal tile's pivots are compared with the tile's
 // diagonal before its factorization; if one lost more than ten bits to
@@ -116,19 +118,31 @@ __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl,
 
 // The task's rows of the finished panel (read back from the L store, which
 // this CTA wrote: zeros above the diagonal and past the last pivot column)
-// split into the panel scratch for 3xTF32: hi = x with the low 13 mantissa
-// bits cleared, lo = x - hi; all kPanel columns.
+// split into the panel scratch for 3xTF32 -- hi = x with the low 13
+// mantissa bits cleared, lo = x - hi -- row-major (a row's kPanel columns
+// contiguous: the K-major operand layout of the Schur update), hi rows from
+// the front's base, lo rows mpad further; all kPanel columns (zeros past
+// the last pivot column).  32-column blocks go through buf (64 x 33 floats)
+// so the global reads run down columns and the writes along rows.
 __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, int nrows,
-                                              int ncols, float* ps, int mpad) {
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kPanel * kTile; idx += 256) {
-        const int q = idx >> 6, r = idx & 63;
-        if (r >= nrows) continue;
-        const float x = q < ncols ? rowp[r + (int64_t)q * ldl] : 0.f;
-        const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
-        float* p = ps + (int64_t)q * (2 * mpad) + r;
-        p[0] = h;
-        p[mpad] = x - h;
+                                              int ncols, float* ps, int mpad, float* buf) {
+    for (int cb = 0; cb < kPanel; cb += 32) {
+        __syncthreads();  // buf free
+        for (int idx = threadIdx.x; idx < kTile * 32; idx += 256) {
+            const int q = idx >> 6, r = idx & 63;
+            buf[r * 33 + q] = (r < nrows && cb + q < ncols) ? rowp[r + (int64_t)(cb + q) * ldl]
+                                                             : 0.f;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kTile * 32; idx += 256) {
+            const int r = idx >> 5, q = idx & 31;
+            if (r >= nrows) continue;
+            const float x = buf[r * 33 + q];
+            const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+            float* p = ps + (int64_t)r * kPanel + cb + q;
+            p[0] = h;
+            p[(int64_t)mpad * kPanel] = x - h;
+        }
     }
 }
 
@@ -173,10 +187,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int ncol = (diag ? min((i + 1) * TB, f.c) : min(khi * TB, f.c)) - col0;
     const int64_t tile0 = dinv_off[s] / (TB * TB);  // flag of pivot tile k: flags[tile0 + k]
     T* rowp = Ls + f.loff + ti.start + (int64_t)col0 * f.ldl;
-    float* ps = nullptr;  // this task's rows of the split panel scratch
+    float* ps = nullptr;  // this task's rows of the split panel scratch (row-major)
     const int mpad = panel_mpad(f.m);
     if constexpr (sizeof(T) == 4)
-        if (pscr) ps = pscr + pscr_off[s] + ti.start;
+        if (pscr) ps = pscr + pscr_off[s] + (int64_t)ti.start * kPanel;
 
     for (int idx = tid; idx < kPanel * TB; idx += 256) {
         const int q = idx >> 6, r = idx & 63;
@@ -263,7 +277,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int pcols = min(kPanel, f.c - col0);
     if (!diag) {
         if constexpr (sizeof(T) == 4)
-            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad);
+            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad, Bs);
         return;
     }
 
@@ -345,7 +359,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);
     // the split for the Schur update, after the flag: off the panel's chain
     if constexpr (sizeof(T) == 4)
-        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad);
+        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad, Bs);
 }
 
 template <typename T>

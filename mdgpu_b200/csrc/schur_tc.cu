@@ -11,23 +11,27 @@
 // C -= lo hi' + hi lo' + hi hi' (close to FP32 accuracy, which keeps the
 // iterative refinement short).
 //
-// One persistent CTA per SM takes tiles round-robin over the launch's tile
-// list and runs three roles (288 threads, nine warps):
-//   warps 0-3  load + split: lane 0 of warp 0 issues the TMA loads of each
-//              16-column chunk of A_I and A_J (32-row boxes from the front's
-//              L panel, rows and columns past the panel's end read as zeros),
-//              then all four warps split the chunk in shared memory (hi in
-//              place, lo beside it) and release it to the MMA warp;
-//   warp 4     MMA issue (one elected thread): per 8-column step three
-//              tcgen05.mma kind::tf32 (M = N = 128) into the tile's TMEM
-//              accumulator, the stage committed back to the loaders;
-//   warps 5-8  epilogue: tcgen05.ld of their 32 TMEM lanes (tile rows),
-//              C -= acc in place (coalesced along the columns), then the
-//              accumulator is handed back to the MMA warp.
+// Persistent CTAs take tiles round-robin over the launch's tile list, with
+// three roles:
+//   loader     3xTF32: lane 0 of warp 0 issues per 32-column chunk one TMA
+//              load each of A_hi, B_hi, A_lo, B_lo (128 rows x 128 bytes,
+//              128-byte swizzle: K-major) from the split scratch the panel
+//              kernel wrote (hi = A with the low 13 mantissa bits cleared,
+//              lo = A - hi; per front 2 mpad rows of 256 columns, row-major;
+//              rows past it read as zeros); BF16: warps 0-3, the TMA of
+//              64-column FP32 chunks of the L panel, then the rounding to
+//              BF16 into a K-major copy (below);
+//   MMA        one elected thread: per 8-column step three tcgen05.mma
+//              kind::tf32 (M = N = 128), or one kind::f16 per 16 columns,
+//              into the tile's TMEM accumulator; each stage is committed
+//              back to the loader, each finished tile to the epilogue;
+//   epilogue   3xTF32: eight warps, two per 32 TMEM lanes (tile rows), each
+//              pair splitting the columns; BF16: four warps.  tcgen05.ld of
+//              the accumulator, handed back once read, then C -= acc in
+//              place (coalesced along the columns).
 // The TMEM accumulator is double-buffered (2 x 128 columns), so tile t's
-// epilogue runs under tile t + 1's MMAs; the chunk ring has four stages.
-// Only the panel itself crosses L2 (the hi / lo split is made here, once per
-// chunk and CTA, instead of being stored and read twice).
+// epilogue runs under tile t + 1's MMAs.  3xTF32: 320 threads, three 64 KB
+// stages; BF16: 288 threads, two 96 KB stages; one CTA per SM.
 //
 // BF16 mode (the MDGPU_BF16 factor): the loaders round each FP32 chunk to
 // BF16 (nearest even) into a K-major copy with the 128-byte swizzle, and one
@@ -36,11 +40,12 @@
 // exponent, so scaling by 2^k would only shift exponents and leave every
 // rounded bit as it is.
 //
-// For 32-bit MN-major operands the only UMMA shared-memory layout is the
-// 128-byte swizzle with 32-byte atoms (32-byte chunks of each 128-byte row
-// permuted by row mod 4, atoms of 4 K-rows); the TMA writes exactly that
-// pattern with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, and the split is
-// elementwise, so lo lands in the same pattern.
+// Both modes feed the MMA K-major operands with the 128-byte swizzle: rows
+// of 128 bytes (32 TF32 or 64 BF16 values along K), 8-row atoms of 1024
+// bytes, the 16-byte chunk c of row r at c ^ (r mod 8) -- the pattern the
+// TMA writes with CU_TENSOR_MAP_SWIZZLE_128B (3xTF32) and the BF16
+// conversion writes by hand.  A K-step of the MMA (8 TF32 or 16 BF16) is 32
+// bytes along the row: the descriptor's start address advances by 32.
 //
 // Every wait on an mbarrier is bounded: on timeout the CTA records an error
 // code in *err and sets its abort word, every role leaves its loop, the
@@ -64,16 +69,17 @@ namespace mdgpu {
 namespace tc {
 
 constexpr int BM = 128, BN = 128;
-constexpr int BOX = 32;               // TMA box: 32 rows x BK columns of FP32
+constexpr int BOX = 32;  // BF16 mode: TMA boxes of 32 rows x BK columns of FP32
 constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
 
-// Per-mode constants.  3xTF32: 16-column chunks; a stage holds A_hi, B_hi,
-// A_lo, B_lo as the panel kernel split them; three stages, two CTAs per SM.
-// BF16: 64-column chunks; a stage holds A, B as loaded (FP32, no swizzle)
-// and their BF16 copies (K-major, 128-byte swizzle); two stages.
+// Per-mode constants.  3xTF32: 32-column chunks; a stage holds A_hi, B_hi,
+// A_lo, B_lo (16 KB each, K-major) as the panel kernel split them; three
+// stages; eight epilogue warps.  BF16: 64-column chunks; a stage holds A, B
+// as loaded (FP32, no swizzle) and their BF16 copies (K-major, 128-byte
+// swizzle); two stages; four epilogue warps.  One CTA per SM.
 template <bool BF>
 struct Cfg {
-    static constexpr int BK = BF ? 64 : 16;       // K columns per chunk
+    static constexpr int BK = BF ? 64 : 32;       // K columns per chunk
     static constexpr int STAGES = BF ? 2 : 3;
     static constexpr int OPER = BM * BK * 4;      // bytes of one FP32 operand chunk
     // what the TMA brings per chunk: A, B (BF16: FP32, to be converted) or
@@ -82,11 +88,12 @@ struct Cfg {
     static constexpr int STAGE_BYTES = BF ? STAGE_TMA + STAGE_TMA / 2 : STAGE_TMA;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
     // warps: loaders (BF16: four, they convert; 3xTF32: one TMA warp), one
-    // MMA warp, four epilogue warps
+    // MMA warp, the epilogue warps (two per 32 TMEM lanes in 3xTF32)
     static constexpr int NLOAD = BF ? 4 : 1;
     static constexpr int MMA_WARP = NLOAD;
-    static constexpr int NTHREADS = (NLOAD + 5) * 32;
-    static constexpr int CTAS_PER_SM = BF ? 1 : 2;
+    static constexpr int NEPI = BF ? 4 : 8;
+    static constexpr int NTHREADS = (NLOAD + 1 + NEPI) * 32;
+    static constexpr int CTAS_PER_SM = 1;
 };
 constexpr long long WAIT_LIMIT = 1ll << 22;                  // polls (with backoff)
 
@@ -140,24 +147,9 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
-// UMMA shared-memory descriptor: MN-major, 128-byte swizzle with 32-byte
-// atoms (layout type 1).  LBO = distance between 32-element (128 B) blocks
-// along M/N (one TMA box, BK K-rows x 128 B), SBO = distance between groups
-// of 4 K-rows (512 B); version 1 (sm_100).
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-    constexpr uint64_t LBO = BOX * 16 * 4, SBO = 512;
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)((LBO >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((SBO >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    d |= (uint64_t)1 << 61;  // SWIZZLE_128B_BASE32B
-    return d;
-}
-
-// instruction descriptor: D f32, A/B tf32, both MN-major, M = 128, N = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
-                           ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N = 128
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db,
                                          uint32_t accumulate) {
@@ -171,9 +163,9 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
 }
 
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle (layout type 2):
-// rows of 64 BF16 K-values (128 B), 8-row atoms 1024 B apart (SBO); the
-// 16-byte chunks of row r of an atom sit at chunk ^ (r mod 8).  A K-step of
-// 16 inside the 128-byte row advances the start address by 32 B.
+// rows of 128 B along K, 8-row atoms 1024 B apart (SBO); the 16-byte chunks
+// of row r of an atom sit at chunk ^ (r mod 8).  A K-step (8 TF32, 16 BF16)
+// inside the 128-byte row advances the start address by 32 B.
 __device__ __forceinline__ uint64_t make_desc_kmajor(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
@@ -290,7 +282,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
         }
         for (int a = 0; a < 2; ++a) {
             tc::mbar_init(&accf_bar[a], 1);
-            tc::mbar_init(&acce_bar[a], 4);
+            tc::mbar_init(&acce_bar[a], C::NEPI);
         }
         tc::mbar_init(&drain_bar, 1);
         abort_sh = 0;
@@ -326,23 +318,24 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                         ok = false;
                     } else {
                         tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
+                        if constexpr (BF) {
+                            // the L panel: 32-row boxes, panel columns from k0
+                            const int col = t.k0 + ch * BK;
 #pragma unroll
-                        for (int q = 0; q < BM / BOX; ++q) {
-                            const int ra = t.I * BM + q * BOX, rb = t.J * BN + q * BOX;
-                            unsigned char* d = a + q * BOX * BK * 4;
-                            if constexpr (BF) {
-                                // the L panel: panel columns from k0
-                                const int col = t.k0 + ch * BK;
-                                tc::tma_load_2d(d, map, &full_bar[st], ra, col);
-                                tc::tma_load_2d(d + OPER, map, &full_bar[st], rb, col);
-                            } else {
-                                // the split scratch: hi rows, then lo rows from mpad
-                                const int col = ch * BK;
-                                tc::tma_load_2d(d, map, &full_bar[st], ra, col);
-                                tc::tma_load_2d(d + OPER, map, &full_bar[st], rb, col);
-                                tc::tma_load_2d(d + 2 * OPER, map, &full_bar[st], mpad + ra, col);
-                                tc::tma_load_2d(d + 3 * OPER, map, &full_bar[st], mpad + rb, col);
+                            for (int q = 0; q < BM / BOX; ++q) {
+                                unsigned char* d = a + q * BOX * BK * 4;
+                                tc::tma_load_2d(d, map, &full_bar[st], t.I * BM + q * BOX, col);
+                                tc::tma_load_2d(d + OPER, map, &full_bar[st], t.J * BN + q * BOX,
+                                                col);
                             }
+                        } else {
+                            // the split scratch (row-major): K columns ch * BK ..,
+                            // 128 rows per box; hi rows, then lo rows from mpad
+                            const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
+                            tc::tma_load_2d(a, map, &full_bar[st], col, ra);
+                            tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
+                            tc::tma_load_2d(a + 2 * OPER, map, &full_bar[st], col, mpad + ra);
+                            tc::tma_load_2d(a + 3 * OPER, map, &full_bar[st], col, mpad + rb);
                         }
                         issued = g + 1;
                     }
@@ -426,11 +419,14 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                         const uint32_t al = ah + 2 * OPER, bl = bh + 2 * OPER;
 #pragma unroll
                         for (int k = 0; k < BK / 8; ++k) {
-                            const uint32_t o = k * 1024;
-                            tc::mma_tf32(d, tc::make_desc(al + o), tc::make_desc(bh + o),
+                            const uint32_t o = k * 32;
+                            tc::mma_tf32(d, tc::make_desc_kmajor(al + o),
+                                         tc::make_desc_kmajor(bh + o),
                                          (ch > 0 || k > 0) ? 1u : 0u);
-                            tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bl + o), 1u);
-                            tc::mma_tf32(d, tc::make_desc(ah + o), tc::make_desc(bh + o), 1u);
+                            tc::mma_tf32(d, tc::make_desc_kmajor(ah + o),
+                                         tc::make_desc_kmajor(bl + o), 1u);
+                            tc::mma_tf32(d, tc::make_desc_kmajor(ah + o),
+                                         tc::make_desc_kmajor(bh + o), 1u);
                         }
                     } else {
                         const uint32_t ab = tc::smem_u32(smem + st * STAGE_BYTES + STAGE_TMA);
@@ -460,8 +456,11 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31; with
+        // eight epilogue warps each pair of a quarter splits the columns
         const int quarter = warp & 3;
+        constexpr int NCB = BN / 32 / (C::NEPI / 4);  // 32-column blocks per warp
+        const int cb0 = ((warp - MMA_WARP - 1) / 4) * NCB;
         int tl = 0;
         for (int b = blockIdx.x; b < ntiles; b += gridDim.x, ++tl) {
             const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
@@ -471,10 +470,10 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int row = t.I * BM + quarter * 32 + lane;
 #pragma unroll 1
-            for (int cb = 0; cb < BN / 32; ++cb) {
+            for (int cb = cb0; cb < cb0 + NCB; ++cb) {
                 float v[32];
                 tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + acc * BN + cb * 32, v);
-                if (cb == BN / 32 - 1) {
+                if (cb == cb0 + NCB - 1) {
                     // every TMEM read of this accumulator is done: hand it back
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                     __syncwarp();
@@ -533,9 +532,9 @@ static EncodeTiledFn encode_fn() {
 // pivot columns, column-major with leading dimension ldl (a multiple of 8,
 // so the column stride is a multiple of 16 bytes; the panel starts on 128
 // bytes), boxes of 32 rows x 64 columns without swizzle.  3xTF32: over its
-// split panel scratch, 2 mpad rows (hi then lo) x kPanel columns, boxes of
-// 32 rows x 16 columns with the 128-byte / 32-byte-atom swizzle.  Reads
-// past the rows or columns return zeros.
+// split panel scratch, row-major, kPanel columns (the inner dimension) x
+// 2 mpad rows (hi then lo; a row is 1 KB), boxes of 32 columns x 128 rows
+// with the 128-byte swizzle.  Reads past the rows or columns return zeros.
 int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t>& scr_off,
                      std::vector<CUtensorMap>& maps, std::vector<int>& idx, bool bf16) {
     EncodeTiledFn enc = encode_fn();
@@ -547,25 +546,28 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
         const FrontDesc& f = P.fronts[s];
         idx[s] = (int)q;
         cuuint64_t dims[2], strides[1];
-        cuuint32_t box[2] = {tc::BOX,
-                             (cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK)};
+        cuuint32_t box[2];
         cuuint32_t estr[2] = {1, 1};
         void* ptr;
         if (bf16) {
             dims[0] = (cuuint64_t)f.m;
             dims[1] = (cuuint64_t)f.c;
             strides[0] = (cuuint64_t)f.ldl * 4;
+            box[0] = tc::BOX;
+            box[1] = tc::Cfg<true>::BK;
             ptr = const_cast<float*>(base + f.loff);
         } else {
             const int mpad = panel_mpad(f.m);
-            dims[0] = (cuuint64_t)(2 * mpad);
-            dims[1] = (cuuint64_t)kPanel;
-            strides[0] = (cuuint64_t)(2 * mpad) * 4;
+            dims[0] = (cuuint64_t)kPanel;
+            dims[1] = (cuuint64_t)(2 * mpad);
+            strides[0] = (cuuint64_t)kPanel * 4;
+            box[0] = tc::Cfg<false>::BK;  // 32 columns = 128 bytes
+            box[1] = tc::BM;
             ptr = const_cast<float*>(base + scr_off[s]);
         }
         CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, ptr, dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         bf16 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+                         bf16 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return -2;
     }
