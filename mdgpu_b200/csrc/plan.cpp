@@ -540,24 +540,6 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         emit(ks);
     }
     S.fwd1_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
-    // one right-hand side, backward: pivot column tiles in groups (key: the
-    // tiles after the group, which it waits for)
-    S.bwd1_task_beg.assign(P.nlevels + 1, 0);
-    for (int l = 0; l < P.nlevels; ++l) {
-        S.bwd1_task_beg[l] = (int)(S.tasks.size() / 2);
-        std::vector<Key> ks;
-        int ord = 0;
-        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-            const int s = P.large_list[q];
-            const int nt1 = (P.fronts[s].c + T - 1) / T;
-            for (int j = 0; j < nt1; j += SolveScheduleHost::kPivotGroup) {
-                const int cnt = std::min(SolveScheduleHost::kPivotGroup, nt1 - j);
-                ks.push_back({nt1 - j - cnt, ord++, s, j | (cnt << 16)});
-            }
-        }
-        emit(ks);
-    }
-    S.bwd1_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
     S.warp_list.assign(P.small_list.size(), 0);
     S.warp_cnt.assign(3 * (size_t)P.nlevels, 0);
     {

@@ -208,10 +208,6 @@ struct SolveScheduleHost {
     // (s, i | cnt << 16), solved one after another inside one CTA
     static constexpr int kPivotGroup = 4;
     std::vector<int> fwd1_task_beg;                // nlevels + 1, in tasks
-    // backward lists for one right-hand side: task (s, j | cnt << 16), pivot
-    // column tiles j .. j + cnt - 1 (cnt <= kPivotGroup), solved from the
-    // last down inside one CTA
-    std::vector<int> bwd1_task_beg;                // nlevels + 1, in tasks
     std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read
     std::vector<double> small_elems;              // per level: L elements of its small fronts
     int nflags = 0;                               // one per pivot tile of a large front

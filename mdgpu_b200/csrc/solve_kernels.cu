@@ -1205,152 +1205,6 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     }
 }
 
-// Backward, one right-hand side, pivot column tiles [j0, j0 + cnt) of front
-// s (cnt <= kPivotGroup): the group's update-row partial sums first, then
-// acc += L(k, group)' x_k over the pivot tiles k after the group as they
-// publish (k descending, a 64 x 64 block per (k, group tile) through a
-// three-stage ring of shared blocks), then the group's tiles from the last
-// down inside the CTA -- x_j = inv(L_jj)' (y_j - acc_j), stored and
-// published, then L(j, earlier group tiles)' x_j added to their sums -- so
-// the backward pivot chain crosses CTAs once per group instead of once per
-// tile.  Threads: l = column in a tile, g = row quarter; acc[gi] is this
-// thread's quarter of the sum of column l of group tile gi.  The block list
-// is fixed in advance (only the vectors wait), so the ring streams the
-// group's own blocks while its chain runs.
-template <typename TL>
-__device__ void bwd_pivot_group_rt1(int s, int j0, int cnt, const FrontDesc& F,
-                                    double* __restrict__ pb, int* __restrict__ abort_flag,
-                                    int* __restrict__ err, const int* __restrict__ gather_nch,
-                                    const int* __restrict__ gather_off,
-                                    const int* __restrict__ gcount, const double* __restrict__ part,
-                                    const int64_t* __restrict__ dinv_off,
-                                    const TL* __restrict__ Ls, const TL* __restrict__ Dinv,
-                                    double* __restrict__ xp, int64_t tile0) {
-    constexpr int T = kTile, LD = kTile + 1, G = SolveScheduleHost::kPivotGroup, STG = 3;
-    const LevelSmem<TL, double> sm(1);
-    __shared__ int s_ok;
-    const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
-    const int nt1 = tiles_l(F.c, T);
-    const int K1 = nt1 - (j0 + cnt);        // pivot tiles after the group
-    const int NB1 = K1 * cnt;               // blocks of the accumulation phase
-    const int NB = NB1 + cnt + cnt * (cnt - 1) / 2;
-    const TL* Lf = Ls + F.loff;
-    TL* ring = sm.Dk;                       // Dk and the stg blocks after it, contiguous
-    double* Xb = sm.Vst;                    // 2 T: polled x_k (phase 1), then t and x_j
-    double* red = sm.red;
-    auto tsize = [&](int k) { return min(T, F.c - k * T); };
-    // block p of the list into ring slot p mod STG
-    auto issue = [&](int p) {
-        if (p < NB) {
-            TL* dst = ring + (p % STG) * T * LD;
-            if (p < NB1) {
-                const int k = nt1 - 1 - p / cnt, gi = p % cnt;
-                load_block_async(dst, Lf + (int64_t)((j0 + gi) * T) * F.ldl + k * T, F.ldl,
-                                 tsize(k), tsize(j0 + gi));
-            } else {
-                int q = p - NB1, gi = cnt - 1;
-                while (q > gi) q -= gi + 1, --gi;
-                const int j = j0 + gi;
-                if (q == 0)
-                    load_block_async(dst, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tsize(j),
-                                     tsize(j));
-                else
-                    load_block_async(dst, Lf + (int64_t)((j0 + q - 1) * T) * F.ldl + j * T,
-                                     F.ldl, tsize(j), tsize(j0 + q - 1));
-            }
-        }
-        cp_async_commit_group();
-    };
-    for (int p = 0; p < STG - 1; ++p) issue(p);
-    double acc[G];
-#pragma unroll
-    for (int a = 0; a < G; ++a) acc[a] = 0.0;
-    auto acc_add = [&](int gi, double v) {
-#pragma unroll
-        for (int a = 0; a < G; ++a)
-            if (a == gi) acc[a] += v;
-    };
-    // y of group tile g (quarter g holds it)
-    const double yq = (g < cnt && l < tsize(j0 + g)) ? xp[F.first_col + (j0 + g) * T + l] : 0.0;
-    // update-row partial sums (the gathers hold lower tickets): quarter g
-    // adds those of group tile g
-    {
-        const int nch = gather_nch[s];
-        if (nch > 0) {
-            if (tid == 0) {
-                int ok = 1;
-                for (int gi = 0; gi < cnt && ok; ++gi)
-                    ok = wait_flag(gcount + tile0 + j0 + gi, nch, abort_flag, err) ? 1 : 0;
-                s_ok = ok;
-            }
-            __syncthreads();
-            if (!s_ok) {
-                cp_async_wait_groups<0>();
-                return;
-            }
-            if (g < cnt) {
-                const double* pj = part + ((int64_t)gather_off[s] + (int64_t)(j0 + g) * nch) * T;
-                double v = 0.0;
-                for (int h = 0; h < nch; ++h) v += __ldcg(pj + (int64_t)h * T + l);
-                acc_add(g, v);
-            }
-        }
-    }
-    int gi2 = cnt - 1, q2 = 0;  // phase-2 position of the block being used
-    for (int p = 0; p < NB; ++p) {
-        issue(p + STG - 1);
-        cp_async_wait_groups<STG - 1>();
-        __syncthreads();
-        const TL* B = ring + (p % STG) * T * LD;
-        if (p < NB1) {
-            const int kk = p / cnt, gi = p % cnt, k = nt1 - 1 - kk;
-            double* X = Xb + (kk & 1) * T;
-            if (gi == 0 && !poll_published(X, pb + (int64_t)k * T, tsize(k), 1, abort_flag, err)) {
-                break;
-            }
-            double v = 0.0;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) v += (double)B[(16 * g + r) + l * LD] * X[16 * g + r];
-            acc_add(gi, v);
-        } else if (q2 == 0) {
-            // x_j = inv(L_jj)' (y_j - acc_j), j = j0 + gi2; B = inv(L_jj)
-            const int j = j0 + gi2, sz = tsize(j);
-            double* tv = Xb + T;
-            double* xj = Xb;
-#pragma unroll
-            for (int a = 0; a < G; ++a)
-                if (a == gi2) red[g * T + l] = acc[a];
-            __syncthreads();
-            if (g == gi2)
-                tv[l] = l < sz ? yq - (red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l]) : 0.0;
-            __syncthreads();
-            double v = 0.0;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) v += (double)B[(16 * g + r) + l * LD] * tv[16 * g + r];
-            red[g * T + l] = v;
-            __syncthreads();
-            if (g == 0) {
-                const double x = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
-                xj[l] = l < sz ? x : 0.0;
-                if (l < sz) {
-                    xp[F.first_col + j * T + l] = x;
-                    st_relaxed_f64(pb + (int64_t)j * T + l, x);
-                }
-            }
-        } else {
-            // acc of group tile q2 - 1 += L(j rows, its columns)' x_j
-            const double* xj = Xb;
-            double v = 0.0;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) v += (double)B[(16 * g + r) + l * LD] * xj[16 * g + r];
-            acc_add(q2 - 1, v);
-        }
-        if (p >= NB1 && ++q2 > gi2) q2 = 0, --gi2;
-        __syncthreads();
-    }
-    cp_async_wait_groups<0>();
-}
-
 // ---------------------------------------------------------------------------
 // forward update tiles with one right-hand side: L read straight from global
 // memory into registers, coalesced (a thread per row), the next columns'
@@ -1656,20 +1510,8 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
                                     dinv_off, Ls, xp, part, n, nrhs);
         return;
     }
-    const int2 tk = tasks[s_task - ngather];
-    if constexpr (NQ == 1) {
-        if (nrhs == 1 && (tk.y >> 16) > 0) {  // a group of pivot tiles (the one-rhs list)
-            constexpr int T = kTile;
-            const int s = tk.x;
-            const int64_t tile0 = dinv_off[s] / (T * T);
-            bwd_pivot_group_rt1<TL>(s, tk.y & 0xffff, tk.y >> 16, fronts[s], pub + tile0 * T,
-                                    abort_flag, err, gather_nch, gather_off, gcount, part,
-                                    dinv_off, Ls, Dinv, xp, tile0);
-            return;
-        }
-    }
-    bwd_chain_task<TL, TV, NQ>(tk, fronts, pub, abort_flag, err, gather_nch, gather_off, gcount,
-                               part, dinv_off, Ls, Dinv, xp, n, nrhs);
+    bwd_chain_task<TL, TV, NQ>(tasks[s_task - ngather], fronts, pub, abort_flag, err, gather_nch,
+                               gather_off, gcount, part, dinv_off, Ls, Dinv, xp, n, nrhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1782,10 +1624,9 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     if (nsm > 0)
         sm = std::max(sm, forward ? small_fwd_smem<TL, TV>(msmall, nrhs)
                                   : small_bwd_smem<TL, TV>(msmall, msmall, nrhs));
-    // one right-hand side: the lists with grouped pivot tiles
-    const bool grouped = NQ == 1 && nrhs == 1;
-    const std::vector<int>& beg = forward ? (grouped ? S.fwd1_task_beg : S.fwd_task_beg)
-                                          : (grouped ? S.bwd1_task_beg : S.bwd_task_beg);
+    // one right-hand side: the forward lists with grouped pivot tiles
+    const std::vector<int>& beg =
+        forward ? ((NQ == 1 && nrhs == 1) ? S.fwd1_task_beg : S.fwd_task_beg) : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
     // tile tasks: registers straight from L with one right-hand side
     const size_t tile_sm = std::max(level_smem_bytes<TL, TV>(nrhs),
