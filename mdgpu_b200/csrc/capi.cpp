@@ -458,7 +458,6 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
         if (tasks.empty()) tasks.assign(2, 0);
         D.solve.tasks = reinterpret_cast<int2*>(h->keep(upload(tasks)));
         D.solve.fwd_task_beg = SS.fwd_task_beg;
-        D.solve.fwd1_task_beg = SS.fwd1_task_beg;
         D.solve.bwd_task_beg = SS.bwd_task_beg;
         D.solve.fwd_elems = SS.fwd_elems;
         D.solve.bwd_elems = SS.bwd_elems;

@@ -98,7 +98,6 @@ struct DevSchedule {
 struct SolveSchedule {
     int2* tasks = nullptr;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1
-    std::vector<int> fwd1_task_beg;               // one right-hand side: grouped pivot tiles
     std::vector<double> fwd_elems, bwd_elems;     // per level: L + Dinv elements
     std::vector<double> small_elems;              // per level: L elements of small fronts
     int* sync = nullptr;

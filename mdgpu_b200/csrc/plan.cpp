@@ -519,27 +519,6 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
         }
         (dir == 0 ? S.fwd_task_beg : S.bwd_task_beg)[P.nlevels] = (int)(S.tasks.size() / 2);
     }
-    // one right-hand side, forward: pivot tiles in groups (key: first tile)
-    S.fwd1_task_beg.assign(P.nlevels + 1, 0);
-    for (int l = 0; l < P.nlevels; ++l) {
-        S.fwd1_task_beg[l] = (int)(S.tasks.size() / 2);
-        std::vector<Key> ks;
-        int ord = 0;
-        for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
-            const int s = P.large_list[q];
-            const FrontDesc& f = P.fronts[s];
-            const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
-            for (int i = 0; i < nt1; i += SolveScheduleHost::kPivotGroup)
-                ks.push_back({i, ord++, s,
-                              i | (std::min(SolveScheduleHost::kPivotGroup, nt1 - i) << 16)});
-            const int G = std::max(1, std::min(SolveScheduleHost::kFwdGroupBlocks / nt1,
-                                               SolveScheduleHost::kFwdGroupTiles));
-            for (int i = nt1; i < NT; i += G)
-                ks.push_back({nt1, ord++, s, i | (std::min(G, NT - i) << 16)});
-        }
-        emit(ks);
-    }
-    S.fwd1_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
     S.warp_list.assign(P.small_list.size(), 0);
     S.warp_cnt.assign(3 * (size_t)P.nlevels, 0);
     {

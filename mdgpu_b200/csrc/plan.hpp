@@ -203,11 +203,6 @@ struct SolveScheduleHost {
     static constexpr int kFwdGroupTiles = 4;  // at most 256 rows: a thread per row
     std::vector<int> tasks;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1 each, in tasks
-    // forward lists for one right-hand side: the same, except that the pivot
-    // tiles come in groups of up to kPivotGroup consecutive tiles per task
-    // (s, i | cnt << 16), solved one after another inside one CTA
-    static constexpr int kPivotGroup = 4;
-    std::vector<int> fwd1_task_beg;                // nlevels + 1, in tasks
     std::vector<double> fwd_elems, bwd_elems;     // per level, L + Dinv elements read
     std::vector<double> small_elems;              // per level: L elements of its small fronts
     int nflags = 0;                               // one per pivot tile of a large front

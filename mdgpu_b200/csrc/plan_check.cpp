@@ -224,11 +224,8 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
         // solve tasks: each tile of each large front once per direction, in
         // dependency order (forward pivot tiles ascending before the front's
         // update tiles; backward pivot tiles descending)
-        for (int dir = 0; dir < 3; ++dir) {
-            // dir 2: the one-right-hand-side forward lists (pivot groups)
-            const std::vector<int>& beg =
-                dir == 0 ? Q.fwd_task_beg : (dir == 1 ? Q.bwd_task_beg : Q.fwd1_task_beg);
-            if ((int)beg.size() != P.nlevels + 1) bad("solve task lists");
+        for (int dir = 0; dir < 2; ++dir) {
+            const std::vector<int>& beg = dir == 0 ? Q.fwd_task_beg : Q.bwd_task_beg;
             for (int l = 0; l < P.nlevels; ++l) {
                 std::vector<int> done_piv(ns, 0), upd(ns, 0);
                 for (int q = beg[l]; q < beg[l + 1]; ++q) {
@@ -236,14 +233,12 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                     if (s < 0 || s >= ns || level[s] != l || !is_large[s]) bad("solve task front");
                     const FrontDesc& f = P.fronts[s];
                     const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
-                    if (dir != 1) {
+                    if (dir == 0) {
                         const int i = t & 0xffff, cnt = t >> 16;
                         if (cnt < 1 || i + cnt > NT) bad("forward task tiles", s);
                         if (i < nt1) {
-                            const int gmax = dir == 0 ? 1 : SolveScheduleHost::kPivotGroup;
-                            if (cnt > gmax || i + cnt > nt1 || i != done_piv[s] || upd[s])
-                                bad("forward pivot order", s);
-                            done_piv[s] += cnt;
+                            if (cnt != 1 || i != done_piv[s] || upd[s]) bad("forward pivot order", s);
+                            done_piv[s]++;
                         } else {
                             if (done_piv[s] != nt1 || i != nt1 + upd[s]) bad("forward update order", s);
                             upd[s] += cnt;
@@ -257,7 +252,7 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                     const int s = P.large_list[q];
                     const FrontDesc& f = P.fronts[s];
                     const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
-                    if (done_piv[s] != nt1 || (dir != 1 && upd[s] != NT - nt1))
+                    if (done_piv[s] != nt1 || (dir == 0 && upd[s] != NT - nt1))
                         bad("solve tasks do not cover the front", s);
                 }
             }

@@ -1283,96 +1283,6 @@ __device__ void fwd_update_rt1(int s, int R0, int R1, const FrontDesc& F, double
     if (rv) f[R] = f0 - acc;
 }
 
-// Forward, one right-hand side, pivot tiles [i0, i0 + cnt) of front s (cnt <=
-// kPivotGroup), a thread per row of the group: first every row's sum over the
-// pivot columns before the group (the published tiles, polled as they come,
-// L read straight from global memory as in fwd_update_rt1), then the group's
-// tiles one after another inside the CTA -- y_i = inv(L_ii) (f_i - acc_i),
-// stored and published, then subtracted from the group's later rows -- so
-// the pivot chain crosses CTAs once per group instead of once per tile.
-template <typename TL>
-__device__ void fwd_pivot_group_rt1(int s, int i0, int cnt, const FrontDesc& F,
-                                    double* __restrict__ pb, int* __restrict__ abort_flag,
-                                    int* __restrict__ err, const int* __restrict__ amap_off,
-                                    const int* __restrict__ amap_row,
-                                    const int* __restrict__ amap_ent,
-                                    const int64_t* __restrict__ dinv_off,
-                                    const TL* __restrict__ Ls, const TL* __restrict__ Dinv,
-                                    double* __restrict__ xp, const double* __restrict__ fv) {
-    constexpr int T = kTile;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* Fs = reinterpret_cast<double*>(smem_raw);  // 4 T: the group's right-hand side
-    double* red = Fs + 4 * T;                           // 4 T: quarter partial sums
-    double* Ys = red + 4 * T;                           // 2 T: polled slots, then y_i
-    const int t = threadIdx.x;
-    const int R0 = i0 * T, R1 = min((i0 + cnt) * T, F.c);
-    const int R = R0 + t;
-    const bool rv = R < R1;
-    const TL* Lr = Ls + F.loff + R;
-    double f0 = 0.0;
-    if (rv) {
-        f0 = xp[F.first_col + R];
-        const int* ar = amap_row + amap_off[s] + R;
-        const int e0 = ar[0], e1 = ar[1];
-        for (int e = e0; e < e1; ++e) f0 += fv[amap_ent[e]];
-    }
-    // the pivot columns before the group
-    constexpr int GW = 8;  // columns per group (registers: the kernel runs 4 CTAs per SM)
-    constexpr int GPB = T / GW;                     // groups per 64-column block
-    const int ng = R0 / GW;
-    double acc = 0.0;
-    if (ng > 0) {
-        auto load = [&](int cg, TL (&v)[GW]) {
-#pragma unroll
-            for (int l = 0; l < GW; ++l)
-                v[l] = rv ? ldL(Lr + (int64_t)(GW * cg + l) * F.ldl) : TL(0);
-        };
-        TL lv[GW], ln[GW];
-        load(0, lv);
-        for (int cg = 0; cg < ng; ++cg) {
-            if (cg + 1 < ng) load(cg + 1, ln);
-            const int k = cg / GPB;
-            double* Yk = Ys + (k & 1) * T;
-            if (cg % GPB == 0 && !poll_published(Yk, pb + (int64_t)k * T, T, 1, abort_flag, err))
-                return;
-            const double* y = Yk + GW * (cg % GPB);
-#pragma unroll
-            for (int l = 0; l < GW; ++l) acc += (double)lv[l] * y[l];
-#pragma unroll
-            for (int l = 0; l < GW; ++l) lv[l] = ln[l];
-        }
-    }
-    Fs[t] = rv ? f0 - acc : 0.0;
-    // the group's tiles, in order
-    const int r = t & (T - 1), g = t >> 6;
-    for (int gi = 0; gi < cnt; ++gi) {
-        const int i = i0 + gi;
-        const int sz = min(T, F.c - i * T);
-        const TL* Dk = Dinv + dinv_off[s] + (int64_t)i * T * T;  // inv(L_ii), zero-padded
-        __syncthreads();  // Fs final for tile i; Ys free
-        double v = 0.0;
-#pragma unroll
-        for (int q = 16 * g; q < 16 * g + 16; ++q) v += (double)Dk[r + q * T] * Fs[gi * T + q];
-        red[g * T + r] = v;
-        __syncthreads();
-        if (t < T) {
-            const double y = red[t] + red[T + t] + red[2 * T + t] + red[3 * T + t];
-            Ys[t] = y;
-            if (t < sz) {
-                xp[F.first_col + i * T + t] = y;
-                st_relaxed_f64(pb + (int64_t)i * T + t, y);
-            }
-        }
-        __syncthreads();
-        if (rv && t >= (gi + 1) * T) {  // rows of the group's later tiles
-            const TL* Lc = Lr + (int64_t)(i * T) * F.ldl;
-            double a = 0.0;
-            for (int q = 0; q < sz; ++q) a += (double)ldL(Lc + (int64_t)q * F.ldl) * Ys[q];
-            Fs[t] -= a;
-        }
-    }
-}
-
 // One launch per level and direction.  Blocks [0, ntile) take tickets for
 // the dependency-ordered tile tasks of the large fronts; the blocks after
 // them run the small fronts: warp tasks (at most kWarpSolveRhs right-hand
@@ -1441,12 +1351,6 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
         const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
         const FrontDesc F = fronts[s];
         const int nt1 = tiles_l(F.c, T);
-        if (nrhs == 1 && i0 < nt1) {  // a group of pivot tiles (the one-rhs list)
-            fwd_pivot_group_rt1<TL>(s, i0, cnt, F, pub + (dinv_off[s] / (T * T)) * T, abort_flag,
-                                    err, amap_off, amap_row, amap_ent, dinv_off, Ls, Dinv, xp,
-                                    fv);
-            return;
-        }
         if (nrhs == 1 && i0 >= nt1 && nt1 <= kRt1MaxPivotTiles) {
             double* pb = pub + (dinv_off[s] / (T * T)) * T;
             {
@@ -1624,9 +1528,7 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     if (nsm > 0)
         sm = std::max(sm, forward ? small_fwd_smem<TL, TV>(msmall, nrhs)
                                   : small_bwd_smem<TL, TV>(msmall, msmall, nrhs));
-    // one right-hand side: the forward lists with grouped pivot tiles
-    const std::vector<int>& beg =
-        forward ? ((NQ == 1 && nrhs == 1) ? S.fwd1_task_beg : S.fwd_task_beg) : S.bwd_task_beg;
+    const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
     const int t0 = beg[l], nt = beg[l + 1] - beg[l];
     // tile tasks: registers straight from L with one right-hand side
     const size_t tile_sm = std::max(level_smem_bytes<TL, TV>(nrhs),
