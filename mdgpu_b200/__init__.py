@@ -139,7 +139,10 @@ def _dev_stream(stream):
         return stream
     import torch
 
-    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    s = torch.cuda.current_stream().cuda_stream
+    # torch's default stream is the legacy NULL stream (handle 0), which the
+    # library would read as "no stream given": name it cudaStreamLegacy (1)
+    return C.c_void_p(s if s else 1)
 
 
 def load_triplet(path, matrix_market=False):
