@@ -703,9 +703,9 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 }
 
 // ---------------------------------------------------------------------------
-// small fronts with at most kWarpSolveRhs right-hand sides: a warp per front,
-// lane l holding rows l, l + 32, ... (R slots, m <= 32 R) of NQ right-hand
-// sides in registers.  Forward: the pivot value is broadcast by a shuffle and
+// small fronts: a warp per front, the right-hand sides in passes of NQ
+// (kWarpSolveRhs, or one), lane l holding rows l, l + 32, ... (R slots,
+// m <= 32 R) of the pass's right-hand sides in registers.  Forward: the pivot value is broadcast by a shuffle and
 // every lane updates its rows below it; backward: a warp reduction per pivot
 // column (dot product with the final rows below it).  No block barriers; the
 // children's update parts are summed into a per-warp shared buffer (child by
@@ -714,6 +714,9 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 
 constexpr int kWarpSolveRhs = 4;   // right-hand sides per pass of the warp path
 constexpr int kSolvePassRhs = 32;  // right-hand sides per pass of the level kernels
+// small fronts run as warp tasks up to this many right-hand sides (a level
+// pass), as a CTA per front above
+constexpr int kWarpPathMaxRhs = 32;
 
 // Fronts of at most W rows (W = 8, 16, 32) on a group of W lanes of a warp
 // (32 / W fronts per warp), one row per lane.  mask: the group's lanes; the
@@ -1298,7 +1301,7 @@ __device__ void small_fronts_fwd(int b, WarpTasks wt, int wblocks, const int* sm
                                  const TL* __restrict__ Ls, TV* __restrict__ xp,
                                  TV* __restrict__ fv, int n, int nrhs, int msmall) {
     if (b < wblocks) {
-        if constexpr (NQ == 1) {  // nrhs <= kWarpSolveRhs
+        {  // right-hand sides in passes of kWarpSolveRhs inside the warp task
             extern __shared__ __align__(16) unsigned char smem_raw[];
             const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
             TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
@@ -1381,7 +1384,7 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
     if ((int)blockIdx.x >= ntk) {
         const int b = blockIdx.x - ntk;
         if (b < wblocks) {
-            if constexpr (NQ == 1) {  // nrhs <= kWarpSolveRhs
+            {  // right-hand sides in passes of kWarpSolveRhs inside the warp task
                 extern __shared__ __align__(16) unsigned char smem_raw[];
                 const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
                 TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
@@ -1510,10 +1513,10 @@ static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, con
     const int ns = se - sb;
     const int nl = D.h_large_ptr[l + 1] - D.h_large_ptr[l];
     const int msmall = level_msmall(D, l);
-    // with at most kWarpSolveRhs right-hand sides (NQ == 1) every small front
-    // is a warp task, else a CTA
+    // small fronts as warp tasks (right-hand sides in passes of
+    // kWarpSolveRhs inside the task) up to kWarpPathMaxRhs, else a CTA each
     static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 160 rows in shared memory");
-    const bool warp = NQ == 1 && nrhs <= kWarpSolveRhs;
+    const bool warp = nrhs <= kWarpPathMaxRhs;
     WarpTasks wt{S.warp_list + sb, 0, 0, 0};
     if (warp) {
         wt.n1 = S.warp_cnt[3 * l];
