@@ -573,12 +573,12 @@ void ensure_factor_storage(mdgpu_handle_s* h, int precision) {
         }
         if (!h->dU32) h->dU32 = dalloc<float>(P.ustore);
         if (!h->dD32) h->dD32 = dalloc<float>(P.dinv_total);
-        // the same panels for the BF16 Schur update (64-column boxes)
-        if (precision == MDGPU_BF16 && !h->D.tmaps_bf16 && h->use_tensor_cores &&
-            !P.large_list.empty()) {
+        // the same scratch read as the BF16 copy of the panels (BF16 Schur
+        // updates)
+        if (precision == MDGPU_BF16 && !h->D.tmaps_bf16 && h->D.pscr) {
             std::vector<CUtensorMap> maps;
             std::vector<int> idx;
-            if (build_panel_maps(P, h->dL32, h->pscr_off, maps, idx, true) == 0)
+            if (build_panel_maps(P, h->D.pscr, h->pscr_off, maps, idx, true) == 0)
                 h->D.tmaps_bf16 = h->keep(upload(maps));
         }
     }

@@ -686,7 +686,10 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
             }
             case OP_PANEL: {
                 ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
-                launch_panel<T>(D, op, Ls, Dinv, status, !bf16, st);
+                // the panel scratch the tensor-core Schur update reads:
+                // the 3xTF32 hi/lo split (1) or the BF16 copy (2)
+                launch_panel<T>(D, op, Ls, Dinv, status, sizeof(T) == 4 ? (bf16 ? 2 : 1) : 0,
+                                st);
                 break;
             }
             case OP_SCHUR_TC: {

@@ -186,7 +186,7 @@ struct DevPlan {
     // FP32 path: per large front a TMA descriptor of its L panel (the
     // operands of the tensor-core Schur updates)
     CUtensorMap* tmaps = nullptr;
-    CUtensorMap* tmaps_bf16 = nullptr;  // over the L panels, for the BF16 Schur update
+    CUtensorMap* tmaps_bf16 = nullptr;  // over the same scratch as BF16, for the BF16 Schur update
     // FP32 (3xTF32) path: the current panel of every large front of a level,
     // split: per front 2 mpad x kPanel floats (column kk: rows [0, mpad) the
     // TF32 part hi, rows [mpad, 2 mpad) lo = x - hi), mpad = m rounded up to
@@ -257,7 +257,7 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
 // one panel launch (OP_PANEL): every row-tile task of the panel's fronts
 // split: also write the panel split for 3xTF32 into the panel scratch
 template <typename T>
-void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, bool split,
+void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, int split_mode,
                   cudaStream_t st);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
                      float* Us, int* err, bool bf16, cudaStream_t st);

@@ -30,20 +30,21 @@
 // diagonal factorization as separate launches (about nine per panel): the
 // critical path of a panel is the chain of its diagonal tiles, each one
 // TRSM product, one SYRK product and one 64 x 64 factorization behind the
-// previous (the in-panel updates run ahead on the step words).  With a
-// panel scratch (FP32 factors
-// with 3xTF32 Schur updates) every task finally writes its rows of the
-// finished panel there split (hi = X with the low 13 mantissa bits cleared,
-// lo = X - hi), columns past the last pivot column as zeros, for the panel's
-// Schur update (row-major: the K-major operands of the tensor-core update)
-// -- a diagonal task after publishing its flag, so the split stays off the
-// chain; BF16 Schur updates read the panel from the L store.
+// previous (the in-panel updates run ahead on the step words).  FP32
+// factors with tensor-core Schur updates: every task finally writes its rows
+// of the finished panel into a panel scratch, row-major (the K-major
+// operands of the update), columns past the last pivot column as zeros --
+// split for 3xTF32 (hi = X with the low 13 mantissa bits cleared, lo =
+// X - hi) or rounded to BF16 -- a diagonal task after publishing its flag,
+// so the copy stays off the chain.
 //
 // FP32 factors: each diagonal tile's pivots are compared with the tile's
 // diagonal before its factorization; if one lost more than ten bits to
 // cancellation (or is not positive) the tile is factored again in FP64 from
 // the same values (the FP64 safeguard for weak pivots; the count is
 // reported in status[3]).
+#include <cuda_bf16.h>
+
 #include <climits>
 #include <cstdio>
 
@@ -118,14 +119,18 @@ __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl,
 
 // The task's rows of the finished panel (read back from the L store, which
 // this CTA wrote: zeros above the diagonal and past the last pivot column)
-// split into the panel scratch for 3xTF32 -- hi = x with the low 13
-// mantissa bits cleared, lo = x - hi -- row-major (a row's kPanel columns
-// contiguous: the K-major operand layout of the Schur update), hi rows from
-// the front's base, lo rows mpad further; all kPanel columns (zeros past
-// the last pivot column).  32-column blocks go through buf (64 x 33 floats)
-// so the global reads run down columns and the writes along rows.
+// into the panel scratch for the tensor-core Schur update, row-major (a
+// row's kPanel columns contiguous: the K-major operand layout), all kPanel
+// columns (zeros past the last pivot column):
+//   mode 1 (3xTF32): hi = x with the low 13 mantissa bits cleared, lo =
+//          x - hi; hi rows from the front's base, lo rows mpad further;
+//   mode 2 (BF16): x rounded to BF16 (nearest even), one copy.
+// 32-column blocks go through buf (64 x 33 floats) so the global reads run
+// down columns and the writes along rows.  ps: the front's scratch base;
+// row0: the task's first row.
 __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, int nrows,
-                                              int ncols, float* ps, int mpad, float* buf) {
+                                              int ncols, float* ps, int row0, int mpad,
+                                              int mode, float* buf) {
     for (int cb = 0; cb < kPanel; cb += 32) {
         __syncthreads();  // buf free
         for (int idx = threadIdx.x; idx < kTile * 32; idx += 256) {
@@ -138,10 +143,14 @@ __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, in
             const int r = idx >> 5, q = idx & 31;
             if (r >= nrows) continue;
             const float x = buf[r * 33 + q];
-            const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
-            float* p = ps + (int64_t)r * kPanel + cb + q;
-            p[0] = h;
-            p[(int64_t)mpad * kPanel] = x - h;
+            const int64_t e = (int64_t)(row0 + r) * kPanel + cb + q;
+            if (mode == 2) {
+                reinterpret_cast<__nv_bfloat16*>(ps)[e] = __float2bfloat16_rn(x);
+            } else {
+                const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+                ps[e] = h;
+                ps[e + (int64_t)mpad * kPanel] = x - h;
+            }
         }
     }
 }
@@ -161,7 +170,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             int panel, int* __restrict__ counter, int* __restrict__ flags,
             int* __restrict__ steps, int* __restrict__ abort_flag, int* __restrict__ err,
             const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
-            float* __restrict__ pscr, const int64_t* __restrict__ pscr_off,
+            float* __restrict__ pscr, const int64_t* __restrict__ pscr_off, int split_mode,
             int* __restrict__ status) {
     constexpr int TB = kTile, PT = kPanel / kTile, LDS = TB + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -187,10 +196,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int ncol = (diag ? min((i + 1) * TB, f.c) : min(khi * TB, f.c)) - col0;
     const int64_t tile0 = dinv_off[s] / (TB * TB);  // flag of pivot tile k: flags[tile0 + k]
     T* rowp = Ls + f.loff + ti.start + (int64_t)col0 * f.ldl;
-    float* ps = nullptr;  // this task's rows of the split panel scratch (row-major)
+    float* ps = nullptr;  // the front's panel scratch (row-major), if any
     const int mpad = panel_mpad(f.m);
     if constexpr (sizeof(T) == 4)
-        if (pscr) ps = pscr + pscr_off[s] + (int64_t)ti.start * kPanel;
+        if (pscr && split_mode) ps = pscr + pscr_off[s];
 
     for (int idx = tid; idx < kPanel * TB; idx += 256) {
         const int q = idx >> 6, r = idx & 63;
@@ -277,7 +286,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int pcols = min(kPanel, f.c - col0);
     if (!diag) {
         if constexpr (sizeof(T) == 4)
-            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad, Bs);
+            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, mpad, split_mode, Bs);
         return;
     }
 
@@ -359,24 +368,25 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);
     // the split for the Schur update, after the flag: off the panel's chain
     if constexpr (sizeof(T) == 4)
-        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, mpad, Bs);
+        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, mpad, split_mode, Bs);
 }
 
 template <typename T>
-void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, bool split,
-                  cudaStream_t st) {
+void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status,
+                  int split_mode, cudaStream_t st) {
     int* counter = D.fsync + op.counter;
     int* flags = D.fsync + D.fsync_flags;
     int* abort_flag = D.fsync + D.fsync_flags + D.nflags_factor;
     int* steps = abort_flag + 1;
     k_panel<T><<<op.ntasks, 256, panel_smem_bytes<T>(), st>>>(
         D.fronts, D.psched.tasks + op.toff, op.ntasks, op.arg, counter, flags, steps, abort_flag,
-        status + 1, D.dinv_off, Ls, Dinv, split ? D.pscr : nullptr, D.pscr_off, status);
+        status + 1, D.dinv_off, Ls, Dinv, split_mode ? D.pscr : nullptr, D.pscr_off, split_mode,
+        status);
 }
 
-template void launch_panel<float>(const DevPlan&, const PanelOp&, float*, float*, int*, bool,
+template void launch_panel<float>(const DevPlan&, const PanelOp&, float*, float*, int*, int,
                                   cudaStream_t);
-template void launch_panel<double>(const DevPlan&, const PanelOp&, double*, double*, int*, bool,
+template void launch_panel<double>(const DevPlan&, const PanelOp&, double*, double*, int*, int,
                                    cudaStream_t);
 
 void init_panel_kernels() {

@@ -69,29 +69,25 @@ namespace mdgpu {
 namespace tc {
 
 constexpr int BM = 128, BN = 128;
-constexpr int BOX = 32;  // BF16 mode: TMA boxes of 32 rows x BK columns of FP32
 constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
 
-// Per-mode constants.  3xTF32: 32-column chunks; a stage holds A_hi, B_hi,
-// A_lo, B_lo (16 KB each, K-major) as the panel kernel split them; three
-// stages; eight epilogue warps.  BF16: 64-column chunks; a stage holds A, B
-// as loaded (FP32, no swizzle) and their BF16 copies (K-major, 128-byte
-// swizzle); two stages; four epilogue warps.  One CTA per SM.
+// Per-mode constants: a chunk is 128 bytes of K per operand row (32 TF32 or
+// 64 BF16 columns); a stage holds A_hi, B_hi, A_lo, B_lo (3xTF32) or A, B
+// (BF16), 16 KB each, as the panel kernel wrote them.  One TMA warp, one MMA
+// warp, eight epilogue warps (two per 32 TMEM lanes); one CTA per SM.
 template <bool BF>
 struct Cfg {
     static constexpr int BK = BF ? 64 : 32;       // K columns per chunk
-    static constexpr int STAGES = BF ? 2 : 3;
-    static constexpr int OPER = BM * BK * 4;      // bytes of one FP32 operand chunk
-    // what the TMA brings per chunk: A, B (BF16: FP32, to be converted) or
-    // A_hi, B_hi, A_lo, B_lo (3xTF32: split by the panel kernel)
-    static constexpr int STAGE_TMA = BF ? 2 * OPER : 4 * OPER;
-    static constexpr int STAGE_BYTES = BF ? STAGE_TMA + STAGE_TMA / 2 : STAGE_TMA;
+    static constexpr int ESZ = BF ? 2 : 4;        // operand element bytes
+    static constexpr int OPER = BM * BK * ESZ;    // bytes of one operand chunk (16 KB)
+    static constexpr int NOPER = BF ? 2 : 4;
+    static constexpr int STAGE_TMA = NOPER * OPER;
+    static constexpr int STAGE_BYTES = STAGE_TMA;
+    static constexpr int STAGES = BF ? 6 : 3;     // 192 KB of stages either way
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
-    // warps: loaders (BF16: four, they convert; 3xTF32: one TMA warp), one
-    // MMA warp, the epilogue warps (two per 32 TMEM lanes in 3xTF32)
-    static constexpr int NLOAD = BF ? 4 : 1;
+    static constexpr int NLOAD = 1;
     static constexpr int MMA_WARP = NLOAD;
-    static constexpr int NEPI = BF ? 4 : 8;
+    static constexpr int NEPI = 8;
     static constexpr int NTHREADS = (NLOAD + 1 + NEPI) * 32;
     static constexpr int CTAS_PER_SM = 1;
 };
@@ -262,7 +258,6 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                   MMA_WARP = C::MMA_WARP;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];   // TMA bytes landed
-    __shared__ __align__(8) uint64_t split_bar[STAGES];  // operands prepared (4 warps)
     __shared__ __align__(8) uint64_t empty_bar[STAGES];  // MMAs done reading the stage
     __shared__ __align__(8) uint64_t accf_bar[2];        // accumulator complete
     __shared__ __align__(8) uint64_t acce_bar[2];        // accumulator read out (4 warps)
@@ -277,7 +272,6 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
     if (tid == 0) {
         for (int q = 0; q < STAGES; ++q) {
             tc::mbar_init(&full_bar[q], 1);
-            tc::mbar_init(&split_bar[q], NLOAD_WARPS);
             tc::mbar_init(&empty_bar[q], 1);
         }
         for (int a = 0; a < 2; ++a) {
@@ -300,8 +294,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
     const uint32_t tmem = tmem_base_sh;
 
     if (warp < NLOAD_WARPS) {
-        // ---- loaders: TMA (warp 0 lane 0); BF16: then the conversion by all
-        // four loader warps
+        // ---- loader: TMA (warp 0, lane 0)
         long long g = 0;  // chunk counter over this CTA's tiles
         long long issued = 0;
         bool ok = true;
@@ -317,23 +310,14 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                     if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1, &abort_sh)) {
                         ok = false;
                     } else {
+                        // the panel scratch (row-major): K columns ch * BK ..,
+                        // 128 rows per box; 3xTF32: hi rows, then lo rows
+                        // from mpad
                         tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
-                        if constexpr (BF) {
-                            // the L panel: 32-row boxes, panel columns from k0
-                            const int col = t.k0 + ch * BK;
-#pragma unroll
-                            for (int q = 0; q < BM / BOX; ++q) {
-                                unsigned char* d = a + q * BOX * BK * 4;
-                                tc::tma_load_2d(d, map, &full_bar[st], t.I * BM + q * BOX, col);
-                                tc::tma_load_2d(d + OPER, map, &full_bar[st], t.J * BN + q * BOX,
-                                                col);
-                            }
-                        } else {
-                            // the split scratch (row-major): K columns ch * BK ..,
-                            // 128 rows per box; hi rows, then lo rows from mpad
-                            const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
-                            tc::tma_load_2d(a, map, &full_bar[st], col, ra);
-                            tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
+                        const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
+                        tc::tma_load_2d(a, map, &full_bar[st], col, ra);
+                        tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
+                        if constexpr (!BF) {
                             tc::tma_load_2d(a + 2 * OPER, map, &full_bar[st], col, mpad + ra);
                             tc::tma_load_2d(a + 3 * OPER, map, &full_bar[st], col, mpad + rb);
                         }
@@ -342,43 +326,6 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                 }
                 ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
                 if (!ok) break;
-                if constexpr (BF) {
-                    // all four warps: wait for the bytes, convert, release
-                    if (!tc::mbar_wait(&full_bar[st], use & 1, &abort_sh)) {
-                        ok = false;
-                        break;
-                    }
-                    // BF16 (round to nearest even), K-major with the 128-byte
-                    // swizzle: thread (m, kc) converts K columns 8 kc .. 8 kc + 7
-                    // of row m into one 16-byte chunk
-#pragma unroll
-                    for (int o = 0; o < 2; ++o) {
-                        const float* src = reinterpret_cast<const float*>(a + o * OPER);
-                        unsigned char* dst = a + STAGE_TMA + o * (OPER / 2);
-#pragma unroll 2
-                        for (int u = 0; u < 8; ++u) {
-                            const int m = tid, kc = u;
-                            // FP32 staging: box m / 32, K column k at k * 32 + m % 32
-                            const float* sp =
-                                src + (m >> 5) * (BOX * BK) + (kc * 8) * BOX + (m & 31);
-                            uint32_t w[4];
-#pragma unroll
-                            for (int h = 0; h < 4; ++h) {
-                                const __nv_bfloat162 p = __floats2bfloat162_rn(
-                                    sp[(2 * h) * BOX], sp[(2 * h + 1) * BOX]);
-                                w[h] = *reinterpret_cast<const uint32_t*>(&p);
-                            }
-                            const int r = m & 7;
-                            *reinterpret_cast<uint4*>(dst + (m >> 3) * 1024 + r * 128 +
-                                                      ((kc ^ r) << 4)) =
-                                make_uint4(w[0], w[1], w[2], w[3]);
-                        }
-                    }
-                    // generic-proxy writes, read next by the tensor core (async proxy)
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) tc::mbar_arrive(&split_bar[st]);
-                }
             }
         }
         if (!ok && tid == 0) {
@@ -407,8 +354,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                 const uint32_t d = tmem + (uint32_t)(acc * BN);
                 for (int ch = 0; ch < t.nk; ++ch, ++g) {
                     const int st = (int)(g % STAGES);
-                    if (!tc::mbar_wait(BF ? &split_bar[st] : &full_bar[st],
-                                       (uint32_t)(g / STAGES) & 1, &abort_sh)) {
+                    if (!tc::mbar_wait(&full_bar[st], (uint32_t)(g / STAGES) & 1, &abort_sh)) {
                         ok = false;
                         break;
                     }
@@ -429,8 +375,8 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                                          tc::make_desc_kmajor(bh + o), 1u);
                         }
                     } else {
-                        const uint32_t ab = tc::smem_u32(smem + st * STAGE_BYTES + STAGE_TMA);
-                        const uint32_t bb = ab + OPER / 2;
+                        const uint32_t ab = tc::smem_u32(smem + st * STAGE_BYTES);
+                        const uint32_t bb = ab + OPER;
 #pragma unroll
                         for (int k = 0; k < BK / 16; ++k)
                             tc::mma_bf16(d, tc::make_desc_kmajor(ab + k * 32),
@@ -528,13 +474,11 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// One tensor map per large front.  BF16: over its FP32 L panel, m rows x c
-// pivot columns, column-major with leading dimension ldl (a multiple of 8,
-// so the column stride is a multiple of 16 bytes; the panel starts on 128
-// bytes), boxes of 32 rows x 64 columns without swizzle.  3xTF32: over its
-// split panel scratch, row-major, kPanel columns (the inner dimension) x
-// 2 mpad rows (hi then lo; a row is 1 KB), boxes of 32 columns x 128 rows
-// with the 128-byte swizzle.  Reads past the rows or columns return zeros.
+// One tensor map per large front, over its panel scratch (row-major: kPanel
+// columns, the inner dimension, of 1 KB (3xTF32) or 512 B (BF16) per row):
+// 3xTF32, FP32 values, 2 mpad rows (hi then lo); BF16, BF16 values, mpad
+// rows.  Boxes of 128 bytes of columns x 128 rows with the 128-byte swizzle;
+// reads past the rows return zeros.
 int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t>& scr_off,
                      std::vector<CUtensorMap>& maps, std::vector<int>& idx, bool bf16) {
     EncodeTiledFn enc = encode_fn();
@@ -545,30 +489,19 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
         const int s = P.large_list[q];
         const FrontDesc& f = P.fronts[s];
         idx[s] = (int)q;
-        cuuint64_t dims[2], strides[1];
-        cuuint32_t box[2];
+        const int mpad = panel_mpad(f.m);
+        const int esz = bf16 ? 2 : 4;
+        cuuint64_t dims[2] = {(cuuint64_t)kPanel, (cuuint64_t)(bf16 ? mpad : 2 * mpad)};
+        cuuint64_t strides[1] = {(cuuint64_t)kPanel * esz};
+        cuuint32_t box[2] = {(cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK),
+                             (cuuint32_t)tc::BM};
         cuuint32_t estr[2] = {1, 1};
-        void* ptr;
-        if (bf16) {
-            dims[0] = (cuuint64_t)f.m;
-            dims[1] = (cuuint64_t)f.c;
-            strides[0] = (cuuint64_t)f.ldl * 4;
-            box[0] = tc::BOX;
-            box[1] = tc::Cfg<true>::BK;
-            ptr = const_cast<float*>(base + f.loff);
-        } else {
-            const int mpad = panel_mpad(f.m);
-            dims[0] = (cuuint64_t)kPanel;
-            dims[1] = (cuuint64_t)(2 * mpad);
-            strides[0] = (cuuint64_t)kPanel * 4;
-            box[0] = tc::Cfg<false>::BK;  // 32 columns = 128 bytes
-            box[1] = tc::BM;
-            ptr = const_cast<float*>(base + scr_off[s]);
-        }
-        CUresult r = enc(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, ptr, dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         bf16 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        void* ptr = const_cast<float*>(base + scr_off[s]);
+        CUresult r = enc(&maps[q],
+                         bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return -2;
     }
     return 0;
