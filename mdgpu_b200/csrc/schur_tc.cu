@@ -25,13 +25,14 @@
 //              kind::tf32 (M = N = 128), or one kind::f16 per 16 columns,
 //              into the tile's TMEM accumulator; each stage is committed
 //              back to the loader, each finished tile to the epilogue;
-//   epilogue   3xTF32: eight warps, two per 32 TMEM lanes (tile rows), each
-//              pair splitting the columns; BF16: four warps.  tcgen05.ld of
-//              the accumulator, handed back once read, then C -= acc in
-//              place (coalesced along the columns).
+//   epilogue   eight warps, two per 32 TMEM lanes (tile rows), each two
+//              32-column blocks: the tile's old C values loaded first (under
+//              the tile's MMAs), then tcgen05.ld of the accumulator, handed
+//              back once read, and C -= acc in place (coalesced along the
+//              columns).
 // The TMEM accumulator is double-buffered (2 x 128 columns), so tile t's
-// epilogue runs under tile t + 1's MMAs.  3xTF32: 320 threads, three 64 KB
-// stages; BF16: 288 threads, two 96 KB stages; one CTA per SM.
+// epilogue runs under tile t + 1's MMAs.  320 threads, one CTA per SM;
+// 3xTF32: three 64 KB stages; BF16: six 32 KB stages.
 //
 // BF16 mode (the MDGPU_BF16 factor): the loaders round each FP32 chunk to
 // BF16 (nearest even) into a K-major copy with the 128-byte swizzle, and one
@@ -74,7 +75,8 @@ constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
 // Per-mode constants: a chunk is 128 bytes of K per operand row (32 TF32 or
 // 64 BF16 columns); a stage holds A_hi, B_hi, A_lo, B_lo (3xTF32) or A, B
 // (BF16), 16 KB each, as the panel kernel wrote them.  One TMA warp, one MMA
-// warp, eight epilogue warps (two per 32 TMEM lanes); one CTA per SM.
+// warp, eight epilogue warps (two per 32 TMEM lanes, two 32-column blocks
+// each); one CTA per SM.
 template <bool BF>
 struct Cfg {
     static constexpr int BK = BF ? 64 : 32;       // K columns per chunk
@@ -402,46 +404,68 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31; with
-        // eight epilogue warps each pair of a quarter splits the columns
-        const int quarter = warp & 3;
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile
+        // rows) and NCB 32-column blocks of them (two warps per lane
+        // quarter).  The tile's old C values are loaded before the
+        // accumulator is waited for, so their latency hides under the MMAs.
         constexpr int NCB = BN / 32 / (C::NEPI / 4);  // 32-column blocks per warp
-        const int cb0 = ((warp - MMA_WARP - 1) / 4) * NCB;
+        const int quarter = warp & 3;
+        const int cb0 = ((warp - MMA_WARP - 1) >> 2) * NCB;
         int tl = 0;
         for (int b = blockIdx.x; b < ntiles; b += gridDim.x, ++tl) {
             const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
             const FrontDesc f = fronts[t.s];
             const int acc = tl & 1;
+            const int row = t.I * BM + quarter * 32 + lane;
+            const int col0 = t.J * BN + cb0 * 32;
+            float* const Lrow = Ls + f.loff + row;          // C(row, col), col < c
+            float* const Urow = Us + f.uoff + (row - f.c);  // C(row, col), col >= c
+            // 32 columns from c0 of this lane's row: a pointer walked along
+            // them (L panel, then the update store from column c on)
+            auto start = [&](int c0) -> float* {
+                return c0 < f.c ? Lrow + (int64_t)c0 * f.ldl : Urow + (int64_t)(c0 - f.c) * f.ldu;
+            };
+            // valid columns of this lane's row: [t.cbeg, chi)
+            const int chi = row < f.m ? min(f.m, row + 1) : t.cbeg;
+            // old C values of a 32-column block into o (zeros outside)
+            auto load_block = [&](int c0, float (&o)[32]) {
+                float* p = start(c0);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int col = c0 + q;
+                    if (col == f.c) p = Urow;
+                    o[q] = (col >= t.cbeg && col < chi) ? *p : 0.f;
+                    p += col < f.c ? f.ldl : f.ldu;
+                }
+            };
+            auto store_block = [&](int c0, const float (&o)[32], const float (&v)[32]) {
+                float* p = start(c0);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int col = c0 + q;
+                    if (col == f.c) p = Urow;
+                    if (col >= t.cbeg && col < chi) *p = o[q] - v[q];
+                    p += col < f.c ? f.ldl : f.ldu;
+                }
+            };
+            // the first block's old values load before the wait (under the
+            // tile's MMAs), each later block's after the previous store
+            float old[32], v[32];
+            load_block(col0, old);
             if (!tc::mbar_wait(&accf_bar[acc], (uint32_t)(tl >> 1) & 1, &abort_sh)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int row = t.I * BM + quarter * 32 + lane;
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + acc * BN + cb0 * 32;
 #pragma unroll 1
-            for (int cb = cb0; cb < cb0 + NCB; ++cb) {
-                float v[32];
-                tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + acc * BN + cb * 32, v);
-                if (cb == cb0 + NCB - 1) {
-                    // every TMEM read of this accumulator is done: hand it back
+            for (int k = 0; k < NCB; ++k) {
+                if (k > 0) load_block(col0 + 32 * k, old);
+                tc::tmem_ld32(taddr + 32 * k, v);
+                if (k == NCB - 1) {
+                    // this warp's TMEM reads of the accumulator are done
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                     __syncwarp();
                     if (lane == 0) tc::mbar_arrive(&acce_bar[acc]);
                 }
-                if (row < f.m) {
-                    // all 32 addresses and old values first (independent
-                    // loads in flight), then the stores
-                    float* p[32];
-                    float old[32];
-#pragma unroll
-                    for (int q = 0; q < 32; ++q) {
-                        const int col = t.J * BN + cb * 32 + q;
-                        const bool in = col >= t.cbeg && col < f.m && row >= col;
-                        p[q] = in ? front_elem(Ls, Us, f, row, col) : nullptr;
-                    }
-#pragma unroll
-                    for (int q = 0; q < 32; ++q) old[q] = p[q] ? *p[q] : 0.f;
-#pragma unroll
-                    for (int q = 0; q < 32; ++q)
-                        if (p[q]) *p[q] = old[q] - v[q];
-                }
+                store_block(col0 + 32 * k, old, v);
             }
         }
     }
