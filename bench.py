@@ -54,8 +54,8 @@ CLASS_KERNELS = {
     "potrf": ["k_tile_potrf"],
     "panel": ["k_panel"],
     "schur_update": ["k_schur_tc"],
-    "solve_small": ["k_fwd_level", "k_bwd_level"],
-    "solve_large": ["k_fwd_level", "k_bwd_level"],
+    "solve_small": ["k_fwd_solve", "k_bwd_solve"],
+    "solve_large": ["k_fwd_solve", "k_bwd_solve"],
 }
 CLASS_KERNELS_FP64 = dict(CLASS_KERNELS, schur_update=["k_schur_f64"])
 

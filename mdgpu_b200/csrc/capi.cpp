@@ -471,7 +471,22 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
         D.solve.gather_nch = h->keep(upload(SS.gather_nch));
         D.solve.gather_off = h->keep(upload(SS.gather_off));
         D.solve.nflags = SS.nflags;
-        D.solve.nsync = 2 * P.nlevels + SS.nflags + 1;
+        auto items = [&](const std::vector<int>& v, int& n) {
+            n = (int)(v.size() / 4);
+            std::vector<int> w = v;
+            if (w.empty()) w.assign(4, 0);
+            return reinterpret_cast<int4*>(h->keep(upload(w)));
+        };
+        D.solve.fwd_items = items(SS.fwd_items, D.solve.nfwd_items);
+        D.solve.bwd_items = items(SS.bwd_items, D.solve.nbwd_items);
+        {
+            std::vector<int> wc = SS.warp_cnt;
+            if (wc.empty()) wc.assign(3, 0);
+            D.solve.warp_cnt_d = h->keep(upload(wc));
+        }
+        D.solve.bwd_target = h->keep(upload(SS.bwd_target));
+        D.solve.nfronts = P.nsuper;
+        D.solve.nsync = 3 + SS.nflags + 3 * P.nsuper;
         D.solve.sync = h->keep(dalloc<int>(D.solve.nsync));
     }
     // algorithmic work per launch, for the profiler's roofline figures

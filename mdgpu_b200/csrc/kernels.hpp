@@ -90,13 +90,21 @@ struct DevSchedule {
     std::vector<PanelOp> h_ops;
 };
 
-// Large-front solve: per level one forward and one backward launch over
-// dependency-ordered (front, tile) tasks.  sync holds 2 * nlevels ticket
-// counters, one flag per pivot tile and the abort word; it is cleared at the
-// start of every solve.  err (not cleared by the solve) gets bit 0 when a
-// dependency wait ran out.
+// Solve: one launch per direction over every level's work items (see
+// SolveScheduleHost).  sync holds the two ticket counters, one count per
+// pivot tile (backward gathers counted in), the abort word, then per front
+// the forward count of finished children, the forward count of finished
+// update tiles and the backward count of finished completions; it is
+// cleared at the start of every solve.  err (not cleared by the solve) gets
+// bit 0 when a dependency wait ran out.
 struct SolveSchedule {
     int2* tasks = nullptr;
+    int4* fwd_items = nullptr;
+    int4* bwd_items = nullptr;
+    int nfwd_items = 0, nbwd_items = 0;
+    int* warp_cnt_d = nullptr;   // 3 per level
+    int* bwd_target = nullptr;   // per front
+    int nfronts = 0;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1
     std::vector<double> fwd_elems, bwd_elems;     // per level: L + Dinv elements
     std::vector<double> small_elems;              // per level: L elements of small fronts

@@ -594,15 +594,17 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     S.gather_nch.assign(P.nsuper, 0);
     S.gather_off.assign(P.nsuper, 0);
     S.gather_vecs = 0;
+    int64_t vecs = 0;
     for (int l = 0; l < P.nlevels; ++l) {
         S.gather_task_beg[l] = (int)(S.tasks.size() / 2);
-        int64_t vecs = 0;
         for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
             const int s = P.large_list[q];
             const FrontDesc& f = P.fronts[s];
             const int nt1 = (f.c + T - 1) / T, nu = (f.m - f.c + T - 1) / T;
             const int nch = (nu + GC - 1) / GC;
             S.gather_nch[s] = nch;
+            if (vecs + (int64_t)nt1 * nch > INT32_MAX)
+                throw std::runtime_error("update-row partial sums exceed 2^31 vectors");
             S.gather_off[s] = (int)vecs;
             vecs += (int64_t)nt1 * nch;
             for (int j = 0; j < nt1; ++j)
@@ -611,9 +613,32 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
                     S.tasks.push_back(j | (h << 16));
                 }
         }
-        S.gather_vecs = std::max(S.gather_vecs, vecs);
     }
+    S.gather_vecs = vecs;
     S.gather_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
+    // the fused launches' item lists
+    const int WPI = SolveScheduleHost::kWarpsPerItem;
+    auto level_items = [&](int l, bool fwd, std::vector<int>& it) {
+        if (!fwd)
+            for (int q = S.gather_task_beg[l]; q < S.gather_task_beg[l + 1]; ++q)
+                it.insert(it.end(), {SolveScheduleHost::kItemGather, S.tasks[2 * q],
+                                     S.tasks[2 * q + 1], 0});
+        const std::vector<int>& beg = fwd ? S.fwd_task_beg : S.bwd_task_beg;
+        for (int q = beg[l]; q < beg[l + 1]; ++q)
+            it.insert(it.end(),
+                      {SolveScheduleHost::kItemTile, S.tasks[2 * q], S.tasks[2 * q + 1], 0});
+        const int n1 = S.warp_cnt[3 * l], n2 = S.warp_cnt[3 * l + 1], n4 = S.warp_cnt[3 * l + 2];
+        const int nw = n1 + (n2 + 1) / 2 + (n4 + 3) / 4;
+        const int sb = P.small_ptr[l * kSmallBuckets];
+        for (int t0 = 0; t0 < nw; t0 += WPI)
+            it.insert(it.end(), {SolveScheduleHost::kItemWarps, l, t0, sb});
+    };
+    S.fwd_items.clear();
+    S.bwd_items.clear();
+    for (int l = 0; l < P.nlevels; ++l) level_items(l, true, S.fwd_items);
+    for (int l = P.nlevels - 1; l >= 0; --l) level_items(l, false, S.bwd_items);
+    S.bwd_target.assign(P.nsuper, 1);
+    for (int s : P.large_list) S.bwd_target[s] = (P.fronts[s].c + T - 1) / T;
 }
 
 void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S) {

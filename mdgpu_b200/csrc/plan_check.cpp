@@ -257,6 +257,43 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                 }
             }
         }
+        // the one-launch solve's item lists: levels in order (forward
+        // bottom-up, backward top-down); per level the backward gathers,
+        // then the tile tasks exactly as the level's task list orders them,
+        // then the warp items covering the level's warp tasks
+        {
+            const int WPI = SolveScheduleHost::kWarpsPerItem;
+            for (int dir = 0; dir < 2; ++dir) {
+                const std::vector<int>& it = dir == 0 ? Q.fwd_items : Q.bwd_items;
+                if (it.size() % 4) bad("solve items");
+                size_t q = 0;
+                for (int step = 0; step < P.nlevels; ++step) {
+                    const int l = dir == 0 ? step : P.nlevels - 1 - step;
+                    if (dir == 1)
+                        for (int t = Q.gather_task_beg[l]; t < Q.gather_task_beg[l + 1]; ++t, q += 4)
+                            if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemGather ||
+                                it[q + 1] != Q.tasks[2 * t] || it[q + 2] != Q.tasks[2 * t + 1])
+                                bad("solve items: gathers", l);
+                    const std::vector<int>& beg = dir == 0 ? Q.fwd_task_beg : Q.bwd_task_beg;
+                    for (int t = beg[l]; t < beg[l + 1]; ++t, q += 4)
+                        if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemTile ||
+                            it[q + 1] != Q.tasks[2 * t] || it[q + 2] != Q.tasks[2 * t + 1])
+                            bad("solve items: tile tasks", l);
+                    const int nw = Q.warp_cnt[3 * l] + (Q.warp_cnt[3 * l + 1] + 1) / 2 +
+                                   (Q.warp_cnt[3 * l + 2] + 3) / 4;
+                    for (int t0 = 0; t0 < nw; t0 += WPI, q += 4)
+                        if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemWarps ||
+                            it[q + 1] != l || it[q + 2] != t0 ||
+                            it[q + 3] != P.small_ptr[l * kSmallBuckets])
+                            bad("solve items: warp tasks", l);
+                }
+                if (q != it.size()) bad("solve items: extra entries");
+            }
+            if ((int)Q.bwd_target.size() != ns) bad("backward targets");
+            for (int s = 0; s < ns; ++s)
+                if (Q.bwd_target[s] != (is_large[s] ? (P.fronts[s].c + T - 1) / T : 1))
+                    bad("backward target", s);
+        }
         // the residual's CSR of the caller's matrix
         if ((int)csr_rowptr.size() != n + 1 || csr_rowptr[0] != 0 || csr_rowptr[n] != csr_nnz)
             bad("CSR row pointers");

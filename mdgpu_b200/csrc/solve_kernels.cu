@@ -40,6 +40,8 @@ __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) 
 // ---------------------------------------------------------------------------
 
 constexpr int kSolveWaitPolls = 1 << 18;  // ~0.1-0.3 s at ~1 us per poll
+constexpr int kWarpSolveRhs = 4;   // right-hand sides per pass of the warp path
+constexpr int kSolvePassRhs = 32;  // right-hand sides per pass of the solve launches
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     int v;
@@ -152,193 +154,6 @@ __device__ __forceinline__ void load_block_async(TL* dst, const TL* src, int64_t
             cp_async_elem(d, src + r + (int64_t)col * ld);
         else
             *d = TL(0);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// small fronts: CTA per front, the L panel staged in shared memory in blocks
-// of kSmallSolveCols columns (a block of a column-major panel is one
-// contiguous range: 16-byte cp.async, the next block loading while the
-// current one is used)
-// ---------------------------------------------------------------------------
-
-constexpr int kSmallSolveCols = 16;
-
-template <typename TL>
-__device__ __forceinline__ void load_panel_cols_async(TL* dst, const TL* src, int ncols, int ldl) {
-    const int nchunk = (int)((size_t)ncols * ldl * sizeof(TL) / 16);
-    const char* s = reinterpret_cast<const char*>(src);
-    char* d = reinterpret_cast<char*>(dst);
-    for (int q = threadIdx.x; q < nchunk; q += blockDim.x) {
-        const uint32_t da = static_cast<uint32_t>(__cvta_generic_to_shared(d + 16 * (size_t)q));
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(da), "l"(s + 16 * (size_t)q)
-                     : "memory");
-    }
-}
-
-// shared memory: front vector (msmall x nrhs) + two panel blocks
-template <typename TL, typename TV>
-__host__ __device__ constexpr size_t small_fwd_smem(int msmall, int nrhs) {
-    return (((size_t)msmall * nrhs * sizeof(TV) + 15) / 16) * 16 +
-           2 * (size_t)kSmallSolveCols * ((msmall + 7) & ~7) * sizeof(TL);
-}
-// shared memory: update-row solution (umax x nrhs) + pivot part (msmall x
-// nrhs) + two panel blocks
-template <typename TL, typename TV>
-__host__ __device__ constexpr size_t small_bwd_smem(int msmall, int umax, int nrhs) {
-    return ((((size_t)umax + msmall) * nrhs * sizeof(TV) + 15) / 16) * 16 +
-           2 * (size_t)kSmallSolveCols * ((msmall + 7) & ~7) * sizeof(TL);
-}
-
-template <typename TL, typename TV>
-__device__ void fwd_small_front(int s, const FrontDesc* __restrict__ fronts,
-                                const int* __restrict__ child, const int* __restrict__ relmap,
-                                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
-                                TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
-                                int msmall) {
-    constexpr int CB = kSmallSolveCols;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TV* f = reinterpret_cast<TV*>(smem_raw);
-    TL* Lb = reinterpret_cast<TL*>(smem_raw + (((size_t)msmall * nrhs * sizeof(TV) + 15) / 16) * 16);
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c, ldl = F.ldl;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const TL* L = Ls + F.loff;
-    const int nb = (c + CB - 1) / CB;
-    load_panel_cols_async(Lb, L, min(CB, c), ldl);
-    cp_async_commit_group();
-    for (int idx = tid; idx < m * nrhs; idx += nt) {
-        int q = idx / m, r = idx - q * m;
-        f[idx] = r < c ? xp[F.first_col + r + (int64_t)q * n] : TV(0);
-    }
-    __syncthreads();
-    for (int h = F.child_beg; h < F.child_end; ++h) {
-        const int ch = child[h];
-        const FrontDesc g = fronts[ch];
-        const int uc = g.m - g.c;
-        const TV* w = front_vec(fv, fv_off, ch, nrhs);
-        const int* rm = relmap + g.rows_off + g.c;
-        for (int idx = tid; idx < uc * nrhs; idx += nt) {
-            int q = idx / uc, r = idx - q * uc;
-            f[rm[r] + q * m] += w[(g.c + r) * nrhs + q];
-        }
-        __syncthreads();
-    }
-    for (int b = 0; b < nb; ++b) {
-        const int j0 = b * CB, j1 = min(c, j0 + CB);
-        if (b + 1 < nb)
-            load_panel_cols_async(Lb + ((b + 1) & 1) * CB * ldl, L + (int64_t)(j0 + CB) * ldl,
-                                  min(CB, c - j0 - CB), ldl);
-        cp_async_commit_group();
-        cp_async_wait_groups<1>();
-        __syncthreads();
-        const TL* Bk = Lb + (b & 1) * CB * ldl;
-        for (int j = j0; j < j1; ++j) {
-            const TL* col = Bk + (j - j0) * ldl;
-            const TV inv = TV(1) / (TV)col[j];
-            for (int q = tid; q < nrhs; q += nt) f[j + q * m] *= inv;
-            __syncthreads();
-            const int rows = m - j - 1;
-            for (int idx = tid; idx < rows * nrhs; idx += nt) {
-                int q = idx / rows, r = j + 1 + (idx - q * rows);
-                f[r + q * m] -= (TV)col[r] * f[j + q * m];
-            }
-            __syncthreads();
-        }
-    }
-    cp_async_wait_groups<0>();
-    TV* out = front_vec(fv, fv_off, s, nrhs);
-    for (int idx = tid; idx < m * nrhs; idx += nt) {
-        int q = idx / m, r = idx - q * m;
-        if (r < c)
-            xp[F.first_col + r + (int64_t)q * n] = f[idx];
-        else
-            out[r * nrhs + q] = f[idx];
-    }
-}
-
-// Backward: t = y - L21' x_u (x_u: the already final update rows), then
-// column blocks from the last: t_B -= L(rows below B in the pivot part, B)'
-// x (dot products, a warp per column), then the block's own triangle from
-// the last column (row j of the block read from the staged columns).
-template <typename TL, typename TV>
-__device__ void bwd_small_front(int s, const FrontDesc* __restrict__ fronts,
-                                const int* __restrict__ rows, const TL* __restrict__ Ls,
-                                TV* __restrict__ xp, int n, int nrhs, int umax, int msmall) {
-    constexpr int CB = kSmallSolveCols;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TV* xb = reinterpret_cast<TV*>(smem_raw);  // u x nrhs
-    TV* t = xb + (size_t)umax * nrhs;          // c x nrhs
-    TL* Lb = reinterpret_cast<TL*>(smem_raw +
-                                   ((((size_t)umax + msmall) * nrhs * sizeof(TV) + 15) / 16) * 16);
-    const FrontDesc F = fronts[s];
-    const int m = F.m, c = F.c, u = m - c, ldl = F.ldl;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    const TL* L = Ls + F.loff;
-    const int* rw = rows + F.rows_off + c;
-    const int nb = (c + CB - 1) / CB;
-    {  // last block first
-        const int j0 = (nb - 1) * CB;
-        load_panel_cols_async(Lb + ((nb - 1) & 1) * CB * ldl, L + (int64_t)j0 * ldl, c - j0, ldl);
-    }
-    cp_async_commit_group();
-    for (int idx = tid; idx < u * nrhs; idx += nt) {
-        int q = idx / u, r = idx - q * u;
-        xb[idx] = xp[rw[r] + (int64_t)q * n];
-    }
-    for (int idx = tid; idx < c * nrhs; idx += nt) {
-        int q = idx / c, j = idx - q * c;
-        t[idx] = xp[F.first_col + j + (int64_t)q * n];
-    }
-    __syncthreads();
-    for (int j = warp; j < c; j += nw) {
-        const TL* col = L + c + (int64_t)j * ldl;
-        for (int q = 0; q < nrhs; ++q) {
-            TV acc = TV(0);
-            for (int r = lane; r < u; r += 32) acc += (TV)col[r] * xb[r + q * u];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) t[j + q * c] -= acc;
-        }
-    }
-    for (int b = nb - 1; b >= 0; --b) {
-        const int j0 = b * CB, j1 = min(c, j0 + CB);
-        if (b > 0)
-            load_panel_cols_async(Lb + ((b - 1) & 1) * CB * ldl, L + (int64_t)(j0 - CB) * ldl, CB,
-                                  ldl);
-        cp_async_commit_group();
-        cp_async_wait_groups<1>();
-        __syncthreads();
-        const TL* Bk = Lb + (b & 1) * CB * ldl;
-        // rows [j1, c) of the pivot part are final
-        for (int j = j0 + warp; j < j1; j += nw) {
-            const TL* col = Bk + (j - j0) * ldl;
-            for (int q = 0; q < nrhs; ++q) {
-                TV acc = TV(0);
-                for (int r = j1 + lane; r < c; r += 32) acc += (TV)col[r] * t[r + q * c];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) t[j + q * c] -= acc;
-            }
-        }
-        __syncthreads();
-        for (int j = j1 - 1; j >= j0; --j) {
-            const TV inv = TV(1) / (TV)Bk[j + (j - j0) * ldl];
-            for (int q = tid; q < nrhs; q += nt) t[j + q * c] *= inv;
-            __syncthreads();
-            const int w = j - j0;
-            for (int idx = tid; idx < w * nrhs; idx += nt) {
-                int q = idx / w, l = j0 + (idx - q * w);
-                t[l + q * c] -= (TV)Bk[j + (l - j0) * ldl] * t[j + q * c];
-            }
-            __syncthreads();
-        }
-    }
-    cp_async_wait_groups<0>();
-    for (int idx = tid; idx < c * nrhs; idx += nt) {
-        int q = idx / c, j = idx - q * c;
-        xp[F.first_col + j + (int64_t)q * n] = t[idx];
     }
 }
 
@@ -471,7 +286,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
             TV x = TV(0);
             if (r < ti.size && q < nrhs && (!lsplit || (g == 0 && j == 0))) {
                 if (R < F.c) x = xp[F.first_col + R + (int64_t)q * n];
-                for (int e = e0; e < e1; ++e) x += fv[(int64_t)amap_ent[e] * nrhs + q];
+                for (int e = e0; e < e1; ++e) x += __ldcg(fv + (int64_t)amap_ent[e] * nrhs + q);
             }
             v[j] = x;
         }
@@ -639,28 +454,50 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
         sm.idx[e] = rr < tkr.size ? rw[tkr.start + rr] : -1;
     }
     __syncthreads();
+    // two stages: the L blocks by cp.async; the ancestors' solution rows
+    // (written in this launch) through L2 into registers one stage ahead,
+    // stored into their stage after the previous stage's products
+    static_assert(kTile * kSolvePassRhs % 256 == 0, "whole vector elements per thread");
+    constexpr int VPT = kTile * kSolvePassRhs / 256;
+    TV pend[VPT];
+    auto fetch = [&](int p) {
+#pragma unroll
+        for (int k = 0; k < VPT; ++k) {
+            const int e = tid + 256 * k;
+            pend[k] = TV(0);
+            if (p < P && e < T * nrhs) {
+                const int row = sm.idx[p * T + (e & (T - 1))], q = e / T;
+                if (row >= 0) pend[k] = __ldcg(xp + row + (int64_t)q * n);
+            }
+        }
+    };
+    auto put = [&](int p) {
+        if (p >= P) return;
+        TV* v = sm.vb(p, nrhs);
+#pragma unroll
+        for (int k = 0; k < VPT; ++k) {
+            const int e = tid + 256 * k;
+            if (e < T * nrhs) v[e] = pend[k];
+        }
+    };
     auto issue = [&](int p) {
         if (p < P) {
             const TileRange tkr = tile_range(k0 + p, F.m, F.c, T);
             load_block_async(sm.lb(p), Lc + tkr.start, F.ldl, tkr.size, tj.size);
-            TV* v = sm.vb(p, nrhs);
-            for (int e = tid; e < T * nrhs; e += blockDim.x) {
-                const int row = sm.idx[p * T + (e & (T - 1))], q = e / T;
-                if (row >= 0)
-                    cp_async_elem(v + e, xp + row + (int64_t)q * n);
-                else
-                    v[e] = TV(0);
-            }
         }
         cp_async_commit_group();
     };
-    for (int p = 0; p < sm.stg - 1; ++p) issue(p);
+    static_assert(level_stages<TL>(1) == 2, "the gather's vector pipeline has two stages");
+    issue(0);
+    fetch(0);
+    put(0);
     TV acc[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) acc[a] = TV(0);
     for (int p = 0; p < P; ++p) {
-        issue(p + sm.stg - 1);
-        cp_async_wait_stages(sm.stg);
+        issue(p + 1);
+        fetch(p + 1);
+        cp_async_wait_groups<1>();
         __syncthreads();
         const TL* Bk = sm.lb(p);
         const TV* X = sm.vb(p, nrhs);
@@ -679,6 +516,7 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
             }
         }
         __syncthreads();
+        put(p + 1);
     }
     cp_async_wait_groups<0>();
     TV* out = part + ((int64_t)gather_off[s] + (int64_t)j * gather_nch[s] + h) * T * nrhs;
@@ -705,18 +543,27 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
 // ---------------------------------------------------------------------------
 // small fronts: a warp per front, the right-hand sides in passes of NQ
 // (kWarpSolveRhs, or one), lane l holding rows l, l + 32, ... (R slots,
-// m <= 32 R) of the pass's right-hand sides in registers.  Forward: the pivot value is broadcast by a shuffle and
-// every lane updates its rows below it; backward: a warp reduction per pivot
-// column (dot product with the final rows below it).  No block barriers; the
-// children's update parts are summed into a per-warp shared buffer (child by
-// child, deterministic) before the rows are taken into registers.
+// m <= 32 R) of the pass's right-hand sides in registers.  Forward: the
+// pivot value is broadcast by a shuffle and every lane updates its rows
+// below it; backward: a warp reduction per pivot column (dot product with
+// the final rows below it).  No block barriers; the children's update parts
+// are summed into a per-warp shared buffer (child by child, deterministic)
+// before the rows are taken into registers.
 // ---------------------------------------------------------------------------
 
-constexpr int kWarpSolveRhs = 4;   // right-hand sides per pass of the warp path
-constexpr int kSolvePassRhs = 32;  // right-hand sides per pass of the level kernels
-// small fronts run as warp tasks up to this many right-hand sides (a level
-// pass), as a CTA per front above
-constexpr int kWarpPathMaxRhs = 32;
+// Dependency words of the one-launch solve.  Forward: front s starts once
+// done[s] (its finished children) reaches its child count, and counts
+// itself in at its parent once its update rows are written.  Backward:
+// front s starts once done[parent] reaches target[parent] (the parent's
+// solution rows are final), and counts one completion of its own once its
+// solution rows are written.  Data written inside the launch by other CTAs
+// (children's update rows, ancestors' solution rows) are read through L2.
+struct FrontDeps {
+    int* done;
+    const int* target;  // backward only
+    int* abort_flag;
+    int* err;
+};
 
 // Fronts of at most W rows (W = 8, 16, 32) on a group of W lanes of a warp
 // (32 / W fronts per warp), one row per lane.  mask: the group's lanes; the
@@ -726,13 +573,31 @@ __device__ __forceinline__ unsigned group_mask() {
     return W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1)));
 }
 
+// the group's first lane waits (bounded) for *word >= target; uniform result
+template <int W>
+__device__ __forceinline__ bool group_wait(const int* word, int target, const FrontDeps& d,
+                                           unsigned mask) {
+    int ok = 1;
+    if ((threadIdx.x & (W - 1)) == 0) ok = wait_flag(word, target, d.abort_flag, d.err) ? 1 : 0;
+    return __shfl_sync(mask, ok, 0, W) != 0;
+}
+// every lane's stores, a device-scope fence, then one increment of *word
+template <int W>
+__device__ __forceinline__ void group_signal(int* word, unsigned mask) {
+    __threadfence();
+    __syncwarp(mask);
+    if (word && (threadIdx.x & (W - 1)) == 0) atomicAdd(word, 1);
+}
+
 template <typename TL, typename TV, int W, int NQ>
-__device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict__ fronts,
+__device__ void fwd_group_front(int s, const FrontDesc& F, const FrontDeps& deps,
+                                const FrontDesc* __restrict__ fronts,
                                 const int* __restrict__ child, const int* __restrict__ relmap,
                                 const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
                                 TV* __restrict__ xp, TV* __restrict__ out, TV* __restrict__ fv,
                                 int n, int nrhs, TV* wbuf) {
     const unsigned mask = group_mask<W>();
+    if (!group_wait<W>(deps.done + s, F.child_end - F.child_beg, deps, mask)) return;
     const int r = threadIdx.x & (W - 1);
     const int m = F.m, c = F.c;
     const int64_t ldl = F.ldl;
@@ -753,7 +618,7 @@ __device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict_
                 const int p = relmap[g.rows_off + g.c + r];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    if (q < nq) wbuf[q * 32 + p] += w[r * nrhs + q];
+                    if (q < nq) wbuf[q * 32 + p] += __ldcg(w + r * nrhs + q);
             }
             __syncwarp(mask);
         }
@@ -790,12 +655,16 @@ __device__ void fwd_group_front(const FrontDesc& F, const FrontDesc* __restrict_
                 out[r * nrhs + q0 + q] = v[q];
         }
     }
+    group_signal<W>(F.parent >= 0 ? deps.done + F.parent : nullptr, mask);
 }
 
 template <typename TL, typename TV, int W, int NQ>
-__device__ void bwd_group_front(const FrontDesc& F, const int* __restrict__ rows,
-                                const TL* __restrict__ Ls, TV* __restrict__ xp, int n, int nrhs) {
+__device__ void bwd_group_front(int s, const FrontDesc& F, const FrontDeps& deps,
+                                const int* __restrict__ rows, const TL* __restrict__ Ls,
+                                TV* __restrict__ xp, int n, int nrhs) {
     const unsigned mask = group_mask<W>();
+    if (F.parent >= 0 && !group_wait<W>(deps.done + F.parent, deps.target[F.parent], deps, mask))
+        return;
     const int r = threadIdx.x & (W - 1);
     const int m = F.m, c = F.c;
     const int64_t ldl = F.ldl;
@@ -807,7 +676,7 @@ __device__ void bwd_group_front(const FrontDesc& F, const int* __restrict__ rows
         TV v[NQ];  // y on the pivot rows (x once solved), final x on the others
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
-            v[q] = (q < nq && r < m) ? xp[src + (int64_t)(q0 + q) * n] : TV(0);
+            v[q] = (q < nq && r < m) ? __ldcg(xp + src + (int64_t)(q0 + q) * n) : TV(0);
         const int jl = c - 1;
         TV lc = (r > jl && r < m) ? (TV)L[r + jl * ldl] : TV(0), d = (TV)L[jl + jl * ldl];
         for (int j = jl; j >= 0; --j) {
@@ -835,16 +704,19 @@ __device__ void bwd_group_front(const FrontDesc& F, const int* __restrict__ rows
         for (int q = 0; q < NQ; ++q)
             if (q < nq && r < c) xp[F.first_col + r + (int64_t)(q0 + q) * n] = v[q];
     }
+    group_signal<W>(deps.done + s, mask);
 }
 
 // Fronts of 33..160 rows: the same sweeps with the front vector kept in the
 // warp's shared buffer (ld MR rows per right-hand side) instead of registers.
 template <typename TL, typename TV, int NQ>
-__device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restrict__ fronts,
+__device__ void fwd_warp_front_smem(int s, const FrontDesc& F, const FrontDeps& deps,
+                                    const FrontDesc* __restrict__ fronts,
                                     const int* __restrict__ child, const int* __restrict__ relmap,
                                     const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
                                     TV* __restrict__ xp, TV* __restrict__ out, TV* __restrict__ fv,
                                     int n, int nrhs, TV* f, int MR) {
+    if (!group_wait<32>(deps.done + s, F.child_end - F.child_beg, deps, 0xffffffffu)) return;
     const int lane = threadIdx.x & 31;
     const int m = F.m, c = F.c;
     const int64_t ldl = F.ldl;
@@ -867,7 +739,7 @@ __device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restr
                 const int p = rm[rr];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    if (q < nq) f[q * MR + p] += w[rr * nrhs + q];
+                    if (q < nq) f[q * MR + p] += __ldcg(w + rr * nrhs + q);
             }
             __syncwarp();
         }
@@ -895,12 +767,16 @@ __device__ void fwd_warp_front_smem(const FrontDesc& F, const FrontDesc* __restr
                 if (q < nq) out[r * nrhs + q0 + q] = f[q * MR + r];
         __syncwarp();
     }
+    group_signal<32>(F.parent >= 0 ? deps.done + F.parent : nullptr, 0xffffffffu);
 }
 
 template <typename TL, typename TV, int NQ>
-__device__ void bwd_warp_front_smem(const FrontDesc& F, const int* __restrict__ rows,
-                                    const TL* __restrict__ Ls, TV* __restrict__ xp, int n,
-                                    int nrhs, TV* x, int MR) {
+__device__ void bwd_warp_front_smem(int s, const FrontDesc& F, const FrontDeps& deps,
+                                    const int* __restrict__ rows, const TL* __restrict__ Ls,
+                                    TV* __restrict__ xp, int n, int nrhs, TV* x, int MR) {
+    if (F.parent >= 0 &&
+        !group_wait<32>(deps.done + F.parent, deps.target[F.parent], deps, 0xffffffffu))
+        return;
     const int lane = threadIdx.x & 31;
     const int m = F.m, c = F.c;
     const int64_t ldl = F.ldl;
@@ -912,7 +788,7 @@ __device__ void bwd_warp_front_smem(const FrontDesc& F, const int* __restrict__ 
             const int src = r < c ? F.first_col + r : rw[r];
 #pragma unroll
             for (int q = 0; q < NQ; ++q)
-                x[q * MR + r] = q < nq ? xp[src + (int64_t)(q0 + q) * n] : TV(0);
+                x[q * MR + r] = q < nq ? __ldcg(xp + src + (int64_t)(q0 + q) * n) : TV(0);
         }
         __syncwarp();
         for (int j = c - 1; j >= 0; --j) {
@@ -941,11 +817,12 @@ __device__ void bwd_warp_front_smem(const FrontDesc& F, const int* __restrict__ 
             __syncwarp();
         }
     }
+    group_signal<32>(deps.done + s, 0xffffffffu);
 }
 
 // dispatch on the front's rows: registers up to 32, the shared buffer above
 template <typename TL, typename TV, int NQ>
-__device__ void fwd_warp_front(int s, const FrontDesc* __restrict__ fronts,
+__device__ void fwd_warp_front(int s, const FrontDeps& deps, const FrontDesc* __restrict__ fronts,
                                const int* __restrict__ child, const int* __restrict__ relmap,
                                const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
                                TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs,
@@ -953,22 +830,22 @@ __device__ void fwd_warp_front(int s, const FrontDesc* __restrict__ fronts,
     const FrontDesc F = fronts[s];
     TV* out = front_vec(fv, fv_off, s, nrhs);
     if (F.m <= 32)
-        fwd_group_front<TL, TV, 32, NQ>(F, fronts, child, relmap, fv_off, Ls, xp, out, fv, n, nrhs,
-                                        wbuf);
+        fwd_group_front<TL, TV, 32, NQ>(s, F, deps, fronts, child, relmap, fv_off, Ls, xp, out,
+                                        fv, n, nrhs, wbuf);
     else
-        fwd_warp_front_smem<TL, TV, NQ>(F, fronts, child, relmap, fv_off, Ls, xp, out, fv, n, nrhs,
-                                        wbuf, MR);
+        fwd_warp_front_smem<TL, TV, NQ>(s, F, deps, fronts, child, relmap, fv_off, Ls, xp, out,
+                                        fv, n, nrhs, wbuf, MR);
 }
 
 template <typename TL, typename TV, int NQ>
-__device__ void bwd_warp_front(int s, const FrontDesc* __restrict__ fronts,
+__device__ void bwd_warp_front(int s, const FrontDeps& deps, const FrontDesc* __restrict__ fronts,
                                const int* __restrict__ rows, const TL* __restrict__ Ls,
                                TV* __restrict__ xp, int n, int nrhs, TV* wbuf, int MR) {
     const FrontDesc F = fronts[s];
     if (F.m <= 32)
-        bwd_group_front<TL, TV, 32, NQ>(F, rows, Ls, xp, n, nrhs);
+        bwd_group_front<TL, TV, 32, NQ>(s, F, deps, rows, Ls, xp, n, nrhs);
     else
-        bwd_warp_front_smem<TL, TV, NQ>(F, rows, Ls, xp, n, nrhs, wbuf, MR);
+        bwd_warp_front_smem<TL, TV, NQ>(s, F, deps, rows, Ls, xp, n, nrhs, wbuf, MR);
 }
 
 // per-warp shared buffer of the warp path: MR = rows rounded up to 32, times
@@ -989,15 +866,16 @@ struct WarpTasks {
 
 
 template <typename TL, typename TV, int NQ>
-__device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __restrict__ fronts,
+__device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDeps& deps,
+                              const FrontDesc* __restrict__ fronts,
                               const int* __restrict__ child, const int* __restrict__ relmap,
                               const int64_t* __restrict__ fv_off, const TL* __restrict__ Ls,
                               TV* __restrict__ xp, TV* __restrict__ fv, int n, int nrhs, TV* wbuf,
                               int MR) {
     const int lane = threadIdx.x & 31;
     if (t < wt.n1) {
-        fwd_warp_front<TL, TV, NQ>(wt.list[t], fronts, child, relmap, fv_off, Ls, xp, fv, n, nrhs,
-                                   wbuf, MR);
+        fwd_warp_front<TL, TV, NQ>(wt.list[t], deps, fronts, child, relmap, fv_off, Ls, xp, fv, n,
+                                   nrhs, wbuf, MR);
         return;
     }
     t -= wt.n1;
@@ -1007,7 +885,7 @@ __device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __res
         if (k < wt.n2) {
             const int s = wt.list[wt.n1 + k];
             const FrontDesc F = fronts[s];
-            fwd_group_front<TL, TV, 16, NQ>(F, fronts, child, relmap, fv_off, Ls, xp,
+            fwd_group_front<TL, TV, 16, NQ>(s, F, deps, fronts, child, relmap, fv_off, Ls, xp,
                                             front_vec(fv, fv_off, s, nrhs), fv, n, nrhs,
                                             wbuf + (lane & 16));
         }
@@ -1017,31 +895,37 @@ __device__ void fwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __res
     if (k < wt.n4) {
         const int s = wt.list[wt.n1 + wt.n2 + k];
         const FrontDesc F = fronts[s];
-        fwd_group_front<TL, TV, 8, NQ>(F, fronts, child, relmap, fv_off, Ls, xp,
+        fwd_group_front<TL, TV, 8, NQ>(s, F, deps, fronts, child, relmap, fv_off, Ls, xp,
                                        front_vec(fv, fv_off, s, nrhs), fv, n, nrhs,
                                        wbuf + (lane & 24));
     }
 }
 
 template <typename TL, typename TV, int NQ>
-__device__ void bwd_warp_task(const WarpTasks& wt, int t, const FrontDesc* __restrict__ fronts,
-                              const int* __restrict__ rows, const TL* __restrict__ Ls,
-                              TV* __restrict__ xp, int n, int nrhs, TV* wbuf, int MR) {
+__device__ void bwd_warp_task(const WarpTasks& wt, int t, const FrontDeps& deps,
+                              const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
+                              const TL* __restrict__ Ls, TV* __restrict__ xp, int n, int nrhs,
+                              TV* wbuf, int MR) {
     const int lane = threadIdx.x & 31;
     if (t < wt.n1) {
-        bwd_warp_front<TL, TV, NQ>(wt.list[t], fronts, rows, Ls, xp, n, nrhs, wbuf, MR);
+        bwd_warp_front<TL, TV, NQ>(wt.list[t], deps, fronts, rows, Ls, xp, n, nrhs, wbuf, MR);
         return;
     }
     t -= wt.n1;
     const int t2 = (wt.n2 + 1) / 2;
     if (t < t2) {
         const int k = 2 * t + (lane >> 4);
-        if (k < wt.n2) bwd_group_front<TL, TV, 16, NQ>(fronts[wt.list[wt.n1 + k]], rows, Ls, xp, n, nrhs);
+        if (k < wt.n2) {
+            const int s = wt.list[wt.n1 + k];
+            bwd_group_front<TL, TV, 16, NQ>(s, fronts[s], deps, rows, Ls, xp, n, nrhs);
+        }
         return;
     }
     const int k = 4 * (t - t2) + (lane >> 3);
-    if (k < wt.n4)
-        bwd_group_front<TL, TV, 8, NQ>(fronts[wt.list[wt.n1 + wt.n2 + k]], rows, Ls, xp, n, nrhs);
+    if (k < wt.n4) {
+        const int s = wt.list[wt.n1 + wt.n2 + k];
+        bwd_group_front<TL, TV, 8, NQ>(s, fronts[s], deps, rows, Ls, xp, n, nrhs);
+    }
 }
 
 // Backward, task (s, j): pivot column tile j of front s accumulates, once
@@ -1091,7 +975,7 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     for (int a = 0; a < NQ; ++a) {
         const int q = lsplit ? 0 : g + 4 * a;
         ypre[a] = (l < tj.size && q < nrhs && (!lsplit || (g == 0 && a == 0)))
-                      ? xp[xj + l + (int64_t)q * n]
+                      ? __ldcg(xp + xj + l + (int64_t)q * n)
                       : TV(0);
     }
     // the update-row partial sums of (s, j) (gathers hold lower tickets), in
@@ -1255,7 +1139,7 @@ __device__ void fwd_update_rt1(int s, int R0, int R1, const FrontDesc& F, double
     if (rv) {
         const int* ar = amap_row + amap_off[s] + R;
         const int e0 = ar[0], e1 = ar[1];
-        for (int e = e0; e < e1; ++e) f0 += fv[amap_ent[e]];
+        for (int e = e0; e < e1; ++e) f0 += __ldcg(fv + amap_ent[e]);
     }
     constexpr int GW = sizeof(TL) == 4 ? 16 : 8;  // columns per group (registers)
     constexpr int GPB = T / GW;                     // groups per 64-column block
@@ -1286,139 +1170,164 @@ __device__ void fwd_update_rt1(int s, int R0, int R1, const FrontDesc& F, double
     if (rv) f[R] = f0 - acc;
 }
 
-// One launch per level and direction.  Blocks [0, ntile) take tickets for
-// the dependency-ordered tile tasks of the large fronts; the blocks after
-// them run the small fronts: warp tasks (at most kWarpSolveRhs right-hand
-// sides; wblocks blocks looping over wt) or a CTA each (small_list, nsm of
-// them).  Small fronts depend only on lower levels (forward) or ancestors
-// (backward), never on this launch's tile tasks.  Backward tickets first
-// hand out the ngather update-row gathers (no waits), then the pivot tasks.
+// One launch per direction over every level's work items (the item lists,
+// in dependency order, and their kinds are described with the solve
+// schedule): persistent CTAs take items by atomic ticket.  An item only
+// waits for items with lower tickets -- children's and ancestors' fronts sit
+// on earlier levels of the list, a front's earlier pivot tiles and the
+// backward gathers earlier in its level -- and a CTA takes a ticket only
+// while it runs, so every wait is for a CTA that is running or done.
+// Forward: a front's items wait for its children (the count of finished
+// children), a small front counts itself in at its parent once written, a
+// large front once its last update tile is (a per-front count of finished
+// update tiles).  Backward: a front's items wait for its parent's solution
+// rows (the parent's count of completions: one per pivot tile of a large
+// front, one for a small front); the pivot tasks wait for their gathers'
+// counts as before.  Every wait polls with an iteration limit; on timeout
+// the launch is aborted (every later wait returns at once) and the error
+// word reaches the host.
 
-template <typename TL, typename TV, int NQ>
-__device__ void small_fronts_fwd(int b, WarpTasks wt, int wblocks, const int* small_list,
-                                 const FrontDesc* __restrict__ fronts, const int* __restrict__ child,
-                                 const int* __restrict__ relmap, const int64_t* __restrict__ fv_off,
-                                 const TL* __restrict__ Ls, TV* __restrict__ xp,
-                                 TV* __restrict__ fv, int n, int nrhs, int msmall) {
-    if (b < wblocks) {
-        {  // right-hand sides in passes of kWarpSolveRhs inside the warp task
-            extern __shared__ __align__(16) unsigned char smem_raw[];
-            const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
-            TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
-            const int ntask = wt.count();
-            for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
-                if (nrhs == 1)
-                    fwd_warp_task<TL, TV, 1>(wt, t, fronts, child, relmap, fv_off, Ls, xp, fv, n,
-                                             nrhs, wbuf, warp_rows(msmall));
-                else
-                    fwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, child, relmap, fv_off, Ls,
-                                                         xp, fv, n, nrhs, wbuf, warp_rows(msmall));
-                __syncwarp();
-            }
-        }
-        return;
-    }
-    fwd_small_front<TL, TV>(small_list[b - wblocks], fronts, child, relmap, fv_off, Ls, xp, fv, n,
-                            nrhs, msmall);
-}
-
-template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
-    k_fwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ tasks, int ntile,
-                int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
-                int* __restrict__ err, const int64_t* __restrict__ fv_off,
-                const int* __restrict__ amap_off, const int* __restrict__ amap_row,
-                const int* __restrict__ amap_ent, const int64_t* __restrict__ dinv_off,
-                WarpTasks wt, int wblocks, const int* __restrict__ small_list,
-                const int* __restrict__ child, const int* __restrict__ relmap,
-                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
-                TV* __restrict__ fv, int n, int nrhs, int msmall) {
-    if ((int)blockIdx.x >= ntile) {
-        small_fronts_fwd<TL, TV, NQ>(blockIdx.x - ntile, wt, wblocks, small_list, fronts, child,
-                                     relmap, fv_off, Ls, xp, fv, n, nrhs, msmall);
-        return;
-    }
-    __shared__ int s_task;
-    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
+// a CTA's tid 0 waits (bounded) for *word >= target; uniform result
+__device__ __forceinline__ bool cta_wait(const int* word, int target, int* abort_flag, int* err) {
+    __shared__ int s_wok;
+    if (threadIdx.x == 0) s_wok = wait_flag(word, target, abort_flag, err) ? 1 : 0;
     __syncthreads();
-    if (s_task >= ntile) {  // counter not cleared: refuse rather than read past the list
-        if (threadIdx.x == 0) atomicOr(err, 2);
-        return;
-    }
-    const int2 tk = tasks[s_task];
-    if constexpr (NQ == 1) {
-        // update tiles of fronts with at most kRt1MaxPivotTiles pivot tiles,
-        // one right-hand side: registers straight from L (measured faster
-        // there; the staged pipeline streams long column ranges better)
-        constexpr int T = kTile;
-        const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
-        const FrontDesc F = fronts[s];
-        const int nt1 = tiles_l(F.c, T);
-        if (nrhs == 1 && i0 >= nt1 && nt1 <= kRt1MaxPivotTiles) {
-            double* pb = pub + (dinv_off[s] / (T * T)) * T;
-            {
-                const TileRange a = tile_range(i0, F.m, F.c, T);
-                const TileRange b = tile_range(i0 + cnt - 1, F.m, F.c, T);
-                fwd_update_rt1<TL>(s, a.start, b.start + b.size, F, pb, abort_flag, err, amap_off,
-                                   amap_row, amap_ent, Ls, xp, front_vec(fv, fv_off, s, 1), fv);
-            }
-            return;
-        }
-    }
-    fwd_tile_task<TL, TV, NQ>(tk, fronts, pub, abort_flag, err, fv_off, amap_off, amap_row,
-                              amap_ent, dinv_off, Ls, Dinv, xp, fv, n, nrhs);
+    return s_wok != 0;
 }
 
 template <typename TL, typename TV, int NQ>
 __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
-    k_bwd_level(const FrontDesc* __restrict__ fronts, const int2* __restrict__ gtasks, int ngather,
-                const int2* __restrict__ tasks, int ntile, int* __restrict__ counter,
-                double* __restrict__ pub, int* __restrict__ abort_flag, int* __restrict__ err,
-                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
-                int* __restrict__ gcount, TV* __restrict__ part,
-                const int64_t* __restrict__ dinv_off, WarpTasks wt, int wblocks,
-                const int* __restrict__ small_list, const int* __restrict__ rows,
-                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp, int n,
-                int nrhs, int msmall) {
-    const int ntk = ngather + ntile;
-    if ((int)blockIdx.x >= ntk) {
-        const int b = blockIdx.x - ntk;
-        if (b < wblocks) {
-            {  // right-hand sides in passes of kWarpSolveRhs inside the warp task
-                extern __shared__ __align__(16) unsigned char smem_raw[];
-                const int wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
-                TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(msmall, nrhs);
-                const int ntask = wt.count();
-                for (int t = b * wpb + w; t < ntask; t += wblocks * wpb) {
-                    if (nrhs == 1)
-                        bwd_warp_task<TL, TV, 1>(wt, t, fronts, rows, Ls, xp, n, nrhs, wbuf,
-                                                 warp_rows(msmall));
-                    else
-                        bwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, fronts, rows, Ls, xp, n, nrhs,
-                                                             wbuf, warp_rows(msmall));
-                    __syncwarp();
+    k_fwd_solve(const FrontDesc* __restrict__ fronts, const int4* __restrict__ items, int nitems,
+                int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
+                int* __restrict__ err, int* __restrict__ fdone, int* __restrict__ udone,
+                const int64_t* __restrict__ fv_off, const int* __restrict__ amap_off,
+                const int* __restrict__ amap_row, const int* __restrict__ amap_ent,
+                const int64_t* __restrict__ dinv_off, const int* __restrict__ warp_list,
+                const int* __restrict__ warp_cnt, const int* __restrict__ child,
+                const int* __restrict__ relmap, const TL* __restrict__ Ls,
+                const TL* __restrict__ Dinv, TV* __restrict__ xp, TV* __restrict__ fv, int n,
+                int nrhs, int MR) {
+    constexpr int T = kTile;
+    __shared__ int s_item;
+    const FrontDeps deps{fdone, nullptr, abort_flag, err};
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int k = s_item;
+        if (k >= nitems) return;
+        const int4 it = items[k];
+        if (it.x == SolveScheduleHost::kItemWarps) {
+            extern __shared__ __align__(16) unsigned char smem_raw[];
+            const WarpTasks wt{warp_list + it.w, warp_cnt[3 * it.y], warp_cnt[3 * it.y + 1],
+                               warp_cnt[3 * it.y + 2]};
+            const int w = threadIdx.x >> 5, t = it.z + w;
+            TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(MR, nrhs);
+            if (t < wt.count()) {
+                if (nrhs == 1)
+                    fwd_warp_task<TL, TV, 1>(wt, t, deps, fronts, child, relmap, fv_off, Ls, xp,
+                                             fv, n, nrhs, wbuf, MR);
+                else
+                    fwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, deps, fronts, child, relmap,
+                                                         fv_off, Ls, xp, fv, n, nrhs, wbuf, MR);
+            }
+        } else {
+            // a tile task of a large front: its children first
+            const int2 tk = make_int2(it.y, it.z);
+            const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
+            const FrontDesc F = fronts[s];
+            const int nt1 = tiles_l(F.c, T);
+            if (cta_wait(fdone + s, F.child_end - F.child_beg, abort_flag, err)) {
+                bool done = false;
+                if constexpr (NQ == 1) {
+                    // update tiles of fronts with at most kRt1MaxPivotTiles
+                    // pivot tiles, one right-hand side: registers straight
+                    // from L (measured faster there; the staged pipeline
+                    // streams long column ranges better)
+                    if (nrhs == 1 && i0 >= nt1 && nt1 <= kRt1MaxPivotTiles) {
+                        double* pb = pub + (dinv_off[s] / (T * T)) * T;
+                        const TileRange a = tile_range(i0, F.m, F.c, T);
+                        const TileRange b = tile_range(i0 + cnt - 1, F.m, F.c, T);
+                        fwd_update_rt1<TL>(s, a.start, b.start + b.size, F, pb, abort_flag, err,
+                                           amap_off, amap_row, amap_ent, Ls, xp,
+                                           front_vec(fv, fv_off, s, 1), fv);
+                        done = true;
+                    }
+                }
+                if (!done)
+                    fwd_tile_task<TL, TV, NQ>(tk, fronts, pub, abort_flag, err, fv_off, amap_off,
+                                              amap_row, amap_ent, dinv_off, Ls, Dinv, xp, fv, n,
+                                              nrhs);
+                // update tiles counted in; the front's last one counts the
+                // front in at its parent
+                if (i0 >= nt1) {
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        __threadfence();
+                        const int ntu = tiles_l(F.m - F.c, T);
+                        if (atomicAdd(udone + s, cnt) + cnt == ntu && F.parent >= 0) {
+                            __threadfence();
+                            atomicAdd(fdone + F.parent, 1);
+                        }
+                    }
                 }
             }
-            return;
         }
-        bwd_small_front<TL, TV>(small_list[b - wblocks], fronts, rows, Ls, xp, n, nrhs, msmall,
-                                msmall);
-        return;
+        __syncthreads();  // shared memory and s_item free for the next item
     }
-    __shared__ int s_task;
-    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
-    __syncthreads();
-    if (s_task >= ntk) {  // counter not cleared: refuse rather than read past the list
-        if (threadIdx.x == 0) atomicOr(err, 2);
-        return;
+}
+
+template <typename TL, typename TV, int NQ>
+__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
+    k_bwd_solve(const FrontDesc* __restrict__ fronts, const int4* __restrict__ items, int nitems,
+                int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
+                int* __restrict__ err, int* __restrict__ bdone, const int* __restrict__ btarget,
+                const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
+                int* __restrict__ gcount, TV* __restrict__ part,
+                const int64_t* __restrict__ dinv_off, const int* __restrict__ warp_list,
+                const int* __restrict__ warp_cnt, const int* __restrict__ rows,
+                const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
+                int n, int nrhs, int MR) {
+    __shared__ int s_item;
+    const FrontDeps deps{bdone, btarget, abort_flag, err};
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int k = s_item;
+        if (k >= nitems) return;
+        const int4 it = items[k];
+        if (it.x == SolveScheduleHost::kItemWarps) {
+            extern __shared__ __align__(16) unsigned char smem_raw[];
+            const WarpTasks wt{warp_list + it.w, warp_cnt[3 * it.y], warp_cnt[3 * it.y + 1],
+                               warp_cnt[3 * it.y + 2]};
+            const int w = threadIdx.x >> 5, t = it.z + w;
+            TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(MR, nrhs);
+            if (t < wt.count()) {
+                if (nrhs == 1)
+                    bwd_warp_task<TL, TV, 1>(wt, t, deps, fronts, rows, Ls, xp, n, nrhs, wbuf, MR);
+                else
+                    bwd_warp_task<TL, TV, kWarpSolveRhs>(wt, t, deps, fronts, rows, Ls, xp, n,
+                                                         nrhs, wbuf, MR);
+            }
+        } else if (it.x == SolveScheduleHost::kItemGather) {
+            // the update rows' partial sums need the ancestors' solution
+            const int2 tk = make_int2(it.y, it.z);
+            const int p = fronts[tk.x].parent;
+            if (p < 0 || cta_wait(bdone + p, btarget[p], abort_flag, err))
+                bwd_gather_task<TL, TV, NQ>(tk, fronts, rows, gather_nch, gather_off, gcount,
+                                            dinv_off, Ls, xp, part, n, nrhs);
+        } else {
+            // a pivot tile: its gathers (counted) waited for the ancestors
+            const int2 tk = make_int2(it.y, it.z);
+            bwd_chain_task<TL, TV, NQ>(tk, fronts, pub, abort_flag, err, gather_nch, gather_off,
+                                       gcount, part, dinv_off, Ls, Dinv, xp, n, nrhs);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(bdone + tk.x, 1);
+            }
+        }
+        __syncthreads();  // shared memory and s_item free for the next item
     }
-    if (s_task < ngather) {
-        bwd_gather_task<TL, TV, NQ>(gtasks[s_task], fronts, rows, gather_nch, gather_off, gcount,
-                                    dinv_off, Ls, xp, part, n, nrhs);
-        return;
-    }
-    bwd_chain_task<TL, TV, NQ>(tasks[s_task - ngather], fronts, pub, abort_flag, err, gather_nch,
-                               gather_off, gcount, part, dinv_off, Ls, Dinv, xp, n, nrhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1463,22 +1372,23 @@ void permute_scatter(const int* perm, const double* xp, double* x, int n, int nr
 // launch sequence
 // ---------------------------------------------------------------------------
 
-// the largest dynamic shared memory any launch of the level kernels asks for
+// rows of a small front's warp buffer (every level's largest small front)
+constexpr int kWarpBufRows = ((Plan::kSmallMaxRows + 31) / 32) * 32;
+
+// dynamic shared memory of a solve launch: the tile tasks' stages or the
+// eight warps' buffers, whichever is larger
 template <typename TL, typename TV>
-static int solve_smem_max() {
-    const int ms = Plan::kSmallMaxRows;
-    size_t m = level_smem_bytes<TL, TV>(kSolvePassRhs);
-    m = std::max(m, small_fwd_smem<TL, TV>(ms, kSolvePassRhs));
-    m = std::max(m, small_bwd_smem<TL, TV>(ms, ms, kSolvePassRhs));
-    m = std::max(m, 8 * (size_t)warp_buf_stride(ms, kWarpSolveRhs) * sizeof(TV));
-    return (int)m;
+static size_t solve_smem(int nrhs) {
+    size_t m = level_smem_bytes<TL, TV>(nrhs);
+    if (nrhs == 1) m = std::max(m, rt1_smem_bytes<TL>());
+    return std::max(m, 8 * (size_t)warp_buf_stride(kWarpBufRows, nrhs) * sizeof(TV));
 }
 
 template <typename TL, typename TV, int NQ>
 static void set_solve_attributes_nq() {
-    const int sm = solve_smem_max<TL, TV>();
-    cudaFuncSetAttribute(k_fwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(k_bwd_level<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const int sm = (int)solve_smem<TL, TV>(kSolvePassRhs);
+    cudaFuncSetAttribute(k_fwd_solve<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_bwd_solve<TL, TV, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
 template <typename TL, typename TV>
@@ -1493,87 +1403,49 @@ void init_solve_kernels() {
     set_solve_attributes<float, double>();
 }
 
-// rows of the largest small front of a level (its highest non-empty bucket):
-// sizes the shared memory of that level's small-front work
-static int level_msmall(const DevPlan& D, int l) {
-    int ms = Plan::small_limit[0];
-    for (int b = 0; b < kSmallBuckets; ++b)
-        if (D.h_small_ptr[l * kSmallBuckets + b + 1] > D.h_small_ptr[l * kSmallBuckets + b])
-            ms = Plan::small_limit[b];
-    return ms;
-}
-
-// One level of the solve: one launch per direction (see k_fwd_level).
-template <typename TL, typename TV, int NQ>
-static void solve_level(bool forward, const DevPlan& D, int l, const TL* Ls, const TL* Dinv,
-                        TV* xp, TV* fv, int nrhs, cudaStream_t st) {
-    const SolveSchedule& S = D.solve;
-    const int n = D.n;
-    const int sb = D.h_small_ptr[l * kSmallBuckets], se = D.h_small_ptr[(l + 1) * kSmallBuckets];
-    const int ns = se - sb;
-    const int nl = D.h_large_ptr[l + 1] - D.h_large_ptr[l];
-    const int msmall = level_msmall(D, l);
-    // small fronts as warp tasks (right-hand sides in passes of
-    // kWarpSolveRhs inside the task) up to kWarpPathMaxRhs, else a CTA each
-    static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 160 rows in shared memory");
-    const bool warp = nrhs <= kWarpPathMaxRhs;
-    WarpTasks wt{S.warp_list + sb, 0, 0, 0};
-    if (warp) {
-        wt.n1 = S.warp_cnt[3 * l];
-        wt.n2 = S.warp_cnt[3 * l + 1];
-        wt.n4 = S.warp_cnt[3 * l + 2];
-    }
-    const int nsm = warp ? 0 : ns;  // small fronts on a CTA each
-    // warp-task blocks: 8 warps each, at most 4 blocks per SM
-    const int wblocks = warp ? std::min((wt.count() + 7) / 8, 148 * 4) : 0;
-    size_t sm = 0;
-    if (warp && wt.count() > 0) sm = 8 * (size_t)warp_buf_stride(msmall, nrhs) * sizeof(TV);
-    if (nsm > 0)
-        sm = std::max(sm, forward ? small_fwd_smem<TL, TV>(msmall, nrhs)
-                                  : small_bwd_smem<TL, TV>(msmall, msmall, nrhs));
-    const std::vector<int>& beg = forward ? S.fwd_task_beg : S.bwd_task_beg;
-    const int t0 = beg[l], nt = beg[l + 1] - beg[l];
-    // tile tasks: registers straight from L with one right-hand side
-    const size_t tile_sm = std::max(level_smem_bytes<TL, TV>(nrhs),
-                                    (NQ == 1 && nrhs == 1) ? rt1_smem_bytes<TL>() : (size_t)0);
-    if (nt > 0) sm = std::max(sm, tile_sm);
-    int* counter = S.sync + 2 * l + (forward ? 0 : 1);
-    int* gcount = S.sync + 2 * D.nlevels;  // one per pivot tile of a large front
-    int* abort_flag = gcount + S.nflags;
-    const double bytes =
-        (S.small_elems[l] + (forward ? S.fwd_elems[l] : S.bwd_elems[l])) * sizeof(TL);
-    ProfScope ps(D.prof, nl > 0 ? KC_SOLVE_LARGE : KC_SOLVE_SMALL, st, 0, bytes);
-    if (forward) {
-        const int grid = nt + wblocks + nsm;
-        if (grid > 0)
-            k_fwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
-                D.fronts, S.tasks + t0, nt, counter, fv + D.fv_pub_off * nrhs, abort_flag, S.err,
-                D.fv_off, S.amap_off, S.amap_row, S.amap_ent, D.dinv_off, wt, wblocks,
-                D.small_list + sb, D.child, D.relmap, Ls, Dinv, xp, fv, n, nrhs, msmall);
-    } else {
-        TV* part = fv + D.fv_fronts * nrhs;
-        const int gb = S.gather_task_beg[l], ng = S.gather_task_beg[l + 1] - gb;
-        if (ng > 0) sm = std::max(sm, tile_sm);
-        const int grid = ng + nt + wblocks + nsm;
-        if (grid > 0)
-            k_bwd_level<TL, TV, NQ><<<grid, 256, sm, st>>>(
-                D.fronts, S.tasks + gb, ng, S.tasks + t0, nt, counter,
-                fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs, abort_flag, S.err,
-                S.gather_nch, S.gather_off, gcount, part, D.dinv_off, wt, wblocks,
-                D.small_list + sb, D.rows, Ls, Dinv, xp, n, nrhs, msmall);
-    }
-}
-
 template <typename TL, typename TV, int NQ>
 static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv,
                             int nrhs, cudaStream_t st) {
-    cudaMemsetAsync(D.solve.sync, 0, (size_t)D.solve.nsync * sizeof(int), st);
+    const SolveSchedule& S = D.solve;
+    static_assert(Plan::kSmallMaxRows <= 32 * 5, "the warp path holds 160 rows in shared memory");
+    // sync: the two ticket counters, the gathers' counts per pivot tile, the
+    // abort word, then per front the forward finished-children and
+    // finished-update-tile counts and the backward completions
+    int* counters = S.sync;
+    int* gcount = S.sync + 2;
+    int* abort_flag = gcount + S.nflags;
+    int* fdone = abort_flag + 1;
+    int* udone = fdone + S.nfronts;
+    int* bdone = udone + S.nfronts;
+    cudaMemsetAsync(S.sync, 0, (size_t)S.nsync * sizeof(int), st);
     // publication slots of the forward and backward pivot tiles: all-ones bits
     cudaMemsetAsync(fv + D.fv_pub_off * nrhs, 0xff,
-                    (size_t)2 * D.solve.nflags * kTile * nrhs * sizeof(TV), st);
-    for (int l = 0; l < D.nlevels; ++l) solve_level<TL, TV, NQ>(true, D, l, Ls, Dinv, xp, fv, nrhs, st);
-    for (int l = D.nlevels - 1; l >= 0; --l)
-        solve_level<TL, TV, NQ>(false, D, l, Ls, Dinv, xp, fv, nrhs, st);
+                    (size_t)2 * S.nflags * kTile * nrhs * sizeof(TV), st);
+    const size_t sm = solve_smem<TL, TV>(nrhs);
+    const int sms = D.num_sms > 0 ? D.num_sms : 148;
+    const int grid = sms * (NQ == 1 ? 4 : 2);  // the launch bounds' residency
+    double fbytes = 0, bbytes = 0;
+    for (int l = 0; l < D.nlevels; ++l) {
+        fbytes += (S.small_elems[l] + S.fwd_elems[l]) * sizeof(TL);
+        bbytes += (S.small_elems[l] + S.bwd_elems[l]) * sizeof(TL);
+    }
+    if (S.nfwd_items > 0) {
+        ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, fbytes);
+        k_fwd_solve<TL, TV, NQ><<<std::min(grid, S.nfwd_items), 256, sm, st>>>(
+            D.fronts, S.fwd_items, S.nfwd_items, counters, fv + D.fv_pub_off * nrhs, abort_flag,
+            S.err, fdone, udone, D.fv_off, S.amap_off, S.amap_row, S.amap_ent, D.dinv_off,
+            S.warp_list, S.warp_cnt_d, D.child, D.relmap, Ls, Dinv, xp, fv, D.n, nrhs,
+            kWarpBufRows);
+    }
+    if (S.nbwd_items > 0) {
+        ProfScope ps(D.prof, KC_SOLVE_LARGE, st, 0, bbytes);
+        k_bwd_solve<TL, TV, NQ><<<std::min(grid, S.nbwd_items), 256, sm, st>>>(
+            D.fronts, S.bwd_items, S.nbwd_items, counters + 1,
+            fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs, abort_flag, S.err, bdone,
+            S.bwd_target, S.gather_nch, S.gather_off, gcount, fv + D.fv_fronts * nrhs,
+            D.dinv_off, S.warp_list, S.warp_cnt_d, D.rows, Ls, Dinv, xp, D.n, nrhs,
+            kWarpBufRows);
+    }
 }
 
 template <typename TL, typename TV>
