@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling helpers: run only one arm of the step (for ncu launch lists)
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None)
+    ap.add_argument("--only-nrhs", type=int, default=1,
+                    help="right-hand sides of the --only step (uniform random columns)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-rhs64", action="store_true",
                     help="skip the 64-right-hand-side measurement")
@@ -472,6 +474,10 @@ def run_gpu_arm(args):
 
     if args.only:
         fn = step_fp32 if args.only == "fp32" else step_fp64
+        if args.only_nrhs > 1:
+            Bq = mg.rhs_uniform(n, seed=1, nrhs=args.only_nrhs)
+            db = torch.from_numpy(np.asfortranarray(Bq)).cuda().t().contiguous().t()
+            dx = torch.empty((args.only_nrhs, n), dtype=torch.float64, device="cuda").t()
         t, _ = timed(fn, args.steps, args.warmup)
         if rank == 0:
             print(json.dumps({"only": args.only, "ms_per_step": statistics.mean(t)}), flush=True)
