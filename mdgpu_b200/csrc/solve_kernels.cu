@@ -635,9 +635,12 @@ __device__ void fwd_group_front(int s, const FrontDesc& F, const FrontDeps& deps
                 dn = (TV)cn[j + 1];
                 ln = (r > j + 1 && r < m) ? (TV)cn[r] : TV(0);
             }
+            // several right-hand sides: one reciprocal per column
+            const TV rd = NQ > 1 ? TV(1) / d : TV(0);
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                const TV y = __shfl_sync(mask, v[q], j, W) / d;
+                const TV sv = __shfl_sync(mask, v[q], j, W);
+                const TV y = NQ > 1 ? sv * rd : sv / d;
                 if (r == j)
                     v[q] = y;
                 else if (r > j)
@@ -746,9 +749,10 @@ __device__ void fwd_warp_front_smem(int s, const FrontDesc& F, const FrontDeps& 
         for (int j = 0; j < c; ++j) {
             const TL* col = L + j * ldl;
             const TV d = (TV)col[j];
+            const TV rd = NQ > 1 ? TV(1) / d : TV(0);  // several right-hand sides
             TV y[NQ];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) y[q] = f[q * MR + j] / d;
+            for (int q = 0; q < NQ; ++q) y[q] = NQ > 1 ? f[q * MR + j] * rd : f[q * MR + j] / d;
             if (lane == (j & 31)) {
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
