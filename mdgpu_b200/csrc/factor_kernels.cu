@@ -391,11 +391,11 @@ __global__ void __launch_bounds__(256)
 // Factor diagonal tile k of front f in place and store its inverse (TB x TB,
 // column-major, zero above the diagonal) at Dk (potrf_tile_core on a copy in
 // shared memory; a partial tile (n < 64) is padded with the identity).
-// S, W: TB x (TB + 1).
+// S, W: TB x kPotrfLD.
 template <typename T, int TB>
 __device__ void potrf_diag_tile(const FrontDesc& f, int k, T* Ls, T* Dk, T* S, T* W,
                                 int* status) {
-    constexpr int LD = TB + 1;
+    constexpr int LD = kPotrfLD;
     const int tid = threadIdx.x, nt = blockDim.x;
     const TileRange tk = tile_range(k, f.m, f.c, TB);
     const int n = tk.size;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256)
                  int* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* S = reinterpret_cast<T*>(smem_raw);
-    T* W = S + TB * (TB + 1);
+    T* W = S + TB * kPotrfLD;
     const int s = list[blockIdx.x];
     const FrontDesc f = fronts[s];
     if (k >= tiles_l(f.c, TB)) return;
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(256)
     if (i == k + 1 && j == k + 1 && i < tiles_l(f.c, TB) && (jcap < 0 || i <= jcap)) {
         __syncthreads();
         potrf_diag_tile<T, TB>(f, i, Ls, Dinv + dinv_off[s] + (int64_t)i * TB * TB, As,
-                               As + TB * (TB + 1), status);
+                               As + TB * kPotrfLD, status);
     }
 }
 
@@ -548,11 +548,12 @@ __global__ void __launch_bounds__(256)
 constexpr int kAssembleWindow = 1024;
 constexpr size_t kAssembleColsSmemMax = 8 * kAssembleWindow * sizeof(double);
 
-// shared memory of the tile kernels: two 64 x 65 buffers (operands of the
-// tile products, or S and W of the diagonal-tile factorization)
+// shared memory of the tile kernels: two 64 x kPotrfLD buffers (operands of
+// the tile products in 64 x 65 of them, or S and W of the diagonal-tile
+// factorization)
 template <typename T>
 static size_t diag_smem() {
-    return (size_t)2 * kTile * (kTile + 1) * sizeof(T);
+    return (size_t)2 * kTile * kPotrfLD * sizeof(T);
 }
 
 template <typename T>

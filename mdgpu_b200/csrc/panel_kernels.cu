@@ -161,7 +161,7 @@ __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, in
 // block, which the diagonal factorization reuses as its S and W
 template <typename T>
 constexpr size_t panel_smem_bytes() {
-    return ((size_t)kPanel * kTile + 2 * (size_t)kTile * (kTile + 1)) * sizeof(T);
+    return ((size_t)kPanel * kTile + 2 * (size_t)kTile * kPotrfLD) * sizeof(T);
 }
 
 template <typename T>
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             const int64_t* __restrict__ dinv_off, T* __restrict__ Ls, T* __restrict__ Dinv,
             float* __restrict__ pscr, const int64_t* __restrict__ pscr_off, int split_mode,
             int* __restrict__ status) {
-    constexpr int TB = kTile, PT = kPanel / kTile, LDS = TB + 1;
+    constexpr int TB = kTile, PT = kPanel / kTile, LDS = kPotrfLD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* Xs = reinterpret_cast<T*>(smem_raw);  // row block: column q at Xs + q * TB
     T* Bs = Xs + (size_t)kPanel * TB;        // operand block; S and W of the factorization
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                     sd[a][b] = v;
                 }
             __syncthreads();  // the row block and S, W are reused below
-            double* S64 = reinterpret_cast<double*>(Xs);  // 2 TB (TB + 1) doubles fit in
+            double* S64 = reinterpret_cast<double*>(Xs);  // 2 TB kPotrfLD doubles fit in
             double* W64 = S64 + TB * LDS;                 // the row block + operand block
 #pragma unroll
             for (int a = 0; a < 4; ++a)
