@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <map>
+#include <set>
 #include <atomic>
 #include <cmath>
 #include <exception>
@@ -55,15 +56,10 @@ int64_t lifetime_alloc(const std::vector<int>& beg, const std::vector<int>& end,
             starts[beg[i]].push_back(i);
             ends[end[i]].push_back(i);
         }
-    std::map<int64_t, int64_t> by_off;        // free ranges: offset -> size
-    std::multimap<int64_t, int64_t> by_size;  // size -> offset
+    std::map<int64_t, int64_t> by_off;                 // free ranges: offset -> size
+    std::set<std::pair<int64_t, int64_t>> by_size;     // (size, offset)
     auto drop = [&](std::map<int64_t, int64_t>::iterator it) {
-        auto r = by_size.equal_range(it->second);
-        for (auto q = r.first; q != r.second; ++q)
-            if (q->second == it->first) {
-                by_size.erase(q);
-                break;
-            }
+        by_size.erase({it->second, it->first});
         by_off.erase(it);
     };
     int64_t top = 0, peak = 0;
@@ -89,7 +85,7 @@ int64_t lifetime_alloc(const std::vector<int>& beg, const std::vector<int>& end,
                     top = o;
                 } else {
                     by_off[o] = z;
-                    by_size.emplace(z, o);
+                    by_size.insert({z, o});
                 }
             }
         std::vector<int>& st = starts[l];
@@ -98,14 +94,16 @@ int64_t lifetime_alloc(const std::vector<int>& beg, const std::vector<int>& end,
         });
         for (int i : st) {
             const int64_t z = size[i];
-            auto fit = by_size.lower_bound(z);
+            // best fit: the smallest free range that holds it (lowest
+            // offset among equals)
+            auto fit = by_size.lower_bound({z, INT64_MIN});
             if (fit != by_size.end()) {
                 const int64_t o = fit->second, fz = fit->first;
                 drop(by_off.find(o));
                 off[i] = o;
                 if (fz > z) {
                     by_off[o + z] = fz - z;
-                    by_size.emplace(fz - z, o + z);
+                    by_size.insert({fz - z, o + z});
                 }
             } else {
                 off[i] = top;
