@@ -68,8 +68,10 @@ def parse():
     ap.add_argument("--side", type=int, default=64)
     ap.add_argument("--impl", default="mdgpu_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    # profiling helpers: run only one arm of the step (for ncu launch lists)
-    ap.add_argument("--only", choices=["fp32", "fp64"], default=None)
+    # profiling helper: only one arm of the step, timed and printed alone --
+    # with a small case (--side 48) for ncu captures of a few launches
+    ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
+                    help="run only this arm's step (use --side 48 or less under ncu)")
     ap.add_argument("--only-nrhs", type=int, default=1,
                     help="right-hand sides of the --only step (uniform random columns)")
     ap.add_argument("--no-e2e", action="store_true")
