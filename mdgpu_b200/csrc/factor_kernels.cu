@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(256)
                     for (int u = 0; u < 8; ++u) {
                         const int ic = ic0 + u * 32;
                         pr[u] = ic < ihi ? __ldg(rm + ic) : -1;
-                        v[u] = ic < ihi ? __ldcs(ucol + ic) : T(0);  // read once: streaming
+                        v[u] = ic < ihi ? __ldg(ucol + ic) : T(0);
                     }
 #pragma unroll
                     for (int u = 0; u < 8; ++u)
