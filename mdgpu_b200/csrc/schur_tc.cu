@@ -136,19 +136,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatil
     }
     return false;
 }
-// L2 policy for the panel operands: kept (evict last) -- every tile of a
-// row or column re-reads them while the trailing matrix streams past
-__device__ __forceinline__ uint64_t l2_evict_last() {
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int x, int y, uint64_t pol) {
+                                            int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        ".L2::cache_hint [%0], [%1, {%3, %4}], [%2], %5;" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "l"(pol)
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
         : "memory");
 }
 
@@ -304,7 +297,6 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
 
     if (warp < NLOAD_WARPS) {
         // ---- loader: TMA (warp 0, lane 0)
-        const uint64_t pol = tc::l2_evict_last();
         long long g = 0;  // chunk counter over this CTA's tiles
         long long issued = 0;
         bool ok = true;
@@ -325,11 +317,11 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                         // from mpad
                         tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
                         const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
-                        tc::tma_load_2d(a, map, &full_bar[st], col, ra, pol);
-                        tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb, pol);
+                        tc::tma_load_2d(a, map, &full_bar[st], col, ra);
+                        tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
                         if constexpr (!BF) {
-                            tc::tma_load_2d(a + 2 * OPER, map, &full_bar[st], col, mpad + ra, pol);
-                            tc::tma_load_2d(a + 3 * OPER, map, &full_bar[st], col, mpad + rb, pol);
+                            tc::tma_load_2d(a + 2 * OPER, map, &full_bar[st], col, mpad + ra);
+                            tc::tma_load_2d(a + 3 * OPER, map, &full_bar[st], col, mpad + rb);
                         }
                         issued = g + 1;
                     }
@@ -435,15 +427,14 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
             };
             // valid columns of this lane's row: [t.cbeg, chi)
             const int chi = row < f.m ? min(f.m, row + 1) : t.cbeg;
-            // old C values of a 32-column block into o (zeros outside); C is
-            // read and written once per launch: streaming (evict first)
+            // old C values of a 32-column block into o (zeros outside)
             auto load_block = [&](int c0, float (&o)[32]) {
                 float* p = start(c0);
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     const int col = c0 + q;
                     if (col == f.c) p = Urow;
-                    o[q] = (col >= t.cbeg && col < chi) ? __ldcs(p) : 0.f;
+                    o[q] = (col >= t.cbeg && col < chi) ? *p : 0.f;
                     p += col < f.c ? f.ldl : f.ldu;
                 }
             };
@@ -453,7 +444,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                 for (int q = 0; q < 32; ++q) {
                     const int col = c0 + q;
                     if (col == f.c) p = Urow;
-                    if (col >= t.cbeg && col < chi) __stcs(p, o[q] - v[q]);
+                    if (col >= t.cbeg && col < chi) *p = o[q] - v[q];
                     p += col < f.c ? f.ldl : f.ldu;
                 }
             };
