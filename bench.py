@@ -590,6 +590,27 @@ def run_gpu_arm(args):
         except Exception as e:  # noqa: BLE001
             gmres = {"error": str(e)[:300]}
 
+    # the one-product TF32 Schur update (MDGPU_TF32) + GMRES-IR: a cheaper
+    # factor against more preconditioned solves
+    tf32 = None
+    if not args.no_gmres:
+        def step_tf32_gmres():
+            S.factor(dAx, M.TF32, stream=sptr)
+            return S.gmres_ir_device(db, dx, tol=1e-14, maxit=10, stream=sptr)
+
+        try:
+            tt, (bet, itt, intt) = timed(step_tf32_gmres, max(1, min(args.steps, 3)), 1)
+            xt = dx.cpu().numpy()
+            tf32 = {"ms_per_step": allmax(statistics.mean(tt)),
+                    "backward_error": float(np.max(bet)),
+                    "backward_error_host": host_berr(xt), "forward_error": fwd_err(xt),
+                    "corrections": int(np.max(itt)), "gmres_steps": int(np.sum(intt)),
+                    "precision_used": int(S.info("precision_used")),
+                    "kernels": S.profile_step(step_tf32_gmres)["classes"],
+                    "note": "FP32 factor with one-product TF32 Schur updates + GMRES-IR"}
+        except Exception as e:  # noqa: BLE001
+            tf32 = {"error": str(e)[:300]}
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -622,6 +643,7 @@ def run_gpu_arm(args):
                 "d2h_bytes_per_step": int(b.nbytes)},
         "rhs64": rhs64,
         "gmres_ir": gmres,
+        "tf32_gmres_ir": tf32,
         "hbm_bytes": hbm,
         "gpu_launches": prof["launches_per_step"],
         "clocks": clocks,
@@ -929,6 +951,10 @@ def run_elasticity_arm(args):
         S.factor(dAx, M.FP32, stream=sptr)
         return S.gmres_ir_device(dB, dX, tol=1e-14, maxit=10, stream=sptr)
 
+    def step_tf32_gmres():
+        S.factor(dAx, M.TF32, stream=sptr)
+        return S.gmres_ir_device(dB, dX, tol=1e-14, maxit=10, stream=sptr)
+
     def step_ir():
         S.factor(dAx, M.FP32, stream=sptr)
         return S.refine_device(dB, dX, tol=1e-14, maxit=30, stream=sptr)
@@ -951,6 +977,8 @@ def run_elasticity_arm(args):
     prec_b = int(S.info("precision_used"))
     ms_g, (be_g, it_g, in_g) = timed(step_gmres, max(1, min(args.steps, 3)), 1)
     x_g = dX.cpu().numpy()
+    ms_t, (be_t, it_t, in_t) = timed(step_tf32_gmres, max(1, min(args.steps, 3)), 1)
+    x_t = dX.cpu().numpy()
     ms_ir, (be_ir, it_ir) = timed(step_ir, max(1, min(args.steps, 3)), 1)
     x_ir = dX.cpu().numpy()
     ms64, (be64, _) = timed(step64, max(1, min(args.steps, 3)), 1)
@@ -958,7 +986,7 @@ def run_elasticity_arm(args):
     # where the time goes: the factor alone per precision, and the kernel
     # classes of one step of each precision mode
     factor_ms = {}
-    for name, prec in (("bf16", M.BF16), ("fp32", M.FP32), ("fp64", M.FP64)):
+    for name, prec in (("bf16", M.BF16), ("tf32", M.TF32), ("fp32", M.FP32), ("fp64", M.FP64)):
         factor_ms[name], _ = timed(lambda: S.factor(dAx, prec, stream=sptr), 2, 1)
     kernels = {"bf16_gmres_ir": S.profile_step(step_bf16_gmres)["classes"],
                "fp32_gmres_ir": S.profile_step(step_gmres)["classes"]}
@@ -981,6 +1009,10 @@ def run_elasticity_arm(args):
             "forward_error": fwd(x_b), "corrections": int(np.max(it_b)),
             "gmres_steps": int(np.sum(in_b)),
             "precision_used": {0: "fp64", 1: "fp32 (bf16 fell back)", 2: "bf16"}[prec_b],
+            "tf32_gmres_ir": {"ms_per_step": ms_t, "backward_error": float(np.max(be_t)),
+                              "backward_error_host": host_berr(x_t), "forward_error": fwd(x_t),
+                              "corrections": int(np.max(it_t)),
+                              "gmres_steps": int(np.sum(in_t))},
             "fp32_gmres_ir": {"ms_per_step": ms_g, "backward_error": float(np.max(be_g)),
                               "backward_error_host": host_berr(x_g), "forward_error": fwd(x_g),
                               "corrections": int(np.max(it_g)),

@@ -45,10 +45,13 @@ enum mdgpu_precision {
     MDGPU_FP64 = 0, /* plain FP64 factor: the drop-in mode */
     MDGPU_FP32 = 1, /* FP32 factor; Schur updates of large fronts on the tensor cores in
                        3xTF32 (close to FP32 accuracy) */
-    MDGPU_BF16 = 2  /* FP32 factor whose large-front Schur updates take BF16 operands (one
+    MDGPU_BF16 = 2, /* FP32 factor whose large-front Schur updates take BF16 operands (one
                        tensor-core product, FP32 accumulation): for GMRES-IR
                        (mdgpu_gmres_ir); a factorization that meets a non-positive pivot is
                        redone in FP32 (mdgpu_info "bf16_fallbacks", "precision_used") */
+    MDGPU_TF32 = 3  /* FP32 factor whose large-front Schur updates are one TF32 tensor-core
+                       product (the operands' low 13 mantissa bits dropped): for GMRES-IR;
+                       redone in FP32 on a non-positive pivot as MDGPU_BF16 */
 };
 
 /*

@@ -15,7 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmdgpu_b200.so")
 
-FP64, FP32, BF16 = 0, 1, 2
+FP64, FP32, BF16, TF32 = 0, 1, 2, 3
 ORDER_NATURAL, ORDER_AMD = 0, 1
 TREE_NODAL, TREE_SUPER, TREE_RELAXED = 0, 1, 2
 

@@ -118,11 +118,11 @@ struct mdgpu_handle_s {
     int nrhs_cap = 0;
     // CUDA graphs of the numeric launch sequences (captured once, replayed)
     bool use_graphs = true;
-    cudaGraphExec_t fgraph[3] = {nullptr, nullptr, nullptr};  // per precision
+    cudaGraphExec_t fgraph[4] = {nullptr, nullptr, nullptr, nullptr};  // per precision
     std::map<int, cudaGraphExec_t> sgraph;  // key: precision * 1024 + rhs count
     int factored = -1;  // precision of the current factor, -1 none
     int fp64_diag_tiles = 0;  // of the last factor: diagonal tiles redone in FP64
-    int bf16_fallbacks = 0;   // BF16 factors redone in FP32 (non-positive pivot)
+    int bf16_fallbacks = 0;   // BF16 or 1xTF32 factors redone in FP32 (non-positive pivot)
     bool tuned = false;       // launch shapes chosen by mdgpu_autotune
     bool selinv_done = false;      // Z of the current FP64 factor in dZ64 / dZu64
     double* dZ64 = nullptr;        // selected inverse, laid out as the L panels
@@ -625,13 +625,13 @@ void ensure_solve_storage(mdgpu_handle_s* h, int nrhs) {
 
 int do_factor_once(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st);
 
-// MDGPU_BF16 whose factorization meets a non-positive pivot (BF16 rounding
-// of the Schur updates can destroy definiteness when cond(A) u_bf16 is near
-// 1) is factored again in FP32; precision_used records which factor the
-// handle holds.
+// MDGPU_BF16 or MDGPU_TF32 whose factorization meets a non-positive pivot
+// (the rounding of the Schur updates' operands can destroy definiteness when
+// cond(A) u is near 1) is factored again in FP32; precision_used records
+// which factor the handle holds.
 int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
     int rc = do_factor_once(h, dAx, precision, st);
-    if (rc == MDGPU_ERR_NOT_SPD && precision == MDGPU_BF16) {
+    if (rc == MDGPU_ERR_NOT_SPD && (precision == MDGPU_BF16 || precision == MDGPU_TF32)) {
         rc = do_factor_once(h, h->d_Ax, MDGPU_FP32, st);
         if (rc == MDGPU_OK) h->bf16_fallbacks++;
     }
@@ -640,7 +640,8 @@ int do_factor(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t 
 
 int do_factor_once(mdgpu_handle_s* h, const double* dAx, int precision, cudaStream_t st) {
     NvtxRange nvtx("mdgpu_factor");
-    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16)
+    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16 &&
+        precision != MDGPU_TF32)
         return fail(MDGPU_ERR_INVALID, "unknown precision");
     ck(cudaSetDevice(h->device), "cudaSetDevice");
     ensure_factor_storage(h, precision);
@@ -660,7 +661,9 @@ int do_factor_once(mdgpu_handle_s* h, const double* dAx, int precision, cudaStre
             factor_levels<double>(h->D, h->dL64, h->dU64, h->dD64, h->d_Ax, h->d_status, s);
         else
             factor_levels<float>(h->D, h->dL32, h->dU32, h->dD32, h->d_Ax, h->d_status, s,
-                                 precision == MDGPU_BF16);
+                                 precision == MDGPU_BF16   ? kSchurBF16
+                                 : precision == MDGPU_TF32 ? kSchur1xTF32
+                                                           : kSchur3xTF32);
     };
     if (h->use_graphs && !h->prof.on) {
         cudaGraphExec_t& g = h->fgraph[precision];
@@ -1659,7 +1662,8 @@ int mdgpu_grad_lower(mdgpu_handle h, const double* x, double* G, void* stream) {
 int mdgpu_autotune(mdgpu_handle h, const double* Ax, int precision, double* ms_best) {
     if (!h || !Ax) return fail(MDGPU_ERR_INVALID, "bad arguments");
     if (!h->on_device) return fail(MDGPU_ERR_NO_DEVICE, "no CUDA device");
-    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16)
+    if (precision != MDGPU_FP64 && precision != MDGPU_FP32 && precision != MDGPU_BF16 &&
+        precision != MDGPU_TF32)
         return fail(MDGPU_ERR_INVALID, "unknown precision");
     return guarded([&]() -> int {
         NvtxRange nvtx("mdgpu_autotune");

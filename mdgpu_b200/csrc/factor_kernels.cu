@@ -645,7 +645,7 @@ void launch_large_level(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv, cons
 // counter not cleared).
 template <typename T>
 static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us, T* Dinv,
-                                      const double* Ax, int* status, bool bf16,
+                                      const double* Ax, int* status, int smode,
                                       cudaStream_t st) {
     const DevSchedule& S = D.psched;
     const size_t gsm = diag_smem<T>();
@@ -689,14 +689,14 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 ProfScope ps(D.prof, KC_TRSM, st, op.flops, op.elems * sizeof(T));
                 // the panel scratch the tensor-core Schur update reads:
                 // the 3xTF32 hi/lo split (1) or the BF16 copy (2)
-                launch_panel<T>(D, op, Ls, Dinv, status, sizeof(T) == 4 ? (bf16 ? 2 : 1) : 0,
-                                st);
+                launch_panel<T>(D, op, Ls, Dinv, status,
+                                sizeof(T) == 4 ? (smode == kSchurBF16 ? 2 : 1) : 0, st);
                 break;
             }
             case OP_SCHUR_TC: {
                 ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
                 if constexpr (sizeof(T) == 4)
-                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, bf16, st);
+                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, smode, st);
                 else
                     launch_schur_f64(D, w, op.arg, kPanel, Ls, Us, st);
                 break;
@@ -733,7 +733,7 @@ void init_factor_kernels() {
 // records, so each class keeps its own time.
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
-                   cudaStream_t st, bool bf16) {
+                   cudaStream_t st, int smode) {
     const bool fork = D.aux && D.fork_ev && D.join_ev && !(D.prof && D.prof->on);
     if (D.fsync && D.nfsync > 0) cudaMemsetAsync(D.fsync, 0, (size_t)D.nfsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
@@ -751,8 +751,8 @@ void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, in
         }
         // FP32 needs the TMA descriptors of the tensor-core path; without them
         // (descriptor encoding unavailable) it keeps the 64-wide tile schedule
-        if (sizeof(T) == 8 || (bf16 ? D.tmaps_bf16 != nullptr : D.tmaps != nullptr))
-            launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, bf16, st);
+        if (sizeof(T) == 8 || (smode == kSchurBF16 ? D.tmaps_bf16 != nullptr : D.tmaps != nullptr))
+            launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, smode, st);
         else
             launch_large_level<T>(D, l, Ls, Us, Dinv, Ax, status, st);
         if (par) cudaStreamWaitEvent(st, D.join_ev, 0);
@@ -760,8 +760,8 @@ void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, in
 }
 
 template void factor_levels<double>(const DevPlan&, double*, double*, double*, const double*,
-                                    int*, cudaStream_t, bool);
+                                    int*, cudaStream_t, int);
 template void factor_levels<float>(const DevPlan&, float*, float*, float*, const double*, int*,
-                                   cudaStream_t, bool);
+                                   cudaStream_t, int);
 
 }  // namespace mdgpu

@@ -241,13 +241,18 @@ void init_selinv();
 // panel scratch rows of a large front (m rounded up to the 128-row tile)
 __host__ __device__ inline int panel_mpad(int m) { return (m + 127) & ~127; }
 
-// bf16 (T = float only): the large fronts' Schur updates take BF16 operands
-// (the MDGPU_BF16 factor); else 3xTF32 (float) or FP64 (double).  status:
-// [0] smallest failing pivot column, [1] device wait error code, [3] count
-// of diagonal tiles refactored in FP64 (weak FP32 pivots)
+// Schur-update modes of an FP32 factor's large fronts on the tensor cores:
+// 3xTF32 (close to FP32 accuracy, MDGPU_FP32), BF16 operands (MDGPU_BF16),
+// one TF32 product (MDGPU_TF32)
+enum SchurMode { kSchur3xTF32 = 0, kSchurBF16 = 1, kSchur1xTF32 = 2 };
+
+// smode (T = float only): the SchurMode of the large fronts' updates (FP64
+// for T = double).  status: [0] smallest failing pivot column, [1] device
+// wait error code, [3] count of diagonal tiles refactored in FP64 (weak FP32
+// pivots)
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
-                   cudaStream_t st, bool bf16 = false);
+                   cudaStream_t st, int smode = kSchur3xTF32);
 
 // Solves with the factor L (scalar TL) on vectors of type TV.  xp holds the
 // permuted right-hand sides on entry (n x nrhs, ld n) and the permuted
@@ -256,10 +261,10 @@ template <typename TL, typename TV>
 void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv, int nrhs,
                   cudaStream_t st);
 
-// bf16: per large front a map over its FP32 L panel (m x c), boxes of 64
-// columns without swizzle (the BF16 Schur update); else over its split
-// panel scratch (2 mpad x kPanel, base scr + scr_off[s]), boxes of 16 columns
-// with the 128-byte / 32-byte-atom swizzle (3xTF32)
+// Per large front a map over its panel scratch (base scr + scr_off[s],
+// row-major, kPanel columns): bf16, the BF16 copy (mpad rows); else the
+// TF32 hi/lo split (2 mpad rows); boxes of 128 bytes x 128 rows, 128-byte
+// swizzle
 int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t>& scr_off,
                      std::vector<CUtensorMap>& maps, std::vector<int>& idx, bool bf16);
 // one panel launch (OP_PANEL): every row-tile task of the panel's fronts
@@ -268,7 +273,7 @@ template <typename T>
 void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, int split_mode,
                   cudaStream_t st);
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, bool bf16, cudaStream_t st);
+                     float* Us, int* err, int mode, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,
                       double* Us, cudaStream_t st);
 

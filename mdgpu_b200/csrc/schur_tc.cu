@@ -77,15 +77,16 @@ constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators
 // (BF16), 16 KB each, as the panel kernel wrote them.  One TMA warp, one MMA
 // warp, eight epilogue warps (two per 32 TMEM lanes, two 32-column blocks
 // each); one CTA per SM.
-template <bool BF>
+template <int MODE>
 struct Cfg {
+    static constexpr bool BF = MODE == kSchurBF16;
     static constexpr int BK = BF ? 64 : 32;       // K columns per chunk
     static constexpr int ESZ = BF ? 2 : 4;        // operand element bytes
     static constexpr int OPER = BM * BK * ESZ;    // bytes of one operand chunk (16 KB)
-    static constexpr int NOPER = BF ? 2 : 4;
+    static constexpr int NOPER = MODE == kSchur3xTF32 ? 4 : 2;
     static constexpr int STAGE_TMA = NOPER * OPER;
     static constexpr int STAGE_BYTES = STAGE_TMA;
-    static constexpr int STAGES = BF ? 6 : 3;     // 192 KB of stages either way
+    static constexpr int STAGES = NOPER == 4 ? 3 : 6;  // 192 KB of stages either way
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
     static constexpr int NLOAD = 1;
     static constexpr int MMA_WARP = NLOAD;
@@ -247,14 +248,14 @@ __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts
 // items/before: one entry per large front (its tile count); ntiles: the
 // launch's total.  maps: per large front a tensor map over its FP32 L panel
 // (rows x pivot columns).
-template <bool BF>
-__global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_SM)
+template <int MODE>
+__global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_PER_SM)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int ntiles,
                const int* __restrict__ tmap_idx, const CUtensorMap* __restrict__ maps, int panel,
                int PW, float* __restrict__ Ls, float* __restrict__ Us, int* __restrict__ err) {
     using namespace tc;
-    using C = Cfg<BF>;
+    using C = Cfg<MODE>;
     constexpr int BK = C::BK, STAGES = C::STAGES, OPER = C::OPER, STAGE_TMA = C::STAGE_TMA,
                   STAGE_BYTES = C::STAGE_BYTES, NLOAD_WARPS = C::NLOAD,
                   MMA_WARP = C::MMA_WARP;
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                         const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
                         tc::tma_load_2d(a, map, &full_bar[st], col, ra);
                         tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
-                        if constexpr (!BF) {
+                        if constexpr (MODE == kSchur3xTF32) {
                             tc::tma_load_2d(a + 2 * OPER, map, &full_bar[st], col, mpad + ra);
                             tc::tma_load_2d(a + 3 * OPER, map, &full_bar[st], col, mpad + rb);
                         }
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    if constexpr (!BF) {
+                    if constexpr (MODE == kSchur3xTF32) {
                         const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
                         const uint32_t bh = ah + OPER;
                         const uint32_t al = ah + 2 * OPER, bl = bh + 2 * OPER;
@@ -376,6 +377,15 @@ __global__ void __launch_bounds__(tc::Cfg<BF>::NTHREADS, tc::Cfg<BF>::CTAS_PER_S
                             tc::mma_tf32(d, tc::make_desc_kmajor(ah + o),
                                          tc::make_desc_kmajor(bh + o), 1u);
                         }
+                    } else if constexpr (MODE == kSchur1xTF32) {
+                        // hi hi' only: one TF32 product
+                        const uint32_t ah = tc::smem_u32(smem + st * STAGE_BYTES);
+                        const uint32_t bh = ah + OPER;
+#pragma unroll
+                        for (int k = 0; k < BK / 8; ++k)
+                            tc::mma_tf32(d, tc::make_desc_kmajor(ah + k * 32),
+                                         tc::make_desc_kmajor(bh + k * 32),
+                                         (ch > 0 || k > 0) ? 1u : 0u);
                     } else {
                         const uint32_t ab = tc::smem_u32(smem + st * STAGE_BYTES);
                         const uint32_t bb = ab + OPER;
@@ -517,7 +527,8 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
         const int esz = bf16 ? 2 : 4;
         cuuint64_t dims[2] = {(cuuint64_t)kPanel, (cuuint64_t)(bf16 ? mpad : 2 * mpad)};
         cuuint64_t strides[1] = {(cuuint64_t)kPanel * esz};
-        cuuint32_t box[2] = {(cuuint32_t)(bf16 ? tc::Cfg<true>::BK : tc::Cfg<false>::BK),
+        cuuint32_t box[2] = {(cuuint32_t)(bf16 ? tc::Cfg<kSchurBF16>::BK
+                                               : tc::Cfg<kSchur3xTF32>::BK),
                              (cuuint32_t)tc::BM};
         cuuint32_t estr[2] = {1, 1};
         void* ptr = const_cast<float*>(base + scr_off[s]);
@@ -532,25 +543,32 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
 }
 
 void init_schur_tc() {
-    cudaFuncSetAttribute(k_schur_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         tc::Cfg<false>::SMEM_BYTES);
-    cudaFuncSetAttribute(k_schur_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         tc::Cfg<true>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_schur_tc<kSchur3xTF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<kSchur3xTF32>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_schur_tc<kSchurBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<kSchurBF16>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_schur_tc<kSchur1xTF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         tc::Cfg<kSchur1xTF32>::SMEM_BYTES);
+}
+
+template <int MODE>
+static void launch_schur_mode(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
+                              float* Us, int* err, const CUtensorMap* maps, cudaStream_t st) {
+    using C = tc::Cfg<MODE>;
+    const int sms = D.num_sms > 0 ? D.num_sms : 148;
+    k_schur_tc<MODE><<<std::min(w.nctas, sms * C::CTAS_PER_SM), C::NTHREADS, C::SMEM_BYTES, st>>>(
+        D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas, D.tmap_idx,
+        maps, panel, PW, Ls, Us, err);
 }
 
 void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, bool bf16, cudaStream_t st) {
-    const int sms = D.num_sms > 0 ? D.num_sms : 148;
-    if (bf16)
-        k_schur_tc<true><<<std::min(w.nctas, sms * tc::Cfg<true>::CTAS_PER_SM),
-                           tc::Cfg<true>::NTHREADS, tc::Cfg<true>::SMEM_BYTES, st>>>(
-            D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
-            D.tmap_idx, D.tmaps_bf16, panel, PW, Ls, Us, err);
+                     float* Us, int* err, int mode, cudaStream_t st) {
+    if (mode == kSchurBF16)
+        launch_schur_mode<kSchurBF16>(D, w, panel, PW, Ls, Us, err, D.tmaps_bf16, st);
+    else if (mode == kSchur1xTF32)
+        launch_schur_mode<kSchur1xTF32>(D, w, panel, PW, Ls, Us, err, D.tmaps, st);
     else
-        k_schur_tc<false><<<std::min(w.nctas, sms * tc::Cfg<false>::CTAS_PER_SM),
-                            tc::Cfg<false>::NTHREADS, tc::Cfg<false>::SMEM_BYTES, st>>>(
-            D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas,
-            D.tmap_idx, D.tmaps, panel, PW, Ls, Us, err);
+        launch_schur_mode<kSchur3xTF32>(D, w, panel, PW, Ls, Us, err, D.tmaps, st);
 }
 
 }  // namespace mdgpu
