@@ -318,7 +318,7 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
             for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) {
                 const int s = P.large_list[q];
                 h->pscr_off[s] = off;
-                off += 2 * (int64_t)panel_mpad(P.fronts[s].m) * kPanel;
+                off += 2 * (int64_t)panel_mpad(P.fronts[s].m) * kScrCols;
             }
             D.pscr_total = std::max(D.pscr_total, off);
         }

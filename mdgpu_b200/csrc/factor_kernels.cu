@@ -694,11 +694,21 @@ static void launch_large_level_panels(const DevPlan& D, int level, T* Ls, T* Us,
                 break;
             }
             case OP_SCHUR_TC: {
-                ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
-                if constexpr (sizeof(T) == 4)
-                    launch_schur_tc(D, w, op.arg, kPanel, Ls, Us, status + 1, smode, st);
-                else
+                // one update per panel: the FP64 factor's (the tensor-core
+                // path runs the deferred updates below instead)
+                if constexpr (sizeof(T) == 8) {
+                    ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
                     launch_schur_f64(D, w, op.arg, kPanel, Ls, Us, st);
+                }
+                break;
+            }
+            case OP_SCHUR_NEXT:
+            case OP_SCHUR_REST: {
+                if constexpr (sizeof(T) == 4) {
+                    ProfScope ps(D.prof, KC_SCHUR, st, op.flops, op.elems * sizeof(T));
+                    launch_schur_tc(D, w, op.arg, kPanel, op.arg2, op.kind == OP_SCHUR_NEXT, Ls,
+                                    Us, status + 1, smode, st);
+                }
                 break;
             }
         }

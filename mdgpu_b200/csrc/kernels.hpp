@@ -75,7 +75,8 @@ struct ProfScope {
     }
 };
 constexpr int kTile = 64;          // tile of the large-front factor and solve kernels
-constexpr int kPanel = 256;        // FP32 path: pivot columns per tensor-core Schur update
+constexpr int kPanel = 256;        // pivot columns per panel of the large fronts
+constexpr int kScrCols = 2 * kPanel;  // panel scratch row: panels of even and odd index
 
 // A work-list schedule resident on the device (items/before arrays) with the
 // host copy of the per-launch descriptors.
@@ -195,11 +196,13 @@ struct DevPlan {
     // operands of the tensor-core Schur updates)
     CUtensorMap* tmaps = nullptr;
     CUtensorMap* tmaps_bf16 = nullptr;  // over the same scratch as BF16, for the BF16 Schur update
-    // FP32 (3xTF32) path: the current panel of every large front of a level,
-    // split: per front 2 mpad x kPanel floats (column kk: rows [0, mpad) the
-    // TF32 part hi, rows [mpad, 2 mpad) lo = x - hi), mpad = m rounded up to
-    // 128; written by the panel kernel, read by the tensor-core Schur update
-    // through tmaps (fronts of a level side by side, levels reuse it)
+    // FP32 tensor-core path: the last two panels of every large front of a
+    // level (panel q at columns (q mod 2) kPanel of a kScrCols-wide row),
+    // row-major, split: per front 2 mpad rows of kScrCols floats (rows [0,
+    // mpad) the TF32 parts hi, rows [mpad, 2 mpad) lo = x - hi; or mpad rows
+    // of BF16 values), mpad = m rounded up to 128; written by the panel
+    // kernel, read by the tensor-core Schur update through tmaps (fronts of
+    // a level side by side, levels reuse it)
     float* pscr = nullptr;
     int64_t* pscr_off = nullptr;  // per supernode (-1 if small)
     int64_t pscr_total = 0;
@@ -272,8 +275,10 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
 template <typename T>
 void launch_panel(const DevPlan& D, const PanelOp& op, T* Ls, T* Dinv, int* status, int split_mode,
                   cudaStream_t st);
-void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, int mode, cudaStream_t st);
+// the update after panel `panel` with the npan panels ending there; strip:
+// only the next panel's two tile columns (see PanelOpKind)
+void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, int npan,
+                     bool strip, float* Ls, float* Us, int* err, int mode, cudaStream_t st);
 void launch_schur_f64(const DevPlan& D, const WorkList& w, int panel, int PW, double* Ls,
                       double* Us, cudaStream_t st);
 

@@ -120,8 +120,9 @@ __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl,
 // The task's rows of the finished panel (read back from the L store, which
 // this CTA wrote: zeros above the diagonal and past the last pivot column)
 // into the panel scratch for the tensor-core Schur update, row-major (a
-// row's kPanel columns contiguous: the K-major operand layout), all kPanel
-// columns (zeros past the last pivot column):
+// kScrCols-wide row, this panel's kPanel columns from column kofs: the
+// K-major operand layout), all kPanel columns (zeros past the last pivot
+// column):
 //   mode 1 (3xTF32): hi = x with the low 13 mantissa bits cleared, lo =
 //          x - hi; hi rows from the front's base, lo rows mpad further;
 //   mode 2 (BF16): x rounded to BF16 (nearest even), one copy.
@@ -129,7 +130,7 @@ __device__ __forceinline__ void pn_write_block(const T* Xk, T* dst, int64_t ldl,
 // down columns and the writes along rows.  ps: the front's scratch base;
 // row0: the task's first row.
 __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, int nrows,
-                                              int ncols, float* ps, int row0, int mpad,
+                                              int ncols, float* ps, int row0, int kofs, int mpad,
                                               int mode, float* buf) {
     for (int cb = 0; cb < kPanel; cb += 32) {
         __syncthreads();  // buf free
@@ -143,13 +144,13 @@ __device__ __forceinline__ void pn_split_rows(const float* rowp, int64_t ldl, in
             const int r = idx >> 5, q = idx & 31;
             if (r >= nrows) continue;
             const float x = buf[r * 33 + q];
-            const int64_t e = (int64_t)(row0 + r) * kPanel + cb + q;
+            const int64_t e = (int64_t)(row0 + r) * kScrCols + kofs + cb + q;
             if (mode == 2) {
                 reinterpret_cast<__nv_bfloat16*>(ps)[e] = __float2bfloat16_rn(x);
             } else {
                 const float h = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
                 ps[e] = h;
-                ps[e + (int64_t)mpad * kPanel] = x - h;
+                ps[e + (int64_t)mpad * kScrCols] = x - h;
             }
         }
     }
@@ -286,7 +287,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     const int pcols = min(kPanel, f.c - col0);
     if (!diag) {
         if constexpr (sizeof(T) == 4)
-            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, mpad, split_mode, Bs);
+            if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, (panel & 1) * kPanel, mpad,
+                              split_mode, Bs);
         return;
     }
 
@@ -368,7 +370,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (tid == 0) pn_st_release(flags + tile0 + i, 1);
     // the split for the Schur update, after the flag: off the panel's chain
     if constexpr (sizeof(T) == 4)
-        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, mpad, split_mode, Bs);
+        if (ps) pn_split_rows(rowp, f.ldl, ti.size, pcols, ps, ti.start, (panel & 1) * kPanel, mpad,
+                              split_mode, Bs);
 }
 
 template <typename T>

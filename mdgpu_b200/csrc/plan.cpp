@@ -745,6 +745,40 @@ void build_panel_schedule(const Plan& P, int T, int PW, int CB, PanelSchedule& S
                 }
             }
             if (!big.empty()) S.ops.push_back({OP_SCHUR_TC, p, 0, S.store.add(big, p), sfl, sel, 0});
+            // the tensor-core path's deferred updates (see PanelOpKind)
+            std::vector<std::pair<int, int>> nxt, rest;
+            double nfl = 0, nel = 0, rfl = 0, rel = 0;
+            for (int s : fr) {
+                const FrontDesc& f = P.fronts[s];
+                const int k0 = p * PW;
+                if (k0 >= f.c) continue;
+                const int cbeg = std::min(k0 + PW, f.c);
+                if (cbeg >= f.m) continue;
+                const int NB = (f.m + 127) / 128, J0 = cbeg / 128, nb = NB - J0;
+                const double tr = f.m - cbeg;
+                const bool hasnext = cbeg < f.c;
+                if (p % 2 == 0 && hasnext) {
+                    // the next panel's columns [cbeg, min(cbeg + 256, c)): two
+                    // tile columns
+                    const double K = std::min(PW, f.c - k0);
+                    const double w = std::min(PW, f.c - cbeg);
+                    const double area = w * tr - w * (w - 1) / 2;
+                    nxt.push_back({s, nb + std::max(nb - 1, 0)});
+                    nfl += 2.0 * K * area;
+                    nel += K * (tr + w) + 2.0 * area;
+                } else {
+                    const int np = p % 2 == 1 ? 2 : 1;
+                    const double K = std::min(np * PW, f.c - (p - np + 1) * PW);
+                    rest.push_back({s, nb * (nb + 1) / 2});
+                    rfl += K * tr * (tr + 1);
+                    rel += K * tr + tr * (tr + 1);
+                }
+            }
+            if (!nxt.empty())
+                S.ops.push_back({OP_SCHUR_NEXT, p, 1, S.store.add(nxt, p), nfl, nel, 0});
+            if (!rest.empty())
+                S.ops.push_back({OP_SCHUR_REST, p, p % 2 == 1 ? 2 : 1, S.store.add(rest, p), rfl,
+                                 rel, 0});
         }
     }
     S.op_beg[P.nlevels] = (int)S.ops.size();

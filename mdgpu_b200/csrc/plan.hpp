@@ -160,13 +160,30 @@ struct TileSchedule {
 
 // Panel schedule of the large fronts: per level, operations in launch order:
 // the assembly, then per 256-column panel one panel factorization (OP_PANEL)
-// and one Schur update of the trailing part (OP_SCHUR_TC).  OP_POTRF,
-// OP_TRSM and OP_UPDATE_PANEL are the 64-wide steps of the tile schedule.
-enum PanelOpKind { OP_ASSEMBLE = 0, OP_POTRF, OP_TRSM, OP_UPDATE_PANEL, OP_SCHUR_TC, OP_PANEL };
+// and the Schur updates after it.  FP64 factors run one update of the whole
+// trailing part per panel (OP_SCHUR_TC).  The tensor-core FP32 factors defer
+// the bulk of it to every second panel, so the trailing matrix is read and
+// written once per two panels: after an even panel p, OP_SCHUR_NEXT updates
+// only the next panel's columns (two 128-column tiles) of the fronts that
+// have panel p + 1, and OP_SCHUR_REST (arg2 = 1) the whole trailing part of
+// the fronts that do not; after an odd panel p, OP_SCHUR_REST (arg2 = 2)
+// updates the trailing part after panel p with panels p - 1 and p together
+// (K = 512).  OP_POTRF, OP_TRSM and OP_UPDATE_PANEL are the 64-wide steps of
+// the tile schedule.
+enum PanelOpKind {
+    OP_ASSEMBLE = 0,
+    OP_POTRF,
+    OP_TRSM,
+    OP_UPDATE_PANEL,
+    OP_SCHUR_TC,
+    OP_PANEL,
+    OP_SCHUR_NEXT,
+    OP_SCHUR_REST
+};
 struct PanelOp {
     int kind;
-    int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_TC, PANEL)
-    int arg2;     // UPDATE_PANEL: last tile index of the panel
+    int arg;      // tile step k (POTRF/TRSM/UPDATE_PANEL) or panel index (SCHUR_*, PANEL)
+    int arg2;     // UPDATE_PANEL: last tile index of the panel; SCHUR_REST: panels (1, 2)
     WorkList w;
     double flops;  // algorithmic flops of the launch
     double elems;  // algorithmic factor-scalar traffic (elements read + written)

@@ -220,23 +220,46 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // Tile number b of the launch -> front s and tile (I, J); the CTAs of a front
 // enumerate the lower 128-tiles (I, J) with J >= J0 = cbeg / 128 row by row.
+// The launch's update (upd = npan | strip << 4): the trailing part after
+// panel `panel` (columns from cbeg = (panel + 1) PW) takes the products of
+// the npan panels ending at `panel` (K = npan PW pivot columns from k0, read
+// from scratch column kofs: panel q sits at column (q mod 2) PW); strip: only
+// the two tile columns of the next panel, else the whole lower trailing part.
 struct TileJob {
-    int s, I, J, nk, k0, cbeg;
+    int s, I, J, nk, k0, kofs, cbeg, cend;  // columns [cbeg, cend) are updated
 };
 __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts,
                                             const int* __restrict__ items,
                                             const int* __restrict__ before, int nitems, int b,
-                                            int panel, int PW, int BK) {
+                                            int panel, int PW, int BK, int upd) {
     TileJob t;
     const int it = find_item(before, nitems, b);
     t.s = items[it];
     const FrontDesc f = fronts[t.s];
-    t.k0 = panel * PW;
-    const int K = min(PW, f.c - t.k0);
-    t.cbeg = min(t.k0 + PW, f.c);
+    const int npan = upd & 15;
+    const int pf = panel - npan + 1;  // first panel of the update
+    t.k0 = pf * PW;
+    t.kofs = (pf & 1) * PW;
+    const int K = min(npan * PW, f.c - t.k0);
+    t.cbeg = min((panel + 1) * PW, f.c);
+    // a strip stops at the next panel's end (the columns after it take this
+    // panel's product with the next one's, in the following update)
+    t.cend = (upd >> 4) ? min((panel + 2) * PW, f.c) : f.m;
     const int J0 = t.cbeg / BM;
     int ii, jj;
-    lower_index(b - before[it], ii, jj);
+    const int q = b - before[it];
+    if (upd >> 4) {  // strip: column J0 (rows J0 ..), then column J0 + 1
+        const int nb = (f.m + BM - 1) / BM - J0;
+        if (q < nb) {
+            ii = q;
+            jj = 0;
+        } else {
+            ii = q - nb + 1;
+            jj = 1;
+        }
+    } else {
+        lower_index(q, ii, jj);
+    }
     t.I = J0 + ii;
     t.J = J0 + jj;
     t.nk = (K + BK - 1) / BK;
@@ -246,14 +269,15 @@ __device__ __forceinline__ TileJob tile_job(const FrontDesc* __restrict__ fronts
 }  // namespace tc
 
 // items/before: one entry per large front (its tile count); ntiles: the
-// launch's total.  maps: per large front a tensor map over its FP32 L panel
-// (rows x pivot columns).
+// launch's total.  maps: per large front a tensor map over its panel scratch
+// (two panels side by side); upd: the update's shape (tile_job).
 template <int MODE>
 __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_PER_SM)
     k_schur_tc(const FrontDesc* __restrict__ fronts, const int* __restrict__ items,
                const int* __restrict__ before, int nitems, int ntiles,
                const int* __restrict__ tmap_idx, const CUtensorMap* __restrict__ maps, int panel,
-               int PW, float* __restrict__ Ls, float* __restrict__ Us, int* __restrict__ err) {
+               int PW, int upd, float* __restrict__ Ls, float* __restrict__ Us,
+               int* __restrict__ err) {
     using namespace tc;
     using C = Cfg<MODE>;
     constexpr int BK = C::BK, STAGES = C::STAGES, OPER = C::OPER, STAGE_TMA = C::STAGE_TMA,
@@ -302,7 +326,7 @@ __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_P
         long long issued = 0;
         bool ok = true;
         for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
-            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK, upd);
             const CUtensorMap* map = maps + tmap_idx[t.s];
             const int mpad = panel_mpad(fronts[t.s].m);
             for (int ch = 0; ch < t.nk; ++ch, ++g) {
@@ -317,7 +341,7 @@ __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_P
                         // 128 rows per box; 3xTF32: hi rows, then lo rows
                         // from mpad
                         tc::mbar_expect_tx(&full_bar[st], STAGE_TMA);
-                        const int col = ch * BK, ra = t.I * BM, rb = t.J * BN;
+                        const int col = t.kofs + ch * BK, ra = t.I * BM, rb = t.J * BN;
                         tc::tma_load_2d(a, map, &full_bar[st], col, ra);
                         tc::tma_load_2d(a + OPER, map, &full_bar[st], col, rb);
                         if constexpr (MODE == kSchur3xTF32) {
@@ -346,7 +370,7 @@ __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_P
             int tl = 0;  // tiles of this CTA
             bool ok = true, any = false;
             for (int b = blockIdx.x; b < ntiles && ok; b += gridDim.x, ++tl) {
-                const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
+                const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK, upd);
                 const int acc = tl & 1;
                 const uint32_t use_acc = (uint32_t)(tl >> 1);
                 if (use_acc > 0 && !tc::mbar_wait(&acce_bar[acc], (use_acc - 1) & 1, &abort_sh)) {
@@ -423,7 +447,7 @@ __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_P
         const int cb0 = ((warp - MMA_WARP - 1) >> 2) * NCB;
         int tl = 0;
         for (int b = blockIdx.x; b < ntiles; b += gridDim.x, ++tl) {
-            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK);
+            const TileJob t = tile_job(fronts, items, before, nitems, b, panel, PW, BK, upd);
             const FrontDesc f = fronts[t.s];
             const int acc = tl & 1;
             const int row = t.I * BM + quarter * 32 + lane;
@@ -436,7 +460,7 @@ __global__ void __launch_bounds__(tc::Cfg<MODE>::NTHREADS, tc::Cfg<MODE>::CTAS_P
                 return c0 < f.c ? Lrow + (int64_t)c0 * f.ldl : Urow + (int64_t)(c0 - f.c) * f.ldu;
             };
             // valid columns of this lane's row: [t.cbeg, chi)
-            const int chi = row < f.m ? min(f.m, row + 1) : t.cbeg;
+            const int chi = row < f.m ? min(t.cend, row + 1) : t.cbeg;
             // old C values of a 32-column block into o (zeros outside)
             auto load_block = [&](int c0, float (&o)[32]) {
                 float* p = start(c0);
@@ -508,8 +532,9 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// One tensor map per large front, over its panel scratch (row-major: kPanel
-// columns, the inner dimension, of 1 KB (3xTF32) or 512 B (BF16) per row):
+// One tensor map per large front, over its panel scratch (row-major: kScrCols
+// columns -- two panels side by side -- the inner dimension, of 2 KB (TF32)
+// or 1 KB (BF16) per row):
 // 3xTF32, FP32 values, 2 mpad rows (hi then lo); BF16, BF16 values, mpad
 // rows.  Boxes of 128 bytes of columns x 128 rows with the 128-byte swizzle;
 // reads past the rows return zeros.
@@ -525,8 +550,8 @@ int build_panel_maps(const Plan& P, const float* base, const std::vector<int64_t
         idx[s] = (int)q;
         const int mpad = panel_mpad(f.m);
         const int esz = bf16 ? 2 : 4;
-        cuuint64_t dims[2] = {(cuuint64_t)kPanel, (cuuint64_t)(bf16 ? mpad : 2 * mpad)};
-        cuuint64_t strides[1] = {(cuuint64_t)kPanel * esz};
+        cuuint64_t dims[2] = {(cuuint64_t)kScrCols, (cuuint64_t)(bf16 ? mpad : 2 * mpad)};
+        cuuint64_t strides[1] = {(cuuint64_t)kScrCols * esz};
         cuuint32_t box[2] = {(cuuint32_t)(bf16 ? tc::Cfg<kSchurBF16>::BK
                                                : tc::Cfg<kSchur3xTF32>::BK),
                              (cuuint32_t)tc::BM};
@@ -552,23 +577,25 @@ void init_schur_tc() {
 }
 
 template <int MODE>
-static void launch_schur_mode(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                              float* Us, int* err, const CUtensorMap* maps, cudaStream_t st) {
+static void launch_schur_mode(const DevPlan& D, const WorkList& w, int panel, int PW, int upd,
+                              float* Ls, float* Us, int* err, const CUtensorMap* maps,
+                              cudaStream_t st) {
     using C = tc::Cfg<MODE>;
     const int sms = D.num_sms > 0 ? D.num_sms : 148;
     k_schur_tc<MODE><<<std::min(w.nctas, sms * C::CTAS_PER_SM), C::NTHREADS, C::SMEM_BYTES, st>>>(
         D.fronts, D.psched.items + w.off, D.psched.before + w.off, w.nitems, w.nctas, D.tmap_idx,
-        maps, panel, PW, Ls, Us, err);
+        maps, panel, PW, upd, Ls, Us, err);
 }
 
-void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, float* Ls,
-                     float* Us, int* err, int mode, cudaStream_t st) {
+void launch_schur_tc(const DevPlan& D, const WorkList& w, int panel, int PW, int npan,
+                     bool strip, float* Ls, float* Us, int* err, int mode, cudaStream_t st) {
+    const int upd = npan | (strip ? 16 : 0);
     if (mode == kSchurBF16)
-        launch_schur_mode<kSchurBF16>(D, w, panel, PW, Ls, Us, err, D.tmaps_bf16, st);
+        launch_schur_mode<kSchurBF16>(D, w, panel, PW, upd, Ls, Us, err, D.tmaps_bf16, st);
     else if (mode == kSchur1xTF32)
-        launch_schur_mode<kSchur1xTF32>(D, w, panel, PW, Ls, Us, err, D.tmaps, st);
+        launch_schur_mode<kSchur1xTF32>(D, w, panel, PW, upd, Ls, Us, err, D.tmaps, st);
     else
-        launch_schur_mode<kSchur3xTF32>(D, w, panel, PW, Ls, Us, err, D.tmaps, st);
+        launch_schur_mode<kSchur3xTF32>(D, w, panel, PW, upd, Ls, Us, err, D.tmaps, st);
 }
 
 }  // namespace mdgpu
