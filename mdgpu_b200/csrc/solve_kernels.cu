@@ -41,12 +41,7 @@ __device__ inline TV* front_vec(TV* fv, const int64_t* fv_off, int s, int nrhs) 
 
 constexpr int kSolveWaitPolls = 1 << 18;  // ~0.1-0.3 s at ~1 us per poll
 constexpr int kWarpSolveRhs = 4;   // right-hand sides per pass of the warp path
-constexpr int kSolvePassRhs = 64;  // right-hand sides per pass of the solve launches
-// resident CTAs per SM of the solve launches with NQ right-hand sides per
-// thread (4 NQ per CTA): shared memory grows with them (64 of them: one)
-__host__ __device__ constexpr int solve_ctas_per_sm(int NQ) {
-    return NQ == 1 ? 4 : (NQ <= 8 ? 2 : 1);
-}
+constexpr int kSolvePassRhs = 32;  // right-hand sides per pass of the solve launches
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     int v;
@@ -462,8 +457,8 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     // two stages: the L blocks by cp.async; the ancestors' solution rows
     // (written in this launch) through L2 into registers one stage ahead,
     // stored into their stage after the previous stage's products
-    // vector elements per thread: T x (4 NQ) right-hand sides over 256 threads
-    constexpr int VPT = kTile * 4 * NQ / 256;
+    static_assert(kTile * kSolvePassRhs % 256 == 0, "whole vector elements per thread");
+    constexpr int VPT = kTile * kSolvePassRhs / 256;
     TV pend[VPT];
     auto fetch = [&](int p) {
 #pragma unroll
@@ -1205,7 +1200,7 @@ __device__ __forceinline__ bool cta_wait(const int* word, int target, int* abort
 }
 
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256, solve_ctas_per_sm(NQ))
+__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
     k_fwd_solve(const FrontDesc* __restrict__ fronts, const int4* __restrict__ items, int nitems,
                 int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
                 int* __restrict__ err, int* __restrict__ fdone, int* __restrict__ udone,
@@ -1286,7 +1281,7 @@ __global__ void __launch_bounds__(256, solve_ctas_per_sm(NQ))
 }
 
 template <typename TL, typename TV, int NQ>
-__global__ void __launch_bounds__(256, solve_ctas_per_sm(NQ))
+__global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
     k_bwd_solve(const FrontDesc* __restrict__ fronts, const int4* __restrict__ items, int nitems,
                 int* __restrict__ counter, double* __restrict__ pub, int* __restrict__ abort_flag,
                 int* __restrict__ err, int* __restrict__ bdone, const int* __restrict__ btarget,
@@ -1405,7 +1400,6 @@ static void set_solve_attributes() {
     set_solve_attributes_nq<TL, TV, 1>();
     set_solve_attributes_nq<TL, TV, 4>();
     set_solve_attributes_nq<TL, TV, 8>();
-    set_solve_attributes_nq<TL, TV, 16>();
 }
 
 void init_solve_kernels() {
@@ -1433,7 +1427,7 @@ static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* 
                     (size_t)2 * S.nflags * kTile * nrhs * sizeof(TV), st);
     const size_t sm = solve_smem<TL, TV>(nrhs);
     const int sms = D.num_sms > 0 ? D.num_sms : 148;
-    const int grid = sms * solve_ctas_per_sm(NQ);  // the launch bounds' residency
+    const int grid = sms * (NQ == 1 ? 4 : 2);  // the launch bounds' residency
     double fbytes = 0, bbytes = 0;
     for (int l = 0; l < D.nlevels; ++l) {
         fbytes += (S.small_elems[l] + S.fwd_elems[l]) * sizeof(TL);
@@ -1470,10 +1464,8 @@ void solve_levels(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* xp, TV* fv
             solve_levels_nq<TL, TV, 1>(D, Ls, Dinv, x, fv, nq, st);
         else if (nq <= 16)
             solve_levels_nq<TL, TV, 4>(D, Ls, Dinv, x, fv, nq, st);
-        else if (nq <= 32)
-            solve_levels_nq<TL, TV, 8>(D, Ls, Dinv, x, fv, nq, st);
         else
-            solve_levels_nq<TL, TV, 16>(D, Ls, Dinv, x, fv, nq, st);
+            solve_levels_nq<TL, TV, 8>(D, Ls, Dinv, x, fv, nq, st);
     }
 }
 
