@@ -480,9 +480,11 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
         D.solve.fwd_items = items(SS.fwd_items, D.solve.nfwd_items);
         D.solve.bwd_items = items(SS.bwd_items, D.solve.nbwd_items);
         {
-            std::vector<int> wc = SS.warp_cnt;
-            if (wc.empty()) wc.assign(3, 0);
-            D.solve.warp_cnt_d = h->keep(upload(wc));
+            std::vector<int> wf = SS.fwd_wlist, wb = SS.bwd_wlist;
+            if (wf.empty()) wf.assign(1, 0);
+            if (wb.empty()) wb.assign(1, 0);
+            D.solve.fwd_wlist = h->keep(upload(wf));
+            D.solve.bwd_wlist = h->keep(upload(wb));
         }
         D.solve.bwd_target = h->keep(upload(SS.bwd_target));
         D.solve.nfronts = P.nsuper;

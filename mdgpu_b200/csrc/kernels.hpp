@@ -103,7 +103,8 @@ struct SolveSchedule {
     int4* fwd_items = nullptr;
     int4* bwd_items = nullptr;
     int nfwd_items = 0, nbwd_items = 0;
-    int* warp_cnt_d = nullptr;   // 3 per level
+    int* fwd_wlist = nullptr;    // the warp items' fronts, per direction
+    int* bwd_wlist = nullptr;
     int* bwd_target = nullptr;   // per front
     int nfronts = 0;
     std::vector<int> fwd_task_beg, bwd_task_beg;  // nlevels + 1

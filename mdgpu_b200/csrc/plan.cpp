@@ -614,27 +614,114 @@ void build_solve_schedule(const Plan& P, int T, SolveScheduleHost& S) {
     }
     S.gather_vecs = vecs;
     S.gather_task_beg[P.nlevels] = (int)(S.tasks.size() / 2);
-    // the fused launches' item lists
-    const int WPI = SolveScheduleHost::kWarpsPerItem;
-    auto level_items = [&](int l, bool fwd, std::vector<int>& it) {
-        if (!fwd)
-            for (int q = S.gather_task_beg[l]; q < S.gather_task_beg[l + 1]; ++q)
-                it.insert(it.end(), {SolveScheduleHost::kItemGather, S.tasks[2 * q],
-                                     S.tasks[2 * q + 1], 0});
-        const std::vector<int>& beg = fwd ? S.fwd_task_beg : S.bwd_task_beg;
-        for (int q = beg[l]; q < beg[l + 1]; ++q)
-            it.insert(it.end(),
-                      {SolveScheduleHost::kItemTile, S.tasks[2 * q], S.tasks[2 * q + 1], 0});
-        const int n1 = S.warp_cnt[3 * l], n2 = S.warp_cnt[3 * l + 1], n4 = S.warp_cnt[3 * l + 2];
-        const int nw = n1 + (n2 + 1) / 2 + (n4 + 3) / 4;
-        const int sb = P.small_ptr[l * kSmallBuckets];
-        for (int t0 = 0; t0 < nw; t0 += WPI)
-            it.insert(it.end(), {SolveScheduleHost::kItemWarps, l, t0, sb});
-    };
-    S.fwd_items.clear();
-    S.bwd_items.clear();
-    for (int l = 0; l < P.nlevels; ++l) level_items(l, true, S.fwd_items);
-    for (int l = P.nlevels - 1; l >= 0; --l) level_items(l, false, S.bwd_items);
+    // the fused launches' item lists: fronts level by level (forward
+    // bottom-up, backward top-down), within a level by critical-path
+    // priority (an estimate of the latency from the front to the end of the
+    // sweep: forward, the front and its ancestors up to the root; backward,
+    // the front and its longest descendant chain), highest first.  A front's
+    // dependencies (forward: its children; backward: its parent) sit on
+    // earlier levels, so the order is topological.  Each large
+    // front's items stay together (forward: pivot tiles in order, then the
+    // update tasks; backward: the gathers, then the pivot tasks from the last
+    // pivot tile down); small fronts are packed into warp items of at most
+    // kWarpsPerItem warps in the same order, and an open warp item is emitted
+    // before any front that depends on one of its fronts.
+    {
+        const int ns = P.nsuper;
+        std::vector<int64_t> lat(ns, 4), pf(ns, 0), pb(ns, 0);
+        for (int s : P.large_list) lat[s] = 6 + 3 * (int64_t)((P.fronts[s].c + T - 1) / T);
+        auto level_fronts = [&](int l, auto&& fn) {
+            for (int q = P.small_ptr[l * kSmallBuckets]; q < P.small_ptr[(l + 1) * kSmallBuckets]; ++q)
+                fn(P.small_list[q]);
+            for (int q = P.large_ptr[l]; q < P.large_ptr[l + 1]; ++q) fn(P.large_list[q]);
+        };
+        for (int l = P.nlevels - 1; l >= 0; --l)  // parents first
+            level_fronts(l, [&](int s) {
+                const int par = P.fronts[s].parent;
+                pf[s] = lat[s] + (par >= 0 ? pf[par] : 0);
+            });
+        for (int l = 0; l < P.nlevels; ++l)  // children first
+            level_fronts(l, [&](int s) {
+                int64_t h = 0;
+                for (int q = P.fronts[s].child_beg; q < P.fronts[s].child_end; ++q)
+                    h = std::max(h, pb[P.child[q]]);
+                pb[s] = lat[s] + h;
+            });
+        std::vector<char> large(ns, 0);
+        for (int s : P.large_list) large[s] = 1;
+        const int WPI = SolveScheduleHost::kWarpsPerItem;
+        std::vector<int> lev(ns, 0);
+        for (int l = 0; l < P.nlevels; ++l) level_fronts(l, [&](int s) { lev[s] = l; });
+        for (int dir = 0; dir < 2; ++dir) {
+            const std::vector<int64_t>& pr = dir == 0 ? pf : pb;
+            std::vector<int> order(ns);
+            for (int s = 0; s < ns; ++s) order[s] = s;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                if (lev[a] != lev[b]) return dir == 0 ? lev[a] < lev[b] : lev[a] > lev[b];
+                return pr[a] > pr[b];
+            });
+            std::vector<int>& it = dir == 0 ? S.fwd_items : S.bwd_items;
+            std::vector<int>& wl = dir == 0 ? S.fwd_wlist : S.bwd_wlist;
+            it.clear();
+            wl.clear();
+            std::vector<char> open(ns, 0);
+            std::vector<int> cls[3];
+            auto warps = [](size_t a, size_t b, size_t c) {
+                return (int)(a + (b + 1) / 2 + (c + 3) / 4);
+            };
+            auto flush = [&]() {
+                if (cls[0].empty() && cls[1].empty() && cls[2].empty()) return;
+                const int off = (int)wl.size();
+                for (int k = 0; k < 3; ++k)
+                    for (int f : cls[k]) {
+                        wl.push_back(f);
+                        open[f] = 0;
+                    }
+                it.insert(it.end(), {SolveScheduleHost::kItemWarps, off,
+                                     (int)cls[0].size() | (int)cls[1].size() << 8 |
+                                         (int)cls[2].size() << 16,
+                                     0});
+                for (auto& v : cls) v.clear();
+            };
+            for (int s : order) {
+                const FrontDesc& f = P.fronts[s];
+                bool dep_open = false;
+                if (dir == 0) {
+                    for (int q = f.child_beg; q < f.child_end; ++q) dep_open |= open[P.child[q]] != 0;
+                } else {
+                    dep_open = f.parent >= 0 && open[f.parent];
+                }
+                if (dep_open) flush();
+                if (large[s]) {
+                    const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                    if (dir == 0) {
+                        for (int i = 0; i < nt1; ++i)
+                            it.insert(it.end(), {SolveScheduleHost::kItemTile, s, i | (1 << 16), 0});
+                        const int G = std::max(1, std::min(SolveScheduleHost::kFwdGroupBlocks / nt1,
+                                                           SolveScheduleHost::kFwdGroupTiles));
+                        for (int i = nt1; i < NT; i += G)
+                            it.insert(it.end(), {SolveScheduleHost::kItemTile, s,
+                                                 i | (std::min(G, NT - i) << 16), 0});
+                    } else {
+                        for (int j = nt1 - 1; j >= 0; --j)
+                            for (int h = 0; h < S.gather_nch[s]; ++h)
+                                it.insert(it.end(),
+                                          {SolveScheduleHost::kItemGather, s, j | (h << 16), 0});
+                        for (int j = nt1 - 1; j >= 0; --j)
+                            it.insert(it.end(), {SolveScheduleHost::kItemTile, s, j, 0});
+                    }
+                } else {
+                    const int k = f.m > 16 ? 0 : (f.m > 8 ? 1 : 2);
+                    const size_t a = cls[0].size() + (k == 0), b = cls[1].size() + (k == 1),
+                                 c = cls[2].size() + (k == 2);
+                    if (warps(a, b, c) > WPI) flush();
+                    cls[k].push_back(s);
+                    open[s] = 1;
+                }
+            }
+            flush();
+        }
+    }
     S.bwd_target.assign(P.nsuper, 1);
     for (int s : P.large_list) S.bwd_target[s] = (P.fronts[s].c + T - 1) / T;
 }

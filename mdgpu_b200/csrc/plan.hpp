@@ -229,28 +229,30 @@ struct SolveScheduleHost {
     // chunk count and the first partial (pivot tile j, chunk h at
     // gather_off + j * gather_nch + h; every level's partials side by side,
     // the levels' launches being one)
-    static constexpr int kGatherTiles = 16;
+    static constexpr int kGatherTiles = 4;
     std::vector<int> gather_task_beg;   // nlevels + 1, in tasks
     std::vector<int> gather_nch, gather_off;  // per supernode
     int64_t gather_vecs = 0;            // partial vectors of all levels
-    // The solve runs one launch per direction over every level's work
-    // items in dependency order -- forward levels bottom-up, backward
-    // top-down -- four ints per item {kind, a, b, c}:
+    // The solve runs one launch per direction over all work items in a
+    // topological order (every item's dependencies come earlier), fronts by
+    // critical-path priority, four ints per item {kind, a, b, c}:
     //   kItemTile    a large-front tile task: front a, task spec b (as in
     //                tasks: the forward row tiles or the backward pivot tile)
     //   kItemGather  a backward update-row gather: front a, spec b
-    //   kItemWarps   warp tasks b .. b + 7 of level a's small fronts (c: the
-    //                level's first entry of warp_list)
-    // Within a level the tile tasks (backward: gathers, then pivot tiles)
-    // come before the warp items.
+    //   kItemWarps   small fronts on up to kWarpsPerItem warps: entries
+    //                a .. of the direction's warp list, b = n1 | n2 << 8 |
+    //                n4 << 16: n1 fronts of more than 16 rows (a warp each),
+    //                then n2 of 9..16 rows (two per warp), then n4 of at
+    //                most 8 rows (four per warp)
     static constexpr int kItemTile = 0, kItemGather = 1, kItemWarps = 2;
     static constexpr int kWarpsPerItem = 8;
     std::vector<int> fwd_items, bwd_items;
+    std::vector<int> fwd_wlist, bwd_wlist;  // the warp items' fronts
     // backward: the solution rows of front s are final once bwd_target[s]
     // completions are counted (one per pivot tile of a large front, one for
     // a small front)
     std::vector<int> bwd_target;
-    // small fronts of each level for the warp-per-front sweeps, by rows
+    // small fronts of each level for the warp-per-front factor, by rows
     // descending (same level ranges as small_list): warp_cnt[3 l + k] fronts
     // of more than 16 rows (k = 0, a warp each), of 9..16 rows (k = 1, two
     // per warp) and of at most 8 rows (k = 2, four per warp)

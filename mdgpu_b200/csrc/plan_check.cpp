@@ -257,37 +257,98 @@ std::string check_plan(const Plan& P, const Symbolic& S, const SolveScheduleHost
                 }
             }
         }
-        // the one-launch solve's item lists: levels in order (forward
-        // bottom-up, backward top-down); per level the backward gathers,
-        // then the tile tasks exactly as the level's task list orders them,
-        // then the warp items covering the level's warp tasks
+        // the one-launch solve's item lists: every front's work exactly once
+        // (forward: each pivot tile alone and in order, then update tasks
+        // covering the update tiles in order; backward: each gather (j, h)
+        // once, each pivot tile once, descending, after its gathers; small
+        // fronts in warp items of at most kWarpsPerItem warps, each once), in
+        // a topological order: forward all of a front's items after all of
+        // its children's, backward after all of its parent's
         {
             const int WPI = SolveScheduleHost::kWarpsPerItem;
             for (int dir = 0; dir < 2; ++dir) {
                 const std::vector<int>& it = dir == 0 ? Q.fwd_items : Q.bwd_items;
+                const std::vector<int>& wl = dir == 0 ? Q.fwd_wlist : Q.bwd_wlist;
                 if (it.size() % 4) bad("solve items");
-                size_t q = 0;
-                for (int step = 0; step < P.nlevels; ++step) {
-                    const int l = dir == 0 ? step : P.nlevels - 1 - step;
-                    if (dir == 1)
-                        for (int t = Q.gather_task_beg[l]; t < Q.gather_task_beg[l + 1]; ++t, q += 4)
-                            if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemGather ||
-                                it[q + 1] != Q.tasks[2 * t] || it[q + 2] != Q.tasks[2 * t + 1])
-                                bad("solve items: gathers", l);
-                    const std::vector<int>& beg = dir == 0 ? Q.fwd_task_beg : Q.bwd_task_beg;
-                    for (int t = beg[l]; t < beg[l + 1]; ++t, q += 4)
-                        if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemTile ||
-                            it[q + 1] != Q.tasks[2 * t] || it[q + 2] != Q.tasks[2 * t + 1])
-                            bad("solve items: tile tasks", l);
-                    const int nw = Q.warp_cnt[3 * l] + (Q.warp_cnt[3 * l + 1] + 1) / 2 +
-                                   (Q.warp_cnt[3 * l + 2] + 3) / 4;
-                    for (int t0 = 0; t0 < nw; t0 += WPI, q += 4)
-                        if (q + 4 > it.size() || it[q] != SolveScheduleHost::kItemWarps ||
-                            it[q + 1] != l || it[q + 2] != t0 ||
-                            it[q + 3] != P.small_ptr[l * kSmallBuckets])
-                            bad("solve items: warp tasks", l);
+                if (wl.size() != P.small_list.size()) bad("solve warp list size");
+                const int64_t nit = (int64_t)it.size() / 4;
+                std::vector<int64_t> first(ns, -1), last(ns, -1);
+                std::vector<int> piv(ns, 0), upd(ns, 0), wseen(ns, 0);
+                std::vector<std::vector<char>> gseen(ns);
+                std::vector<int> gcnt(ns, 0);
+                std::vector<char> wl_used(wl.size(), 0);
+                auto touch = [&](int s, int64_t k) {
+                    if (first[s] < 0) first[s] = k;
+                    last[s] = k;
+                };
+                for (int64_t k = 0; k < nit; ++k) {
+                    const int* e = it.data() + 4 * k;
+                    if (e[0] == SolveScheduleHost::kItemWarps) {
+                        const int n1 = e[2] & 0xff, n2 = (e[2] >> 8) & 0xff, n4 = e[2] >> 16;
+                        const int nf = n1 + n2 + n4;
+                        if (nf < 1 || n1 + (n2 + 1) / 2 + (n4 + 3) / 4 > WPI || e[1] < 0 ||
+                            (size_t)e[1] + nf > wl.size())
+                            bad("solve warp item");
+                        for (int q = 0; q < nf; ++q) {
+                            if (wl_used[e[1] + q]++) bad("solve warp list entry used twice");
+                            const int s = wl[e[1] + q];
+                            if (s < 0 || s >= ns || is_large[s]) bad("solve warp list entry");
+                            const int m = P.fronts[s].m;
+                            if ((q < n1) != (m > 16) || (q >= n1 + n2) != (m <= 8))
+                                bad("solve warp item size class", s);
+                            wseen[s]++;
+                            touch(s, k);
+                        }
+                        continue;
+                    }
+                    const int s = e[1], t = e[2];
+                    if (s < 0 || s >= ns || !is_large[s]) bad("solve item front");
+                    const FrontDesc& f = P.fronts[s];
+                    const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                    const int nch = Q.gather_nch[s];
+                    if (gseen[s].empty()) gseen[s].assign((size_t)nt1 * std::max(nch, 1), 0);
+                    touch(s, k);
+                    if (e[0] == SolveScheduleHost::kItemGather) {
+                        const int j = t & 0xffff, h = t >> 16;
+                        if (dir != 1 || j >= nt1 || h >= nch || gseen[s][(size_t)j * nch + h]++ ||
+                            piv[s] > nt1 - 1 - j)
+                            bad("solve gather item", s);
+                        gcnt[s]++;
+                    } else if (e[0] != SolveScheduleHost::kItemTile) {
+                        bad("solve item kind", s);
+                    } else if (dir == 0) {
+                        const int i = t & 0xffff, cnt = t >> 16;
+                        if (cnt < 1 || i + cnt > NT) bad("forward item tiles", s);
+                        if (i < nt1) {
+                            if (cnt != 1 || i != piv[s] || upd[s]) bad("forward pivot order", s);
+                            piv[s]++;
+                        } else {
+                            if (piv[s] != nt1 || i != nt1 + upd[s]) bad("forward update order", s);
+                            upd[s] += cnt;
+                        }
+                    } else {
+                        if (t != nt1 - 1 - piv[s]) bad("backward pivot order", s);
+                        for (int h = 0; h < nch; ++h)
+                            if (!gseen[s][(size_t)t * nch + h]) bad("backward pivot before its gathers", s);
+                        piv[s]++;
+                    }
                 }
-                if (q != it.size()) bad("solve items: extra entries");
+                for (int s = 0; s < ns; ++s) {
+                    const FrontDesc& f = P.fronts[s];
+                    if (is_large[s]) {
+                        const int nt1 = (f.c + T - 1) / T, NT = front_tiles(f.m, f.c, T);
+                        if (piv[s] != nt1 || (dir == 0 && upd[s] != NT - nt1) ||
+                            (dir == 1 && gcnt[s] != nt1 * Q.gather_nch[s]))
+                            bad("solve items do not cover the front", s);
+                    } else if (wseen[s] != 1) {
+                        bad("small front not in exactly one warp item", s);
+                    }
+                    if (f.parent >= 0) {
+                        const bool ok = dir == 0 ? last[s] < first[f.parent]
+                                                 : last[f.parent] < first[s];
+                        if (!ok) bad("solve items out of dependency order", s);
+                    }
+                }
             }
             if ((int)Q.bwd_target.size() != ns) bad("backward targets");
             for (int s = 0; s < ns; ++s)

@@ -79,7 +79,10 @@ __device__ bool wait_flag(const int* flag, int target, int* abort_flag, int* err
 // (a NaN that arithmetic never produces), and a producer stores final values
 // only (aligned 8-byte stores are single-copy atomic), so a consumer that
 // sees no sentinel has the data: one round trip instead of flag then data.
-// All threads poll together (uniform result); iteration limit as wait_flag.
+// All threads poll together (uniform result): the warps that hold slot
+// elements spin on their own elements (a warp vote per round, no block
+// barrier, a short sleep and an abort check every 32 rounds), the others go
+// straight to the closing barrier; iteration limit as wait_flag.
 __device__ __forceinline__ double ld_relaxed_f64(const double* p) {
     double v;
     asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
@@ -99,30 +102,35 @@ __device__ __forceinline__ bool is_unpublished(double v) {
 __device__ bool poll_published(double* dst, const double* src, int nk, int nrhs, int* abort_flag,
                                int* err) {
     constexpr int T = kTile;
-    __shared__ int s_abort[2];
-    for (int it = 0; it < kSolveWaitPolls; ++it) {
-        bool mine = true;
-        for (int e = threadIdx.x; e < T * nrhs; e += blockDim.x) {
-            if ((e & (T - 1)) < nk) {
-                const double v = ld_relaxed_f64(src + e);
-                if (is_unpublished(v))
-                    mine = false;
-                else
-                    dst[e] = v;
-            } else {
-                dst[e] = 0.0;
+    const int total = T * nrhs, lane = threadIdx.x & 31;  // total: a multiple of 64
+    bool ok = true;
+    for (int base = threadIdx.x & ~31; ok && base < total; base += blockDim.x) {
+        const int e = base + lane;
+        const bool need = (e & (T - 1)) < nk;
+        double v = 0.0;
+        for (int it = 0;; ++it) {
+            if (need) v = ld_relaxed_f64(src + e);
+            if (__all_sync(0xffffffffu, !need || !is_unpublished(v))) break;
+            if (it + 1 >= kSolveWaitPolls) {
+                if (lane == 0) {
+                    atomicExch(abort_flag, 1);
+                    atomicOr(err, 1);
+                }
+                ok = false;
+                break;
+            }
+            if ((it & 31) == 31) {
+                const int a = lane == 0 ? ld_relaxed_gpu(abort_flag) : 0;
+                if (__shfl_sync(0xffffffffu, a, 0)) {
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
             }
         }
-        if (threadIdx.x == 0) s_abort[it & 1] = ld_relaxed_gpu(abort_flag);
-        if (__syncthreads_and(mine)) return true;
-        if (s_abort[it & 1]) return false;
-        __nanosleep(32);
+        if (ok) dst[e] = need ? v : 0.0;
     }
-    if (threadIdx.x == 0) {
-        atomicExch(abort_flag, 1);
-        atomicOr(err, 1);
-    }
-    return false;
+    return __syncthreads_and(ok);
 }
 
 template <typename TL>
@@ -141,19 +149,37 @@ __device__ __forceinline__ void cp_async_wait_groups() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Rows [0, nr) x columns [0, nc) of a column-major block (leading dimension
-// ld) into a kTile x (kTile + 1) shared array, zeros elsewhere.
+// Stage layout of a 64 x 64 block of L (or of a diagonal inverse): column-
+// major, columns of blk_ld elements (a multiple of 16 bytes), copied in
+// 16-byte chunks from the 16-byte boundary at or below the block's first
+// row, so row r of column c sits at c * blk_ld + d + r with d =
+// blk_off(first row).  Rows past the block and columns past nc are
+// zero-filled by the copies themselves (source size below 16 bytes).  The L
+// store's columns start on 32-byte boundaries (ldl a multiple of 8, front
+// offsets of 32), the inverses' on 64 * 64 elements.
 template <typename TL>
-__device__ __forceinline__ void load_block_async(TL* dst, const TL* src, int64_t ld, int nr,
-                                                 int nc) {
-    constexpr int T = kTile, LD = kTile + 1;
-    for (int e = threadIdx.x; e < T * T; e += blockDim.x) {
-        const int r = e & (T - 1), col = e / T;
-        TL* d = dst + r + col * LD;
-        if (r < nr && col < nc)
-            cp_async_elem(d, src + r + (int64_t)col * ld);
-        else
-            *d = TL(0);
+__host__ __device__ constexpr int blk_ld() {
+    return kTile + 16 / (int)sizeof(TL);
+}
+template <typename TL>
+__device__ __forceinline__ int blk_off(int start) {
+    return start & (16 / (int)sizeof(TL) - 1);
+}
+// rows start .. start + nr - 1 and columns 0 .. nc - 1 of the matrix at src
+// (column stride ld)
+template <typename TL>
+__device__ __forceinline__ void load_block_async(TL* dst, const TL* src, int64_t ld, int start,
+                                                 int nr, int nc) {
+    constexpr int E = 16 / (int)sizeof(TL), LDB = blk_ld<TL>(), CH = LDB / E;
+    const int r0 = start - blk_off<TL>(start);
+    for (int e = threadIdx.x; e < kTile * CH; e += blockDim.x) {
+        const int col = e / CH, u = e - col * CH;
+        const int row = r0 + u * E;
+        const int bytes = col < nc ? min(max(start + nr - row, 0), E) * (int)sizeof(TL) : 0;
+        const TL* sp = bytes ? src + row + (int64_t)col * ld : src;
+        const uint32_t da = static_cast<uint32_t>(__cvta_generic_to_shared(dst + col * LDB + u * E));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(da), "l"(sp), "r"(bytes)
+                     : "memory");
     }
 }
 
@@ -175,7 +201,7 @@ __host__ __device__ constexpr int level_stages(int nrhs) {
 // vector, the quarter reduction, the gather's row indices
 template <typename TL, typename TV>
 __host__ __device__ constexpr size_t level_smem_bytes(int nrhs) {
-    return (((1 + (size_t)level_stages<TL>(nrhs)) * kTile * (kTile + 1) * sizeof(TL) + 15) / 16) * 16 +
+    return (((1 + (size_t)level_stages<TL>(nrhs)) * kTile * blk_ld<TL>() * sizeof(TL) + 15) / 16) * 16 +
            (((size_t)level_stages<TL>(nrhs) + 1) * kTile * nrhs + 4 * kTile) * sizeof(TV) +
            (size_t)SolveScheduleHost::kGatherTiles * kTile * sizeof(int);
 }
@@ -190,7 +216,7 @@ struct LevelSmem {
     int* idx; // kGatherTiles x T
     int stg;
     __device__ explicit LevelSmem(int nrhs) {
-        constexpr int T = kTile, LD = kTile + 1;
+        constexpr int T = kTile, LD = blk_ld<TL>();
         extern __shared__ __align__(16) unsigned char smem_raw[];
         stg = level_stages<TL>(nrhs);
         Dk = reinterpret_cast<TL*>(smem_raw);
@@ -201,7 +227,7 @@ struct LevelSmem {
         red = Y + T * nrhs;
         idx = reinterpret_cast<int*>(red + 4 * T);
     }
-    __device__ TL* lb(int p) const { return Lst + (p % stg) * kTile * (kTile + 1); }
+    __device__ TL* lb(int p) const { return Lst + (p % stg) * kTile * blk_ld<TL>(); }
     __device__ TV* vb(int p, int nrhs) const { return Vst + (size_t)(p % stg) * kTile * nrhs; }
 };
 
@@ -257,7 +283,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
                               const TL* __restrict__ Dinv, TV* __restrict__ xp,
                               TV* __restrict__ fv, int n, int nrhs) {
     static_assert(sizeof(TV) == 8, "solve vectors are double");
-    constexpr int T = kTile, LD = kTile + 1;
+    constexpr int T = kTile, LD = blk_ld<TL>();
     const LevelSmem<TL, TV> sm(nrhs);
     const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
     const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
@@ -270,6 +296,10 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
     const TL* L = Ls + F.loff;
     double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
     TV* f = front_vec(fv, fv_off, s, nrhs);
+    // the row offset of this task's blocks in their stage columns (every row
+    // tile of a task starts at the same residue: 0 for a pivot tile, c for
+    // update tiles)
+    const int db = blk_off<TL>(tile_range(i0, F.m, F.c, T).start);
     const int aoff = amap_off[s];
     // rows of tile i of the front vector into v (this thread's share)
     auto gather_rows = [&](int i, TV (&v)[NQ]) {
@@ -295,7 +325,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         if (p < P) {
             const int i = i0 + p / kend, k = p % kend;
             const TileRange ti = tile_range(i, F.m, F.c, T);
-            load_block_async(sm.lb(p), L + ti.start + (int64_t)k * T * F.ldl, F.ldl, ti.size,
+            load_block_async(sm.lb(p), L + (int64_t)k * T * F.ldl, F.ldl, ti.start, ti.size,
                              min(T, F.c - k * T));
             load_slot_async(sm.vb(p, nrhs), pb + (int64_t)k * T * nrhs, nrhs);
         }
@@ -303,7 +333,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
     };
     if (pivot) {
         const TileRange ti = tile_range(i0, F.m, F.c, T);
-        load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)i0 * T * T, T, ti.size, ti.size);
+        load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)i0 * T * T, T, 0, ti.size, ti.size);
     }
     for (int p = 0; p < sm.stg - 1; ++p) issue(p);
     TV fcur[NQ], fnext[NQ], acc[NQ];
@@ -314,6 +344,8 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         acc[j] = TV(0);
     }
     if (cnt > 1) gather_rows(i0 + 1, fnext);
+    // a pivot tile's f_i (one right-hand side) for the solve at the end
+    if (pivot && lsplit && g == 0) sm.Y[r] = fcur[0];
     bool ok = true;
     for (int p = 0; p < P; ++p) {
         issue(p + sm.stg - 1);
@@ -329,11 +361,12 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         const TL* B = sm.lb(p);
         if (lsplit) {
 #pragma unroll
-            for (int l = 0; l < 16; ++l) acc[0] += (TV)B[r + (16 * g + l) * LD] * Yk[16 * g + l];
+            for (int l = 0; l < 16; ++l)
+                acc[0] += (TV)B[db + r + (16 * g + l) * LD] * Yk[16 * g + l];
         } else {
 #pragma unroll 4
             for (int l = 0; l < T; ++l) {
-                const TV lv = (TV)B[r + l * LD];
+                const TV lv = (TV)B[db + r + l * LD];
 #pragma unroll
                 for (int j = 0; j < NQ; ++j) {
                     const int q = g + 4 * j;
@@ -363,42 +396,47 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
             }
             if (i + 2 < i0 + cnt) gather_rows(i + 2, fnext);
         }
-        __syncthreads();
+        if (p + 1 < P) __syncthreads();  // the stages are reused; after the last, nothing is
     }
     cp_async_wait_groups<0>();
     if (!ok || !pivot) return;
-    __syncthreads();
     // pivot tile: F = f_i - acc (zero beyond the tile), then y = Dk F
     const TileRange ti = tile_range(i0, F.m, F.c, T);
     TV* Y = sm.Y;
     TV* red = sm.red;
     const TL* Dk = sm.Dk;
     if (lsplit) {
+        // one right-hand side, two barriers: the quarters' sums, then each
+        // thread forms the 16 entries of F its quarter multiplies (f_i from
+        // sm.Y) and the partial products meet in a stage buffer (free now)
         red[g * T + r] = acc[0];
         __syncthreads();
-        if (g == 0)
-            Y[r] = r < ti.size ? fcur[0] - (red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r])
-                               : TV(0);
-    } else {
-#pragma unroll
-        for (int j = 0; j < NQ; ++j) {
-            const int q = g + 4 * j;
-            if (q < nrhs) Y[r + T * q] = r < ti.size ? fcur[j] - acc[j] : TV(0);
-        }
-    }
-    __syncthreads();
-    if (lsplit) {
+        TV* red2 = reinterpret_cast<TV*>(sm.lb(0));
         TV y = TV(0);
 #pragma unroll
-        for (int l = 0; l < 16; ++l) y += (TV)Dk[r + (16 * g + l) * LD] * Y[16 * g + l];
-        red[g * T + r] = y;
+        for (int l = 0; l < 16; ++l) {
+            const int x = 16 * g + l;
+            const TV t = x < ti.size ? Y[x] - (red[x] + red[T + x] + red[2 * T + x] + red[3 * T + x])
+                                     : TV(0);
+            y += (TV)Dk[r + x * LD] * t;
+        }
+        red2[g * T + r] = y;
         __syncthreads();
         if (g == 0 && r < ti.size) {
-            const TV v = red[r] + red[T + r] + red[2 * T + r] + red[3 * T + r];
+            const TV v = red2[r] + red2[T + r] + red2[2 * T + r] + red2[3 * T + r];
             xp[F.first_col + ti.start + r] = v;
             st_relaxed_f64(pb + (int64_t)i0 * T + r, v);
         }
-    } else {
+        return;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+        const int q = g + 4 * j;
+        if (q < nrhs) Y[r + T * q] = r < ti.size ? fcur[j] - acc[j] : TV(0);
+    }
+    __syncthreads();
+    {
         TV y[NQ];
 #pragma unroll
         for (int j = 0; j < NQ; ++j) y[j] = TV(0);
@@ -436,7 +474,7 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                 const int64_t* __restrict__ dinv_off, const TL* __restrict__ Ls,
                                 const TV* __restrict__ xp, TV* __restrict__ part, int n,
                                 int nrhs) {
-    constexpr int T = kTile, LD = kTile + 1, GC = SolveScheduleHost::kGatherTiles;
+    constexpr int T = kTile, LD = blk_ld<TL>(), GC = SolveScheduleHost::kGatherTiles;
     const LevelSmem<TL, TV> sm(nrhs);
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
     const int s = tk.x, j = tk.y & 0xffff, h = tk.y >> 16;
@@ -447,6 +485,12 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     const TL* Lc = Ls + F.loff + (int64_t)tj.start * F.ldl;
     const int* rw = rows + F.rows_off;
     const int k0 = nt1 + h * GC, P = min(NT, k0 + GC) - k0;
+    // update row tiles start at c + 64 u: one row offset for every block
+    const int db = blk_off<TL>(F.c);
+    // one right-hand side: warp w takes columns 8w .. 8w + 7, lane (c1 =
+    // column, q1 = row phase) the rows q1, q1 + 4, ...: conflict-free reads
+    // of the 16-byte-column stage layout, the phases summed by shuffles
+    const int c1 = 8 * (tid >> 5) + (tid & 7), q1 = (tid >> 3) & 3;
     // the chunk's solution rows (ancestors), then the pipeline
     for (int e = tid; e < P * T; e += blockDim.x) {
         const TileRange tkr = tile_range(k0 + e / T, F.m, F.c, T);
@@ -483,7 +527,7 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     auto issue = [&](int p) {
         if (p < P) {
             const TileRange tkr = tile_range(k0 + p, F.m, F.c, T);
-            load_block_async(sm.lb(p), Lc + tkr.start, F.ldl, tkr.size, tj.size);
+            load_block_async(sm.lb(p), Lc, F.ldl, tkr.start, tkr.size, tj.size);
         }
         cp_async_commit_group();
     };
@@ -503,11 +547,12 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
         const TV* X = sm.vb(p, nrhs);
         if (lsplit) {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) acc[0] += (TV)Bk[(16 * g + r) + l * LD] * X[16 * g + r];
+            for (int u = 0; u < 16; ++u)
+                acc[0] += (TV)Bk[db + q1 + 4 * u + c1 * LD] * X[q1 + 4 * u];
         } else {
 #pragma unroll 4
             for (int r = 0; r < T; ++r) {
-                const TV lv = (TV)Bk[r + l * LD];
+                const TV lv = (TV)Bk[db + r + l * LD];
 #pragma unroll
                 for (int a = 0; a < NQ; ++a) {
                     const int q = g + 4 * a;
@@ -521,9 +566,9 @@ __device__ void bwd_gather_task(int2 tk, const FrontDesc* __restrict__ fronts,
     cp_async_wait_groups<0>();
     TV* out = part + ((int64_t)gather_off[s] + (int64_t)j * gather_nch[s] + h) * T * nrhs;
     if (lsplit) {
-        sm.red[g * T + l] = acc[0];
-        __syncthreads();
-        if (g == 0) out[l] = sm.red[l] + sm.red[T + l] + sm.red[2 * T + l] + sm.red[3 * T + l];
+        TV v = acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        if (q1 == 0) out[c1] = v;
     } else {
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
@@ -859,9 +904,9 @@ __host__ __device__ constexpr int warp_buf_stride(int msmall, int nrhs) {
     return warp_rows(msmall) * (nrhs == 1 ? 1 : kWarpSolveRhs);
 }
 
-// Warp tasks of one level's small fronts (the level's slice of the rows-
-// descending warp list): tasks [0, n1) one front each, then two fronts of
-// 9..16 rows per task, then four of at most 8 rows.
+// Warp tasks of one warp item (its slice of the direction's warp list):
+// tasks [0, n1) one front each, then two fronts of 9..16 rows per task, then
+// four of at most 8 rows.
 struct WarpTasks {
     const int* list;
     int n1, n2, n4;
@@ -946,10 +991,14 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
                                const TL* __restrict__ Ls, const TL* __restrict__ Dinv,
                                TV* __restrict__ xp, int n, int nrhs) {
     static_assert(sizeof(TV) == 8, "solve vectors are double");
-    constexpr int T = kTile, LD = kTile + 1;
+    constexpr int T = kTile, LD = blk_ld<TL>();
     const LevelSmem<TL, TV> sm(nrhs);
     __shared__ int s_ok;
     const int tid = threadIdx.x, l = tid & (T - 1), g = tid >> 6;
+    // one right-hand side: warp w takes columns 8w .. 8w + 7, lane (c1 =
+    // column, q1 = row phase) the rows q1, q1 + 4, ...: conflict-free reads
+    // of the 16-byte-column stage layout, the phases summed by shuffles
+    const int c1 = 8 * (tid >> 5) + (tid & 7), q1 = (tid >> 3) & 3;
     const int s = tk.x, j = tk.y;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T);
@@ -962,12 +1011,12 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     auto issue = [&](int p) {
         if (p < P) {
             const TileRange tkr = tile_range(nt1 - 1 - p, F.m, F.c, T);
-            load_block_async(sm.lb(p), Lc + tkr.start, F.ldl, tkr.size, tj.size);
+            load_block_async(sm.lb(p), Lc, F.ldl, tkr.start, tkr.size, tj.size);
             load_slot_async(sm.vb(p, nrhs), pb + (int64_t)(nt1 - 1 - p) * T * nrhs, nrhs);
         }
         cp_async_commit_group();
     };
-    load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, tj.size, tj.size);
+    load_block_async(sm.Dk, Dinv + dinv_off[s] + (int64_t)j * T * T, T, 0, tj.size, tj.size);
     for (int p = 0; p < sm.stg - 1; ++p) issue(p);
     TV acc[NQ];
 #pragma unroll
@@ -977,10 +1026,12 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
     TV ypre[NQ];
 #pragma unroll
     for (int a = 0; a < NQ; ++a) {
-        const int q = lsplit ? 0 : g + 4 * a;
-        ypre[a] = (l < tj.size && q < nrhs && (!lsplit || (g == 0 && a == 0)))
-                      ? __ldcg(xp + xj + l + (int64_t)q * n)
-                      : TV(0);
+        if (lsplit)
+            ypre[a] = (a == 0 && q1 == 0 && c1 < tj.size) ? __ldcg(xp + xj + c1) : TV(0);
+        else
+            ypre[a] = (l < tj.size && g + 4 * a < nrhs)
+                          ? __ldcg(xp + xj + l + (int64_t)(g + 4 * a) * n)
+                          : TV(0);
     }
     // the update-row partial sums of (s, j) (gathers hold lower tickets), in
     // chunk order, before the chain's first wait
@@ -996,7 +1047,7 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
             const TV* pj = part + ((int64_t)gather_off[s] + (int64_t)j * nch) * T * nrhs;
             for (int h = 0; h < nch; ++h, pj += (int64_t)T * nrhs) {
                 if (lsplit) {
-                    if (g == 0) acc[0] += __ldcg(pj + l);
+                    if (q1 == 0) acc[0] += __ldcg(pj + c1);
                 } else {
 #pragma unroll
                     for (int a = 0; a < NQ; ++a) {
@@ -1022,7 +1073,7 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
         const TL* B = sm.lb(p);
         if (lsplit) {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) acc[0] += (TV)B[(16 * g + r) + l * LD] * X[16 * g + r];
+            for (int u = 0; u < 16; ++u) acc[0] += (TV)B[q1 + 4 * u + c1 * LD] * X[q1 + 4 * u];
         } else {
 #pragma unroll 4
             for (int r = 0; r < T; ++r) {
@@ -1034,43 +1085,39 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
                 }
             }
         }
-        __syncthreads();
+        if (p + 1 < P) __syncthreads();  // the stages are reused; after the last, nothing is
     }
     cp_async_wait_groups<0>();
     if (!ok) return;
-    __syncthreads();
     TV* X = sm.Y;
-    TV* red = sm.red;
     const TL* Dk = sm.Dk;
-    if (lsplit) {
-        red[g * T + l] = acc[0];
-        __syncthreads();
-        acc[0] = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
-        __syncthreads();
-    }
     // t = y_j - acc (y_j: this front's forward solution), then x_j = Dk' t
     if (lsplit) {
-        if (g == 0) X[l] = l < tj.size ? ypre[0] - acc[0] : TV(0);
-    } else {
-#pragma unroll
-        for (int a = 0; a < NQ; ++a) {
-            const int q = g + 4 * a;
-            if (q < nrhs) X[l + T * q] = l < tj.size ? ypre[a] - acc[a] : TV(0);
-        }
-    }
-    __syncthreads();
-    if (lsplit) {
+        // one right-hand side, one barrier: the row phases' sums by
+        // shuffles, t into sm.Y, then x_j = Dk' t the same way
+        TV a = acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 8);
+        a += __shfl_xor_sync(0xffffffffu, a, 16);
+        if (q1 == 0) X[c1] = c1 < tj.size ? ypre[0] - a : TV(0);
+        __syncthreads();
         TV x = TV(0);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) x += (TV)Dk[(16 * g + r) + l * LD] * X[16 * g + r];
-        red[g * T + l] = x;
-        __syncthreads();
-        if (g == 0 && l < tj.size) {
-            const TV v = red[l] + red[T + l] + red[2 * T + l] + red[3 * T + l];
-            xp[xj + l] = v;
-            st_relaxed_f64(pb + (int64_t)j * T + l, v);
+        for (int u = 0; u < 16; ++u) x += (TV)Dk[q1 + 4 * u + c1 * LD] * X[q1 + 4 * u];
+        x += __shfl_xor_sync(0xffffffffu, x, 8);
+        x += __shfl_xor_sync(0xffffffffu, x, 16);
+        if (q1 == 0 && c1 < tj.size) {
+            xp[xj + c1] = x;
+            st_relaxed_f64(pb + (int64_t)j * T + c1, x);
         }
-    } else {
+        return;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < NQ; ++a) {
+        const int q = g + 4 * a;
+        if (q < nrhs) X[l + T * q] = l < tj.size ? ypre[a] - acc[a] : TV(0);
+    }
+    __syncthreads();
+    {
         TV x[NQ];
 #pragma unroll
         for (int a = 0; a < NQ; ++a) x[a] = TV(0);
@@ -1105,7 +1152,11 @@ __device__ void bwd_chain_task(int2 tk, const FrontDesc* __restrict__ fronts,
 // the barrier of the poll between).
 // ---------------------------------------------------------------------------
 
-constexpr int kRt1MaxPivotTiles = 4;
+// (fronts of one pivot tile only: with more, one column group of loads in
+// flight per iteration leaves a tail of one memory latency per 16 columns
+// after the last pivot tile, where the staged tile path keeps two 64-column
+// blocks in flight)
+constexpr int kRt1MaxPivotTiles = 1;
 
 struct Rt1Smem {
     double* Ys;  // 2 x T: published slots
@@ -1174,13 +1225,14 @@ __device__ void fwd_update_rt1(int s, int R0, int R1, const FrontDesc& F, double
     if (rv) f[R] = f0 - acc;
 }
 
-// One launch per direction over every level's work items (the item lists,
-// in dependency order, and their kinds are described with the solve
-// schedule): persistent CTAs take items by atomic ticket.  An item only
-// waits for items with lower tickets -- children's and ancestors' fronts sit
-// on earlier levels of the list, a front's earlier pivot tiles and the
-// backward gathers earlier in its level -- and a CTA takes a ticket only
-// while it runs, so every wait is for a CTA that is running or done.
+// One launch per direction over all work items (the item lists, in a
+// topological order by critical-path priority, and their kinds are
+// described with the solve schedule): persistent CTAs take items by atomic
+// ticket.  An item only waits for items with lower tickets -- children's
+// (forward) and parents' (backward) items come earlier in the list, and so
+// do a front's earlier pivot tiles and its backward gathers -- and a CTA
+// takes a ticket only while it runs, so every wait is for a CTA that is
+// running or done.
 // Forward: a front's items wait for its children (the count of finished
 // children), a small front counts itself in at its parent once written, a
 // large front once its last update tile is (a per-front count of finished
@@ -1206,8 +1258,8 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
                 int* __restrict__ err, int* __restrict__ fdone, int* __restrict__ udone,
                 const int64_t* __restrict__ fv_off, const int* __restrict__ amap_off,
                 const int* __restrict__ amap_row, const int* __restrict__ amap_ent,
-                const int64_t* __restrict__ dinv_off, const int* __restrict__ warp_list,
-                const int* __restrict__ warp_cnt, const int* __restrict__ child,
+                const int64_t* __restrict__ dinv_off, const int* __restrict__ wlist,
+                const int* __restrict__ child,
                 const int* __restrict__ relmap, const TL* __restrict__ Ls,
                 const TL* __restrict__ Dinv, TV* __restrict__ xp, TV* __restrict__ fv, int n,
                 int nrhs, int MR) {
@@ -1222,9 +1274,8 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
         const int4 it = items[k];
         if (it.x == SolveScheduleHost::kItemWarps) {
             extern __shared__ __align__(16) unsigned char smem_raw[];
-            const WarpTasks wt{warp_list + it.w, warp_cnt[3 * it.y], warp_cnt[3 * it.y + 1],
-                               warp_cnt[3 * it.y + 2]};
-            const int w = threadIdx.x >> 5, t = it.z + w;
+            const WarpTasks wt{wlist + it.y, it.z & 0xff, (it.z >> 8) & 0xff, it.z >> 16};
+            const int w = threadIdx.x >> 5, t = w;
             TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(MR, nrhs);
             if (t < wt.count()) {
                 if (nrhs == 1)
@@ -1287,8 +1338,8 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
                 int* __restrict__ err, int* __restrict__ bdone, const int* __restrict__ btarget,
                 const int* __restrict__ gather_nch, const int* __restrict__ gather_off,
                 int* __restrict__ gcount, TV* __restrict__ part,
-                const int64_t* __restrict__ dinv_off, const int* __restrict__ warp_list,
-                const int* __restrict__ warp_cnt, const int* __restrict__ rows,
+                const int64_t* __restrict__ dinv_off, const int* __restrict__ wlist,
+                const int* __restrict__ rows,
                 const TL* __restrict__ Ls, const TL* __restrict__ Dinv, TV* __restrict__ xp,
                 int n, int nrhs, int MR) {
     __shared__ int s_item;
@@ -1301,9 +1352,8 @@ __global__ void __launch_bounds__(256, NQ == 1 ? 4 : 2)
         const int4 it = items[k];
         if (it.x == SolveScheduleHost::kItemWarps) {
             extern __shared__ __align__(16) unsigned char smem_raw[];
-            const WarpTasks wt{warp_list + it.w, warp_cnt[3 * it.y], warp_cnt[3 * it.y + 1],
-                               warp_cnt[3 * it.y + 2]};
-            const int w = threadIdx.x >> 5, t = it.z + w;
+            const WarpTasks wt{wlist + it.y, it.z & 0xff, (it.z >> 8) & 0xff, it.z >> 16};
+            const int w = threadIdx.x >> 5, t = w;
             TV* wbuf = reinterpret_cast<TV*>(smem_raw) + w * warp_buf_stride(MR, nrhs);
             if (t < wt.count()) {
                 if (nrhs == 1)
@@ -1438,7 +1488,7 @@ static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* 
         k_fwd_solve<TL, TV, NQ><<<std::min(grid, S.nfwd_items), 256, sm, st>>>(
             D.fronts, S.fwd_items, S.nfwd_items, counters, fv + D.fv_pub_off * nrhs, abort_flag,
             S.err, fdone, udone, D.fv_off, S.amap_off, S.amap_row, S.amap_ent, D.dinv_off,
-            S.warp_list, S.warp_cnt_d, D.child, D.relmap, Ls, Dinv, xp, fv, D.n, nrhs,
+            S.fwd_wlist, D.child, D.relmap, Ls, Dinv, xp, fv, D.n, nrhs,
             kWarpBufRows);
     }
     if (S.nbwd_items > 0) {
@@ -1447,7 +1497,7 @@ static void solve_levels_nq(const DevPlan& D, const TL* Ls, const TL* Dinv, TV* 
             D.fronts, S.bwd_items, S.nbwd_items, counters + 1,
             fv + (D.fv_pub_off + (int64_t)S.nflags * kTile) * nrhs, abort_flag, S.err, bdone,
             S.bwd_target, S.gather_nch, S.gather_off, gcount, fv + D.fv_fronts * nrhs,
-            D.dinv_off, S.warp_list, S.warp_cnt_d, D.rows, Ls, Dinv, xp, D.n, nrhs,
+            D.dinv_off, S.bwd_wlist, D.rows, Ls, Dinv, xp, D.n, nrhs,
             kWarpBufRows);
     }
 }

@@ -132,6 +132,30 @@ int main(int argc, char** argv) {
         bad.push_back({"tasks", c});
     }
     {
+        // the forward item list: a large front's first item swapped with
+        // the last item of one of its children
+        Case c = base;
+        const FrontDesc& f = c.P.fronts[s_piv];
+        if (f.child_end <= f.child_beg) return 7;
+        const int ch = c.P.child[f.child_beg];
+        const std::vector<int>& it = c.Q.fwd_items;
+        int64_t kc = -1, kp = -1;
+        for (int64_t k = 0; k < (int64_t)it.size() / 4; ++k) {
+            const int* e = it.data() + 4 * k;
+            if (e[0] == SolveScheduleHost::kItemWarps) {
+                const int nf = (e[2] & 0xff) + ((e[2] >> 8) & 0xff) + (e[2] >> 16);
+                for (int q = 0; q < nf; ++q)
+                    if (c.Q.fwd_wlist[e[1] + q] == ch) kc = k;
+            } else {
+                if (e[1] == ch) kc = k;
+                if (e[1] == s_piv && kp < 0) kp = k;
+            }
+        }
+        if (kc < 0 || kp < 0 || kc >= kp) return 8;
+        for (int q = 0; q < 4; ++q) std::swap(c.Q.fwd_items[4 * kc + q], c.Q.fwd_items[4 * kp + q]);
+        bad.push_back({"items", c});
+    }
+    {
         Case c = base;
         const int off = c.Q.amap_off[s_piv];
         const int e = c.Q.amap_row[off + c.P.fronts[s_piv].m - 1];  // an entry of a late row

@@ -1,6 +1,6 @@
 """The plan self-check (mdgpu_check_plan, mdgpu_b200/csrc/plan_check.cpp):
 every invariant the device kernels rely on when they index the plan's tables
-holds on the plans of many kinds of input, and each of eleven broken
+holds on the plans of many kinds of input, and each of twelve broken
 invariants is caught and named (tests/plan_check_host.cpp compiles the
 library's own host analysis, plan builders and check with g++).  CPU only.
 """
@@ -53,6 +53,7 @@ EXPECT = {
     "loff": "L panel offset",
     "warp_list": "warp list",
     "tasks": "forward pivot order",
+    "items": "solve items out of dependency order",
     "amap": "assembly map",
     "csr": "CSR entry out of range",
     "level": "child level not below",
