@@ -270,9 +270,10 @@ __device__ __forceinline__ bool settle_slot(double* v, const double* src, int nk
 // accumulates acc = sum_{k < min(i, nt1)} L(i, k) y_k over the pivot tiles.
 // A pivot tile (i0 < nt1, cnt = 1) then solves y_i = inv(L_ii) (f_i - acc)
 // into the solution and publishes it; an update tile leaves f_i - acc in the
-// front vector for the parent.  Threads: r = row in the tile, g = quarter;
-// one right-hand side splits the 64 columns of a block over the quarters,
-// several split the right-hand sides (NQ per thread).
+// front vector for the parent.  Threads: r = row in the tile; one
+// right-hand side splits the 64 columns of a block over four column phases
+// held by lanes of one warp, several split the right-hand sides (NQ per
+// thread).
 template <typename TL, typename TV, int NQ>
 __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
                               double* __restrict__ pub, int* __restrict__ abort_flag,
@@ -285,14 +286,20 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
     static_assert(sizeof(TV) == 8, "solve vectors are double");
     constexpr int T = kTile, LD = blk_ld<TL>();
     const LevelSmem<TL, TV> sm(nrhs);
-    const int tid = threadIdx.x, r = tid & (T - 1), g = tid >> 6;
+    const bool lsplit = nrhs == 1;
+    // one right-hand side: r = row, g = column phase (columns g, g + 4, ...),
+    // the four phases of a row in one warp (rows 8w .. 8w + 7 of warp w), so
+    // a row's sum is two shuffles; several: r = row, g = quarter of the
+    // right-hand sides
+    const int tid = threadIdx.x;
+    const int r = lsplit ? 8 * (tid >> 5) + (tid & 7) : tid & (T - 1);
+    const int g = lsplit ? (tid >> 3) & 3 : tid >> 6;
     const int s = tk.x, i0 = tk.y & 0xffff, cnt = tk.y >> 16;
     const FrontDesc F = fronts[s];
     const int nt1 = tiles_l(F.c, T);
     const bool pivot = i0 < nt1;
     const int kend = pivot ? i0 : nt1;  // L blocks per tile
     const int P = cnt * kend;
-    const bool lsplit = nrhs == 1;
     const TL* L = Ls + F.loff;
     double* pb = pub + (dinv_off[s] / (T * T)) * T * nrhs;  // this front's pivot tiles
     TV* f = front_vec(fv, fv_off, s, nrhs);
@@ -344,8 +351,6 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         acc[j] = TV(0);
     }
     if (cnt > 1) gather_rows(i0 + 1, fnext);
-    // a pivot tile's f_i (one right-hand side) for the solve at the end
-    if (pivot && lsplit && g == 0) sm.Y[r] = fcur[0];
     bool ok = true;
     for (int p = 0; p < P; ++p) {
         issue(p + sm.stg - 1);
@@ -362,7 +367,7 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         if (lsplit) {
 #pragma unroll
             for (int l = 0; l < 16; ++l)
-                acc[0] += (TV)B[db + r + (16 * g + l) * LD] * Yk[16 * g + l];
+                acc[0] += (TV)B[db + r + (g + 4 * l) * LD] * Yk[g + 4 * l];
         } else {
 #pragma unroll 4
             for (int l = 0; l < T; ++l) {
@@ -377,11 +382,9 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
         if (!pivot && k == kend - 1) {  // update tile i complete: f_i - acc to the front vector
             const TileRange ti = tile_range(i, F.m, F.c, T);
             if (lsplit) {
-                sm.red[g * T + r] = acc[0];
-                __syncthreads();
-                if (g == 0 && r < ti.size)
-                    f[ti.start + r] =
-                        fcur[0] - (sm.red[r] + sm.red[T + r] + sm.red[2 * T + r] + sm.red[3 * T + r]);
+                TV v = acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 8);
+                v += __shfl_xor_sync(0xffffffffu, v, 16);
+                if (g == 0 && r < ti.size) f[ti.start + r] = fcur[0] - v;
             } else if (r < ti.size) {
 #pragma unroll
                 for (int j = 0; j < NQ; ++j) {
@@ -403,29 +406,22 @@ __device__ void fwd_tile_task(int2 tk, const FrontDesc* __restrict__ fronts,
     // pivot tile: F = f_i - acc (zero beyond the tile), then y = Dk F
     const TileRange ti = tile_range(i0, F.m, F.c, T);
     TV* Y = sm.Y;
-    TV* red = sm.red;
     const TL* Dk = sm.Dk;
     if (lsplit) {
-        // one right-hand side, two barriers: the quarters' sums, then each
-        // thread forms the 16 entries of F its quarter multiplies (f_i from
-        // sm.Y) and the partial products meet in a stage buffer (free now)
-        red[g * T + r] = acc[0];
+        // one right-hand side, one barrier: the row's phases summed by
+        // shuffles, F into sm.Y, then y = Dk F the same way
+        TV a = acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 8);
+        a += __shfl_xor_sync(0xffffffffu, a, 16);
+        if (g == 0) Y[r] = r < ti.size ? fcur[0] - a : TV(0);
         __syncthreads();
-        TV* red2 = reinterpret_cast<TV*>(sm.lb(0));
         TV y = TV(0);
 #pragma unroll
-        for (int l = 0; l < 16; ++l) {
-            const int x = 16 * g + l;
-            const TV t = x < ti.size ? Y[x] - (red[x] + red[T + x] + red[2 * T + x] + red[3 * T + x])
-                                     : TV(0);
-            y += (TV)Dk[r + x * LD] * t;
-        }
-        red2[g * T + r] = y;
-        __syncthreads();
+        for (int l = 0; l < 16; ++l) y += (TV)Dk[r + (g + 4 * l) * LD] * Y[g + 4 * l];
+        y += __shfl_xor_sync(0xffffffffu, y, 8);
+        y += __shfl_xor_sync(0xffffffffu, y, 16);
         if (g == 0 && r < ti.size) {
-            const TV v = red2[r] + red2[T + r] + red2[2 * T + r] + red2[3 * T + r];
-            xp[F.first_col + ti.start + r] = v;
-            st_relaxed_f64(pb + (int64_t)i0 * T + r, v);
+            xp[F.first_col + ti.start + r] = y;
+            st_relaxed_f64(pb + (int64_t)i0 * T + r, y);
         }
         return;
     }
