@@ -45,7 +45,7 @@ CPU_BASELINE_SIDE = 42  # about 15 s of single-core reference work
 # class's algorithmic bytes of one profiled 48^3 step.  The roofline line
 # scales the class's algorithmic bytes per launch at the bench size by it
 # (traffic grows with the units processed).
-TRAFFIC_PER_ALGO_BYTE = {"panel": 0.73, "schur_update": 0.70, "solve_large": 1.06,
+TRAFFIC_PER_ALGO_BYTE = {"panel": 0.79, "schur_update": 0.78, "solve_large": 1.06,
                          "solve_small": 1.06, "small_front": 1.01, "assemble": 0.53}
 # the kernels behind each profiler class (one class launch = one timed group)
 CLASS_KERNELS = {
