@@ -3,8 +3,8 @@ and d(log det A + b' A^-1 b)/d Ax for the caller's lower-triangle values.
 
 Checked against dense FP64 (numpy inverse and slogdet) on small 2D / 3D
 grids (supernodal and relaxed trees, fronts above 160 rows included), by
-central finite differences on single entries, and through the torch
-autograd front-end.  The oracle's Takahashi restatement is itself checked
+central finite differences on single entries, against a reference gradient
+by FP64 solves on a 32^3 grid, and through the torch autograd front-end.  The oracle's Takahashi restatement is itself checked
 against the dense inverse on the CPU.
 """
 import numpy as np
@@ -81,6 +81,44 @@ def test_logdet_and_gradient_match_dense(name, gen, tree, z):
     # twice in a row, and from device vectors: the same numbers
     dG = S.grad_lower(torch.from_numpy(x).cuda()).cpu().numpy()
     np.testing.assert_array_equal(dG, G)
+
+
+@pytest.mark.gpu
+def test_theta_gradient_matches_a_solve_reference_at_32_cubed():
+    """d loss / d theta_e (loss = log det A + b' A^-1 b, edge conductances
+    theta lognormal(0, 1) on a 32^3 grid, shift 1e-2) from the selected
+    inverse, against an FP64 reference gradient on 64 random edges computed
+    by solves instead: u' A^-1 u - (x_i - x_j)^2 with u = e_i - e_j.  The grid
+    is too large for a dense gradient, and central differences lose digits to
+    the size of the loss; the two FP64 routes agree to 1e-8 relative."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    n, Ap, Ai, Ax, lo, hi, cond = mg.laplacian_grid_edges((32,) * 3, seed=3, sigma=1.0,
+                                                          shift=1e-2)
+    S = M.Solver(n, Ap, Ai)
+    assert np.diff(S.array("rows_ptr")).max() > 1000  # tiled large fronts on the path
+    S.factor(Ax, M.FP64)
+    b = mg.rhs_uniform(n, seed=4)
+    x = S.solve(b)
+    S.selinv()
+    G = S.grad_lower(x)
+
+    def pos(r, c):
+        seg = Ai[Ap[c]:Ap[c + 1]]
+        return Ap[c] + int(np.searchsorted(seg, r))
+
+    picked = np.random.default_rng(5).choice(len(cond), 64, replace=False)
+    U = np.zeros((n, len(picked)))
+    U[lo[picked], np.arange(len(picked))] = 1.0
+    U[hi[picked], np.arange(len(picked))] = -1.0
+    Zu = S.solve(U)
+    g = np.array([G[pos(lo[e], lo[e])] + G[pos(hi[e], hi[e])] - G[pos(hi[e], lo[e])]
+                  for e in picked])
+    gref = np.array([Zu[lo[e], k] - Zu[hi[e], k] - (x[lo[e]] - x[hi[e]]) ** 2
+                     for k, e in enumerate(picked)])
+    err = np.abs(g - gref) / np.maximum(np.abs(gref), 1e-6 * np.abs(gref).max())
+    assert err.max() <= 1e-8, (err.max(), int(np.argmax(err)))
 
 
 @pytest.mark.gpu
