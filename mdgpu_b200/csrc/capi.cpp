@@ -755,8 +755,7 @@ int do_refine(mdgpu_handle_s* h, const double* dB, int ldb, double* dX, int ldx,
         }
         if (done || it >= maxit) break;
         do_solve(h, h->d_R, n, h->d_D, n, nrhs, st);
-        for (int q = 0; q < nrhs; ++q)
-            launch_axpy(n, h->d_D + (int64_t)q * n, dX + (int64_t)q * ldx, st);
+        launch_axpy(n, nrhs, h->d_D, dX, ldx, st);
     }
     if (berr) std::copy(be.begin(), be.end(), berr);
     if (iters) *iters = it;

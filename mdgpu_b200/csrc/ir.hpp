@@ -22,7 +22,7 @@ void launch_residual(const SymCsr& A, const double* Ax, const double* x, int ldx
 void launch_anorm(const SymCsr& A, const double* Ax, unsigned long long* out, cudaStream_t st);
 void launch_absmax3(int n, int nrhs, const double* r, int ldr, const double* x, int ldx,
                     const double* b, int ldb, unsigned long long* out, cudaStream_t st);
-void launch_axpy(int64_t len, const double* d, double* x, cudaStream_t st);
+void launch_axpy(int n, int nrhs, const double* d, double* x, int ldx, cudaStream_t st);
 
 // GMRES-IR vector operations: w = A v; out[i] = <V(:, i), w> for i < k
 // (deterministic two-stage sums; partial holds dots_partial_size(k) values);

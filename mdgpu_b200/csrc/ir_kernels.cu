@@ -3,7 +3,12 @@
 // The residual r = b - A x uses the caller's ORIGINAL matrix (lower triangle,
 // CSC) through a full symmetric CSR pattern built once on the host whose
 // entries point back into the caller's value array, so no permuted copy of
-// the values is ever made.  One warp per row, deterministic.
+// the values is ever made.  One thread per (row, right-hand side), the row's
+// entries summed in their CSR order: the rows of the 3D grids have about
+// seven entries, too few to spread over a warp, and consecutive threads take
+// consecutive rows of one right-hand side, so their index and value loads
+// fall together.  Deterministic.
+#include <algorithm>
 #include <cstdint>
 
 #include "ir.hpp"
@@ -14,17 +19,14 @@ __global__ void k_residual(int n, int nrhs, const int* __restrict__ rowptr,
                            const int* __restrict__ col, const int* __restrict__ src,
                            const double* __restrict__ Ax, const double* __restrict__ x, int ldx,
                            const double* __restrict__ b, int ldb, double* __restrict__ r, int ldr) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = warp; row < (int64_t)n * nrhs; row += nwarps) {
-        int q = (int)(row / n), i = (int)(row - (int64_t)q * n);
+    const int64_t total = (int64_t)n * nrhs;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t / n), i = (int)(t - (int64_t)q * n);
         const double* xq = x + (int64_t)q * ldx;
         double acc = 0;
-        for (int p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) acc += Ax[src[p]] * xq[col[p]];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) r[i + (int64_t)q * ldr] = b[i + (int64_t)q * ldb] - acc;
+        for (int p = rowptr[i], pe = rowptr[i + 1]; p < pe; ++p) acc += Ax[src[p]] * xq[col[p]];
+        r[i + (int64_t)q * ldr] = b[i + (int64_t)q * ldb] - acc;
     }
 }
 
@@ -46,54 +48,65 @@ __global__ void k_row_abs_sum_max(int n, const int* __restrict__ rowptr,
     if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
 }
 
-// per right-hand side q: out[3q+0] = max|r|, out[3q+1] = max|x|, out[3q+2] = max|b|
-__global__ void k_absmax3(int n, int nrhs, const double* __restrict__ r, int ldr,
-                          const double* __restrict__ x, int ldx, const double* __restrict__ b,
-                          int ldb, unsigned long long* __restrict__ out) {
-    for (int q = 0; q < nrhs; ++q) {
-        double m0 = 0, m1 = 0, m2 = 0;
-        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-             i += (int64_t)gridDim.x * blockDim.x) {
-            m0 = fmax(m0, fabs(r[i + (int64_t)q * ldr]));
-            m1 = fmax(m1, fabs(x[i + (int64_t)q * ldx]));
-            m2 = fmax(m2, fabs(b[i + (int64_t)q * ldb]));
-        }
+// per right-hand side q = blockIdx.y: out[3q+0] = max|r|, out[3q+1] =
+// max|x|, out[3q+2] = max|b|; each block reduces its rows in shared memory
+// and adds three atomics
+__global__ void __launch_bounds__(256) k_absmax3(int n, const double* __restrict__ r, int ldr,
+                                                 const double* __restrict__ x, int ldx,
+                                                 const double* __restrict__ b, int ldb,
+                                                 unsigned long long* __restrict__ out) {
+    __shared__ double red[3][8];
+    const int q = blockIdx.y;
+    const double* rq = r + (int64_t)q * ldr;
+    const double* xq = x + (int64_t)q * ldx;
+    const double* bq = b + (int64_t)q * ldb;
+    double m0 = 0, m1 = 0, m2 = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        m0 = fmax(m0, fabs(rq[i]));
+        m1 = fmax(m1, fabs(xq[i]));
+        m2 = fmax(m2, fabs(bq[i]));
+    }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
-            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
-            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicMax(out + 3 * q + 0, (unsigned long long)__double_as_longlong(m0));
-            atomicMax(out + 3 * q + 1, (unsigned long long)__double_as_longlong(m1));
-            atomicMax(out + 3 * q + 2, (unsigned long long)__double_as_longlong(m2));
-        }
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+        m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[0][warp] = m0, red[1][warp] = m1, red[2][warp] = m2;
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[threadIdx.x][w]);
+        atomicMax(out + 3 * q + threadIdx.x, (unsigned long long)__double_as_longlong(m));
     }
 }
 
-__global__ void k_axpy(int64_t len, const double* __restrict__ d, double* __restrict__ x) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
-         i += (int64_t)gridDim.x * blockDim.x)
-        x[i] += d[i];
+// x(:, q) += d(:, q) for every right-hand side q (d: n x nrhs, leading
+// dimension n; x: leading dimension ldx)
+__global__ void k_axpy(int n, int nrhs, const double* __restrict__ d, double* __restrict__ x,
+                       int ldx) {
+    const int64_t total = (int64_t)n * nrhs;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t / n), i = (int)(t - (int64_t)q * n);
+        x[i + (int64_t)q * ldx] += d[t];
+    }
 }
 
 // ---- GMRES-IR vector operations (one right-hand side) ----
 
-// w = A v with the caller's FP64 values, one warp per row (the residual's
-// access pattern without b)
+// w = A v with the caller's FP64 values, one thread per row (the
+// residual's access pattern without b)
 __global__ void k_spmv(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
                        const int* __restrict__ src, const double* __restrict__ Ax,
                        const double* __restrict__ v, double* __restrict__ w) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < n; i += nwarps) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
         double acc = 0;
-        for (int p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) acc += Ax[src[p]] * v[col[p]];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) w[i] = acc;
+        for (int p = rowptr[i], pe = rowptr[i + 1]; p < pe; ++p) acc += Ax[src[p]] * v[col[p]];
+        w[i] = acc;
     }
 }
 
@@ -157,7 +170,7 @@ static int grid_for(int64_t work, int per_block) {
 
 void launch_residual(const SymCsr& A, const double* Ax, const double* x, int ldx,
                      const double* b, int ldb, double* r, int ldr, int nrhs, cudaStream_t st) {
-    k_residual<<<grid_for((int64_t)A.n * nrhs * 32, 256), 256, 0, st>>>(
+    k_residual<<<grid_for((int64_t)A.n * nrhs, 256), 256, 0, st>>>(
         A.n, nrhs, A.rowptr, A.col, A.src, Ax, x, ldx, b, ldb, r, ldr);
 }
 
@@ -170,16 +183,24 @@ void launch_anorm(const SymCsr& A, const double* Ax, unsigned long long* out, cu
 void launch_absmax3(int n, int nrhs, const double* r, int ldr, const double* x, int ldx,
                     const double* b, int ldb, unsigned long long* out, cudaStream_t st) {
     cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long) * nrhs, st);
-    k_absmax3<<<grid_for(n, 256), 256, 0, st>>>(n, nrhs, r, ldr, x, ldx, b, ldb, out);
+    // about four blocks per SM over all right-hand sides, at most one per 256
+    // rows; grid rows of at most 65535 right-hand sides
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256,
+                                                                (148 * 4 + nrhs - 1) / nrhs));
+    for (int q0 = 0; q0 < nrhs; q0 += 65535) {
+        const int nq = std::min(65535, nrhs - q0);
+        k_absmax3<<<dim3(gx, nq), 256, 0, st>>>(n, r + (int64_t)q0 * ldr, ldr,
+                                                x + (int64_t)q0 * ldx, ldx,
+                                                b + (int64_t)q0 * ldb, ldb, out + 3 * (int64_t)q0);
+    }
 }
 
-void launch_axpy(int64_t len, const double* d, double* x, cudaStream_t st) {
-    k_axpy<<<grid_for(len, 256), 256, 0, st>>>(len, d, x);
+void launch_axpy(int n, int nrhs, const double* d, double* x, int ldx, cudaStream_t st) {
+    k_axpy<<<grid_for((int64_t)n * nrhs, 256), 256, 0, st>>>(n, nrhs, d, x, ldx);
 }
 
 void launch_spmv(const SymCsr& A, const double* Ax, const double* v, double* w, cudaStream_t st) {
-    k_spmv<<<grid_for((int64_t)A.n * 32, 256), 256, 0, st>>>(A.n, A.rowptr, A.col, A.src, Ax, v,
-                                                            w);
+    k_spmv<<<grid_for(A.n, 256), 256, 0, st>>>(A.n, A.rowptr, A.col, A.src, Ax, v, w);
 }
 
 int dots_partial_size(int kmax) { return kmax * kDotBlocks; }
