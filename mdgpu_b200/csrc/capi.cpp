@@ -167,9 +167,11 @@ struct mdgpu_handle_s {
                         (void*)dD64, (void*)dD32,
                         (void*)d_xp, (void*)d_fv, (void*)d_B, (void*)d_X, (void*)d_R, (void*)d_D})
             if (p) cudaFree(p);
+        for (int i = 0; i < DevPlan::kSmallPieces; ++i) {
+            if (D.piece_join[i]) cudaEventDestroy(D.piece_join[i]);
+            if (D.piece_st[i]) cudaStreamDestroy(D.piece_st[i]);
+        }
         if (D.fork_ev) cudaEventDestroy(D.fork_ev);
-        if (D.join_ev) cudaEventDestroy(D.join_ev);
-        if (D.aux) cudaStreamDestroy(D.aux);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -270,9 +272,11 @@ void upload_plan(mdgpu_handle_s* h, bool check = false) {
     }
     h->on_device = true;
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
-    ck(cudaStreamCreateWithFlags(&h->D.aux, cudaStreamNonBlocking), "stream");
     ck(cudaEventCreateWithFlags(&h->D.fork_ev, cudaEventDisableTiming), "event");
-    ck(cudaEventCreateWithFlags(&h->D.join_ev, cudaEventDisableTiming), "event");
+    for (int i = 0; i < DevPlan::kSmallPieces; ++i) {
+        ck(cudaStreamCreateWithFlags(&h->D.piece_st[i], cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreateWithFlags(&h->D.piece_join[i], cudaEventDisableTiming), "event");
+    }
     const Plan& P = h->plan;
     DevPlan& D = h->D;
     D.n = P.n;

@@ -556,12 +556,15 @@ static size_t diag_smem() {
     return (size_t)2 * kTile * kPotrfLD * sizeof(T);
 }
 
+// The level's small fronts in pieces, piece i on sts[i]: the tiny fronts
+// (piece 0), then one k_small_front launch per size bucket.
 template <typename T>
 void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double* Ax,
-                         int* status, cudaStream_t st) {
+                         int* status, const cudaStream_t* sts) {
     {  // fronts of at most 32 rows (the first two buckets): one, two or four per warp
         const int beg = D.h_small_ptr[level * kSmallBuckets];
         const int end = D.h_small_ptr[level * kSmallBuckets + Plan::kTinyBuckets];
+        const cudaStream_t st = sts[0];
         if (end > beg) {
             double by = 0;
             for (int b = 0; b < Plan::kTinyBuckets; ++b)
@@ -589,6 +592,7 @@ void launch_small_fronts(const DevPlan& D, int level, T* Ls, T* Us, const double
         int LD = MB + 1;
         size_t smem = (size_t)MB * LD * sizeof(T) + (size_t)MB * sizeof(int);
         const int threads = D.small_threads[b];
+        const cudaStream_t st = sts[1 + b - Plan::kTinyBuckets];
         ProfScope ps(D.prof, KC_SMALL_FRONT, st, 0,
                      D.h_small_bytes[level * kSmallBuckets + b] * sizeof(T) / 8.0);
         k_small_front<T><<<end - beg, threads, smem, st>>>(D.fronts, D.small_list + beg, D.child,
@@ -737,27 +741,42 @@ void init_factor_kernels() {
 }
 
 // Level by level.  A level's small and large fronts depend only on lower
-// levels, so where a level has both, its small fronts run on the second
-// stream beside the large fronts (fork and join by events; inside a stream
-// capture these become parallel graph branches).  Serial while the profiler
-// records, so each class keeps its own time.
+// levels, so its small fronts run beside its large fronts, each piece (the
+// tiny fronts, each k_small_front size bucket) on a stream of its own (fork
+// and join by events; inside a stream capture these become parallel graph
+// branches).  Serial while the profiler records, so each class keeps its own
+// time.
 template <typename T>
 void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, int* status,
                    cudaStream_t st, int smode) {
-    const bool fork = D.aux && D.fork_ev && D.join_ev && !(D.prof && D.prof->on);
+    const bool fork = D.fork_ev && !(D.prof && D.prof->on);
     if (D.fsync && D.nfsync > 0) cudaMemsetAsync(D.fsync, 0, (size_t)D.nfsync * sizeof(int), st);
     for (int l = 0; l < D.nlevels; ++l) {
         const bool has_small =
             D.h_small_ptr[(l + 1) * kSmallBuckets] > D.h_small_ptr[l * kSmallBuckets];
         const bool has_large = D.h_large_ptr[l + 1] > D.h_large_ptr[l];
-        const bool par = fork && has_small && has_large;
+        // pieces of the level's small fronts that have fronts
+        bool piece[DevPlan::kSmallPieces];
+        int npieces = 0;
+        piece[0] = D.h_small_ptr[l * kSmallBuckets + Plan::kTinyBuckets] >
+                   D.h_small_ptr[l * kSmallBuckets];
+        for (int b = Plan::kTinyBuckets; b < kSmallBuckets; ++b)
+            piece[1 + b - Plan::kTinyBuckets] =
+                D.h_small_ptr[l * kSmallBuckets + b + 1] > D.h_small_ptr[l * kSmallBuckets + b];
+        for (int i = 0; i < DevPlan::kSmallPieces; ++i) npieces += piece[i];
+        const bool par = fork && D.piece_st[0] && has_small && (has_large || npieces > 1);
         if (par) {
+            // every piece on its own stream beside the large fronts
             cudaEventRecord(D.fork_ev, st);
-            cudaStreamWaitEvent(D.aux, D.fork_ev, 0);
-            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, D.aux);
-            cudaEventRecord(D.join_ev, D.aux);
+            for (int i = 0; i < DevPlan::kSmallPieces; ++i)
+                if (piece[i]) cudaStreamWaitEvent(D.piece_st[i], D.fork_ev, 0);
+            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, D.piece_st);
+            for (int i = 0; i < DevPlan::kSmallPieces; ++i)
+                if (piece[i]) cudaEventRecord(D.piece_join[i], D.piece_st[i]);
         } else {
-            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, st);
+            cudaStream_t serial[DevPlan::kSmallPieces];
+            for (int i = 0; i < DevPlan::kSmallPieces; ++i) serial[i] = st;
+            launch_small_fronts<T>(D, l, Ls, Us, Ax, status, serial);
         }
         // FP32 needs the TMA descriptors of the tensor-core path; without them
         // (descriptor encoding unavailable) it keeps the 64-wide tile schedule
@@ -765,7 +784,9 @@ void factor_levels(const DevPlan& D, T* Ls, T* Us, T* Dinv, const double* Ax, in
             launch_large_level_panels<T>(D, l, Ls, Us, Dinv, Ax, status, smode, st);
         else
             launch_large_level<T>(D, l, Ls, Us, Dinv, Ax, status, st);
-        if (par) cudaStreamWaitEvent(st, D.join_ev, 0);
+        if (par)
+            for (int i = 0; i < DevPlan::kSmallPieces; ++i)
+                if (piece[i]) cudaStreamWaitEvent(st, D.piece_join[i], 0);
     }
 }
 

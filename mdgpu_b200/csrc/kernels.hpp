@@ -161,10 +161,14 @@ struct DevPlan {
     // bucket
     int tiny_blocks_cap = 148 * 8;
     int small_threads[kSmallBuckets] = {64, 128, 256, 256, 256, 256};
-    // a second stream and two events: the factor runs a level's small fronts
-    // beside its large fronts (both depend only on lower levels)
-    cudaStream_t aux = nullptr;
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // the factor runs a level's small fronts beside its large fronts (both
+    // depend only on lower levels), and the small fronts' pieces (the tiny
+    // fronts, then each k_small_front size bucket) beside one another: a
+    // fork event, and a stream and a join event per piece
+    cudaEvent_t fork_ev = nullptr;
+    static constexpr int kSmallPieces = 1 + kSmallBuckets - Plan::kTinyBuckets;
+    cudaStream_t piece_st[kSmallPieces] = {};
+    cudaEvent_t piece_join[kSmallPieces] = {};
     int max_u = 0;  // largest update-matrix order (child relative maps in shared memory)
     int max_m_large = 0, max_nch_large = 0;  // largest large front, most children of one
     std::vector<int> h_level_max_m;          // per level: largest large front
