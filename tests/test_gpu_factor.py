@@ -153,3 +153,37 @@ def test_fp32_tensor_core_factor_close_to_reference(side):
     x, berr, iters = S.refine(b, tol=1e-14, maxit=30)
     assert berr[0] <= 1e-14
     assert O.residual(n, Ap, Ai, Ax, x, b) <= 1e-14
+
+
+@pytest.mark.parametrize("prec", [M.FP32, M.FP64], ids=["fp32", "fp64"])
+def test_refine_device_with_padded_leading_dimensions(prec):
+    """Refinement on device arrays whose columns are longer than n (leading
+    dimensions n + 3 for B and n + 5 for X, five right-hand sides): the same
+    numbers as the host-buffer entry point (the residual, the max-norms and
+    the column updates take their leading dimensions from the caller), the
+    padding rows left as they were, and a backward error below 1e-14 by the
+    host's own product with A."""
+    from scipy.sparse.linalg import norm as sparse_norm
+
+    n, Ap, Ai, Ax = mg.laplacian_3d_varcoef(12, seed=6)
+    S = M.Solver(n, Ap, Ai)
+    S.factor(Ax, prec)
+    k = 5
+    B = mg.rhs_uniform(n, seed=7, nrhs=k).reshape(n, k)
+    xh, berr_h, it_h = S.refine(B)
+    bbig = torch.full((k, n + 3), 7.0, dtype=torch.float64, device="cuda")
+    xbig = torch.full((k, n + 5), float("nan"), dtype=torch.float64, device="cuda")
+    dB = bbig.t()[:n]
+    dX = xbig.t()[:n]
+    dB.copy_(torch.from_numpy(B))
+    berr_d, it_d = S.refine_device(dB, dX)
+    torch.cuda.synchronize()
+    x = dX.cpu().numpy()
+    assert it_d == it_h
+    np.testing.assert_array_equal(x, xh)
+    np.testing.assert_array_equal(berr_d, berr_h)
+    assert torch.isnan(xbig[:, n:]).all() and (bbig[:, n:] == 7.0).all()
+    A = mg.lower_to_full_scipy(n, Ap, Ai, Ax)
+    r = B - A @ x
+    den = sparse_norm(A, np.inf) * np.abs(x).max(axis=0) + np.abs(B).max(axis=0)
+    assert (np.abs(r).max(axis=0) / den).max() <= 1e-14
