@@ -88,7 +88,39 @@ def parse():
                          "elasticity: 3 unknowns per node on a 40^3 27-point node grid, "
                          "BF16-update factor + GMRES-IR vs FP32 + GMRES-IR vs FP32 + plain "
                          "refinement vs FP64")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="default run: skip the adjoint and elasticity workloads that a "
+                         "single-GPU run carries in its line under 'workloads'")
     return ap.parse_args()
+
+
+# The adjoint (48^3) and 3-unknowns-per-node (40^3 nodes) workloads: a
+# default single-GPU run also runs them, each as a child process of its own
+# mode, and carries their lines under "workloads"; a child that fails or runs
+# past its time limit leaves an "error" entry instead and never stops the
+# bench.
+SUB_WORKLOADS = (("adjoint", ["--workload", "adjoint", "--steps", "3", "--warmup", "3"]),
+                 ("elasticity", ["--workload", "elasticity", "--steps", "3", "--warmup", "3"]))
+
+
+def run_sub_workloads(workloads=SUB_WORKLOADS, timeout_s=300.0, script=None):
+    script = script or os.path.abspath(__file__)
+    out = {}
+    for name, extra in workloads:
+        t0 = time.perf_counter()
+        try:
+            p = subprocess.run([sys.executable, script] + list(extra), capture_output=True,
+                               text=True, timeout=timeout_s, cwd=ROOT)
+            lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+            if p.returncode == 0 and lines:
+                res = json.loads(lines[-1])
+            else:
+                res = {"error": "exit %d: %s" % (p.returncode, (p.stderr or p.stdout)[-300:])}
+        except Exception as e:  # noqa: BLE001 - a timeout or a bad line is recorded
+            res = {"error": str(e)[:300]}
+        res["wall_s"] = time.perf_counter() - t0
+        out[name] = res
+    return out
 
 
 def workload(side):
@@ -652,6 +684,11 @@ def run_gpu_arm(args):
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = reference_cpu_sample(CPU_BASELINE_SIDE)
+    if not args.no_workloads and world == 1 and args.side == 64:
+        try:
+            line["workloads"] = run_sub_workloads()
+        except Exception as e:  # noqa: BLE001 - never lose the line
+            line["workloads"] = {"error": str(e)[:300]}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
